@@ -1,0 +1,355 @@
+"""Benchmark: Louvain edges/s per pass (and final Q) on the power-law
+co-purchase-like workload (334,863 vertices, ~925k undirected unit-weight
+edges, Chung-Lu degrees exponent 2.3 / max 550, planted communities mu=0.3,
+seed 0, min gain 1e-6), on 1..N B200s.
+
+One step = one complete Louvain run (every level until the first pass of a
+phase gains less than min gain).  edges/s per pass = sum over passes of the
+pass's stored adjacency entries / time.
+
+  value      inputs resident in HBM (lv_run_device), device time of K steps
+             measured with CUDA events on the engine's stream, L2 flushed
+             (256 MB write) between steps outside the timed events
+  e2e        same metric through the C ABI with host buffers (lv_run +
+             lv_get_assignment: CSR upload and assignment download inside)
+  roofline   the kernel group with the largest device time in the timed
+             steps: algorithmic bytes / its CUDA-event time, against the
+             measured HBM copy bandwidth
+  cpu_baseline  the reference's CPU path (louvian.py restated in C by the
+             oracle, FP64, single thread) on the same graph
+N > 1 (torchrun): every rank runs its own replica (the single-graph path
+does not shard); value = edges of all ranks / max-over-ranks time.
+--impl reference: the reference's CPU implementation (oracle port) alone.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "louvain-community-detection_b200", "python"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import numpy as np  # noqa: E402
+
+import lvgen  # noqa: E402
+
+METRIC = "Louvain edges/s per pass & final Q; batched graphs/s & p99 vs plain, 1 B200"
+UNIT = "edges/s"
+MIN_GAIN = 1e-6
+
+
+def workload(name: str):
+    if name == "powerlaw":
+        n, s, d, w = lvgen.planted_powerlaw(seed=0)
+        desc = {"workload": "planted power-law co-purchase-like graph",
+                "n_vertices": n, "gamma": 2.3, "max_degree": 550, "mu": 0.3,
+                "weights": "unit FP32", "seed": 0}
+    elif name == "banded":
+        n, s, d, w = lvgen.banded_fem(seed=0)
+        desc = {"workload": "banded FEM-like matrix", "n_vertices": n,
+                "half_band": 60, "weights": "U(0.1,1.0) FP32", "seed": 0}
+    elif name.startswith("rmat"):
+        scale = int(name[4:])
+        n, s, d, w = lvgen.rmat(scale, seed=0)
+        desc = {"workload": f"R-MAT scale {scale}", "n_vertices": n,
+                "abcd": [0.57, 0.19, 0.19, 0.05], "weights": "unit FP32", "seed": 0}
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    off, col, ww = lvgen.csr_from_edges(n, s, d, w)
+    desc.update({"n_edges": int(len(s)), "n_entries": int(len(col)),
+                 "min_gain": MIN_GAIN, "rule": "louvian.py (max_gain > 0)"})
+    return n, off, col, ww, desc
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (200 ms period)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                 "-lms", "200", "-i", self.gpu_id],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1].split()[0]))
+                smax = float(parts[2].split()[0])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_group: str):
+    """DRAM bytes per launch of a kernel group from the committed ncu
+    summary (profiles/ncu_traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d.get(kernel_group, {}).get("dram_bytes_per_launch")
+
+
+def cpu_baseline(n, off, col, ww, budget_s=12.0):
+    """The reference's CPU path (louvian.py's algorithm, restated in C by the
+    oracle: FP64, first-seen row order), single thread, on the same graph,
+    repeated until about `budget_s` seconds of CPU work."""
+    import pyoracle
+
+    g = pyoracle.CSR(n, off, col, ww.astype(np.float64))
+    runs, t_tot, edges = 0, 0.0, 0
+    q = None
+    while t_tot < budget_s or runs == 0:
+        t0 = time.perf_counter()
+        r = pyoracle.louvain(g, MIN_GAIN, rule="py", prec="fp64", rows="first_seen")
+        t_tot += time.perf_counter() - t0
+        edges += sum(l.passes * l.n_entries for l in r.levels)
+        q = r.q
+        runs += 1
+        if runs >= 50:
+            break
+    return {"value": edges / t_tot, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"full workload, {runs} complete runs ({t_tot:.1f} s)",
+            "final_q": q}
+
+
+def run_reference(args, rank, world):
+    n, off, col, ww, desc = workload(args.workload)
+    if rank != 0:
+        return
+    import pyoracle
+
+    g = pyoracle.CSR(n, off, col, ww.astype(np.float64))
+    for _ in range(args.warmup):
+        pyoracle.louvain(g, MIN_GAIN, rule="py", prec="fp64", rows="first_seen")
+    times, edges, q = [], 0, None
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r = pyoracle.louvain(g, MIN_GAIN, rule="py", prec="fp64", rows="first_seen")
+        times.append(time.perf_counter() - t0)
+        edges += sum(l.passes * l.n_entries for l in r.levels)
+        q = r.q
+    total = sum(times)
+    value = edges / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(desc, parallelism="replicas only (1 CPU thread)",
+                       l2="n/a (CPU)"),
+        "final_q": q,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                         "sample": f"full workload, {args.steps} timed runs"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_engine(args, rank, world):
+    import torch
+
+    import lvb200
+
+    torch.cuda.set_device(rank % max(torch.cuda.device_count(), 1))
+    dev = torch.cuda.current_device()
+    n, off, col, ww, desc = workload(args.workload)
+    nnz = len(col)
+    stream = torch.cuda.Stream()
+    d_off = torch.from_numpy(off.view(np.int64)).cuda()
+    d_col = torch.from_numpy(col.view(np.int32)).cuda()
+    d_w = torch.from_numpy(ww).cuda()
+    d_asg = torch.empty(n, dtype=torch.int32, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB
+    torch.cuda.synchronize()
+    eng = lvb200.Engine(device=dev, rule="py", stream=stream.cuda_stream)
+
+    def step():
+        return eng.run_device(n, nnz, d_off.data_ptr(), d_col.data_ptr(),
+                              d_w.data_ptr(), MIN_GAIN, d_asg.data_ptr())
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        props = torch.cuda.get_device_properties(dev)
+        gpu_id = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(dev)
+        eng.set_profiling(True)
+        eng.reset_kernel_stats()
+        launches0 = lvb200.launch_count()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+        edges, q, levels = 0, None, None
+        with ClockSampler(gpu_id) as clocks:
+            for i in range(args.steps):
+                flush.zero_()  # evict the previous step's working set from L2
+                ev[i][0].record(stream)
+                r = step()
+                ev[i][1].record(stream)
+                edges += r.edges_processed
+                q = r.modularity
+            torch.cuda.synchronize()
+        launches = lvb200.launch_count() - launches0
+        eng.set_profiling(False)
+        kstats = eng.kernel_stats()
+        levels = eng.levels()
+        ms = sum(a.elapsed_time(b) for a, b in ev)
+        if world > 1:
+            torch.distributed.barrier()
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e = torch.tensor([edges], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(e)
+            ms, edges_all = float(t.item()), float(e.item())
+        else:
+            edges_all = float(edges)
+        value = edges_all / (ms / 1000.0)
+
+        # e2e: host buffers through lv_run (+ assignment download)
+        g = lvb200.Graph.from_csr(n, off, col, ww)
+        e2e_times, e2e_edges = [], 0
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rr = eng.run(g, MIN_GAIN)  # includes lv_get_assignment
+            e2e_times.append(time.perf_counter() - t0)
+            e2e_edges += rr.edges_processed
+        e2e_value = e2e_edges / sum(e2e_times)
+        if world > 1:
+            t = torch.tensor([e2e_value], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(t)  # replicas: throughputs add up
+            e2e_value = float(t.item())
+
+    eng.close()
+    if rank != 0:
+        return
+    # roofline of the dominant kernel group
+    peak, peak_kind = measured_peak()
+    dom = max(kstats.items(), key=lambda kv: kv[1]["total_ms"])
+    name, st = dom
+    launches_k = max(st["launches"], 1)
+    achieved = (st["bytes"] / launches_k) / (st["total_ms"] / launches_k / 1000.0) / 1e9
+    traffic = ncu_traffic(name)
+    cpu = cpu_baseline(n, off, col, ww) if world == 1 else None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": dict(desc, parallelism="replicas only" if world > 1 else "single GPU",
+                       l2="flushed (256 MB write) between timed steps"),
+        "final_q": q,
+        "levels": [{"V": l["n_vertices"], "E": l["n_entries"], "passes": l["passes"]}
+                   for l in levels],
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": int((n + 1) * 8 + nnz * 8),
+                "d2h_bytes_per_step": int(n * 4)},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind,
+                     "traffic": traffic,
+                     "bytes_per_launch": st["bytes"] / launches_k,
+                     "ms_per_launch": st["total_ms"] / launches_k},
+        "kernel_ms": {k: round(v["total_ms"], 4) for k, v in kstats.items()},
+        "clocks": clocks.summary(),
+    }
+    if cpu:
+        line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind",
+                                                    "sample")}
+        line["cpu_baseline"]["final_q"] = cpu["final_q"]
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="powerlaw")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    if world > 1 and args.impl == "b200":
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group(
+            "nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_engine(args, local if world > 1 else 0, world)
+    finally:
+        if world > 1 and args.impl == "b200":
+            import torch
+
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,229 @@
+/*
+ * louvain_b200.h -- C ABI of the B200 Louvain engine.
+ *
+ * Plain C types only (no CUDA or torch types): pointers, sizes, status
+ * codes.  Every entry point returns an lv_status and never exits the
+ * process; lv_last_error() gives the message of the calling thread's last
+ * failure.
+ *
+ * Reference interfaces replaced (upicine/louvain-community-detection):
+ *   parseGraph            utils.cu:168-229   -> lv_graph_load_mtx
+ *   initHostGraph         utils.cu:13-28     -> lv_graph_from_edges / _csr
+ *   initDevGraph+copyToDevice+initCommAggr+setInitComm
+ *                         utils.cu:66-108    -> lv_engine_load
+ *   modularityOptimization modularity.cu:438-520 / modularity.cuh:6
+ *                                            -> lv_phase_move
+ *   aggregation           aggregation.cu:387-462 / aggregation.cuh:6
+ *                                            -> lv_phase_aggregate
+ *   main's phase loop     main.cu:43-48      -> lv_run / lv_run_device
+ *   computeModularity     modularity.cu:428-436 -> lv_modularity_fp64
+ *   printCommunities      utils.cu:270-293   -> lv_get_assignment
+ *   deleteDevGraph/deleteAggrData/deleteHostGraph utils.cu:30-64
+ *                                            -> lv_engine_destroy,
+ *                                               lv_graph_destroy
+ *
+ * Identifiers are 32-bit unsigned (as the reference's `unsigned int`),
+ * weights FP32, CSR offsets 64-bit so graphs with more than 2^32 stored
+ * entries fit.
+ */
+#ifndef LOUVAIN_B200_H
+#define LOUVAIN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LV_ABI_VERSION 1
+
+typedef enum lv_status {
+    LV_OK = 0,
+    LV_ERR_ARG = 1,        /* invalid argument                              */
+    LV_ERR_IO = 2,         /* file could not be opened (utils.cu:171-174)   */
+    LV_ERR_PARSE = 3,      /* malformed Matrix Market input                 */
+    LV_ERR_NOMEM = 4,      /* host or device allocation failed              */
+    LV_ERR_CUDA = 5,       /* CUDA runtime error                            */
+    LV_ERR_STATE = 6,      /* call out of order (e.g. no graph loaded)      */
+    LV_ERR_LIMIT = 7,      /* size beyond a documented limit                */
+    LV_ERR_TIMEOUT = 8     /* a bounded device wait gave up                 */
+} lv_status;
+
+/* Move decision rule (the two reference implementations differ here).
+ * LV_RULE_PY:   move iff max_gain > 0                 (louvian.py:148-151)
+ * LV_RULE_CUDA: move iff max_gain - e_own/m > 0       (modularity.cu:182,
+ *                                                      278, 374)          */
+typedef enum lv_rule { LV_RULE_PY = 0, LV_RULE_CUDA = 1 } lv_rule;
+
+typedef struct lv_config {
+    int device;             /* CUDA device ordinal                          */
+    lv_rule rule;           /* decision rule, default LV_RULE_PY            */
+    uint32_t max_passes;    /* cap on passes per level (0 = 100000)         */
+    uint32_t max_levels;    /* cap on levels (0 = no cap)                   */
+    int use_graphs;         /* capture each level's pass in a CUDA graph    */
+    void *stream;           /* cudaStream_t to run on; NULL = own stream    */
+} lv_config;
+
+/* Per-level record (the reference prints none of this; -v here adds it). */
+typedef struct lv_level_info {
+    uint32_t n_vertices;    /* V of the level                               */
+    uint64_t n_entries;     /* E of the level (stored adjacency entries)    */
+    uint32_t passes;        /* move passes run                              */
+    uint32_t moved;         /* 1 if the level's first pass gained >= g      */
+    double q_start;         /* Q of the singleton partition                 */
+    double q_end;           /* Q after the last pass                        */
+    float move_ms;          /* device time of the move phase                */
+    float aggregate_ms;     /* device time of the contraction (0 if none)   */
+} lv_level_info;
+
+typedef struct lv_result {
+    double modularity;      /* Q the reference prints (modularity.cu:504)   */
+    uint32_t n_vertices;    /* input vertex count                           */
+    uint32_t n_communities; /* communities in the final assignment          */
+    uint32_t n_levels;      /* phases run                                   */
+    uint64_t edges_processed; /* sum over passes of that pass's E           */
+    float alg_ms;           /* device time of the phase loop (main.cu:56)   */
+    float copy_ms;          /* device time of upload + set-up (main.cu:19-35)*/
+} lv_result;
+
+typedef struct lv_graph lv_graph;   /* host CSR, owned by the library      */
+typedef struct lv_engine lv_engine; /* device state, owned by the library  */
+
+/* ---- status ---------------------------------------------------------- */
+const char *lv_status_string(lv_status s);
+const char *lv_last_error(void);
+int lv_abi_version(void);
+void lv_config_default(lv_config *cfg);
+
+/* ---- host graphs ------------------------------------------------------ */
+/* Matrix Market reader with the reference's semantics (utils.cu:132-229):
+ * '%' lines before the size header are skipped; the header is
+ * `rows cols nnz` and V = cols; indices are 1-based unless any entry line
+ * holds a 0; |weight| is used, 1.0 when a line has none (a missing weight
+ * repeats the previous line's); every off-diagonal entry is stored in both
+ * rows, a diagonal entry once, rows in file order.  Unlike the reference,
+ * malformed lines, truncated files and out-of-range indices are errors
+ * (LV_ERR_PARSE) instead of undefined behaviour.                          */
+lv_status lv_graph_load_mtx(const char *path, lv_graph **out);
+
+/* Same CSR construction from an edge list (the lines of an MTX file). */
+lv_status lv_graph_from_edges(uint32_t n_vertices, uint64_t n_edges,
+                              const uint32_t *src, const uint32_t *dst,
+                              const float *weights, lv_graph **out);
+
+/* Adopts a ready CSR (copied): offsets[n+1], cols[E], weights[E]. */
+lv_status lv_graph_from_csr(uint32_t n_vertices, const uint64_t *offsets,
+                            const uint32_t *cols, const float *weights,
+                            lv_graph **out);
+
+/* Read-only views of a host graph (valid until lv_graph_destroy). */
+lv_status lv_graph_view(const lv_graph *g, uint32_t *n_vertices,
+                        uint64_t *n_entries, const uint64_t **offsets,
+                        const uint32_t **cols, const float **weights,
+                        uint32_t *max_degree);
+void lv_graph_destroy(lv_graph *g);
+
+/* ---- engine ----------------------------------------------------------- */
+lv_status lv_engine_create(const lv_config *cfg, lv_engine **out);
+void lv_engine_destroy(lv_engine *e);
+
+/* Uploads a host graph and resets the state (every vertex its own
+ * community, assignment = identity): initDevGraph + copyToDevice +
+ * initCommAggr + setInitComm (utils.cu:66-108).                          */
+lv_status lv_engine_load(lv_engine *e, const lv_graph *g);
+
+/* Same from a CSR already in device memory (caller keeps ownership and
+ * must keep it alive and unchanged until the next load or destroy).      */
+lv_status lv_engine_load_device(lv_engine *e, uint32_t n_vertices,
+                                uint64_t n_entries, const uint64_t *d_offsets,
+                                const uint32_t *d_cols, const float *d_weights);
+
+/* One phase of local moving on the current level (modularityOptimization,
+ * modularity.cu:438-520).  *more = 1 when the first pass gained at least
+ * min_gain (the caller should aggregate and call again), 0 when the run
+ * is over; *q = the modularity the reference would print on return 0
+ * (Q before the failing pass), or Q after the last pass on return 1.
+ * Like the reference, on *more = 0 the failing pass's moves are dropped
+ * from the assignment.                                                   */
+lv_status lv_phase_move(lv_engine *e, float min_gain, int *more, double *q);
+
+/* Contracts the current level's communities into the next level's graph
+ * (aggregation, aggregation.cu:387-462).                                 */
+lv_status lv_phase_aggregate(lv_engine *e);
+
+/* Whole run (main.cu:43-48) on a host graph: upload, phases, contraction,
+ * final assignment left on the device (lv_get_assignment reads it).      */
+lv_status lv_run(lv_engine *e, const lv_graph *g, float min_gain,
+                 lv_result *res);
+
+/* Whole run with inputs and output in device memory: d_assignment
+ * receives n_vertices community ids; nothing crosses PCIe except a few
+ * scalars per level.                                                      */
+lv_status lv_run_device(lv_engine *e, uint32_t n_vertices, uint64_t n_entries,
+                        const uint64_t *d_offsets, const uint32_t *d_cols,
+                        const float *d_weights, float min_gain,
+                        uint32_t *d_assignment, lv_result *res);
+
+/* Final (or current) community of every input vertex -> host buffer.  */
+lv_status lv_get_assignment(lv_engine *e, uint32_t *out, size_t n);
+
+/* Per-level records of the last run; *count receives how many exist.    */
+lv_status lv_get_levels(lv_engine *e, lv_level_info *out, uint32_t cap,
+                        uint32_t *count);
+
+/* Current level's sizes.                                                */
+lv_status lv_get_level_size(lv_engine *e, uint32_t *n_vertices,
+                            uint64_t *n_entries);
+
+/* Current level state -> host buffers (each NULL or n_vertices long):
+ * community of every vertex, community sizes, weighted degrees.  For
+ * parity tests and debugging.                                            */
+lv_status lv_get_level_state(lv_engine *e, uint32_t *comm, uint32_t *comm_size,
+                             float *weighted_degree);
+
+/* Current level CSR -> host buffers (offsets n+1, cols/weights E).       */
+lv_status lv_get_level_csr(lv_engine *e, uint64_t *offsets, uint32_t *cols,
+                           float *weights);
+
+/* Overwrites the current level's communities (n_vertices ids < n) and
+ * recomputes sizes and totals, so contraction can be checked on a given
+ * partition.                                                             */
+lv_status lv_set_level_comm(lv_engine *e, const uint32_t *comm);
+
+/* FP64 modularity of an arbitrary partition of the CURRENT level graph,
+ * computed on the device:  sum intra w / 2m - sum a_c^2 / 4m^2.          */
+lv_status lv_modularity_fp64(lv_engine *e, const uint32_t *partition,
+                             double *q);
+
+/* Degree bucket (0 = degree 0, else 1..7 for (0,4] ... (319,inf)) of every
+ * vertex of the current level, as the move phase groups them
+ * (modularity.cu:5-18,439).                                              */
+lv_status lv_get_buckets(lv_engine *e, uint8_t *bucket_of, size_t n);
+
+/* ---- kernel timing (no counterpart in the reference, whose only timers
+ * are main.cu:19-56's two regions) --------------------------------------
+ * With profiling on, every launch group is bracketed by CUDA events on the
+ * engine's stream and its device time accumulated with its algorithmic
+ * HBM bytes (reads + writes the algorithm needs, counted from the level's
+ * V, E and bucket sizes).                                                */
+typedef struct lv_kernel_stat {
+    char name[32];          /* move_b1..move_b7, apply, modularity,
+                               level_init, contract                        */
+    uint64_t launches;      /* launch groups timed                          */
+    double total_ms;        /* summed device time                           */
+    double bytes;           /* summed algorithmic bytes                     */
+} lv_kernel_stat;
+
+lv_status lv_set_profiling(lv_engine *e, int on);
+lv_status lv_get_kernel_stats(lv_engine *e, lv_kernel_stat *out, uint32_t cap,
+                              uint32_t *count);
+lv_status lv_reset_kernel_stats(lv_engine *e);
+
+/* Kernels this library has launched in the process so far (all engines). */
+lv_status lv_get_launch_count(uint64_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

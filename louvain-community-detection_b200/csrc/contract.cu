@@ -1,0 +1,616 @@
+// contract.cu -- aggregation of a level's communities into the next level's
+// graph on sm_100a.
+//
+// Reference semantics (upicine/louvain-community-detection):
+//   non-empty flags + renumber by exclusive scan ... aggregation.cu:21-36,
+//                                                   389-393
+//   vertices grouped by community ................. aggregation.cu:38-45,
+//                                                   396-399
+//   per-community merge of member edges keyed by
+//   neighbour community, weights summed ........... aggregation.cu:57-357
+//   new offsets (scan of distinct counts) ......... aggregation.cu:452-456
+//   final CSR, neighbour ids renumbered ........... aggregation.cu:359-378
+//   louvian.py:163-215 states the same contraction.
+//
+// Design:
+//   * new ids, member offsets and each member's start in the flattened
+//     edge space of its community come from scans, so every kernel walks a
+//     community's edges as one flat range (load-balanced across members,
+//     where the reference walks members one after another).
+//   * communities are split by entry count into warp (<= 128 entries,
+//     256-slot shared table), block (<= 4096 entries, 8192-slot shared
+//     table) and multi-block classes (global table sized from the
+//     community's own entry count; the reference sizes every table from the
+//     level's vertex count).
+//   * neighbour ids are renumbered before hashing (cnew[u]), so rows are
+//     emitted in final ids and the last copy is a plain gather.
+//   * weights are summed in FP64 and rounded once to FP32.  A row's entries
+//     come out in table order; as in the reference (whose order depends on
+//     atomicCAS winners) only the set of (neighbour, weight) pairs of a row
+//     is defined.
+#include <algorithm>
+#include <vector>
+
+#include "lv_internal.h"
+
+namespace lvb {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kWarpSlots = 256;                 // class W table
+constexpr int kBlockSlots = 8192;               // class B table
+constexpr int kBlockSmem = kBlockSlots * 12 + kThreads * 16;
+
+__device__ __forceinline__ uint32_t hash_slot(uint32_t key, uint32_t mask) {
+  return (key * 2654435761u) & mask;
+}
+
+__device__ __forceinline__ uint32_t table_insert(uint32_t* keys, uint32_t mask,
+                                                 uint32_t key, uint32_t* err) {
+  uint32_t h = hash_slot(key, mask);
+  for (uint32_t it = 0; it <= mask; it++) {
+    uint32_t cur = keys[h];
+    if (cur == key) return h;
+    if (cur == kEmptyKey) {
+      uint32_t prev = atomicCAS(&keys[h], kEmptyKey, key);
+      if (prev == kEmptyKey || prev == key) return h;
+    }
+    h = (h + 1) & mask;
+  }
+  atomicExch(err, 1u);
+  return 0;
+}
+
+struct Ctx {
+  const uint64_t* off;
+  const uint32_t* col;
+  const float* w;
+  const uint32_t* comm_sz;
+  const uint32_t* members;
+  const uint32_t* mem_off;
+  const uint32_t* cnew;
+  const uint64_t* mstart;
+  const uint32_t* comm_list;
+  uint32_t* tcol;
+  float* tw;
+  uint64_t* new_deg;
+  uint32_t* err;
+};
+
+// flag_id[c] = comm_sz[c] > 0 ; mem_off[c] = comm_sz[c]  (scanned after)
+__global__ void flags_kernel(const uint32_t* comm_sz, uint32_t n,
+                             uint32_t* flag_id, uint32_t* mem_off,
+                             uint32_t* cursor) {
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    const uint32_t s = comm_sz[c];
+    flag_id[c] = s ? 1u : 0u;
+    mem_off[c] = s;
+    cursor[c] = 0u;
+  }
+}
+
+// members grouped by community; cnew[v] = new id of comm[v];
+// comm_list[new id] = old id.
+__global__ void members_kernel(const uint32_t* comm, const uint32_t* comm_sz,
+                               uint32_t n, const uint32_t* flag_id,
+                               const uint32_t* mem_off, uint32_t* cursor,
+                               uint32_t* members, uint32_t* cnew,
+                               uint32_t* comm_list) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += gridDim.x * blockDim.x) {
+    const uint32_t c = comm[v];
+    const uint32_t pos = mem_off[c] + atomicAdd(&cursor[c], 1u);
+    members[pos] = v;
+    cnew[v] = flag_id[c];
+    if (comm_sz[v]) comm_list[flag_id[v]] = v;
+  }
+}
+
+__global__ void member_deg_kernel(const uint64_t* off, const uint32_t* members,
+                                  uint32_t n, uint64_t* mstart) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= n;
+       i += gridDim.x * blockDim.x) {
+    uint64_t d = 0;
+    if (i < n) {
+      const uint32_t v = members[i];
+      d = off[v + 1] - off[v];
+    }
+    mstart[i] = d;
+  }
+}
+
+// entries and staging offset of every new community; new_deg zeroed.
+__global__ void comm_deg_kernel(const uint32_t* comm_list, uint32_t new_n,
+                                const uint32_t* comm_sz, const uint32_t* mem_off,
+                                const uint64_t* mstart, uint64_t* comm_deg,
+                                uint64_t* seg, uint64_t* new_deg) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= new_n;
+       i += gridDim.x * blockDim.x) {
+    new_deg[i] = 0ull;
+    if (i < new_n) {
+      const uint32_t c = comm_list[i];
+      const uint32_t m0 = mem_off[c];
+      const uint64_t s = mstart[m0];
+      seg[i] = s;
+      comm_deg[i] = mstart[m0 + comm_sz[c]] - s;
+    }
+  }
+}
+
+// Class W: one warp per community, flattened member edges, 256-slot table.
+__global__ void __launch_bounds__(kThreads)
+    merge_warp_kernel(Ctx C, const uint32_t* list, uint32_t count) {
+  __shared__ double vals_sm[kWarps][kWarpSlots];
+  __shared__ uint32_t keys_sm[kWarps][kWarpSlots];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double* vals = vals_sm[wib];
+  uint32_t* keys = keys_sm[wib];
+  constexpr uint32_t mask = kWarpSlots - 1;
+  for (uint32_t idx = blockIdx.x * kWarps + wib; idx < count;
+       idx += gridDim.x * kWarps) {
+    for (int i = lane; i < kWarpSlots; i += 32) {
+      keys[i] = kEmptyKey;
+      vals[i] = 0.0;
+    }
+    __syncwarp();
+    const uint32_t cn = list[idx];
+    const uint32_t c = C.comm_list[cn];
+    const uint32_t m0 = C.mem_off[c], msz = C.comm_sz[c];
+    const uint64_t seg = C.mstart[m0];
+    const uint64_t total = C.mstart[m0 + msz] - seg;
+    for (uint32_t mb = 0; mb < msz; mb += 32) {
+      const uint32_t mi = mb + lane;
+      const bool mv = mi < msz;
+      const uint32_t nvalid = min(32u, msz - mb);
+      uint64_t my_start = mv ? C.mstart[m0 + mi] - seg : ~0ull;
+      uint64_t my_off = 0;
+      if (mv) my_off = C.off[C.members[m0 + mi]];
+      const uint64_t lo = __shfl_sync(kFull, my_start, 0);
+      const uint64_t hi = (mb + 32 < msz) ? C.mstart[m0 + mb + 32] - seg : total;
+      for (uint64_t p0 = lo; p0 < hi; p0 += 32) {
+        const uint64_t p = p0 + lane;
+        const bool has = p < hi;
+        // largest member k with start_k <= p
+        int klo = 0, khi = (int)nvalid - 1;
+#pragma unroll
+        for (int it = 0; it < 5; it++) {
+          const int mid = (klo + khi + 1) >> 1;
+          const uint64_t sm = __shfl_sync(kFull, my_start, mid);
+          if (sm <= p) klo = mid; else khi = mid - 1;
+          if (khi < klo) khi = klo;
+        }
+        const uint64_t vo = __shfl_sync(kFull, my_off, klo);
+        const uint64_t vs = __shfl_sync(kFull, my_start, klo);
+        uint32_t key = kEmptyKey;
+        float wt = 0.0f;
+        if (has) {
+          const uint64_t j = vo + (p - vs);
+          key = C.cnew[C.col[j]];
+          wt = C.w[j];
+        }
+        const unsigned long long mk =
+            has ? (unsigned long long)key : (0x100000000ull | (unsigned)lane);
+        const unsigned peers = __match_any_sync(kFull, mk);
+        const int leader = __ffs(peers) - 1;
+        uint32_t slot = 0;
+        if (has && lane == leader) slot = table_insert(keys, mask, key, C.err);
+        slot = __shfl_sync(kFull, slot, leader);
+        if (has) atomicAdd(&vals[slot], (double)wt);
+      }
+    }
+    __syncwarp();
+    uint32_t cnt = 0;
+    for (int i0 = 0; i0 < kWarpSlots; i0 += 32) {
+      const uint32_t key = keys[i0 + lane];
+      const bool occ = key != kEmptyKey;
+      const unsigned b = __ballot_sync(kFull, occ);
+      if (occ) {
+        const uint32_t pos = cnt + __popc(b & ((1u << lane) - 1u));
+        C.tcol[seg + pos] = key;
+        C.tw[seg + pos] = (float)vals[i0 + lane];
+      }
+      cnt += __popc(b);
+    }
+    if (lane == 0) C.new_deg[cn] = cnt;
+    __syncwarp();
+  }
+}
+
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t x, uint32_t* sm,
+                                                    uint32_t* total) {
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  uint32_t incl = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) sm[wib] = incl;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    for (int i = 0; i < kWarps; i++) {
+      uint32_t t = sm[i];
+      sm[i] = run;
+      run += t;
+    }
+    sm[kWarps] = run;
+  }
+  __syncthreads();
+  const uint32_t r = sm[wib] + incl - x;
+  *total = sm[kWarps];
+  __syncthreads();
+  return r;
+}
+
+// Inserts positions [lo, hi) of a community's flattened edge range into a
+// table; members are staged through shared memory 256 at a time.
+__device__ __forceinline__ void insert_range(const Ctx& C, uint32_t m0,
+                                             uint32_t msz, uint64_t seg,
+                                             uint64_t total, uint64_t lo,
+                                             uint64_t hi, uint32_t* keys,
+                                             double* vals, uint32_t mask,
+                                             uint64_t* s_start,
+                                             uint64_t* s_off) {
+  const int lane = threadIdx.x & 31;
+  // first member whose range contains lo: largest k with start_k <= lo
+  __shared__ uint32_t s_k;
+  if (threadIdx.x == 0) {
+    uint32_t a = 0, b = msz - 1;
+    while (a < b) {
+      const uint32_t mid = (a + b + 1) >> 1;
+      if (C.mstart[m0 + mid] - seg <= lo) a = mid; else b = mid - 1;
+    }
+    s_k = a;
+  }
+  __syncthreads();
+  uint32_t k0 = s_k;
+  uint64_t pos = lo;
+  while (pos < hi) {
+    const uint32_t kk = k0 + threadIdx.x;
+    if (kk < msz) {
+      s_start[threadIdx.x] = C.mstart[m0 + kk] - seg;
+      s_off[threadIdx.x] = C.off[C.members[m0 + kk]];
+    } else {
+      s_start[threadIdx.x] = ~0ull;
+      s_off[threadIdx.x] = 0;
+    }
+    __syncthreads();
+    const uint32_t nvalid = min((uint32_t)kThreads, msz - k0);
+    const uint64_t chunk_end =
+        (k0 + kThreads < msz) ? min(hi, C.mstart[m0 + k0 + kThreads] - seg) : hi;
+    for (uint64_t p0 = pos; p0 < chunk_end; p0 += kThreads) {
+      const uint64_t p = p0 + threadIdx.x;
+      const bool has = p < chunk_end;
+      uint32_t key = kEmptyKey;
+      float wt = 0.0f;
+      if (has) {
+        int a = 0, b = (int)nvalid - 1;
+        while (a < b) {
+          const int mid = (a + b + 1) >> 1;
+          if (s_start[mid] <= p) a = mid; else b = mid - 1;
+        }
+        const uint64_t j = s_off[a] + (p - s_start[a]);
+        key = C.cnew[C.col[j]];
+        wt = C.w[j];
+      }
+      const unsigned long long mk =
+          has ? (unsigned long long)key : (0x100000000ull | (unsigned)lane);
+      const unsigned peers = __match_any_sync(kFull, mk);
+      const int leader = __ffs(peers) - 1;
+      uint32_t slot = 0;
+      if (has && lane == leader) slot = table_insert(keys, mask, key, C.err);
+      slot = __shfl_sync(kFull, slot, leader);
+      if (has) atomicAdd(&vals[slot], (double)wt);
+    }
+    pos = chunk_end;
+    k0 += kThreads;
+    __syncthreads();
+  }
+  (void)total;
+}
+
+// Class B: one block per community, 8192-slot shared table.
+__global__ void __launch_bounds__(kThreads)
+    merge_block_kernel(Ctx C, const uint32_t* list, uint32_t count) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* vals = reinterpret_cast<double*>(smem_raw);
+  uint64_t* s_start = reinterpret_cast<uint64_t*>(smem_raw + kBlockSlots * 8);
+  uint64_t* s_off = s_start + kThreads;
+  uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + kBlockSlots * 8 + kThreads * 16);
+  __shared__ uint32_t scan_sm[kWarps + 1];
+  constexpr uint32_t mask = kBlockSlots - 1;
+  for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
+    for (int i = threadIdx.x; i < kBlockSlots; i += kThreads) {
+      keys[i] = kEmptyKey;
+      vals[i] = 0.0;
+    }
+    __syncthreads();
+    const uint32_t cn = list[idx];
+    const uint32_t c = C.comm_list[cn];
+    const uint32_t m0 = C.mem_off[c], msz = C.comm_sz[c];
+    const uint64_t seg = C.mstart[m0];
+    const uint64_t total = C.mstart[m0 + msz] - seg;
+    insert_range(C, m0, msz, seg, total, 0, total, keys, vals, mask, s_start, s_off);
+    __syncthreads();
+    // emit: thread t owns slots [t*32, t*32+32)
+    constexpr int per = kBlockSlots / kThreads;
+    uint32_t local = 0;
+    for (int i = 0; i < per; i++) local += keys[threadIdx.x * per + i] != kEmptyKey;
+    uint32_t tot;
+    uint32_t pos = block_excl_scan(local, scan_sm, &tot);
+    for (int i = 0; i < per; i++) {
+      const int sl = threadIdx.x * per + i;
+      const uint32_t key = keys[sl];
+      if (key != kEmptyKey) {
+        C.tcol[seg + pos] = key;
+        C.tw[seg + pos] = (float)vals[sl];
+        pos++;
+      }
+    }
+    if (threadIdx.x == 0) C.new_deg[cn] = tot;
+    __syncthreads();
+  }
+}
+
+struct GArgs {
+  const uint32_t* list;      // class G new ids
+  const uint64_t* tab_off;   // per class-G index
+  const uint32_t* tab_size;  // per class-G index (power of two)
+  const uint32_t* blk_comm;  // per block: class-G index
+  const uint32_t* blk_chunk; // per block: chunk index
+  const uint32_t* blk_nchunks;
+  uint32_t* keys;
+  double* vals;
+  uint32_t nblocks;
+};
+
+// Class G: blocks insert chunks of a community's flattened range into its
+// global table.
+__global__ void __launch_bounds__(kThreads)
+    merge_global_insert_kernel(Ctx C, GArgs G) {
+  __shared__ uint64_t s_start[kThreads];
+  __shared__ uint64_t s_off[kThreads];
+  for (uint32_t b = blockIdx.x; b < G.nblocks; b += gridDim.x) {
+    const uint32_t gi = G.blk_comm[b], ch = G.blk_chunk[b];
+    const uint32_t cn = G.list[gi];
+    const uint32_t c = C.comm_list[cn];
+    const uint32_t m0 = C.mem_off[c], msz = C.comm_sz[c];
+    const uint64_t seg = C.mstart[m0];
+    const uint64_t total = C.mstart[m0 + msz] - seg;
+    const uint64_t lo = (uint64_t)ch * kMergeChunk;
+    const uint64_t hi = min(total, lo + kMergeChunk);
+    insert_range(C, m0, msz, seg, total, lo, hi, G.keys + G.tab_off[gi],
+                 G.vals + G.tab_off[gi], G.tab_size[gi] - 1, s_start, s_off);
+  }
+}
+
+// Class G: blocks compact slices of the tables into the staging rows.
+__global__ void __launch_bounds__(kThreads)
+    merge_global_emit_kernel(Ctx C, GArgs G) {
+  __shared__ uint32_t scan_sm[kWarps + 1];
+  __shared__ uint32_t base_sm;
+  for (uint32_t b = blockIdx.x; b < G.nblocks; b += gridDim.x) {
+    const uint32_t gi = G.blk_comm[b], ch = G.blk_chunk[b];
+    const uint32_t nch = G.blk_nchunks[b];
+    const uint32_t cn = G.list[gi];
+    const uint32_t c = C.comm_list[cn];
+    const uint64_t seg = C.mstart[C.mem_off[c]];
+    const uint64_t T = G.tab_size[gi];
+    const uint64_t s0 = T * ch / nch, s1 = T * (ch + 1) / nch;
+    const uint32_t* keys = G.keys + G.tab_off[gi];
+    const double* vals = G.vals + G.tab_off[gi];
+    for (uint64_t i0 = s0; i0 < s1; i0 += kThreads) {
+      const uint64_t i = i0 + threadIdx.x;
+      const bool occ = i < s1 && keys[i] != kEmptyKey;
+      uint32_t tot;
+      const uint32_t r = block_excl_scan(occ ? 1u : 0u, scan_sm, &tot);
+      if (threadIdx.x == 0 && tot)
+        base_sm = (uint32_t)atomicAdd((unsigned long long*)&C.new_deg[cn],
+                                      (unsigned long long)tot);
+      __syncthreads();
+      if (occ) {
+        const uint64_t pos = seg + base_sm + r;
+        C.tcol[pos] = keys[i];
+        C.tw[pos] = (float)vals[i];
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Final CSR: row cn copied from its staging range to new offsets.
+__global__ void __launch_bounds__(kThreads)
+    compress_kernel(const uint64_t* seg, const uint64_t* new_off, uint32_t new_n,
+                    const uint32_t* tcol, const float* tw, uint32_t* out_col,
+                    float* out_w) {
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  for (uint32_t cn = blockIdx.x * kWarps + wib; cn < new_n;
+       cn += gridDim.x * kWarps) {
+    const uint64_t dst = new_off[cn];
+    const uint64_t cnt = new_off[cn + 1] - dst;
+    const uint64_t src = seg[cn];
+    for (uint64_t j = lane; j < cnt; j += 32) {
+      out_col[dst + j] = tcol[src + j];
+      out_w[dst + j] = tw[src + j];
+    }
+  }
+}
+
+unsigned gridcap(uint64_t work, unsigned per_sm) {
+  const uint64_t cap = (uint64_t)sm_count_cached() * per_sm;
+  if (work == 0) return 1;
+  return (unsigned)(work < cap ? work : cap);
+}
+
+uint64_t next_pow2(uint64_t x) {
+  uint64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+}  // namespace
+
+cudaError_t configure_contract_kernels() {
+  return cudaFuncSetAttribute(merge_block_kernel,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kBlockSmem);
+}
+
+#define LV_TRY(x)                              \
+  do {                                         \
+    cudaError_t e_ = (x);                      \
+    if (e_ != cudaSuccess) return e_;          \
+  } while (0)
+
+cudaError_t contract_level(const LevelView& L, uint64_t nnz,
+                           ContractBuffers& B, ScanScratch& S,
+                           uint64_t* out_off, uint32_t* out_col, float* out_w,
+                           ContractResult* res, cudaStream_t st,
+                           cudaError_t (*grow)(void*, size_t, size_t),
+                           void* grow_ctx) {
+  const uint32_t n = L.n;
+  (void)nnz;
+  uint32_t* h_counts = nullptr;
+  LV_TRY(cudaMallocHost(&h_counts, 16 * sizeof(uint32_t)));
+  struct Free {
+    uint32_t* p;
+    ~Free() { cudaFreeHost(p); }
+  } free_guard{h_counts};
+
+  const unsigned g1 = gridcap((n + 255) / 256, 8);
+  (count_launches(1), flags_kernel<<<g1, 256, 0, st>>>(L.comm_sz, n, B.flag_id, B.mem_off, B.cursor));
+  LV_TRY(cudaGetLastError());
+  LV_TRY(exclusive_scan_u32(B.flag_id, B.flag_id, n, B.counts + 0, S, st));
+  LV_TRY(exclusive_scan_u32(B.mem_off, B.mem_off, n, B.counts + 1, S, st));
+  (count_launches(1), members_kernel<<<g1, 256, 0, st>>>(L.comm, L.comm_sz, n, B.flag_id, B.mem_off,
+                                     B.cursor, B.members, B.cnew, B.comm_list));
+  LV_TRY(cudaGetLastError());
+  (count_launches(1), member_deg_kernel<<<gridcap((n + 256) / 256, 8), 256, 0, st>>>(L.off, B.members, n,
+                                                                 B.mstart));
+  LV_TRY(cudaGetLastError());
+  LV_TRY(exclusive_scan_u64(B.mstart, B.mstart, (size_t)n + 1, nullptr, S, st));
+  LV_TRY(cudaMemcpyAsync(h_counts, B.counts, 2 * sizeof(uint32_t),
+                         cudaMemcpyDeviceToHost, st));
+  LV_TRY(cudaStreamSynchronize(st));
+  const uint32_t new_n = h_counts[0];
+
+  (count_launches(1), comm_deg_kernel<<<gridcap((new_n + 256) / 256, 8), 256, 0, st>>>(
+      B.comm_list, new_n, L.comm_sz, B.mem_off, B.mstart, B.comm_deg, B.seg,
+      B.new_deg));
+  LV_TRY(cudaGetLastError());
+  LV_TRY(partition_by_size3(B.comm_deg, new_n, kMergeWarpMax, kMergeBlockMax,
+                            B.comm_cls, B.counts + 4, B.tmp, S, st));
+  LV_TRY(cudaMemcpyAsync(h_counts + 4, B.counts + 4, 3 * sizeof(uint32_t),
+                         cudaMemcpyDeviceToHost, st));
+  LV_TRY(cudaStreamSynchronize(st));
+  const uint32_t cntW = h_counts[4], cntB = h_counts[5], cntG = h_counts[6];
+
+  Ctx C;
+  C.off = L.off;
+  C.col = L.col;
+  C.w = L.w;
+  C.comm_sz = L.comm_sz;
+  C.members = B.members;
+  C.mem_off = B.mem_off;
+  C.cnew = B.cnew;
+  C.mstart = B.mstart;
+  C.comm_list = B.comm_list;
+  C.tcol = B.tcol;
+  C.tw = B.tw;
+  C.new_deg = B.new_deg;
+  C.err = &L.sc->error;
+
+  if (cntW) {
+    (count_launches(1), merge_warp_kernel<<<gridcap((cntW + kWarps - 1) / kWarps, 4), kThreads, 0, st>>>(
+        C, B.comm_cls, cntW));
+    LV_TRY(cudaGetLastError());
+  }
+  if (cntB) {
+    (count_launches(1), merge_block_kernel<<<gridcap(cntB, 2), kThreads, kBlockSmem, st>>>(
+        C, B.comm_cls + cntW, cntB));
+    LV_TRY(cudaGetLastError());
+  }
+  if (cntG) {
+    // plan class-G tables and blocks on the host (few, very large rows)
+    std::vector<uint32_t> gids(cntG);
+    std::vector<uint64_t> gdeg(cntG);
+    LV_TRY(cudaMemcpyAsync(gids.data(), B.comm_cls + cntW + cntB,
+                           cntG * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    LV_TRY(cudaStreamSynchronize(st));
+    std::vector<uint64_t> all_deg(new_n);
+    LV_TRY(cudaMemcpyAsync(all_deg.data(), B.comm_deg, new_n * sizeof(uint64_t),
+                           cudaMemcpyDeviceToHost, st));
+    LV_TRY(cudaStreamSynchronize(st));
+    std::vector<uint64_t> tab_off(cntG);
+    std::vector<uint32_t> tab_size(cntG);
+    std::vector<uint32_t> blk_comm, blk_chunk, blk_nch;
+    uint64_t slots = 0;
+    for (uint32_t i = 0; i < cntG; i++) {
+      const uint64_t d = all_deg[gids[i]];
+      const uint64_t distinct = std::min<uint64_t>(d, new_n);
+      const uint64_t T = next_pow2(2 * distinct + 1);
+      tab_off[i] = slots;
+      tab_size[i] = (uint32_t)T;
+      slots += T;
+      const uint32_t nch = (uint32_t)((d + kMergeChunk - 1) / kMergeChunk);
+      for (uint32_t ch = 0; ch < nch; ch++) {
+        blk_comm.push_back(i);
+        blk_chunk.push_back(ch);
+        blk_nch.push_back(nch);
+      }
+    }
+    const size_t nblk = blk_comm.size();
+    if (slots > B.table_cap || std::max<size_t>(nblk, cntG) > B.g_cap) {
+      LV_TRY(grow(grow_ctx, slots, std::max<size_t>(nblk, cntG)));
+    }
+    LV_TRY(cudaMemsetAsync(B.keys, 0xFF, slots * sizeof(uint32_t), st));
+    LV_TRY(cudaMemsetAsync(B.vals, 0, slots * sizeof(double), st));
+    // block map packed as [comm | chunk | nchunks] in g_blk_comm/g_blk_chunk
+    LV_TRY(cudaMemcpyAsync(B.g_tab_off, tab_off.data(), cntG * sizeof(uint64_t),
+                           cudaMemcpyHostToDevice, st));
+    LV_TRY(cudaMemcpyAsync(B.g_tab_size, tab_size.data(), cntG * sizeof(uint32_t),
+                           cudaMemcpyHostToDevice, st));
+    std::vector<uint32_t> packed(2 * nblk);
+    std::copy(blk_chunk.begin(), blk_chunk.end(), packed.begin());
+    std::copy(blk_nch.begin(), blk_nch.end(), packed.begin() + nblk);
+    LV_TRY(cudaMemcpyAsync(B.g_blk_comm, blk_comm.data(), nblk * sizeof(uint32_t),
+                           cudaMemcpyHostToDevice, st));
+    LV_TRY(cudaMemcpyAsync(B.g_blk_chunk, packed.data(), 2 * nblk * sizeof(uint32_t),
+                           cudaMemcpyHostToDevice, st));
+    GArgs G;
+    G.list = B.comm_cls + cntW + cntB;
+    G.tab_off = B.g_tab_off;
+    G.tab_size = B.g_tab_size;
+    G.blk_comm = B.g_blk_comm;
+    G.blk_chunk = B.g_blk_chunk;
+    G.blk_nchunks = B.g_blk_chunk + nblk;
+    G.keys = B.keys;
+    G.vals = B.vals;
+    G.nblocks = (uint32_t)nblk;
+    (count_launches(1), merge_global_insert_kernel<<<gridcap(nblk, 8), kThreads, 0, st>>>(C, G));
+    LV_TRY(cudaGetLastError());
+    (count_launches(1), merge_global_emit_kernel<<<gridcap(nblk, 8), kThreads, 0, st>>>(C, G));
+    LV_TRY(cudaGetLastError());
+    // host vectors must outlive the async copies
+    LV_TRY(cudaStreamSynchronize(st));
+  }
+  // new offsets: exclusive scan of the n'+1 counts (last one is 0)
+  uint64_t* d_total = reinterpret_cast<uint64_t*>(B.counts + 8);
+  LV_TRY(exclusive_scan_u64(B.new_deg, out_off, (size_t)new_n + 1, d_total, S, st));
+  (count_launches(1), compress_kernel<<<gridcap((new_n + kWarps - 1) / kWarps, 8), kThreads, 0, st>>>(
+      B.seg, out_off, new_n, B.tcol, B.tw, out_col, out_w));
+  LV_TRY(cudaGetLastError());
+  uint64_t h_total = 0;
+  LV_TRY(cudaMemcpyAsync(&h_total, d_total, sizeof(uint64_t),
+                         cudaMemcpyDeviceToHost, st));
+  LV_TRY(cudaStreamSynchronize(st));
+  res->new_n = new_n;
+  res->new_nnz = h_total;
+  return cudaSuccess;
+}
+
+}  // namespace lvb

@@ -1,0 +1,1065 @@
+// engine.cu -- host side of the B200 Louvain engine: device state, level
+// loop, the C ABI (include/louvain_b200.h).
+//
+// Replaces the reference's host orchestration:
+//   main.cu:5-70            run loop and timing            -> lv_run
+//   modularity.cu:438-520   modularityOptimization          -> lv_phase_move
+//   aggregation.cu:387-462  aggregation                     -> lv_phase_aggregate
+//   utils.cu:30-108         allocation, upload, teardown    -> lv_engine_*
+// Status codes instead of HANDLE_ERROR's exit() (utils.cuh:95-100).
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/louvain_b200.h"
+#include "lv_graph.h"
+#include "lv_internal.h"
+
+using namespace lvb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+lv_status fail(lv_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+lv_status cuda_fail(cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();  // clear a non-sticky error
+  return fail(e == cudaErrorMemoryAllocation ? LV_ERR_NOMEM : LV_ERR_CUDA, m);
+}
+
+#define CU(expr)                                          \
+  do {                                                    \
+    cudaError_t e_ = (expr);                              \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #expr);   \
+  } while (0)
+
+#define LVTRY(expr)                   \
+  do {                                \
+    lv_status s_ = (expr);            \
+    if (s_ != LV_OK) return s_;       \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  return cudaMalloc((void**)p, count * sizeof(T));
+}
+
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+uint64_t next_pow2(uint64_t x) {
+  uint64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+__global__ void gather_degrees_kernel(const uint64_t* off, const uint32_t* ids,
+                                      uint32_t n, uint64_t* out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    const uint32_t v = ids[i];
+    out[i] = off[v + 1] - off[v];
+  }
+}
+
+// Sum of degrees per move class (only for the byte counts of profiling).
+__global__ void class_degree_kernel(const uint64_t* off, uint32_t n,
+                                    unsigned long long* out) {
+  __shared__ unsigned long long s[kClasses];
+  if (threadIdx.x < kClasses) s[threadIdx.x] = 0ull;
+  __syncthreads();
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += gridDim.x * blockDim.x) {
+    const uint64_t d = off[v + 1] - off[v];
+    atomicAdd(&s[move_class_of_degree(d)], (unsigned long long)d);
+  }
+  __syncthreads();
+  if (threadIdx.x < kClasses) atomicAdd(&out[threadIdx.x], s[threadIdx.x]);
+}
+
+// Timed launch groups.
+enum KId {
+  K_MOVE1 = 0,  // .. K_MOVE1 + 6 = bucket 7
+  K_APPLY = 7,
+  K_MODULARITY = 8,
+  K_LEVEL_INIT = 9,
+  K_CONTRACT = 10,
+  K_COUNT = 11
+};
+const char* kKName[K_COUNT] = {"move_b1", "move_b2", "move_b3",    "move_b4",
+                               "move_b5", "move_b6", "move_b7",    "apply",
+                               "modularity", "level_init", "contract"};
+
+struct KStat {
+  uint64_t launches = 0;
+  double ms = 0.0;
+  double bytes = 0.0;
+};
+
+struct PendingTiming {
+  int id;
+  cudaEvent_t a, b;
+  double bytes;
+};
+
+}  // namespace
+
+void lvb_set_error(const std::string& msg) { g_last_error = msg; }
+
+namespace lvb {
+static std::atomic<unsigned long long> g_launches{0};
+void count_launches(unsigned k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+}  // namespace lvb
+
+struct lv_engine {
+  lv_config cfg;
+  cudaStream_t st = nullptr;
+  bool own_stream = false;
+  int device = 0;
+
+  // capacities of the allocations below
+  uint32_t cap_n = 0;
+  uint64_t cap_e = 0;
+
+  // level-0 CSR: engine copy or caller device buffers
+  uint64_t* in_off = nullptr;
+  uint32_t* in_col = nullptr;
+  float* in_w = nullptr;
+  bool in_owned = false;
+  uint64_t* own_off = nullptr;
+  uint32_t* own_col = nullptr;
+  float* own_w = nullptr;
+
+  // contracted levels, ping-pong
+  uint64_t* c_off[2] = {nullptr, nullptr};
+  uint32_t* c_col[2] = {nullptr, nullptr};
+  float* c_w[2] = {nullptr, nullptr};
+  int cur = -1;  // -1: level 0 reads the input CSR
+
+  // per-vertex state
+  float* k = nullptr;
+  uint32_t* comm = nullptr;
+  uint32_t* comm_sz = nullptr;
+  double* tot = nullptr;
+  uint32_t* order = nullptr;
+  uint32_t* prop = nullptr;
+  uint32_t* cls_count = nullptr;
+  uint32_t* assignment = nullptr;  // [n0]
+  uint32_t* part_tmp = nullptr;
+  LevelScalars* sc = nullptr;
+  LevelScalars* sc_host = nullptr;  // pinned
+  uint32_t* h_counts = nullptr;     // pinned [16]
+
+  double* partials = nullptr;
+  size_t partials_cap = 0;
+  uint32_t* hub_map = nullptr;  // [blk_vertex | blk_chunk] for dispatch
+  size_t hub_map_cap = 0;
+  HubArena hub;
+  size_t hub_slots_cap = 0, hub_count_cap = 0, hub_blocks_cap = 0;
+  uint64_t* hub_deg = nullptr;
+
+  ContractBuffers cb{};
+  ScanScratch scan;
+
+  // current level
+  uint32_t n0 = 0;
+  uint32_t n = 0;
+  uint64_t e = 0;
+  bool loaded = false;
+  bool level_ready = false;
+  bool finished = false;
+  DispatchPlan plan{};
+  double q_last = 0.0;
+  std::vector<lv_level_info> levels;
+
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  // kernel timing
+  bool profiling = false;
+  KStat kst[K_COUNT];
+  std::vector<cudaEvent_t> ev_free;
+  std::vector<PendingTiming> pending;
+  unsigned long long* d_class_deg = nullptr;
+  uint64_t class_deg[kClasses] = {};
+
+  const uint64_t* off() const { return cur < 0 ? in_off : c_off[cur]; }
+  const uint32_t* col() const { return cur < 0 ? in_col : c_col[cur]; }
+  const float* wts() const { return cur < 0 ? in_w : c_w[cur]; }
+
+  LevelView view() const {
+    LevelView L;
+    L.n = n;
+    L.off = off();
+    L.col = col();
+    L.w = wts();
+    L.k = k;
+    L.comm = comm;
+    L.comm_sz = comm_sz;
+    L.tot = tot;
+    L.sc = sc;
+    return L;
+  }
+};
+
+namespace {
+
+cudaEvent_t take_event(lv_engine* E) {
+  if (!E->ev_free.empty()) {
+    cudaEvent_t e = E->ev_free.back();
+    E->ev_free.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Opens a timed launch group; returns the start event (nullptr when off).
+cudaEvent_t prof_begin(lv_engine* E) {
+  if (!E->profiling) return nullptr;
+  cudaEvent_t a = take_event(E);
+  cudaEventRecord(a, E->st);
+  return a;
+}
+
+void prof_end(lv_engine* E, cudaEvent_t a, int id, double bytes) {
+  if (!a) return;
+  cudaEvent_t b = take_event(E);
+  cudaEventRecord(b, E->st);
+  E->pending.push_back(PendingTiming{id, a, b, bytes});
+}
+
+// Folds the finished groups into the totals (call after a stream sync).
+void prof_collect(lv_engine* E) {
+  for (const PendingTiming& p : E->pending) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+      E->kst[p.id].launches++;
+      E->kst[p.id].ms += ms;
+      E->kst[p.id].bytes += p.bytes;
+    }
+    E->ev_free.push_back(p.a);
+    E->ev_free.push_back(p.b);
+  }
+  E->pending.clear();
+  cudaGetLastError();
+}
+
+void free_state(lv_engine* E) {
+  dfree(E->own_off);
+  dfree(E->own_col);
+  dfree(E->own_w);
+  for (int i = 0; i < 2; i++) {
+    dfree(E->c_off[i]);
+    dfree(E->c_col[i]);
+    dfree(E->c_w[i]);
+  }
+  dfree(E->k);
+  dfree(E->comm);
+  dfree(E->comm_sz);
+  dfree(E->tot);
+  dfree(E->order);
+  dfree(E->prop);
+  dfree(E->cls_count);
+  dfree(E->assignment);
+  dfree(E->part_tmp);
+  dfree(E->partials);
+  dfree(E->hub_map);
+  dfree(E->hub.keys);
+  dfree(E->hub.vals);
+  dfree(E->hub.tab_off);
+  dfree(E->hub.tab_size);
+  dfree(E->hub.best);
+  dfree(E->hub.own);
+  dfree(E->hub.blk_vertex);
+  dfree(E->hub.blk_chunk);
+  dfree(E->hub.blk_nchunks);
+  dfree(E->hub_deg);
+  ContractBuffers& B = E->cb;
+  dfree(B.flag_id);
+  dfree(B.mem_off);
+  dfree(B.cursor);
+  dfree(B.members);
+  dfree(B.cnew);
+  dfree(B.mstart);
+  dfree(B.comm_list);
+  dfree(B.comm_cls);
+  dfree(B.comm_deg);
+  dfree(B.seg);
+  dfree(B.new_deg);
+  dfree(B.tcol);
+  dfree(B.tw);
+  dfree(B.tmp);
+  dfree(B.counts);
+  dfree(B.keys);
+  dfree(B.vals);
+  dfree(B.g_tab_off);
+  dfree(B.g_tab_size);
+  dfree(B.g_blk_comm);
+  dfree(B.g_blk_chunk);
+  B.table_cap = 0;
+  B.g_cap = 0;
+  if (E->scan.buf) cudaFree(E->scan.buf);
+  E->scan.buf = nullptr;
+  E->scan.bytes = 0;
+  E->partials_cap = E->hub_map_cap = 0;
+  E->hub_slots_cap = E->hub_count_cap = E->hub_blocks_cap = 0;
+  E->cap_n = 0;
+  E->cap_e = 0;
+  E->in_off = nullptr;
+  E->in_col = nullptr;
+  E->in_w = nullptr;
+}
+
+cudaError_t grow_tables(void* ctx, size_t slots, size_t entries) {
+  lv_engine* E = static_cast<lv_engine*>(ctx);
+  ContractBuffers& B = E->cb;
+  if (slots > B.table_cap) {
+    dfree(B.keys);
+    dfree(B.vals);
+    size_t cap = std::max<size_t>(slots, 1 << 16);
+    cudaError_t e = dalloc(&B.keys, cap);
+    if (e != cudaSuccess) return e;
+    e = dalloc(&B.vals, cap);
+    if (e != cudaSuccess) return e;
+    B.table_cap = cap;
+  }
+  if (entries > B.g_cap) {
+    dfree(B.g_tab_off);
+    dfree(B.g_tab_size);
+    dfree(B.g_blk_comm);
+    dfree(B.g_blk_chunk);
+    size_t cap = std::max<size_t>(entries, 1024);
+    cudaError_t e = dalloc(&B.g_tab_off, cap);
+    if (e != cudaSuccess) return e;
+    e = dalloc(&B.g_tab_size, cap);
+    if (e != cudaSuccess) return e;
+    e = dalloc(&B.g_blk_comm, cap);
+    if (e != cudaSuccess) return e;
+    e = dalloc(&B.g_blk_chunk, 2 * cap);
+    if (e != cudaSuccess) return e;
+    B.g_cap = cap;
+  }
+  return cudaSuccess;
+}
+
+lv_status ensure_capacity(lv_engine* E, uint32_t n, uint64_t e, bool need_input) {
+  if (n <= E->cap_n && e <= E->cap_e && (!need_input || E->own_off)) return LV_OK;
+  free_state(E);
+  const size_t N = n, N1 = (size_t)n + 1, EE = e;
+  CU(dalloc(&E->k, N));
+  CU(dalloc(&E->comm, N));
+  CU(dalloc(&E->comm_sz, N));
+  CU(dalloc(&E->tot, N));
+  CU(dalloc(&E->order, N));
+  CU(dalloc(&E->prop, N));
+  CU(dalloc(&E->cls_count, 16));
+  CU(dalloc(&E->assignment, N));
+  const size_t ptw = partition_tmp_words(N) + 64;
+  CU(dalloc(&E->part_tmp, ptw));
+  for (int i = 0; i < 2; i++) {
+    CU(dalloc(&E->c_off[i], N1));
+    CU(dalloc(&E->c_col[i], EE));
+    CU(dalloc(&E->c_w[i], EE));
+  }
+  if (need_input) {
+    CU(dalloc(&E->own_off, N1));
+    CU(dalloc(&E->own_col, EE));
+    CU(dalloc(&E->own_w, EE));
+  }
+  ContractBuffers& B = E->cb;
+  CU(dalloc(&B.flag_id, N));
+  CU(dalloc(&B.mem_off, N));
+  CU(dalloc(&B.cursor, N));
+  CU(dalloc(&B.members, N));
+  CU(dalloc(&B.cnew, N));
+  CU(dalloc(&B.mstart, N1));
+  CU(dalloc(&B.comm_list, N));
+  CU(dalloc(&B.comm_cls, N));
+  CU(dalloc(&B.comm_deg, N));
+  CU(dalloc(&B.seg, N));
+  CU(dalloc(&B.new_deg, N1));
+  CU(dalloc(&B.tcol, EE));
+  CU(dalloc(&B.tw, EE));
+  CU(dalloc(&B.tmp, ptw));
+  CU(dalloc(&B.counts, 16));
+  B.table_cap = 0;
+  B.g_cap = 0;
+  const size_t scan_cap = std::max<size_t>(N1, partition_tmp_words(N)) + 1024;
+  E->scan.bytes = scan_scratch_bytes(scan_cap);
+  CU(cudaMalloc(&E->scan.buf, E->scan.bytes));
+  E->cap_n = n;
+  E->cap_e = e;
+  return LV_OK;
+}
+
+// Degree classes, work plan, hub tables for the current level.
+lv_status prepare_level(lv_engine* E) {
+  const uint32_t n = E->n;
+  cudaStream_t st = E->st;
+  CU(partition_by_degree(E->off(), n, E->order, E->cls_count, E->part_tmp,
+                         E->scan, st));
+  CU(cudaMemcpyAsync(E->h_counts, E->cls_count, kClasses * sizeof(uint32_t),
+                     cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  DispatchPlan& P = E->plan;
+  memset(&P, 0, sizeof(P));
+  P.cls_start[0] = 0;
+  for (int c = 0; c < kClasses; c++) P.cls_start[c + 1] = P.cls_start[c] + E->h_counts[c];
+  const uint32_t hs = P.cls_start[8];
+  const uint32_t hc = P.cls_start[9] - hs;
+  // hub plan
+  std::vector<uint32_t> blk_vertex, blk_chunk, blk_nch;
+  std::vector<uint64_t> tab_off;
+  std::vector<uint32_t> tab_size;
+  uint64_t slots = 0;
+  if (hc) {
+    if (hc > E->hub_count_cap) {
+      dfree(E->hub_deg);
+      dfree(E->hub.tab_off);
+      dfree(E->hub.tab_size);
+      dfree(E->hub.best);
+      dfree(E->hub.own);
+      CU(dalloc(&E->hub_deg, hc));
+      CU(dalloc(&E->hub.tab_off, hc));
+      CU(dalloc(&E->hub.tab_size, hc));
+      CU(dalloc(&E->hub.best, hc));
+      CU(dalloc(&E->hub.own, hc));
+      E->hub_count_cap = hc;
+    }
+    (count_launches(1), gather_degrees_kernel<<<(hc + 255) / 256, 256, 0, st>>>(E->off(), E->order + hs,
+                                                            hc, E->hub_deg));
+    CU(cudaGetLastError());
+    std::vector<uint64_t> deg(hc);
+    CU(cudaMemcpyAsync(deg.data(), E->hub_deg, hc * sizeof(uint64_t),
+                       cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    tab_off.resize(hc);
+    tab_size.resize(hc);
+    for (uint32_t i = 0; i < hc; i++) {
+      const uint64_t distinct = std::min<uint64_t>(deg[i], n);
+      const uint64_t T = next_pow2(2 * distinct + 1);
+      tab_off[i] = slots;
+      tab_size[i] = (uint32_t)T;
+      slots += T;
+      const uint32_t nch = (uint32_t)((deg[i] + kHubChunk - 1) / kHubChunk);
+      for (uint32_t ch = 0; ch < nch; ch++) {
+        blk_vertex.push_back(i);
+        blk_chunk.push_back(ch);
+        blk_nch.push_back(nch);
+      }
+    }
+  }
+  P.hub_count = hc;
+  P.hub_blocks = (uint32_t)blk_vertex.size();
+  // dispatch units per class
+  const uint32_t per_unit[kClasses] = {0, 64, 32, 16, 8, 8, 8, 1, 0};
+  uint32_t u = 0;
+  for (int c = 1; c <= 7; c++) {
+    P.blk_start[c] = u;
+    const uint32_t cnt = P.cls_start[c + 1] - P.cls_start[c];
+    u += (cnt + per_unit[c] - 1) / per_unit[c];
+  }
+  P.blk_start[8] = u;
+  u += P.hub_blocks;
+  P.blk_start[9] = u;
+  P.total_blocks = u;
+  // partials: hub accumulators + 2 per dispatch block
+  const size_t need_partials = hc + 2 * (size_t)dispatch_grid(P) + 16;
+  if (need_partials > E->partials_cap) {
+    dfree(E->partials);
+    CU(dalloc(&E->partials, need_partials));
+    E->partials_cap = need_partials;
+  }
+  if (hc) {
+    const size_t hb = P.hub_blocks;
+    if (hb > E->hub_blocks_cap) {
+      dfree(E->hub_map);
+      dfree(E->hub.blk_vertex);
+      dfree(E->hub.blk_chunk);
+      dfree(E->hub.blk_nchunks);
+      CU(dalloc(&E->hub_map, 2 * hb));
+      CU(dalloc(&E->hub.blk_vertex, hb));
+      CU(dalloc(&E->hub.blk_chunk, hb));
+      CU(dalloc(&E->hub.blk_nchunks, hb));
+      E->hub_blocks_cap = hb;
+    }
+    if (slots > E->hub_slots_cap) {
+      dfree(E->hub.keys);
+      dfree(E->hub.vals);
+      CU(dalloc(&E->hub.keys, slots));
+      CU(dalloc(&E->hub.vals, slots));
+      E->hub_slots_cap = slots;
+    }
+    std::vector<uint32_t> map(2 * hb);
+    std::copy(blk_vertex.begin(), blk_vertex.end(), map.begin());
+    std::copy(blk_chunk.begin(), blk_chunk.end(), map.begin() + hb);
+    CU(cudaMemcpyAsync(E->hub_map, map.data(), 2 * hb * sizeof(uint32_t),
+                       cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(E->hub.blk_vertex, blk_vertex.data(), hb * sizeof(uint32_t),
+                       cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(E->hub.blk_chunk, blk_chunk.data(), hb * sizeof(uint32_t),
+                       cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(E->hub.blk_nchunks, blk_nch.data(), hb * sizeof(uint32_t),
+                       cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(E->hub.tab_off, tab_off.data(), hc * sizeof(uint64_t),
+                       cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(E->hub.tab_size, tab_size.data(), hc * sizeof(uint32_t),
+                       cudaMemcpyHostToDevice, st));
+    CU(cudaMemsetAsync(E->hub.keys, 0xFF, slots * sizeof(uint32_t), st));
+    CU(cudaMemsetAsync(E->hub.vals, 0, slots * sizeof(double), st));
+    CU(cudaMemsetAsync(E->hub.best, 0, hc * sizeof(unsigned long long), st));
+    CU(cudaMemsetAsync(E->hub.own, 0, hc * sizeof(double), st));
+    CU(cudaMemsetAsync(E->partials, 0, hc * sizeof(double), st));
+  }
+  // entries per move class (byte counts of the kernel timings)
+  if (!E->d_class_deg) CU(dalloc(&E->d_class_deg, kClasses));
+  CU(cudaMemsetAsync(E->d_class_deg, 0, kClasses * sizeof(unsigned long long), st));
+  if (n) {
+    (count_launches(1), class_degree_kernel<<<std::min<uint32_t>((n + 255) / 256, 1184), 256, 0, st>>>(
+        E->off(), n, E->d_class_deg));
+    CU(cudaGetLastError());
+  }
+  CU(cudaMemcpyAsync(E->class_deg, E->d_class_deg, kClasses * sizeof(uint64_t),
+                     cudaMemcpyDeviceToHost, st));
+  // row sums, singleton state, m; then Q of the singleton partition
+  const LevelView L = E->view();
+  const double Vd = (double)n, Ed = (double)E->e;
+  cudaEvent_t t0 = prof_begin(E);
+  CU(launch_level_init(L, E->order, P, hc ? E->hub_map : nullptr, E->partials, st));
+  prof_end(E, t0, K_LEVEL_INIT, Ed * 4.0 + Vd * 32.0);
+  t0 = prof_begin(E);
+  CU(launch_modularity(L, E->order, P, hc ? E->hub_map : nullptr, E->partials, st));
+  prof_end(E, t0, K_MODULARITY, Ed * 12.0 + Vd * 24.0);
+  CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars),
+                     cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  prof_collect(E);
+  // tables of E->n vertices (blocking host copies above must be done
+  // before the vectors go out of scope: synchronised)
+  E->level_ready = true;
+  return LV_OK;
+}
+
+lv_status run_pass(lv_engine* E) {
+  const LevelView L = E->view();
+  const int rule = (E->cfg.rule == LV_RULE_CUDA) ? LV_RULE_CUDA_I : LV_RULE_PY_I;
+  HubArena H = E->hub;
+  for (int b = 1; b <= kBuckets; b++) {
+    const uint32_t s = E->plan.cls_start[b];
+    const uint32_t e = (b == 7) ? E->plan.cls_start[9] : E->plan.cls_start[b + 1];
+    if (e == s) continue;
+    // algorithmic bytes: every entry's (col, w, comm[col]) and, per vertex,
+    // order id, offset, comm, k, a_C(v) (FP64) and the proposal
+    const double vb = (double)(e - s);
+    const double eb = (double)(E->class_deg[b] + (b == 7 ? E->class_deg[8] : 0));
+    cudaEvent_t t0 = prof_begin(E);
+    CU(launch_move_bucket(L, b, rule, E->order, E->prop, E->plan, H, E->st));
+    prof_end(E, t0, K_MOVE1 + b - 1, eb * 12.0 + vb * 32.0);
+    t0 = prof_begin(E);
+    CU(launch_apply_bucket(L, b, E->order, E->prop, E->plan, E->st));
+    prof_end(E, t0, K_APPLY, vb * 12.0);
+  }
+  cudaEvent_t t0 = prof_begin(E);
+  CU(launch_modularity(L, E->order, E->plan, E->plan.hub_count ? E->hub_map : nullptr,
+                       E->partials, E->st));
+  prof_end(E, t0, K_MODULARITY, (double)E->e * 12.0 + (double)E->n * 24.0);
+  return LV_OK;
+}
+
+lv_status check_device_error(lv_engine* E) {
+  if (E->sc_host->error) {
+    return fail(LV_ERR_LIMIT, "a device hash table overflowed (bounded probe gave up)");
+  }
+  return LV_OK;
+}
+
+lv_status load_common(lv_engine* E, uint32_t n, uint64_t e) {
+  E->n0 = n;
+  E->n = n;
+  E->e = e;
+  E->cur = -1;
+  E->loaded = true;
+  E->level_ready = false;
+  E->finished = false;
+  E->levels.clear();
+  E->q_last = 0.0;
+  CU(launch_fill_iota(E->assignment, n, E->st));  // setInitComm, utils.cu:67
+  CU(cudaMemsetAsync(E->sc, 0, sizeof(LevelScalars), E->st));
+  return LV_OK;
+}
+
+lv_status validate_sizes(uint32_t n, uint64_t e) {
+  if (n >= 0xFFFFFFFFu) return fail(LV_ERR_LIMIT, "vertex count must be < 2^32-1");
+  (void)e;
+  return LV_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* lv_status_string(lv_status s) {
+  switch (s) {
+    case LV_OK: return "ok";
+    case LV_ERR_ARG: return "invalid argument";
+    case LV_ERR_IO: return "Error opening file";
+    case LV_ERR_PARSE: return "malformed Matrix Market input";
+    case LV_ERR_NOMEM: return "out of memory";
+    case LV_ERR_CUDA: return "CUDA error";
+    case LV_ERR_STATE: return "call out of order";
+    case LV_ERR_LIMIT: return "size limit exceeded";
+    case LV_ERR_TIMEOUT: return "device wait timed out";
+  }
+  return "unknown status";
+}
+
+const char* lv_last_error(void) { return g_last_error.c_str(); }
+
+int lv_abi_version(void) { return LV_ABI_VERSION; }
+
+void lv_config_default(lv_config* cfg) {
+  if (!cfg) return;
+  memset(cfg, 0, sizeof(*cfg));
+  cfg->device = 0;
+  cfg->rule = LV_RULE_PY;
+  cfg->max_passes = 0;
+  cfg->max_levels = 0;
+  cfg->use_graphs = 0;
+  cfg->stream = nullptr;
+}
+
+lv_status lv_engine_create(const lv_config* cfg, lv_engine** out) {
+  if (!out) return fail(LV_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  lv_engine* E = new (std::nothrow) lv_engine();
+  if (!E) return fail(LV_ERR_NOMEM, "engine allocation failed");
+  if (cfg) {
+    E->cfg = *cfg;
+  } else {
+    lv_config_default(&E->cfg);
+  }
+  if (E->cfg.rule != LV_RULE_PY && E->cfg.rule != LV_RULE_CUDA) {
+    delete E;
+    return fail(LV_ERR_ARG, "unknown rule");
+  }
+  if (E->cfg.max_passes == 0) E->cfg.max_passes = 100000;
+  E->device = E->cfg.device;
+  cudaError_t ce = cudaSetDevice(E->device);
+  if (ce != cudaSuccess) {
+    delete E;
+    return cuda_fail(ce, "cudaSetDevice");
+  }
+  ce = configure_kernels();
+  if (ce != cudaSuccess) {
+    delete E;
+    return cuda_fail(ce, "configure_kernels");
+  }
+  if (E->cfg.stream) {
+    E->st = (cudaStream_t)E->cfg.stream;
+  } else {
+    ce = cudaStreamCreateWithFlags(&E->st, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) {
+      delete E;
+      return cuda_fail(ce, "cudaStreamCreate");
+    }
+    E->own_stream = true;
+  }
+  if ((ce = cudaMalloc(&E->sc, sizeof(LevelScalars))) != cudaSuccess ||
+      (ce = cudaMallocHost(&E->sc_host, sizeof(LevelScalars))) != cudaSuccess ||
+      (ce = cudaMallocHost(&E->h_counts, 16 * sizeof(uint32_t))) != cudaSuccess ||
+      (ce = cudaEventCreate(&E->ev0)) != cudaSuccess ||
+      (ce = cudaEventCreate(&E->ev1)) != cudaSuccess) {
+    lv_engine_destroy(E);
+    return cuda_fail(ce, "engine set-up");
+  }
+  memset(E->sc_host, 0, sizeof(LevelScalars));
+  *out = E;
+  return LV_OK;
+}
+
+void lv_engine_destroy(lv_engine* E) {
+  if (!E) return;
+  cudaSetDevice(E->device);
+  if (E->st) cudaStreamSynchronize(E->st);
+  free_state(E);
+  prof_collect(E);
+  for (cudaEvent_t ev : E->ev_free) cudaEventDestroy(ev);
+  E->ev_free.clear();
+  dfree(E->d_class_deg);
+  if (E->sc) cudaFree(E->sc);
+  if (E->sc_host) cudaFreeHost(E->sc_host);
+  if (E->h_counts) cudaFreeHost(E->h_counts);
+  if (E->ev0) cudaEventDestroy(E->ev0);
+  if (E->ev1) cudaEventDestroy(E->ev1);
+  if (E->own_stream && E->st) cudaStreamDestroy(E->st);
+  delete E;
+}
+
+lv_status lv_engine_load(lv_engine* E, const lv_graph* g) {
+  if (!E || !g) return fail(LV_ERR_ARG, "NULL engine or graph");
+  LVTRY(validate_sizes(g->n, g->nnz));
+  cudaSetDevice(E->device);
+  LVTRY(ensure_capacity(E, g->n, g->nnz, true));
+  E->in_off = E->own_off;
+  E->in_col = E->own_col;
+  E->in_w = E->own_w;
+  CU(cudaMemcpyAsync(E->own_off, g->off.data(), ((size_t)g->n + 1) * sizeof(uint64_t),
+                     cudaMemcpyHostToDevice, E->st));
+  if (g->nnz) {
+    CU(cudaMemcpyAsync(E->own_col, g->col.data(), g->nnz * sizeof(uint32_t),
+                       cudaMemcpyHostToDevice, E->st));
+    CU(cudaMemcpyAsync(E->own_w, g->w.data(), g->nnz * sizeof(float),
+                       cudaMemcpyHostToDevice, E->st));
+  }
+  return load_common(E, g->n, g->nnz);
+}
+
+lv_status lv_engine_load_device(lv_engine* E, uint32_t n, uint64_t nnz,
+                                const uint64_t* d_off, const uint32_t* d_col,
+                                const float* d_w) {
+  if (!E || !d_off || (nnz && (!d_col || !d_w)))
+    return fail(LV_ERR_ARG, "NULL engine or device buffer");
+  LVTRY(validate_sizes(n, nnz));
+  cudaSetDevice(E->device);
+  LVTRY(ensure_capacity(E, n, nnz, false));
+  E->in_off = const_cast<uint64_t*>(d_off);
+  E->in_col = const_cast<uint32_t*>(d_col);
+  E->in_w = const_cast<float*>(d_w);
+  return load_common(E, n, nnz);
+}
+
+lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
+  if (!E) return fail(LV_ERR_ARG, "NULL engine");
+  if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
+  if (E->finished) return fail(LV_ERR_STATE, "the run has ended; load a graph again");
+  cudaSetDevice(E->device);
+  CU(cudaEventRecord(E->ev0, E->st));
+  if (!E->level_ready) LVTRY(prepare_level(E));
+  lv_level_info info{};
+  info.n_vertices = E->n;
+  info.n_entries = E->e;
+  const double m64 = E->sc_host->m64;
+  double act = E->sc_host->q, old = act;
+  info.q_start = act;
+  int ret = 1;
+  uint32_t passes = 0;
+  if (!(m64 > 0.0)) {
+    // no edge weight: nothing can move (the reference loops forever here)
+    ret = 0;
+    act = old = 0.0;
+    info.q_start = 0.0;
+  } else {
+    bool first = true;
+    do {
+      LVTRY(run_pass(E));
+      CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars),
+                         cudaMemcpyDeviceToHost, E->st));
+      CU(cudaStreamSynchronize(E->st));
+      prof_collect(E);
+      LVTRY(check_device_error(E));
+      old = act;
+      act = E->sc_host->q;
+      passes++;
+      if (first && act - old < (double)min_gain) ret = 0;  // modularity.cu:503
+      first = false;
+    } while (act - old >= (double)min_gain && passes < E->cfg.max_passes);
+  }
+  if (ret) CU(launch_compose(E->assignment, E->n0, E->comm, E->st));  // :515-517
+  CU(cudaEventRecord(E->ev1, E->st));
+  CU(cudaEventSynchronize(E->ev1));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, E->ev0, E->ev1);
+  info.passes = passes;
+  info.moved = (uint32_t)ret;
+  info.q_end = act;
+  info.move_ms = ms;
+  E->levels.push_back(info);
+  if (!ret) E->finished = true;
+  E->q_last = ret ? act : old;
+  if (more) *more = ret;
+  if (q) *q = E->q_last;
+  return LV_OK;
+}
+
+lv_status lv_phase_aggregate(lv_engine* E) {
+  if (!E) return fail(LV_ERR_ARG, "NULL engine");
+  if (!E->loaded || !E->level_ready) return fail(LV_ERR_STATE, "no move phase to aggregate");
+  cudaSetDevice(E->device);
+  CU(cudaEventRecord(E->ev0, E->st));
+  const int next = (E->cur == 0) ? 1 : 0;
+  ContractResult r{};
+  cudaEvent_t t0 = prof_begin(E);
+  CU(contract_level(E->view(), E->e, E->cb, E->scan, E->c_off[next], E->c_col[next],
+                    E->c_w[next], &r, E->st, grow_tables, E));
+  // B_agg = E*12 + V*(off + comm + new id + member) + E'*8 + (V'+1)*off
+  prof_end(E, t0, K_CONTRACT,
+           (double)E->e * 12.0 + (double)E->n * 20.0 + (double)r.new_nnz * 8.0 +
+               ((double)r.new_n + 1.0) * 8.0);
+  CU(launch_compose(E->assignment, E->n0, E->cb.flag_id, E->st));  // aggregation.cu:459
+  CU(cudaEventRecord(E->ev1, E->st));
+  CU(cudaEventSynchronize(E->ev1));
+  CU(cudaMemcpy(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost));
+  LVTRY(check_device_error(E));
+  prof_collect(E);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, E->ev0, E->ev1);
+  if (!E->levels.empty()) E->levels.back().aggregate_ms = ms;
+  E->cur = next;
+  E->n = r.new_n;
+  E->e = r.new_nnz;
+  E->level_ready = false;
+  return LV_OK;
+}
+
+static lv_status run_loaded(lv_engine* E, float min_gain, lv_result* res) {
+  CU(cudaEventRecord(E->ev0, E->st));
+  cudaEvent_t a0, a1;
+  CU(cudaEventCreate(&a0));
+  CU(cudaEventCreate(&a1));
+  CU(cudaEventRecord(a0, E->st));
+  double q = 0.0;
+  uint64_t processed = 0;
+  for (;;) {
+    int more = 0;
+    lv_status s = lv_phase_move(E, min_gain, &more, &q);
+    if (s != LV_OK) {
+      cudaEventDestroy(a0);
+      cudaEventDestroy(a1);
+      return s;
+    }
+    processed += (uint64_t)E->levels.back().passes * E->levels.back().n_entries;
+    if (!more) break;
+    const uint32_t before = E->n;
+    s = lv_phase_aggregate(E);
+    if (s != LV_OK) {
+      cudaEventDestroy(a0);
+      cudaEventDestroy(a1);
+      return s;
+    }
+    if (E->n == before) {  // merged nothing (threshold <= 0): stop
+      E->finished = true;
+      break;
+    }
+    if (E->cfg.max_levels && E->levels.size() >= E->cfg.max_levels) {
+      E->finished = true;
+      break;
+    }
+  }
+  CU(cudaEventRecord(a1, E->st));
+  CU(cudaEventSynchronize(a1));
+  float alg = 0.0f;
+  cudaEventElapsedTime(&alg, a0, a1);
+  cudaEventDestroy(a0);
+  cudaEventDestroy(a1);
+  if (res) {
+    res->modularity = q;
+    res->n_vertices = E->n0;
+    res->n_communities = E->n;
+    res->n_levels = (uint32_t)E->levels.size();
+    res->edges_processed = processed;
+    res->alg_ms = alg;
+  }
+  return LV_OK;
+}
+
+lv_status lv_run(lv_engine* E, const lv_graph* g, float min_gain, lv_result* res) {
+  if (!E || !g) return fail(LV_ERR_ARG, "NULL engine or graph");
+  cudaSetDevice(E->device);
+  cudaEvent_t c0, c1;
+  CU(cudaEventCreate(&c0));
+  CU(cudaEventCreate(&c1));
+  CU(cudaEventRecord(c0, E->st));
+  lv_status s = lv_engine_load(E, g);
+  if (s != LV_OK) {
+    cudaEventDestroy(c0);
+    cudaEventDestroy(c1);
+    return s;
+  }
+  CU(cudaEventRecord(c1, E->st));
+  CU(cudaEventSynchronize(c1));
+  float copy = 0.0f;
+  cudaEventElapsedTime(&copy, c0, c1);
+  cudaEventDestroy(c0);
+  cudaEventDestroy(c1);
+  s = run_loaded(E, min_gain, res);
+  if (s == LV_OK && res) res->copy_ms = copy;
+  return s;
+}
+
+lv_status lv_run_device(lv_engine* E, uint32_t n, uint64_t nnz, const uint64_t* d_off,
+                        const uint32_t* d_col, const float* d_w, float min_gain,
+                        uint32_t* d_assignment, lv_result* res) {
+  if (!E) return fail(LV_ERR_ARG, "NULL engine");
+  LVTRY(lv_engine_load_device(E, n, nnz, d_off, d_col, d_w));
+  LVTRY(run_loaded(E, min_gain, res));
+  if (res) res->copy_ms = 0.0f;
+  if (d_assignment && n) {
+    CU(cudaMemcpyAsync(d_assignment, E->assignment, (size_t)n * sizeof(uint32_t),
+                       cudaMemcpyDeviceToDevice, E->st));
+    CU(cudaStreamSynchronize(E->st));
+  }
+  return LV_OK;
+}
+
+lv_status lv_get_assignment(lv_engine* E, uint32_t* out, size_t n) {
+  if (!E || (!out && n)) return fail(LV_ERR_ARG, "NULL argument");
+  if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
+  if (n != E->n0) return fail(LV_ERR_ARG, "buffer length must equal the input vertex count");
+  cudaSetDevice(E->device);
+  if (n) {
+    CU(cudaMemcpyAsync(out, E->assignment, n * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                       E->st));
+    CU(cudaStreamSynchronize(E->st));
+  }
+  return LV_OK;
+}
+
+lv_status lv_get_levels(lv_engine* E, lv_level_info* out, uint32_t cap, uint32_t* count) {
+  if (!E) return fail(LV_ERR_ARG, "NULL engine");
+  const uint32_t nl = (uint32_t)E->levels.size();
+  if (count) *count = nl;
+  if (out)
+    for (uint32_t i = 0; i < nl && i < cap; i++) out[i] = E->levels[i];
+  return LV_OK;
+}
+
+lv_status lv_get_level_size(lv_engine* E, uint32_t* n, uint64_t* e) {
+  if (!E) return fail(LV_ERR_ARG, "NULL engine");
+  if (n) *n = E->n;
+  if (e) *e = E->e;
+  return LV_OK;
+}
+
+lv_status lv_get_level_state(lv_engine* E, uint32_t* comm, uint32_t* comm_size,
+                             float* weighted_degree) {
+  if (!E) return fail(LV_ERR_ARG, "NULL engine");
+  if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
+  cudaSetDevice(E->device);
+  if (!E->level_ready) LVTRY(prepare_level(E));
+  const size_t n = E->n;
+  if (n) {
+    if (comm) CU(cudaMemcpyAsync(comm, E->comm, n * 4, cudaMemcpyDeviceToHost, E->st));
+    if (comm_size)
+      CU(cudaMemcpyAsync(comm_size, E->comm_sz, n * 4, cudaMemcpyDeviceToHost, E->st));
+    if (weighted_degree)
+      CU(cudaMemcpyAsync(weighted_degree, E->k, n * 4, cudaMemcpyDeviceToHost, E->st));
+  }
+  CU(cudaStreamSynchronize(E->st));
+  return LV_OK;
+}
+
+lv_status lv_get_level_csr(lv_engine* E, uint64_t* offsets, uint32_t* cols,
+                           float* weights) {
+  if (!E) return fail(LV_ERR_ARG, "NULL engine");
+  if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
+  cudaSetDevice(E->device);
+  if (offsets)
+    CU(cudaMemcpyAsync(offsets, E->off(), ((size_t)E->n + 1) * 8, cudaMemcpyDeviceToHost,
+                       E->st));
+  if (E->e) {
+    if (cols) CU(cudaMemcpyAsync(cols, E->col(), E->e * 4, cudaMemcpyDeviceToHost, E->st));
+    if (weights)
+      CU(cudaMemcpyAsync(weights, E->wts(), E->e * 4, cudaMemcpyDeviceToHost, E->st));
+  }
+  CU(cudaStreamSynchronize(E->st));
+  return LV_OK;
+}
+
+lv_status lv_set_level_comm(lv_engine* E, const uint32_t* comm) {
+  if (!E || !comm) return fail(LV_ERR_ARG, "NULL argument");
+  if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
+  cudaSetDevice(E->device);
+  for (uint32_t i = 0; i < E->n; i++)
+    if (comm[i] >= E->n) return fail(LV_ERR_ARG, "community id out of range");
+  if (!E->level_ready) LVTRY(prepare_level(E));
+  if (E->n) CU(cudaMemcpyAsync(E->comm, comm, (size_t)E->n * 4, cudaMemcpyHostToDevice, E->st));
+  CU(launch_recount(E->view(), E->st));
+  CU(cudaStreamSynchronize(E->st));
+  return LV_OK;
+}
+
+lv_status lv_modularity_fp64(lv_engine* E, const uint32_t* partition, double* q) {
+  if (!E || !partition || !q) return fail(LV_ERR_ARG, "NULL argument");
+  if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
+  cudaSetDevice(E->device);
+  for (uint32_t i = 0; i < E->n; i++)
+    if (partition[i] >= E->n) return fail(LV_ERR_ARG, "community id out of range");
+  uint32_t* d_part = E->cb.cursor;
+  double* d_tot = reinterpret_cast<double*>(E->cb.comm_deg);
+  double* d_out = reinterpret_cast<double*>(E->cb.new_deg);
+  if (E->n) CU(cudaMemcpyAsync(d_part, partition, (size_t)E->n * 4, cudaMemcpyHostToDevice, E->st));
+  CU(launch_modularity_of(E->view(), d_part, d_tot, d_out, E->st));
+  double h[3] = {0, 0, 0};
+  CU(cudaMemcpyAsync(h, d_out, sizeof(h), cudaMemcpyDeviceToHost, E->st));
+  CU(cudaStreamSynchronize(E->st));
+  const double m = h[2] / 2.0;
+  *q = (m > 0.0) ? h[0] / (2.0 * m) - h[1] / (4.0 * m * m) : 0.0;
+  return LV_OK;
+}
+
+lv_status lv_set_profiling(lv_engine* E, int on) {
+  if (!E) return fail(LV_ERR_ARG, "NULL engine");
+  E->profiling = on != 0;
+  return LV_OK;
+}
+
+lv_status lv_get_kernel_stats(lv_engine* E, lv_kernel_stat* out, uint32_t cap,
+                              uint32_t* count) {
+  if (!E) return fail(LV_ERR_ARG, "NULL engine");
+  if (count) *count = K_COUNT;
+  if (out) {
+    for (uint32_t i = 0; i < K_COUNT && i < cap; i++) {
+      memset(&out[i], 0, sizeof(out[i]));
+      strncpy(out[i].name, kKName[i], sizeof(out[i].name) - 1);
+      out[i].launches = E->kst[i].launches;
+      out[i].total_ms = E->kst[i].ms;
+      out[i].bytes = E->kst[i].bytes;
+    }
+  }
+  return LV_OK;
+}
+
+lv_status lv_get_launch_count(uint64_t* count) {
+  if (!count) return fail(LV_ERR_ARG, "NULL argument");
+  *count = launch_count();
+  return LV_OK;
+}
+
+lv_status lv_reset_kernel_stats(lv_engine* E) {
+  if (!E) return fail(LV_ERR_ARG, "NULL engine");
+  for (int i = 0; i < K_COUNT; i++) E->kst[i] = KStat{};
+  return LV_OK;
+}
+
+lv_status lv_get_buckets(lv_engine* E, uint8_t* bucket_of, size_t n) {
+  if (!E || (!bucket_of && n)) return fail(LV_ERR_ARG, "NULL argument");
+  if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
+  if (n != E->n) return fail(LV_ERR_ARG, "buffer length must equal the level's vertex count");
+  cudaSetDevice(E->device);
+  uint8_t* d = reinterpret_cast<uint8_t*>(E->cb.cursor);
+  CU(launch_bucket_ids(E->off(), E->n, d, E->st));
+  if (n) CU(cudaMemcpyAsync(bucket_of, d, n, cudaMemcpyDeviceToHost, E->st));
+  CU(cudaStreamSynchronize(E->st));
+  return LV_OK;
+}
+
+}  // extern "C"

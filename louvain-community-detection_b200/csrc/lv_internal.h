@@ -1,0 +1,221 @@
+// lv_internal.h -- internal interface between the host engine and the
+// sm_100a kernels.  Not part of the C ABI.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lvb {
+
+// Process-wide count of kernels this library has launched.
+void count_launches(unsigned k);
+unsigned long long launch_count();
+
+// Move-phase degree buckets (modularity.cu:439): bucket b in 1..7 holds the
+// vertices with hi[b-1] < deg <= hi[b]; degree 0 is in no bucket and never
+// moves.  Every bucket is one Jacobi step of a pass, in this order.
+constexpr int kBuckets = 7;
+constexpr uint64_t kBucketHi[kBuckets + 1] = {0, 4, 8, 16, 32, 84, 319,
+                                              ~0ull};
+
+// Kernel classes: which kernel processes a vertex.  Classes 1..6 are the
+// buckets 1..6; bucket 7 splits into class 7 (shared-memory table, one
+// block per vertex) and class 8 (global-memory table, several blocks per
+// vertex).  Classes are contiguous in the order array, so bucket 7 is the
+// union of classes 7 and 8.
+constexpr int kClasses = 9;                 // 0..8, class 0 = degree 0
+constexpr uint64_t kHubSmemMaxDeg = 2048;   // class 7 upper degree
+constexpr int kHubSmemSlots = 4096;         // table slots of class 7
+constexpr uint32_t kHubChunk = 4096;        // edges per block, class 8
+
+__host__ __device__ inline int move_class_of_degree(uint64_t d) {
+  return d == 0      ? 0
+         : d <= 4    ? 1
+         : d <= 8    ? 2
+         : d <= 16   ? 3
+         : d <= 32   ? 4
+         : d <= 84   ? 5
+         : d <= 319  ? 6
+         : d <= kHubSmemMaxDeg ? 7
+                     : 8;
+}
+
+constexpr uint32_t kEmptyKey = 0xFFFFFFFFu;
+
+// Decision rules, numbered as lv_rule in the C ABI.
+constexpr int LV_RULE_PY_I = 0;    // louvian.py:148-151
+constexpr int LV_RULE_CUDA_I = 1;  // modularity.cu:182,278,374
+
+// Scalars of the current level, resident in device memory so no kernel
+// needs a host round trip to learn them.
+struct LevelScalars {
+  double m64;        // sum_v k_v / 2 (FP64)
+  float m;           // FP32 copy used by the gains (modularity.cu:149-152)
+  float den;         // 2 * m * m in FP32, evaluated as (2*m)*m
+  double q;          // modularity after the most recent sweep
+  double intra;      // last sweep's intra-community weight
+  double asq;        // last sweep's sum of squared community totals
+  uint32_t error;    // set by a kernel when a bounded loop gave up
+  uint32_t done_blocks;  // last-block-done counter of reductions
+};
+
+// Read-mostly view of the current level passed to kernels by value.
+struct LevelView {
+  uint32_t n;
+  const uint64_t* __restrict__ off;
+  const uint32_t* __restrict__ col;
+  const float* __restrict__ w;
+  float* k;            // weighted degree (FP32 value of an FP64 row sum)
+  uint32_t* comm;      // community of every vertex
+  uint32_t* comm_sz;   // vertices per community
+  double* tot;         // community totals a_c (FP64, exact for FP32 inputs)
+  LevelScalars* sc;
+};
+
+// Work partition of a level for the "class dispatch" kernels (row sums and
+// the modularity sweep): consecutive block ranges serve consecutive classes.
+struct DispatchPlan {
+  uint32_t cls_start[kClasses + 1];   // order[] offsets per class
+  uint32_t blk_start[kClasses + 1];   // first block of each class (1..8)
+  uint32_t hub_count;                 // class 8 vertex count
+  uint32_t hub_blocks;                // blocks of class 8 (sum of chunks)
+  uint32_t total_blocks;
+};
+
+// ---------------------------------------------------------------------------
+// scan.cu
+// ---------------------------------------------------------------------------
+// Scratch for scans of up to `cap` elements.
+struct ScanScratch {
+  void* buf = nullptr;
+  size_t bytes = 0;
+};
+size_t scan_scratch_bytes(size_t cap);
+// Exclusive scans; out may alias in.  When total != nullptr the grand
+// total is written there (device pointer).
+cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n,
+                               uint32_t* total, ScanScratch& s,
+                               cudaStream_t st);
+cudaError_t exclusive_scan_u64(const uint64_t* in, uint64_t* out, size_t n,
+                               uint64_t* total, ScanScratch& s,
+                               cudaStream_t st);
+
+// Stable partition of [0, n) by vertex degree class: order receives the
+// vertices class by class, ascending within a class; cls_count (device,
+// kClasses entries) the class sizes.  `tmp` needs partition_tmp_words(n).
+size_t partition_tmp_words(size_t n);
+cudaError_t partition_by_degree(const uint64_t* off, uint32_t n,
+                                uint32_t* order, uint32_t* cls_count,
+                                uint32_t* tmp, ScanScratch& s,
+                                cudaStream_t st);
+
+// Stable partition of the indices [0, n) into 3 classes by sizes[i]:
+// <= lim0, <= lim1, larger.
+cudaError_t partition_by_size3(const uint64_t* sizes,
+                               uint32_t n, uint64_t lim0, uint64_t lim1,
+                               uint32_t* out, uint32_t* cls_count,
+                               uint32_t* tmp, ScanScratch& s,
+                               cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// move.cu
+// ---------------------------------------------------------------------------
+// Row sums k_v, singleton state (comm=id, sizes 1, totals k) and m.
+cudaError_t launch_level_init(const LevelView& L, const uint32_t* order,
+                              const DispatchPlan& P, const uint32_t* hub_map,
+                              double* partials, cudaStream_t st);
+// Modularity of the current state into sc->q (FP64, deterministic).
+cudaError_t launch_modularity(const LevelView& L, const uint32_t* order,
+                              const DispatchPlan& P, const uint32_t* hub_map,
+                              double* partials, cudaStream_t st);
+// Hub (class 8) arenas: per hub vertex a table of tab_size[i] slots at
+// tab_off[i] (FP64 values, u32 keys), a best key and an own-weight sum.
+struct HubArena {
+  uint32_t* keys = nullptr;
+  double* vals = nullptr;
+  uint64_t* tab_off = nullptr;     // [hub_count]
+  uint32_t* tab_size = nullptr;    // [hub_count] power of two
+  unsigned long long* best = nullptr;  // [hub_count]
+  double* own = nullptr;           // [hub_count]
+  uint32_t* blk_vertex = nullptr;  // [hub_blocks] hub index of each block
+  uint32_t* blk_chunk = nullptr;   // [hub_blocks] chunk within the vertex
+  uint32_t* blk_nchunks = nullptr; // [hub_blocks] chunks of that vertex
+};
+// One Jacobi step: proposals for every vertex of bucket b (1..7), then the
+// moves applied (sizes, totals, comm).  proposal[] is parallel to order[].
+cudaError_t launch_move_bucket(const LevelView& L, int bucket, int rule,
+                               const uint32_t* order, uint32_t* proposal,
+                               const DispatchPlan& P, const HubArena& H,
+                               cudaStream_t st);
+cudaError_t launch_apply_bucket(const LevelView& L, int bucket,
+                                const uint32_t* order,
+                                const uint32_t* proposal,
+                                const DispatchPlan& P, cudaStream_t st);
+// assignment[i] = map[assignment[i]]
+cudaError_t launch_compose(uint32_t* assignment, size_t n0,
+                           const uint32_t* map, cudaStream_t st);
+cudaError_t launch_fill_iota(uint32_t* a, size_t n, cudaStream_t st);
+// Recompute sizes and totals from comm (used when a caller sets comm).
+cudaError_t launch_recount(const LevelView& L, cudaStream_t st);
+// FP64 modularity of an arbitrary partition (one-off, not hot).
+cudaError_t launch_modularity_of(const LevelView& L, const uint32_t* part,
+                                 double* tot_scratch, double* out,
+                                 cudaStream_t st);
+cudaError_t launch_bucket_ids(const uint64_t* off, uint32_t n, uint8_t* out,
+                              cudaStream_t st);
+unsigned dispatch_grid(const DispatchPlan& P);
+unsigned sm_count_cached();
+// Opts kernels with more than 48 KB of shared memory in (once per device).
+cudaError_t configure_kernels();
+cudaError_t configure_contract_kernels();
+
+// ---------------------------------------------------------------------------
+// contract.cu
+// ---------------------------------------------------------------------------
+struct ContractBuffers {
+  uint32_t* flag_id;     // [n] flags -> new ids
+  uint32_t* mem_off;     // [n] exclusive scan of comm_sz
+  uint32_t* cursor;      // [n]
+  uint32_t* members;     // [n] vertices grouped by community
+  uint32_t* cnew;        // [n] new id of every vertex's community
+  uint64_t* mstart;      // [n+1] flattened edge start of every member
+  uint32_t* comm_list;   // [n] old id of every new community
+  uint32_t* comm_cls;    // [n] comm_list partitioned by size class
+  uint64_t* comm_deg;    // [n] entries per new community
+  uint64_t* seg;         // [n] staging offset of every new community's row
+  uint64_t* new_deg;     // [n+1] entries per new row -> new offsets
+  uint32_t* tcol;        // [E] row staging (cols)
+  float* tw;             // [E] row staging (weights)
+  uint32_t* tmp;         // partition scratch
+  uint32_t* counts;      // [16] device counters
+  uint32_t* keys;        // global tables (class G), u32
+  double* vals;          // global tables (class G), FP64
+  size_t table_cap;      // slots available in keys/vals
+  uint64_t* g_tab_off;   // [cap] per class-G community table offset
+  uint32_t* g_tab_size;  // [cap]
+  uint32_t* g_blk_comm;  // [cap] per block: index in class-G list
+  uint32_t* g_blk_chunk; // [cap]
+  size_t g_cap;          // entries available in the g_* arrays
+};
+constexpr uint64_t kMergeWarpMax = 128;    // entries: warp per community
+constexpr uint64_t kMergeBlockMax = 4096;  // entries: block, shared table
+constexpr uint32_t kMergeChunk = 8192;     // entries per block, class G
+
+struct ContractResult {
+  uint32_t new_n;
+  uint64_t new_nnz;
+};
+// Contracts level (L, comm) into (out_off, out_col, out_w); writes cnew
+// (vertex -> new id) for composing the assignment.  Synchronises the
+// stream internally (sizes are needed on the host).
+cudaError_t contract_level(const LevelView& L, uint64_t nnz,
+                           ContractBuffers& B, ScanScratch& S,
+                           uint64_t* out_off, uint32_t* out_col, float* out_w,
+                           ContractResult* res, cudaStream_t st,
+                           // host-side growable arena callback
+                           cudaError_t (*grow)(void* ctx, size_t slots,
+                                               size_t entries),
+                           void* grow_ctx);
+
+}  // namespace lvb

@@ -1,0 +1,962 @@
+// move.cu -- local-moving phase of one Louvain level on sm_100a.
+//
+// Reference semantics (upicine/louvain-community-detection):
+//   weighted degree k_v ............... modularity.cu:27-49
+//   m = sum k / 2 ..................... modularity.cu:457-458
+//   singleton state ................... modularity.cu:459-462
+//   buckets, one Jacobi step each ..... modularity.cu:439-499
+//   isLowerIdx eligibility ............ modularity.cu:85-93
+//   gain (FP32) ....................... modularity.cu:149-152
+//   argmax, ties -> lower community ... modularity.cu:169-179,359-368
+//   decision .......................... louvian.py:148-151 (LV_RULE_PY),
+//                                       modularity.cu:182,278,374 (LV_RULE_CUDA)
+//   apply moves + community totals .... modularity.cu:382-398
+//   modularity ........................ modularity.cu:400-436
+//
+// Design (B200-first, not a translation):
+//   * Degree classes are computed once per level (degrees do not change
+//     within a level) by a stable partition; the reference re-partitions
+//     seven times per pass with a host read-back each.
+//   * Neighbour-community weights are summed in FP64 (exact for FP32
+//     inputs of ordinary dynamic range, hence independent of the order in
+//     which concurrent threads add them), then rounded once to FP32 for the
+//     gain, which follows the reference expression operation by operation
+//     with round-to-nearest intrinsics.
+//   * A candidate is evaluated once per distinct neighbour community, and
+//     the argmax is a max over packed (gain, ~community) 64-bit keys, so
+//     the lowest community id wins ties deterministically.
+//   * deg <= 32: G lanes per vertex (G = 4, 8, 16, 32), one edge per lane,
+//     __match_any_sync groups equal communities, no hash table at all.
+//     32 < deg <= 319: one warp per vertex, open-addressing table in shared
+//     memory.  319 < deg <= 2048: one block per vertex, 4096-slot shared
+//     table.  deg > 2048: several blocks per vertex on a global-memory table
+//     sized from the vertex's own degree.
+//   * Community totals are updated incrementally by the moved vertices
+//     only (FP64 atomics), instead of a full recount after every bucket.
+#include "lv_internal.h"
+
+#include <cfloat>
+
+namespace lvb {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+
+__device__ __forceinline__ unsigned long long umax64(unsigned long long a,
+                                                     unsigned long long b) {
+  return a > b ? a : b;
+}
+
+// Total order on floats mapped to unsigned integers.
+__device__ __forceinline__ uint32_t float_key(float f) {
+  uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+// max over keys = max gain, then lowest community id.  0 = no candidate.
+__device__ __forceinline__ unsigned long long pack_best(float gain,
+                                                        uint32_t c) {
+  return ((unsigned long long)float_key(gain) << 32) | (uint32_t)(~c);
+}
+
+struct GainCtx {
+  float m, den, kv, aown_minus_kv;
+  uint32_t cv, szv;
+};
+
+__device__ __forceinline__ GainCtx make_ctx(const LevelView& L, uint32_t v,
+                                            uint32_t cv) {
+  GainCtx g;
+  g.m = L.sc->m;
+  g.den = L.sc->den;
+  g.kv = L.k[v];
+  g.aown_minus_kv = __fsub_rn((float)L.tot[cv], g.kv);
+  g.cv = cv;
+  g.szv = L.comm_sz[cv];
+  return g;
+}
+
+// (e_c / m) + (k_v * ((a_own - k_v) - a_c) / (2 m m))  -- modularity.cu:149
+__device__ __forceinline__ float gain_of(float ec, float ac, const GainCtx& g) {
+  float t1 = __fdiv_rn(ec, g.m);
+  float t2 = __fsub_rn(g.aown_minus_kv, ac);
+  float t3 = __fmul_rn(g.kv, t2);
+  float t4 = __fdiv_rn(t3, g.den);
+  return __fadd_rn(t1, t4);
+}
+
+// Candidate key of neighbour community c with summed weight ec (0 if c is
+// not eligible under isLowerIdx, modularity.cu:85-93).
+__device__ __forceinline__ unsigned long long candidate(const LevelView& L,
+                                                        const GainCtx& g,
+                                                        uint32_t c,
+                                                        double ec) {
+  const uint32_t szc = L.comm_sz[c];
+  if (g.szv == 1 && szc == 1 && !(c < g.cv)) return 0ull;
+  const float gain = gain_of((float)ec, (float)L.tot[c], g);
+  return pack_best(gain, c);
+}
+
+template <int RULE>
+__device__ __forceinline__ uint32_t decide(unsigned long long best, double own,
+                                           const GainCtx& g) {
+  if (best == 0ull) return g.cv;
+  const float bg = key_float((uint32_t)(best >> 32));
+  const uint32_t bc = ~(uint32_t)best;
+  bool move;
+  if (RULE == LV_RULE_CUDA_I) {
+    move = __fsub_rn(bg, __fdiv_rn((float)own, g.m)) > 0.0f;
+  } else {
+    move = bg > 0.0f;
+  }
+  return move ? bc : g.cv;
+}
+
+template <int G>
+__device__ __forceinline__ unsigned long long group_max(unsigned long long x) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) x = umax64(x, __shfl_xor_sync(kFull, x, o));
+  return x;
+}
+template <int G>
+__device__ __forceinline__ double group_sum(double x) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+  return x;
+}
+
+// Open addressing with linear probing; multiplicative hash.  The probe
+// count is bounded by the table size; a full table (impossible when the
+// table holds more slots than the row has entries) sets the error flag.
+__device__ __forceinline__ uint32_t hash_slot(uint32_t key, uint32_t mask) {
+  return (key * 2654435761u) & mask;
+}
+__device__ __forceinline__ uint32_t table_insert(uint32_t* keys, uint32_t mask,
+                                                 uint32_t key,
+                                                 LevelScalars* sc) {
+  uint32_t h = hash_slot(key, mask);
+  for (uint32_t it = 0; it <= mask; it++) {
+    uint32_t cur = keys[h];
+    if (cur == key) return h;
+    if (cur == kEmptyKey) {
+      uint32_t prev = atomicCAS(&keys[h], kEmptyKey, key);
+      if (prev == kEmptyKey || prev == key) return h;
+    }
+    h = (h + 1) & mask;
+  }
+  atomicExch(&sc->error, 1u);
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Move kernels
+// ---------------------------------------------------------------------------
+
+// deg <= G: G lanes per vertex, one edge per lane.
+template <int G, int RULE>
+__global__ void __launch_bounds__(kThreads)
+    move_small_kernel(LevelView L, const uint32_t* __restrict__ verts,
+                      uint32_t count, uint32_t* __restrict__ prop) {
+  __shared__ double sums[kWarps][32];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int gl = lane & (G - 1);
+  const uint32_t per_block = kThreads / G;
+  for (uint32_t base = blockIdx.x * per_block; base < count;
+       base += gridDim.x * per_block) {
+    const uint32_t vidx = base + threadIdx.x / G;
+    const bool vvalid = vidx < count;
+    uint32_t v = 0, d = 0, cv = 0;
+    uint64_t s = 0;
+    if (vvalid) {
+      v = verts[vidx];
+      s = L.off[v];
+      d = (uint32_t)(L.off[v + 1] - s);
+      cv = L.comm[v];
+    }
+    const bool has = gl < (int)d;
+    uint32_t u = 0, cu = 0;
+    float wt = 0.0f;
+    if (has) {
+      u = L.col[s + gl];
+      wt = L.w[s + gl];
+      cu = L.comm[u];
+    }
+    const unsigned long long mk =
+        has ? (((unsigned long long)(lane / G) << 32) | cu)
+            : (0xFFFFFFFF00000000ull | (unsigned)lane);
+    const unsigned peers = __match_any_sync(kFull, mk);
+    const int leader = __ffs(peers) - 1;
+    sums[wib][lane] = 0.0;
+    __syncwarp();
+    if (has) atomicAdd(&sums[wib][leader], (double)wt);
+    double own = 0.0;
+    if (RULE == LV_RULE_CUDA_I && has && cu == cv && u != v) own = (double)wt;
+    __syncwarp();
+    unsigned long long best = 0ull;
+    GainCtx g;
+    if (vvalid) g = make_ctx(L, v, cv);
+    if (has && leader == lane) best = candidate(L, g, cu, sums[wib][lane]);
+    best = group_max<G>(best);
+    if (RULE == LV_RULE_CUDA_I) own = group_sum<G>(own);
+    if (vvalid && gl == 0) prop[vidx] = decide<RULE>(best, own, g);
+    __syncwarp();
+  }
+}
+
+// 32 < deg <= 319: one warp per vertex, T-slot table per warp.
+template <int T, int RULE>
+__global__ void __launch_bounds__(kThreads)
+    move_warp_kernel(LevelView L, const uint32_t* __restrict__ verts,
+                     uint32_t count, uint32_t* __restrict__ prop) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double* vals = reinterpret_cast<double*>(smem_raw) + wib * T;
+  uint32_t* keys =
+      reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T * kWarps) + wib * T;
+  for (uint32_t vidx = blockIdx.x * kWarps + wib; vidx < count;
+       vidx += gridDim.x * kWarps) {
+    for (int i = lane; i < T; i += 32) {
+      keys[i] = kEmptyKey;
+      vals[i] = 0.0;
+    }
+    __syncwarp();
+    const uint32_t v = verts[vidx];
+    const uint64_t s = L.off[v];
+    const uint32_t d = (uint32_t)(L.off[v + 1] - s);
+    const uint32_t cv = L.comm[v];
+    double own = 0.0;
+    for (uint32_t j0 = 0; j0 < d; j0 += 32) {
+      const uint32_t j = j0 + lane;
+      const bool has = j < d;
+      uint32_t u = 0, cu = kEmptyKey;
+      float wt = 0.0f;
+      if (has) {
+        u = L.col[s + j];
+        wt = L.w[s + j];
+        cu = L.comm[u];
+      }
+      const unsigned long long mk =
+          has ? (unsigned long long)cu : (0x100000000ull | (unsigned)lane);
+      const unsigned peers = __match_any_sync(kFull, mk);
+      const int leader = __ffs(peers) - 1;
+      uint32_t slot = 0;
+      if (has && lane == leader) slot = table_insert(keys, T - 1, cu, L.sc);
+      slot = __shfl_sync(kFull, slot, leader);
+      if (has) atomicAdd(&vals[slot], (double)wt);
+      if (RULE == LV_RULE_CUDA_I && has && cu == cv && u != v) own += (double)wt;
+    }
+    __syncwarp();
+    const GainCtx g = make_ctx(L, v, cv);
+    unsigned long long best = 0ull;
+    for (int i = lane; i < T; i += 32) {
+      const uint32_t c = keys[i];
+      if (c != kEmptyKey) best = umax64(best, candidate(L, g, c, vals[i]));
+    }
+    best = group_max<32>(best);
+    if (RULE == LV_RULE_CUDA_I) own = group_sum<32>(own);
+    if (lane == 0) prop[vidx] = decide<RULE>(best, own, g);
+    __syncwarp();
+  }
+}
+
+__device__ __forceinline__ unsigned long long block_max(unsigned long long x,
+                                                        unsigned long long* red) {
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  x = group_max<32>(x);
+  if (lane == 0) red[wib] = x;
+  __syncthreads();
+  unsigned long long r = 0ull;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kWarps; i++) r = umax64(r, red[i]);
+  }
+  __syncthreads();
+  return r;  // valid in thread 0
+}
+
+__device__ __forceinline__ double block_sum(double x, double* red) {
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  x = group_sum<32>(x);
+  if (lane == 0) red[wib] = x;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kWarps; i++) r += red[i];
+  }
+  __syncthreads();
+  return r;  // valid in thread 0
+}
+
+// Inserts one wave of a block's edges [j0, j0 + kThreads) into a table.
+template <int RULE>
+__device__ __forceinline__ void insert_wave(const LevelView& L, uint64_t s,
+                                            uint64_t j, uint64_t end,
+                                            uint32_t v, uint32_t cv,
+                                            uint32_t* keys, double* vals,
+                                            uint32_t mask, double& own) {
+  const int lane = threadIdx.x & 31;
+  const bool has = j < end;
+  uint32_t u = 0, cu = kEmptyKey;
+  float wt = 0.0f;
+  if (has) {
+    u = L.col[s + j];
+    wt = L.w[s + j];
+    cu = L.comm[u];
+  }
+  const unsigned long long mk =
+      has ? (unsigned long long)cu : (0x100000000ull | (unsigned)lane);
+  const unsigned peers = __match_any_sync(kFull, mk);
+  const int leader = __ffs(peers) - 1;
+  uint32_t slot = 0;
+  if (has && lane == leader) slot = table_insert(keys, mask, cu, L.sc);
+  slot = __shfl_sync(kFull, slot, leader);
+  if (has) atomicAdd(&vals[slot], (double)wt);
+  if (RULE == LV_RULE_CUDA_I && has && cu == cv && u != v) own += (double)wt;
+}
+
+// 319 < deg <= 2048: one block per vertex, shared 4096-slot table.
+template <int RULE>
+__global__ void __launch_bounds__(kThreads)
+    move_block_kernel(LevelView L, const uint32_t* __restrict__ verts,
+                      uint32_t count, uint32_t* __restrict__ prop) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int T = kHubSmemSlots;
+  double* vals = reinterpret_cast<double*>(smem_raw);
+  uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T);
+  __shared__ unsigned long long red_best[kWarps];
+  __shared__ double red_own[kWarps];
+  for (uint32_t vidx = blockIdx.x; vidx < count; vidx += gridDim.x) {
+    for (int i = threadIdx.x; i < T; i += kThreads) {
+      keys[i] = kEmptyKey;
+      vals[i] = 0.0;
+    }
+    __syncthreads();
+    const uint32_t v = verts[vidx];
+    const uint64_t s = L.off[v];
+    const uint32_t d = (uint32_t)(L.off[v + 1] - s);
+    const uint32_t cv = L.comm[v];
+    double own = 0.0;
+    for (uint32_t j0 = 0; j0 < d; j0 += kThreads)
+      insert_wave<RULE>(L, s, j0 + threadIdx.x, d, v, cv, keys, vals, T - 1, own);
+    __syncthreads();
+    const GainCtx g = make_ctx(L, v, cv);
+    unsigned long long best = 0ull;
+    for (int i = threadIdx.x; i < T; i += kThreads) {
+      const uint32_t c = keys[i];
+      if (c != kEmptyKey) best = umax64(best, candidate(L, g, c, vals[i]));
+    }
+    best = block_max(best, red_best);
+    if (RULE == LV_RULE_CUDA_I) own = block_sum(own, red_own);
+    if (threadIdx.x == 0) prop[vidx] = decide<RULE>(best, own, g);
+    __syncthreads();
+  }
+}
+
+// deg > 2048: the vertex's edges are split in chunks of kHubChunk, one
+// block per chunk, all inserting into the vertex's global table.
+template <int RULE>
+__global__ void __launch_bounds__(kThreads)
+    hub_insert_kernel(LevelView L, const uint32_t* __restrict__ hubs,
+                      HubArena H, uint32_t hub_blocks) {
+  __shared__ double red_own[kWarps];
+  for (uint32_t b = blockIdx.x; b < hub_blocks; b += gridDim.x) {
+    const uint32_t hi = H.blk_vertex[b], ch = H.blk_chunk[b];
+    const uint32_t v = hubs[hi];
+    const uint64_t s = L.off[v];
+    const uint64_t d = L.off[v + 1] - s;
+    const uint32_t cv = L.comm[v];
+    const uint64_t lo = (uint64_t)ch * kHubChunk;
+    const uint64_t end = min(d, lo + kHubChunk);
+    uint32_t* keys = H.keys + H.tab_off[hi];
+    double* vals = H.vals + H.tab_off[hi];
+    const uint32_t mask = H.tab_size[hi] - 1;
+    double own = 0.0;
+    for (uint64_t j0 = lo; j0 < end; j0 += kThreads)
+      insert_wave<RULE>(L, s, j0 + threadIdx.x, end, v, cv, keys, vals, mask, own);
+    if (RULE == LV_RULE_CUDA_I) {
+      own = block_sum(own, red_own);
+      if (threadIdx.x == 0 && own != 0.0) atomicAdd(&H.own[hi], own);
+    }
+  }
+}
+
+// Evaluates the hub tables' candidates (each block a slice of one table),
+// clears the slots it read, and folds its best key into H.best.
+__global__ void __launch_bounds__(kThreads)
+    hub_scan_kernel(LevelView L, const uint32_t* __restrict__ hubs, HubArena H,
+                    uint32_t hub_blocks) {
+  __shared__ unsigned long long red_best[kWarps];
+  for (uint32_t b = blockIdx.x; b < hub_blocks; b += gridDim.x) {
+    const uint32_t hi = H.blk_vertex[b], ch = H.blk_chunk[b];
+    const uint32_t nch = H.blk_nchunks[b];
+    const uint32_t v = hubs[hi];
+    const uint32_t cv = L.comm[v];
+    const GainCtx g = make_ctx(L, v, cv);
+    const uint64_t T = H.tab_size[hi];
+    const uint64_t lo = T * ch / nch, hi_s = T * (ch + 1) / nch;
+    uint32_t* keys = H.keys + H.tab_off[hi];
+    double* vals = H.vals + H.tab_off[hi];
+    unsigned long long best = 0ull;
+    for (uint64_t i = lo + threadIdx.x; i < hi_s; i += kThreads) {
+      const uint32_t c = keys[i];
+      if (c != kEmptyKey) {
+        best = umax64(best, candidate(L, g, c, vals[i]));
+        keys[i] = kEmptyKey;
+        vals[i] = 0.0;
+      }
+    }
+    best = block_max(best, red_best);
+    if (threadIdx.x == 0 && best) atomicMax(&H.best[hi], best);
+  }
+}
+
+template <int RULE>
+__global__ void hub_decide_kernel(LevelView L, const uint32_t* __restrict__ hubs,
+                                  HubArena H, uint32_t hub_count,
+                                  uint32_t* __restrict__ prop) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < hub_count;
+       i += gridDim.x * blockDim.x) {
+    const uint32_t v = hubs[i];
+    const GainCtx g = make_ctx(L, v, L.comm[v]);
+    prop[i] = decide<RULE>(H.best[i], H.own[i], g);
+    H.best[i] = 0ull;
+    H.own[i] = 0.0;
+  }
+}
+
+// Applies a bucket's proposals (assignCommunity + incremental totals).
+__global__ void __launch_bounds__(kThreads)
+    apply_kernel(LevelView L, const uint32_t* __restrict__ verts,
+                 const uint32_t* __restrict__ prop, uint32_t count) {
+  for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < count;
+       i += gridDim.x * kThreads) {
+    const uint32_t v = verts[i];
+    const uint32_t nc = prop[i];
+    const uint32_t oc = L.comm[v];
+    if (nc != oc) {
+      atomicSub(&L.comm_sz[oc], 1u);
+      atomicAdd(&L.comm_sz[nc], 1u);
+      const double kv = (double)L.k[v];
+      atomicAdd(&L.tot[oc], -kv);
+      atomicAdd(&L.tot[nc], kv);
+      L.comm[v] = nc;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Class-dispatch row reductions (row sums at level start, modularity sweep)
+// ---------------------------------------------------------------------------
+struct DispatchArgs {
+  DispatchPlan P;
+  const uint32_t* order;
+  const uint32_t* hub_blk_vertex;
+  const uint32_t* hub_blk_chunk;
+  double* hub_acc;
+  double* partials;  // [2 * gridDim.x]
+};
+
+// Row sum: k_v = (float) sum_j w_vj.
+struct RowSumOp {
+  __device__ uint32_t ctx(const LevelView&, uint32_t) const { return 0; }
+  __device__ double edge(const LevelView&, uint32_t, uint32_t, float w) const {
+    return (double)w;
+  }
+  __device__ void vertex(const LevelView& L, uint32_t v, double sum,
+                         double& part) const {
+    const float kf = (float)sum;
+    L.k[v] = kf;
+    L.tot[v] = (double)kf;
+    part += (double)kf;
+  }
+  __device__ void hub(const DispatchArgs& A, uint32_t hi, double sum,
+                      double&) const {
+    atomicAdd(&A.hub_acc[hi], sum);
+  }
+};
+
+// Intra-community weight: sum_j w_vj [comm(u) == comm(v)].
+struct IntraOp {
+  __device__ uint32_t ctx(const LevelView& L, uint32_t v) const {
+    return L.comm[v];
+  }
+  __device__ double edge(const LevelView& L, uint32_t cv, uint32_t u,
+                         float w) const {
+    return L.comm[u] == cv ? (double)w : 0.0;
+  }
+  __device__ void vertex(const LevelView&, uint32_t, double sum,
+                         double& part) const {
+    part += sum;
+  }
+  __device__ void hub(const DispatchArgs&, uint32_t, double sum,
+                      double& part) const {
+    part += sum;
+  }
+};
+
+template <int G, class Op>
+__device__ __forceinline__ void unit_small(const LevelView& L,
+                                           const DispatchArgs& A, int cls,
+                                           uint32_t unit, const Op& op,
+                                           double& part) {
+  const int lane = threadIdx.x & 31, gl = lane & (G - 1);
+  const uint32_t cnt = A.P.cls_start[cls + 1] - A.P.cls_start[cls];
+  const uint32_t idx = (unit - A.P.blk_start[cls]) * (kThreads / G) + threadIdx.x / G;
+  double x = 0.0;
+  uint32_t v = 0;
+  if (idx < cnt) {
+    v = A.order[A.P.cls_start[cls] + idx];
+    const uint64_t s = L.off[v];
+    const uint32_t d = (uint32_t)(L.off[v + 1] - s);
+    if (gl < (int)d) {
+      const uint32_t c = op.ctx(L, v);
+      x = op.edge(L, c, L.col[s + gl], L.w[s + gl]);
+    }
+  }
+  x = group_sum<G>(x);
+  if (idx < cnt && gl == 0) op.vertex(L, v, x, part);
+}
+
+template <class Op>
+__device__ __forceinline__ void unit_warp(const LevelView& L,
+                                          const DispatchArgs& A, int cls,
+                                          uint32_t unit, const Op& op,
+                                          double& part) {
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t cnt = A.P.cls_start[cls + 1] - A.P.cls_start[cls];
+  const uint32_t idx = (unit - A.P.blk_start[cls]) * kWarps + wib;
+  if (idx >= cnt) return;  // warp-uniform
+  const uint32_t v = A.order[A.P.cls_start[cls] + idx];
+  const uint64_t s = L.off[v];
+  const uint32_t d = (uint32_t)(L.off[v + 1] - s);
+  const uint32_t c = op.ctx(L, v);
+  double x = 0.0;
+  for (uint32_t j = lane; j < d; j += 32) x += op.edge(L, c, L.col[s + j], L.w[s + j]);
+  x = group_sum<32>(x);
+  if (lane == 0) op.vertex(L, v, x, part);
+}
+
+template <class Op>
+__device__ __forceinline__ void unit_block(const LevelView& L,
+                                           const DispatchArgs& A,
+                                           uint32_t unit, const Op& op,
+                                           double& part, double* red) {
+  const uint32_t idx = unit - A.P.blk_start[7];
+  const uint32_t v = A.order[A.P.cls_start[7] + idx];
+  const uint64_t s = L.off[v];
+  const uint32_t d = (uint32_t)(L.off[v + 1] - s);
+  const uint32_t c = op.ctx(L, v);
+  double x = 0.0;
+  for (uint32_t j = threadIdx.x; j < d; j += kThreads)
+    x += op.edge(L, c, L.col[s + j], L.w[s + j]);
+  x = block_sum(x, red);
+  if (threadIdx.x == 0) op.vertex(L, v, x, part);
+}
+
+template <class Op>
+__device__ __forceinline__ void unit_hub(const LevelView& L,
+                                         const DispatchArgs& A, uint32_t unit,
+                                         const Op& op, double& part,
+                                         double* red) {
+  const uint32_t hb = unit - A.P.blk_start[8];
+  const uint32_t hi = A.hub_blk_vertex[hb], ch = A.hub_blk_chunk[hb];
+  const uint32_t v = A.order[A.P.cls_start[8] + hi];
+  const uint64_t s = L.off[v];
+  const uint64_t d = L.off[v + 1] - s;
+  const uint64_t lo = (uint64_t)ch * kHubChunk, end = min(d, lo + kHubChunk);
+  const uint32_t c = op.ctx(L, v);
+  double x = 0.0;
+  for (uint64_t j = lo + threadIdx.x; j < end; j += kThreads)
+    x += op.edge(L, c, L.col[s + j], L.w[s + j]);
+  x = block_sum(x, red);
+  if (threadIdx.x == 0) op.hub(A, hi, x, part);
+}
+
+// Deterministic block reduction into partials, then the last block to
+// finish sums all partials in index order.
+__device__ __forceinline__ bool publish_and_check_last(double a, double b,
+                                                       const DispatchArgs& A,
+                                                       LevelScalars* sc,
+                                                       double* red) {
+  __shared__ bool last;
+  double ra = block_sum(a, red);
+  double rb = block_sum(b, red);
+  if (threadIdx.x == 0) {
+    A.partials[blockIdx.x] = ra;
+    A.partials[gridDim.x + blockIdx.x] = rb;
+    __threadfence();
+    const uint32_t t = atomicAdd(&sc->done_blocks, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+__device__ __forceinline__ void sum_partials(const DispatchArgs& A, double* red,
+                                             double& a, double& b) {
+  double x = 0.0, y = 0.0;
+  for (uint32_t i = threadIdx.x; i < gridDim.x; i += kThreads) {
+    x += __ldcg(&A.partials[i]);
+    y += __ldcg(&A.partials[gridDim.x + i]);
+  }
+  a = block_sum(x, red);
+  b = block_sum(y, red);
+}
+
+template <class Op>
+__device__ __forceinline__ void dispatch_units(const LevelView& L,
+                                               const DispatchArgs& A,
+                                               const Op& op, double& part,
+                                               double* red) {
+  for (uint32_t unit = blockIdx.x; unit < A.P.total_blocks; unit += gridDim.x) {
+    int cls = 8;
+    while (cls > 1 && unit < A.P.blk_start[cls]) cls--;
+    switch (cls) {  // block-uniform
+      case 1: unit_small<4>(L, A, 1, unit, op, part); break;
+      case 2: unit_small<8>(L, A, 2, unit, op, part); break;
+      case 3: unit_small<16>(L, A, 3, unit, op, part); break;
+      case 4: unit_small<32>(L, A, 4, unit, op, part); break;
+      case 5:
+      case 6: unit_warp(L, A, cls, unit, op, part); break;
+      case 7: unit_block(L, A, unit, op, part, red); break;
+      default: unit_hub(L, A, unit, op, part, red); break;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    level_init_kernel(LevelView L, DispatchArgs A) {
+  __shared__ double red[kWarps];
+  double part = 0.0;
+  dispatch_units(L, A, RowSumOp{}, part, red);
+  // singleton state for a slice of ids (modularity.cu:459-462)
+  const uint32_t chunk = (L.n + gridDim.x - 1) / gridDim.x;
+  const uint32_t c0 = blockIdx.x * chunk;
+  const uint32_t c1 = min(L.n, c0 + chunk);
+  for (uint32_t c = c0 + threadIdx.x; c < c1; c += kThreads) {
+    L.comm[c] = c;
+    L.comm_sz[c] = 1u;
+    if (L.off[c + 1] == L.off[c]) {
+      L.k[c] = 0.0f;
+      L.tot[c] = 0.0;
+    }
+  }
+  if (!publish_and_check_last(part, 0.0, A, L.sc, red)) return;
+  double msum, unused;
+  sum_partials(A, red, msum, unused);
+  // hubs: finalise their row sums in index order
+  double hs = 0.0;
+  for (uint32_t i = threadIdx.x; i < A.P.hub_count; i += kThreads) {
+    const uint32_t v = A.order[A.P.cls_start[8] + i];
+    const float kf = (float)__ldcg(&A.hub_acc[i]);
+    L.k[v] = kf;
+    L.tot[v] = (double)kf;
+    A.hub_acc[i] = 0.0;
+    hs += (double)kf;
+  }
+  hs = block_sum(hs, red);
+  if (threadIdx.x == 0) {
+    const double m64 = (msum + hs) / 2.0;
+    const float m = (float)m64;
+    L.sc->m64 = m64;
+    L.sc->m = m;
+    L.sc->den = __fmul_rn(__fmul_rn(2.0f, m), m);
+    L.sc->done_blocks = 0u;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    modularity_kernel(LevelView L, DispatchArgs A) {
+  __shared__ double red[kWarps];
+  double part = 0.0;
+  dispatch_units(L, A, IntraOp{}, part, red);
+  const uint32_t chunk = (L.n + gridDim.x - 1) / gridDim.x;
+  const uint32_t c0 = blockIdx.x * chunk;
+  const uint32_t c1 = min(L.n, c0 + chunk);
+  double asq = 0.0;
+  for (uint32_t c = c0 + threadIdx.x; c < c1; c += kThreads) {
+    const double a = L.tot[c];
+    asq += a * a;
+  }
+  if (!publish_and_check_last(part, asq, A, L.sc, red)) return;
+  double intra, sq;
+  sum_partials(A, red, intra, sq);
+  if (threadIdx.x == 0) {
+    const double m = L.sc->m64;
+    L.sc->intra = intra;
+    L.sc->asq = sq;
+    L.sc->q = (m > 0.0) ? (intra / (2.0 * m)) - (sq / (4.0 * m * m)) : 0.0;
+    L.sc->done_blocks = 0u;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Small helpers
+// ---------------------------------------------------------------------------
+__global__ void compose_kernel(uint32_t* a, size_t n, const uint32_t* map) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    a[i] = map[a[i]];
+}
+__global__ void iota_kernel(uint32_t* a, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    a[i] = (uint32_t)i;
+}
+__global__ void recount_zero_kernel(LevelView L) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n;
+       i += gridDim.x * blockDim.x) {
+    L.comm_sz[i] = 0u;
+    L.tot[i] = 0.0;
+  }
+}
+__global__ void recount_kernel(LevelView L) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < L.n;
+       v += gridDim.x * blockDim.x) {
+    const uint32_t c = L.comm[v];
+    atomicAdd(&L.comm_sz[c], 1u);
+    atomicAdd(&L.tot[c], (double)L.k[v]);
+  }
+}
+__global__ void bucket_ids_kernel(const uint64_t* off, uint32_t n, uint8_t* out) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += gridDim.x * blockDim.x) {
+    const uint64_t d = off[v + 1] - off[v];
+    int c = move_class_of_degree(d);
+    out[v] = (uint8_t)(c == 8 ? 7 : c);
+  }
+}
+// FP64 modularity of an arbitrary partition (part[v] < n).
+__global__ void part_totals_kernel(const LevelView L, const uint32_t* part,
+                                   double* tot) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < L.n;
+       v += gridDim.x * blockDim.x) {
+    double k = 0.0;
+    for (uint64_t j = L.off[v]; j < L.off[v + 1]; j++) k += (double)L.w[j];
+    atomicAdd(&tot[part[v]], k);
+  }
+}
+__global__ void part_q_kernel(const LevelView L, const uint32_t* part,
+                              const double* tot, double* out /*[3]*/) {
+  __shared__ double red[kWarps];
+  double intra = 0.0, sq = 0.0, all = 0.0;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < L.n;
+       v += gridDim.x * blockDim.x) {
+    const uint32_t p = part[v];
+    for (uint64_t j = L.off[v]; j < L.off[v + 1]; j++) {
+      all += (double)L.w[j];
+      if (part[L.col[j]] == p) intra += (double)L.w[j];
+    }
+    sq += tot[v] * tot[v];
+  }
+  intra = block_sum(intra, red);
+  sq = block_sum(sq, red);
+  all = block_sum(all, red);
+  if (threadIdx.x == 0) {
+    atomicAdd(&out[0], intra);
+    atomicAdd(&out[1], sq);
+    atomicAdd(&out[2], all);
+  }
+}
+
+unsigned grid_for(uint64_t work_blocks, unsigned cap) {
+  if (work_blocks == 0) return 0;
+  return (unsigned)(work_blocks < cap ? work_blocks : cap);
+}
+
+unsigned sm_count() { return sm_count_cached(); }
+
+DispatchArgs make_args(const uint32_t* order, const DispatchPlan& P,
+                       const uint32_t* hub_map, double* partials) {
+  DispatchArgs A;
+  A.P = P;
+  A.order = order;
+  A.hub_blk_vertex = hub_map;
+  A.hub_blk_chunk = hub_map ? hub_map + P.hub_blocks : nullptr;
+  A.hub_acc = partials;  // first hub_count doubles; partials follow
+  A.partials = partials + P.hub_count;
+  return A;
+}
+
+}  // namespace
+
+unsigned sm_count_cached() {
+  static int num_sms = 0;
+  if (!num_sms) {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    num_sms = v > 0 ? v : 148;
+  }
+  return (unsigned)num_sms;
+}
+
+cudaError_t configure_kernels() {
+  cudaError_t e;
+  const int warp512 = kWarps * 512 * 12;
+  const int block_tab = kHubSmemSlots * 12;
+  e = cudaFuncSetAttribute(move_warp_kernel<512, LV_RULE_PY_I>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, warp512);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(move_warp_kernel<512, LV_RULE_CUDA_I>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, warp512);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(move_block_kernel<LV_RULE_PY_I>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, block_tab);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(move_block_kernel<LV_RULE_CUDA_I>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, block_tab);
+  if (e != cudaSuccess) return e;
+  return configure_contract_kernels();
+}
+
+unsigned dispatch_grid(const DispatchPlan& P) {
+  return grid_for(P.total_blocks ? P.total_blocks : 1, sm_count() * 8);
+}
+
+cudaError_t launch_level_init(const LevelView& L, const uint32_t* order,
+                              const DispatchPlan& P, const uint32_t* hub_map,
+                              double* partials, cudaStream_t st) {
+  DispatchArgs A = make_args(order, P, hub_map, partials);
+  (count_launches(1), level_init_kernel<<<dispatch_grid(P), kThreads, 0, st>>>(L, A));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_modularity(const LevelView& L, const uint32_t* order,
+                              const DispatchPlan& P, const uint32_t* hub_map,
+                              double* partials, cudaStream_t st) {
+  DispatchArgs A = make_args(order, P, hub_map, partials);
+  (count_launches(1), modularity_kernel<<<dispatch_grid(P), kThreads, 0, st>>>(L, A));
+  return cudaGetLastError();
+}
+
+template <int RULE>
+static cudaError_t move_bucket_impl(const LevelView& L, int bucket,
+                                    const uint32_t* order, uint32_t* prop,
+                                    const DispatchPlan& P, const HubArena& H,
+                                    cudaStream_t st) {
+  const unsigned cap = sm_count() * 8;
+  const uint32_t s = P.cls_start[bucket];
+  const uint32_t cnt = P.cls_start[bucket + 1] - s;
+  const uint32_t* verts = order + s;
+  uint32_t* pr = prop + s;
+  switch (bucket) {
+    case 1:
+      if (cnt) (count_launches(1), move_small_kernel<4, RULE><<<grid_for((cnt + 63) / 64, cap), kThreads, 0, st>>>(L, verts, cnt, pr));
+      break;
+    case 2:
+      if (cnt) (count_launches(1), move_small_kernel<8, RULE><<<grid_for((cnt + 31) / 32, cap), kThreads, 0, st>>>(L, verts, cnt, pr));
+      break;
+    case 3:
+      if (cnt) (count_launches(1), move_small_kernel<16, RULE><<<grid_for((cnt + 15) / 16, cap), kThreads, 0, st>>>(L, verts, cnt, pr));
+      break;
+    case 4:
+      if (cnt) (count_launches(1), move_small_kernel<32, RULE><<<grid_for((cnt + 7) / 8, cap), kThreads, 0, st>>>(L, verts, cnt, pr));
+      break;
+    case 5:
+      if (cnt) {
+        constexpr int T = 128;
+        (count_launches(1), move_warp_kernel<T, RULE><<<grid_for((cnt + 7) / 8, cap), kThreads,
+                                    kWarps * T * 12, st>>>(L, verts, cnt, pr));
+      }
+      break;
+    case 6:
+      if (cnt) {
+        constexpr int T = 512;
+        (count_launches(1), move_warp_kernel<T, RULE><<<grid_for((cnt + 7) / 8, sm_count() * 4), kThreads,
+                                    kWarps * T * 12, st>>>(L, verts, cnt, pr));
+      }
+      break;
+    case 7: {
+      // class 7: shared table; class 8: global tables
+      if (cnt) {
+        (count_launches(1), move_block_kernel<RULE><<<grid_for(cnt, sm_count() * 4), kThreads,
+                                  kHubSmemSlots * 12, st>>>(L, verts, cnt, pr));
+      }
+      const uint32_t hs = P.cls_start[8];
+      const uint32_t hc = P.cls_start[9] - hs;
+      if (hc) {
+        (count_launches(1), hub_insert_kernel<RULE><<<grid_for(P.hub_blocks, cap), kThreads, 0, st>>>(
+            L, order + hs, H, P.hub_blocks));
+        (count_launches(1), hub_scan_kernel<<<grid_for(P.hub_blocks, cap), kThreads, 0, st>>>(
+            L, order + hs, H, P.hub_blocks));
+        (count_launches(1), hub_decide_kernel<RULE><<<(hc + 127) / 128, 128, 0, st>>>(
+            L, order + hs, H, hc, prop + hs));
+      }
+      break;
+    }
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_move_bucket(const LevelView& L, int bucket, int rule,
+                               const uint32_t* order, uint32_t* proposal,
+                               const DispatchPlan& P, const HubArena& H,
+                               cudaStream_t st) {
+  if (rule == LV_RULE_CUDA_I)
+    return move_bucket_impl<LV_RULE_CUDA_I>(L, bucket, order, proposal, P, H, st);
+  return move_bucket_impl<LV_RULE_PY_I>(L, bucket, order, proposal, P, H, st);
+}
+
+cudaError_t launch_apply_bucket(const LevelView& L, int bucket,
+                                const uint32_t* order,
+                                const uint32_t* proposal,
+                                const DispatchPlan& P, cudaStream_t st) {
+  const uint32_t s = P.cls_start[bucket];
+  const uint32_t e = (bucket == 7) ? P.cls_start[9] : P.cls_start[bucket + 1];
+  const uint32_t cnt = e - s;
+  if (!cnt) return cudaSuccess;
+  (count_launches(1), apply_kernel<<<grid_for((cnt + kThreads - 1) / kThreads, sm_count() * 8), kThreads, 0, st>>>(
+      L, order + s, proposal + s, cnt));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_compose(uint32_t* assignment, size_t n0,
+                           const uint32_t* map, cudaStream_t st) {
+  if (!n0) return cudaSuccess;
+  (count_launches(1), compose_kernel<<<grid_for((n0 + 255) / 256, sm_count() * 8), 256, 0, st>>>(assignment, n0, map));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_iota(uint32_t* a, size_t n, cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  (count_launches(1), iota_kernel<<<grid_for((n + 255) / 256, sm_count() * 8), 256, 0, st>>>(a, n));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_recount(const LevelView& L, cudaStream_t st) {
+  if (!L.n) return cudaSuccess;
+  const unsigned g = grid_for((L.n + 255) / 256, sm_count() * 8);
+  (count_launches(1), recount_zero_kernel<<<g, 256, 0, st>>>(L));
+  (count_launches(1), recount_kernel<<<g, 256, 0, st>>>(L));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bucket_ids(const uint64_t* off, uint32_t n, uint8_t* out,
+                              cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  (count_launches(1), bucket_ids_kernel<<<grid_for((n + 255) / 256, sm_count() * 8), 256, 0, st>>>(off, n, out));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_modularity_of(const LevelView& L, const uint32_t* part,
+                                 double* tot_scratch, double* out,
+                                 cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(tot_scratch, 0, sizeof(double) * (L.n ? L.n : 1), st);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(out, 0, sizeof(double) * 3, st);
+  if (e != cudaSuccess) return e;
+  if (!L.n) return cudaSuccess;
+  const unsigned g = grid_for((L.n + 255) / 256, sm_count() * 8);
+  (count_launches(1), part_totals_kernel<<<g, 256, 0, st>>>(L, part, tot_scratch));
+  (count_launches(1), part_q_kernel<<<g, kThreads, 0, st>>>(L, part, tot_scratch, out));
+  return cudaGetLastError();
+}
+
+}  // namespace lvb

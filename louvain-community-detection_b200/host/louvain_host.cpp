@@ -1,0 +1,160 @@
+// louvain_host.cpp -- the reference-named C++ host API over the C ABI.
+#include "louvain_host.h"
+
+#include <getopt.h>
+
+#include <cstdlib>
+#include <iostream>
+#include <iterator>
+
+namespace lvb_host {
+
+static void check(lv_status s) {
+  if (s != LV_OK) throw Error(s, lv_last_error());
+}
+
+void parseGraph(Graph& graph, const char* filename) {
+  lv_graph* g = nullptr;
+  check(lv_graph_load_mtx(filename, &g));
+  graph.host = g;
+  uint32_t n = 0, md = 0;
+  uint64_t e = 0;
+  check(lv_graph_view(g, &n, &e, nullptr, nullptr, nullptr, &md));
+  graph.vert_sz = n;
+  graph.init_sz = n;
+  graph.edges_sz = e;
+  graph.max_deg = md;
+}
+
+void initDevGraph(Graph& dev_graph, const Graph& host_graph, const lv_config* cfg) {
+  lv_engine* e = nullptr;
+  check(lv_engine_create(cfg, &e));
+  dev_graph.dev = e;
+  dev_graph.rule = cfg ? cfg->rule : LV_RULE_PY;
+  lv_status s = lv_engine_load(e, host_graph.host);
+  if (s != LV_OK) {
+    lv_engine_destroy(e);
+    dev_graph.dev = nullptr;
+    check(s);
+  }
+  dev_graph.vert_sz = host_graph.vert_sz;
+  dev_graph.init_sz = host_graph.init_sz;
+  dev_graph.edges_sz = host_graph.edges_sz;
+  dev_graph.max_deg = host_graph.max_deg;
+}
+
+bool modularityOptimization(Graph& dev_graph, float threshold) {
+  int more = 0;
+  double q = 0.0;
+  check(lv_phase_move(dev_graph.dev, threshold, &more, &q));
+  if (!more) {
+    // modularity.cu:504 prints the FP32 value with default stream format
+    std::cout << static_cast<float>(q) << std::endl;
+  }
+  return more != 0;
+}
+
+void aggregation(Graph& dev_graph) {
+  check(lv_phase_aggregate(dev_graph.dev));
+  uint32_t n = 0;
+  uint64_t e = 0;
+  check(lv_get_level_size(dev_graph.dev, &n, &e));
+  dev_graph.vert_sz = n;
+  dev_graph.edges_sz = e;
+}
+
+void printCommunities(Graph& dev_graph) {
+  std::vector<uint32_t> comm(dev_graph.init_sz);
+  check(lv_get_assignment(dev_graph.dev, comm.data(), comm.size()));
+  std::vector<std::vector<unsigned int>> comm_vert(dev_graph.vert_sz);
+  for (size_t i = 0; i < dev_graph.init_sz; i++) {
+    if (comm[i] < comm_vert.size()) comm_vert[comm[i]].push_back((unsigned)i + 1);
+  }
+  unsigned int comm_n = 1;
+  std::cout << dev_graph.vert_sz << std::endl;
+  for (size_t i = 0; i < dev_graph.vert_sz; i++) {
+    if (!comm_vert[i].empty()) {
+      std::cout << comm_n << " ";
+      std::copy(comm_vert[i].begin(), comm_vert[i].end(),
+                std::ostream_iterator<unsigned int>(std::cout, " "));
+      std::cout << std::endl;
+      comm_n++;
+    }
+  }
+}
+
+void parseArgs(int argc, char** argv, float& threshold, bool& verbose,
+               char*& filename, lv_rule& rule, bool& timing) {
+  static const struct option longopts[] = {
+      {"rule", required_argument, nullptr, 'r'},
+      {"timing", no_argument, nullptr, 't'},
+      {nullptr, 0, nullptr, 0}};
+  const char* usage = "Usage: ./gpulouvain -f mtx-matrix-file -g min-gain [-v]";
+  bool fopt = false, gopt = false;
+  int c;
+  while ((c = getopt_long(argc, argv, "f:g:v", longopts, nullptr)) != -1) {
+    switch (c) {
+      case 'f':
+        filename = optarg;
+        fopt = true;
+        break;
+      case 'g':
+        try {
+          threshold = std::stof(std::string(optarg));
+        } catch (const std::invalid_argument& ia) {
+          std::cout << "-g option invalid argument: " << ia.what() << std::endl;
+          exit(1);
+        } catch (const std::out_of_range& oor) {
+          std::cout << "-g option error out of range: " << oor.what() << std::endl;
+          exit(1);
+        }
+        gopt = true;
+        break;
+      case 'v':
+        verbose = true;
+        break;
+      case 'r':
+        if (std::string(optarg) == "py") {
+          rule = LV_RULE_PY;
+        } else if (std::string(optarg) == "cuda") {
+          rule = LV_RULE_CUDA;
+        } else {
+          std::cout << "--rule must be py or cuda" << std::endl;
+          exit(1);
+        }
+        break;
+      case 't':
+        timing = true;
+        break;
+      case '?':
+        std::cout << usage << std::endl;
+        exit(1);
+      default:
+        std::cout << "?? arg_parser error ??" << std::endl;
+    }
+  }
+  if (!fopt || !gopt) {
+    std::cout << usage << std::endl;
+    exit(1);
+  }
+}
+
+void deleteDevGraph(Graph& dev_graph) {
+  lv_engine_destroy(dev_graph.dev);
+  dev_graph.dev = nullptr;
+}
+
+void deleteHostGraph(Graph& host_graph) {
+  lv_graph_destroy(host_graph.host);
+  host_graph.host = nullptr;
+}
+
+std::vector<lv_level_info> levelInfo(Graph& dev_graph) {
+  uint32_t count = 0;
+  check(lv_get_levels(dev_graph.dev, nullptr, 0, &count));
+  std::vector<lv_level_info> v(count);
+  check(lv_get_levels(dev_graph.dev, v.data(), count, &count));
+  return v;
+}
+
+}  // namespace lvb_host

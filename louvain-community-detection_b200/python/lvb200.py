@@ -1,0 +1,381 @@
+"""ctypes binding of the B200 Louvain engine's C ABI (include/louvain_b200.h).
+
+The engine is the CUDA library lib/liblouvain_b200.so; this module only
+marshals arguments.  There is no CPU fallback: if the library cannot be
+loaded, or no CUDA device is usable, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "liblouvain_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(PKG_DIR), "include", "louvain_b200.h")
+
+RULE_PY = 0
+RULE_CUDA = 1
+RULES = {"py": RULE_PY, "cuda": RULE_CUDA}
+
+STATUS = {
+    0: "LV_OK", 1: "LV_ERR_ARG", 2: "LV_ERR_IO", 3: "LV_ERR_PARSE",
+    4: "LV_ERR_NOMEM", 5: "LV_ERR_CUDA", 6: "LV_ERR_STATE", 7: "LV_ERR_LIMIT",
+    8: "LV_ERR_TIMEOUT",
+}
+
+
+class LouvainError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int),
+        ("rule", ctypes.c_int),
+        ("max_passes", ctypes.c_uint32),
+        ("max_levels", ctypes.c_uint32),
+        ("use_graphs", ctypes.c_int),
+        ("stream", ctypes.c_void_p),
+    ]
+
+
+class LevelInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_vertices", ctypes.c_uint32),
+        ("n_entries", ctypes.c_uint64),
+        ("passes", ctypes.c_uint32),
+        ("moved", ctypes.c_uint32),
+        ("q_start", ctypes.c_double),
+        ("q_end", ctypes.c_double),
+        ("move_ms", ctypes.c_float),
+        ("aggregate_ms", ctypes.c_float),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("modularity", ctypes.c_double),
+        ("n_vertices", ctypes.c_uint32),
+        ("n_communities", ctypes.c_uint32),
+        ("n_levels", ctypes.c_uint32),
+        ("edges_processed", ctypes.c_uint64),
+        ("alg_ms", ctypes.c_float),
+        ("copy_ms", ctypes.c_float),
+    ]
+
+
+class KernelStat(ctypes.Structure):
+    _fields_ = [
+        ("name", ctypes.c_char * 32),
+        ("launches", ctypes.c_uint64),
+        ("total_ms", ctypes.c_double),
+        ("bytes", ctypes.c_double),
+    ]
+
+
+# symbol -> (restype, argtypes)
+_VP = ctypes.c_void_p
+_U32 = ctypes.c_uint32
+_U64 = ctypes.c_uint64
+_SIGS = {
+    "lv_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "lv_last_error": (ctypes.c_char_p, []),
+    "lv_abi_version": (ctypes.c_int, []),
+    "lv_config_default": (None, [ctypes.POINTER(Config)]),
+    "lv_graph_load_mtx": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_VP)]),
+    "lv_graph_from_edges": (ctypes.c_int, [_U32, _U64, _VP, _VP, _VP, ctypes.POINTER(_VP)]),
+    "lv_graph_from_csr": (ctypes.c_int, [_U32, _VP, _VP, _VP, ctypes.POINTER(_VP)]),
+    "lv_graph_view": (ctypes.c_int, [_VP, ctypes.POINTER(_U32), ctypes.POINTER(_U64),
+                                     ctypes.POINTER(_VP), ctypes.POINTER(_VP),
+                                     ctypes.POINTER(_VP), ctypes.POINTER(_U32)]),
+    "lv_graph_destroy": (None, [_VP]),
+    "lv_engine_create": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(_VP)]),
+    "lv_engine_destroy": (None, [_VP]),
+    "lv_engine_load": (ctypes.c_int, [_VP, _VP]),
+    "lv_engine_load_device": (ctypes.c_int, [_VP, _U32, _U64, _VP, _VP, _VP]),
+    "lv_phase_move": (ctypes.c_int, [_VP, ctypes.c_float, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_double)]),
+    "lv_phase_aggregate": (ctypes.c_int, [_VP]),
+    "lv_run": (ctypes.c_int, [_VP, _VP, ctypes.c_float, ctypes.POINTER(Result)]),
+    "lv_run_device": (ctypes.c_int, [_VP, _U32, _U64, _VP, _VP, _VP, ctypes.c_float, _VP,
+                                     ctypes.POINTER(Result)]),
+    "lv_get_assignment": (ctypes.c_int, [_VP, _VP, ctypes.c_size_t]),
+    "lv_get_levels": (ctypes.c_int, [_VP, ctypes.POINTER(LevelInfo), _U32,
+                                     ctypes.POINTER(_U32)]),
+    "lv_get_level_size": (ctypes.c_int, [_VP, ctypes.POINTER(_U32), ctypes.POINTER(_U64)]),
+    "lv_get_level_state": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
+    "lv_get_level_csr": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
+    "lv_set_level_comm": (ctypes.c_int, [_VP, _VP]),
+    "lv_modularity_fp64": (ctypes.c_int, [_VP, _VP, ctypes.POINTER(ctypes.c_double)]),
+    "lv_get_buckets": (ctypes.c_int, [_VP, _VP, ctypes.c_size_t]),
+    "lv_set_profiling": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "lv_get_kernel_stats": (ctypes.c_int, [_VP, ctypes.POINTER(KernelStat), _U32,
+                                           ctypes.POINTER(_U32)]),
+    "lv_reset_kernel_stats": (ctypes.c_int, [_VP]),
+    "lv_get_launch_count": (ctypes.c_int, [ctypes.POINTER(_U64)]),
+}
+
+_lib = None
+
+
+def header_symbols() -> list[str]:
+    """Function names declared in include/louvain_b200.h."""
+    import re
+
+    text = open(HEADER_PATH).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"\b(lv_[a-z0-9_]+)\s*\(", text)
+    return sorted(set(names))
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing: build it with "
+                          "`python -c 'import __graft_entry__ as g; g.build()'`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def launch_count() -> int:
+    """Kernels the library has launched in this process."""
+    c = _U64()
+    _check(lib().lv_get_launch_count(ctypes.byref(c)))
+    return c.value
+
+
+def _check(status: int):
+    if status != 0:
+        raise LouvainError(status, lib().lv_last_error().decode(errors="replace"))
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Graph:
+    """Host CSR graph owned by the library."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def load_mtx(cls, path: str) -> "Graph":
+        h = ctypes.c_void_p()
+        _check(lib().lv_graph_load_mtx(path.encode(), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_edges(cls, n: int, src, dst, w=None) -> "Graph":
+        src = np.ascontiguousarray(src, dtype=np.uint32)
+        dst = np.ascontiguousarray(dst, dtype=np.uint32)
+        wp = None
+        if w is not None:
+            w = np.ascontiguousarray(w, dtype=np.float32)
+            wp = _p(w)
+        h = ctypes.c_void_p()
+        _check(lib().lv_graph_from_edges(n, len(src), _p(src), _p(dst), wp,
+                                         ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_csr(cls, n: int, off, col, w) -> "Graph":
+        off = np.ascontiguousarray(off, dtype=np.uint64)
+        col = np.ascontiguousarray(col, dtype=np.uint32)
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        h = ctypes.c_void_p()
+        _check(lib().lv_graph_from_csr(n, _p(off), _p(col), _p(w), ctypes.byref(h)))
+        return cls(h)
+
+    def csr(self):
+        n = _U32()
+        e = _U64()
+        po, pc, pw = _VP(), _VP(), _VP()
+        md = _U32()
+        _check(lib().lv_graph_view(self._h, ctypes.byref(n), ctypes.byref(e),
+                                   ctypes.byref(po), ctypes.byref(pc),
+                                   ctypes.byref(pw), ctypes.byref(md)))
+        N, E = n.value, e.value
+        off = np.ctypeslib.as_array(ctypes.cast(po, ctypes.POINTER(_U64)),
+                                    shape=(N + 1,)).copy()
+        if E:
+            col = np.ctypeslib.as_array(ctypes.cast(pc, ctypes.POINTER(_U32)),
+                                        shape=(E,)).copy()
+            w = np.ctypeslib.as_array(ctypes.cast(pw, ctypes.POINTER(ctypes.c_float)),
+                                      shape=(E,)).copy()
+        else:
+            col = np.zeros(0, np.uint32)
+            w = np.zeros(0, np.float32)
+        return N, off, col, w, md.value
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.lv_graph_destroy(self._h)
+            self._h = None
+
+
+@dataclass
+class RunResult:
+    modularity: float
+    assignment: np.ndarray
+    n_communities: int
+    levels: list
+    edges_processed: int
+    alg_ms: float
+    copy_ms: float
+
+
+class Engine:
+    def __init__(self, device: int = 0, rule: str = "py", max_passes: int = 0,
+                 max_levels: int = 0, use_graphs: bool = False, stream: int = 0):
+        cfg = Config()
+        lib().lv_config_default(ctypes.byref(cfg))
+        cfg.device = device
+        cfg.rule = RULES[rule]
+        cfg.max_passes = max_passes
+        cfg.max_levels = max_levels
+        cfg.use_graphs = int(use_graphs)
+        cfg.stream = stream or None
+        h = ctypes.c_void_p()
+        _check(lib().lv_engine_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self.n0 = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lv_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- loading ---------------------------------------------------------
+    def load(self, g: Graph):
+        _check(lib().lv_engine_load(self._h, g._h))
+        self.n0 = self._level_size()[0]
+
+    def load_device(self, n: int, nnz: int, d_off: int, d_col: int, d_w: int):
+        _check(lib().lv_engine_load_device(self._h, n, nnz, d_off, d_col, d_w))
+        self.n0 = n
+
+    # -- phases ----------------------------------------------------------
+    def phase_move(self, min_gain: float):
+        more = ctypes.c_int()
+        q = ctypes.c_double()
+        _check(lib().lv_phase_move(self._h, min_gain, ctypes.byref(more), ctypes.byref(q)))
+        return bool(more.value), q.value
+
+    def phase_aggregate(self):
+        _check(lib().lv_phase_aggregate(self._h))
+
+    def run(self, g: Graph, min_gain: float) -> RunResult:
+        r = Result()
+        _check(lib().lv_run(self._h, g._h, min_gain, ctypes.byref(r)))
+        self.n0 = r.n_vertices
+        return self._result(r)
+
+    def run_device(self, n: int, nnz: int, d_off: int, d_col: int, d_w: int,
+                   min_gain: float, d_assignment: int = 0) -> Result:
+        r = Result()
+        _check(lib().lv_run_device(self._h, n, nnz, d_off, d_col, d_w, min_gain,
+                                   d_assignment or None, ctypes.byref(r)))
+        self.n0 = n
+        return r
+
+    def _result(self, r: Result) -> RunResult:
+        return RunResult(r.modularity, self.assignment(), r.n_communities,
+                         self.levels(), r.edges_processed, r.alg_ms, r.copy_ms)
+
+    # -- introspection ---------------------------------------------------
+    def assignment(self) -> np.ndarray:
+        out = np.zeros(max(self.n0, 1), dtype=np.uint32)
+        _check(lib().lv_get_assignment(self._h, _p(out), self.n0))
+        return out[: self.n0]
+
+    def levels(self) -> list:
+        cnt = _U32()
+        _check(lib().lv_get_levels(self._h, None, 0, ctypes.byref(cnt)))
+        arr = (LevelInfo * max(cnt.value, 1))()
+        _check(lib().lv_get_levels(self._h, arr, cnt.value, ctypes.byref(cnt)))
+        return [
+            dict(n_vertices=a.n_vertices, n_entries=a.n_entries, passes=a.passes,
+                 moved=bool(a.moved), q_start=a.q_start, q_end=a.q_end,
+                 move_ms=a.move_ms, aggregate_ms=a.aggregate_ms)
+            for a in arr[: cnt.value]
+        ]
+
+    def _level_size(self):
+        n = _U32()
+        e = _U64()
+        _check(lib().lv_get_level_size(self._h, ctypes.byref(n), ctypes.byref(e)))
+        return n.value, e.value
+
+    def level_size(self):
+        return self._level_size()
+
+    def level_state(self):
+        n, _ = self._level_size()
+        comm = np.zeros(max(n, 1), np.uint32)
+        sz = np.zeros(max(n, 1), np.uint32)
+        k = np.zeros(max(n, 1), np.float32)
+        _check(lib().lv_get_level_state(self._h, _p(comm), _p(sz), _p(k)))
+        return comm[:n], sz[:n], k[:n]
+
+    def level_csr(self):
+        n, e = self._level_size()
+        off = np.zeros(n + 1, np.uint64)
+        col = np.zeros(max(e, 1), np.uint32)
+        w = np.zeros(max(e, 1), np.float32)
+        _check(lib().lv_get_level_csr(self._h, _p(off), _p(col), _p(w)))
+        return n, off, col[:e], w[:e]
+
+    def set_level_comm(self, comm):
+        comm = np.ascontiguousarray(comm, dtype=np.uint32)
+        _check(lib().lv_set_level_comm(self._h, _p(comm)))
+
+    def modularity(self, partition) -> float:
+        part = np.ascontiguousarray(partition, dtype=np.uint32)
+        q = ctypes.c_double()
+        _check(lib().lv_modularity_fp64(self._h, _p(part), ctypes.byref(q)))
+        return q.value
+
+    def buckets(self) -> np.ndarray:
+        n, _ = self._level_size()
+        out = np.zeros(max(n, 1), np.uint8)
+        _check(lib().lv_get_buckets(self._h, _p(out), n))
+        return out[:n]
+
+    # -- kernel timing ---------------------------------------------------
+    def set_profiling(self, on: bool = True):
+        _check(lib().lv_set_profiling(self._h, int(on)))
+
+    def reset_kernel_stats(self):
+        _check(lib().lv_reset_kernel_stats(self._h))
+
+    def kernel_stats(self) -> dict:
+        arr = (KernelStat * 32)()
+        cnt = _U32()
+        _check(lib().lv_get_kernel_stats(self._h, arr, 32, ctypes.byref(cnt)))
+        return {a.name.decode(): dict(launches=a.launches, total_ms=a.total_ms,
+                                      bytes=a.bytes)
+                for a in arr[: cnt.value]}

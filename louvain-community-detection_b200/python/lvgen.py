@@ -1,0 +1,284 @@
+"""Seeded synthetic graphs with the shapes of the benchmark workloads, and
+Matrix Market I/O with the reference reader's semantics.
+
+Every generator returns an undirected edge list (src, dst, w) in "file
+order"; `csr_from_edges` turns it into the CSR the reference's reader
+builds from the same lines (utils.cu:200-227: each edge stored in both
+rows, a self-loop once, every row in file order).
+
+Workloads (sizes as in the benchmark descriptions):
+  banded_fem      symmetric banded FEM-like matrix (n=4,884, half-band 60,
+                  ~290k stored entries, weights U(0.1, 1.0))
+  planted_powerlaw  Chung-Lu degrees (exponent 2.3, max 550) with planted
+                  LFR-style communities (size exponent 1.5, mixing mu)
+  rmat            R-MAT (a, b, c, d) = (.57, .19, .19, .05), duplicates
+                  merged, self-loops dropped
+  sbm             stochastic block model with p_in / p_out = 20
+"""
+from __future__ import annotations
+
+import numpy as np
+
+F32 = np.float32
+
+
+def csr_from_edges(n: int, src: np.ndarray, dst: np.ndarray,
+                   w: np.ndarray):
+    """CSR (off u64[n+1], col u32[E], w f32[E]) with the reference layout."""
+    src = np.asarray(src, dtype=np.int64)
+    dst = np.asarray(dst, dtype=np.int64)
+    w = np.asarray(w, dtype=F32)
+    m = len(src)
+    loop = src == dst
+    # entries in file order: edge i contributes (src->dst) then (dst->src)
+    rows = np.empty(2 * m, dtype=np.int64)
+    cols = np.empty(2 * m, dtype=np.int64)
+    ws = np.empty(2 * m, dtype=F32)
+    rows[0::2], rows[1::2] = src, dst
+    cols[0::2], cols[1::2] = dst, src
+    ws[0::2], ws[1::2] = w, w
+    keep = np.ones(2 * m, dtype=bool)
+    keep[1::2] = ~loop
+    rows, cols, ws = rows[keep], cols[keep], ws[keep]
+    order = np.argsort(rows, kind="stable")
+    rows, cols, ws = rows[order], cols[order], ws[order]
+    deg = np.bincount(rows, minlength=n).astype(np.uint64)
+    off = np.zeros(n + 1, dtype=np.uint64)
+    np.cumsum(deg, out=off[1:])
+    return off, cols.astype(np.uint32), ws
+
+
+def write_mtx(path: str, n: int, src, dst, w, one_based: bool = True,
+              banner: bool = False, comments=(), with_weights: bool = True):
+    """Writes `rows cols nnz` + `i j w` lines (readable by both the
+    reference CLI and louvian.py when banner/comments are off)."""
+    src = np.asarray(src, dtype=np.int64)
+    dst = np.asarray(dst, dtype=np.int64)
+    w = np.asarray(w, dtype=F32)
+    b = 1 if one_based else 0
+    with open(path, "w") as f:
+        if banner:
+            f.write("%%MatrixMarket matrix coordinate real symmetric\n")
+        for c in comments:
+            f.write("%" + c + "\n")
+        f.write(f"{n} {n} {len(src)}\n")
+        if with_weights:
+            # The shortest repr of the float32 value taken as a double parses
+            # to that same value with strtof (reference CLI) and with float()
+            # (louvian.py), so both readers see identical weights.
+            for a, c, x in zip(src.tolist(), dst.tolist(), _fmt_weights(w)):
+                f.write(f"{a + b} {c + b} {x}\n")
+        else:
+            for a, c in zip(src.tolist(), dst.tolist()):
+                f.write(f"{a + b} {c + b}\n")
+
+
+def _fmt_weights(w):
+    return [repr(float(np.float32(x))) for x in w]
+
+
+def banded_fem(n: int = 4884, half_band: int = 60, target_entries: int = 290_000,
+               seed: int = 0):
+    """Lower-triangle banded matrix (diagonal included), listed column by
+    column like a Harwell-Boeing stiffness matrix."""
+    rng = np.random.default_rng(seed)
+    # off-diagonal pairs needed so that 2*offdiag + n ~= target_entries
+    off_pairs = max(0, (target_entries - n) // 2)
+    full = sum(min(half_band, n - 1 - j) for j in range(n))
+    p = min(1.0, off_pairs / max(full, 1))
+    src, dst = [], []
+    for j in range(n):
+        src.append(j)
+        dst.append(j)
+        hi = min(n - 1, j + half_band)
+        if hi > j:
+            rows = np.arange(j + 1, hi + 1)
+            rows = rows[rng.random(len(rows)) < p]
+            src.extend(rows.tolist())
+            dst.extend([j] * len(rows))
+    src = np.array(src, dtype=np.int64)
+    dst = np.array(dst, dtype=np.int64)
+    w = rng.uniform(0.1, 1.0, size=len(src)).astype(F32)
+    return n, src, dst, w
+
+
+def _powerlaw_ints(rng, size, exponent, lo, hi):
+    """Discrete power law P(k) ~ k^-exponent on [lo, hi]."""
+    ks = np.arange(lo, hi + 1, dtype=np.float64)
+    p = ks ** (-exponent)
+    p /= p.sum()
+    return rng.choice(np.arange(lo, hi + 1), size=size, p=p)
+
+
+def planted_powerlaw(n: int = 334_863, target_edges: int = 925_872,
+                     gamma: float = 2.3, max_deg: int = 550, mu: float = 0.3,
+                     comm_exp: float = 1.5, comm_min: int = 10,
+                     comm_max: int = 2000, seed: int = 0, unit: bool = True):
+    """Chung-Lu style degrees with planted communities (LFR-like):
+    a (1-mu) share of each vertex's stubs pairs inside its community, the
+    rest pairs globally; duplicates and self-loops are removed."""
+    rng = np.random.default_rng(seed)
+    mean_target = 2.0 * target_edges / n
+    # choose the minimum degree so the power law's mean is near the target
+    deg = None
+    for dmin in range(1, 20):
+        ks = np.arange(dmin, max_deg + 1, dtype=np.float64)
+        p = ks ** (-gamma)
+        mean = (ks * p).sum() / p.sum()
+        if mean >= mean_target * 0.93:
+            deg = _powerlaw_ints(rng, n, gamma, dmin, max_deg)
+            break
+    if deg is None:
+        deg = _powerlaw_ints(rng, n, gamma, 1, max_deg)
+    deg = deg.astype(np.int64)
+    # community sizes ~ power law (exponent comm_exp) covering n vertices
+    sizes = []
+    total = 0
+    while total < n:
+        s = int(_powerlaw_ints(rng, 1, comm_exp, comm_min, comm_max)[0])
+        s = min(s, n - total)
+        sizes.append(s)
+        total += s
+    sizes = np.array(sizes, dtype=np.int64)
+    perm = rng.permutation(n)
+    comm_of = np.empty(n, dtype=np.int64)
+    comm_of[perm] = np.repeat(np.arange(len(sizes)), sizes)
+    k_in = np.rint((1.0 - mu) * deg).astype(np.int64)
+    # a vertex cannot have more intra stubs than its community can absorb
+    k_in = np.minimum(k_in, sizes[comm_of] - 1)
+    k_out = deg - k_in
+    # intra: configuration model inside every community
+    stub_v = np.repeat(np.arange(n), k_in)
+    key = comm_of[stub_v].astype(np.float64) + rng.random(len(stub_v))
+    stub_v = stub_v[np.argsort(key, kind="stable")]
+    stub_c = comm_of[stub_v]
+    # pair consecutive stubs of the same community
+    same = np.zeros(len(stub_v), dtype=bool)
+    if len(stub_v) > 1:
+        # greedy: take pairs (0,1),(2,3)... within each community run
+        starts = np.flatnonzero(np.r_[True, stub_c[1:] != stub_c[:-1]])
+        idx = np.arange(len(stub_v))
+        run_start = np.repeat(starts, np.diff(np.r_[starts, len(stub_v)]))
+        pos = idx - run_start
+        first = (pos % 2 == 0) & (idx + 1 < len(stub_v))
+        first &= np.r_[stub_c[1:] == stub_c[:-1], False]
+        same = first
+    a1 = stub_v[same]
+    b1 = stub_v[np.flatnonzero(same) + 1]
+    # inter: global configuration model
+    stub_o = np.repeat(np.arange(n), k_out)
+    stub_o = stub_o[rng.permutation(len(stub_o))]
+    h = len(stub_o) // 2
+    a2, b2 = stub_o[:h], stub_o[h:2 * h]
+    src = np.concatenate([a1, a2])
+    dst = np.concatenate([b1, b2])
+    src, dst = _simple(n, src, dst, rng)
+    w = np.ones(len(src), dtype=F32) if unit else \
+        rng.uniform(0.5, 1.5, len(src)).astype(F32)
+    return n, src, dst, w
+
+
+def _simple(n, src, dst, rng, shuffle=True):
+    """Drops self-loops and duplicate undirected edges; random file order."""
+    keep = src != dst
+    src, dst = src[keep], dst[keep]
+    lo = np.minimum(src, dst)
+    hi = np.maximum(src, dst)
+    key = lo * np.int64(n) + hi
+    _, first = np.unique(key, return_index=True)
+    src, dst = src[first], dst[first]
+    if shuffle:
+        p = rng.permutation(len(src))
+        src, dst = src[p], dst[p]
+    return src, dst
+
+
+def rmat(scale: int, edge_factor: int = 16, a=0.57, b=0.19, c=0.19,
+         seed: int = 0, unit: bool = True):
+    """R-MAT edges (duplicates merged, self-loops dropped)."""
+    rng = np.random.default_rng(seed)
+    n = 1 << scale
+    m = edge_factor * n
+    src = np.zeros(m, dtype=np.int64)
+    dst = np.zeros(m, dtype=np.int64)
+    ab, abc = a + b, a + b + c
+    for lvl in range(scale):
+        r = rng.random(m)
+        bit = np.int64(1) << (scale - 1 - lvl)
+        down = r >= ab  # quadrants c, d: row bit set
+        right = ((r >= a) & (r < ab)) | (r >= abc)  # quadrants b, d
+        src += np.where(down, bit, 0)
+        dst += np.where(right, bit, 0)
+    src, dst = _simple(n, src, dst, rng)
+    w = np.ones(len(src), dtype=F32) if unit else \
+        rng.uniform(0.1, 1.0, len(src)).astype(F32)
+    return n, src, dst, w
+
+
+def sbm(n: int, blocks: int, mean_deg: float = 16.0, ratio: float = 20.0,
+        seed: int = 0, wlo: float = 0.5, whi: float = 1.5):
+    """Stochastic block model with equal blocks, p_in/p_out = ratio, mean
+    degree mean_deg, weights U(wlo, whi)."""
+    rng = np.random.default_rng(seed)
+    bs = n // blocks
+    sizes = np.full(blocks, bs, dtype=np.int64)
+    sizes[: n - bs * blocks] += 1
+    block_of = np.repeat(np.arange(blocks), sizes)
+    # expected degree = p_in*(s-1) + p_out*(n-s) = mean_deg
+    s = n / blocks
+    p_out = mean_deg / (ratio * (s - 1) + (n - s))
+    p_in = ratio * p_out
+    m_in = int(round(p_in * sum(int(x) * (int(x) - 1) // 2 for x in sizes)))
+    m_out = int(round(p_out * (n * (n - 1) // 2 - sum(int(x) * (int(x) - 1) // 2
+                                                      for x in sizes))))
+    starts = np.r_[0, np.cumsum(sizes)[:-1]]
+    # intra edges: pick a block proportional to its pair count, then two members
+    pairs = sizes * (sizes - 1) / 2.0
+    bsel = rng.choice(blocks, size=m_in, p=pairs / pairs.sum())
+    u = starts[bsel] + (rng.random(m_in) * sizes[bsel]).astype(np.int64)
+    v = starts[bsel] + (rng.random(m_in) * sizes[bsel]).astype(np.int64)
+    # inter edges: two uniform vertices in different blocks
+    x = rng.integers(0, n, size=2 * m_out + 16)
+    y = rng.integers(0, n, size=2 * m_out + 16)
+    ok = block_of[x] != block_of[y]
+    x, y = x[ok][:m_out], y[ok][:m_out]
+    src = np.concatenate([u, x])
+    dst = np.concatenate([v, y])
+    src, dst = _simple(n, src, dst, rng)
+    w = rng.uniform(wlo, whi, len(src)).astype(F32)
+    return n, src, dst, w
+
+
+def two_cliques_bridge(k: int = 5):
+    """Two k-cliques joined by one bridge edge."""
+    src, dst = [], []
+    for base in (0, k):
+        for i in range(k):
+            for j in range(i + 1, k):
+                src.append(base + i)
+                dst.append(base + j)
+    src.append(k - 1)
+    dst.append(k)
+    return 2 * k, np.array(src), np.array(dst), np.ones(len(src), dtype=F32)
+
+
+def ring_of_cliques(cliques: int = 8, k: int = 6):
+    src, dst = [], []
+    for c in range(cliques):
+        base = c * k
+        for i in range(k):
+            for j in range(i + 1, k):
+                src.append(base + i)
+                dst.append(base + j)
+        src.append(base + k - 1)
+        dst.append(((c + 1) % cliques) * k)
+    n = cliques * k
+    return n, np.array(src), np.array(dst), np.ones(len(src), dtype=F32)
+
+
+def star(leaves: int = 1000, seed: int = 0):
+    rng = np.random.default_rng(seed)
+    src = np.zeros(leaves, dtype=np.int64)
+    dst = np.arange(1, leaves + 1)
+    w = rng.uniform(0.5, 1.5, leaves).astype(F32)
+    return leaves + 1, src, dst, w
