@@ -61,7 +61,8 @@ typedef struct lv_config {
     lv_rule rule;           /* decision rule, default LV_RULE_PY            */
     uint32_t max_passes;    /* cap on passes per level (0 = 100000)         */
     uint32_t max_levels;    /* cap on levels (0 = no cap)                   */
-    int use_graphs;         /* capture each level's pass in a CUDA graph    */
+    int use_graphs;         /* capture each level's pass in a CUDA graph
+                               and replay it (default 1)                    */
     void *stream;           /* cudaStream_t to run on; NULL = own stream    */
 } lv_config;
 

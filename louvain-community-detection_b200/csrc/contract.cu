@@ -474,12 +474,7 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
                            void* grow_ctx) {
   const uint32_t n = L.n;
   (void)nnz;
-  uint32_t* h_counts = nullptr;
-  LV_TRY(cudaMallocHost(&h_counts, 16 * sizeof(uint32_t)));
-  struct Free {
-    uint32_t* p;
-    ~Free() { cudaFreeHost(p); }
-  } free_guard{h_counts};
+  uint32_t* h_counts = B.host_counts;
 
   const unsigned g1 = gridcap((n + 255) / 256, 8);
   (count_launches(1), flags_kernel<<<g1, 256, 0, st>>>(L.comm_sz, n, B.flag_id, B.mem_off, B.cursor));

@@ -183,6 +183,11 @@ struct lv_engine {
   bool loaded = false;
   bool level_ready = false;
   bool finished = false;
+  // The level's communities count as moves of the assignment (the
+  // reference's graphVertToComm, modularity.cu:515-517) when the move phase
+  // returned true or a caller set them; `assignment` itself holds the
+  // level-start map and is composed once per level, at aggregation.
+  bool accepted = false;
   DispatchPlan plan{};
   double q_last = 0.0;
   std::vector<lv_level_info> levels;
@@ -194,6 +199,11 @@ struct lv_engine {
   KStat kst[K_COUNT];
   std::vector<cudaEvent_t> ev_free;
   std::vector<PendingTiming> pending;
+  // one pass of the current level captured as a CUDA graph
+  cudaGraphExec_t pass_exec = nullptr;
+  bool capturing = false;
+  std::vector<PendingTiming> graph_timings;  // event pairs inside the graph
+  unsigned long long pass_launches = 0;      // kernels per replay
   unsigned long long* d_class_deg = nullptr;
   uint64_t class_deg[kClasses] = {};
 
@@ -229,19 +239,52 @@ cudaEvent_t take_event(lv_engine* E) {
   return e;
 }
 
+// Records an event; inside a stream capture it becomes an external event
+// node of the graph, so every replay re-records it.
+void record_event(lv_engine* E, cudaEvent_t ev) {
+  if (E->capturing)
+    cudaEventRecordWithFlags(ev, E->st, cudaEventRecordExternal);
+  else
+    cudaEventRecord(ev, E->st);
+}
+
 // Opens a timed launch group; returns the start event (nullptr when off).
 cudaEvent_t prof_begin(lv_engine* E) {
   if (!E->profiling) return nullptr;
   cudaEvent_t a = take_event(E);
-  cudaEventRecord(a, E->st);
+  record_event(E, a);
   return a;
 }
 
 void prof_end(lv_engine* E, cudaEvent_t a, int id, double bytes) {
   if (!a) return;
   cudaEvent_t b = take_event(E);
-  cudaEventRecord(b, E->st);
+  record_event(E, b);
   E->pending.push_back(PendingTiming{id, a, b, bytes});
+}
+
+// Accumulates the timings of the last replay of the pass graph.
+void prof_collect_graph(lv_engine* E) {
+  for (const PendingTiming& p : E->graph_timings) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+      E->kst[p.id].launches++;
+      E->kst[p.id].ms += ms;
+      E->kst[p.id].bytes += p.bytes;
+    }
+  }
+  cudaGetLastError();
+}
+
+void drop_pass_graph(lv_engine* E) {
+  if (E->pass_exec) cudaGraphExecDestroy(E->pass_exec);
+  E->pass_exec = nullptr;
+  for (const PendingTiming& p : E->graph_timings) {
+    E->ev_free.push_back(p.a);
+    E->ev_free.push_back(p.b);
+  }
+  E->graph_timings.clear();
+  E->pass_launches = 0;
 }
 
 // Folds the finished groups into the totals (call after a stream sync).
@@ -398,6 +441,7 @@ lv_status ensure_capacity(lv_engine* E, uint32_t n, uint64_t e, bool need_input)
   CU(dalloc(&B.tw, EE));
   CU(dalloc(&B.tmp, ptw));
   CU(dalloc(&B.counts, 16));
+  B.host_counts = E->h_counts + 16;
   B.table_cap = 0;
   B.g_cap = 0;
   const size_t scan_cap = std::max<size_t>(N1, partition_tmp_words(N)) + 1024;
@@ -412,6 +456,7 @@ lv_status ensure_capacity(lv_engine* E, uint32_t n, uint64_t e, bool need_input)
 lv_status prepare_level(lv_engine* E) {
   const uint32_t n = E->n;
   cudaStream_t st = E->st;
+  drop_pass_graph(E);
   CU(partition_by_degree(E->off(), n, E->order, E->cls_count, E->part_tmp,
                          E->scan, st));
   CU(cudaMemcpyAsync(E->h_counts, E->cls_count, kClasses * sizeof(uint32_t),
@@ -556,7 +601,41 @@ lv_status prepare_level(lv_engine* E) {
   return LV_OK;
 }
 
+lv_status issue_pass(lv_engine* E);
+
+// One pass: the 7 Jacobi steps and the modularity sweep.  With graphs on,
+// the first pass of a level is captured and every pass replays it.
 lv_status run_pass(lv_engine* E) {
+  if (!E->cfg.use_graphs) return issue_pass(E);
+  if (!E->pass_exec) {
+    const unsigned long long l0 = launch_count();
+    CU(cudaStreamBeginCapture(E->st, cudaStreamCaptureModeThreadLocal));
+    E->capturing = true;
+    lv_status s = issue_pass(E);
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(E->st, &g);
+    E->capturing = false;
+    if (s != LV_OK) {
+      if (g) cudaGraphDestroy(g);
+      return s;
+    }
+    CU(ce);
+    ce = cudaGraphInstantiate(&E->pass_exec, g, 0);
+    cudaGraphDestroy(g);
+    CU(ce);
+    E->pass_launches = launch_count() - l0;
+    E->graph_timings.swap(E->pending);
+    E->pending.clear();
+    // the capture counted its kernels once, which stands for this launch
+    CU(cudaGraphLaunch(E->pass_exec, E->st));
+    return LV_OK;
+  }
+  CU(cudaGraphLaunch(E->pass_exec, E->st));
+  count_launches((unsigned)E->pass_launches);
+  return LV_OK;
+}
+
+lv_status issue_pass(lv_engine* E) {
   const LevelView L = E->view();
   const int rule = (E->cfg.rule == LV_RULE_CUDA) ? LV_RULE_CUDA_I : LV_RULE_PY_I;
   HubArena H = E->hub;
@@ -590,6 +669,7 @@ lv_status check_device_error(lv_engine* E) {
 }
 
 lv_status load_common(lv_engine* E, uint32_t n, uint64_t e) {
+  drop_pass_graph(E);
   E->n0 = n;
   E->n = n;
   E->e = e;
@@ -597,6 +677,7 @@ lv_status load_common(lv_engine* E, uint32_t n, uint64_t e) {
   E->loaded = true;
   E->level_ready = false;
   E->finished = false;
+  E->accepted = false;
   E->levels.clear();
   E->q_last = 0.0;
   CU(launch_fill_iota(E->assignment, n, E->st));  // setInitComm, utils.cu:67
@@ -643,7 +724,7 @@ void lv_config_default(lv_config* cfg) {
   cfg->rule = LV_RULE_PY;
   cfg->max_passes = 0;
   cfg->max_levels = 0;
-  cfg->use_graphs = 0;
+  cfg->use_graphs = 1;
   cfg->stream = nullptr;
 }
 
@@ -685,7 +766,7 @@ lv_status lv_engine_create(const lv_config* cfg, lv_engine** out) {
   }
   if ((ce = cudaMalloc(&E->sc, sizeof(LevelScalars))) != cudaSuccess ||
       (ce = cudaMallocHost(&E->sc_host, sizeof(LevelScalars))) != cudaSuccess ||
-      (ce = cudaMallocHost(&E->h_counts, 16 * sizeof(uint32_t))) != cudaSuccess ||
+      (ce = cudaMallocHost(&E->h_counts, 32 * sizeof(uint32_t))) != cudaSuccess ||
       (ce = cudaEventCreate(&E->ev0)) != cudaSuccess ||
       (ce = cudaEventCreate(&E->ev1)) != cudaSuccess) {
     lv_engine_destroy(E);
@@ -700,6 +781,7 @@ void lv_engine_destroy(lv_engine* E) {
   if (!E) return;
   cudaSetDevice(E->device);
   if (E->st) cudaStreamSynchronize(E->st);
+  drop_pass_graph(E);
   free_state(E);
   prof_collect(E);
   for (cudaEvent_t ev : E->ev_free) cudaEventDestroy(ev);
@@ -774,6 +856,7 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
       CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars),
                          cudaMemcpyDeviceToHost, E->st));
       CU(cudaStreamSynchronize(E->st));
+      if (E->pass_exec) prof_collect_graph(E);
       prof_collect(E);
       LVTRY(check_device_error(E));
       old = act;
@@ -783,7 +866,7 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
       first = false;
     } while (act - old >= (double)min_gain && passes < E->cfg.max_passes);
   }
-  if (ret) CU(launch_compose(E->assignment, E->n0, E->comm, E->st));  // :515-517
+  E->accepted = ret != 0;  // modularity.cu:515-517 (applied at aggregation)
   CU(cudaEventRecord(E->ev1, E->st));
   CU(cudaEventSynchronize(E->ev1));
   float ms = 0.0f;
@@ -814,7 +897,10 @@ lv_status lv_phase_aggregate(lv_engine* E) {
   prof_end(E, t0, K_CONTRACT,
            (double)E->e * 12.0 + (double)E->n * 20.0 + (double)r.new_nnz * 8.0 +
                ((double)r.new_n + 1.0) * 8.0);
-  CU(launch_compose(E->assignment, E->n0, E->cb.flag_id, E->st));  // aggregation.cu:459
+  // graphVertToComm then graphVertToNewComm (modularity.cu:51-56,
+  // aggregation.cu:380-385) in one gather: cnew[v] = new_id[comm[v]]
+  CU(launch_compose(E->assignment, E->n0, E->cb.cnew, E->st));
+  E->accepted = false;
   CU(cudaEventRecord(E->ev1, E->st));
   CU(cudaEventSynchronize(E->ev1));
   CU(cudaMemcpy(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost));
@@ -823,6 +909,7 @@ lv_status lv_phase_aggregate(lv_engine* E) {
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, E->ev0, E->ev1);
   if (!E->levels.empty()) E->levels.back().aggregate_ms = ms;
+  drop_pass_graph(E);
   E->cur = next;
   E->n = r.new_n;
   E->e = r.new_nnz;
@@ -913,8 +1000,12 @@ lv_status lv_run_device(lv_engine* E, uint32_t n, uint64_t nnz, const uint64_t* 
   LVTRY(run_loaded(E, min_gain, res));
   if (res) res->copy_ms = 0.0f;
   if (d_assignment && n) {
-    CU(cudaMemcpyAsync(d_assignment, E->assignment, (size_t)n * sizeof(uint32_t),
-                       cudaMemcpyDeviceToDevice, E->st));
+    if (E->accepted) {
+      CU(launch_gather(d_assignment, E->assignment, n, E->comm, E->st));
+    } else {
+      CU(cudaMemcpyAsync(d_assignment, E->assignment, (size_t)n * sizeof(uint32_t),
+                         cudaMemcpyDeviceToDevice, E->st));
+    }
     CU(cudaStreamSynchronize(E->st));
   }
   return LV_OK;
@@ -926,8 +1017,12 @@ lv_status lv_get_assignment(lv_engine* E, uint32_t* out, size_t n) {
   if (n != E->n0) return fail(LV_ERR_ARG, "buffer length must equal the input vertex count");
   cudaSetDevice(E->device);
   if (n) {
-    CU(cudaMemcpyAsync(out, E->assignment, n * sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                       E->st));
+    const uint32_t* src = E->assignment;
+    if (E->accepted) {  // the level's moves count: read comm[assignment]
+      CU(launch_gather(E->cb.members, E->assignment, n, E->comm, E->st));
+      src = E->cb.members;
+    }
+    CU(cudaMemcpyAsync(out, src, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, E->st));
     CU(cudaStreamSynchronize(E->st));
   }
   return LV_OK;
@@ -993,7 +1088,12 @@ lv_status lv_set_level_comm(lv_engine* E, const uint32_t* comm) {
   if (!E->level_ready) LVTRY(prepare_level(E));
   if (E->n) CU(cudaMemcpyAsync(E->comm, comm, (size_t)E->n * 4, cudaMemcpyHostToDevice, E->st));
   CU(launch_recount(E->view(), E->st));
+  CU(launch_modularity(E->view(), E->order, E->plan,
+                       E->plan.hub_count ? E->hub_map : nullptr, E->partials, E->st));
+  CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost,
+                     E->st));
   CU(cudaStreamSynchronize(E->st));
+  E->accepted = true;
   return LV_OK;
 }
 

@@ -155,6 +155,9 @@ cudaError_t launch_apply_bucket(const LevelView& L, int bucket,
 // assignment[i] = map[assignment[i]]
 cudaError_t launch_compose(uint32_t* assignment, size_t n0,
                            const uint32_t* map, cudaStream_t st);
+// out[i] = map[in[i]]
+cudaError_t launch_gather(uint32_t* out, const uint32_t* in, size_t n,
+                          const uint32_t* map, cudaStream_t st);
 cudaError_t launch_fill_iota(uint32_t* a, size_t n, cudaStream_t st);
 // Recompute sizes and totals from comm (used when a caller sets comm).
 cudaError_t launch_recount(const LevelView& L, cudaStream_t st);
@@ -189,6 +192,7 @@ struct ContractBuffers {
   float* tw;             // [E] row staging (weights)
   uint32_t* tmp;         // partition scratch
   uint32_t* counts;      // [16] device counters
+  uint32_t* host_counts; // [16] pinned host mirror (engine-owned)
   uint32_t* keys;        // global tables (class G), u32
   double* vals;          // global tables (class G), FP64
   size_t table_cap;      // slots available in keys/vals

@@ -702,6 +702,12 @@ __global__ void compose_kernel(uint32_t* a, size_t n, const uint32_t* map) {
        i += (size_t)gridDim.x * blockDim.x)
     a[i] = map[a[i]];
 }
+__global__ void gather_kernel(uint32_t* out, const uint32_t* in, size_t n,
+                              const uint32_t* map) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = map[in[i]];
+}
 __global__ void iota_kernel(uint32_t* a, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
@@ -921,6 +927,14 @@ cudaError_t launch_compose(uint32_t* assignment, size_t n0,
                            const uint32_t* map, cudaStream_t st) {
   if (!n0) return cudaSuccess;
   (count_launches(1), compose_kernel<<<grid_for((n0 + 255) / 256, sm_count() * 8), 256, 0, st>>>(assignment, n0, map));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather(uint32_t* out, const uint32_t* in, size_t n,
+                          const uint32_t* map, cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  (count_launches(1), gather_kernel<<<grid_for((n + 255) / 256, sm_count() * 8), 256, 0, st>>>(
+      out, in, n, map));
   return cudaGetLastError();
 }
 

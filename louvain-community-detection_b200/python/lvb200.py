@@ -238,7 +238,7 @@ class RunResult:
 
 class Engine:
     def __init__(self, device: int = 0, rule: str = "py", max_passes: int = 0,
-                 max_levels: int = 0, use_graphs: bool = False, stream: int = 0):
+                 max_levels: int = 0, use_graphs: bool = True, stream: int = 0):
         cfg = Config()
         lib().lv_config_default(ctypes.byref(cfg))
         cfg.device = device

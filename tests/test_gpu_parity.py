@@ -213,6 +213,18 @@ def test_run_device_equals_run():
     assert np.array_equal(d_asg.cpu().numpy().view(np.uint32), ref.assignment)
 
 
+@pytest.mark.parametrize("name", ["planted_small", "rmat11", "hub3000"])
+def test_graph_replay_equals_direct_launches(name):
+    """Capturing a level's pass in a CUDA graph changes nothing."""
+    out = []
+    for ug in (False, True):
+        with lvb200.Engine(rule="py", use_graphs=ug) as e:
+            out.append(e.run(lvb200.Graph.load_mtx(golden_mtx(name)), 1e-6))
+    assert out[0].modularity == out[1].modularity
+    assert np.array_equal(out[0].assignment, out[1].assignment)
+    assert [l["passes"] for l in out[0].levels] == [l["passes"] for l in out[1].levels]
+
+
 def test_kernel_profiling_counts(eng):
     eng.set_profiling(True)
     eng.reset_kernel_stats()
