@@ -224,6 +224,28 @@ lv_status lv_reset_kernel_stats(lv_engine *e);
 /* Kernels this library has launched in the process so far (all engines). */
 lv_status lv_get_launch_count(uint64_t *count);
 
+/* ---- modularity without allocation (no counterpart in the reference) ----
+ * The FP64 modularity of lv_modularity_fp64 for a graph and partition that
+ * the caller keeps in device memory, for callers that must not allocate on
+ * the call path: code running under CUDA-graph stream capture (cudaMalloc
+ * and cudaFree cannot be captured, and cudaFree synchronises the device),
+ * latency-bound serving loops, and processes whose device memory belongs to
+ * another allocator.  It allocates nothing: its scratch is a fixed array in
+ * the library's device memory (8 MiB per device that loads the library,
+ * held until the process exits).
+ *   n_vertices <= 1048576 (else LV_ERR_LIMIT); partition ids must be
+ *   < n_vertices (else LV_ERR_ARG); *d_q receives Q, and *q_host too when
+ *   q_host is not NULL.  Runs on `stream` (a cudaStream_t, NULL = legacy
+ *   default stream) and returns after the stream has finished the work.
+ * Every call shares the one array (cleared at the start of each call), so
+ * calls that overlap on the GPU race.  The first call on a device looks up
+ * the array's address with that device current: make it before any stream
+ * capture begins.                                                         */
+lv_status lv_modularity_noalloc(uint32_t n_vertices, const uint64_t *d_offsets,
+                                const uint32_t *d_cols, const float *d_weights,
+                                const uint32_t *d_partition, double *d_q,
+                                double *q_host, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -118,7 +118,22 @@ _SIGS = {
                                            ctypes.POINTER(_U32)]),
     "lv_reset_kernel_stats": (ctypes.c_int, [_VP]),
     "lv_get_launch_count": (ctypes.c_int, [ctypes.POINTER(_U64)]),
+    "lv_modularity_noalloc": (ctypes.c_int, [_U32, _VP, _VP, _VP, _VP, _VP,
+                                             ctypes.POINTER(ctypes.c_double), _VP]),
 }
+
+NOALLOC_MAX_VERTICES = 1 << 20
+
+
+def modularity_noalloc(n: int, d_off: int, d_col: int, d_w: int, d_part: int,
+                       d_q: int, stream: int = 0) -> float:
+    """FP64 modularity of a partition kept in device memory, computed
+    without any allocation (fixed scratch inside the library).  Returns Q
+    and also leaves it at d_q."""
+    q = ctypes.c_double()
+    _check(lib().lv_modularity_noalloc(n, d_off, d_col, d_w, d_part, d_q,
+                                       ctypes.byref(q), stream or None))
+    return q.value
 
 _lib = None
 
