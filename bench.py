@@ -12,9 +12,10 @@ pass's stored adjacency entries / time.
              (256 MB write) between steps outside the timed events
   e2e        same metric through the C ABI with host buffers (lv_run +
              lv_get_assignment: CSR upload and assignment download inside)
-  roofline   the kernel group with the largest device time in the timed
-             steps: algorithmic bytes / its CUDA-event time, against the
-             measured HBM copy bandwidth
+  roofline   the kernel group with the largest device time, from K further
+             steps run with a CUDA event pair around every launch group
+             (on the engine's stream): algorithmic bytes / event time,
+             against the measured HBM copy bandwidth
   cpu_baseline  the reference's CPU path (louvian.py restated in C by the
              oracle, FP64, single thread) on the same graph
 N > 1 (torchrun): every rank runs its own replica (the single-graph path
@@ -232,8 +233,6 @@ def run_engine(args, rank, world):
         torch.cuda.synchronize()
         props = torch.cuda.get_device_properties(dev)
         gpu_id = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(dev)
-        eng.set_profiling(True)
-        eng.reset_kernel_stats()
         launches0 = lvb200.launch_count()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(args.steps)]
@@ -248,10 +247,23 @@ def run_engine(args, rank, world):
                 q = r.modularity
             torch.cuda.synchronize()
         launches = lvb200.launch_count() - launches0
-        eng.set_profiling(False)
-        kstats = eng.kernel_stats()
         levels = eng.levels()
         ms = sum(a.elapsed_time(b) for a, b in ev)
+        # kernel timing: K more steps with a CUDA event pair around every
+        # launch group (the pass loop then replays a captured pass per pass,
+        # since event nodes cannot sit inside the graph's WHILE body)
+        eng.set_profiling(True)
+        eng.reset_kernel_stats()
+        prof_ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        prof_ev[0].record(stream)
+        for i in range(args.steps):
+            flush.zero_()
+            step()
+        prof_ev[1].record(stream)
+        torch.cuda.synchronize()
+        eng.set_profiling(False)
+        kstats = eng.kernel_stats()
+        prof_ms = prof_ev[0].elapsed_time(prof_ev[1]) / args.steps
         if world > 1:
             torch.distributed.barrier()
             t = torch.tensor([ms], device="cuda", dtype=torch.float64)
@@ -298,8 +310,12 @@ def run_engine(args, rank, world):
         "config": dict(desc, parallelism="replicas only" if world > 1 else "single GPU",
                        l2="flushed (256 MB write) between timed steps"),
         "final_q": q,
-        "levels": [{"V": l["n_vertices"], "E": l["n_entries"], "passes": l["passes"]}
+        "levels": [{"V": l["n_vertices"], "E": l["n_entries"], "passes": l["passes"],
+                    "prepare_ms": round(l["prepare_ms"], 4),
+                    "move_ms": round(l["move_ms"], 4),
+                    "aggregate_ms": round(l["aggregate_ms"], 4)}
                    for l in levels],
+        "profiled_ms_per_step": prof_ms,
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": int((n + 1) * 8 + nnz * 8),
                 "d2h_bytes_per_step": int(n * 4)},

@@ -74,8 +74,10 @@ typedef struct lv_level_info {
     uint32_t moved;         /* 1 if the level's first pass gained >= g      */
     double q_start;         /* Q of the singleton partition                 */
     double q_end;           /* Q after the last pass                        */
-    float move_ms;          /* device time of the move phase                */
+    float move_ms;          /* device time of the move phase (incl. set-up) */
     float aggregate_ms;     /* device time of the contraction (0 if none)   */
+    float prepare_ms;       /* part of move_ms: degree classes, row sums,
+                               initial modularity                           */
 } lv_level_info;
 
 typedef struct lv_result {

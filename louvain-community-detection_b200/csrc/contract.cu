@@ -47,6 +47,15 @@ __device__ __forceinline__ uint32_t hash_slot(uint32_t key, uint32_t mask) {
   return (key * 2654435761u) & mask;
 }
 
+// Table slots used for a row of d entries: a power of two >= 1.5 d (load
+// factor <= 2/3), at most tmax.
+__device__ __forceinline__ uint32_t table_size_for(uint32_t d, uint32_t tmax) {
+  const uint32_t want = d + (d >> 1) + 1;
+  uint32_t t = 32;
+  while (t < want) t <<= 1;
+  return t < tmax ? t : tmax;
+}
+
 __device__ __forceinline__ uint32_t table_insert(uint32_t* keys, uint32_t mask,
                                                  uint32_t key, uint32_t* err) {
   uint32_t h = hash_slot(key, mask);
@@ -123,11 +132,14 @@ __global__ void member_deg_kernel(const uint64_t* off, const uint32_t* members,
 }
 
 // entries and staging offset of every new community; new_deg zeroed.
-__global__ void comm_deg_kernel(const uint32_t* comm_list, uint32_t new_n,
+// n_upper bounds the new vertex count *d_new_n.
+__global__ void comm_deg_kernel(const uint32_t* comm_list, uint32_t n_upper,
+                                const uint32_t* d_new_n,
                                 const uint32_t* comm_sz, const uint32_t* mem_off,
                                 const uint64_t* mstart, uint64_t* comm_deg,
                                 uint64_t* seg, uint64_t* new_deg) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= new_n;
+  const uint32_t new_n = *d_new_n;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= n_upper && i <= new_n;
        i += gridDim.x * blockDim.x) {
     new_deg[i] = 0ull;
     if (i < new_n) {
@@ -140,6 +152,13 @@ __global__ void comm_deg_kernel(const uint32_t* comm_list, uint32_t new_n,
   }
 }
 
+__global__ void gather_u64_kernel(const uint64_t* src, const uint32_t* idx, uint32_t n,
+                                  uint64_t* out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x)
+    out[i] = src[idx[i]];
+}
+
 // Class W: one warp per community, flattened member edges, 256-slot table.
 __global__ void __launch_bounds__(kThreads)
     merge_warp_kernel(Ctx C, const uint32_t* list, uint32_t count) {
@@ -148,19 +167,20 @@ __global__ void __launch_bounds__(kThreads)
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   double* vals = vals_sm[wib];
   uint32_t* keys = keys_sm[wib];
-  constexpr uint32_t mask = kWarpSlots - 1;
   for (uint32_t idx = blockIdx.x * kWarps + wib; idx < count;
        idx += gridDim.x * kWarps) {
-    for (int i = lane; i < kWarpSlots; i += 32) {
-      keys[i] = kEmptyKey;
-      vals[i] = 0.0;
-    }
-    __syncwarp();
     const uint32_t cn = list[idx];
     const uint32_t c = C.comm_list[cn];
     const uint32_t m0 = C.mem_off[c], msz = C.comm_sz[c];
     const uint64_t seg = C.mstart[m0];
     const uint64_t total = C.mstart[m0 + msz] - seg;
+    const uint32_t tv = table_size_for((uint32_t)total, kWarpSlots);
+    const uint32_t mask = tv - 1;
+    for (uint32_t i = lane; i < tv; i += 32) {
+      keys[i] = kEmptyKey;
+      vals[i] = 0.0;
+    }
+    __syncwarp();
     for (uint32_t mb = 0; mb < msz; mb += 32) {
       const uint32_t mi = mb + lane;
       const bool mv = mi < msz;
@@ -203,7 +223,7 @@ __global__ void __launch_bounds__(kThreads)
     }
     __syncwarp();
     uint32_t cnt = 0;
-    for (int i0 = 0; i0 < kWarpSlots; i0 += 32) {
+    for (uint32_t i0 = 0; i0 < tv; i0 += 32) {
       const uint32_t key = keys[i0 + lane];
       const bool occ = key != kEmptyKey;
       const unsigned b = __ballot_sync(kFull, occ);
@@ -322,28 +342,29 @@ __global__ void __launch_bounds__(kThreads)
   uint64_t* s_off = s_start + kThreads;
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + kBlockSlots * 8 + kThreads * 16);
   __shared__ uint32_t scan_sm[kWarps + 1];
-  constexpr uint32_t mask = kBlockSlots - 1;
   for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
-    for (int i = threadIdx.x; i < kBlockSlots; i += kThreads) {
-      keys[i] = kEmptyKey;
-      vals[i] = 0.0;
-    }
-    __syncthreads();
     const uint32_t cn = list[idx];
     const uint32_t c = C.comm_list[cn];
     const uint32_t m0 = C.mem_off[c], msz = C.comm_sz[c];
     const uint64_t seg = C.mstart[m0];
     const uint64_t total = C.mstart[m0 + msz] - seg;
-    insert_range(C, m0, msz, seg, total, 0, total, keys, vals, mask, s_start, s_off);
+    // class B rows hold > 128 entries, so tv >= 256 = kThreads
+    const uint32_t tv = table_size_for((uint32_t)total, kBlockSlots);
+    for (uint32_t i = threadIdx.x; i < tv; i += kThreads) {
+      keys[i] = kEmptyKey;
+      vals[i] = 0.0;
+    }
     __syncthreads();
-    // emit: thread t owns slots [t*32, t*32+32)
-    constexpr int per = kBlockSlots / kThreads;
+    insert_range(C, m0, msz, seg, total, 0, total, keys, vals, tv - 1, s_start, s_off);
+    __syncthreads();
+    // emit: thread t owns slots [t*per, t*per + per)
+    const uint32_t per = tv / kThreads;
     uint32_t local = 0;
-    for (int i = 0; i < per; i++) local += keys[threadIdx.x * per + i] != kEmptyKey;
+    for (uint32_t i = 0; i < per; i++) local += keys[threadIdx.x * per + i] != kEmptyKey;
     uint32_t tot;
     uint32_t pos = block_excl_scan(local, scan_sm, &tot);
-    for (int i = 0; i < per; i++) {
-      const int sl = threadIdx.x * per + i;
+    for (uint32_t i = 0; i < per; i++) {
+      const uint32_t sl = threadIdx.x * per + i;
       const uint32_t key = keys[sl];
       if (key != kEmptyKey) {
         C.tcol[seg + pos] = key;
@@ -488,20 +509,18 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
                                                                  B.mstart));
   LV_TRY(cudaGetLastError());
   LV_TRY(exclusive_scan_u64(B.mstart, B.mstart, (size_t)n + 1, nullptr, S, st));
-  LV_TRY(cudaMemcpyAsync(h_counts, B.counts, 2 * sizeof(uint32_t),
+  // sizes of the new communities and their classes, with the new vertex
+  // count read on the device (no host round trip before the merges)
+  (count_launches(1), comm_deg_kernel<<<gridcap((n + 256) / 256, 8), 256, 0, st>>>(
+      B.comm_list, n, B.counts + 0, L.comm_sz, B.mem_off, B.mstart, B.comm_deg,
+      B.seg, B.new_deg));
+  LV_TRY(cudaGetLastError());
+  LV_TRY(partition_by_size3(B.comm_deg, n, B.counts + 0, kMergeWarpMax, kMergeBlockMax,
+                            B.comm_cls, B.counts + 4, B.tmp, S, st));
+  LV_TRY(cudaMemcpyAsync(h_counts, B.counts, 8 * sizeof(uint32_t),
                          cudaMemcpyDeviceToHost, st));
   LV_TRY(cudaStreamSynchronize(st));
   const uint32_t new_n = h_counts[0];
-
-  (count_launches(1), comm_deg_kernel<<<gridcap((new_n + 256) / 256, 8), 256, 0, st>>>(
-      B.comm_list, new_n, L.comm_sz, B.mem_off, B.mstart, B.comm_deg, B.seg,
-      B.new_deg));
-  LV_TRY(cudaGetLastError());
-  LV_TRY(partition_by_size3(B.comm_deg, new_n, kMergeWarpMax, kMergeBlockMax,
-                            B.comm_cls, B.counts + 4, B.tmp, S, st));
-  LV_TRY(cudaMemcpyAsync(h_counts + 4, B.counts + 4, 3 * sizeof(uint32_t),
-                         cudaMemcpyDeviceToHost, st));
-  LV_TRY(cudaStreamSynchronize(st));
   const uint32_t cntW = h_counts[4], cntB = h_counts[5], cntG = h_counts[6];
 
   Ctx C;
@@ -531,13 +550,12 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
   }
   if (cntG) {
     // plan class-G tables and blocks on the host (few, very large rows)
-    std::vector<uint32_t> gids(cntG);
+    if (cntG > B.g_cap) LV_TRY(grow(grow_ctx, 0, cntG));
+    (count_launches(1), gather_u64_kernel<<<gridcap((cntG + 255) / 256, 8), 256, 0, st>>>(
+        B.comm_deg, B.comm_cls + cntW + cntB, cntG, B.g_tab_off));
+    LV_TRY(cudaGetLastError());
     std::vector<uint64_t> gdeg(cntG);
-    LV_TRY(cudaMemcpyAsync(gids.data(), B.comm_cls + cntW + cntB,
-                           cntG * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    LV_TRY(cudaStreamSynchronize(st));
-    std::vector<uint64_t> all_deg(new_n);
-    LV_TRY(cudaMemcpyAsync(all_deg.data(), B.comm_deg, new_n * sizeof(uint64_t),
+    LV_TRY(cudaMemcpyAsync(gdeg.data(), B.g_tab_off, cntG * sizeof(uint64_t),
                            cudaMemcpyDeviceToHost, st));
     LV_TRY(cudaStreamSynchronize(st));
     std::vector<uint64_t> tab_off(cntG);
@@ -545,7 +563,7 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
     std::vector<uint32_t> blk_comm, blk_chunk, blk_nch;
     uint64_t slots = 0;
     for (uint32_t i = 0; i < cntG; i++) {
-      const uint64_t d = all_deg[gids[i]];
+      const uint64_t d = gdeg[i];
       const uint64_t distinct = std::min<uint64_t>(d, new_n);
       const uint64_t T = next_pow2(2 * distinct + 1);
       tab_off[i] = slots;

@@ -199,7 +199,9 @@ struct lv_engine {
   KStat kst[K_COUNT];
   std::vector<cudaEvent_t> ev_free;
   std::vector<PendingTiming> pending;
-  // one pass of the current level captured as a CUDA graph
+  // all passes of the current level as one graph (WHILE node)
+  cudaGraphExec_t level_exec = nullptr;
+  // one pass of the current level captured as a CUDA graph (timing mode)
   cudaGraphExec_t pass_exec = nullptr;
   bool capturing = false;
   std::vector<PendingTiming> graph_timings;  // event pairs inside the graph
@@ -279,6 +281,8 @@ void prof_collect_graph(lv_engine* E) {
 void drop_pass_graph(lv_engine* E) {
   if (E->pass_exec) cudaGraphExecDestroy(E->pass_exec);
   E->pass_exec = nullptr;
+  if (E->level_exec) cudaGraphExecDestroy(E->level_exec);
+  E->level_exec = nullptr;
   for (const PendingTiming& p : E->graph_timings) {
     E->ev_free.push_back(p.a);
     E->ev_free.push_back(p.b);
@@ -601,17 +605,81 @@ lv_status prepare_level(lv_engine* E) {
   return LV_OK;
 }
 
-lv_status issue_pass(lv_engine* E);
+lv_status issue_pass(lv_engine* E, const PassControl* ctl);
 
-// One pass: the 7 Jacobi steps and the modularity sweep.  With graphs on,
-// the first pass of a level is captured and every pass replays it.
+// Every pass of a level in one graph launch: [control init] -> WHILE
+// { 7 Jacobi steps; modularity sweep + stop rule }.  The body is captured
+// once per level; the modularity kernel's last block evaluates the stop
+// rule (modularity.cu:501-508) and sets the loop condition, so the host
+// waits once per level instead of once per pass.
+lv_status run_level_graph(lv_engine* E, float min_gain) {
+  if (!E->level_exec) {
+    const unsigned long long l0 = launch_count();
+    cudaGraph_t g = nullptr;
+    CU(cudaGraphCreate(&g, 0));
+    struct GraphGuard {
+      cudaGraph_t g;
+      ~GraphGuard() { if (g) cudaGraphDestroy(g); }
+    } guard{g};
+    CU(cudaStreamBeginCaptureToGraph(E->st, g, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    cudaError_t ce = launch_pass_control_init(E->sc, E->st);
+    cudaGraph_t cap = nullptr;
+    cudaError_t ce2 = cudaStreamEndCapture(E->st, &cap);
+    CU(ce);
+    CU(ce2);
+    cudaGraphNode_t init_node = nullptr;
+    size_t nn = 1;
+    CU(cudaGraphGetNodes(g, &init_node, &nn));
+    cudaGraphConditionalHandle h;
+    CU(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t cond_node = nullptr;
+    CU(cudaGraphAddNode(&cond_node, g, &init_node, 1, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    PassControl ctl{};
+    ctl.enabled = 1;
+    ctl.handle = (unsigned long long)h;
+    ctl.min_gain = (double)min_gain;
+    ctl.max_passes = E->cfg.max_passes;
+    CU(cudaStreamBeginCaptureToGraph(E->st, body, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    E->capturing = true;
+    const unsigned long long lb = launch_count();
+    lv_status s = issue_pass(E, &ctl);
+    E->pass_launches = launch_count() - lb;
+    cudaGraph_t bcap = nullptr;
+    ce = cudaStreamEndCapture(E->st, &bcap);
+    E->capturing = false;
+    E->pending.clear();
+    if (s != LV_OK) return s;
+    CU(ce);
+    CU(cudaGraphInstantiate(&E->level_exec, g, 0));
+    // capture counted the init kernel and one pass; lv_phase_move adds the
+    // kernels of the further passes once their number is known
+    (void)l0;
+  }
+  CU(cudaGraphLaunch(E->level_exec, E->st));
+  CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost,
+                     E->st));
+  CU(cudaStreamSynchronize(E->st));
+  return LV_OK;
+}
+
+// One pass (used when timing kernels: event nodes cannot live in a
+// conditional body).  With graphs on, the first pass of a level is captured
+// and every pass replays it.
 lv_status run_pass(lv_engine* E) {
-  if (!E->cfg.use_graphs) return issue_pass(E);
+  if (!E->cfg.use_graphs) return issue_pass(E, nullptr);
   if (!E->pass_exec) {
     const unsigned long long l0 = launch_count();
     CU(cudaStreamBeginCapture(E->st, cudaStreamCaptureModeThreadLocal));
     E->capturing = true;
-    lv_status s = issue_pass(E);
+    lv_status s = issue_pass(E, nullptr);
     cudaGraph_t g = nullptr;
     cudaError_t ce = cudaStreamEndCapture(E->st, &g);
     E->capturing = false;
@@ -635,7 +703,7 @@ lv_status run_pass(lv_engine* E) {
   return LV_OK;
 }
 
-lv_status issue_pass(lv_engine* E) {
+lv_status issue_pass(lv_engine* E, const PassControl* ctl) {
   const LevelView L = E->view();
   const int rule = (E->cfg.rule == LV_RULE_CUDA) ? LV_RULE_CUDA_I : LV_RULE_PY_I;
   HubArena H = E->hub;
@@ -656,7 +724,7 @@ lv_status issue_pass(lv_engine* E) {
   }
   cudaEvent_t t0 = prof_begin(E);
   CU(launch_modularity(L, E->order, E->plan, E->plan.hub_count ? E->hub_map : nullptr,
-                       E->partials, E->st));
+                       E->partials, E->st, ctl));
   prof_end(E, t0, K_MODULARITY, (double)E->e * 12.0 + (double)E->n * 24.0);
   return LV_OK;
 }
@@ -836,6 +904,8 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
   cudaSetDevice(E->device);
   CU(cudaEventRecord(E->ev0, E->st));
   if (!E->level_ready) LVTRY(prepare_level(E));
+  cudaEvent_t ev_prep = take_event(E);
+  CU(cudaEventRecord(ev_prep, E->st));
   lv_level_info info{};
   info.n_vertices = E->n;
   info.n_entries = E->e;
@@ -849,6 +919,14 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
     ret = 0;
     act = old = 0.0;
     info.q_start = 0.0;
+  } else if (E->cfg.use_graphs && !E->profiling) {
+    LVTRY(run_level_graph(E, min_gain));
+    LVTRY(check_device_error(E));
+    passes = E->sc_host->passes;
+    ret = E->sc_host->first_fail ? 0 : 1;
+    act = E->sc_host->q;
+    old = E->sc_host->q_before;
+    if (passes > 1) count_launches((unsigned)((passes - 1) * E->pass_launches));
   } else {
     bool first = true;
     do {
@@ -869,12 +947,15 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
   E->accepted = ret != 0;  // modularity.cu:515-517 (applied at aggregation)
   CU(cudaEventRecord(E->ev1, E->st));
   CU(cudaEventSynchronize(E->ev1));
-  float ms = 0.0f;
+  float ms = 0.0f, prep_ms = 0.0f;
   cudaEventElapsedTime(&ms, E->ev0, E->ev1);
+  cudaEventElapsedTime(&prep_ms, E->ev0, ev_prep);
+  E->ev_free.push_back(ev_prep);
   info.passes = passes;
   info.moved = (uint32_t)ret;
   info.q_end = act;
   info.move_ms = ms;
+  info.prepare_ms = prep_ms;
   E->levels.push_back(info);
   if (!ret) E->finished = true;
   E->q_last = ret ? act : old;

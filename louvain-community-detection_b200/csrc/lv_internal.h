@@ -58,6 +58,20 @@ struct LevelScalars {
   double asq;        // last sweep's sum of squared community totals
   uint32_t error;    // set by a kernel when a bounded loop gave up
   uint32_t done_blocks;  // last-block-done counter of reductions
+  // device-side pass loop (modularity.cu:466-508 run on the GPU)
+  uint32_t passes;       // passes run in the current level
+  uint32_t first_fail;   // the first pass gained less than min gain
+  double q_prev;         // Q after the previous pass
+  double q_before;       // Q before the last pass
+};
+
+// Stop rule evaluated by the modularity sweep's last block when the pass
+// loop runs inside a CUDA graph WHILE node.
+struct PassControl {
+  int enabled;
+  unsigned long long handle;  // cudaGraphConditionalHandle
+  double min_gain;
+  uint32_t max_passes;
 };
 
 // Read-mostly view of the current level passed to kernels by value.
@@ -110,13 +124,14 @@ cudaError_t partition_by_degree(const uint64_t* off, uint32_t n,
                                 uint32_t* tmp, ScanScratch& s,
                                 cudaStream_t st);
 
-// Stable partition of the indices [0, n) into 3 classes by sizes[i]:
-// <= lim0, <= lim1, larger.
-cudaError_t partition_by_size3(const uint64_t* sizes,
-                               uint32_t n, uint64_t lim0, uint64_t lim1,
-                               uint32_t* out, uint32_t* cls_count,
-                               uint32_t* tmp, ScanScratch& s,
-                               cudaStream_t st);
+// Stable partition of the indices [0, *d_live) into 3 classes by sizes[i]:
+// <= lim0, <= lim1, larger.  n_upper bounds *d_live (which is read on the
+// device, so no host round trip is needed).
+cudaError_t partition_by_size3(const uint64_t* sizes, uint32_t n_upper,
+                               const uint32_t* d_live, uint64_t lim0,
+                               uint64_t lim1, uint32_t* out,
+                               uint32_t* cls_count, uint32_t* tmp,
+                               ScanScratch& s, cudaStream_t st);
 
 // ---------------------------------------------------------------------------
 // move.cu
@@ -125,10 +140,15 @@ cudaError_t partition_by_size3(const uint64_t* sizes,
 cudaError_t launch_level_init(const LevelView& L, const uint32_t* order,
                               const DispatchPlan& P, const uint32_t* hub_map,
                               double* partials, cudaStream_t st);
-// Modularity of the current state into sc->q (FP64, deterministic).
+// Modularity of the current state into sc->q (FP64, deterministic).  With
+// ctl->enabled the last block also applies the pass stop rule and sets the
+// graph condition.
 cudaError_t launch_modularity(const LevelView& L, const uint32_t* order,
                               const DispatchPlan& P, const uint32_t* hub_map,
-                              double* partials, cudaStream_t st);
+                              double* partials, cudaStream_t st,
+                              const PassControl* ctl = nullptr);
+// passes = 0, first_fail = 0, q_prev = q (start of a level's pass loop)
+cudaError_t launch_pass_control_init(LevelScalars* sc, cudaStream_t st);
 // Hub (class 8) arenas: per hub vertex a table of tab_size[i] slots at
 // tab_off[i] (FP64 values, u32 keys), a best key and an own-weight sum.
 struct HubArena {

@@ -152,6 +152,15 @@ __device__ __forceinline__ uint32_t table_insert(uint32_t* keys, uint32_t mask,
   return 0;
 }
 
+// Table slots used for a row of d entries: a power of two >= 1.5 d (load
+// factor <= 2/3), at most tmax (the class's shared-memory table).
+__device__ __forceinline__ uint32_t table_size_for(uint32_t d, uint32_t tmax) {
+  const uint32_t want = d + (d >> 1) + 1;
+  uint32_t t = 32;
+  while (t < want) t <<= 1;
+  return t < tmax ? t : tmax;
+}
+
 // ---------------------------------------------------------------------------
 // Move kernels
 // ---------------------------------------------------------------------------
@@ -219,15 +228,16 @@ __global__ void __launch_bounds__(kThreads)
       reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T * kWarps) + wib * T;
   for (uint32_t vidx = blockIdx.x * kWarps + wib; vidx < count;
        vidx += gridDim.x * kWarps) {
-    for (int i = lane; i < T; i += 32) {
-      keys[i] = kEmptyKey;
-      vals[i] = 0.0;
-    }
-    __syncwarp();
     const uint32_t v = verts[vidx];
     const uint64_t s = L.off[v];
     const uint32_t d = (uint32_t)(L.off[v + 1] - s);
     const uint32_t cv = L.comm[v];
+    const uint32_t tv = table_size_for(d, T);
+    for (uint32_t i = lane; i < tv; i += 32) {
+      keys[i] = kEmptyKey;
+      vals[i] = 0.0;
+    }
+    __syncwarp();
     double own = 0.0;
     for (uint32_t j0 = 0; j0 < d; j0 += 32) {
       const uint32_t j = j0 + lane;
@@ -244,7 +254,7 @@ __global__ void __launch_bounds__(kThreads)
       const unsigned peers = __match_any_sync(kFull, mk);
       const int leader = __ffs(peers) - 1;
       uint32_t slot = 0;
-      if (has && lane == leader) slot = table_insert(keys, T - 1, cu, L.sc);
+      if (has && lane == leader) slot = table_insert(keys, tv - 1, cu, L.sc);
       slot = __shfl_sync(kFull, slot, leader);
       if (has) atomicAdd(&vals[slot], (double)wt);
       if (RULE == LV_RULE_CUDA_I && has && cu == cv && u != v) own += (double)wt;
@@ -252,7 +262,7 @@ __global__ void __launch_bounds__(kThreads)
     __syncwarp();
     const GainCtx g = make_ctx(L, v, cv);
     unsigned long long best = 0ull;
-    for (int i = lane; i < T; i += 32) {
+    for (uint32_t i = lane; i < tv; i += 32) {
       const uint32_t c = keys[i];
       if (c != kEmptyKey) best = umax64(best, candidate(L, g, c, vals[i]));
     }
@@ -329,22 +339,23 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ unsigned long long red_best[kWarps];
   __shared__ double red_own[kWarps];
   for (uint32_t vidx = blockIdx.x; vidx < count; vidx += gridDim.x) {
-    for (int i = threadIdx.x; i < T; i += kThreads) {
-      keys[i] = kEmptyKey;
-      vals[i] = 0.0;
-    }
-    __syncthreads();
     const uint32_t v = verts[vidx];
     const uint64_t s = L.off[v];
     const uint32_t d = (uint32_t)(L.off[v + 1] - s);
     const uint32_t cv = L.comm[v];
+    const uint32_t tv = table_size_for(d, T);
+    for (uint32_t i = threadIdx.x; i < tv; i += kThreads) {
+      keys[i] = kEmptyKey;
+      vals[i] = 0.0;
+    }
+    __syncthreads();
     double own = 0.0;
     for (uint32_t j0 = 0; j0 < d; j0 += kThreads)
-      insert_wave<RULE>(L, s, j0 + threadIdx.x, d, v, cv, keys, vals, T - 1, own);
+      insert_wave<RULE>(L, s, j0 + threadIdx.x, d, v, cv, keys, vals, tv - 1, own);
     __syncthreads();
     const GainCtx g = make_ctx(L, v, cv);
     unsigned long long best = 0ull;
-    for (int i = threadIdx.x; i < T; i += kThreads) {
+    for (uint32_t i = threadIdx.x; i < tv; i += kThreads) {
       const uint32_t c = keys[i];
       if (c != kEmptyKey) best = umax64(best, candidate(L, g, c, vals[i]));
     }
@@ -670,7 +681,7 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 __global__ void __launch_bounds__(kThreads)
-    modularity_kernel(LevelView L, DispatchArgs A) {
+    modularity_kernel(LevelView L, DispatchArgs A, PassControl ctl) {
   __shared__ double red[kWarps];
   double part = 0.0;
   dispatch_units(L, A, IntraOp{}, part, red);
@@ -687,11 +698,30 @@ __global__ void __launch_bounds__(kThreads)
   sum_partials(A, red, intra, sq);
   if (threadIdx.x == 0) {
     const double m = L.sc->m64;
+    const double q = (m > 0.0) ? (intra / (2.0 * m)) - (sq / (4.0 * m * m)) : 0.0;
     L.sc->intra = intra;
     L.sc->asq = sq;
-    L.sc->q = (m > 0.0) ? (intra / (2.0 * m)) - (sq / (4.0 * m * m)) : 0.0;
+    L.sc->q = q;
     L.sc->done_blocks = 0u;
+    if (ctl.enabled) {
+      // stop rule of modularity.cu:501-508 / louvian.py:91-99
+      const uint32_t p = L.sc->passes + 1;
+      const double old = L.sc->q_prev;
+      if (p == 1 && q - old < ctl.min_gain) L.sc->first_fail = 1u;
+      const bool cont = (q - old >= ctl.min_gain) && p < ctl.max_passes;
+      L.sc->passes = p;
+      L.sc->q_before = old;
+      L.sc->q_prev = q;
+      cudaGraphSetConditional((cudaGraphConditionalHandle)ctl.handle, cont ? 1u : 0u);
+    }
   }
+}
+
+__global__ void pass_control_init_kernel(LevelScalars* sc) {
+  sc->passes = 0u;
+  sc->first_fail = 0u;
+  sc->q_prev = sc->q;
+  sc->q_before = sc->q;
 }
 
 // ---------------------------------------------------------------------------
@@ -834,9 +864,17 @@ cudaError_t launch_level_init(const LevelView& L, const uint32_t* order,
 
 cudaError_t launch_modularity(const LevelView& L, const uint32_t* order,
                               const DispatchPlan& P, const uint32_t* hub_map,
-                              double* partials, cudaStream_t st) {
+                              double* partials, cudaStream_t st,
+                              const PassControl* ctl) {
   DispatchArgs A = make_args(order, P, hub_map, partials);
-  (count_launches(1), modularity_kernel<<<dispatch_grid(P), kThreads, 0, st>>>(L, A));
+  PassControl c{};
+  if (ctl) c = *ctl;
+  (count_launches(1), modularity_kernel<<<dispatch_grid(P), kThreads, 0, st>>>(L, A, c));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pass_control_init(LevelScalars* sc, cudaStream_t st) {
+  (count_launches(1), pass_control_init_kernel<<<1, 1, 0, st>>>(sc));
   return cudaGetLastError();
 }
 

@@ -219,8 +219,10 @@ struct Identity {
 };
 struct SizeClass3 {
   const uint64_t* sizes;
+  const uint32_t* live;  // items i >= *live belong to no class
   uint64_t lim0, lim1;
   __device__ int operator()(uint32_t i) const {
+    if (i >= *live) return -1;
     uint64_t s = sizes[i];
     return s <= lim0 ? 0 : (s <= lim1 ? 1 : 2);
   }
@@ -263,13 +265,13 @@ cudaError_t partition_by_degree(const uint64_t* off, uint32_t n,
                                   cls_count, tmp, s, st);
 }
 
-cudaError_t partition_by_size3(const uint64_t* sizes,
-                               uint32_t n, uint64_t lim0, uint64_t lim1,
-                               uint32_t* out, uint32_t* cls_count,
-                               uint32_t* tmp, ScanScratch& s,
-                               cudaStream_t st) {
-  return partition_impl<3>(n, SizeClass3{sizes, lim0, lim1}, Identity{},
-                           out, cls_count, tmp, s, st);
+cudaError_t partition_by_size3(const uint64_t* sizes, uint32_t n_upper,
+                               const uint32_t* d_live, uint64_t lim0,
+                               uint64_t lim1, uint32_t* out,
+                               uint32_t* cls_count, uint32_t* tmp,
+                               ScanScratch& s, cudaStream_t st) {
+  return partition_impl<3>(n_upper, SizeClass3{sizes, d_live, lim0, lim1},
+                           Identity{}, out, cls_count, tmp, s, st);
 }
 
 }  // namespace lvb

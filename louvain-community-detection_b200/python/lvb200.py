@@ -54,6 +54,7 @@ class LevelInfo(ctypes.Structure):
         ("q_end", ctypes.c_double),
         ("move_ms", ctypes.c_float),
         ("aggregate_ms", ctypes.c_float),
+        ("prepare_ms", ctypes.c_float),
     ]
 
 
@@ -335,7 +336,8 @@ class Engine:
         return [
             dict(n_vertices=a.n_vertices, n_entries=a.n_entries, passes=a.passes,
                  moved=bool(a.moved), q_start=a.q_start, q_end=a.q_end,
-                 move_ms=a.move_ms, aggregate_ms=a.aggregate_ms)
+                 move_ms=a.move_ms, aggregate_ms=a.aggregate_ms,
+                 prepare_ms=a.prepare_ms)
             for a in arr[: cnt.value]
         ]
 

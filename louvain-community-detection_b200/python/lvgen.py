@@ -117,20 +117,46 @@ def planted_powerlaw(n: int = 334_863, target_edges: int = 925_872,
     """Chung-Lu style degrees with planted communities (LFR-like):
     a (1-mu) share of each vertex's stubs pairs inside its community, the
     rest pairs globally; duplicates and self-loops are removed."""
+    # Degrees follow a continuous power law on [xmin, max_deg], rounded; the
+    # stub budget is calibrated (two deterministic rounds) so that the
+    # simple graph left after removing loops and duplicates has about
+    # target_edges edges.
+    scale = 1.0
+    for _ in range(3):
+        src, dst, comm_of, sizes = _planted_edges(n, target_edges * scale, gamma,
+                                                  max_deg, mu, comm_exp, comm_min,
+                                                  comm_max, seed)
+        got = len(src)
+        if abs(got - target_edges) <= 0.002 * target_edges:
+            break
+        scale *= target_edges / max(got, 1)
+    rng = np.random.default_rng(seed + 7919)
+    w = np.ones(len(src), dtype=F32) if unit else \
+        rng.uniform(0.5, 1.5, len(src)).astype(F32)
+    return n, src, dst, w
+
+
+def _cont_powerlaw_mean(gamma, xmin, xmax):
+    a, b = 1.0 - gamma, 2.0 - gamma
+    return (a / b) * (xmax ** b - xmin ** b) / (xmax ** a - xmin ** a)
+
+
+def _planted_edges(n, target_edges, gamma, max_deg, mu, comm_exp, comm_min,
+                   comm_max, seed):
     rng = np.random.default_rng(seed)
     mean_target = 2.0 * target_edges / n
-    # choose the minimum degree so the power law's mean is near the target
-    deg = None
-    for dmin in range(1, 20):
-        ks = np.arange(dmin, max_deg + 1, dtype=np.float64)
-        p = ks ** (-gamma)
-        mean = (ks * p).sum() / p.sum()
-        if mean >= mean_target * 0.93:
-            deg = _powerlaw_ints(rng, n, gamma, dmin, max_deg)
-            break
-    if deg is None:
-        deg = _powerlaw_ints(rng, n, gamma, 1, max_deg)
-    deg = deg.astype(np.int64)
+    lo, hi = 0.5, 60.0
+    for _ in range(60):  # xmin giving the target mean
+        mid = 0.5 * (lo + hi)
+        if _cont_powerlaw_mean(gamma, mid, max_deg) < mean_target:
+            lo = mid
+        else:
+            hi = mid
+    xmin = 0.5 * (lo + hi)
+    a = 1.0 - gamma
+    u = rng.random(n)
+    x = ((max_deg ** a - xmin ** a) * u + xmin ** a) ** (1.0 / a)
+    deg = np.clip(np.rint(x), 1, max_deg).astype(np.int64)
     # community sizes ~ power law (exponent comm_exp) covering n vertices
     sizes = []
     total = 0
@@ -173,9 +199,7 @@ def planted_powerlaw(n: int = 334_863, target_edges: int = 925_872,
     src = np.concatenate([a1, a2])
     dst = np.concatenate([b1, b2])
     src, dst = _simple(n, src, dst, rng)
-    w = np.ones(len(src), dtype=F32) if unit else \
-        rng.uniform(0.5, 1.5, len(src)).astype(F32)
-    return n, src, dst, w
+    return src, dst, comm_of, sizes
 
 
 def _simple(n, src, dst, rng, shuffle=True):

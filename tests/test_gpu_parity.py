@@ -217,12 +217,17 @@ def test_run_device_equals_run():
 def test_graph_replay_equals_direct_launches(name):
     """Capturing a level's pass in a CUDA graph changes nothing."""
     out = []
-    for ug in (False, True):
+    # host pass loop; device pass loop (graph WHILE node); per-pass replay
+    # of a captured pass (the mode kernel timing uses)
+    for ug, prof in ((False, False), (True, False), (True, True)):
         with lvb200.Engine(rule="py", use_graphs=ug) as e:
+            e.set_profiling(prof)
             out.append(e.run(lvb200.Graph.load_mtx(golden_mtx(name)), 1e-6))
-    assert out[0].modularity == out[1].modularity
-    assert np.array_equal(out[0].assignment, out[1].assignment)
-    assert [l["passes"] for l in out[0].levels] == [l["passes"] for l in out[1].levels]
+    for o in out[1:]:
+        assert o.modularity == out[0].modularity
+        assert np.array_equal(o.assignment, out[0].assignment)
+        assert [l["passes"] for l in o.levels] == [l["passes"] for l in out[0].levels]
+        assert [l["q_end"] for l in o.levels] == [l["q_end"] for l in out[0].levels]
 
 
 def test_kernel_profiling_counts(eng):
