@@ -239,6 +239,53 @@ def rmat(scale: int, edge_factor: int = 16, a=0.57, b=0.19, c=0.19,
     return n, src, dst, w
 
 
+def rmat_device(scale: int, edge_factor: int = 16, a=0.57, b=0.19, c=0.19,
+                seed: int = 0, device: str = "cuda"):
+    """R-MAT generated and symmetrised on the GPU (torch), for sizes numpy
+    cannot produce quickly (scale 24: 268M draws, 537M stored entries).
+    Duplicates merged, self-loops dropped, unit weights.  Returns
+    (n, off int64[n+1], col int32[E], w float32[E], n_edges) as device
+    tensors; a row lists its higher-numbered neighbours, then its
+    lower-numbered ones, each group ascending."""
+    import torch
+
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    n = 1 << scale
+    m = edge_factor * n
+    src = torch.zeros(m, dtype=torch.int64, device=device)
+    dst = torch.zeros(m, dtype=torch.int64, device=device)
+    ab, abc = a + b, a + b + c
+    for lvl in range(scale):
+        r = torch.rand(m, generator=gen, device=device)
+        bit = 1 << (scale - 1 - lvl)
+        src += (r >= ab).to(torch.int64) * bit
+        dst += (((r >= a) & (r < ab)) | (r >= abc)).to(torch.int64) * bit
+        del r
+    keep = src != dst
+    lo = torch.minimum(src, dst)[keep]
+    hi = torch.maximum(src, dst)[keep]
+    del src, dst, keep
+    key = torch.unique(lo * n + hi)  # sorted, duplicates merged
+    del lo, hi
+    lo = key // n
+    hi = key % n
+    del key
+    n_edges = int(lo.numel())
+    rows = torch.cat([lo, hi])
+    cols = torch.cat([hi, lo])
+    del lo, hi
+    rows, order = torch.sort(rows, stable=True)
+    cols = cols[order].to(torch.int32)
+    del order
+    counts = torch.bincount(rows, minlength=n)
+    del rows
+    off = torch.zeros(n + 1, dtype=torch.int64, device=device)
+    off[1:] = torch.cumsum(counts, 0)
+    w = torch.ones(cols.numel(), dtype=torch.float32, device=device)
+    return n, off, cols, w, n_edges
+
+
 def sbm(n: int, blocks: int, mean_deg: float = 16.0, ratio: float = 20.0,
         seed: int = 0, wlo: float = 0.5, whi: float = 1.5):
     """Stochastic block model with equal blocks, p_in/p_out = ratio, mean
