@@ -93,16 +93,17 @@ __global__ void class_degree_kernel(const uint64_t* off, uint32_t n,
 
 // Timed launch groups.
 enum KId {
-  K_MOVE1 = 0,  // .. K_MOVE1 + 6 = bucket 7
-  K_APPLY = 7,
-  K_MODULARITY = 8,
-  K_LEVEL_INIT = 9,
-  K_CONTRACT = 10,
-  K_COUNT = 11
+  K_MOVE1 = 0,  // .. K_MOVE1 + 6 = bucket 7's shared-table class
+  K_HUB = 7,    // bucket 7's multi-block class (degree > 2048)
+  K_APPLY = 8,
+  K_MODULARITY = 9,
+  K_LEVEL_INIT = 10,
+  K_CONTRACT = 11,
+  K_COUNT = 12
 };
 const char* kKName[K_COUNT] = {"move_b1", "move_b2", "move_b3",    "move_b4",
-                               "move_b5", "move_b6", "move_b7",    "apply",
-                               "modularity", "level_init", "contract"};
+                               "move_b5", "move_b6", "move_b7",    "move_hub",
+                               "apply",   "modularity", "level_init", "contract"};
 
 struct KStat {
   uint64_t launches = 0;
@@ -336,6 +337,9 @@ void free_state(lv_engine* E) {
   dfree(E->hub.blk_vertex);
   dfree(E->hub.blk_chunk);
   dfree(E->hub.blk_nchunks);
+  dfree(E->hub.list);
+  dfree(E->hub.list_off);
+  dfree(E->hub.list_cnt);
   dfree(E->hub_deg);
   ContractBuffers& B = E->cb;
   dfree(B.flag_id);
@@ -474,9 +478,9 @@ lv_status prepare_level(lv_engine* E) {
   const uint32_t hc = P.cls_start[9] - hs;
   // hub plan
   std::vector<uint32_t> blk_vertex, blk_chunk, blk_nch;
-  std::vector<uint64_t> tab_off;
+  std::vector<uint64_t> tab_off, list_off;
   std::vector<uint32_t> tab_size;
-  uint64_t slots = 0;
+  uint64_t slots = 0, list_total = 0;
   if (hc) {
     if (hc > E->hub_count_cap) {
       dfree(E->hub_deg);
@@ -484,11 +488,15 @@ lv_status prepare_level(lv_engine* E) {
       dfree(E->hub.tab_size);
       dfree(E->hub.best);
       dfree(E->hub.own);
+      dfree(E->hub.list_off);
+      dfree(E->hub.list_cnt);
       CU(dalloc(&E->hub_deg, hc));
       CU(dalloc(&E->hub.tab_off, hc));
       CU(dalloc(&E->hub.tab_size, hc));
       CU(dalloc(&E->hub.best, hc));
       CU(dalloc(&E->hub.own, hc));
+      CU(dalloc(&E->hub.list_off, hc));
+      CU(dalloc(&E->hub.list_cnt, hc));
       E->hub_count_cap = hc;
     }
     (count_launches(1), gather_degrees_kernel<<<(hc + 255) / 256, 256, 0, st>>>(E->off(), E->order + hs,
@@ -500,12 +508,15 @@ lv_status prepare_level(lv_engine* E) {
     CU(cudaStreamSynchronize(st));
     tab_off.resize(hc);
     tab_size.resize(hc);
+    list_off.resize(hc);
     for (uint32_t i = 0; i < hc; i++) {
       const uint64_t distinct = std::min<uint64_t>(deg[i], n);
       const uint64_t T = next_pow2(2 * distinct + 1);
       tab_off[i] = slots;
       tab_size[i] = (uint32_t)T;
       slots += T;
+      list_off[i] = list_total;
+      list_total += distinct;
       const uint32_t nch = (uint32_t)((deg[i] + kHubChunk - 1) / kHubChunk);
       for (uint32_t ch = 0; ch < nch; ch++) {
         blk_vertex.push_back(i);
@@ -551,8 +562,11 @@ lv_status prepare_level(lv_engine* E) {
     if (slots > E->hub_slots_cap) {
       dfree(E->hub.keys);
       dfree(E->hub.vals);
+      dfree(E->hub.list);
       CU(dalloc(&E->hub.keys, slots));
       CU(dalloc(&E->hub.vals, slots));
+      // a table holds at most half its slots, so the lists fit in slots/2
+      CU(dalloc(&E->hub.list, slots / 2 + 1));
       E->hub_slots_cap = slots;
     }
     std::vector<uint32_t> map(2 * hb);
@@ -574,6 +588,9 @@ lv_status prepare_level(lv_engine* E) {
     CU(cudaMemsetAsync(E->hub.vals, 0, slots * sizeof(double), st));
     CU(cudaMemsetAsync(E->hub.best, 0, hc * sizeof(unsigned long long), st));
     CU(cudaMemsetAsync(E->hub.own, 0, hc * sizeof(double), st));
+    CU(cudaMemsetAsync(E->hub.list_cnt, 0, hc * sizeof(uint32_t), st));
+    CU(cudaMemcpyAsync(E->hub.list_off, list_off.data(), hc * sizeof(uint64_t),
+                       cudaMemcpyHostToDevice, st));
     CU(cudaMemsetAsync(E->partials, 0, hc * sizeof(double), st));
   }
   // entries per move class (byte counts of the kernel timings)
@@ -714,10 +731,16 @@ lv_status issue_pass(lv_engine* E, const PassControl* ctl) {
     // algorithmic bytes: every entry's (col, w, comm[col]) and, per vertex,
     // order id, offset, comm, k, a_C(v) (FP64) and the proposal
     const double vb = (double)(e - s);
-    const double eb = (double)(E->class_deg[b] + (b == 7 ? E->class_deg[8] : 0));
+    const double v7 = (double)(E->plan.cls_start[b + 1] - s);
     cudaEvent_t t0 = prof_begin(E);
     CU(launch_move_bucket(L, b, rule, E->order, E->prop, E->plan, H, E->st));
-    prof_end(E, t0, K_MOVE1 + b - 1, eb * 12.0 + vb * 32.0);
+    prof_end(E, t0, K_MOVE1 + b - 1, (double)E->class_deg[b] * 12.0 + v7 * 32.0);
+    if (b == 7 && E->plan.hub_count) {
+      t0 = prof_begin(E);
+      CU(launch_move_bucket(L, 8, rule, E->order, E->prop, E->plan, H, E->st));
+      prof_end(E, t0, K_HUB,
+               (double)E->class_deg[8] * 12.0 + (double)E->plan.hub_count * 32.0);
+    }
     t0 = prof_begin(E);
     CU(launch_apply_bucket(L, b, E->order, E->prop, E->plan, E->st));
     prof_end(E, t0, K_APPLY, vb * 12.0);

@@ -27,7 +27,7 @@ constexpr uint64_t kBucketHi[kBuckets + 1] = {0, 4, 8, 16, 32, 84, 319,
 constexpr int kClasses = 9;                 // 0..8, class 0 = degree 0
 constexpr uint64_t kHubSmemMaxDeg = 2048;   // class 7 upper degree
 constexpr int kHubSmemSlots = 4096;         // table slots of class 7
-constexpr uint32_t kHubChunk = 4096;        // edges per block, class 8
+constexpr uint32_t kHubChunk = 2048;        // edges per block, class 8
 
 __host__ __device__ inline int move_class_of_degree(uint64_t d) {
   return d == 0      ? 0
@@ -161,9 +161,13 @@ struct HubArena {
   uint32_t* blk_vertex = nullptr;  // [hub_blocks] hub index of each block
   uint32_t* blk_chunk = nullptr;   // [hub_blocks] chunk within the vertex
   uint32_t* blk_nchunks = nullptr; // [hub_blocks] chunks of that vertex
+  uint32_t* list = nullptr;        // occupied slots of every table
+  uint64_t* list_off = nullptr;    // [hub_count] start of a hub's list
+  uint32_t* list_cnt = nullptr;    // [hub_count] entries in a hub's list
 };
-// One Jacobi step: proposals for every vertex of bucket b (1..7), then the
-// moves applied (sizes, totals, comm).  proposal[] is parallel to order[].
+// Proposals for the vertices of kernel class c (1..8; bucket 7 is classes 7
+// and 8, both launched before its apply).  proposal[] is parallel to
+// order[].
 cudaError_t launch_move_bucket(const LevelView& L, int bucket, int rule,
                                const uint32_t* order, uint32_t* proposal,
                                const DispatchPlan& P, const HubArena& H,

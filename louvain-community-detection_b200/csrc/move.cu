@@ -367,11 +367,17 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // deg > 2048: the vertex's edges are split in chunks of kHubChunk, one
-// block per chunk, all inserting into the vertex's global table.
+// block per chunk.  A block first sums its chunk per neighbour community in
+// a shared table, then adds one total per distinct community to the
+// vertex's global table; a community seen for the first time is appended
+// to the vertex's list, so the scan below walks only the distinct entries.
 template <int RULE>
 __global__ void __launch_bounds__(kThreads)
     hub_insert_kernel(LevelView L, const uint32_t* __restrict__ hubs,
                       HubArena H, uint32_t hub_blocks) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* lvals = reinterpret_cast<double*>(smem_raw);
+  uint32_t* lkeys = reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * kHubSmemSlots);
   __shared__ double red_own[kWarps];
   for (uint32_t b = blockIdx.x; b < hub_blocks; b += gridDim.x) {
     const uint32_t hi = H.blk_vertex[b], ch = H.blk_chunk[b];
@@ -381,21 +387,50 @@ __global__ void __launch_bounds__(kThreads)
     const uint32_t cv = L.comm[v];
     const uint64_t lo = (uint64_t)ch * kHubChunk;
     const uint64_t end = min(d, lo + kHubChunk);
-    uint32_t* keys = H.keys + H.tab_off[hi];
-    double* vals = H.vals + H.tab_off[hi];
-    const uint32_t mask = H.tab_size[hi] - 1;
+    const uint32_t tl = table_size_for((uint32_t)(end - lo), kHubSmemSlots);
+    for (uint32_t i = threadIdx.x; i < tl; i += kThreads) {
+      lkeys[i] = kEmptyKey;
+      lvals[i] = 0.0;
+    }
+    __syncthreads();
     double own = 0.0;
     for (uint64_t j0 = lo; j0 < end; j0 += kThreads)
-      insert_wave<RULE>(L, s, j0 + threadIdx.x, end, v, cv, keys, vals, mask, own);
+      insert_wave<RULE>(L, s, j0 + threadIdx.x, end, v, cv, lkeys, lvals, tl - 1, own);
+    __syncthreads();
+    uint32_t* keys = H.keys + H.tab_off[hi];
+    double* vals = H.vals + H.tab_off[hi];
+    uint32_t* list = H.list + H.list_off[hi];
+    const uint32_t mask = H.tab_size[hi] - 1;
+    for (uint32_t i = threadIdx.x; i < tl; i += kThreads) {
+      const uint32_t c = lkeys[i];
+      if (c == kEmptyKey) continue;
+      uint32_t h = hash_slot(c, mask);
+      for (uint32_t it = 0; it <= mask; it++) {
+        const uint32_t cur = keys[h];
+        if (cur == c) break;
+        if (cur == kEmptyKey) {
+          const uint32_t prev = atomicCAS(&keys[h], kEmptyKey, c);
+          if (prev == kEmptyKey) {
+            list[atomicAdd(&H.list_cnt[hi], 1u)] = h;
+            break;
+          }
+          if (prev == c) break;
+        }
+        h = (h + 1) & mask;
+        if (it == mask) atomicExch(&L.sc->error, 1u);
+      }
+      atomicAdd(&vals[h], lvals[i]);
+    }
     if (RULE == LV_RULE_CUDA_I) {
       own = block_sum(own, red_own);
       if (threadIdx.x == 0 && own != 0.0) atomicAdd(&H.own[hi], own);
     }
+    __syncthreads();
   }
 }
 
-// Evaluates the hub tables' candidates (each block a slice of one table),
-// clears the slots it read, and folds its best key into H.best.
+// Evaluates a slice of a hub's distinct communities (its list), clears the
+// table slots it read, and folds its best key into H.best.
 __global__ void __launch_bounds__(kThreads)
     hub_scan_kernel(LevelView L, const uint32_t* __restrict__ hubs, HubArena H,
                     uint32_t hub_blocks) {
@@ -406,18 +441,18 @@ __global__ void __launch_bounds__(kThreads)
     const uint32_t v = hubs[hi];
     const uint32_t cv = L.comm[v];
     const GainCtx g = make_ctx(L, v, cv);
-    const uint64_t T = H.tab_size[hi];
-    const uint64_t lo = T * ch / nch, hi_s = T * (ch + 1) / nch;
+    const uint64_t cnt = H.list_cnt[hi];
+    const uint64_t lo = cnt * ch / nch, hi_s = cnt * (ch + 1) / nch;
     uint32_t* keys = H.keys + H.tab_off[hi];
     double* vals = H.vals + H.tab_off[hi];
+    const uint32_t* list = H.list + H.list_off[hi];
     unsigned long long best = 0ull;
     for (uint64_t i = lo + threadIdx.x; i < hi_s; i += kThreads) {
-      const uint32_t c = keys[i];
-      if (c != kEmptyKey) {
-        best = umax64(best, candidate(L, g, c, vals[i]));
-        keys[i] = kEmptyKey;
-        vals[i] = 0.0;
-      }
+      const uint32_t slot = list[i];
+      const uint32_t c = keys[slot];
+      best = umax64(best, candidate(L, g, c, vals[slot]));
+      keys[slot] = kEmptyKey;
+      vals[slot] = 0.0;
     }
     best = block_max(best, red_best);
     if (threadIdx.x == 0 && best) atomicMax(&H.best[hi], best);
@@ -435,6 +470,7 @@ __global__ void hub_decide_kernel(LevelView L, const uint32_t* __restrict__ hubs
     prop[i] = decide<RULE>(H.best[i], H.own[i], g);
     H.best[i] = 0ull;
     H.own[i] = 0.0;
+    H.list_cnt[i] = 0u;
   }
 }
 
@@ -847,6 +883,12 @@ cudaError_t configure_kernels() {
   e = cudaFuncSetAttribute(move_block_kernel<LV_RULE_CUDA_I>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, block_tab);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(hub_insert_kernel<LV_RULE_PY_I>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, block_tab);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(hub_insert_kernel<LV_RULE_CUDA_I>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, block_tab);
+  if (e != cudaSuccess) return e;
   return configure_contract_kernels();
 }
 
@@ -915,16 +957,18 @@ static cudaError_t move_bucket_impl(const LevelView& L, int bucket,
                                     kWarps * T * 12, st>>>(L, verts, cnt, pr));
       }
       break;
-    case 7: {
-      // class 7: shared table; class 8: global tables
+    case 7:  // class 7 of bucket 7: shared table, one block per vertex
       if (cnt) {
         (count_launches(1), move_block_kernel<RULE><<<grid_for(cnt, sm_count() * 4), kThreads,
                                   kHubSmemSlots * 12, st>>>(L, verts, cnt, pr));
       }
+      break;
+    case 8: {  // class 8 of bucket 7: global tables, several blocks per vertex
       const uint32_t hs = P.cls_start[8];
       const uint32_t hc = P.cls_start[9] - hs;
       if (hc) {
-        (count_launches(1), hub_insert_kernel<RULE><<<grid_for(P.hub_blocks, cap), kThreads, 0, st>>>(
+        (count_launches(1), hub_insert_kernel<RULE><<<grid_for(P.hub_blocks, sm_count() * 4),
+                                                     kThreads, kHubSmemSlots * 12, st>>>(
             L, order + hs, H, P.hub_blocks));
         (count_launches(1), hub_scan_kernel<<<grid_for(P.hub_blocks, cap), kThreads, 0, st>>>(
             L, order + hs, H, P.hub_blocks));

@@ -49,6 +49,8 @@ def main():
     ap.add_argument("--runs", type=int, default=1)
     ap.add_argument("--min-gain", type=float, default=1e-6)
     ap.add_argument("--timing", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="time every launch group with CUDA events")
     args = ap.parse_args()
     import torch
 
@@ -62,7 +64,9 @@ def main():
     print(f"workload={args.workload} V={n} edges={m} entries={nnz} gen_s={gen_s:.1f}")
     asg = torch.empty(n, dtype=torch.int32, device="cuda")
     with lvb200.Engine(rule=args.rule, use_graphs=not args.no_graphs) as e:
+        e.set_profiling(args.profile)
         for i in range(args.runs):
+            e.reset_kernel_stats()
             t0 = time.perf_counter()
             r = e.run_device(n, nnz, off.data_ptr(), col.data_ptr(), w.data_ptr(),
                              args.min_gain, asg.data_ptr())
@@ -75,6 +79,13 @@ def main():
                 print("  level V={n_vertices} E={n_entries} passes={passes} "
                       "prepare_ms={prepare_ms:.3f} move_ms={move_ms:.3f} "
                       "aggregate_ms={aggregate_ms:.3f} q_end={q_end:.8f}".format(**lv))
+        if args.profile:
+            for name, st in e.kernel_stats().items():
+                if st["launches"]:
+                    gbs = st["bytes"] / (st["total_ms"] / 1e3) / 1e9
+                    print(f"  kernel {name:11s} launches={st['launches']:5d} "
+                          f"ms={st['total_ms']:9.3f} avg_us={1e3 * st['total_ms'] / st['launches']:9.2f} "
+                          f"alg_GB/s={gbs:8.1f}")
 
 
 if __name__ == "__main__":
