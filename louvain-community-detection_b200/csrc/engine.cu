@@ -9,7 +9,9 @@
 // Status codes instead of HANDLE_ERROR's exit() (utils.cuh:95-100).
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -121,6 +123,25 @@ struct PendingTiming {
 
 void lvb_set_error(const std::string& msg) { g_last_error = msg; }
 
+// Opt-in host-side trace (LVB200_TRACE=1): wall-clock time of each step of
+// the level loop on stderr.
+namespace {
+struct Trace {
+  bool on;
+  std::chrono::steady_clock::time_point t0;
+  Trace() : on(getenv("LVB200_TRACE") != nullptr), t0(std::chrono::steady_clock::now()) {}
+  void mark(const char* what, uint32_t level, uint32_t n) {
+    if (!on) return;
+    const auto t = std::chrono::steady_clock::now();
+    fprintf(stderr, "[lvb200] level=%u V=%u %-28s %9.3f ms\n", level, n, what,
+            std::chrono::duration<double, std::milli>(t - t0).count());
+    t0 = t;
+  }
+  void reset() { t0 = std::chrono::steady_clock::now(); }
+};
+Trace g_trace;
+}  // namespace
+
 namespace lvb {
 static std::atomic<unsigned long long> g_launches{0};
 void count_launches(unsigned k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
@@ -171,8 +192,9 @@ struct lv_engine {
   uint32_t* hub_map = nullptr;  // [blk_vertex | blk_chunk] for dispatch
   size_t hub_map_cap = 0;
   HubArena hub;
-  size_t hub_slots_cap = 0, hub_count_cap = 0, hub_blocks_cap = 0;
+  size_t hub_slots_cap = 0, hub_count_cap = 0, hub_blocks_cap = 0, hub_list_cap = 0;
   uint64_t* hub_deg = nullptr;
+  std::vector<uint32_t> hub_batches;  // block boundaries of the hub batches
 
   ContractBuffers cb{};
   ScanScratch scan;
@@ -369,7 +391,7 @@ void free_state(lv_engine* E) {
   E->scan.buf = nullptr;
   E->scan.bytes = 0;
   E->partials_cap = E->hub_map_cap = 0;
-  E->hub_slots_cap = E->hub_count_cap = E->hub_blocks_cap = 0;
+  E->hub_slots_cap = E->hub_count_cap = E->hub_blocks_cap = E->hub_list_cap = 0;
   E->cap_n = 0;
   E->cap_e = 0;
   E->in_off = nullptr;
@@ -470,6 +492,7 @@ lv_status prepare_level(lv_engine* E) {
   CU(cudaMemcpyAsync(E->h_counts, E->cls_count, kClasses * sizeof(uint32_t),
                      cudaMemcpyDeviceToHost, st));
   CU(cudaStreamSynchronize(st));
+  g_trace.mark("  degree classes", (uint32_t)E->levels.size(), n);
   DispatchPlan& P = E->plan;
   memset(&P, 0, sizeof(P));
   P.cls_start[0] = 0;
@@ -509,12 +532,22 @@ lv_status prepare_level(lv_engine* E) {
     tab_off.resize(hc);
     tab_size.resize(hc);
     list_off.resize(hc);
+    // Hubs are grouped into batches of at most kHubBatchSlots table slots
+    // (a single larger hub forms its own batch); every batch reuses the
+    // same table region, which therefore stays L2-resident while filled.
+    E->hub_batches.assign(1, 0u);
+    uint64_t batch_slots = 0;
     for (uint32_t i = 0; i < hc; i++) {
       const uint64_t distinct = std::min<uint64_t>(deg[i], n);
       const uint64_t T = next_pow2(2 * distinct + 1);
-      tab_off[i] = slots;
+      if (batch_slots && batch_slots + T > kHubBatchSlots) {
+        E->hub_batches.push_back((uint32_t)blk_vertex.size());
+        slots = std::max(slots, batch_slots);
+        batch_slots = 0;
+      }
+      tab_off[i] = batch_slots;
       tab_size[i] = (uint32_t)T;
-      slots += T;
+      batch_slots += T;
       list_off[i] = list_total;
       list_total += distinct;
       const uint32_t nch = (uint32_t)((deg[i] + kHubChunk - 1) / kHubChunk);
@@ -524,7 +557,11 @@ lv_status prepare_level(lv_engine* E) {
         blk_nch.push_back(nch);
       }
     }
+    E->hub_batches.push_back((uint32_t)blk_vertex.size());
+    slots = std::max(slots, batch_slots);
   }
+  E->hub.batch_blk = E->hub_batches.data();
+  E->hub.n_batches = hc ? (uint32_t)E->hub_batches.size() - 1 : 0u;
   P.hub_count = hc;
   P.hub_blocks = (uint32_t)blk_vertex.size();
   // dispatch units per class
@@ -562,12 +599,14 @@ lv_status prepare_level(lv_engine* E) {
     if (slots > E->hub_slots_cap) {
       dfree(E->hub.keys);
       dfree(E->hub.vals);
-      dfree(E->hub.list);
       CU(dalloc(&E->hub.keys, slots));
       CU(dalloc(&E->hub.vals, slots));
-      // a table holds at most half its slots, so the lists fit in slots/2
-      CU(dalloc(&E->hub.list, slots / 2 + 1));
       E->hub_slots_cap = slots;
+    }
+    if (list_total > E->hub_list_cap) {
+      dfree(E->hub.list);
+      CU(dalloc(&E->hub.list, list_total));
+      E->hub_list_cap = list_total;
     }
     std::vector<uint32_t> map(2 * hb);
     std::copy(blk_vertex.begin(), blk_vertex.end(), map.begin());
@@ -679,11 +718,13 @@ lv_status run_level_graph(lv_engine* E, float min_gain) {
     // capture counted the init kernel and one pass; lv_phase_move adds the
     // kernels of the further passes once their number is known
     (void)l0;
+    g_trace.mark("capture+instantiate", (uint32_t)E->levels.size(), E->n);
   }
   CU(cudaGraphLaunch(E->level_exec, E->st));
   CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost,
                      E->st));
   CU(cudaStreamSynchronize(E->st));
+  g_trace.mark("graph run (all passes)", (uint32_t)E->levels.size(), E->n);
   return LV_OK;
 }
 
@@ -926,7 +967,9 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
   if (E->finished) return fail(LV_ERR_STATE, "the run has ended; load a graph again");
   cudaSetDevice(E->device);
   CU(cudaEventRecord(E->ev0, E->st));
+  g_trace.reset();
   if (!E->level_ready) LVTRY(prepare_level(E));
+  g_trace.mark("prepare", (uint32_t)E->levels.size(), E->n);
   cudaEvent_t ev_prep = take_event(E);
   CU(cudaEventRecord(ev_prep, E->st));
   lv_level_info info{};
@@ -995,8 +1038,10 @@ lv_status lv_phase_aggregate(lv_engine* E) {
   const int next = (E->cur == 0) ? 1 : 0;
   ContractResult r{};
   cudaEvent_t t0 = prof_begin(E);
+  g_trace.reset();
   CU(contract_level(E->view(), E->e, E->cb, E->scan, E->c_off[next], E->c_col[next],
                     E->c_w[next], &r, E->st, grow_tables, E));
+  g_trace.mark("contract", (uint32_t)E->levels.size(), E->n);
   // B_agg = E*12 + V*(off + comm + new id + member) + E'*8 + (V'+1)*off
   prof_end(E, t0, K_CONTRACT,
            (double)E->e * 12.0 + (double)E->n * 20.0 + (double)r.new_nnz * 8.0 +

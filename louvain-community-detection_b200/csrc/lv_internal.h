@@ -164,7 +164,15 @@ struct HubArena {
   uint32_t* list = nullptr;        // occupied slots of every table
   uint64_t* list_off = nullptr;    // [hub_count] start of a hub's list
   uint32_t* list_cnt = nullptr;    // [hub_count] entries in a hub's list
+  // Host side: hubs are processed in batches whose tables fit in L2 and
+  // share one table region; batch k covers blocks [batch_blk[k],
+  // batch_blk[k+1]).  Kernels never read these two fields.
+  const uint32_t* batch_blk = nullptr;
+  uint32_t n_batches = 0;
 };
+// Table slots of one hub batch (12 bytes each: key + FP64 value), sized to
+// stay resident in the B200's 126 MB L2 next to the streamed CSR.
+constexpr uint64_t kHubBatchSlots = 4u << 20;
 // Proposals for the vertices of kernel class c (1..8; bucket 7 is classes 7
 // and 8, both launched before its apply).  proposal[] is parallel to
 // order[].

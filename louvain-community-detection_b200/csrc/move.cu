@@ -43,6 +43,8 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+// hub insert: shared table (FP64 values + keys) + list of fresh slots
+constexpr int kHubInsertSmem = kHubSmemSlots * 16;
 
 __device__ __forceinline__ unsigned long long umax64(unsigned long long a,
                                                      unsigned long long b) {
@@ -216,8 +218,47 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// 32 < deg <= 319: one warp per vertex, T-slot table per warp.
-template <int T, int RULE>
+// Candidate key from values already loaded (see candidate()).
+__device__ __forceinline__ unsigned long long candidate_loaded(const GainCtx& g,
+                                                               uint32_t c, double ec,
+                                                               uint32_t szc, double ac) {
+  if (g.szv == 1 && szc == 1 && !(c < g.cv)) return 0ull;
+  return pack_best(gain_of((float)ec, (float)ac, g), c);
+}
+
+// Best candidate among `tv` table slots, scanned by `nthr` threads starting
+// at `tid`; four slots per thread at a time so their gathers overlap.
+__device__ __forceinline__ unsigned long long scan_candidates(
+    const LevelView& L, const GainCtx& g, const uint32_t* keys, const double* vals,
+    uint32_t tv, uint32_t tid, uint32_t nthr) {
+  unsigned long long best = 0ull;
+  for (uint32_t i0 = tid; i0 < tv; i0 += 4 * nthr) {
+    uint32_t c[4], szc[4];
+    double ec[4], ac[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const uint32_t i = i0 + q * nthr;
+      c[q] = i < tv ? keys[i] : kEmptyKey;
+      ec[q] = i < tv ? vals[i] : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      if (c[q] != kEmptyKey) {
+        szc[q] = L.comm_sz[c[q]];
+        ac[q] = L.tot[c[q]];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (c[q] != kEmptyKey) best = umax64(best, candidate_loaded(g, c[q], ec[q], szc[q], ac[q]));
+  }
+  return best;
+}
+
+// 32 < deg <= 319: one warp per vertex, T-slot table per warp.  All of a
+// row's loads (at most MAXW waves of 32) are issued before any insertion,
+// so a vertex costs one memory latency chain instead of one per wave.
+template <int T, int MAXW, int RULE>
 __global__ void __launch_bounds__(kThreads)
     move_warp_kernel(LevelView L, const uint32_t* __restrict__ verts,
                      uint32_t count, uint32_t* __restrict__ prop) {
@@ -233,39 +274,49 @@ __global__ void __launch_bounds__(kThreads)
     const uint32_t d = (uint32_t)(L.off[v + 1] - s);
     const uint32_t cv = L.comm[v];
     const uint32_t tv = table_size_for(d, T);
+    uint32_t cu[MAXW];
+    float wt[MAXW];
+    unsigned self_mask = 0u;  // waves whose entry is the self-loop
+#pragma unroll
+    for (int k = 0; k < MAXW; k++) {
+      const uint32_t j = k * 32 + lane;
+      cu[k] = v;
+      wt[k] = 0.0f;
+      if (j < d) {
+        cu[k] = L.col[s + j];
+        wt[k] = L.w[s + j];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < MAXW; k++) {
+      const uint32_t j = k * 32 + lane;
+      if (cu[k] == v) self_mask |= 1u << k;
+      cu[k] = (j < d) ? L.comm[cu[k]] : kEmptyKey;
+    }
     for (uint32_t i = lane; i < tv; i += 32) {
       keys[i] = kEmptyKey;
       vals[i] = 0.0;
     }
     __syncwarp();
     double own = 0.0;
-    for (uint32_t j0 = 0; j0 < d; j0 += 32) {
-      const uint32_t j = j0 + lane;
-      const bool has = j < d;
-      uint32_t u = 0, cu = kEmptyKey;
-      float wt = 0.0f;
-      if (has) {
-        u = L.col[s + j];
-        wt = L.w[s + j];
-        cu = L.comm[u];
-      }
+#pragma unroll
+    for (int k = 0; k < MAXW; k++) {
+      if ((uint32_t)k * 32 >= d) break;  // warp-uniform
+      const bool has = (uint32_t)k * 32 + lane < d;
       const unsigned long long mk =
-          has ? (unsigned long long)cu : (0x100000000ull | (unsigned)lane);
+          has ? (unsigned long long)cu[k] : (0x100000000ull | (unsigned)lane);
       const unsigned peers = __match_any_sync(kFull, mk);
       const int leader = __ffs(peers) - 1;
       uint32_t slot = 0;
-      if (has && lane == leader) slot = table_insert(keys, tv - 1, cu, L.sc);
+      if (has && lane == leader) slot = table_insert(keys, tv - 1, cu[k], L.sc);
       slot = __shfl_sync(kFull, slot, leader);
-      if (has) atomicAdd(&vals[slot], (double)wt);
-      if (RULE == LV_RULE_CUDA_I && has && cu == cv && u != v) own += (double)wt;
+      if (has) atomicAdd(&vals[slot], (double)wt[k]);
+      if (RULE == LV_RULE_CUDA_I && has && cu[k] == cv && !(self_mask >> k & 1u))
+        own += (double)wt[k];
     }
     __syncwarp();
     const GainCtx g = make_ctx(L, v, cv);
-    unsigned long long best = 0ull;
-    for (uint32_t i = lane; i < tv; i += 32) {
-      const uint32_t c = keys[i];
-      if (c != kEmptyKey) best = umax64(best, candidate(L, g, c, vals[i]));
-    }
+    unsigned long long best = scan_candidates(L, g, keys, vals, tv, lane, 32);
     best = group_max<32>(best);
     if (RULE == LV_RULE_CUDA_I) own = group_sum<32>(own);
     if (lane == 0) prop[vidx] = decide<RULE>(best, own, g);
@@ -327,6 +378,52 @@ __device__ __forceinline__ void insert_wave(const LevelView& L, uint64_t s,
   if (RULE == LV_RULE_CUDA_I && has && cu == cv && u != v) own += (double)wt;
 }
 
+// Loads entries [lo, end) of row s (at most MAXW waves of the block) into
+// registers -- every load issued before any is used -- then inserts them
+// into a table (clear it before, synchronise after).
+template <int MAXW, int RULE>
+__device__ __forceinline__ void insert_block_range(const LevelView& L, uint64_t s,
+                                                   uint64_t lo, uint64_t end,
+                                                   uint32_t v, uint32_t cv,
+                                                   uint32_t* keys, double* vals,
+                                                   uint32_t mask, double& own) {
+  const int lane = threadIdx.x & 31;
+  uint32_t cu[MAXW];
+  float wt[MAXW];
+  unsigned self_mask = 0u;
+#pragma unroll
+  for (int k = 0; k < MAXW; k++) {
+    const uint64_t j = lo + (uint64_t)k * kThreads + threadIdx.x;
+    cu[k] = v;
+    wt[k] = 0.0f;
+    if (j < end) {
+      cu[k] = L.col[s + j];
+      wt[k] = L.w[s + j];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < MAXW; k++) {
+    const uint64_t j = lo + (uint64_t)k * kThreads + threadIdx.x;
+    if (cu[k] == v) self_mask |= 1u << k;
+    cu[k] = (j < end) ? L.comm[cu[k]] : kEmptyKey;
+  }
+#pragma unroll
+  for (int k = 0; k < MAXW; k++) {
+    if (lo + (uint64_t)k * kThreads >= end) break;  // block-uniform
+    const bool has = lo + (uint64_t)k * kThreads + threadIdx.x < end;
+    const unsigned long long mk =
+        has ? (unsigned long long)cu[k] : (0x100000000ull | (unsigned)lane);
+    const unsigned peers = __match_any_sync(kFull, mk);
+    const int leader = __ffs(peers) - 1;
+    uint32_t slot = 0;
+    if (has && lane == leader) slot = table_insert(keys, mask, cu[k], L.sc);
+    slot = __shfl_sync(kFull, slot, leader);
+    if (has) atomicAdd(&vals[slot], (double)wt[k]);
+    if (RULE == LV_RULE_CUDA_I && has && cu[k] == cv && !(self_mask >> k & 1u))
+      own += (double)wt[k];
+  }
+}
+
 // 319 < deg <= 2048: one block per vertex, shared 4096-slot table.
 template <int RULE>
 __global__ void __launch_bounds__(kThreads)
@@ -334,6 +431,7 @@ __global__ void __launch_bounds__(kThreads)
                       uint32_t count, uint32_t* __restrict__ prop) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int T = kHubSmemSlots;
+  constexpr int MAXW = (int)(kHubSmemMaxDeg / kThreads);
   double* vals = reinterpret_cast<double*>(smem_raw);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T);
   __shared__ unsigned long long red_best[kWarps];
@@ -350,15 +448,10 @@ __global__ void __launch_bounds__(kThreads)
     }
     __syncthreads();
     double own = 0.0;
-    for (uint32_t j0 = 0; j0 < d; j0 += kThreads)
-      insert_wave<RULE>(L, s, j0 + threadIdx.x, d, v, cv, keys, vals, tv - 1, own);
+    insert_block_range<MAXW, RULE>(L, s, 0, d, v, cv, keys, vals, tv - 1, own);
     __syncthreads();
     const GainCtx g = make_ctx(L, v, cv);
-    unsigned long long best = 0ull;
-    for (uint32_t i = threadIdx.x; i < tv; i += kThreads) {
-      const uint32_t c = keys[i];
-      if (c != kEmptyKey) best = umax64(best, candidate(L, g, c, vals[i]));
-    }
+    unsigned long long best = scan_candidates(L, g, keys, vals, tv, threadIdx.x, kThreads);
     best = block_max(best, red_best);
     if (RULE == LV_RULE_CUDA_I) own = block_sum(own, red_own);
     if (threadIdx.x == 0) prop[vidx] = decide<RULE>(best, own, g);
@@ -374,12 +467,14 @@ __global__ void __launch_bounds__(kThreads)
 template <int RULE>
 __global__ void __launch_bounds__(kThreads)
     hub_insert_kernel(LevelView L, const uint32_t* __restrict__ hubs,
-                      HubArena H, uint32_t hub_blocks) {
+                      HubArena H, uint32_t blk_begin, uint32_t blk_end) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* lvals = reinterpret_cast<double*>(smem_raw);
   uint32_t* lkeys = reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * kHubSmemSlots);
+  uint32_t* fresh = lkeys + kHubSmemSlots;  // slots this block inserted first
   __shared__ double red_own[kWarps];
-  for (uint32_t b = blockIdx.x; b < hub_blocks; b += gridDim.x) {
+  __shared__ uint32_t n_fresh, fresh_base;
+  for (uint32_t b = blk_begin + blockIdx.x; b < blk_end; b += gridDim.x) {
     const uint32_t hi = H.blk_vertex[b], ch = H.blk_chunk[b];
     const uint32_t v = hubs[hi];
     const uint64_t s = L.off[v];
@@ -392,35 +487,51 @@ __global__ void __launch_bounds__(kThreads)
       lkeys[i] = kEmptyKey;
       lvals[i] = 0.0;
     }
+    if (threadIdx.x == 0) n_fresh = 0u;
     __syncthreads();
     double own = 0.0;
-    for (uint64_t j0 = lo; j0 < end; j0 += kThreads)
-      insert_wave<RULE>(L, s, j0 + threadIdx.x, end, v, cv, lkeys, lvals, tl - 1, own);
+    insert_block_range<(int)(kHubChunk / kThreads), RULE>(L, s, lo, end, v, cv, lkeys, lvals,
+                                                         tl - 1, own);
     __syncthreads();
     uint32_t* keys = H.keys + H.tab_off[hi];
     double* vals = H.vals + H.tab_off[hi];
-    uint32_t* list = H.list + H.list_off[hi];
     const uint32_t mask = H.tab_size[hi] - 1;
     for (uint32_t i = threadIdx.x; i < tl; i += kThreads) {
       const uint32_t c = lkeys[i];
       if (c == kEmptyKey) continue;
       uint32_t h = hash_slot(c, mask);
+      bool placed = false;
       for (uint32_t it = 0; it <= mask; it++) {
         const uint32_t cur = keys[h];
-        if (cur == c) break;
+        if (cur == c) {
+          placed = true;
+          break;
+        }
         if (cur == kEmptyKey) {
           const uint32_t prev = atomicCAS(&keys[h], kEmptyKey, c);
           if (prev == kEmptyKey) {
-            list[atomicAdd(&H.list_cnt[hi], 1u)] = h;
+            fresh[atomicAdd(&n_fresh, 1u)] = h;
+            placed = true;
             break;
           }
-          if (prev == c) break;
+          if (prev == c) {
+            placed = true;
+            break;
+          }
         }
         h = (h + 1) & mask;
-        if (it == mask) atomicExch(&L.sc->error, 1u);
       }
-      atomicAdd(&vals[h], lvals[i]);
+      if (placed)
+        atomicAdd(&vals[h], lvals[i]);
+      else
+        atomicExch(&L.sc->error, 1u);
     }
+    __syncthreads();
+    // one list reservation per block instead of one per new community
+    if (threadIdx.x == 0) fresh_base = n_fresh ? atomicAdd(&H.list_cnt[hi], n_fresh) : 0u;
+    __syncthreads();
+    uint32_t* list = H.list + H.list_off[hi] + fresh_base;
+    for (uint32_t i = threadIdx.x; i < n_fresh; i += kThreads) list[i] = fresh[i];
     if (RULE == LV_RULE_CUDA_I) {
       own = block_sum(own, red_own);
       if (threadIdx.x == 0 && own != 0.0) atomicAdd(&H.own[hi], own);
@@ -433,9 +544,9 @@ __global__ void __launch_bounds__(kThreads)
 // table slots it read, and folds its best key into H.best.
 __global__ void __launch_bounds__(kThreads)
     hub_scan_kernel(LevelView L, const uint32_t* __restrict__ hubs, HubArena H,
-                    uint32_t hub_blocks) {
+                    uint32_t blk_begin, uint32_t blk_end) {
   __shared__ unsigned long long red_best[kWarps];
-  for (uint32_t b = blockIdx.x; b < hub_blocks; b += gridDim.x) {
+  for (uint32_t b = blk_begin + blockIdx.x; b < blk_end; b += gridDim.x) {
     const uint32_t hi = H.blk_vertex[b], ch = H.blk_chunk[b];
     const uint32_t nch = H.blk_nchunks[b];
     const uint32_t v = hubs[hi];
@@ -871,10 +982,10 @@ cudaError_t configure_kernels() {
   cudaError_t e;
   const int warp512 = kWarps * 512 * 12;
   const int block_tab = kHubSmemSlots * 12;
-  e = cudaFuncSetAttribute(move_warp_kernel<512, LV_RULE_PY_I>,
+  e = cudaFuncSetAttribute(move_warp_kernel<512, 10, LV_RULE_PY_I>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, warp512);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(move_warp_kernel<512, LV_RULE_CUDA_I>,
+  e = cudaFuncSetAttribute(move_warp_kernel<512, 10, LV_RULE_CUDA_I>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, warp512);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(move_block_kernel<LV_RULE_PY_I>,
@@ -884,10 +995,10 @@ cudaError_t configure_kernels() {
                            cudaFuncAttributeMaxDynamicSharedMemorySize, block_tab);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(hub_insert_kernel<LV_RULE_PY_I>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, block_tab);
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, kHubInsertSmem);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(hub_insert_kernel<LV_RULE_CUDA_I>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, block_tab);
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, kHubInsertSmem);
   if (e != cudaSuccess) return e;
   return configure_contract_kernels();
 }
@@ -946,14 +1057,14 @@ static cudaError_t move_bucket_impl(const LevelView& L, int bucket,
     case 5:
       if (cnt) {
         constexpr int T = 128;
-        (count_launches(1), move_warp_kernel<T, RULE><<<grid_for((cnt + 7) / 8, cap), kThreads,
+        (count_launches(1), move_warp_kernel<T, 3, RULE><<<grid_for((cnt + 7) / 8, cap), kThreads,
                                     kWarps * T * 12, st>>>(L, verts, cnt, pr));
       }
       break;
     case 6:
       if (cnt) {
         constexpr int T = 512;
-        (count_launches(1), move_warp_kernel<T, RULE><<<grid_for((cnt + 7) / 8, sm_count() * 4), kThreads,
+        (count_launches(1), move_warp_kernel<T, 10, RULE><<<grid_for((cnt + 7) / 8, sm_count() * 4), kThreads,
                                     kWarps * T * 12, st>>>(L, verts, cnt, pr));
       }
       break;
@@ -967,11 +1078,15 @@ static cudaError_t move_bucket_impl(const LevelView& L, int bucket,
       const uint32_t hs = P.cls_start[8];
       const uint32_t hc = P.cls_start[9] - hs;
       if (hc) {
-        (count_launches(1), hub_insert_kernel<RULE><<<grid_for(P.hub_blocks, sm_count() * 4),
-                                                     kThreads, kHubSmemSlots * 12, st>>>(
-            L, order + hs, H, P.hub_blocks));
-        (count_launches(1), hub_scan_kernel<<<grid_for(P.hub_blocks, cap), kThreads, 0, st>>>(
-            L, order + hs, H, P.hub_blocks));
+        // batch by batch, so the tables being filled stay in L2
+        for (uint32_t k = 0; k < H.n_batches; k++) {
+          const uint32_t b0 = H.batch_blk[k], b1 = H.batch_blk[k + 1];
+          (count_launches(1), hub_insert_kernel<RULE><<<grid_for(b1 - b0, sm_count() * 3),
+                                                       kThreads, kHubInsertSmem, st>>>(
+              L, order + hs, H, b0, b1));
+          (count_launches(1), hub_scan_kernel<<<grid_for(b1 - b0, cap), kThreads, 0, st>>>(
+              L, order + hs, H, b0, b1));
+        }
         (count_launches(1), hub_decide_kernel<RULE><<<(hc + 127) / 128, 128, 0, st>>>(
             L, order + hs, H, hc, prop + hs));
       }
