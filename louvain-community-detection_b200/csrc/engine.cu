@@ -63,12 +63,6 @@ void dfree(T*& p) {
   p = nullptr;
 }
 
-uint64_t next_pow2(uint64_t x) {
-  uint64_t p = 1;
-  while (p < x) p <<= 1;
-  return p;
-}
-
 __global__ void gather_degrees_kernel(const uint64_t* off, const uint32_t* ids,
                                       uint32_t n, uint64_t* out) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -192,9 +186,8 @@ struct lv_engine {
   uint32_t* hub_map = nullptr;  // [blk_vertex | blk_chunk] for dispatch
   size_t hub_map_cap = 0;
   HubArena hub;
-  size_t hub_slots_cap = 0, hub_count_cap = 0, hub_blocks_cap = 0, hub_list_cap = 0;
+  size_t hub_count_cap = 0, hub_blocks_cap = 0, hub_units_cap = 0;
   uint64_t* hub_deg = nullptr;
-  std::vector<uint32_t> hub_batches;  // block boundaries of the hub batches
 
   ContractBuffers cb{};
   ScanScratch scan;
@@ -350,18 +343,11 @@ void free_state(lv_engine* E) {
   dfree(E->part_tmp);
   dfree(E->partials);
   dfree(E->hub_map);
-  dfree(E->hub.keys);
-  dfree(E->hub.vals);
-  dfree(E->hub.tab_off);
-  dfree(E->hub.tab_size);
   dfree(E->hub.best);
   dfree(E->hub.own);
   dfree(E->hub.blk_vertex);
   dfree(E->hub.blk_chunk);
   dfree(E->hub.blk_nchunks);
-  dfree(E->hub.list);
-  dfree(E->hub.list_off);
-  dfree(E->hub.list_cnt);
   dfree(E->hub_deg);
   ContractBuffers& B = E->cb;
   dfree(B.flag_id);
@@ -391,7 +377,7 @@ void free_state(lv_engine* E) {
   E->scan.buf = nullptr;
   E->scan.bytes = 0;
   E->partials_cap = E->hub_map_cap = 0;
-  E->hub_slots_cap = E->hub_count_cap = E->hub_blocks_cap = E->hub_list_cap = 0;
+  E->hub_count_cap = E->hub_blocks_cap = E->hub_units_cap = 0;
   E->cap_n = 0;
   E->cap_e = 0;
   E->in_off = nullptr;
@@ -499,71 +485,45 @@ lv_status prepare_level(lv_engine* E) {
   for (int c = 0; c < kClasses; c++) P.cls_start[c + 1] = P.cls_start[c] + E->h_counts[c];
   const uint32_t hs = P.cls_start[8];
   const uint32_t hc = P.cls_start[9] - hs;
-  // hub plan
-  std::vector<uint32_t> blk_vertex, blk_chunk, blk_nch;
-  std::vector<uint64_t> tab_off, list_off;
-  std::vector<uint32_t> tab_size;
-  uint64_t slots = 0, list_total = 0;
+  // hub plan: dispatch chunks (row sums, modularity) of kHubChunk entries,
+  // and move units (hub, hash partition of about kHubPartKeys communities)
+  std::vector<uint32_t> blk_vertex, blk_chunk;            // dispatch chunks
+  std::vector<uint32_t> unit_vertex, unit_part, unit_np;  // move units
   if (hc) {
     if (hc > E->hub_count_cap) {
       dfree(E->hub_deg);
-      dfree(E->hub.tab_off);
-      dfree(E->hub.tab_size);
       dfree(E->hub.best);
       dfree(E->hub.own);
-      dfree(E->hub.list_off);
-      dfree(E->hub.list_cnt);
       CU(dalloc(&E->hub_deg, hc));
-      CU(dalloc(&E->hub.tab_off, hc));
-      CU(dalloc(&E->hub.tab_size, hc));
       CU(dalloc(&E->hub.best, hc));
       CU(dalloc(&E->hub.own, hc));
-      CU(dalloc(&E->hub.list_off, hc));
-      CU(dalloc(&E->hub.list_cnt, hc));
       E->hub_count_cap = hc;
     }
-    (count_launches(1), gather_degrees_kernel<<<(hc + 255) / 256, 256, 0, st>>>(E->off(), E->order + hs,
-                                                            hc, E->hub_deg));
+    (count_launches(1), gather_degrees_kernel<<<(hc + 255) / 256, 256, 0, st>>>(
+        E->off(), E->order + hs, hc, E->hub_deg));
     CU(cudaGetLastError());
     std::vector<uint64_t> deg(hc);
     CU(cudaMemcpyAsync(deg.data(), E->hub_deg, hc * sizeof(uint64_t),
                        cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
-    tab_off.resize(hc);
-    tab_size.resize(hc);
-    list_off.resize(hc);
-    // Hubs are grouped into batches of at most kHubBatchSlots table slots
-    // (a single larger hub forms its own batch); every batch reuses the
-    // same table region, which therefore stays L2-resident while filled.
-    E->hub_batches.assign(1, 0u);
-    uint64_t batch_slots = 0;
     for (uint32_t i = 0; i < hc; i++) {
-      const uint64_t distinct = std::min<uint64_t>(deg[i], n);
-      const uint64_t T = next_pow2(2 * distinct + 1);
-      if (batch_slots && batch_slots + T > kHubBatchSlots) {
-        E->hub_batches.push_back((uint32_t)blk_vertex.size());
-        slots = std::max(slots, batch_slots);
-        batch_slots = 0;
-      }
-      tab_off[i] = batch_slots;
-      tab_size[i] = (uint32_t)T;
-      batch_slots += T;
-      list_off[i] = list_total;
-      list_total += distinct;
       const uint32_t nch = (uint32_t)((deg[i] + kHubChunk - 1) / kHubChunk);
       for (uint32_t ch = 0; ch < nch; ch++) {
         blk_vertex.push_back(i);
         blk_chunk.push_back(ch);
-        blk_nch.push_back(nch);
+      }
+      const uint64_t distinct = std::min<uint64_t>(deg[i], n);
+      const uint32_t np = (uint32_t)std::max<uint64_t>(1, (distinct + kHubPartKeys - 1) / kHubPartKeys);
+      for (uint32_t p = 0; p < np; p++) {  // a hub's partitions are adjacent
+        unit_vertex.push_back(i);
+        unit_part.push_back(p);
+        unit_np.push_back(np);
       }
     }
-    E->hub_batches.push_back((uint32_t)blk_vertex.size());
-    slots = std::max(slots, batch_slots);
   }
-  E->hub.batch_blk = E->hub_batches.data();
-  E->hub.n_batches = hc ? (uint32_t)E->hub_batches.size() - 1 : 0u;
   P.hub_count = hc;
   P.hub_blocks = (uint32_t)blk_vertex.size();
+  E->hub.units = (uint32_t)unit_vertex.size();
   // dispatch units per class
   const uint32_t per_unit[kClasses] = {0, 64, 32, 16, 8, 8, 8, 1, 0};
   uint32_t u = 0;
@@ -585,51 +545,34 @@ lv_status prepare_level(lv_engine* E) {
   }
   if (hc) {
     const size_t hb = P.hub_blocks;
+    const size_t hu = E->hub.units;
     if (hb > E->hub_blocks_cap) {
       dfree(E->hub_map);
+      CU(dalloc(&E->hub_map, 2 * hb));
+      E->hub_blocks_cap = hb;
+    }
+    if (hu > E->hub_units_cap) {
       dfree(E->hub.blk_vertex);
       dfree(E->hub.blk_chunk);
       dfree(E->hub.blk_nchunks);
-      CU(dalloc(&E->hub_map, 2 * hb));
-      CU(dalloc(&E->hub.blk_vertex, hb));
-      CU(dalloc(&E->hub.blk_chunk, hb));
-      CU(dalloc(&E->hub.blk_nchunks, hb));
-      E->hub_blocks_cap = hb;
-    }
-    if (slots > E->hub_slots_cap) {
-      dfree(E->hub.keys);
-      dfree(E->hub.vals);
-      CU(dalloc(&E->hub.keys, slots));
-      CU(dalloc(&E->hub.vals, slots));
-      E->hub_slots_cap = slots;
-    }
-    if (list_total > E->hub_list_cap) {
-      dfree(E->hub.list);
-      CU(dalloc(&E->hub.list, list_total));
-      E->hub_list_cap = list_total;
+      CU(dalloc(&E->hub.blk_vertex, hu));
+      CU(dalloc(&E->hub.blk_chunk, hu));
+      CU(dalloc(&E->hub.blk_nchunks, hu));
+      E->hub_units_cap = hu;
     }
     std::vector<uint32_t> map(2 * hb);
     std::copy(blk_vertex.begin(), blk_vertex.end(), map.begin());
     std::copy(blk_chunk.begin(), blk_chunk.end(), map.begin() + hb);
     CU(cudaMemcpyAsync(E->hub_map, map.data(), 2 * hb * sizeof(uint32_t),
                        cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(E->hub.blk_vertex, blk_vertex.data(), hb * sizeof(uint32_t),
+    CU(cudaMemcpyAsync(E->hub.blk_vertex, unit_vertex.data(), hu * sizeof(uint32_t),
                        cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(E->hub.blk_chunk, blk_chunk.data(), hb * sizeof(uint32_t),
+    CU(cudaMemcpyAsync(E->hub.blk_chunk, unit_part.data(), hu * sizeof(uint32_t),
                        cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(E->hub.blk_nchunks, blk_nch.data(), hb * sizeof(uint32_t),
+    CU(cudaMemcpyAsync(E->hub.blk_nchunks, unit_np.data(), hu * sizeof(uint32_t),
                        cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(E->hub.tab_off, tab_off.data(), hc * sizeof(uint64_t),
-                       cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(E->hub.tab_size, tab_size.data(), hc * sizeof(uint32_t),
-                       cudaMemcpyHostToDevice, st));
-    CU(cudaMemsetAsync(E->hub.keys, 0xFF, slots * sizeof(uint32_t), st));
-    CU(cudaMemsetAsync(E->hub.vals, 0, slots * sizeof(double), st));
     CU(cudaMemsetAsync(E->hub.best, 0, hc * sizeof(unsigned long long), st));
     CU(cudaMemsetAsync(E->hub.own, 0, hc * sizeof(double), st));
-    CU(cudaMemsetAsync(E->hub.list_cnt, 0, hc * sizeof(uint32_t), st));
-    CU(cudaMemcpyAsync(E->hub.list_off, list_off.data(), hc * sizeof(uint64_t),
-                       cudaMemcpyHostToDevice, st));
     CU(cudaMemsetAsync(E->partials, 0, hc * sizeof(double), st));
   }
   // entries per move class (byte counts of the kernel timings)

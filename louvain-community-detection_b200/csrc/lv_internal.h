@@ -149,30 +149,21 @@ cudaError_t launch_modularity(const LevelView& L, const uint32_t* order,
                               const PassControl* ctl = nullptr);
 // passes = 0, first_fail = 0, q_prev = q (start of a level's pass loop)
 cudaError_t launch_pass_control_init(LevelScalars* sc, cudaStream_t st);
-// Hub (class 8) arenas: per hub vertex a table of tab_size[i] slots at
-// tab_off[i] (FP64 values, u32 keys), a best key and an own-weight sum.
+// Hubs (class 8): work units are (hub, hash partition of its neighbour
+// communities); per hub a best packed (gain, ~community) key and an
+// own-community weight sum.
 struct HubArena {
-  uint32_t* keys = nullptr;
-  double* vals = nullptr;
-  uint64_t* tab_off = nullptr;     // [hub_count]
-  uint32_t* tab_size = nullptr;    // [hub_count] power of two
   unsigned long long* best = nullptr;  // [hub_count]
   double* own = nullptr;           // [hub_count]
-  uint32_t* blk_vertex = nullptr;  // [hub_blocks] hub index of each block
-  uint32_t* blk_chunk = nullptr;   // [hub_blocks] chunk within the vertex
-  uint32_t* blk_nchunks = nullptr; // [hub_blocks] chunks of that vertex
-  uint32_t* list = nullptr;        // occupied slots of every table
-  uint64_t* list_off = nullptr;    // [hub_count] start of a hub's list
-  uint32_t* list_cnt = nullptr;    // [hub_count] entries in a hub's list
-  // Host side: hubs are processed in batches whose tables fit in L2 and
-  // share one table region; batch k covers blocks [batch_blk[k],
-  // batch_blk[k+1]).  Kernels never read these two fields.
-  const uint32_t* batch_blk = nullptr;
-  uint32_t n_batches = 0;
+  uint32_t* blk_vertex = nullptr;  // [units] hub index of each unit
+  uint32_t* blk_chunk = nullptr;   // [units] partition of the unit
+  uint32_t* blk_nchunks = nullptr; // [units] partitions of that hub
+  uint32_t units = 0;
 };
-// Table slots of one hub batch (12 bytes each: key + FP64 value), sized to
-// stay resident in the B200's 126 MB L2 next to the streamed CSR.
-constexpr uint64_t kHubBatchSlots = 4u << 20;
+// Shared table of a hub unit (8192 slots, about kHubPartKeys communities
+// per partition, load factor ~1/2).
+constexpr int kHubPartSlots = 8192;
+constexpr uint32_t kHubPartKeys = 4096;
 // Proposals for the vertices of kernel class c (1..8; bucket 7 is classes 7
 // and 8, both launched before its apply).  proposal[] is parallel to
 // order[].

@@ -29,8 +29,11 @@
 //     __match_any_sync groups equal communities, no hash table at all.
 //     32 < deg <= 319: one warp per vertex, open-addressing table in shared
 //     memory.  319 < deg <= 2048: one block per vertex, 4096-slot shared
-//     table.  deg > 2048: several blocks per vertex on a global-memory table
-//     sized from the vertex's own degree.
+//     table.  deg > 2048: one block per (vertex, hash partition of its
+//     neighbour communities), 8192-slot shared table, the partitions' best
+//     candidates merged with one 64-bit atomicMax each -- no global hash
+//     table, whatever the degree.  Shared tables are self-cleaning: taken
+//     slots are listed, and only they are scanned and cleared.
 //   * Community totals are updated incrementally by the moved vertices
 //     only (FP64 atomics), instead of a full recount after every bucket.
 #include "lv_internal.h"
@@ -43,8 +46,10 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-// hub insert: shared table (FP64 values + keys) + list of fresh slots
-constexpr int kHubInsertSmem = kHubSmemSlots * 16;
+// shared tables: FP64 values + u32 keys + u16 list of taken slots
+constexpr int kSlotBytes = 14;
+constexpr int kHubPartSmem = kHubPartSlots * kSlotBytes;
+constexpr int kBlockTabSmem = kHubSmemSlots * kSlotBytes;
 
 __device__ __forceinline__ unsigned long long umax64(unsigned long long a,
                                                      unsigned long long b) {
@@ -131,29 +136,12 @@ __device__ __forceinline__ double group_sum(double x) {
   return x;
 }
 
-// Open addressing with linear probing; multiplicative hash.  The probe
-// count is bounded by the table size; a full table (impossible when the
-// table holds more slots than the row has entries) sets the error flag.
+// Open addressing with linear probing; multiplicative hash.  Probe counts
+// are bounded by the table size; a full table (impossible while a table
+// holds more slots than the row has entries) sets the error flag.
 __device__ __forceinline__ uint32_t hash_slot(uint32_t key, uint32_t mask) {
   return (key * 2654435761u) & mask;
 }
-__device__ __forceinline__ uint32_t table_insert(uint32_t* keys, uint32_t mask,
-                                                 uint32_t key,
-                                                 LevelScalars* sc) {
-  uint32_t h = hash_slot(key, mask);
-  for (uint32_t it = 0; it <= mask; it++) {
-    uint32_t cur = keys[h];
-    if (cur == key) return h;
-    if (cur == kEmptyKey) {
-      uint32_t prev = atomicCAS(&keys[h], kEmptyKey, key);
-      if (prev == kEmptyKey || prev == key) return h;
-    }
-    h = (h + 1) & mask;
-  }
-  atomicExch(&sc->error, 1u);
-  return 0;
-}
-
 // Table slots used for a row of d entries: a power of two >= 1.5 d (load
 // factor <= 2/3), at most tmax (the class's shared-memory table).
 __device__ __forceinline__ uint32_t table_size_for(uint32_t d, uint32_t tmax) {
@@ -161,6 +149,32 @@ __device__ __forceinline__ uint32_t table_size_for(uint32_t d, uint32_t tmax) {
   uint32_t t = 32;
   while (t < want) t <<= 1;
   return t < tmax ? t : tmax;
+}
+
+// Self-cleaning shared tables: a slot taken for the first time is appended
+// to `fresh`, so the candidates are read from the list (O(distinct), not
+// O(table)) and only listed slots are cleared afterwards.  The table is
+// cleared in full once, when a warp or block starts.
+__device__ __forceinline__ uint32_t table_insert_fresh(uint32_t* keys, uint32_t mask,
+                                                       uint32_t key, uint16_t* fresh,
+                                                       uint32_t* n_fresh,
+                                                       LevelScalars* sc) {
+  uint32_t h = hash_slot(key, mask);
+  for (uint32_t it = 0; it <= mask; it++) {
+    uint32_t cur = keys[h];
+    if (cur == key) return h;
+    if (cur == kEmptyKey) {
+      uint32_t prev = atomicCAS(&keys[h], kEmptyKey, key);
+      if (prev == kEmptyKey) {
+        fresh[atomicAdd(n_fresh, 1u)] = (uint16_t)h;
+        return h;
+      }
+      if (prev == key) return h;
+    }
+    h = (h + 1) & mask;
+  }
+  atomicExch(&sc->error, 1u);
+  return 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -226,20 +240,22 @@ __device__ __forceinline__ unsigned long long candidate_loaded(const GainCtx& g,
   return pack_best(gain_of((float)ec, (float)ac, g), c);
 }
 
-// Best candidate among `tv` table slots, scanned by `nthr` threads starting
-// at `tid`; four slots per thread at a time so their gathers overlap.
-__device__ __forceinline__ unsigned long long scan_candidates(
-    const LevelView& L, const GainCtx& g, const uint32_t* keys, const double* vals,
-    uint32_t tv, uint32_t tid, uint32_t nthr) {
+// Best candidate among the listed slots (nthr threads from tid, four per
+// thread at a time so the gathers overlap); each thread then clears the
+// slots it read, leaving the table clean.
+__device__ __forceinline__ unsigned long long scan_fresh_and_clear(
+    const LevelView& L, const GainCtx& g, uint32_t* keys, double* vals,
+    const uint16_t* fresh, uint32_t cnt, uint32_t tid, uint32_t nthr) {
   unsigned long long best = 0ull;
-  for (uint32_t i0 = tid; i0 < tv; i0 += 4 * nthr) {
-    uint32_t c[4], szc[4];
+  for (uint32_t i0 = tid; i0 < cnt; i0 += 4 * nthr) {
+    uint32_t sl[4], c[4], szc[4];
     double ec[4], ac[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const uint32_t i = i0 + q * nthr;
-      c[q] = i < tv ? keys[i] : kEmptyKey;
-      ec[q] = i < tv ? vals[i] : 0.0;
+      sl[q] = i < cnt ? fresh[i] : 0u;
+      c[q] = i < cnt ? keys[sl[q]] : kEmptyKey;
+      ec[q] = i < cnt ? vals[sl[q]] : 0.0;
     }
 #pragma unroll
     for (int q = 0; q < 4; q++) {
@@ -249,8 +265,13 @@ __device__ __forceinline__ unsigned long long scan_candidates(
       }
     }
 #pragma unroll
-    for (int q = 0; q < 4; q++)
-      if (c[q] != kEmptyKey) best = umax64(best, candidate_loaded(g, c[q], ec[q], szc[q], ac[q]));
+    for (int q = 0; q < 4; q++) {
+      if (c[q] != kEmptyKey) {
+        best = umax64(best, candidate_loaded(g, c[q], ec[q], szc[q], ac[q]));
+        keys[sl[q]] = kEmptyKey;
+        vals[sl[q]] = 0.0;
+      }
+    }
   }
   return best;
 }
@@ -263,10 +284,20 @@ __global__ void __launch_bounds__(kThreads)
     move_warp_kernel(LevelView L, const uint32_t* __restrict__ verts,
                      uint32_t count, uint32_t* __restrict__ prop) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint32_t n_fresh_sm[kWarps];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   double* vals = reinterpret_cast<double*>(smem_raw) + wib * T;
   uint32_t* keys =
       reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T * kWarps) + wib * T;
+  uint16_t* fresh =
+      reinterpret_cast<uint16_t*>(smem_raw + 12 * T * kWarps) + wib * T;
+  uint32_t* n_fresh = &n_fresh_sm[wib];
+  for (uint32_t i = lane; i < T; i += 32) {
+    keys[i] = kEmptyKey;
+    vals[i] = 0.0;
+  }
+  if (lane == 0) *n_fresh = 0u;
+  __syncwarp();
   for (uint32_t vidx = blockIdx.x * kWarps + wib; vidx < count;
        vidx += gridDim.x * kWarps) {
     const uint32_t v = verts[vidx];
@@ -293,11 +324,6 @@ __global__ void __launch_bounds__(kThreads)
       if (cu[k] == v) self_mask |= 1u << k;
       cu[k] = (j < d) ? L.comm[cu[k]] : kEmptyKey;
     }
-    for (uint32_t i = lane; i < tv; i += 32) {
-      keys[i] = kEmptyKey;
-      vals[i] = 0.0;
-    }
-    __syncwarp();
     double own = 0.0;
 #pragma unroll
     for (int k = 0; k < MAXW; k++) {
@@ -308,7 +334,8 @@ __global__ void __launch_bounds__(kThreads)
       const unsigned peers = __match_any_sync(kFull, mk);
       const int leader = __ffs(peers) - 1;
       uint32_t slot = 0;
-      if (has && lane == leader) slot = table_insert(keys, tv - 1, cu[k], L.sc);
+      if (has && lane == leader)
+        slot = table_insert_fresh(keys, tv - 1, cu[k], fresh, n_fresh, L.sc);
       slot = __shfl_sync(kFull, slot, leader);
       if (has) atomicAdd(&vals[slot], (double)wt[k]);
       if (RULE == LV_RULE_CUDA_I && has && cu[k] == cv && !(self_mask >> k & 1u))
@@ -316,10 +343,14 @@ __global__ void __launch_bounds__(kThreads)
     }
     __syncwarp();
     const GainCtx g = make_ctx(L, v, cv);
-    unsigned long long best = scan_candidates(L, g, keys, vals, tv, lane, 32);
+    unsigned long long best =
+        scan_fresh_and_clear(L, g, keys, vals, fresh, *n_fresh, lane, 32);
     best = group_max<32>(best);
     if (RULE == LV_RULE_CUDA_I) own = group_sum<32>(own);
-    if (lane == 0) prop[vidx] = decide<RULE>(best, own, g);
+    if (lane == 0) {
+      prop[vidx] = decide<RULE>(best, own, g);
+      *n_fresh = 0u;
+    }
     __syncwarp();
   }
 }
@@ -351,33 +382,6 @@ __device__ __forceinline__ double block_sum(double x, double* red) {
   return r;  // valid in thread 0
 }
 
-// Inserts one wave of a block's edges [j0, j0 + kThreads) into a table.
-template <int RULE>
-__device__ __forceinline__ void insert_wave(const LevelView& L, uint64_t s,
-                                            uint64_t j, uint64_t end,
-                                            uint32_t v, uint32_t cv,
-                                            uint32_t* keys, double* vals,
-                                            uint32_t mask, double& own) {
-  const int lane = threadIdx.x & 31;
-  const bool has = j < end;
-  uint32_t u = 0, cu = kEmptyKey;
-  float wt = 0.0f;
-  if (has) {
-    u = L.col[s + j];
-    wt = L.w[s + j];
-    cu = L.comm[u];
-  }
-  const unsigned long long mk =
-      has ? (unsigned long long)cu : (0x100000000ull | (unsigned)lane);
-  const unsigned peers = __match_any_sync(kFull, mk);
-  const int leader = __ffs(peers) - 1;
-  uint32_t slot = 0;
-  if (has && lane == leader) slot = table_insert(keys, mask, cu, L.sc);
-  slot = __shfl_sync(kFull, slot, leader);
-  if (has) atomicAdd(&vals[slot], (double)wt);
-  if (RULE == LV_RULE_CUDA_I && has && cu == cv && u != v) own += (double)wt;
-}
-
 // Loads entries [lo, end) of row s (at most MAXW waves of the block) into
 // registers -- every load issued before any is used -- then inserts them
 // into a table (clear it before, synchronise after).
@@ -386,7 +390,8 @@ __device__ __forceinline__ void insert_block_range(const LevelView& L, uint64_t 
                                                    uint64_t lo, uint64_t end,
                                                    uint32_t v, uint32_t cv,
                                                    uint32_t* keys, double* vals,
-                                                   uint32_t mask, double& own) {
+                                                   uint32_t mask, double& own,
+                                                   uint16_t* fresh, uint32_t* n_fresh) {
   const int lane = threadIdx.x & 31;
   uint32_t cu[MAXW];
   float wt[MAXW];
@@ -416,7 +421,8 @@ __device__ __forceinline__ void insert_block_range(const LevelView& L, uint64_t 
     const unsigned peers = __match_any_sync(kFull, mk);
     const int leader = __ffs(peers) - 1;
     uint32_t slot = 0;
-    if (has && lane == leader) slot = table_insert(keys, mask, cu[k], L.sc);
+    if (has && lane == leader)
+      slot = table_insert_fresh(keys, mask, cu[k], fresh, n_fresh, L.sc);
     slot = __shfl_sync(kFull, slot, leader);
     if (has) atomicAdd(&vals[slot], (double)wt[k]);
     if (RULE == LV_RULE_CUDA_I && has && cu[k] == cv && !(self_mask >> k & 1u))
@@ -434,139 +440,128 @@ __global__ void __launch_bounds__(kThreads)
   constexpr int MAXW = (int)(kHubSmemMaxDeg / kThreads);
   double* vals = reinterpret_cast<double*>(smem_raw);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T);
+  uint16_t* fresh = reinterpret_cast<uint16_t*>(smem_raw + 12 * T);
   __shared__ unsigned long long red_best[kWarps];
   __shared__ double red_own[kWarps];
+  __shared__ uint32_t n_fresh;
+  for (uint32_t i = threadIdx.x; i < T; i += kThreads) {
+    keys[i] = kEmptyKey;
+    vals[i] = 0.0;
+  }
+  if (threadIdx.x == 0) n_fresh = 0u;
+  __syncthreads();
   for (uint32_t vidx = blockIdx.x; vidx < count; vidx += gridDim.x) {
     const uint32_t v = verts[vidx];
     const uint64_t s = L.off[v];
     const uint32_t d = (uint32_t)(L.off[v + 1] - s);
     const uint32_t cv = L.comm[v];
     const uint32_t tv = table_size_for(d, T);
-    for (uint32_t i = threadIdx.x; i < tv; i += kThreads) {
-      keys[i] = kEmptyKey;
-      vals[i] = 0.0;
-    }
-    __syncthreads();
     double own = 0.0;
-    insert_block_range<MAXW, RULE>(L, s, 0, d, v, cv, keys, vals, tv - 1, own);
+    insert_block_range<MAXW, RULE>(L, s, 0, d, v, cv, keys, vals, tv - 1, own,
+                                   fresh, &n_fresh);
     __syncthreads();
     const GainCtx g = make_ctx(L, v, cv);
-    unsigned long long best = scan_candidates(L, g, keys, vals, tv, threadIdx.x, kThreads);
+    unsigned long long best =
+        scan_fresh_and_clear(L, g, keys, vals, fresh, n_fresh, threadIdx.x, kThreads);
     best = block_max(best, red_best);
     if (RULE == LV_RULE_CUDA_I) own = block_sum(own, red_own);
-    if (threadIdx.x == 0) prop[vidx] = decide<RULE>(best, own, g);
+    if (threadIdx.x == 0) {
+      prop[vidx] = decide<RULE>(best, own, g);
+      n_fresh = 0u;  // every thread read it before block_max's barriers
+    }
     __syncthreads();
   }
 }
 
-// deg > 2048: the vertex's edges are split in chunks of kHubChunk, one
-// block per chunk.  A block first sums its chunk per neighbour community in
-// a shared table, then adds one total per distinct community to the
-// vertex's global table; a community seen for the first time is appended
-// to the vertex's list, so the scan below walks only the distinct entries.
+// deg > 2048 (hubs): the neighbour communities of a hub are split into P
+// hash partitions (P from the hub's degree, about kHubPartKeys distinct
+// communities each).  One block per (hub, partition) streams the whole row
+// -- the other partitions' blocks of the same hub run alongside, so the
+// re-reads come from L2 -- and sums only its partition's communities in a
+// self-cleaning shared table.  Its best candidate is folded into the hub's
+// packed (gain, ~community) key with one atomicMax; no global hash table,
+// no per-entry global atomics.
+__device__ __forceinline__ uint32_t hub_part_of(uint32_t c, uint32_t nparts) {
+  return __umulhi(c * 0x85EBCA6Bu, nparts);
+}
+
 template <int RULE>
 __global__ void __launch_bounds__(kThreads)
-    hub_insert_kernel(LevelView L, const uint32_t* __restrict__ hubs,
-                      HubArena H, uint32_t blk_begin, uint32_t blk_end) {
+    hub_part_kernel(LevelView L, const uint32_t* __restrict__ hubs, HubArena H,
+                    uint32_t units) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* lvals = reinterpret_cast<double*>(smem_raw);
-  uint32_t* lkeys = reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * kHubSmemSlots);
-  uint32_t* fresh = lkeys + kHubSmemSlots;  // slots this block inserted first
+  constexpr int T = kHubPartSlots;
+  constexpr int PF = 4;  // waves prefetched per iteration
+  double* vals = reinterpret_cast<double*>(smem_raw);
+  uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T);
+  uint16_t* fresh = reinterpret_cast<uint16_t*>(smem_raw + 12 * T);
+  __shared__ unsigned long long red_best[kWarps];
   __shared__ double red_own[kWarps];
-  __shared__ uint32_t n_fresh, fresh_base;
-  for (uint32_t b = blk_begin + blockIdx.x; b < blk_end; b += gridDim.x) {
-    const uint32_t hi = H.blk_vertex[b], ch = H.blk_chunk[b];
+  __shared__ uint32_t n_fresh;
+  const int lane = threadIdx.x & 31;
+  for (uint32_t i = threadIdx.x; i < T; i += kThreads) {
+    keys[i] = kEmptyKey;
+    vals[i] = 0.0;
+  }
+  if (threadIdx.x == 0) n_fresh = 0u;
+  __syncthreads();
+  for (uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
+    const uint32_t hi = H.blk_vertex[u], part = H.blk_chunk[u];
+    const uint32_t nparts = H.blk_nchunks[u];
     const uint32_t v = hubs[hi];
     const uint64_t s = L.off[v];
     const uint64_t d = L.off[v + 1] - s;
     const uint32_t cv = L.comm[v];
-    const uint64_t lo = (uint64_t)ch * kHubChunk;
-    const uint64_t end = min(d, lo + kHubChunk);
-    const uint32_t tl = table_size_for((uint32_t)(end - lo), kHubSmemSlots);
-    for (uint32_t i = threadIdx.x; i < tl; i += kThreads) {
-      lkeys[i] = kEmptyKey;
-      lvals[i] = 0.0;
-    }
-    if (threadIdx.x == 0) n_fresh = 0u;
-    __syncthreads();
     double own = 0.0;
-    insert_block_range<(int)(kHubChunk / kThreads), RULE>(L, s, lo, end, v, cv, lkeys, lvals,
-                                                         tl - 1, own);
-    __syncthreads();
-    uint32_t* keys = H.keys + H.tab_off[hi];
-    double* vals = H.vals + H.tab_off[hi];
-    const uint32_t mask = H.tab_size[hi] - 1;
-    for (uint32_t i = threadIdx.x; i < tl; i += kThreads) {
-      const uint32_t c = lkeys[i];
-      if (c == kEmptyKey) continue;
-      uint32_t h = hash_slot(c, mask);
-      bool placed = false;
-      for (uint32_t it = 0; it <= mask; it++) {
-        const uint32_t cur = keys[h];
-        if (cur == c) {
-          placed = true;
-          break;
+    for (uint64_t j0 = 0; j0 < d; j0 += (uint64_t)PF * kThreads) {
+      uint32_t cu[PF];
+      float wt[PF];
+      unsigned self_mask = 0u;
+#pragma unroll
+      for (int k = 0; k < PF; k++) {
+        const uint64_t j = j0 + (uint64_t)k * kThreads + threadIdx.x;
+        cu[k] = v;
+        wt[k] = 0.0f;
+        if (j < d) {
+          cu[k] = L.col[s + j];
+          wt[k] = L.w[s + j];
         }
-        if (cur == kEmptyKey) {
-          const uint32_t prev = atomicCAS(&keys[h], kEmptyKey, c);
-          if (prev == kEmptyKey) {
-            fresh[atomicAdd(&n_fresh, 1u)] = h;
-            placed = true;
-            break;
-          }
-          if (prev == c) {
-            placed = true;
-            break;
-          }
-        }
-        h = (h + 1) & mask;
       }
-      if (placed)
-        atomicAdd(&vals[h], lvals[i]);
-      else
-        atomicExch(&L.sc->error, 1u);
+#pragma unroll
+      for (int k = 0; k < PF; k++) {
+        const uint64_t j = j0 + (uint64_t)k * kThreads + threadIdx.x;
+        if (cu[k] == v) self_mask |= 1u << k;
+        cu[k] = (j < d) ? L.comm[cu[k]] : kEmptyKey;
+      }
+#pragma unroll
+      for (int k = 0; k < PF; k++) {
+        if (j0 + (uint64_t)k * kThreads >= d) break;  // block-uniform
+        const bool has = cu[k] != kEmptyKey && hub_part_of(cu[k], nparts) == part;
+        const unsigned long long mk =
+            has ? (unsigned long long)cu[k] : (0x100000000ull | (unsigned)lane);
+        const unsigned peers = __match_any_sync(kFull, mk);
+        const int leader = __ffs(peers) - 1;
+        uint32_t slot = 0;
+        if (has && lane == leader)
+          slot = table_insert_fresh(keys, T - 1, cu[k], fresh, &n_fresh, L.sc);
+        slot = __shfl_sync(kFull, slot, leader);
+        if (has) atomicAdd(&vals[slot], (double)wt[k]);
+        if (RULE == LV_RULE_CUDA_I && has && cu[k] == cv && !(self_mask >> k & 1u))
+          own += (double)wt[k];
+      }
     }
     __syncthreads();
-    // one list reservation per block instead of one per new community
-    if (threadIdx.x == 0) fresh_base = n_fresh ? atomicAdd(&H.list_cnt[hi], n_fresh) : 0u;
-    __syncthreads();
-    uint32_t* list = H.list + H.list_off[hi] + fresh_base;
-    for (uint32_t i = threadIdx.x; i < n_fresh; i += kThreads) list[i] = fresh[i];
-    if (RULE == LV_RULE_CUDA_I) {
-      own = block_sum(own, red_own);
-      if (threadIdx.x == 0 && own != 0.0) atomicAdd(&H.own[hi], own);
-    }
-    __syncthreads();
-  }
-}
-
-// Evaluates a slice of a hub's distinct communities (its list), clears the
-// table slots it read, and folds its best key into H.best.
-__global__ void __launch_bounds__(kThreads)
-    hub_scan_kernel(LevelView L, const uint32_t* __restrict__ hubs, HubArena H,
-                    uint32_t blk_begin, uint32_t blk_end) {
-  __shared__ unsigned long long red_best[kWarps];
-  for (uint32_t b = blk_begin + blockIdx.x; b < blk_end; b += gridDim.x) {
-    const uint32_t hi = H.blk_vertex[b], ch = H.blk_chunk[b];
-    const uint32_t nch = H.blk_nchunks[b];
-    const uint32_t v = hubs[hi];
-    const uint32_t cv = L.comm[v];
     const GainCtx g = make_ctx(L, v, cv);
-    const uint64_t cnt = H.list_cnt[hi];
-    const uint64_t lo = cnt * ch / nch, hi_s = cnt * (ch + 1) / nch;
-    uint32_t* keys = H.keys + H.tab_off[hi];
-    double* vals = H.vals + H.tab_off[hi];
-    const uint32_t* list = H.list + H.list_off[hi];
-    unsigned long long best = 0ull;
-    for (uint64_t i = lo + threadIdx.x; i < hi_s; i += kThreads) {
-      const uint32_t slot = list[i];
-      const uint32_t c = keys[slot];
-      best = umax64(best, candidate(L, g, c, vals[slot]));
-      keys[slot] = kEmptyKey;
-      vals[slot] = 0.0;
-    }
+    unsigned long long best =
+        scan_fresh_and_clear(L, g, keys, vals, fresh, n_fresh, threadIdx.x, kThreads);
     best = block_max(best, red_best);
-    if (threadIdx.x == 0 && best) atomicMax(&H.best[hi], best);
+    if (RULE == LV_RULE_CUDA_I) own = block_sum(own, red_own);
+    if (threadIdx.x == 0) {
+      if (best) atomicMax(&H.best[hi], best);
+      if (RULE == LV_RULE_CUDA_I && own != 0.0) atomicAdd(&H.own[hi], own);
+      n_fresh = 0u;
+    }
+    __syncthreads();
   }
 }
 
@@ -581,7 +576,6 @@ __global__ void hub_decide_kernel(LevelView L, const uint32_t* __restrict__ hubs
     prop[i] = decide<RULE>(H.best[i], H.own[i], g);
     H.best[i] = 0ull;
     H.own[i] = 0.0;
-    H.list_cnt[i] = 0u;
   }
 }
 
@@ -980,8 +974,7 @@ unsigned sm_count_cached() {
 
 cudaError_t configure_kernels() {
   cudaError_t e;
-  const int warp512 = kWarps * 512 * 12;
-  const int block_tab = kHubSmemSlots * 12;
+  const int warp512 = kWarps * 512 * kSlotBytes;
   e = cudaFuncSetAttribute(move_warp_kernel<512, 10, LV_RULE_PY_I>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, warp512);
   if (e != cudaSuccess) return e;
@@ -989,16 +982,16 @@ cudaError_t configure_kernels() {
                            cudaFuncAttributeMaxDynamicSharedMemorySize, warp512);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(move_block_kernel<LV_RULE_PY_I>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, block_tab);
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, kBlockTabSmem);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(move_block_kernel<LV_RULE_CUDA_I>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, block_tab);
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, kBlockTabSmem);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(hub_insert_kernel<LV_RULE_PY_I>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, kHubInsertSmem);
+  e = cudaFuncSetAttribute(hub_part_kernel<LV_RULE_PY_I>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, kHubPartSmem);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(hub_insert_kernel<LV_RULE_CUDA_I>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, kHubInsertSmem);
+  e = cudaFuncSetAttribute(hub_part_kernel<LV_RULE_CUDA_I>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, kHubPartSmem);
   if (e != cudaSuccess) return e;
   return configure_contract_kernels();
 }
@@ -1058,35 +1051,28 @@ static cudaError_t move_bucket_impl(const LevelView& L, int bucket,
       if (cnt) {
         constexpr int T = 128;
         (count_launches(1), move_warp_kernel<T, 3, RULE><<<grid_for((cnt + 7) / 8, cap), kThreads,
-                                    kWarps * T * 12, st>>>(L, verts, cnt, pr));
+                                    kWarps * T * kSlotBytes, st>>>(L, verts, cnt, pr));
       }
       break;
     case 6:
       if (cnt) {
         constexpr int T = 512;
         (count_launches(1), move_warp_kernel<T, 10, RULE><<<grid_for((cnt + 7) / 8, sm_count() * 4), kThreads,
-                                    kWarps * T * 12, st>>>(L, verts, cnt, pr));
+                                    kWarps * T * kSlotBytes, st>>>(L, verts, cnt, pr));
       }
       break;
     case 7:  // class 7 of bucket 7: shared table, one block per vertex
       if (cnt) {
         (count_launches(1), move_block_kernel<RULE><<<grid_for(cnt, sm_count() * 4), kThreads,
-                                  kHubSmemSlots * 12, st>>>(L, verts, cnt, pr));
+                                  kBlockTabSmem, st>>>(L, verts, cnt, pr));
       }
       break;
-    case 8: {  // class 8 of bucket 7: global tables, several blocks per vertex
+    case 8: {  // class 8 of bucket 7: one block per (hub, partition)
       const uint32_t hs = P.cls_start[8];
       const uint32_t hc = P.cls_start[9] - hs;
       if (hc) {
-        // batch by batch, so the tables being filled stay in L2
-        for (uint32_t k = 0; k < H.n_batches; k++) {
-          const uint32_t b0 = H.batch_blk[k], b1 = H.batch_blk[k + 1];
-          (count_launches(1), hub_insert_kernel<RULE><<<grid_for(b1 - b0, sm_count() * 3),
-                                                       kThreads, kHubInsertSmem, st>>>(
-              L, order + hs, H, b0, b1));
-          (count_launches(1), hub_scan_kernel<<<grid_for(b1 - b0, cap), kThreads, 0, st>>>(
-              L, order + hs, H, b0, b1));
-        }
+        (count_launches(1), hub_part_kernel<RULE><<<grid_for(H.units, sm_count() * 2), kThreads,
+                                                  kHubPartSmem, st>>>(L, order + hs, H, H.units));
         (count_launches(1), hub_decide_kernel<RULE><<<(hc + 127) / 128, 128, 0, st>>>(
             L, order + hs, H, hc, prop + hs));
       }
