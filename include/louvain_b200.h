@@ -204,6 +204,35 @@ lv_status lv_modularity_fp64(lv_engine *e, const uint32_t *partition,
  * (modularity.cu:5-18,439).                                              */
 lv_status lv_get_buckets(lv_engine *e, uint8_t *bucket_of, size_t n);
 
+/* ---- batched form (no counterpart in the reference, which runs one graph
+ * per process: main.cu:5-70) --------------------------------------------
+ * Runs the reference's whole phase loop on many graphs at once: they are
+ * packed as one block-diagonal union (vertex ids offset per graph) and every
+ * kernel serves all of them; each graph keeps its own m, modularity, stop
+ * rule and levels, so its result equals a run of that graph alone
+ * (lv_run).  A graph whose phase ends is finalised and leaves the union.
+ *
+ * lv_batch_run_device: the union CSR is in device memory; graph g owns the
+ * vertices [graph_offsets[g], graph_offsets[g+1]) (host array, n_graphs+1
+ * entries) and its rows may only name its own vertices.  d_assignment
+ * (n_vertices) receives every vertex's community id local to its graph;
+ * modularity (host, n_graphs) each graph's final Q; levels (host,
+ * n_graphs, may be NULL) its number of phases.                            */
+lv_status lv_batch_run_device(lv_engine *e, uint32_t n_graphs,
+                              const uint64_t *graph_offsets, uint32_t n_vertices,
+                              uint64_t n_entries, const uint64_t *d_offsets,
+                              const uint32_t *d_cols, const float *d_weights,
+                              float min_gain, uint32_t *d_assignment,
+                              double *modularity, uint32_t *levels,
+                              lv_result *res);
+
+/* Same from host graphs (packed and uploaded by the call); assignment
+ * (host) receives the local ids of graph 0's vertices, then graph 1's...  */
+lv_status lv_batch_run(lv_engine *e, uint32_t n_graphs,
+                       const lv_graph *const *graphs, float min_gain,
+                       uint32_t *assignment, double *modularity,
+                       uint32_t *levels, lv_result *res);
+
 /* ---- kernel timing (no counterpart in the reference, whose only timers
  * are main.cu:19-56's two regions) --------------------------------------
  * With profiling on, every launch group is bracketed by CUDA events on the

@@ -111,6 +111,10 @@ __global__ void members_kernel(const uint32_t* comm, const uint32_t* comm_sz,
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n;
        v += gridDim.x * blockDim.x) {
     const uint32_t c = comm[v];
+    if (comm_sz[c] == 0u) {  // dropped graph (batched form): no new vertex
+      cnew[v] = 0u;
+      continue;
+    }
     const uint32_t pos = mem_off[c] + atomicAdd(&cursor[c], 1u);
     members[pos] = v;
     cnew[v] = flag_id[c];
@@ -118,12 +122,16 @@ __global__ void members_kernel(const uint32_t* comm, const uint32_t* comm_sz,
   }
 }
 
+// mstart[i] = degree of members[i] for the *d_members grouped vertices
+// (fewer than n when the batched form drops graphs), 0 beyond.
 __global__ void member_deg_kernel(const uint64_t* off, const uint32_t* members,
-                                  uint32_t n, uint64_t* mstart) {
+                                  uint32_t n, const uint32_t* d_members,
+                                  uint64_t* mstart) {
+  const uint32_t nm = *d_members;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= n;
        i += gridDim.x * blockDim.x) {
     uint64_t d = 0;
-    if (i < n) {
+    if (i < nm) {
       const uint32_t v = members[i];
       d = off[v + 1] - off[v];
     }
@@ -505,8 +513,8 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
   (count_launches(1), members_kernel<<<g1, 256, 0, st>>>(L.comm, L.comm_sz, n, B.flag_id, B.mem_off,
                                      B.cursor, B.members, B.cnew, B.comm_list));
   LV_TRY(cudaGetLastError());
-  (count_launches(1), member_deg_kernel<<<gridcap((n + 256) / 256, 8), 256, 0, st>>>(L.off, B.members, n,
-                                                                 B.mstart));
+  (count_launches(1), member_deg_kernel<<<gridcap((n + 256) / 256, 8), 256, 0, st>>>(
+      L.off, B.members, n, B.counts + 1, B.mstart));
   LV_TRY(cudaGetLastError());
   LV_TRY(exclusive_scan_u64(B.mstart, B.mstart, (size_t)n + 1, nullptr, S, st));
   // sizes of the new communities and their classes, with the new vertex

@@ -215,6 +215,20 @@ struct lv_engine {
   KStat kst[K_COUNT];
   std::vector<cudaEvent_t> ev_free;
   std::vector<PendingTiming> pending;
+  // batched form: the level holds n_graphs graphs (block-diagonal union)
+  bool batch = false;
+  uint32_t n_graphs = 0;
+  GraphState* gs = nullptr;       // [graph cap] device
+  GraphState* gs_host = nullptr;  // [graph cap] pinned
+  uint32_t* gid = nullptr;        // [cap_n] graph of every level vertex
+  uint32_t* goff_dev = nullptr;   // [graph cap + 1] level vertex offsets
+  uint32_t* graph0 = nullptr;     // [n0] input graph of every input vertex
+  uint32_t* gbase = nullptr;      // [graph cap] finalisation bases
+  uint32_t* gdrop = nullptr;      // [graph cap] graphs dropped at contraction
+  size_t graph_cap = 0;
+  uint32_t* batch_out = nullptr;  // local assignment of lv_batch_run
+  size_t batch_out_cap = 0;
+
   // all passes of the current level as one graph (WHILE node)
   cudaGraphExec_t level_exec = nullptr;
   // one pass of the current level captured as a CUDA graph (timing mode)
@@ -240,6 +254,9 @@ struct lv_engine {
     L.comm_sz = comm_sz;
     L.tot = tot;
     L.sc = sc;
+    L.gid = batch ? gid : nullptr;
+    L.gs = batch ? gs : nullptr;
+    L.n_graphs = batch ? n_graphs : 0u;
     return L;
   }
 };
@@ -340,6 +357,8 @@ void free_state(lv_engine* E) {
   dfree(E->prop);
   dfree(E->cls_count);
   dfree(E->assignment);
+  dfree(E->gid);
+  dfree(E->graph0);
   dfree(E->part_tmp);
   dfree(E->partials);
   dfree(E->hub_map);
@@ -429,6 +448,8 @@ lv_status ensure_capacity(lv_engine* E, uint32_t n, uint64_t e, bool need_input)
   CU(dalloc(&E->prop, N));
   CU(dalloc(&E->cls_count, 16));
   CU(dalloc(&E->assignment, N));
+  CU(dalloc(&E->gid, N));
+  CU(dalloc(&E->graph0, N));
   const size_t ptw = partition_tmp_words(N) + 64;
   CU(dalloc(&E->part_tmp, ptw));
   for (int i = 0; i < 2; i++) {
@@ -622,7 +643,8 @@ lv_status run_level_graph(lv_engine* E, float min_gain) {
     } guard{g};
     CU(cudaStreamBeginCaptureToGraph(E->st, g, nullptr, nullptr, 0,
                                      cudaStreamCaptureModeThreadLocal));
-    cudaError_t ce = launch_pass_control_init(E->sc, E->st);
+    cudaError_t ce = launch_pass_control_init(E->sc, E->batch ? E->gs : nullptr,
+                                              E->batch ? E->n_graphs : 0u, E->st);
     cudaGraph_t cap = nullptr;
     cudaError_t ce2 = cudaStreamEndCapture(E->st, &cap);
     CU(ce);
@@ -642,6 +664,7 @@ lv_status run_level_graph(lv_engine* E, float min_gain) {
     cudaGraph_t body = np.conditional.phGraph_out[0];
     PassControl ctl{};
     ctl.enabled = 1;
+    ctl.use_handle = 1;
     ctl.handle = (unsigned long long)h;
     ctl.min_gain = (double)min_gain;
     ctl.max_passes = E->cfg.max_passes;
@@ -674,13 +697,13 @@ lv_status run_level_graph(lv_engine* E, float min_gain) {
 // One pass (used when timing kernels: event nodes cannot live in a
 // conditional body).  With graphs on, the first pass of a level is captured
 // and every pass replays it.
-lv_status run_pass(lv_engine* E) {
-  if (!E->cfg.use_graphs) return issue_pass(E, nullptr);
+lv_status run_pass(lv_engine* E, const PassControl* ctl = nullptr) {
+  if (!E->cfg.use_graphs) return issue_pass(E, ctl);
   if (!E->pass_exec) {
     const unsigned long long l0 = launch_count();
     CU(cudaStreamBeginCapture(E->st, cudaStreamCaptureModeThreadLocal));
     E->capturing = true;
-    lv_status s = issue_pass(E, nullptr);
+    lv_status s = issue_pass(E, ctl);
     cudaGraph_t g = nullptr;
     cudaError_t ce = cudaStreamEndCapture(E->st, &g);
     E->capturing = false;
@@ -753,6 +776,8 @@ lv_status load_common(lv_engine* E, uint32_t n, uint64_t e) {
   E->level_ready = false;
   E->finished = false;
   E->accepted = false;
+  E->batch = false;
+  E->n_graphs = 0;
   E->levels.clear();
   E->q_last = 0.0;
   CU(launch_fill_iota(E->assignment, n, E->st));  // setInitComm, utils.cu:67
@@ -766,7 +791,211 @@ lv_status validate_sizes(uint32_t n, uint64_t e) {
   return LV_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Batched form: many graphs as one block-diagonal union.  Every graph runs
+// the reference's phase loop on its own (own m, modularity, stop rule);
+// the kernels serve all graphs of a level at once.  A graph whose phase
+// ends is finalised (its community ids made local) and dropped from the
+// union at the next contraction.
+// ---------------------------------------------------------------------------
+lv_status batch_alloc(lv_engine* E, uint32_t G) {
+  if (G <= E->graph_cap && E->gs) return LV_OK;
+  dfree(E->gs);
+  dfree(E->goff_dev);
+  dfree(E->gbase);
+  dfree(E->gdrop);
+  if (E->gs_host) cudaFreeHost(E->gs_host);
+  E->gs_host = nullptr;
+  CU(dalloc(&E->gs, G));
+  CU(dalloc(&E->goff_dev, (size_t)G + 1));
+  CU(dalloc(&E->gbase, G));
+  CU(dalloc(&E->gdrop, G));
+  CU(cudaMallocHost(&E->gs_host, sizeof(GraphState) * (G ? G : 1)));
+  E->graph_cap = G;
+  return LV_OK;
+}
+
+// One level's pass loop over every graph of the union; afterwards
+// gs_host holds every graph's passes, stop flags and modularity values.
+lv_status batch_passes(lv_engine* E, float min_gain) {
+  if (!E->level_ready) LVTRY(prepare_level(E));
+  if (E->cfg.use_graphs && !E->profiling) {
+    LVTRY(run_level_graph(E, min_gain));
+  } else {
+    CU(launch_pass_control_init(E->sc, E->gs, E->n_graphs, E->st));
+    PassControl ctl{};
+    ctl.enabled = 1;
+    ctl.use_handle = 0;
+    ctl.min_gain = (double)min_gain;
+    ctl.max_passes = E->cfg.max_passes;
+    for (;;) {
+      LVTRY(run_pass(E, &ctl));
+      CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost,
+                         E->st));
+      CU(cudaStreamSynchronize(E->st));
+      if (E->pass_exec) prof_collect_graph(E);
+      prof_collect(E);
+      if (!E->sc_host->any_active) break;
+    }
+  }
+  CU(cudaMemcpyAsync(E->gs_host, E->gs, sizeof(GraphState) * E->n_graphs,
+                     cudaMemcpyDeviceToHost, E->st));
+  CU(cudaStreamSynchronize(E->st));
+  if (E->cfg.use_graphs && !E->profiling) {  // replays of the WHILE body
+    uint32_t maxp = 0;
+    for (uint32_t g = 0; g < E->n_graphs; g++) maxp = std::max(maxp, E->gs_host[g].passes);
+    if (maxp > 1) count_launches((unsigned)((maxp - 1) * E->pass_launches));
+  }
+  return check_device_error(E);
+}
+
 }  // namespace
+
+// Drives the batched run; see lv_batch_run_device in the C ABI.
+static lv_status batch_run(lv_engine* E, uint32_t G, const uint64_t* goff_in,
+                           float min_gain, uint32_t* d_out, double* q_out,
+                           uint32_t* levels_out, lv_result* res) {
+  LVTRY(batch_alloc(E, G));
+  cudaStream_t st = E->st;
+  const uint32_t n0 = E->n0;
+  // level-0 graph list and input-vertex -> graph map
+  std::vector<uint32_t> goff(G + 1), ids(G);  // level offsets, level -> input graph
+  for (uint32_t g = 0; g <= G; g++) goff[g] = (uint32_t)goff_in[g];
+  for (uint32_t g = 0; g < G; g++) ids[g] = g;
+  CU(cudaMemcpyAsync(E->goff_dev, goff.data(), (G + 1) * sizeof(uint32_t),
+                     cudaMemcpyHostToDevice, st));
+  CU(launch_graph_ids(E->goff_dev, G, n0, E->cb.cursor, st));  // scratch
+  CU(cudaMemcpyAsync(E->graph0, E->cb.cursor, (size_t)n0 * sizeof(uint32_t),
+                     cudaMemcpyDeviceToDevice, st));
+  CU(cudaMemsetAsync(E->gs, 0, sizeof(GraphState) * G, st));
+  std::vector<uint32_t> lv(G, 0), base(G), drop(G);
+  std::vector<uint8_t> fz(G, 0);  // frozen: the graph's run ended at the last contraction
+  std::vector<double> qf(G, 0.0);
+  E->batch = true;
+  cudaEvent_t a0, a1;
+  CU(cudaEventCreate(&a0));
+  CU(cudaEventCreate(&a1));
+  CU(cudaEventRecord(a0, st));
+  uint64_t processed = 0, n_comm = 0;
+  lv_status status = LV_OK;
+  for (;;) {
+    const uint32_t Gl = (uint32_t)ids.size();
+    E->n_graphs = Gl;
+    bool all_frozen = true;
+    for (uint32_t g = 0; g < Gl; g++) all_frozen = all_frozen && fz[g];
+    if (!all_frozen) {
+      CU(cudaMemcpyAsync(E->goff_dev, goff.data(), (Gl + 1) * sizeof(uint32_t),
+                         cudaMemcpyHostToDevice, st));
+      CU(launch_graph_ids(E->goff_dev, Gl, E->n, E->gid, st));
+      status = batch_passes(E, min_gain);
+      if (status != LV_OK) break;
+    }
+    // per graph: its run ends here (frozen, no edge weight, or the first
+    // pass gained too little: modularity.cu:501-508) or goes on to
+    // contraction, as run_loaded decides for a single graph
+    bool any_continue = false;
+    const bool last_level =
+        E->cfg.max_levels && (uint32_t)(E->levels.size() + 1) >= E->cfg.max_levels;
+    uint64_t lvl_passes = 0;
+    for (uint32_t g = 0; g < Gl; g++) {
+      const uint32_t og = ids[g];
+      bool ended = true;
+      if (!fz[g]) {  // a frozen graph keeps the result of its last level
+        const GraphState& s = E->gs_host[g];
+        lv[og]++;
+        lvl_passes = std::max<uint64_t>(lvl_passes, s.passes);
+        if (s.passes == 0) qf[og] = 0.0;  // no edge weight: nothing moves
+        else if (s.first_fail) qf[og] = s.q_before;  // moves of the pass discarded
+        else {
+          qf[og] = s.q;
+          ended = false;
+        }
+      }
+      base[g] = ended ? goff[g] : 0xFFFFFFFFu;
+      drop[g] = ended ? 1u : 0u;
+      if (ended) n_comm += goff[g + 1] - goff[g];
+      any_continue = any_continue || !ended;
+    }
+    if (!all_frozen) {
+      lv_level_info info{};
+      info.n_vertices = E->n;
+      info.n_entries = E->e;
+      info.passes = (uint32_t)lvl_passes;
+      info.moved = any_continue ? 1u : 0u;
+      E->levels.push_back(info);
+      processed += lvl_passes * E->e;
+    }
+    // finalise the graphs that ended here: ids local to their graph
+    {
+      std::vector<uint32_t> b_in(G, 0xFFFFFFFFu);
+      for (uint32_t g = 0; g < Gl; g++)
+        if (drop[g]) b_in[ids[g]] = base[g];
+      CU(cudaMemcpyAsync(E->gbase, b_in.data(), G * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+      CU(launch_finalize_graphs(E->assignment, n0, E->graph0, E->gbase, d_out, st));
+      CU(cudaStreamSynchronize(st));
+    }
+    if (!any_continue) break;
+    // contract the graphs that go on; the others leave the union
+    CU(cudaMemcpyAsync(E->gdrop, drop.data(), Gl * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    CU(launch_drop_graphs(E->comm_sz, E->gid, E->n, E->gdrop, st));
+    E->accepted = true;
+    status = lv_phase_aggregate(E);
+    if (status != LV_OK) break;
+    // new offsets of the remaining graphs: new id of their first community
+    std::vector<uint32_t> keep_idx, keep_ids;
+    for (uint32_t g = 0; g < Gl; g++)
+      if (!drop[g]) {
+        keep_idx.push_back(goff[g]);
+        keep_ids.push_back(ids[g]);
+      }
+    const uint32_t Gn = (uint32_t)keep_ids.size();
+    CU(cudaMemcpyAsync(E->gbase, keep_idx.data(), Gn * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    CU(launch_gather_u32(E->cb.flag_id, E->gbase, Gn, E->goff_dev, st));
+    std::vector<uint32_t> ng(Gn + 1);
+    CU(cudaMemcpyAsync(ng.data(), E->goff_dev, Gn * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    ng[Gn] = E->n;
+    // a graph whose level merged nothing would repeat forever (min gain
+    // <= 0): freeze it, so its next level ends at once
+    std::vector<GraphState> init(Gn);
+    memset(init.data(), 0, sizeof(GraphState) * Gn);
+    std::vector<uint8_t> nfz(Gn, 0);
+    for (uint32_t g = 0, i = 0; g < Gl; g++) {
+      if (drop[g]) continue;
+      const uint32_t before = goff[g + 1] - goff[g];
+      nfz[i] = (ng[i + 1] - ng[i] == before || last_level) ? 1u : 0u;
+      init[i].frozen = nfz[i];
+      i++;
+    }
+    CU(cudaMemcpyAsync(E->gs, init.data(), sizeof(GraphState) * Gn, cudaMemcpyHostToDevice, st));
+    goff.swap(ng);
+    ids.swap(keep_ids);
+    fz.swap(nfz);
+  }
+  CU(cudaEventRecord(a1, st));
+  CU(cudaEventSynchronize(a1));
+  float alg = 0.0f;
+  cudaEventElapsedTime(&alg, a0, a1);
+  cudaEventDestroy(a0);
+  cudaEventDestroy(a1);
+  E->batch = false;
+  E->finished = true;
+  if (status != LV_OK) return status;
+  if (q_out)
+    for (uint32_t g = 0; g < G; g++) q_out[g] = qf[g];
+  if (levels_out)
+    for (uint32_t g = 0; g < G; g++) levels_out[g] = lv[g];
+  if (res) {
+    res->modularity = 0.0;
+    res->n_vertices = n0;
+    res->n_communities = (uint32_t)n_comm;
+    res->n_levels = (uint32_t)E->levels.size();
+    res->edges_processed = processed;
+    res->alg_ms = alg;
+    res->copy_ms = 0.0f;
+  }
+  return LV_OK;
+}
 
 // ===========================================================================
 // C ABI
@@ -858,6 +1087,12 @@ void lv_engine_destroy(lv_engine* E) {
   if (E->st) cudaStreamSynchronize(E->st);
   drop_pass_graph(E);
   free_state(E);
+  dfree(E->gs);
+  dfree(E->goff_dev);
+  dfree(E->gbase);
+  dfree(E->gdrop);
+  dfree(E->batch_out);
+  if (E->gs_host) cudaFreeHost(E->gs_host);
   prof_collect(E);
   for (cudaEvent_t ev : E->ev_free) cudaEventDestroy(ev);
   E->ev_free.clear();
@@ -1227,6 +1462,73 @@ lv_status lv_get_kernel_stats(lv_engine* E, lv_kernel_stat* out, uint32_t cap,
       out[i].bytes = E->kst[i].bytes;
     }
   }
+  return LV_OK;
+}
+
+lv_status lv_batch_run_device(lv_engine* E, uint32_t n_graphs, const uint64_t* graph_offsets,
+                              uint32_t n_vertices, uint64_t n_entries, const uint64_t* d_offsets,
+                              const uint32_t* d_cols, const float* d_weights, float min_gain,
+                              uint32_t* d_assignment, double* modularity, uint32_t* levels,
+                              lv_result* res) {
+  if (!E || !graph_offsets || !d_assignment || (n_graphs && !modularity))
+    return fail(LV_ERR_ARG, "NULL argument");
+  if (n_graphs == 0) return fail(LV_ERR_ARG, "no graphs");
+  if (graph_offsets[0] != 0 || graph_offsets[n_graphs] != n_vertices)
+    return fail(LV_ERR_ARG, "graph offsets must run from 0 to the vertex count");
+  for (uint32_t g = 0; g < n_graphs; g++)
+    if (graph_offsets[g + 1] < graph_offsets[g])
+      return fail(LV_ERR_ARG, "graph offsets must be non-decreasing");
+  LVTRY(lv_engine_load_device(E, n_vertices, n_entries, d_offsets, d_cols, d_weights));
+  return batch_run(E, n_graphs, graph_offsets, min_gain, d_assignment, modularity, levels, res);
+}
+
+lv_status lv_batch_run(lv_engine* E, uint32_t n_graphs, const lv_graph* const* graphs,
+                       float min_gain, uint32_t* assignment, double* modularity,
+                       uint32_t* levels, lv_result* res) {
+  if (!E || !graphs || !assignment || !modularity) return fail(LV_ERR_ARG, "NULL argument");
+  if (n_graphs == 0) return fail(LV_ERR_ARG, "no graphs");
+  // pack the graphs into one block-diagonal CSR (vertex ids offset per graph)
+  std::vector<uint64_t> goff(n_graphs + 1, 0), eoff(n_graphs + 1, 0);
+  for (uint32_t g = 0; g < n_graphs; g++) {
+    if (!graphs[g]) return fail(LV_ERR_ARG, "NULL graph");
+    goff[g + 1] = goff[g] + graphs[g]->n;
+    eoff[g + 1] = eoff[g] + graphs[g]->nnz;
+  }
+  if (goff[n_graphs] >= 0xFFFFFFFFull) return fail(LV_ERR_LIMIT, "too many vertices in the batch");
+  lv_graph u;
+  const uint32_t N = (uint32_t)goff[n_graphs];
+  try {
+    u.n = N;
+    u.nnz = eoff[n_graphs];
+    for (uint32_t g = 0; g < n_graphs; g++) u.max_deg = std::max(u.max_deg, graphs[g]->max_deg);
+    u.off.resize((size_t)N + 1);
+    u.col.resize(u.nnz);
+    u.w.resize(u.nnz);
+    for (uint32_t g = 0; g < n_graphs; g++) {
+      const lv_graph* h = graphs[g];
+      const uint32_t vb = (uint32_t)goff[g];
+      const uint64_t eb = eoff[g];
+      for (uint32_t v = 0; v < h->n; v++) u.off[vb + v] = eb + h->off[v];
+      for (uint64_t j = 0; j < h->nnz; j++) {
+        u.col[eb + j] = vb + h->col[j];
+        u.w[eb + j] = h->w[j];
+      }
+    }
+    u.off[N] = u.nnz;
+  } catch (const std::bad_alloc&) {
+    return fail(LV_ERR_NOMEM, "batch does not fit in host memory");
+  }
+  LVTRY(lv_engine_load(E, &u));
+  if (N > E->batch_out_cap) {
+    dfree(E->batch_out);
+    CU(dalloc(&E->batch_out, N));
+    E->batch_out_cap = N;
+  }
+  uint32_t* d_out = E->batch_out;
+  LVTRY(batch_run(E, n_graphs, goff.data(), min_gain, d_out, modularity, levels, res));
+  CU(cudaMemcpyAsync(assignment, d_out, (size_t)N * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                     E->st));
+  CU(cudaStreamSynchronize(E->st));
   return LV_OK;
 }
 

@@ -63,16 +63,55 @@ struct LevelScalars {
   uint32_t first_fail;   // the first pass gained less than min gain
   double q_prev;         // Q after the previous pass
   double q_before;       // Q before the last pass
+  uint32_t any_active;   // some graph's pass loop goes on
+  uint32_t pad;
 };
 
 // Stop rule evaluated by the modularity sweep's last block when the pass
 // loop runs inside a CUDA graph WHILE node.
 struct PassControl {
   int enabled;
+  int use_handle;             // set the graph condition (WHILE node)
   unsigned long long handle;  // cudaGraphConditionalHandle
   double min_gain;
   uint32_t max_passes;
 };
+
+// Per-graph state when a level holds many graphs (batched form): the
+// union of the graphs is one block-diagonal CSR and every graph keeps its
+// own m, modularity and pass control.
+struct GraphState {
+  double m_acc;      // sum of k over the graph's vertices (accumulated)
+  double m64;        // m = m_acc / 2
+  float m;           // FP32 m of the gains
+  float den;         // 2 m m in FP32
+  double intra_acc;  // modularity sweep accumulators
+  double asq_acc;
+  double q;          // Q after the latest sweep
+  double q_prev;     // Q after the previous pass
+  double q_before;   // Q before the last pass
+  uint32_t passes;   // passes run at this level
+  uint32_t active;   // still moving in this level's pass loop
+  uint32_t first_fail;  // first pass gained less than min gain
+  uint32_t frozen;   // set by the host: the graph takes no more passes
+};
+
+// Batched-form helpers (move.cu).
+// gid[v] = graph of vertex v, from the graphs' vertex offsets goff[0..G].
+cudaError_t launch_graph_ids(const uint32_t* goff, uint32_t n_graphs, uint32_t n,
+                             uint32_t* gid, cudaStream_t st);
+// out[i] = asg[i] - base[graph0[i]] for the input vertices whose graph has
+// a base (finished now); base[g] == 0xFFFFFFFF leaves out[i] untouched.
+cudaError_t launch_finalize_graphs(const uint32_t* asg, size_t n0,
+                                   const uint32_t* graph0, const uint32_t* base,
+                                   uint32_t* out, cudaStream_t st);
+// comm_sz[v] = 0 for the vertices of graphs flagged in drop[] (their
+// communities then take no part in the contraction).
+cudaError_t launch_drop_graphs(uint32_t* comm_sz, const uint32_t* gid, uint32_t n,
+                               const uint32_t* drop, cudaStream_t st);
+// out[i] = src[idx[i]]
+cudaError_t launch_gather_u32(const uint32_t* src, const uint32_t* idx, uint32_t n,
+                              uint32_t* out, cudaStream_t st);
 
 // Read-mostly view of the current level passed to kernels by value.
 struct LevelView {
@@ -85,6 +124,11 @@ struct LevelView {
   uint32_t* comm_sz;   // vertices per community
   double* tot;         // community totals a_c (FP64, exact for FP32 inputs)
   LevelScalars* sc;
+  // batched form only (nullptr for a single graph): graph of every vertex
+  // of the level, and the graphs' state
+  const uint32_t* gid;
+  GraphState* gs;
+  uint32_t n_graphs;
 };
 
 // Work partition of a level for the "class dispatch" kernels (row sums and
@@ -147,8 +191,10 @@ cudaError_t launch_modularity(const LevelView& L, const uint32_t* order,
                               const DispatchPlan& P, const uint32_t* hub_map,
                               double* partials, cudaStream_t st,
                               const PassControl* ctl = nullptr);
-// passes = 0, first_fail = 0, q_prev = q (start of a level's pass loop)
-cudaError_t launch_pass_control_init(LevelScalars* sc, cudaStream_t st);
+// passes = 0, first_fail = 0, q_prev = q (start of a level's pass loop),
+// for the single graph and for every graph of a batch
+cudaError_t launch_pass_control_init(LevelScalars* sc, GraphState* gs,
+                                     uint32_t n_graphs, cudaStream_t st);
 // Hubs (class 8): work units are (hub, hash partition of its neighbour
 // communities); per hub a best packed (gain, ~community) key and an
 // own-community weight sum.

@@ -73,13 +73,27 @@ __device__ __forceinline__ unsigned long long pack_best(float gain,
 struct GainCtx {
   float m, den, kv, aown_minus_kv;
   uint32_t cv, szv;
+  bool active;  // the vertex's graph still moves (batched form)
 };
+
+// Batched form: a vertex moves only while its graph's pass loop runs.
+__device__ __forceinline__ bool vertex_active(const LevelView& L, uint32_t v) {
+  return !L.gid || L.gs[L.gid[v]].active;
+}
 
 __device__ __forceinline__ GainCtx make_ctx(const LevelView& L, uint32_t v,
                                             uint32_t cv) {
   GainCtx g;
-  g.m = L.sc->m;
-  g.den = L.sc->den;
+  if (L.gid) {
+    const GraphState& gs = L.gs[L.gid[v]];
+    g.m = gs.m;
+    g.den = gs.den;
+    g.active = gs.active != 0u;
+  } else {
+    g.m = L.sc->m;
+    g.den = L.sc->den;
+    g.active = true;
+  }
   g.kv = L.k[v];
   g.aown_minus_kv = __fsub_rn((float)L.tot[cv], g.kv);
   g.cv = cv;
@@ -111,7 +125,7 @@ __device__ __forceinline__ unsigned long long candidate(const LevelView& L,
 template <int RULE>
 __device__ __forceinline__ uint32_t decide(unsigned long long best, double own,
                                            const GainCtx& g) {
-  if (best == 0ull) return g.cv;
+  if (best == 0ull || !g.active) return g.cv;
   const float bg = key_float((uint32_t)(best >> 32));
   const uint32_t bc = ~(uint32_t)best;
   bool move;
@@ -196,13 +210,15 @@ __global__ void __launch_bounds__(kThreads)
     const bool vvalid = vidx < count;
     uint32_t v = 0, d = 0, cv = 0;
     uint64_t s = 0;
+    bool act = false;
     if (vvalid) {
       v = verts[vidx];
       s = L.off[v];
       d = (uint32_t)(L.off[v + 1] - s);
       cv = L.comm[v];
+      act = vertex_active(L, v);
     }
-    const bool has = gl < (int)d;
+    const bool has = act && gl < (int)d;
     uint32_t u = 0, cu = 0;
     float wt = 0.0f;
     if (has) {
@@ -304,6 +320,10 @@ __global__ void __launch_bounds__(kThreads)
     const uint64_t s = L.off[v];
     const uint32_t d = (uint32_t)(L.off[v + 1] - s);
     const uint32_t cv = L.comm[v];
+    if (!vertex_active(L, v)) {  // warp-uniform: one vertex per warp
+      if (lane == 0) prop[vidx] = cv;
+      continue;
+    }
     const uint32_t tv = table_size_for(d, T);
     uint32_t cu[MAXW];
     float wt[MAXW];
@@ -455,6 +475,10 @@ __global__ void __launch_bounds__(kThreads)
     const uint64_t s = L.off[v];
     const uint32_t d = (uint32_t)(L.off[v + 1] - s);
     const uint32_t cv = L.comm[v];
+    if (!vertex_active(L, v)) {  // block-uniform: one vertex per block
+      if (threadIdx.x == 0) prop[vidx] = cv;
+      continue;
+    }
     const uint32_t tv = table_size_for(d, T);
     double own = 0.0;
     insert_block_range<MAXW, RULE>(L, s, 0, d, v, cv, keys, vals, tv - 1, own,
@@ -512,6 +536,7 @@ __global__ void __launch_bounds__(kThreads)
     const uint64_t s = L.off[v];
     const uint64_t d = L.off[v + 1] - s;
     const uint32_t cv = L.comm[v];
+    if (!vertex_active(L, v)) continue;  // block-uniform; decide keeps cv
     double own = 0.0;
     for (uint64_t j0 = 0; j0 < d; j0 += (uint64_t)PF * kThreads) {
       uint32_t cu[PF];
@@ -623,9 +648,10 @@ struct RowSumOp {
     L.k[v] = kf;
     L.tot[v] = (double)kf;
     part += (double)kf;
+    if (L.gid && kf != 0.0f) atomicAdd(&L.gs[L.gid[v]].m_acc, (double)kf);
   }
-  __device__ void hub(const DispatchArgs& A, uint32_t hi, double sum,
-                      double&) const {
+  __device__ void hub(const LevelView&, const DispatchArgs& A, uint32_t hi, uint32_t,
+                      double sum, double&) const {
     atomicAdd(&A.hub_acc[hi], sum);
   }
 };
@@ -639,13 +665,15 @@ struct IntraOp {
                          float w) const {
     return L.comm[u] == cv ? (double)w : 0.0;
   }
-  __device__ void vertex(const LevelView&, uint32_t, double sum,
+  __device__ void vertex(const LevelView& L, uint32_t v, double sum,
                          double& part) const {
     part += sum;
+    if (L.gid && sum != 0.0) atomicAdd(&L.gs[L.gid[v]].intra_acc, sum);
   }
-  __device__ void hub(const DispatchArgs&, uint32_t, double sum,
-                      double& part) const {
+  __device__ void hub(const LevelView& L, const DispatchArgs&, uint32_t, uint32_t v,
+                      double sum, double& part) const {
     part += sum;
+    if (L.gid && sum != 0.0) atomicAdd(&L.gs[L.gid[v]].intra_acc, sum);
   }
 };
 
@@ -724,7 +752,7 @@ __device__ __forceinline__ void unit_hub(const LevelView& L,
   for (uint64_t j = lo + threadIdx.x; j < end; j += kThreads)
     x += op.edge(L, c, L.col[s + j], L.w[s + j]);
   x = block_sum(x, red);
-  if (threadIdx.x == 0) op.hub(A, hi, x, part);
+  if (threadIdx.x == 0) op.hub(L, A, hi, v, x, part);
 }
 
 // Deterministic block reduction into partials, then the last block to
@@ -809,6 +837,7 @@ __global__ void __launch_bounds__(kThreads)
     L.tot[v] = (double)kf;
     A.hub_acc[i] = 0.0;
     hs += (double)kf;
+    if (L.gid && kf != 0.0f) atomicAdd(&L.gs[L.gid[v]].m_acc, (double)kf);
   }
   hs = block_sum(hs, red);
   if (threadIdx.x == 0) {
@@ -818,6 +847,18 @@ __global__ void __launch_bounds__(kThreads)
     L.sc->m = m;
     L.sc->den = __fmul_rn(__fmul_rn(2.0f, m), m);
     L.sc->done_blocks = 0u;
+  }
+  // batched form: every graph's own m (the union's m above is unused)
+  if (L.gid) {
+    for (uint32_t g = threadIdx.x; g < L.n_graphs; g += kThreads) {
+      GraphState& gs = L.gs[g];
+      const double m64 = __ldcg(&gs.m_acc) / 2.0;
+      const float m = (float)m64;
+      gs.m64 = m64;
+      gs.m = m;
+      gs.den = __fmul_rn(__fmul_rn(2.0f, m), m);
+      gs.m_acc = 0.0;
+    }
   }
 }
 
@@ -833,36 +874,90 @@ __global__ void __launch_bounds__(kThreads)
   for (uint32_t c = c0 + threadIdx.x; c < c1; c += kThreads) {
     const double a = L.tot[c];
     asq += a * a;
+    // community ids are vertex ids, so community c belongs to gid[c]
+    if (L.gid && a != 0.0) atomicAdd(&L.gs[L.gid[c]].asq_acc, a * a);
   }
   if (!publish_and_check_last(part, asq, A, L.sc, red)) return;
   double intra, sq;
   sum_partials(A, red, intra, sq);
+  if (!L.gid) {
+    if (threadIdx.x == 0) {
+      const double m = L.sc->m64;
+      const double q = (m > 0.0) ? (intra / (2.0 * m)) - (sq / (4.0 * m * m)) : 0.0;
+      L.sc->intra = intra;
+      L.sc->asq = sq;
+      L.sc->q = q;
+      L.sc->done_blocks = 0u;
+      if (ctl.enabled) {
+        // stop rule of modularity.cu:501-508 / louvian.py:91-99
+        const uint32_t p = L.sc->passes + 1;
+        const double old = L.sc->q_prev;
+        if (p == 1 && q - old < ctl.min_gain) L.sc->first_fail = 1u;
+        const bool cont = (q - old >= ctl.min_gain) && p < ctl.max_passes;
+        L.sc->passes = p;
+        L.sc->q_before = old;
+        L.sc->q_prev = q;
+        L.sc->any_active = cont ? 1u : 0u;
+        if (ctl.use_handle)
+          cudaGraphSetConditional((cudaGraphConditionalHandle)ctl.handle, cont ? 1u : 0u);
+      }
+    }
+    return;
+  }
+  // batched form: every graph's modularity and stop rule; the loop goes on
+  // while any graph still gains
+  int any = 0;
+  for (uint32_t g = threadIdx.x; g < L.n_graphs; g += kThreads) {
+    GraphState& s = L.gs[g];
+    const double gi = __ldcg(&s.intra_acc), gq = __ldcg(&s.asq_acc);
+    s.intra_acc = 0.0;
+    s.asq_acc = 0.0;
+    if (ctl.enabled && !s.active) continue;  // finished its pass loop
+    const double m = s.m64;
+    const double q = (m > 0.0) ? (gi / (2.0 * m)) - (gq / (4.0 * m * m)) : 0.0;
+    s.q = q;
+    if (ctl.enabled) {
+      const uint32_t p = s.passes + 1;
+      const double old = s.q_prev;
+      if (p == 1 && q - old < ctl.min_gain) s.first_fail = 1u;
+      const bool cont = (q - old >= ctl.min_gain) && p < ctl.max_passes;
+      s.passes = p;
+      s.q_before = old;
+      s.q_prev = q;
+      s.active = cont ? 1u : 0u;
+      any |= cont ? 1 : 0;
+    }
+  }
+  any = __syncthreads_or(any);
   if (threadIdx.x == 0) {
-    const double m = L.sc->m64;
-    const double q = (m > 0.0) ? (intra / (2.0 * m)) - (sq / (4.0 * m * m)) : 0.0;
-    L.sc->intra = intra;
-    L.sc->asq = sq;
-    L.sc->q = q;
     L.sc->done_blocks = 0u;
     if (ctl.enabled) {
-      // stop rule of modularity.cu:501-508 / louvian.py:91-99
-      const uint32_t p = L.sc->passes + 1;
-      const double old = L.sc->q_prev;
-      if (p == 1 && q - old < ctl.min_gain) L.sc->first_fail = 1u;
-      const bool cont = (q - old >= ctl.min_gain) && p < ctl.max_passes;
-      L.sc->passes = p;
-      L.sc->q_before = old;
-      L.sc->q_prev = q;
-      cudaGraphSetConditional((cudaGraphConditionalHandle)ctl.handle, cont ? 1u : 0u);
+      L.sc->any_active = any ? 1u : 0u;
+      if (ctl.use_handle)
+        cudaGraphSetConditional((cudaGraphConditionalHandle)ctl.handle, any ? 1u : 0u);
     }
   }
 }
 
-__global__ void pass_control_init_kernel(LevelScalars* sc) {
-  sc->passes = 0u;
-  sc->first_fail = 0u;
-  sc->q_prev = sc->q;
-  sc->q_before = sc->q;
+__global__ void pass_control_init_kernel(LevelScalars* sc, GraphState* gs,
+                                         uint32_t n_graphs) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) {
+    sc->passes = 0u;
+    sc->first_fail = 0u;
+    sc->q_prev = sc->q;
+    sc->q_before = sc->q;
+    sc->any_active = 1u;
+  }
+  for (uint32_t g = t; g < n_graphs; g += gridDim.x * blockDim.x) {
+    GraphState& s = gs[g];
+    s.passes = 0u;
+    s.first_fail = 0u;
+    s.q_prev = s.q;
+    s.q_before = s.q;
+    // nothing moves in an edgeless graph, nor in one the host froze
+    s.active = (s.m64 > 0.0 && !s.frozen) ? 1u : 0u;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -878,6 +973,39 @@ __global__ void gather_kernel(uint32_t* out, const uint32_t* in, size_t n,
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
     out[i] = map[in[i]];
+}
+__global__ void graph_ids_kernel(const uint32_t* goff, uint32_t n_graphs, uint32_t n,
+                                 uint32_t* gid) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = n_graphs - 1;  // largest g with goff[g] <= v
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (goff[mid] <= v) lo = mid; else hi = mid - 1;
+    }
+    gid[v] = lo;
+  }
+}
+__global__ void finalize_graphs_kernel(const uint32_t* asg, size_t n0,
+                                       const uint32_t* graph0, const uint32_t* base,
+                                       uint32_t* out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n0;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t b = base[graph0[i]];
+    if (b != 0xFFFFFFFFu) out[i] = asg[i] - b;
+  }
+}
+__global__ void drop_graphs_kernel(uint32_t* comm_sz, const uint32_t* gid, uint32_t n,
+                                   const uint32_t* drop) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += gridDim.x * blockDim.x)
+    if (drop[gid[v]]) comm_sz[v] = 0u;
+}
+__global__ void gather_u32_kernel(const uint32_t* src, const uint32_t* idx, uint32_t n,
+                                  uint32_t* out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x)
+    out[i] = src[idx[i]];
 }
 __global__ void iota_kernel(uint32_t* a, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
@@ -1019,8 +1147,10 @@ cudaError_t launch_modularity(const LevelView& L, const uint32_t* order,
   return cudaGetLastError();
 }
 
-cudaError_t launch_pass_control_init(LevelScalars* sc, cudaStream_t st) {
-  (count_launches(1), pass_control_init_kernel<<<1, 1, 0, st>>>(sc));
+cudaError_t launch_pass_control_init(LevelScalars* sc, GraphState* gs,
+                                     uint32_t n_graphs, cudaStream_t st) {
+  const unsigned g = n_graphs ? (n_graphs + 255) / 256 : 1;
+  (count_launches(1), pass_control_init_kernel<<<g, 256, 0, st>>>(sc, gs, n_graphs));
   return cudaGetLastError();
 }
 
@@ -1118,6 +1248,38 @@ cudaError_t launch_gather(uint32_t* out, const uint32_t* in, size_t n,
   if (!n) return cudaSuccess;
   (count_launches(1), gather_kernel<<<grid_for((n + 255) / 256, sm_count() * 8), 256, 0, st>>>(
       out, in, n, map));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_graph_ids(const uint32_t* goff, uint32_t n_graphs, uint32_t n,
+                             uint32_t* gid, cudaStream_t st) {
+  if (!n || !n_graphs) return cudaSuccess;
+  (count_launches(1), graph_ids_kernel<<<grid_for((n + 255) / 256, sm_count() * 8), 256, 0, st>>>(
+      goff, n_graphs, n, gid));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finalize_graphs(const uint32_t* asg, size_t n0, const uint32_t* graph0,
+                                   const uint32_t* base, uint32_t* out, cudaStream_t st) {
+  if (!n0) return cudaSuccess;
+  (count_launches(1), finalize_graphs_kernel<<<grid_for((n0 + 255) / 256, sm_count() * 8), 256, 0, st>>>(
+      asg, n0, graph0, base, out));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_drop_graphs(uint32_t* comm_sz, const uint32_t* gid, uint32_t n,
+                               const uint32_t* drop, cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  (count_launches(1), drop_graphs_kernel<<<grid_for((n + 255) / 256, sm_count() * 8), 256, 0, st>>>(
+      comm_sz, gid, n, drop));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_u32(const uint32_t* src, const uint32_t* idx, uint32_t n,
+                              uint32_t* out, cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  (count_launches(1), gather_u32_kernel<<<grid_for((n + 255) / 256, sm_count() * 8), 256, 0, st>>>(
+      src, idx, n, out));
   return cudaGetLastError();
 }
 

@@ -121,6 +121,11 @@ _SIGS = {
     "lv_get_launch_count": (ctypes.c_int, [ctypes.POINTER(_U64)]),
     "lv_modularity_noalloc": (ctypes.c_int, [_U32, _VP, _VP, _VP, _VP, _VP,
                                              ctypes.POINTER(ctypes.c_double), _VP]),
+    "lv_batch_run_device": (ctypes.c_int, [_VP, _U32, _VP, _U32, _U64, _VP, _VP, _VP,
+                                           ctypes.c_float, _VP, _VP, _VP,
+                                           ctypes.POINTER(Result)]),
+    "lv_batch_run": (ctypes.c_int, [_VP, _U32, _VP, ctypes.c_float, _VP, _VP, _VP,
+                                    ctypes.POINTER(Result)]),
 }
 
 NOALLOC_MAX_VERTICES = 1 << 20
@@ -135,6 +140,30 @@ def modularity_noalloc(n: int, d_off: int, d_col: int, d_w: int, d_part: int,
     _check(lib().lv_modularity_noalloc(n, d_off, d_col, d_w, d_part, d_q,
                                        ctypes.byref(q), stream or None))
     return q.value
+
+def pack_graphs(csrs):
+    """Block-diagonal union of CSR graphs [(n, off, col, w), ...], the input
+    layout of lv_batch_run_device.  Returns (graph_offsets u64[G+1],
+    off u64[N+1], col u32[E], w f32[E]): graph g's vertices are renumbered
+    by graph_offsets[g] and its entries keep their order."""
+    G = len(csrs)
+    goff = np.zeros(G + 1, dtype=np.uint64)
+    eoff = np.zeros(G + 1, dtype=np.uint64)
+    for g, (n, off, col, w) in enumerate(csrs):
+        goff[g + 1] = goff[g] + np.uint64(n)
+        eoff[g + 1] = eoff[g] + np.uint64(len(col))
+    N, E = int(goff[G]), int(eoff[G])
+    off = np.empty(N + 1, dtype=np.uint64)
+    col = np.empty(E, dtype=np.uint32)
+    w = np.empty(E, dtype=np.float32)
+    for g, (n, o, c, x) in enumerate(csrs):
+        vb, eb = int(goff[g]), int(eoff[g])
+        off[vb:vb + n] = np.asarray(o[:n], dtype=np.uint64) + np.uint64(eb)
+        col[eb:eb + len(c)] = np.asarray(c, dtype=np.uint64) + np.uint64(vb)
+        w[eb:eb + len(c)] = x
+    off[N] = E
+    return goff, off, col, w
+
 
 _lib = None
 
@@ -317,6 +346,40 @@ class Engine:
                                    d_assignment or None, ctypes.byref(r)))
         self.n0 = n
         return r
+
+    def batch_run(self, graphs, min_gain: float):
+        """Runs every graph of `graphs` (Graph objects) in one batched run.
+        Returns (list of per-graph local assignments, modularity array,
+        levels array, Result)."""
+        G = len(graphs)
+        arr = (_VP * max(G, 1))(*[g._h for g in graphs])
+        sizes = [g.csr()[0] for g in graphs]
+        out = np.zeros(max(sum(sizes), 1), dtype=np.uint32)
+        q = np.zeros(max(G, 1), dtype=np.float64)
+        lv = np.zeros(max(G, 1), dtype=np.uint32)
+        r = Result()
+        _check(lib().lv_batch_run(self._h, G, arr, min_gain, _p(out), _p(q), _p(lv),
+                                  ctypes.byref(r)))
+        parts, s = [], 0
+        for n in sizes:
+            parts.append(out[s:s + n].copy())
+            s += n
+        return parts, q[:G].copy(), lv[:G].copy(), r
+
+    def batch_run_device(self, graph_offsets, n: int, nnz: int, d_off: int, d_col: int,
+                         d_w: int, min_gain: float, d_assignment: int):
+        """Batched run over a block-diagonal union CSR in device memory;
+        graph g owns vertices [graph_offsets[g], graph_offsets[g+1]).
+        Returns (modularity array, levels array, Result)."""
+        goff = np.ascontiguousarray(graph_offsets, dtype=np.uint64)
+        G = len(goff) - 1
+        q = np.zeros(max(G, 1), dtype=np.float64)
+        lv = np.zeros(max(G, 1), dtype=np.uint32)
+        r = Result()
+        _check(lib().lv_batch_run_device(self._h, G, _p(goff), n, nnz, d_off, d_col, d_w,
+                                         min_gain, d_assignment, _p(q), _p(lv),
+                                         ctypes.byref(r)))
+        return q[:G].copy(), lv[:G].copy(), r
 
     def _result(self, r: Result) -> RunResult:
         return RunResult(r.modularity, self.assignment(), r.n_communities,

@@ -143,3 +143,22 @@ def test_cli_usage_and_missing_file(tmp_path):
     r = subprocess.run([cli, "-f", "x", "-g", "abc"], capture_output=True, text=True)
     assert r.returncode == 1
     assert r.stdout.strip() == "-g option invalid argument: stof"
+
+
+def test_pack_graphs_block_diagonal():
+    """The batched input layout: graph g's rows and column ids are shifted
+    by its vertex offset, entry order kept."""
+    parts = [lvgen.two_cliques_bridge(4), lvgen.star(7), (3, np.zeros(0), np.zeros(0),
+                                                          np.zeros(0, np.float32))]
+    csrs = [(n,) + tuple(lvgen.csr_from_edges(n, s, d, w)) for n, s, d, w in parts]
+    goff, off, col, w = lvb200.pack_graphs(csrs)
+    assert goff.tolist() == [0, 8, 16, 19]
+    assert off[-1] == len(col) == sum(len(c[2]) for c in csrs)
+    for g, (n, o, c, x) in enumerate(csrs):
+        vb = int(goff[g])
+        rows = off[vb:vb + n + 1] - off[vb]
+        assert np.array_equal(rows, o - o[0])
+        seg = slice(int(off[vb]), int(off[vb + n]))
+        assert np.array_equal(col[seg], c.astype(np.uint32) + vb)
+        assert np.array_equal(w[seg], x)
+        assert (col[seg] >= vb).all() and (col[seg] < vb + n).all()
