@@ -228,6 +228,13 @@ struct lv_engine {
   size_t graph_cap = 0;
   uint32_t* batch_out = nullptr;  // local assignment of lv_batch_run
   size_t batch_out_cap = 0;
+  // per-pass lists of the vertices of graphs still moving (classes 1..7;
+  // class 8 copied once per level), their lengths, and the runs' places
+  uint32_t* act_order = nullptr;
+  size_t act_order_cap = 0;
+  uint32_t* act_cnt = nullptr;  // [16]
+  uint32_t* cg = nullptr;       // [kMoveClasses * (graph cap + 1)]
+  uint32_t* cg_new = nullptr;
 
   // all passes of the current level as one graph (WHILE node)
   cudaGraphExec_t level_exec = nullptr;
@@ -546,12 +553,11 @@ lv_status prepare_level(lv_engine* E) {
   P.hub_blocks = (uint32_t)blk_vertex.size();
   E->hub.units = (uint32_t)unit_vertex.size();
   // dispatch units per class
-  const uint32_t per_unit[kClasses] = {0, 64, 32, 16, 8, 8, 8, 1, 0};
   uint32_t u = 0;
   for (int c = 1; c <= 7; c++) {
     P.blk_start[c] = u;
     const uint32_t cnt = P.cls_start[c + 1] - P.cls_start[c];
-    u += (cnt + per_unit[c] - 1) / per_unit[c];
+    u += (cnt + class_per_unit(c) - 1) / class_per_unit(c);
   }
   P.blk_start[8] = u;
   u += P.hub_blocks;
@@ -595,6 +601,14 @@ lv_status prepare_level(lv_engine* E) {
     CU(cudaMemsetAsync(E->hub.best, 0, hc * sizeof(unsigned long long), st));
     CU(cudaMemsetAsync(E->hub.own, 0, hc * sizeof(double), st));
     CU(cudaMemsetAsync(E->partials, 0, hc * sizeof(double), st));
+  }
+  if (E->batch) {
+    // batched form: where each graph's run starts in every class list; the
+    // hub list is never compacted
+    CU(launch_class_graph_starts(E->order, P, E->goff_dev, E->n_graphs, E->cg, st));
+    if (hc)
+      CU(cudaMemcpyAsync(E->act_order + hs, E->order + hs, hc * sizeof(uint32_t),
+                         cudaMemcpyDeviceToDevice, st));
   }
   // entries per move class (byte counts of the kernel timings)
   if (!E->d_class_deg) CU(dalloc(&E->d_class_deg, kClasses));
@@ -731,6 +745,15 @@ lv_status issue_pass(lv_engine* E, const PassControl* ctl) {
   const LevelView L = E->view();
   const int rule = (E->cfg.rule == LV_RULE_CUDA) ? LV_RULE_CUDA_I : LV_RULE_PY_I;
   HubArena H = E->hub;
+  // batched form: this pass visits only the graphs still moving
+  const uint32_t* ord = E->order;
+  const uint32_t* ac = nullptr;
+  if (E->batch) {
+    CU(launch_compact_active(E->order, E->plan, E->cg, E->cg_new, E->gs, E->n_graphs,
+                             E->act_cnt, E->act_order, E->st));
+    ord = E->act_order;
+    ac = E->act_cnt;
+  }
   for (int b = 1; b <= kBuckets; b++) {
     const uint32_t s = E->plan.cls_start[b];
     const uint32_t e = (b == 7) ? E->plan.cls_start[9] : E->plan.cls_start[b + 1];
@@ -740,21 +763,21 @@ lv_status issue_pass(lv_engine* E, const PassControl* ctl) {
     const double vb = (double)(e - s);
     const double v7 = (double)(E->plan.cls_start[b + 1] - s);
     cudaEvent_t t0 = prof_begin(E);
-    CU(launch_move_bucket(L, b, rule, E->order, E->prop, E->plan, H, E->st));
+    CU(launch_move_bucket(L, b, rule, ord, E->prop, E->plan, H, E->st, ac));
     prof_end(E, t0, K_MOVE1 + b - 1, (double)E->class_deg[b] * 12.0 + v7 * 32.0);
     if (b == 7 && E->plan.hub_count) {
       t0 = prof_begin(E);
-      CU(launch_move_bucket(L, 8, rule, E->order, E->prop, E->plan, H, E->st));
+      CU(launch_move_bucket(L, 8, rule, ord, E->prop, E->plan, H, E->st, ac));
       prof_end(E, t0, K_HUB,
                (double)E->class_deg[8] * 12.0 + (double)E->plan.hub_count * 32.0);
     }
     t0 = prof_begin(E);
-    CU(launch_apply_bucket(L, b, E->order, E->prop, E->plan, E->st));
+    CU(launch_apply_bucket(L, b, ord, E->prop, E->plan, E->st, ac));
     prof_end(E, t0, K_APPLY, vb * 12.0);
   }
   cudaEvent_t t0 = prof_begin(E);
-  CU(launch_modularity(L, E->order, E->plan, E->plan.hub_count ? E->hub_map : nullptr,
-                       E->partials, E->st, ctl));
+  CU(launch_modularity(L, ord, E->plan, E->plan.hub_count ? E->hub_map : nullptr,
+                       E->partials, E->st, ctl, ac));
   prof_end(E, t0, K_MODULARITY, (double)E->e * 12.0 + (double)E->n * 24.0);
   return LV_OK;
 }
@@ -804,8 +827,14 @@ lv_status batch_alloc(lv_engine* E, uint32_t G) {
   dfree(E->goff_dev);
   dfree(E->gbase);
   dfree(E->gdrop);
+  dfree(E->cg);
+  dfree(E->cg_new);
+  dfree(E->act_cnt);
   if (E->gs_host) cudaFreeHost(E->gs_host);
   E->gs_host = nullptr;
+  CU(dalloc(&E->cg, (size_t)kMoveClasses * (G + 1)));
+  CU(dalloc(&E->cg_new, (size_t)kMoveClasses * (G + 1)));
+  CU(dalloc(&E->act_cnt, 16));
   CU(dalloc(&E->gs, G));
   CU(dalloc(&E->goff_dev, (size_t)G + 1));
   CU(dalloc(&E->gbase, G));
@@ -858,6 +887,11 @@ static lv_status batch_run(lv_engine* E, uint32_t G, const uint64_t* goff_in,
   LVTRY(batch_alloc(E, G));
   cudaStream_t st = E->st;
   const uint32_t n0 = E->n0;
+  if (n0 > E->act_order_cap) {
+    dfree(E->act_order);
+    CU(dalloc(&E->act_order, n0));
+    E->act_order_cap = n0;
+  }
   // level-0 graph list and input-vertex -> graph map
   std::vector<uint32_t> goff(G + 1), ids(G);  // level offsets, level -> input graph
   for (uint32_t g = 0; g <= G; g++) goff[g] = (uint32_t)goff_in[g];
@@ -1092,6 +1126,10 @@ void lv_engine_destroy(lv_engine* E) {
   dfree(E->gbase);
   dfree(E->gdrop);
   dfree(E->batch_out);
+  dfree(E->act_order);
+  dfree(E->cg);
+  dfree(E->cg_new);
+  dfree(E->act_cnt);
   if (E->gs_host) cudaFreeHost(E->gs_host);
   prof_collect(E);
   for (cudaEvent_t ev : E->ev_free) cudaEventDestroy(ev);

@@ -133,6 +133,19 @@ struct LevelView {
 
 // Work partition of a level for the "class dispatch" kernels (row sums and
 // the modularity sweep): consecutive block ranges serve consecutive classes.
+constexpr int kMoveClasses = 7;  // classes 1..7 (class 8, hubs, is never compacted)
+
+// Vertices per dispatch unit (a 256-thread block's share) of classes 1..7:
+// G-lane groups for classes 1-4, a warp per vertex for 5-6, a block for 7.
+__host__ __device__ constexpr uint32_t class_per_unit(int c) {
+  return c <= 4 ? (256u >> (c + 1)) : (c <= 6 ? 8u : 1u);
+}
+
+// Class offsets of the vertex order, passed to kernels by value.
+struct ClassStarts {
+  uint32_t s[kClasses + 1];
+};
+
 struct DispatchPlan {
   uint32_t cls_start[kClasses + 1];   // order[] offsets per class
   uint32_t blk_start[kClasses + 1];   // first block of each class (1..8)
@@ -187,10 +200,14 @@ cudaError_t launch_level_init(const LevelView& L, const uint32_t* order,
 // Modularity of the current state into sc->q (FP64, deterministic).  With
 // ctl->enabled the last block also applies the pass stop rule and sets the
 // graph condition.
+// With act_cnt (batched form) classes 1..7 of `order` are the compacted
+// active lists and act_cnt[c] their device-side lengths; every graph's
+// modularity then comes from its own vertices' rows and totals.
 cudaError_t launch_modularity(const LevelView& L, const uint32_t* order,
                               const DispatchPlan& P, const uint32_t* hub_map,
                               double* partials, cudaStream_t st,
-                              const PassControl* ctl = nullptr);
+                              const PassControl* ctl = nullptr,
+                              const uint32_t* act_cnt = nullptr);
 // passes = 0, first_fail = 0, q_prev = q (start of a level's pass loop),
 // for the single graph and for every graph of a batch
 cudaError_t launch_pass_control_init(LevelScalars* sc, GraphState* gs,
@@ -213,14 +230,27 @@ constexpr uint32_t kHubPartKeys = 4096;
 // Proposals for the vertices of kernel class c (1..8; bucket 7 is classes 7
 // and 8, both launched before its apply).  proposal[] is parallel to
 // order[].
+// act_cnt: as for launch_modularity (null: whole classes).
 cudaError_t launch_move_bucket(const LevelView& L, int bucket, int rule,
                                const uint32_t* order, uint32_t* proposal,
                                const DispatchPlan& P, const HubArena& H,
-                               cudaStream_t st);
+                               cudaStream_t st, const uint32_t* act_cnt = nullptr);
 cudaError_t launch_apply_bucket(const LevelView& L, int bucket,
                                 const uint32_t* order,
                                 const uint32_t* proposal,
-                                const DispatchPlan& P, cudaStream_t st);
+                                const DispatchPlan& P, cudaStream_t st,
+                                const uint32_t* act_cnt = nullptr);
+// Batched form.  cg[(c-1)*(G+1) + g] = first index of class c's list
+// holding a vertex of graph g (goff: the G+1 graph offsets of the level).
+cudaError_t launch_class_graph_starts(const uint32_t* order, const DispatchPlan& P,
+                                      const uint32_t* goff, uint32_t G, uint32_t* cg,
+                                      cudaStream_t st);
+// Compacted lists of classes 1..7 holding only the vertices of graphs
+// still active (same class offsets as order), lengths into act_cnt[1..7].
+cudaError_t launch_compact_active(const uint32_t* order, const DispatchPlan& P,
+                                  const uint32_t* cg, uint32_t* cg_new, const GraphState* gs,
+                                  uint32_t G, uint32_t* act_cnt, uint32_t* act_order,
+                                  cudaStream_t st);
 // assignment[i] = map[assignment[i]]
 cudaError_t launch_compose(uint32_t* assignment, size_t n0,
                            const uint32_t* map, cudaStream_t st);

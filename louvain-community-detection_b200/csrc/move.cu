@@ -46,6 +46,8 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+static_assert(class_per_unit(1) * 4 == kThreads && class_per_unit(5) == kWarps,
+              "dispatch units assume 256-thread blocks");
 // shared tables: FP64 values + u32 keys + u16 list of taken slots
 constexpr int kSlotBytes = 14;
 constexpr int kHubPartSmem = kHubPartSlots * kSlotBytes;
@@ -150,6 +152,28 @@ __device__ __forceinline__ double group_sum(double x) {
   return x;
 }
 
+// Batched form: adds every lane's val into gs[key].*field with one atomic
+// per run of equal keys.  Called by all 32 lanes; keys must be
+// non-decreasing across the lanes (vertex ids ascend within a class order,
+// and graphs own contiguous id ranges), a lane without a value passes
+// kNoGraph.  A segmented suffix sum leaves each run's total in its first
+// lane.
+constexpr uint32_t kNoGraph = 0xFFFFFFFFu;
+using GraphField = double GraphState::*;
+__device__ __forceinline__ void warp_graph_add(GraphState* gs, GraphField field, uint32_t key,
+                                               double val) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double ov = __shfl_down_sync(kFull, val, o);
+    const uint32_t ok = __shfl_down_sync(kFull, key, o);
+    if (lane + o < 32 && ok == key) val += ov;
+  }
+  const uint32_t pk = __shfl_up_sync(kFull, key, 1);
+  if (key != kNoGraph && (lane == 0 || pk != key) && val != 0.0)
+    atomicAdd(&(gs[key].*field), val);
+}
+
 // Open addressing with linear probing; multiplicative hash.  Probe counts
 // are bounded by the table size; a full table (impossible while a table
 // holds more slots than the row has entries) sets the error flag.
@@ -199,7 +223,9 @@ __device__ __forceinline__ uint32_t table_insert_fresh(uint32_t* keys, uint32_t 
 template <int G, int RULE>
 __global__ void __launch_bounds__(kThreads)
     move_small_kernel(LevelView L, const uint32_t* __restrict__ verts,
-                      uint32_t count, uint32_t* __restrict__ prop) {
+                      uint32_t count, uint32_t* __restrict__ prop,
+                      const uint32_t* __restrict__ dcnt) {
+  if (dcnt) count = *dcnt;  // batched form: active vertices of the class
   __shared__ double sums[kWarps][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int gl = lane & (G - 1);
@@ -298,7 +324,9 @@ __device__ __forceinline__ unsigned long long scan_fresh_and_clear(
 template <int T, int MAXW, int RULE>
 __global__ void __launch_bounds__(kThreads)
     move_warp_kernel(LevelView L, const uint32_t* __restrict__ verts,
-                     uint32_t count, uint32_t* __restrict__ prop) {
+                     uint32_t count, uint32_t* __restrict__ prop,
+                      const uint32_t* __restrict__ dcnt) {
+  if (dcnt) count = *dcnt;  // batched form: active vertices of the class
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t n_fresh_sm[kWarps];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -454,7 +482,9 @@ __device__ __forceinline__ void insert_block_range(const LevelView& L, uint64_t 
 template <int RULE>
 __global__ void __launch_bounds__(kThreads)
     move_block_kernel(LevelView L, const uint32_t* __restrict__ verts,
-                      uint32_t count, uint32_t* __restrict__ prop) {
+                      uint32_t count, uint32_t* __restrict__ prop,
+                      const uint32_t* __restrict__ dcnt) {
+  if (dcnt) count = *dcnt;  // batched form: active vertices of the class
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int T = kHubSmemSlots;
   constexpr int MAXW = (int)(kHubSmemMaxDeg / kThreads);
@@ -607,7 +637,9 @@ __global__ void hub_decide_kernel(LevelView L, const uint32_t* __restrict__ hubs
 // Applies a bucket's proposals (assignCommunity + incremental totals).
 __global__ void __launch_bounds__(kThreads)
     apply_kernel(LevelView L, const uint32_t* __restrict__ verts,
-                 const uint32_t* __restrict__ prop, uint32_t count) {
+                 const uint32_t* __restrict__ prop, uint32_t count,
+                 const uint32_t* __restrict__ dcnt) {
+  if (dcnt) count = *dcnt;
   for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < count;
        i += gridDim.x * kThreads) {
     const uint32_t v = verts[i];
@@ -634,21 +666,25 @@ struct DispatchArgs {
   const uint32_t* hub_blk_chunk;
   double* hub_acc;
   double* partials;  // [2 * gridDim.x]
+  const uint32_t* act_cnt;  // batched form: active lengths of classes 1..7
 };
 
-// Row sum: k_v = (float) sum_j w_vj.
+// Row sum: k_v = (float) sum_j w_vj.  vertex() returns the vertex's share
+// of its graph's accumulator (batched form).
 struct RowSumOp {
+  static constexpr GraphField kField = &GraphState::m_acc;
+  static constexpr bool kAsq = false;
   __device__ uint32_t ctx(const LevelView&, uint32_t) const { return 0; }
   __device__ double edge(const LevelView&, uint32_t, uint32_t, float w) const {
     return (double)w;
   }
-  __device__ void vertex(const LevelView& L, uint32_t v, double sum,
-                         double& part) const {
+  __device__ double vertex(const LevelView& L, uint32_t v, double sum,
+                           double& part) const {
     const float kf = (float)sum;
     L.k[v] = kf;
     L.tot[v] = (double)kf;
     part += (double)kf;
-    if (L.gid && kf != 0.0f) atomicAdd(&L.gs[L.gid[v]].m_acc, (double)kf);
+    return (double)kf;
   }
   __device__ void hub(const LevelView&, const DispatchArgs& A, uint32_t hi, uint32_t,
                       double sum, double&) const {
@@ -658,6 +694,10 @@ struct RowSumOp {
 
 // Intra-community weight: sum_j w_vj [comm(u) == comm(v)].
 struct IntraOp {
+  static constexpr GraphField kField = &GraphState::intra_acc;
+  // batched form: the vertex's community total squared (community ids are
+  // vertex ids), so an active graph's sum of a_c^2 comes with its rows
+  static constexpr bool kAsq = true;
   __device__ uint32_t ctx(const LevelView& L, uint32_t v) const {
     return L.comm[v];
   }
@@ -665,10 +705,9 @@ struct IntraOp {
                          float w) const {
     return L.comm[u] == cv ? (double)w : 0.0;
   }
-  __device__ void vertex(const LevelView& L, uint32_t v, double sum,
-                         double& part) const {
+  __device__ double vertex(const LevelView&, uint32_t, double sum, double& part) const {
     part += sum;
-    if (L.gid && sum != 0.0) atomicAdd(&L.gs[L.gid[v]].intra_acc, sum);
+    return sum;
   }
   __device__ void hub(const LevelView& L, const DispatchArgs&, uint32_t, uint32_t v,
                       double sum, double& part) const {
@@ -677,14 +716,34 @@ struct IntraOp {
   }
 };
 
+__device__ __forceinline__ double sq(double a) { return a * a; }
+
+// Length of class cls's list: the active length in the batched form's
+// compacted lists, else the whole class.
+__device__ __forceinline__ uint32_t class_count(const DispatchArgs& A, int cls) {
+  return A.act_cnt ? A.act_cnt[cls] : A.P.cls_start[cls + 1] - A.P.cls_start[cls];
+}
+
+// Batched form, one lane for one vertex: its share of its graph's
+// accumulator (and its community total squared for the sweep).
+template <class Op>
+__device__ __forceinline__ void graph_add_one(const LevelView& L, uint32_t v, double share) {
+  GraphState& s = L.gs[L.gid[v]];
+  if (share != 0.0) atomicAdd(&(s.*Op::kField), share);
+  if (Op::kAsq) {
+    const double a = L.tot[v];
+    if (a != 0.0) atomicAdd(&s.asq_acc, a * a);
+  }
+}
+
 template <int G, class Op>
 __device__ __forceinline__ void unit_small(const LevelView& L,
                                            const DispatchArgs& A, int cls,
                                            uint32_t unit, const Op& op,
                                            double& part) {
   const int lane = threadIdx.x & 31, gl = lane & (G - 1);
-  const uint32_t cnt = A.P.cls_start[cls + 1] - A.P.cls_start[cls];
-  const uint32_t idx = (unit - A.P.blk_start[cls]) * (kThreads / G) + threadIdx.x / G;
+  const uint32_t cnt = class_count(A, cls);
+  const uint32_t idx = unit * (kThreads / G) + threadIdx.x / G;
   double x = 0.0;
   uint32_t v = 0;
   if (idx < cnt) {
@@ -697,7 +756,16 @@ __device__ __forceinline__ void unit_small(const LevelView& L,
     }
   }
   x = group_sum<G>(x);
-  if (idx < cnt && gl == 0) op.vertex(L, v, x, part);
+  double share = 0.0, a2 = 0.0;
+  if (idx < cnt && gl == 0) {
+    share = op.vertex(L, v, x, part);
+    if (Op::kAsq && L.gid) a2 = sq(L.tot[v]);
+  }
+  if (L.gid) {  // warp-uniform
+    const uint32_t key = idx < cnt ? L.gid[v] : kNoGraph;
+    warp_graph_add(L.gs, Op::kField, key, share);
+    if (Op::kAsq) warp_graph_add(L.gs, &GraphState::asq_acc, key, a2);
+  }
 }
 
 template <class Op>
@@ -706,8 +774,8 @@ __device__ __forceinline__ void unit_warp(const LevelView& L,
                                           uint32_t unit, const Op& op,
                                           double& part) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const uint32_t cnt = A.P.cls_start[cls + 1] - A.P.cls_start[cls];
-  const uint32_t idx = (unit - A.P.blk_start[cls]) * kWarps + wib;
+  const uint32_t cnt = class_count(A, cls);
+  const uint32_t idx = unit * kWarps + wib;
   if (idx >= cnt) return;  // warp-uniform
   const uint32_t v = A.order[A.P.cls_start[cls] + idx];
   const uint64_t s = L.off[v];
@@ -716,7 +784,10 @@ __device__ __forceinline__ void unit_warp(const LevelView& L,
   double x = 0.0;
   for (uint32_t j = lane; j < d; j += 32) x += op.edge(L, c, L.col[s + j], L.w[s + j]);
   x = group_sum<32>(x);
-  if (lane == 0) op.vertex(L, v, x, part);
+  if (lane == 0) {
+    const double share = op.vertex(L, v, x, part);
+    if (L.gid) graph_add_one<Op>(L, v, share);
+  }
 }
 
 template <class Op>
@@ -724,7 +795,8 @@ __device__ __forceinline__ void unit_block(const LevelView& L,
                                            const DispatchArgs& A,
                                            uint32_t unit, const Op& op,
                                            double& part, double* red) {
-  const uint32_t idx = unit - A.P.blk_start[7];
+  const uint32_t idx = unit;
+  if (idx >= class_count(A, 7)) return;  // block-uniform
   const uint32_t v = A.order[A.P.cls_start[7] + idx];
   const uint64_t s = L.off[v];
   const uint32_t d = (uint32_t)(L.off[v + 1] - s);
@@ -733,7 +805,10 @@ __device__ __forceinline__ void unit_block(const LevelView& L,
   for (uint32_t j = threadIdx.x; j < d; j += kThreads)
     x += op.edge(L, c, L.col[s + j], L.w[s + j]);
   x = block_sum(x, red);
-  if (threadIdx.x == 0) op.vertex(L, v, x, part);
+  if (threadIdx.x == 0) {
+    const double share = op.vertex(L, v, x, part);
+    if (L.gid) graph_add_one<Op>(L, v, share);
+  }
 }
 
 template <class Op>
@@ -741,9 +816,11 @@ __device__ __forceinline__ void unit_hub(const LevelView& L,
                                          const DispatchArgs& A, uint32_t unit,
                                          const Op& op, double& part,
                                          double* red) {
-  const uint32_t hb = unit - A.P.blk_start[8];
+  const uint32_t hb = unit;
   const uint32_t hi = A.hub_blk_vertex[hb], ch = A.hub_blk_chunk[hb];
   const uint32_t v = A.order[A.P.cls_start[8] + hi];
+  // batched pass loop: a finished graph's hubs need no sweep (block-uniform)
+  if (A.act_cnt && !L.gs[L.gid[v]].active) return;
   const uint64_t s = L.off[v];
   const uint64_t d = L.off[v + 1] - s;
   const uint64_t lo = (uint64_t)ch * kHubChunk, end = min(d, lo + kHubChunk);
@@ -752,7 +829,11 @@ __device__ __forceinline__ void unit_hub(const LevelView& L,
   for (uint64_t j = lo + threadIdx.x; j < end; j += kThreads)
     x += op.edge(L, c, L.col[s + j], L.w[s + j]);
   x = block_sum(x, red);
-  if (threadIdx.x == 0) op.hub(L, A, hi, v, x, part);
+  if (threadIdx.x == 0) {
+    op.hub(L, A, hi, v, x, part);
+    if (Op::kAsq && L.gid && ch == 0 && L.tot[v] != 0.0)
+      atomicAdd(&L.gs[L.gid[v]].asq_acc, sq(L.tot[v]));
+  }
 }
 
 // Deterministic block reduction into partials, then the last block to
@@ -787,23 +868,43 @@ __device__ __forceinline__ void sum_partials(const DispatchArgs& A, double* red,
   b = block_sum(y, red);
 }
 
+// Units of the class lists, grid-strided.  Every unit function gets its
+// unit's index within the class.  With act_cnt (batched pass loop) the
+// classes 1..7 hold only their active prefix, so the unit ranges are
+// derived from the device-side lengths and finished graphs cost nothing.
 template <class Op>
 __device__ __forceinline__ void dispatch_units(const LevelView& L,
                                                const DispatchArgs& A,
                                                const Op& op, double& part,
                                                double* red) {
-  for (uint32_t unit = blockIdx.x; unit < A.P.total_blocks; unit += gridDim.x) {
+  __shared__ uint32_t bs[kClasses + 1];
+  if (threadIdx.x == 0) {
+    if (A.act_cnt) {
+      bs[0] = bs[1] = 0u;
+      for (int c = 1; c <= kMoveClasses; c++) {
+        const uint32_t pu = class_per_unit(c);
+        bs[c + 1] = bs[c] + (A.act_cnt[c] + pu - 1) / pu;
+      }
+      bs[9] = bs[8] + A.P.hub_blocks;
+    } else {
+      for (int c = 0; c <= kClasses; c++) bs[c] = A.P.blk_start[c];
+    }
+  }
+  __syncthreads();
+  const uint32_t total = bs[9];
+  for (uint32_t unit = blockIdx.x; unit < total; unit += gridDim.x) {
     int cls = 8;
-    while (cls > 1 && unit < A.P.blk_start[cls]) cls--;
+    while (cls > 1 && unit < bs[cls]) cls--;
+    const uint32_t u = unit - bs[cls];
     switch (cls) {  // block-uniform
-      case 1: unit_small<4>(L, A, 1, unit, op, part); break;
-      case 2: unit_small<8>(L, A, 2, unit, op, part); break;
-      case 3: unit_small<16>(L, A, 3, unit, op, part); break;
-      case 4: unit_small<32>(L, A, 4, unit, op, part); break;
+      case 1: unit_small<4>(L, A, 1, u, op, part); break;
+      case 2: unit_small<8>(L, A, 2, u, op, part); break;
+      case 3: unit_small<16>(L, A, 3, u, op, part); break;
+      case 4: unit_small<32>(L, A, 4, u, op, part); break;
       case 5:
-      case 6: unit_warp(L, A, cls, unit, op, part); break;
-      case 7: unit_block(L, A, unit, op, part, red); break;
-      default: unit_hub(L, A, unit, op, part, red); break;
+      case 6: unit_warp(L, A, cls, u, op, part); break;
+      case 7: unit_block(L, A, u, op, part, red); break;
+      default: unit_hub(L, A, u, op, part, red); break;
     }
   }
 }
@@ -871,11 +972,11 @@ __global__ void __launch_bounds__(kThreads)
   const uint32_t c0 = blockIdx.x * chunk;
   const uint32_t c1 = min(L.n, c0 + chunk);
   double asq = 0.0;
-  for (uint32_t c = c0 + threadIdx.x; c < c1; c += kThreads) {
-    const double a = L.tot[c];
-    asq += a * a;
-    // community ids are vertex ids, so community c belongs to gid[c]
-    if (L.gid && a != 0.0) atomicAdd(&L.gs[L.gid[c]].asq_acc, a * a);
+  if (!L.gid) {  // the batched form summed a_c^2 with the rows above
+    for (uint32_t c = c0 + threadIdx.x; c < c1; c += kThreads) {
+      const double a = L.tot[c];
+      asq += a * a;
+    }
   }
   if (!publish_and_check_last(part, asq, A, L.sc, red)) return;
   double intra, sq;
@@ -1084,6 +1185,7 @@ DispatchArgs make_args(const uint32_t* order, const DispatchPlan& P,
   A.hub_blk_chunk = hub_map ? hub_map + P.hub_blocks : nullptr;
   A.hub_acc = partials;  // first hub_count doubles; partials follow
   A.partials = partials + P.hub_count;
+  A.act_cnt = nullptr;
   return A;
 }
 
@@ -1139,8 +1241,9 @@ cudaError_t launch_level_init(const LevelView& L, const uint32_t* order,
 cudaError_t launch_modularity(const LevelView& L, const uint32_t* order,
                               const DispatchPlan& P, const uint32_t* hub_map,
                               double* partials, cudaStream_t st,
-                              const PassControl* ctl) {
+                              const PassControl* ctl, const uint32_t* act_cnt) {
   DispatchArgs A = make_args(order, P, hub_map, partials);
+  A.act_cnt = act_cnt;
   PassControl c{};
   if (ctl) c = *ctl;
   (count_launches(1), modularity_kernel<<<dispatch_grid(P), kThreads, 0, st>>>(L, A, c));
@@ -1158,43 +1261,46 @@ template <int RULE>
 static cudaError_t move_bucket_impl(const LevelView& L, int bucket,
                                     const uint32_t* order, uint32_t* prop,
                                     const DispatchPlan& P, const HubArena& H,
-                                    cudaStream_t st) {
+                                    const uint32_t* act_cnt, cudaStream_t st) {
   const unsigned cap = sm_count() * 8;
   const uint32_t s = P.cls_start[bucket];
   const uint32_t cnt = P.cls_start[bucket + 1] - s;
   const uint32_t* verts = order + s;
   uint32_t* pr = prop + s;
+  // grids are sized for the whole class; with act_cnt the kernels read the
+  // active count and their grid-stride loops end early
+  const uint32_t* dc = (act_cnt && bucket <= 7) ? act_cnt + bucket : nullptr;
   switch (bucket) {
     case 1:
-      if (cnt) (count_launches(1), move_small_kernel<4, RULE><<<grid_for((cnt + 63) / 64, cap), kThreads, 0, st>>>(L, verts, cnt, pr));
+      if (cnt) (count_launches(1), move_small_kernel<4, RULE><<<grid_for((cnt + 63) / 64, cap), kThreads, 0, st>>>(L, verts, cnt, pr, dc));
       break;
     case 2:
-      if (cnt) (count_launches(1), move_small_kernel<8, RULE><<<grid_for((cnt + 31) / 32, cap), kThreads, 0, st>>>(L, verts, cnt, pr));
+      if (cnt) (count_launches(1), move_small_kernel<8, RULE><<<grid_for((cnt + 31) / 32, cap), kThreads, 0, st>>>(L, verts, cnt, pr, dc));
       break;
     case 3:
-      if (cnt) (count_launches(1), move_small_kernel<16, RULE><<<grid_for((cnt + 15) / 16, cap), kThreads, 0, st>>>(L, verts, cnt, pr));
+      if (cnt) (count_launches(1), move_small_kernel<16, RULE><<<grid_for((cnt + 15) / 16, cap), kThreads, 0, st>>>(L, verts, cnt, pr, dc));
       break;
     case 4:
-      if (cnt) (count_launches(1), move_small_kernel<32, RULE><<<grid_for((cnt + 7) / 8, cap), kThreads, 0, st>>>(L, verts, cnt, pr));
+      if (cnt) (count_launches(1), move_small_kernel<32, RULE><<<grid_for((cnt + 7) / 8, cap), kThreads, 0, st>>>(L, verts, cnt, pr, dc));
       break;
     case 5:
       if (cnt) {
         constexpr int T = 128;
         (count_launches(1), move_warp_kernel<T, 3, RULE><<<grid_for((cnt + 7) / 8, cap), kThreads,
-                                    kWarps * T * kSlotBytes, st>>>(L, verts, cnt, pr));
+                                    kWarps * T * kSlotBytes, st>>>(L, verts, cnt, pr, dc));
       }
       break;
     case 6:
       if (cnt) {
         constexpr int T = 512;
         (count_launches(1), move_warp_kernel<T, 10, RULE><<<grid_for((cnt + 7) / 8, sm_count() * 4), kThreads,
-                                    kWarps * T * kSlotBytes, st>>>(L, verts, cnt, pr));
+                                    kWarps * T * kSlotBytes, st>>>(L, verts, cnt, pr, dc));
       }
       break;
     case 7:  // class 7 of bucket 7: shared table, one block per vertex
       if (cnt) {
         (count_launches(1), move_block_kernel<RULE><<<grid_for(cnt, sm_count() * 4), kThreads,
-                                  kBlockTabSmem, st>>>(L, verts, cnt, pr));
+                                  kBlockTabSmem, st>>>(L, verts, cnt, pr, dc));
       }
       break;
     case 8: {  // class 8 of bucket 7: one block per (hub, partition)
@@ -1217,22 +1323,148 @@ static cudaError_t move_bucket_impl(const LevelView& L, int bucket,
 cudaError_t launch_move_bucket(const LevelView& L, int bucket, int rule,
                                const uint32_t* order, uint32_t* proposal,
                                const DispatchPlan& P, const HubArena& H,
-                               cudaStream_t st) {
+                               cudaStream_t st, const uint32_t* act_cnt) {
   if (rule == LV_RULE_CUDA_I)
-    return move_bucket_impl<LV_RULE_CUDA_I>(L, bucket, order, proposal, P, H, st);
-  return move_bucket_impl<LV_RULE_PY_I>(L, bucket, order, proposal, P, H, st);
+    return move_bucket_impl<LV_RULE_CUDA_I>(L, bucket, order, proposal, P, H, act_cnt, st);
+  return move_bucket_impl<LV_RULE_PY_I>(L, bucket, order, proposal, P, H, act_cnt, st);
 }
 
 cudaError_t launch_apply_bucket(const LevelView& L, int bucket,
                                 const uint32_t* order,
                                 const uint32_t* proposal,
-                                const DispatchPlan& P, cudaStream_t st) {
+                                const DispatchPlan& P, cudaStream_t st,
+                                const uint32_t* act_cnt) {
   const uint32_t s = P.cls_start[bucket];
-  const uint32_t e = (bucket == 7) ? P.cls_start[9] : P.cls_start[bucket + 1];
+  // bucket 7 applies classes 7 and 8 (hubs); with compacted lists class 7's
+  // active part and the hubs are not adjacent, so they go separately
+  const bool split = act_cnt && bucket == 7;
+  const uint32_t e = (bucket == 7 && !split) ? P.cls_start[9] : P.cls_start[bucket + 1];
   const uint32_t cnt = e - s;
-  if (!cnt) return cudaSuccess;
-  (count_launches(1), apply_kernel<<<grid_for((cnt + kThreads - 1) / kThreads, sm_count() * 8), kThreads, 0, st>>>(
-      L, order + s, proposal + s, cnt));
+  const unsigned cap = sm_count() * 8;
+  if (cnt)
+    (count_launches(1), apply_kernel<<<grid_for((cnt + kThreads - 1) / kThreads, cap), kThreads, 0, st>>>(
+        L, order + s, proposal + s, cnt, act_cnt ? act_cnt + bucket : nullptr));
+  if (split) {
+    const uint32_t hs = P.cls_start[8], hc = P.cls_start[9] - hs;
+    if (hc)
+      (count_launches(1), apply_kernel<<<grid_for((hc + kThreads - 1) / kThreads, cap), kThreads, 0, st>>>(
+          L, order + hs, proposal + hs, hc, nullptr));
+  }
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Batched form: per-pass lists of the vertices whose graph still moves.
+// A class list is ascending in vertex id and a graph owns a contiguous id
+// range, so graph g's vertices form one run of every class list; the
+// compacted list keeps the runs of active graphs in order.
+// ---------------------------------------------------------------------------
+__global__ void class_graph_starts_kernel(const uint32_t* __restrict__ order, ClassStarts cs,
+                                          const uint32_t* __restrict__ goff, uint32_t G,
+                                          uint32_t* __restrict__ cg) {
+  const uint32_t per = G + 1;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < kMoveClasses * per;
+       t += gridDim.x * blockDim.x) {
+    const uint32_t c = 1 + t / per, g = t % per;
+    const uint32_t* list = order + cs.s[c];
+    const uint32_t n = cs.s[c + 1] - cs.s[c];
+    const uint32_t key = goff[g];
+    uint32_t lo = 0, hi = n;  // first index with list[i] >= key
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (list[mid] < key) lo = mid + 1; else hi = mid;
+    }
+    cg[t] = lo;
+  }
+}
+
+// One block per class: exclusive scan over graphs of the active run
+// lengths -> each active run's place in the compacted list, and the
+// class's active count.
+__global__ void __launch_bounds__(1024)
+    compact_scan_kernel(const uint32_t* __restrict__ cg, const GraphState* __restrict__ gs,
+                        uint32_t G, uint32_t* __restrict__ cg_new, uint32_t* __restrict__ act_cnt) {
+  __shared__ uint32_t warp_tot[32];
+  __shared__ uint32_t carry;
+  const uint32_t per = G + 1, c = blockIdx.x;
+  const uint32_t* row = cg + c * per;
+  uint32_t* out = cg_new + c * per;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0u;
+  __syncthreads();
+  for (uint32_t b = 0; b < G; b += 1024) {
+    const uint32_t g = b + threadIdx.x;
+    const uint32_t len = (g < G && gs[g].active) ? row[g + 1] - row[g] : 0u;
+    uint32_t x = len;  // inclusive warp scan
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      uint32_t t = warp_tot[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, t, o);
+        if (lane >= o) t += y;
+      }
+      warp_tot[lane] = t;  // inclusive over warps
+    }
+    __syncthreads();
+    const uint32_t before = carry + (wid ? warp_tot[wid - 1] : 0u) + x - len;
+    if (g < G) out[g] = before;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry = before + len;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) act_cnt[1 + c] = carry;
+}
+
+// One warp per (class, graph): copies an active graph's run.
+__global__ void compact_copy_kernel(const uint32_t* __restrict__ order, ClassStarts cs,
+                                    const uint32_t* __restrict__ cg,
+                                    const uint32_t* __restrict__ cg_new,
+                                    const GraphState* __restrict__ gs, uint32_t G,
+                                    uint32_t* __restrict__ act_order) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < kMoveClasses * G;
+       t += warps) {
+    const uint32_t ci = t / G, g = t % G;
+    if (!gs[g].active) continue;  // warp-uniform
+    const uint32_t per = G + 1;
+    const uint32_t a = cg[ci * per + g], e = cg[ci * per + g + 1];
+    const uint32_t base = cs.s[ci + 1];
+    const uint32_t dst = base + cg_new[ci * per + g];
+    for (uint32_t i = a + lane; i < e; i += 32) act_order[dst + (i - a)] = order[base + i];
+  }
+}
+
+cudaError_t launch_class_graph_starts(const uint32_t* order, const DispatchPlan& P,
+                                      const uint32_t* goff, uint32_t G, uint32_t* cg,
+                                      cudaStream_t st) {
+  ClassStarts cs;
+  for (int c = 0; c <= kClasses; c++) cs.s[c] = P.cls_start[c];
+  if (!G) return cudaSuccess;
+  const uint32_t total = kMoveClasses * (G + 1);
+  (count_launches(1), class_graph_starts_kernel<<<grid_for((total + 255) / 256, sm_count() * 8), 256, 0, st>>>(
+      order, cs, goff, G, cg));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_compact_active(const uint32_t* order, const DispatchPlan& P,
+                                  const uint32_t* cg, uint32_t* cg_new, const GraphState* gs,
+                                  uint32_t G, uint32_t* act_cnt, uint32_t* act_order,
+                                  cudaStream_t st) {
+  ClassStarts cs;
+  for (int c = 0; c <= kClasses; c++) cs.s[c] = P.cls_start[c];
+  if (!G) return cudaSuccess;
+  (count_launches(1), compact_scan_kernel<<<kMoveClasses, 1024, 0, st>>>(cg, gs, G, cg_new, act_cnt));
+  const uint32_t warps = kMoveClasses * G;
+  (count_launches(1), compact_copy_kernel<<<grid_for((warps + 7) / 8, sm_count() * 8), 256, 0, st>>>(
+      order, cs, cg, cg_new, gs, G, act_order));
   return cudaGetLastError();
 }
 

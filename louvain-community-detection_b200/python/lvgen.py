@@ -286,6 +286,126 @@ def rmat_device(scale: int, edge_factor: int = 16, a=0.57, b=0.19, c=0.19,
     return n, off, cols, w, n_edges
 
 
+def sbm_batch_sizes(count: int, seed: int = 0, lo: int = 64, hi: int = 65_536,
+                    min_blocks: int = 4, max_blocks: int = 32):
+    """Per-graph vertex and block counts of a batch: sizes log-uniform in
+    [lo, hi], blocks uniform in [min_blocks, max_blocks] (at most n/4)."""
+    rng = np.random.default_rng(seed)
+    n = np.exp(rng.uniform(np.log(lo), np.log(hi + 1), count)).astype(np.int64)
+    n = np.clip(n, lo, hi)
+    b = rng.integers(min_blocks, max_blocks + 1, count)
+    b = np.maximum(1, np.minimum(b, n // 4))
+    return n, b
+
+
+def sbm_batch_device(count: int, seed: int = 0, lo: int = 64, hi: int = 65_536,
+                     mean_deg: float = 16.0, ratio: float = 20.0, wlo: float = 0.5,
+                     whi: float = 1.5, device: str = "cuda"):
+    """`count` stochastic-block-model graphs (sizes from sbm_batch_sizes,
+    equal blocks, p_in/p_out = ratio, mean degree mean_deg, weights
+    U(wlo, whi)) generated on the device (torch) and packed as one
+    block-diagonal union CSR.  Intra-block edges pick a block uniformly and
+    two of its members; inter-block edges a vertex and a member of another
+    block.  Duplicates merged, self-loops dropped.  Returns (goff u64[G+1]
+    numpy, off int64[N+1], col int32[E], w float32[E], n_edges) with the
+    tensors on `device`; graph g owns vertices [goff[g], goff[g+1])."""
+    import torch
+
+    ns, bs = sbm_batch_sizes(count, seed, lo, hi)
+    goff = np.zeros(count + 1, dtype=np.uint64)
+    goff[1:] = np.cumsum(ns)
+    N = int(goff[-1])
+    # expected edge counts per graph
+    s = ns / bs
+    p_out = mean_deg / (ratio * (s - 1) + (ns - s))
+    p_in = ratio * p_out
+    m_in = np.rint(p_in * bs * s * (s - 1) / 2).astype(np.int64)
+    m_out = np.rint(p_out * (ns * (ns - 1) / 2 - bs * s * (s - 1) / 2)).astype(np.int64)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)
+    t_n, t_b = T(ns), T(bs)
+    t_base = T(goff[:-1].astype(np.int64))
+
+    def member(g, blk):
+        # vertex of block blk of graph g; blocks of size n//B, the first
+        # n % B of them one larger
+        q, r = t_n[g] // t_b[g], t_n[g] % t_b[g]
+        start = blk * q + torch.minimum(blk, r)
+        size = q + (blk < r).to(torch.int64)
+        off = (torch.rand(g.numel(), generator=gen, device=device) * size).to(torch.int64)
+        return t_base[g] + start + torch.minimum(off, size - 1)
+
+    gi = torch.repeat_interleave(torch.arange(count, device=device), T(m_in))
+    blk = (torch.rand(gi.numel(), generator=gen, device=device) * t_b[gi]).to(torch.int64)
+    blk = torch.minimum(blk, t_b[gi] - 1)
+    u1, v1 = member(gi, blk), member(gi, blk)
+    go = torch.repeat_interleave(torch.arange(count, device=device), T(m_out))
+    bo = torch.minimum((torch.rand(go.numel(), generator=gen, device=device) * t_b[go])
+                       .to(torch.int64), t_b[go] - 1)
+    shift = 1 + torch.minimum((torch.rand(go.numel(), generator=gen, device=device)
+                               * (t_b[go] - 1)).to(torch.int64),
+                              torch.clamp(t_b[go] - 2, min=0))
+    keep_o = t_b[go] > 1
+    u2 = member(go, bo)
+    v2 = member(go, (bo + shift) % t_b[go])
+    u2, v2 = u2[keep_o], v2[keep_o]
+    src = torch.cat([u1, u2])
+    dst = torch.cat([v1, v2])
+    del u1, v1, u2, v2, gi, blk, go, bo, shift
+    keep = src != dst
+    lo_ = torch.minimum(src, dst)[keep]
+    hi_ = torch.maximum(src, dst)[keep]
+    del src, dst, keep
+    key = torch.unique(lo_ * N + hi_)
+    del lo_, hi_
+    a, b = key // N, key % N
+    del key
+    n_edges = int(a.numel())
+    w1 = torch.rand(n_edges, generator=gen, device=device) * (whi - wlo) + wlo
+    rows = torch.cat([a, b])
+    cols = torch.cat([b, a])
+    ww = torch.cat([w1, w1]).to(torch.float32)
+    del a, b, w1
+    rows, order = torch.sort(rows, stable=True)
+    cols = cols[order].to(torch.int32)
+    ww = ww[order]
+    del order
+    counts = torch.bincount(rows, minlength=N)
+    del rows
+    off = torch.zeros(N + 1, dtype=torch.int64, device=device)
+    off[1:] = torch.cumsum(counts, 0)
+    return goff, off, cols, ww, n_edges
+
+
+def localize_batch(goff, off, col):
+    """Per-graph CSR views of a block-diagonal union, for running the
+    graphs one by one: returns (loff int64[N+G], lcol int32[E]) where graph
+    g's offsets (n_g+1 of them, starting at 0) sit at loff[goff[g]+g:] and
+    its column ids are local (col - goff[g])."""
+    import torch
+
+    G = len(goff) - 1
+    dev = off.device
+    ns = torch.from_numpy((goff[1:] - goff[:-1]).astype(np.int64)).to(dev)
+    gid_v = torch.repeat_interleave(torch.arange(G, device=dev), ns)
+    base_v = torch.from_numpy(goff[:-1].astype(np.int64)).to(dev)
+    N = int(goff[-1])
+    # graph of every entry: gid of its row
+    deg = off[1:] - off[:-1]
+    gid_e = torch.repeat_interleave(gid_v, deg)
+    lcol = (col.to(torch.int64) - base_v[gid_e]).to(torch.int32)
+    del gid_e
+    e0 = off[base_v]  # first entry of each graph
+    loff = torch.empty(N + G, dtype=torch.int64, device=dev)
+    pos = torch.arange(N, device=dev) + gid_v  # row v of graph g at goff[g] + g + local
+    loff[pos] = off[:-1] - e0[gid_v]
+    ends = torch.from_numpy((goff[1:] + np.arange(G, dtype=np.uint64)).astype(np.int64)).to(dev)
+    ends_val = off[torch.from_numpy(goff[1:].astype(np.int64)).to(dev)] - e0
+    loff[ends] = ends_val
+    return loff, lcol
+
+
 def sbm(n: int, blocks: int, mean_deg: float = 16.0, ratio: float = 20.0,
         seed: int = 0, wlo: float = 0.5, whi: float = 1.5):
     """Stochastic block model with equal blocks, p_in/p_out = ratio, mean
