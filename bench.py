@@ -20,6 +20,9 @@ pass's stored adjacency entries / time.
              oracle, FP64, single thread) on the same graph
 N > 1 (torchrun): every rank runs its own replica (the single-graph path
 does not shard); value = edges of all ranks / max-over-ranks time.
+  batched    (N=1) the batched form on 4,096 SBM graphs against the plain
+             engine looped over the same graphs: graphs/s of each, and whether
+             every partition is identical
 --impl reference: the reference's CPU implementation (oracle port) alone.
 """
 from __future__ import annotations
@@ -168,6 +171,80 @@ def cpu_baseline(n, off, col, ww, budget_s=12.0):
             "final_q": q}
 
 
+def batched_measure(stream, count: int, steps: int = 2):
+    """Batched form on the SBM batch workload (count graphs, sizes
+    log-uniform 64..65,536, 4-32 equal blocks, mean degree 16,
+    p_in/p_out = 20, weights U(0.5, 1.5), generated on the device):
+    graphs/s of one batched run (lv_batch_run_device) against the plain
+    engine looped over the same device-resident graphs (lv_run_device per
+    graph), and whether every graph's partition is identical."""
+    import torch
+
+    import lvb200
+
+    goff, off, col, w, n_edges = lvgen.sbm_batch_device(count, seed=0)
+    N, E = int(goff[-1]), int(col.numel())
+    out = torch.zeros(N, dtype=torch.int32, device="cuda")
+    out_plain = torch.zeros(N, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    res = {"workload": "SBM batch", "graphs": count, "n_vertices": N,
+           "n_edges": int(n_edges), "n_entries": E, "sizes": "log-uniform 64..65536",
+           "blocks": "4..32", "mean_degree": 16, "p_in/p_out": 20,
+           "weights": "U(0.5,1.5) FP32", "seed": 0}
+    with torch.cuda.stream(stream):
+        eng = lvb200.Engine(stream=stream.cuda_stream)
+
+        def batch_step():
+            return eng.batch_run_device(goff, N, E, off.data_ptr(), col.data_ptr(),
+                                        w.data_ptr(), MIN_GAIN, out.data_ptr())
+
+        batch_step()  # warm-up: buffers, graph instantiation paths
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            q_b, lv_b, r = batch_step()
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        eng.close()
+        # plain engine looped over the same graphs (local CSR views)
+        loff, lcol = lvgen.localize_batch(goff, off, col)
+        eoff = off[torch.from_numpy(goff.astype(np.int64)).cuda()].cpu().numpy()
+        plain = lvb200.Engine(stream=stream.cuda_stream)
+        q_p = np.zeros(count)
+
+        def one(g):
+            n = int(goff[g + 1] - goff[g])
+            b0, e0, e1 = int(goff[g]), int(eoff[g]), int(eoff[g + 1])
+            return plain.run_device(n, e1 - e0, loff.data_ptr() + 8 * (b0 + g),
+                                    lcol.data_ptr() + 4 * e0, w.data_ptr() + 4 * e0,
+                                    MIN_GAIN, out_plain.data_ptr() + 4 * b0)
+
+        one(int(np.argmax(goff[1:] - goff[:-1])))  # warm-up at the largest size
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for g in range(count):
+            q_p[g] = one(g).modularity
+        b.record(stream)
+        torch.cuda.synchronize()
+        plain_ms = a.elapsed_time(b)
+        plain.close()
+    o1, o2 = out.cpu().numpy(), out_plain.cpu().numpy()
+    batch_ms = min(ms)
+    res.update({
+        "batched_ms": batch_ms, "batched_graphs_per_s": count / (batch_ms / 1000.0),
+        "plain_looped_ms": plain_ms, "plain_looped_graphs_per_s": count / (plain_ms / 1000.0),
+        "speedup": plain_ms / batch_ms,
+        "partitions_identical": bool(np.array_equal(o1, o2)),
+        "max_abs_dq": float(np.max(np.abs(q_b - q_p))),
+        "levels_max": int(lv_b.max()), "mean_q": float(q_b.mean()),
+    })
+    return res
+
+
 def run_reference(args, rank, world):
     n, off, col, ww, desc = workload(args.workload)
     if rank != 0:
@@ -292,6 +369,9 @@ def run_engine(args, rank, world):
             e2e_value = float(t.item())
 
     eng.close()
+    batched = None
+    if world == 1 and args.batch_graphs > 0:
+        batched = batched_measure(stream, args.batch_graphs)
     if rank != 0:
         return
     # roofline of the dominant kernel group
@@ -329,6 +409,8 @@ def run_engine(args, rank, world):
         "kernel_ms": {k: round(v["total_ms"], 4) for k, v in kstats.items()},
         "clocks": clocks.summary(),
     }
+    if batched:
+        line["batched"] = batched
     if cpu:
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind",
                                                     "sample")}
@@ -343,6 +425,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="powerlaw")
+    ap.add_argument("--batch-graphs", type=int, default=4096,
+                    help="graphs of the batched-form measurement (0: skip)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -40,8 +40,13 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kWarpSlots = 256;                 // class W table
-constexpr int kBlockSlots = 8192;               // class B table
+constexpr int kMidSlots = 2048;                 // class B table
+constexpr int kMidSmem = kMidSlots * 12 + kThreads * 16;
+constexpr int kBlockSlots = 8192;               // class B2 table
 constexpr int kBlockSmem = kBlockSlots * 12 + kThreads * 16;
+static_assert(kMergeMidMax * 3 / 2 + 1 <= kMidSlots &&
+                  kMergeBlockMax * 3 / 2 + 1 <= kBlockSlots,
+              "tables keep load factor <= 2/3");
 
 __device__ __forceinline__ uint32_t hash_slot(uint32_t key, uint32_t mask) {
   return (key * 2654435761u) & mask;
@@ -70,6 +75,25 @@ __device__ __forceinline__ uint32_t table_insert(uint32_t* keys, uint32_t mask,
   }
   atomicExch(err, 1u);
   return 0;
+}
+
+__device__ __forceinline__ double warp_sum(double x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+  return x;
+}
+
+// Sum over the block, returned to every thread (red: kWarps doubles).
+__device__ __forceinline__ double block_sum_d(double x, double* red) {
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  x = warp_sum(x);
+  __syncthreads();
+  if (lane == 0) red[wib] = x;
+  __syncthreads();
+  double t = 0.0;
+#pragma unroll
+  for (int i = 0; i < kWarps; i++) t += red[i];
+  return t;
 }
 
 struct Ctx {
@@ -189,6 +213,10 @@ __global__ void __launch_bounds__(kThreads)
       vals[i] = 0.0;
     }
     __syncwarp();
+    // edges into the community itself (most of them, once the moves have
+    // converged) are summed in registers instead of one contended slot
+    double hot_acc = 0.0;
+    bool hot_seen = false;
     for (uint32_t mb = 0; mb < msz; mb += 32) {
       const uint32_t mi = mb + lane;
       const bool mv = mi < msz;
@@ -214,20 +242,34 @@ __global__ void __launch_bounds__(kThreads)
         const uint64_t vs = __shfl_sync(kFull, my_start, klo);
         uint32_t key = kEmptyKey;
         float wt = 0.0f;
+        bool ins = false;
         if (has) {
           const uint64_t j = vo + (p - vs);
           key = C.cnew[C.col[j]];
           wt = C.w[j];
+          if (key == cn) {  // intra-community edge: the new self-loop
+            hot_acc += (double)wt;
+            hot_seen = true;
+          } else {
+            ins = true;
+          }
         }
         const unsigned long long mk =
-            has ? (unsigned long long)key : (0x100000000ull | (unsigned)lane);
+            ins ? (unsigned long long)key : (0x100000000ull | (unsigned)lane);
         const unsigned peers = __match_any_sync(kFull, mk);
         const int leader = __ffs(peers) - 1;
         uint32_t slot = 0;
-        if (has && lane == leader) slot = table_insert(keys, mask, key, C.err);
+        if (ins && lane == leader) slot = table_insert(keys, mask, key, C.err);
         slot = __shfl_sync(kFull, slot, leader);
-        if (has) atomicAdd(&vals[slot], (double)wt);
+        if (ins) atomicAdd(&vals[slot], (double)wt);
       }
+    }
+    hot_acc = warp_sum(hot_acc);
+    const bool any_hot = __any_sync(kFull, hot_seen);
+    __syncwarp();
+    if (lane == 0 && any_hot) {
+      const uint32_t slot = table_insert(keys, mask, cn, C.err);
+      vals[slot] += hot_acc;
     }
     __syncwarp();
     uint32_t cnt = 0;
@@ -282,7 +324,8 @@ __device__ __forceinline__ void insert_range(const Ctx& C, uint32_t m0,
                                              uint64_t hi, uint32_t* keys,
                                              double* vals, uint32_t mask,
                                              uint64_t* s_start,
-                                             uint64_t* s_off) {
+                                             uint64_t* s_off, uint32_t hot,
+                                             double& hot_acc, bool& hot_seen) {
   const int lane = threadIdx.x & 31;
   // first member whose range contains lo: largest k with start_k <= lo
   __shared__ uint32_t s_k;
@@ -315,6 +358,7 @@ __device__ __forceinline__ void insert_range(const Ctx& C, uint32_t m0,
       const bool has = p < chunk_end;
       uint32_t key = kEmptyKey;
       float wt = 0.0f;
+      bool ins = false;
       if (has) {
         int a = 0, b = (int)nvalid - 1;
         while (a < b) {
@@ -324,15 +368,21 @@ __device__ __forceinline__ void insert_range(const Ctx& C, uint32_t m0,
         const uint64_t j = s_off[a] + (p - s_start[a]);
         key = C.cnew[C.col[j]];
         wt = C.w[j];
+        if (key == hot) {
+          hot_acc += (double)wt;
+          hot_seen = true;
+        } else {
+          ins = true;
+        }
       }
       const unsigned long long mk =
-          has ? (unsigned long long)key : (0x100000000ull | (unsigned)lane);
+          ins ? (unsigned long long)key : (0x100000000ull | (unsigned)lane);
       const unsigned peers = __match_any_sync(kFull, mk);
       const int leader = __ffs(peers) - 1;
       uint32_t slot = 0;
-      if (has && lane == leader) slot = table_insert(keys, mask, key, C.err);
+      if (ins && lane == leader) slot = table_insert(keys, mask, key, C.err);
       slot = __shfl_sync(kFull, slot, leader);
-      if (has) atomicAdd(&vals[slot], (double)wt);
+      if (ins) atomicAdd(&vals[slot], (double)wt);
     }
     pos = chunk_end;
     k0 += kThreads;
@@ -341,15 +391,18 @@ __device__ __forceinline__ void insert_range(const Ctx& C, uint32_t m0,
   (void)total;
 }
 
-// Class B: one block per community, 8192-slot shared table.
+// Classes B (SLOTS = 2048: <= 1024 entries) and B2 (8192: <= 4096): one
+// block per community, shared table of up to SLOTS slots.
+template <int SLOTS>
 __global__ void __launch_bounds__(kThreads)
     merge_block_kernel(Ctx C, const uint32_t* list, uint32_t count) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* vals = reinterpret_cast<double*>(smem_raw);
-  uint64_t* s_start = reinterpret_cast<uint64_t*>(smem_raw + kBlockSlots * 8);
+  uint64_t* s_start = reinterpret_cast<uint64_t*>(smem_raw + SLOTS * 8);
   uint64_t* s_off = s_start + kThreads;
-  uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + kBlockSlots * 8 + kThreads * 16);
+  uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + SLOTS * 8 + kThreads * 16);
   __shared__ uint32_t scan_sm[kWarps + 1];
+  __shared__ double red[kWarps];
   for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
     const uint32_t cn = list[idx];
     const uint32_t c = C.comm_list[cn];
@@ -357,13 +410,21 @@ __global__ void __launch_bounds__(kThreads)
     const uint64_t seg = C.mstart[m0];
     const uint64_t total = C.mstart[m0 + msz] - seg;
     // class B rows hold > 128 entries, so tv >= 256 = kThreads
-    const uint32_t tv = table_size_for((uint32_t)total, kBlockSlots);
+    const uint32_t tv = table_size_for((uint32_t)total, SLOTS);
     for (uint32_t i = threadIdx.x; i < tv; i += kThreads) {
       keys[i] = kEmptyKey;
       vals[i] = 0.0;
     }
     __syncthreads();
-    insert_range(C, m0, msz, seg, total, 0, total, keys, vals, tv - 1, s_start, s_off);
+    double hot_acc = 0.0;
+    bool hot_seen = false;
+    insert_range(C, m0, msz, seg, total, 0, total, keys, vals, tv - 1, s_start, s_off, cn,
+                 hot_acc, hot_seen);
+    const double hs = block_sum_d(hot_acc, red);
+    if (__syncthreads_or(hot_seen) && threadIdx.x == 0) {
+      const uint32_t slot = table_insert(keys, tv - 1, cn, C.err);
+      vals[slot] += hs;
+    }
     __syncthreads();
     // emit: thread t owns slots [t*per, t*per + per)
     const uint32_t per = tv / kThreads;
@@ -403,6 +464,7 @@ __global__ void __launch_bounds__(kThreads)
     merge_global_insert_kernel(Ctx C, GArgs G) {
   __shared__ uint64_t s_start[kThreads];
   __shared__ uint64_t s_off[kThreads];
+  __shared__ double red[kWarps];
   for (uint32_t b = blockIdx.x; b < G.nblocks; b += gridDim.x) {
     const uint32_t gi = G.blk_comm[b], ch = G.blk_chunk[b];
     const uint32_t cn = G.list[gi];
@@ -412,8 +474,19 @@ __global__ void __launch_bounds__(kThreads)
     const uint64_t total = C.mstart[m0 + msz] - seg;
     const uint64_t lo = (uint64_t)ch * kMergeChunk;
     const uint64_t hi = min(total, lo + kMergeChunk);
-    insert_range(C, m0, msz, seg, total, lo, hi, G.keys + G.tab_off[gi],
-                 G.vals + G.tab_off[gi], G.tab_size[gi] - 1, s_start, s_off);
+    uint32_t* keys = G.keys + G.tab_off[gi];
+    double* vals = G.vals + G.tab_off[gi];
+    const uint32_t mask = G.tab_size[gi] - 1;
+    double hot_acc = 0.0;
+    bool hot_seen = false;
+    insert_range(C, m0, msz, seg, total, lo, hi, keys, vals, mask, s_start, s_off, cn,
+                 hot_acc, hot_seen);
+    const double hs = block_sum_d(hot_acc, red);
+    if (__syncthreads_or(hot_seen) && threadIdx.x == 0) {
+      const uint32_t slot = table_insert(keys, mask, cn, C.err);
+      atomicAdd(&vals[slot], hs);
+    }
+    __syncthreads();
   }
 }
 
@@ -484,9 +557,12 @@ uint64_t next_pow2(uint64_t x) {
 }  // namespace
 
 cudaError_t configure_contract_kernels() {
-  return cudaFuncSetAttribute(merge_block_kernel,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              kBlockSmem);
+  cudaError_t e = cudaFuncSetAttribute(merge_block_kernel<kMidSlots>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kMidSmem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(merge_block_kernel<kBlockSlots>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, kBlockSmem);
 }
 
 #define LV_TRY(x)                              \
@@ -523,13 +599,15 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
       B.comm_list, n, B.counts + 0, L.comm_sz, B.mem_off, B.mstart, B.comm_deg,
       B.seg, B.new_deg));
   LV_TRY(cudaGetLastError());
-  LV_TRY(partition_by_size3(B.comm_deg, n, B.counts + 0, kMergeWarpMax, kMergeBlockMax,
-                            B.comm_cls, B.counts + 4, B.tmp, S, st));
+  LV_TRY(partition_by_size4(B.comm_deg, n, B.counts + 0, kMergeWarpMax, kMergeMidMax,
+                            kMergeBlockMax, B.comm_cls, B.counts + 4, B.tmp, S, st));
   LV_TRY(cudaMemcpyAsync(h_counts, B.counts, 8 * sizeof(uint32_t),
                          cudaMemcpyDeviceToHost, st));
   LV_TRY(cudaStreamSynchronize(st));
   const uint32_t new_n = h_counts[0];
-  const uint32_t cntW = h_counts[4], cntB = h_counts[5], cntG = h_counts[6];
+  const uint32_t cntW = h_counts[4], cntM = h_counts[5], cntB2 = h_counts[6];
+  const uint32_t cntB = cntM + cntB2;  // both block classes
+  const uint32_t cntG = h_counts[7];
 
   Ctx C;
   C.off = L.off;
@@ -551,9 +629,14 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
         C, B.comm_cls, cntW));
     LV_TRY(cudaGetLastError());
   }
-  if (cntB) {
-    (count_launches(1), merge_block_kernel<<<gridcap(cntB, 2), kThreads, kBlockSmem, st>>>(
-        C, B.comm_cls + cntW, cntB));
+  if (cntM) {
+    (count_launches(1), merge_block_kernel<kMidSlots><<<gridcap(cntM, 7), kThreads, kMidSmem, st>>>(
+        C, B.comm_cls + cntW, cntM));
+    LV_TRY(cudaGetLastError());
+  }
+  if (cntB2) {
+    (count_launches(1), merge_block_kernel<kBlockSlots><<<gridcap(cntB2, 2), kThreads, kBlockSmem, st>>>(
+        C, B.comm_cls + cntW + cntM, cntB2));
     LV_TRY(cudaGetLastError());
   }
   if (cntG) {

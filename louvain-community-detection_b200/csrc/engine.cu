@@ -187,6 +187,7 @@ struct lv_engine {
   size_t hub_map_cap = 0;
   HubArena hub;
   size_t hub_count_cap = 0, hub_blocks_cap = 0, hub_units_cap = 0;
+  size_t hub_stage_cap = 0, hub_ct_cap = 0;
   uint64_t* hub_deg = nullptr;
 
   ContractBuffers cb{};
@@ -371,6 +372,14 @@ void free_state(lv_engine* E) {
   dfree(E->hub_map);
   dfree(E->hub.best);
   dfree(E->hub.own);
+  dfree(E->hub.hot);
+  dfree(E->hub.hot_any);
+  dfree(E->hub.nparts);
+  dfree(E->hub.stage_off);
+  dfree(E->hub.ct_off);
+  dfree(E->hub.stage_c);
+  dfree(E->hub.stage_w);
+  dfree(E->hub.ct);
   dfree(E->hub.blk_vertex);
   dfree(E->hub.blk_chunk);
   dfree(E->hub.blk_nchunks);
@@ -404,6 +413,7 @@ void free_state(lv_engine* E) {
   E->scan.bytes = 0;
   E->partials_cap = E->hub_map_cap = 0;
   E->hub_count_cap = E->hub_blocks_cap = E->hub_units_cap = 0;
+  E->hub_stage_cap = E->hub_ct_cap = 0;
   E->cap_n = 0;
   E->cap_e = 0;
   E->in_off = nullptr;
@@ -517,14 +527,28 @@ lv_status prepare_level(lv_engine* E) {
   // and move units (hub, hash partition of about kHubPartKeys communities)
   std::vector<uint32_t> blk_vertex, blk_chunk;            // dispatch chunks
   std::vector<uint32_t> unit_vertex, unit_part, unit_np;  // move units
+  std::vector<uint32_t> hub_np;                           // partitions per hub
+  std::vector<uint64_t> hub_stage, hub_ct;                // staging / chunk-table offsets
+  uint64_t stage_total = 0, ct_total = 0;
   if (hc) {
     if (hc > E->hub_count_cap) {
+      HubArena& H = E->hub;
       dfree(E->hub_deg);
-      dfree(E->hub.best);
-      dfree(E->hub.own);
+      dfree(H.best);
+      dfree(H.own);
+      dfree(H.hot);
+      dfree(H.hot_any);
+      dfree(H.nparts);
+      dfree(H.stage_off);
+      dfree(H.ct_off);
       CU(dalloc(&E->hub_deg, hc));
-      CU(dalloc(&E->hub.best, hc));
-      CU(dalloc(&E->hub.own, hc));
+      CU(dalloc(&H.best, hc));
+      CU(dalloc(&H.own, hc));
+      CU(dalloc(&H.hot, hc));
+      CU(dalloc(&H.hot_any, hc));
+      CU(dalloc(&H.nparts, hc));
+      CU(dalloc(&H.stage_off, hc));
+      CU(dalloc(&H.ct_off, hc));
       E->hub_count_cap = hc;
     }
     (count_launches(1), gather_degrees_kernel<<<(hc + 255) / 256, 256, 0, st>>>(
@@ -541,12 +565,18 @@ lv_status prepare_level(lv_engine* E) {
         blk_chunk.push_back(ch);
       }
       const uint64_t distinct = std::min<uint64_t>(deg[i], n);
-      const uint32_t np = (uint32_t)std::max<uint64_t>(1, (distinct + kHubPartKeys - 1) / kHubPartKeys);
+      const uint32_t np = (uint32_t)std::min<uint64_t>(
+          kHubMaxParts, std::max<uint64_t>(1, (distinct + kHubPartKeys - 1) / kHubPartKeys));
       for (uint32_t p = 0; p < np; p++) {  // a hub's partitions are adjacent
         unit_vertex.push_back(i);
         unit_part.push_back(p);
         unit_np.push_back(np);
       }
+      hub_np.push_back(np);
+      hub_stage.push_back(stage_total);
+      hub_ct.push_back(ct_total);
+      stage_total += deg[i];
+      ct_total += (uint64_t)nch * (np + 1);
     }
   }
   P.hub_count = hc;
@@ -598,8 +628,30 @@ lv_status prepare_level(lv_engine* E) {
                        cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync(E->hub.blk_nchunks, unit_np.data(), hu * sizeof(uint32_t),
                        cudaMemcpyHostToDevice, st));
-    CU(cudaMemsetAsync(E->hub.best, 0, hc * sizeof(unsigned long long), st));
-    CU(cudaMemsetAsync(E->hub.own, 0, hc * sizeof(double), st));
+    // split/merge plan: partitions, staging copy of the hub rows, chunk table
+    HubArena& H = E->hub;
+    if (stage_total > E->hub_stage_cap) {
+      dfree(H.stage_c);
+      dfree(H.stage_w);
+      CU(dalloc(&H.stage_c, stage_total));
+      CU(dalloc(&H.stage_w, stage_total));
+      E->hub_stage_cap = stage_total;
+    }
+    if (ct_total > E->hub_ct_cap) {
+      dfree(H.ct);
+      CU(dalloc(&H.ct, ct_total));
+      E->hub_ct_cap = ct_total;
+    }
+    CU(cudaMemcpyAsync(H.nparts, hub_np.data(), hc * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                       st));
+    CU(cudaMemcpyAsync(H.stage_off, hub_stage.data(), hc * sizeof(uint64_t),
+                       cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(H.ct_off, hub_ct.data(), hc * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                       st));
+    CU(cudaMemsetAsync(H.best, 0, hc * sizeof(unsigned long long), st));
+    CU(cudaMemsetAsync(H.own, 0, hc * sizeof(double), st));
+    CU(cudaMemsetAsync(H.hot, 0, hc * sizeof(double), st));
+    CU(cudaMemsetAsync(H.hot_any, 0, hc * sizeof(uint32_t), st));
     CU(cudaMemsetAsync(E->partials, 0, hc * sizeof(double), st));
   }
   if (E->batch) {
@@ -767,7 +819,7 @@ lv_status issue_pass(lv_engine* E, const PassControl* ctl) {
     prof_end(E, t0, K_MOVE1 + b - 1, (double)E->class_deg[b] * 12.0 + v7 * 32.0);
     if (b == 7 && E->plan.hub_count) {
       t0 = prof_begin(E);
-      CU(launch_move_bucket(L, 8, rule, ord, E->prop, E->plan, H, E->st, ac));
+      CU(launch_move_bucket(L, 8, rule, ord, E->prop, E->plan, H, E->st, ac, E->hub_map));
       prof_end(E, t0, K_HUB,
                (double)E->class_deg[8] * 12.0 + (double)E->plan.hub_count * 32.0);
     }

@@ -181,12 +181,12 @@ cudaError_t partition_by_degree(const uint64_t* off, uint32_t n,
                                 uint32_t* tmp, ScanScratch& s,
                                 cudaStream_t st);
 
-// Stable partition of the indices [0, *d_live) into 3 classes by sizes[i]:
-// <= lim0, <= lim1, larger.  n_upper bounds *d_live (which is read on the
-// device, so no host round trip is needed).
-cudaError_t partition_by_size3(const uint64_t* sizes, uint32_t n_upper,
+// Stable partition of the indices [0, *d_live) into 4 classes by sizes[i]:
+// <= lim0, <= lim1, <= lim2, larger.  n_upper bounds *d_live (which is read
+// on the device, so no host round trip is needed).
+cudaError_t partition_by_size4(const uint64_t* sizes, uint32_t n_upper,
                                const uint32_t* d_live, uint64_t lim0,
-                               uint64_t lim1, uint32_t* out,
+                               uint64_t lim1, uint64_t lim2, uint32_t* out,
                                uint32_t* cls_count, uint32_t* tmp,
                                ScanScratch& s, cudaStream_t st);
 
@@ -212,29 +212,48 @@ cudaError_t launch_modularity(const LevelView& L, const uint32_t* order,
 // for the single graph and for every graph of a batch
 cudaError_t launch_pass_control_init(LevelScalars* sc, GraphState* gs,
                                      uint32_t n_graphs, cudaStream_t st);
-// Hubs (class 8): work units are (hub, hash partition of its neighbour
-// communities); per hub a best packed (gain, ~community) key and an
-// own-community weight sum.
+// Hubs (class 8).  A split pass reads every hub row once in chunks of
+// kHubChunk entries and writes each chunk's (community, weight) pairs
+// grouped by hash partition of the community (partitions of about
+// kHubPartKeys distinct communities) into a staging copy of the hub rows;
+// entries into the hub's own community are summed there and then.  A merge
+// pass runs one block per (hub, partition) over that partition's segment of
+// every chunk.  Per hub: the best packed (gain, ~community) key, the
+// own-community sums and the plan arrays (fixed for a level).
 struct HubArena {
   unsigned long long* best = nullptr;  // [hub_count]
-  double* own = nullptr;           // [hub_count]
-  uint32_t* blk_vertex = nullptr;  // [units] hub index of each unit
+  double* own = nullptr;           // [hub_count] own-community weight w/o self-loop
+  double* hot = nullptr;           // [hub_count] own-community weight (all)
+  uint32_t* hot_any = nullptr;     // [hub_count] an entry into the own community exists
+  uint32_t* nparts = nullptr;      // [hub_count] partitions of the hub
+  uint64_t* stage_off = nullptr;   // [hub_count] first staging entry of the hub
+  uint64_t* ct_off = nullptr;      // [hub_count] first chunk-table entry of the hub
+  uint32_t* stage_c = nullptr;     // [hub entries] staged communities
+  float* stage_w = nullptr;        // [hub entries] staged weights
+  uint32_t* ct = nullptr;          // per hub: chunks x (nparts + 1) segment starts
+  uint32_t* blk_vertex = nullptr;  // [units] hub index of each merge unit
   uint32_t* blk_chunk = nullptr;   // [units] partition of the unit
   uint32_t* blk_nchunks = nullptr; // [units] partitions of that hub
   uint32_t units = 0;
 };
-// Shared table of a hub unit (8192 slots, about kHubPartKeys communities
-// per partition, load factor ~1/2).
-constexpr int kHubPartSlots = 8192;
-constexpr uint32_t kHubPartKeys = 4096;
+// Shared table of a hub merge unit (4096 slots, about kHubPartKeys
+// communities per partition, load factor ~1/2), and the most partitions a
+// hub may have (the split pass keeps one counter per partition in shared
+// memory).
+constexpr int kHubPartSlots = 4096;
+constexpr uint32_t kHubPartKeys = 2048;
+constexpr uint32_t kHubMaxParts = 8192;
 // Proposals for the vertices of kernel class c (1..8; bucket 7 is classes 7
 // and 8, both launched before its apply).  proposal[] is parallel to
 // order[].
 // act_cnt: as for launch_modularity (null: whole classes).
+// Bucket 8 (hubs) also needs the hub dispatch map (hub index | chunk of
+// every kHubChunk-entry block, P.hub_blocks of each).
 cudaError_t launch_move_bucket(const LevelView& L, int bucket, int rule,
                                const uint32_t* order, uint32_t* proposal,
                                const DispatchPlan& P, const HubArena& H,
-                               cudaStream_t st, const uint32_t* act_cnt = nullptr);
+                               cudaStream_t st, const uint32_t* act_cnt = nullptr,
+                               const uint32_t* hub_map = nullptr);
 cudaError_t launch_apply_bucket(const LevelView& L, int bucket,
                                 const uint32_t* order,
                                 const uint32_t* proposal,
@@ -302,7 +321,8 @@ struct ContractBuffers {
   size_t g_cap;          // entries available in the g_* arrays
 };
 constexpr uint64_t kMergeWarpMax = 128;    // entries: warp per community
-constexpr uint64_t kMergeBlockMax = 4096;  // entries: block, shared table
+constexpr uint64_t kMergeMidMax = 1024;    // entries: block, 2048-slot table
+constexpr uint64_t kMergeBlockMax = 4096;  // entries: block, 8192-slot table
 constexpr uint32_t kMergeChunk = 8192;     // entries per block, class G
 
 struct ContractResult {

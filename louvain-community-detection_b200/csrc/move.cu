@@ -252,21 +252,31 @@ __global__ void __launch_bounds__(kThreads)
       wt = L.w[s + gl];
       cu = L.comm[u];
     }
+    // the own community's entries are summed with shuffles (its lowest
+    // lane holds the sum); the others through one shared slot per distinct
+    // community
+    const bool is_hot = has && cu == cv;
+    const bool ins = has && !is_hot;
+    const double hv = group_sum<G>(is_hot ? (double)wt : 0.0);
+    const unsigned gmask = (G == 32) ? kFull : (((1u << G) - 1u) << (lane & ~(G - 1)));
+    const unsigned hmask = __ballot_sync(kFull, is_hot) & gmask;
+    const int hot_leader = hmask ? __ffs(hmask) - 1 : -1;
     const unsigned long long mk =
-        has ? (((unsigned long long)(lane / G) << 32) | cu)
+        ins ? (((unsigned long long)(lane / G) << 32) | cu)
             : (0xFFFFFFFF00000000ull | (unsigned)lane);
     const unsigned peers = __match_any_sync(kFull, mk);
     const int leader = __ffs(peers) - 1;
-    sums[wib][lane] = 0.0;
+    sums[wib][lane] = (lane == hot_leader) ? hv : 0.0;
     __syncwarp();
-    if (has) atomicAdd(&sums[wib][leader], (double)wt);
+    if (ins) atomicAdd(&sums[wib][leader], (double)wt);
     double own = 0.0;
-    if (RULE == LV_RULE_CUDA_I && has && cu == cv && u != v) own = (double)wt;
+    if (RULE == LV_RULE_CUDA_I && is_hot && u != v) own = (double)wt;
     __syncwarp();
     unsigned long long best = 0ull;
     GainCtx g;
     if (vvalid) g = make_ctx(L, v, cv);
-    if (has && leader == lane) best = candidate(L, g, cu, sums[wib][lane]);
+    if ((ins && leader == lane) || lane == hot_leader)
+      best = candidate(L, g, cu, sums[wib][lane]);
     best = group_max<G>(best);
     if (RULE == LV_RULE_CUDA_I) own = group_sum<G>(own);
     if (vvalid && gl == 0) prop[vidx] = decide<RULE>(best, own, g);
@@ -372,22 +382,35 @@ __global__ void __launch_bounds__(kThreads)
       if (cu[k] == v) self_mask |= 1u << k;
       cu[k] = (j < d) ? L.comm[cu[k]] : kEmptyKey;
     }
-    double own = 0.0;
+    double own = 0.0, hot = 0.0;
+    bool hot_seen = false;
 #pragma unroll
     for (int k = 0; k < MAXW; k++) {
       if ((uint32_t)k * 32 >= d) break;  // warp-uniform
       const bool has = (uint32_t)k * 32 + lane < d;
+      // entries into the vertex's own community (most of them once moves
+      // converge) are summed in registers, not in one contended slot
+      const bool is_hot = has && cu[k] == cv;
+      const bool ins = has && !is_hot;
+      if (is_hot) {
+        hot += (double)wt[k];
+        hot_seen = true;
+        if (RULE == LV_RULE_CUDA_I && !(self_mask >> k & 1u)) own += (double)wt[k];
+      }
       const unsigned long long mk =
-          has ? (unsigned long long)cu[k] : (0x100000000ull | (unsigned)lane);
+          ins ? (unsigned long long)cu[k] : (0x100000000ull | (unsigned)lane);
       const unsigned peers = __match_any_sync(kFull, mk);
       const int leader = __ffs(peers) - 1;
       uint32_t slot = 0;
-      if (has && lane == leader)
+      if (ins && lane == leader)
         slot = table_insert_fresh(keys, tv - 1, cu[k], fresh, n_fresh, L.sc);
       slot = __shfl_sync(kFull, slot, leader);
-      if (has) atomicAdd(&vals[slot], (double)wt[k]);
-      if (RULE == LV_RULE_CUDA_I && has && cu[k] == cv && !(self_mask >> k & 1u))
-        own += (double)wt[k];
+      if (ins) atomicAdd(&vals[slot], (double)wt[k]);
+    }
+    hot = group_sum<32>(hot);
+    if (__any_sync(kFull, hot_seen) && lane == 0) {
+      const uint32_t slot = table_insert_fresh(keys, tv - 1, cv, fresh, n_fresh, L.sc);
+      vals[slot] += hot;
     }
     __syncwarp();
     const GainCtx g = make_ctx(L, v, cv);
@@ -439,7 +462,8 @@ __device__ __forceinline__ void insert_block_range(const LevelView& L, uint64_t 
                                                    uint32_t v, uint32_t cv,
                                                    uint32_t* keys, double* vals,
                                                    uint32_t mask, double& own,
-                                                   uint16_t* fresh, uint32_t* n_fresh) {
+                                                   uint16_t* fresh, uint32_t* n_fresh,
+                                                   double& hot, bool& hot_seen) {
   const int lane = threadIdx.x & 31;
   uint32_t cu[MAXW];
   float wt[MAXW];
@@ -464,17 +488,23 @@ __device__ __forceinline__ void insert_block_range(const LevelView& L, uint64_t 
   for (int k = 0; k < MAXW; k++) {
     if (lo + (uint64_t)k * kThreads >= end) break;  // block-uniform
     const bool has = lo + (uint64_t)k * kThreads + threadIdx.x < end;
+    // own-community entries go to the caller's register sum (hot)
+    const bool is_hot = has && cu[k] == cv;
+    const bool ins = has && !is_hot;
+    if (is_hot) {
+      hot += (double)wt[k];
+      hot_seen = true;
+      if (RULE == LV_RULE_CUDA_I && !(self_mask >> k & 1u)) own += (double)wt[k];
+    }
     const unsigned long long mk =
-        has ? (unsigned long long)cu[k] : (0x100000000ull | (unsigned)lane);
+        ins ? (unsigned long long)cu[k] : (0x100000000ull | (unsigned)lane);
     const unsigned peers = __match_any_sync(kFull, mk);
     const int leader = __ffs(peers) - 1;
     uint32_t slot = 0;
-    if (has && lane == leader)
+    if (ins && lane == leader)
       slot = table_insert_fresh(keys, mask, cu[k], fresh, n_fresh, L.sc);
     slot = __shfl_sync(kFull, slot, leader);
-    if (has) atomicAdd(&vals[slot], (double)wt[k]);
-    if (RULE == LV_RULE_CUDA_I && has && cu[k] == cv && !(self_mask >> k & 1u))
-      own += (double)wt[k];
+    if (ins) atomicAdd(&vals[slot], (double)wt[k]);
   }
 }
 
@@ -511,8 +541,16 @@ __global__ void __launch_bounds__(kThreads)
     }
     const uint32_t tv = table_size_for(d, T);
     double own = 0.0;
+    double hot = 0.0;
+    bool hot_seen = false;
     insert_block_range<MAXW, RULE>(L, s, 0, d, v, cv, keys, vals, tv - 1, own,
-                                   fresh, &n_fresh);
+                                   fresh, &n_fresh, hot, hot_seen);
+    const int any_hot = __syncthreads_or(hot_seen);
+    hot = block_sum(hot, red_own);  // thread 0
+    if (threadIdx.x == 0 && any_hot) {
+      const uint32_t slot = table_insert_fresh(keys, tv - 1, cv, fresh, &n_fresh, L.sc);
+      vals[slot] += hot;
+    }
     __syncthreads();
     const GainCtx g = make_ctx(L, v, cv);
     unsigned long long best =
@@ -527,31 +565,153 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// deg > 2048 (hubs): the neighbour communities of a hub are split into P
+// deg > 2048 (hubs).  The neighbour communities of a hub are split into P
 // hash partitions (P from the hub's degree, about kHubPartKeys distinct
-// communities each).  One block per (hub, partition) streams the whole row
-// -- the other partitions' blocks of the same hub run alongside, so the
-// re-reads come from L2 -- and sums only its partition's communities in a
-// self-cleaning shared table.  Its best candidate is folded into the hub's
-// packed (gain, ~community) key with one atomicMax; no global hash table,
-// no per-entry global atomics.
+// communities each).  hub_split_kernel: one block per kHubChunk-entry chunk
+// of a hub row gathers the chunk's communities, sums the entries into the
+// hub's own community on the spot and writes the others to the staging
+// copy grouped by partition (a counting sort in shared memory), with the
+// partition starts in the chunk table.  hub_merge_kernel: one block per
+// (hub, partition) sums that partition's segments of all chunks in a
+// self-cleaning shared table and folds its best candidate into the hub's
+// packed (gain, ~community) key with one atomicMax.  Every hub entry is
+// read once from the CSR and once from the staging copy; no global hash
+// table, no per-entry global atomics.
 __device__ __forceinline__ uint32_t hub_part_of(uint32_t c, uint32_t nparts) {
   return __umulhi(c * 0x85EBCA6Bu, nparts);
 }
 
+// In-place exclusive scan of a[0, n) (n <= kHubMaxParts) by the block;
+// returns the total to every thread.
+__device__ __forceinline__ uint32_t block_scan_inplace(uint32_t* a, uint32_t n,
+                                                       uint32_t* wsum) {
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t per = (n + kThreads - 1) / kThreads;
+  const uint32_t a0 = min(n, threadIdx.x * per), a1 = min(n, a0 + per);
+  uint32_t local = 0;
+  for (uint32_t i = a0; i < a1; i++) local += a[i];
+  uint32_t incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) wsum[wib] = incl;
+  __syncthreads();
+  uint32_t before = 0, total = 0;
+#pragma unroll
+  for (int i = 0; i < kWarps; i++) {
+    const uint32_t t = wsum[i];
+    if (i < wib) before += t;
+    total += t;
+  }
+  uint32_t run = before + incl - local;
+  for (uint32_t i = a0; i < a1; i++) {
+    const uint32_t t = a[i];
+    a[i] = run;
+    run += t;
+  }
+  __syncthreads();
+  return total;
+}
+
 template <int RULE>
 __global__ void __launch_bounds__(kThreads)
-    hub_part_kernel(LevelView L, const uint32_t* __restrict__ hubs, HubArena H,
-                    uint32_t units) {
+    hub_split_kernel(LevelView L, const uint32_t* __restrict__ hubs, HubArena H,
+                     const uint32_t* __restrict__ blk_hub,
+                     const uint32_t* __restrict__ blk_ch, uint32_t nblocks) {
+  constexpr int EPT = kHubChunk / kThreads;  // entries per thread
+  static_assert(EPT * kThreads == (int)kHubChunk, "chunk = whole waves");
+  __shared__ uint32_t cnt[kHubMaxParts];
+  __shared__ uint32_t wsum[kWarps];
+  __shared__ double red[kWarps];
+  for (uint32_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
+    const uint32_t hi = blk_hub[b], ch = blk_ch[b];
+    const uint32_t v = hubs[hi];
+    if (!vertex_active(L, v)) continue;  // block-uniform
+    const uint64_t s = L.off[v];
+    const uint64_t lo = (uint64_t)ch * kHubChunk;
+    const uint64_t rest = L.off[v + 1] - s - lo;
+    const uint32_t n_in = rest < kHubChunk ? (uint32_t)rest : kHubChunk;
+    const uint32_t P = H.nparts[hi];
+    const uint32_t cv = L.comm[v];
+    for (uint32_t p = threadIdx.x; p < P; p += kThreads) cnt[p] = 0u;
+    __syncthreads();
+    uint32_t c[EPT], part[EPT], rank[EPT];
+    float w[EPT];
+    bool self[EPT];
+#pragma unroll
+    for (int k = 0; k < EPT; k++) {  // every load before any use
+      const uint32_t j = k * kThreads + threadIdx.x;
+      c[k] = v;
+      w[k] = 0.0f;
+      if (j < n_in) {
+        c[k] = L.col[s + lo + j];
+        w[k] = L.w[s + lo + j];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < EPT; k++) {
+      const uint32_t j = k * kThreads + threadIdx.x;
+      self[k] = c[k] == v;
+      c[k] = (j < n_in) ? L.comm[c[k]] : kEmptyKey;
+    }
+    double hot = 0.0, own = 0.0;
+    bool hot_seen = false;
+#pragma unroll
+    for (int k = 0; k < EPT; k++) {
+      part[k] = kEmptyKey;
+      if (c[k] == kEmptyKey) continue;
+      if (c[k] == cv) {  // own community: summed here, not staged
+        hot += (double)w[k];
+        hot_seen = true;
+        if (RULE == LV_RULE_CUDA_I && !self[k]) own += (double)w[k];
+      } else {
+        part[k] = hub_part_of(c[k], P);
+        rank[k] = atomicAdd(&cnt[part[k]], 1u);
+      }
+    }
+    __syncthreads();
+    const uint32_t staged = block_scan_inplace(cnt, P, wsum);
+    uint32_t* ct = H.ct + H.ct_off[hi] + (uint64_t)ch * (P + 1);
+    for (uint32_t p = threadIdx.x; p < P; p += kThreads) ct[p] = cnt[p];
+    if (threadIdx.x == 0) ct[P] = staged;
+    const uint64_t base = H.stage_off[hi] + lo;
+#pragma unroll
+    for (int k = 0; k < EPT; k++) {
+      if (part[k] == kEmptyKey) continue;
+      const uint64_t pos = base + cnt[part[k]] + rank[k];
+      H.stage_c[pos] = c[k];
+      H.stage_w[pos] = w[k];
+    }
+    const int any_hot = __syncthreads_or(hot_seen);
+    if (any_hot) {
+      hot = block_sum(hot, red);
+      if (threadIdx.x == 0) {
+        atomicAdd(&H.hot[hi], hot);
+        atomicOr(&H.hot_any[hi], 1u);
+      }
+    }
+    if (RULE == LV_RULE_CUDA_I) {
+      own = block_sum(own, red);
+      if (threadIdx.x == 0 && own != 0.0) atomicAdd(&H.own[hi], own);
+    }
+    __syncthreads();  // cnt is reused by the next chunk
+  }
+}
+
+template <int RULE>
+__global__ void __launch_bounds__(kThreads)
+    hub_merge_kernel(LevelView L, const uint32_t* __restrict__ hubs, HubArena H,
+                     uint32_t units) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int T = kHubPartSlots;
-  constexpr int PF = 4;  // waves prefetched per iteration
   double* vals = reinterpret_cast<double*>(smem_raw);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T);
   uint16_t* fresh = reinterpret_cast<uint16_t*>(smem_raw + 12 * T);
   __shared__ unsigned long long red_best[kWarps];
-  __shared__ double red_own[kWarps];
   __shared__ uint32_t n_fresh;
+  __shared__ uint32_t seg_a[kThreads], seg_pre[kThreads], wsum[kWarps];
   const int lane = threadIdx.x & 31;
   for (uint32_t i = threadIdx.x; i < T; i += kThreads) {
     keys[i] = kEmptyKey;
@@ -561,59 +721,59 @@ __global__ void __launch_bounds__(kThreads)
   __syncthreads();
   for (uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
     const uint32_t hi = H.blk_vertex[u], part = H.blk_chunk[u];
-    const uint32_t nparts = H.blk_nchunks[u];
+    const uint32_t P = H.blk_nchunks[u];
     const uint32_t v = hubs[hi];
-    const uint64_t s = L.off[v];
-    const uint64_t d = L.off[v + 1] - s;
-    const uint32_t cv = L.comm[v];
     if (!vertex_active(L, v)) continue;  // block-uniform; decide keeps cv
-    double own = 0.0;
-    for (uint64_t j0 = 0; j0 < d; j0 += (uint64_t)PF * kThreads) {
-      uint32_t cu[PF];
-      float wt[PF];
-      unsigned self_mask = 0u;
-#pragma unroll
-      for (int k = 0; k < PF; k++) {
-        const uint64_t j = j0 + (uint64_t)k * kThreads + threadIdx.x;
-        cu[k] = v;
-        wt[k] = 0.0f;
-        if (j < d) {
-          cu[k] = L.col[s + j];
-          wt[k] = L.w[s + j];
+    const uint64_t d = L.off[v + 1] - L.off[v];
+    const uint32_t nch = (uint32_t)((d + kHubChunk - 1) / kHubChunk);
+    const uint32_t* ct = H.ct + H.ct_off[hi];
+    const uint64_t sb = H.stage_off[hi];
+    // the partition's segments of up to kThreads chunks at a time, walked
+    // as one flat range by the whole block
+    for (uint32_t cb = 0; cb < nch; cb += kThreads) {
+      const uint32_t nb = min((uint32_t)kThreads, nch - cb);
+      uint32_t len = 0;
+      if (threadIdx.x < nb) {
+        const uint64_t r = (uint64_t)(cb + threadIdx.x) * (P + 1) + part;
+        seg_a[threadIdx.x] = ct[r];
+        len = ct[r + 1] - ct[r];
+      }
+      seg_pre[threadIdx.x] = len;
+      __syncthreads();
+      const uint32_t total = block_scan_inplace(seg_pre, kThreads, wsum);
+      for (uint32_t f0 = 0; f0 < total; f0 += kThreads) {  // block-uniform
+        const uint32_t f = f0 + threadIdx.x;
+        const bool has = f < total;
+        uint32_t c = 0;
+        float w = 0.0f;
+        if (has) {
+          uint32_t lo = 0, hi2 = nb - 1;  // last segment starting at or before f
+          while (lo < hi2) {
+            const uint32_t mid = (lo + hi2 + 1) >> 1;
+            if (seg_pre[mid] <= f) lo = mid; else hi2 = mid - 1;
+          }
+          const uint64_t pos = sb + (uint64_t)(cb + lo) * kHubChunk + seg_a[lo] + (f - seg_pre[lo]);
+          c = H.stage_c[pos];
+          w = H.stage_w[pos];
         }
-      }
-#pragma unroll
-      for (int k = 0; k < PF; k++) {
-        const uint64_t j = j0 + (uint64_t)k * kThreads + threadIdx.x;
-        if (cu[k] == v) self_mask |= 1u << k;
-        cu[k] = (j < d) ? L.comm[cu[k]] : kEmptyKey;
-      }
-#pragma unroll
-      for (int k = 0; k < PF; k++) {
-        if (j0 + (uint64_t)k * kThreads >= d) break;  // block-uniform
-        const bool has = cu[k] != kEmptyKey && hub_part_of(cu[k], nparts) == part;
         const unsigned long long mk =
-            has ? (unsigned long long)cu[k] : (0x100000000ull | (unsigned)lane);
+            has ? (unsigned long long)c : (0x100000000ull | (unsigned)lane);
         const unsigned peers = __match_any_sync(kFull, mk);
         const int leader = __ffs(peers) - 1;
         uint32_t slot = 0;
         if (has && lane == leader)
-          slot = table_insert_fresh(keys, T - 1, cu[k], fresh, &n_fresh, L.sc);
+          slot = table_insert_fresh(keys, T - 1, c, fresh, &n_fresh, L.sc);
         slot = __shfl_sync(kFull, slot, leader);
-        if (has) atomicAdd(&vals[slot], (double)wt[k]);
-        if (RULE == LV_RULE_CUDA_I && has && cu[k] == cv && !(self_mask >> k & 1u))
-          own += (double)wt[k];
+        if (has) atomicAdd(&vals[slot], (double)w);
       }
+      __syncthreads();  // seg_a / seg_pre are refilled
     }
-    __syncthreads();
-    const GainCtx g = make_ctx(L, v, cv);
+    const GainCtx g = make_ctx(L, v, L.comm[v]);
     unsigned long long best =
         scan_fresh_and_clear(L, g, keys, vals, fresh, n_fresh, threadIdx.x, kThreads);
     best = block_max(best, red_best);
-    if (RULE == LV_RULE_CUDA_I) own = block_sum(own, red_own);
     if (threadIdx.x == 0) {
       if (best) atomicMax(&H.best[hi], best);
-      if (RULE == LV_RULE_CUDA_I && own != 0.0) atomicAdd(&H.own[hi], own);
       n_fresh = 0u;
     }
     __syncthreads();
@@ -628,9 +788,14 @@ __global__ void hub_decide_kernel(LevelView L, const uint32_t* __restrict__ hubs
        i += gridDim.x * blockDim.x) {
     const uint32_t v = hubs[i];
     const GainCtx g = make_ctx(L, v, L.comm[v]);
-    prop[i] = decide<RULE>(H.best[i], H.own[i], g);
+    unsigned long long best = H.best[i];
+    // the own community's candidate from the split pass's sums
+    if (H.hot_any[i]) best = umax64(best, candidate(L, g, g.cv, H.hot[i]));
+    prop[i] = decide<RULE>(best, H.own[i], g);
     H.best[i] = 0ull;
     H.own[i] = 0.0;
+    H.hot[i] = 0.0;
+    H.hot_any[i] = 0u;
   }
 }
 
@@ -1217,10 +1382,10 @@ cudaError_t configure_kernels() {
   e = cudaFuncSetAttribute(move_block_kernel<LV_RULE_CUDA_I>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, kBlockTabSmem);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(hub_part_kernel<LV_RULE_PY_I>,
+  e = cudaFuncSetAttribute(hub_merge_kernel<LV_RULE_PY_I>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, kHubPartSmem);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(hub_part_kernel<LV_RULE_CUDA_I>,
+  e = cudaFuncSetAttribute(hub_merge_kernel<LV_RULE_CUDA_I>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, kHubPartSmem);
   if (e != cudaSuccess) return e;
   return configure_contract_kernels();
@@ -1261,7 +1426,8 @@ template <int RULE>
 static cudaError_t move_bucket_impl(const LevelView& L, int bucket,
                                     const uint32_t* order, uint32_t* prop,
                                     const DispatchPlan& P, const HubArena& H,
-                                    const uint32_t* act_cnt, cudaStream_t st) {
+                                    const uint32_t* act_cnt, const uint32_t* hub_map,
+                                    cudaStream_t st) {
   const unsigned cap = sm_count() * 8;
   const uint32_t s = P.cls_start[bucket];
   const uint32_t cnt = P.cls_start[bucket + 1] - s;
@@ -1303,12 +1469,15 @@ static cudaError_t move_bucket_impl(const LevelView& L, int bucket,
                                   kBlockTabSmem, st>>>(L, verts, cnt, pr, dc));
       }
       break;
-    case 8: {  // class 8 of bucket 7: one block per (hub, partition)
+    case 8: {  // class 8 of bucket 7: split chunks, merge (hub, partition)
       const uint32_t hs = P.cls_start[8];
       const uint32_t hc = P.cls_start[9] - hs;
       if (hc) {
-        (count_launches(1), hub_part_kernel<RULE><<<grid_for(H.units, sm_count() * 2), kThreads,
-                                                  kHubPartSmem, st>>>(L, order + hs, H, H.units));
+        const uint32_t hb = P.hub_blocks;
+        (count_launches(1), hub_split_kernel<RULE><<<grid_for(hb, sm_count() * 6), kThreads, 0, st>>>(
+            L, order + hs, H, hub_map, hub_map + hb, hb));
+        (count_launches(1), hub_merge_kernel<RULE><<<grid_for(H.units, sm_count() * 3), kThreads,
+                                                   kHubPartSmem, st>>>(L, order + hs, H, H.units));
         (count_launches(1), hub_decide_kernel<RULE><<<(hc + 127) / 128, 128, 0, st>>>(
             L, order + hs, H, hc, prop + hs));
       }
@@ -1323,10 +1492,13 @@ static cudaError_t move_bucket_impl(const LevelView& L, int bucket,
 cudaError_t launch_move_bucket(const LevelView& L, int bucket, int rule,
                                const uint32_t* order, uint32_t* proposal,
                                const DispatchPlan& P, const HubArena& H,
-                               cudaStream_t st, const uint32_t* act_cnt) {
+                               cudaStream_t st, const uint32_t* act_cnt,
+                               const uint32_t* hub_map) {
+  if (bucket == 8 && !hub_map) return cudaErrorInvalidValue;
   if (rule == LV_RULE_CUDA_I)
-    return move_bucket_impl<LV_RULE_CUDA_I>(L, bucket, order, proposal, P, H, act_cnt, st);
-  return move_bucket_impl<LV_RULE_PY_I>(L, bucket, order, proposal, P, H, act_cnt, st);
+    return move_bucket_impl<LV_RULE_CUDA_I>(L, bucket, order, proposal, P, H, act_cnt, hub_map,
+                                            st);
+  return move_bucket_impl<LV_RULE_PY_I>(L, bucket, order, proposal, P, H, act_cnt, hub_map, st);
 }
 
 cudaError_t launch_apply_bucket(const LevelView& L, int bucket,

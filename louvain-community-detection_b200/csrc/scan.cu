@@ -217,14 +217,14 @@ struct DegreeClass {
 struct Identity {
   __device__ uint32_t operator()(uint32_t i) const { return i; }
 };
-struct SizeClass3 {
+struct SizeClass4 {
   const uint64_t* sizes;
   const uint32_t* live;  // items i >= *live belong to no class
-  uint64_t lim0, lim1;
+  uint64_t lim0, lim1, lim2;
   __device__ int operator()(uint32_t i) const {
     if (i >= *live) return -1;
     uint64_t s = sizes[i];
-    return s <= lim0 ? 0 : (s <= lim1 ? 1 : 2);
+    return s <= lim0 ? 0 : (s <= lim1 ? 1 : (s <= lim2 ? 2 : 3));
   }
 };
 
@@ -265,12 +265,12 @@ cudaError_t partition_by_degree(const uint64_t* off, uint32_t n,
                                   cls_count, tmp, s, st);
 }
 
-cudaError_t partition_by_size3(const uint64_t* sizes, uint32_t n_upper,
+cudaError_t partition_by_size4(const uint64_t* sizes, uint32_t n_upper,
                                const uint32_t* d_live, uint64_t lim0,
-                               uint64_t lim1, uint32_t* out,
+                               uint64_t lim1, uint64_t lim2, uint32_t* out,
                                uint32_t* cls_count, uint32_t* tmp,
                                ScanScratch& s, cudaStream_t st) {
-  return partition_impl<3>(n_upper, SizeClass3{sizes, d_live, lim0, lim1},
+  return partition_impl<4>(n_upper, SizeClass4{sizes, d_live, lim0, lim1, lim2},
                            Identity{}, out, cls_count, tmp, s, st);
 }
 
