@@ -233,6 +233,58 @@ lv_status lv_batch_run(lv_engine *e, uint32_t n_graphs,
                        uint32_t *assignment, double *modularity,
                        uint32_t *levels, lv_result *res);
 
+/* ---- served form (no counterpart in the reference) ----------------------
+ * Continuous batching of graph requests on one device.  lv_serve_submit
+ * queues a copy of a graph and returns at once (thread-safe beside
+ * lv_serve_step and lv_serve_poll).  Each lv_serve_step admits the queued
+ * graphs that fit (first come first served, while slots and the device
+ * budget last), appends them to the resident union at the level boundary
+ * and runs one level for every resident graph (the batched form's level);
+ * graphs whose run ends are finalised, copied out and leave, freeing their
+ * slot and memory for the next admissions.  Every graph keeps its own m,
+ * modularity, stop rule and levels, so its result equals lv_run on it
+ * alone.  Times are milliseconds on the server's clock (from creation).
+ * After an error other than LV_ERR_ARG / LV_ERR_LIMIT from submit, the
+ * server should be destroyed.                                              */
+typedef struct lv_server lv_server;
+
+typedef struct {
+  uint64_t ticket;
+  double modularity;
+  uint32_t n_vertices;
+  uint32_t n_communities;
+  uint32_t levels;
+  uint32_t reserved;
+  double submit_ms; /* lv_serve_submit */
+  double admit_ms;  /* joined the union */
+  double done_ms;   /* result copied out */
+} lv_serve_result;
+
+typedef struct {
+  uint32_t queued, resident, finished, slot_cap;
+  uint64_t resident_vertices, resident_entries; /* input sizes, resident graphs */
+  uint64_t cap_vertices, cap_entries, budget_bytes;
+  uint64_t steps, admitted, completed;
+} lv_serve_stats;
+
+/* budget_bytes: device memory the server may hold (a fifth for per-vertex
+ * state at 192 B a vertex, the rest for adjacency at 40 B an entry);
+ * max_graphs: resident graphs at most (0: 4096).                           */
+lv_status lv_serve_create(const lv_config *cfg, float min_gain,
+                          uint64_t budget_bytes, uint32_t max_graphs,
+                          lv_server **out);
+lv_status lv_serve_submit(lv_server *s, const lv_graph *g, uint64_t *ticket);
+/* resident / queued (may be NULL): graphs resident and waiting after the
+ * step.  With nothing resident or admissible the step returns at once.    */
+lv_status lv_serve_step(lv_server *s, uint32_t *resident, uint32_t *queued);
+/* Pops the oldest finished request: *got = 1 and its result (assignment:
+ * n_vertices local community ids, may be NULL; cap its capacity), or
+ * *got = 0 when none is finished.                                          */
+lv_status lv_serve_poll(lv_server *s, lv_serve_result *res,
+                        uint32_t *assignment, size_t cap, int *got);
+lv_status lv_serve_get_stats(lv_server *s, lv_serve_stats *out);
+void lv_serve_destroy(lv_server *s);
+
 /* ---- kernel timing (no counterpart in the reference, whose only timers
  * are main.cu:19-56's two regions) --------------------------------------
  * With profiling on, every launch group is bracketed by CUDA events on the

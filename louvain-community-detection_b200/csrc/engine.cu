@@ -13,6 +13,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -930,6 +932,125 @@ lv_status batch_passes(lv_engine* E, float min_gain) {
   return check_device_error(E);
 }
 
+// A graph of the union: its input vertices carry `slot` in graph0 (and
+// gbase[slot] finalises them), it owns `nv` consecutive vertices of the
+// current level.
+struct UnionGraph {
+  uint32_t slot;
+  uint32_t nv;
+  uint32_t levels;  // move phases run so far
+  uint8_t frozen;   // its run ended at the last contraction (merged nothing
+                    // or reached max_levels); only its result is reported
+  double q;         // modularity after its last move phase
+};
+
+// One level of the union.  Every graph that is not frozen runs its pass
+// loop (modularity.cu:438-508, per graph); a graph whose run ends here --
+// frozen, no edge weight, or a first pass below min gain -- has its input
+// vertices' community ids written to `out` local to the graph (through the
+// arena map graph0 -> gbase) and moves to `done`; the others are contracted
+// (aggregation.cu:387-462) and stay in `graphs` with their new sizes, in
+// union order.  The decisions are those run_loaded takes for one graph.
+lv_status union_level(lv_engine* E, std::vector<UnionGraph>& graphs, float min_gain,
+                      uint32_t* out, std::vector<UnionGraph>& done, uint64_t* processed) {
+  cudaStream_t st = E->st;
+  const uint32_t Gl = (uint32_t)graphs.size();
+  E->n_graphs = Gl;
+  std::vector<uint32_t> goff(Gl + 1, 0);
+  bool all_frozen = true;
+  for (uint32_t g = 0; g < Gl; g++) {
+    goff[g + 1] = goff[g] + graphs[g].nv;
+    all_frozen = all_frozen && graphs[g].frozen;
+  }
+  if (goff[Gl] != E->n) return fail(LV_ERR_STATE, "union sizes out of step");
+  if (!all_frozen) {
+    std::vector<GraphState> init(Gl);
+    memset(init.data(), 0, sizeof(GraphState) * Gl);
+    for (uint32_t g = 0; g < Gl; g++) init[g].frozen = graphs[g].frozen;
+    CU(cudaMemcpyAsync(E->gs, init.data(), sizeof(GraphState) * Gl, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(E->goff_dev, goff.data(), (Gl + 1) * sizeof(uint32_t),
+                       cudaMemcpyHostToDevice, st));
+    CU(launch_graph_ids(E->goff_dev, Gl, E->n, E->gid, st));
+    LVTRY(batch_passes(E, min_gain));  // synchronises: init/goff may go
+  }
+  std::vector<uint32_t> base(E->graph_cap, 0xFFFFFFFFu), drop(Gl, 0u);
+  std::vector<uint8_t> last(Gl, 0);
+  bool any_continue = false;
+  uint64_t lvl_passes = 0;
+  for (uint32_t g = 0; g < Gl; g++) {
+    UnionGraph& u = graphs[g];
+    bool ended = true;
+    if (!u.frozen) {
+      const GraphState& s = E->gs_host[g];
+      u.levels++;
+      lvl_passes = std::max<uint64_t>(lvl_passes, s.passes);
+      if (s.passes == 0) u.q = 0.0;                 // no edge weight: nothing moves
+      else if (s.first_fail) u.q = s.q_before;      // the pass's moves are discarded
+      else {
+        u.q = s.q;
+        ended = false;
+        last[g] = E->cfg.max_levels && u.levels >= E->cfg.max_levels;
+      }
+    }
+    if (ended) {
+      base[u.slot] = goff[g];
+      drop[g] = 1u;
+    }
+    any_continue = any_continue || !ended;
+  }
+  if (!all_frozen) {
+    lv_level_info info{};
+    info.n_vertices = E->n;
+    info.n_entries = E->e;
+    info.passes = (uint32_t)lvl_passes;
+    info.moved = any_continue ? 1u : 0u;
+    E->levels.push_back(info);
+    if (processed) *processed += lvl_passes * E->e;
+  }
+  // finalise the graphs that end here
+  CU(cudaMemcpyAsync(E->gbase, base.data(), E->graph_cap * sizeof(uint32_t),
+                     cudaMemcpyHostToDevice, st));
+  CU(launch_finalize_graphs(E->assignment, E->n0, E->graph0, E->gbase, out, st));
+  std::vector<UnionGraph> kept;
+  for (uint32_t g = 0; g < Gl; g++) (drop[g] ? done : kept).push_back(graphs[g]);
+  if (!any_continue) {
+    CU(cudaStreamSynchronize(st));
+    graphs.clear();
+    E->n = 0;
+    E->e = 0;
+    E->level_ready = false;
+    return LV_OK;
+  }
+  // contract the graphs that go on; the others leave the union
+  CU(cudaMemcpyAsync(E->gdrop, drop.data(), Gl * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  CU(launch_drop_graphs(E->comm_sz, E->gid, E->n, E->gdrop, st));
+  E->accepted = true;
+  LVTRY(lv_phase_aggregate(E));  // synchronises
+  // new offsets: the new id of each kept graph's first vertex (flag_id is
+  // the exclusive scan of non-empty communities in old-id order)
+  std::vector<uint32_t> first;
+  for (uint32_t g = 0; g < Gl; g++)
+    if (!drop[g]) first.push_back(goff[g]);
+  const uint32_t Gn = (uint32_t)first.size();
+  CU(cudaMemcpyAsync(E->gbase, first.data(), Gn * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  CU(launch_gather_u32(E->cb.flag_id, E->gbase, Gn, E->goff_dev, st));
+  std::vector<uint32_t> ng(Gn + 1);
+  CU(cudaMemcpyAsync(ng.data(), E->goff_dev, Gn * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  ng[Gn] = E->n;
+  for (uint32_t g = 0, i = 0; g < Gl; g++) {
+    if (drop[g]) continue;
+    UnionGraph& u = kept[i];
+    const uint32_t nv = ng[i + 1] - ng[i];
+    // a level that merged nothing would repeat forever (min gain <= 0)
+    u.frozen = (nv == u.nv || last[g]) ? 1u : 0u;
+    u.nv = nv;
+    i++;
+  }
+  graphs.swap(kept);
+  return LV_OK;
+}
+
 }  // namespace
 
 // Drives the batched run; see lv_batch_run_device in the C ABI.
@@ -944,120 +1065,23 @@ static lv_status batch_run(lv_engine* E, uint32_t G, const uint64_t* goff_in,
     CU(dalloc(&E->act_order, n0));
     E->act_order_cap = n0;
   }
-  // level-0 graph list and input-vertex -> graph map
-  std::vector<uint32_t> goff(G + 1), ids(G);  // level offsets, level -> input graph
+  // input vertex -> graph (its slot)
+  std::vector<uint32_t> goff(G + 1);
   for (uint32_t g = 0; g <= G; g++) goff[g] = (uint32_t)goff_in[g];
-  for (uint32_t g = 0; g < G; g++) ids[g] = g;
   CU(cudaMemcpyAsync(E->goff_dev, goff.data(), (G + 1) * sizeof(uint32_t),
                      cudaMemcpyHostToDevice, st));
-  CU(launch_graph_ids(E->goff_dev, G, n0, E->cb.cursor, st));  // scratch
-  CU(cudaMemcpyAsync(E->graph0, E->cb.cursor, (size_t)n0 * sizeof(uint32_t),
-                     cudaMemcpyDeviceToDevice, st));
-  CU(cudaMemsetAsync(E->gs, 0, sizeof(GraphState) * G, st));
-  std::vector<uint32_t> lv(G, 0), base(G), drop(G);
-  std::vector<uint8_t> fz(G, 0);  // frozen: the graph's run ended at the last contraction
-  std::vector<double> qf(G, 0.0);
+  CU(launch_graph_ids(E->goff_dev, G, n0, E->graph0, st));
+  std::vector<UnionGraph> graphs(G), done;
+  for (uint32_t g = 0; g < G; g++) graphs[g] = UnionGraph{g, goff[g + 1] - goff[g], 0u, 0u, 0.0};
   E->batch = true;
   cudaEvent_t a0, a1;
   CU(cudaEventCreate(&a0));
   CU(cudaEventCreate(&a1));
   CU(cudaEventRecord(a0, st));
-  uint64_t processed = 0, n_comm = 0;
+  uint64_t processed = 0;
   lv_status status = LV_OK;
-  for (;;) {
-    const uint32_t Gl = (uint32_t)ids.size();
-    E->n_graphs = Gl;
-    bool all_frozen = true;
-    for (uint32_t g = 0; g < Gl; g++) all_frozen = all_frozen && fz[g];
-    if (!all_frozen) {
-      CU(cudaMemcpyAsync(E->goff_dev, goff.data(), (Gl + 1) * sizeof(uint32_t),
-                         cudaMemcpyHostToDevice, st));
-      CU(launch_graph_ids(E->goff_dev, Gl, E->n, E->gid, st));
-      status = batch_passes(E, min_gain);
-      if (status != LV_OK) break;
-    }
-    // per graph: its run ends here (frozen, no edge weight, or the first
-    // pass gained too little: modularity.cu:501-508) or goes on to
-    // contraction, as run_loaded decides for a single graph
-    bool any_continue = false;
-    const bool last_level =
-        E->cfg.max_levels && (uint32_t)(E->levels.size() + 1) >= E->cfg.max_levels;
-    uint64_t lvl_passes = 0;
-    for (uint32_t g = 0; g < Gl; g++) {
-      const uint32_t og = ids[g];
-      bool ended = true;
-      if (!fz[g]) {  // a frozen graph keeps the result of its last level
-        const GraphState& s = E->gs_host[g];
-        lv[og]++;
-        lvl_passes = std::max<uint64_t>(lvl_passes, s.passes);
-        if (s.passes == 0) qf[og] = 0.0;  // no edge weight: nothing moves
-        else if (s.first_fail) qf[og] = s.q_before;  // moves of the pass discarded
-        else {
-          qf[og] = s.q;
-          ended = false;
-        }
-      }
-      base[g] = ended ? goff[g] : 0xFFFFFFFFu;
-      drop[g] = ended ? 1u : 0u;
-      if (ended) n_comm += goff[g + 1] - goff[g];
-      any_continue = any_continue || !ended;
-    }
-    if (!all_frozen) {
-      lv_level_info info{};
-      info.n_vertices = E->n;
-      info.n_entries = E->e;
-      info.passes = (uint32_t)lvl_passes;
-      info.moved = any_continue ? 1u : 0u;
-      E->levels.push_back(info);
-      processed += lvl_passes * E->e;
-    }
-    // finalise the graphs that ended here: ids local to their graph
-    {
-      std::vector<uint32_t> b_in(G, 0xFFFFFFFFu);
-      for (uint32_t g = 0; g < Gl; g++)
-        if (drop[g]) b_in[ids[g]] = base[g];
-      CU(cudaMemcpyAsync(E->gbase, b_in.data(), G * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-      CU(launch_finalize_graphs(E->assignment, n0, E->graph0, E->gbase, d_out, st));
-      CU(cudaStreamSynchronize(st));
-    }
-    if (!any_continue) break;
-    // contract the graphs that go on; the others leave the union
-    CU(cudaMemcpyAsync(E->gdrop, drop.data(), Gl * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-    CU(launch_drop_graphs(E->comm_sz, E->gid, E->n, E->gdrop, st));
-    E->accepted = true;
-    status = lv_phase_aggregate(E);
-    if (status != LV_OK) break;
-    // new offsets of the remaining graphs: new id of their first community
-    std::vector<uint32_t> keep_idx, keep_ids;
-    for (uint32_t g = 0; g < Gl; g++)
-      if (!drop[g]) {
-        keep_idx.push_back(goff[g]);
-        keep_ids.push_back(ids[g]);
-      }
-    const uint32_t Gn = (uint32_t)keep_ids.size();
-    CU(cudaMemcpyAsync(E->gbase, keep_idx.data(), Gn * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-    CU(launch_gather_u32(E->cb.flag_id, E->gbase, Gn, E->goff_dev, st));
-    std::vector<uint32_t> ng(Gn + 1);
-    CU(cudaMemcpyAsync(ng.data(), E->goff_dev, Gn * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    CU(cudaStreamSynchronize(st));
-    ng[Gn] = E->n;
-    // a graph whose level merged nothing would repeat forever (min gain
-    // <= 0): freeze it, so its next level ends at once
-    std::vector<GraphState> init(Gn);
-    memset(init.data(), 0, sizeof(GraphState) * Gn);
-    std::vector<uint8_t> nfz(Gn, 0);
-    for (uint32_t g = 0, i = 0; g < Gl; g++) {
-      if (drop[g]) continue;
-      const uint32_t before = goff[g + 1] - goff[g];
-      nfz[i] = (ng[i + 1] - ng[i] == before || last_level) ? 1u : 0u;
-      init[i].frozen = nfz[i];
-      i++;
-    }
-    CU(cudaMemcpyAsync(E->gs, init.data(), sizeof(GraphState) * Gn, cudaMemcpyHostToDevice, st));
-    goff.swap(ng);
-    ids.swap(keep_ids);
-    fz.swap(nfz);
-  }
+  while (!graphs.empty() && status == LV_OK)
+    status = union_level(E, graphs, min_gain, d_out, done, &processed);
   CU(cudaEventRecord(a1, st));
   CU(cudaEventSynchronize(a1));
   float alg = 0.0f;
@@ -1067,10 +1091,12 @@ static lv_status batch_run(lv_engine* E, uint32_t G, const uint64_t* goff_in,
   E->batch = false;
   E->finished = true;
   if (status != LV_OK) return status;
-  if (q_out)
-    for (uint32_t g = 0; g < G; g++) q_out[g] = qf[g];
-  if (levels_out)
-    for (uint32_t g = 0; g < G; g++) levels_out[g] = lv[g];
+  uint64_t n_comm = 0;
+  for (const UnionGraph& u : done) {
+    if (q_out) q_out[u.slot] = u.q;
+    if (levels_out) levels_out[u.slot] = u.levels;
+    n_comm += u.nv;
+  }
   if (res) {
     res->modularity = 0.0;
     res->n_vertices = n0;
@@ -1082,6 +1108,132 @@ static lv_status batch_run(lv_engine* E, uint32_t G, const uint64_t* goff_in,
   }
   return LV_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Served form: continuous batching.  Requests queue on submit; every step
+// admits the queued graphs that fit the device budget (FIFO), appends them
+// to the union at the level boundary -- so a new graph's level 0 runs
+// beside the resident graphs' later levels -- and runs one union level.
+// Graphs whose run ends are finalised, copied out and leave at once; their
+// slots and memory serve the next admissions.  A graph's kernels read only
+// its own rows and state, so its result equals a run of it alone.
+// ---------------------------------------------------------------------------
+namespace {
+
+// Device bytes that a resident vertex / adjacency entry may hold across the
+// engine's buffers (CSR ping-pong, per-vertex state, contraction and hub
+// staging, scans), for admission against the budget.
+constexpr uint64_t kServeBytesPerVertex = 192;
+constexpr uint64_t kServeBytesPerEntry = 40;
+
+struct ServeRequest {
+  uint64_t ticket = 0;
+  lv_graph g;
+  double t_submit = 0.0, t_admit = -1.0, t_done = -1.0;
+  uint32_t slot = 0, a0 = 0;  // slot and arena range while resident
+  double q = 0.0;
+  uint32_t levels = 0, n_comm = 0;
+  std::vector<uint32_t> assignment;
+};
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace
+
+struct lv_server {
+  lv_engine* E = nullptr;
+  float min_gain = 0.0f;
+  uint64_t budget = 0;
+  uint32_t cap_n = 0, slot_cap = 0;
+  uint64_t cap_e = 0;
+  std::mutex mu;  // queue, finished, next_ticket (submit/poll may run beside step)
+  std::deque<ServeRequest*> queue;
+  std::deque<ServeRequest*> finished;
+  uint64_t next_ticket = 1;
+  std::vector<ServeRequest*> by_slot;
+  std::vector<uint32_t> free_slots;
+  std::vector<UnionGraph> graphs;  // resident, in union order
+  uint32_t arena_used = 0;         // input-vertex arena bump pointer
+  uint64_t res_n = 0, res_e = 0;   // input sizes of the resident graphs
+  uint32_t* out = nullptr;         // arena-indexed local ids
+  std::chrono::steady_clock::time_point t0;
+  uint64_t steps = 0, admitted = 0, completed = 0;
+};
+
+namespace {
+
+// Moves the resident graphs' arena ranges to the front (the arena is a bump
+// allocator; finished graphs leave holes).
+lv_status serve_compact(lv_server* S) {
+  lv_engine* E = S->E;
+  cudaStream_t st = E->st;
+  std::vector<ServeRequest*> live;
+  for (const UnionGraph& u : S->graphs) live.push_back(S->by_slot[u.slot]);
+  std::sort(live.begin(), live.end(),
+            [](const ServeRequest* a, const ServeRequest* b) { return a->a0 < b->a0; });
+  uint32_t w = 0;
+  uint32_t* tmp = E->cb.cursor;  // contraction scratch, idle between levels
+  for (ServeRequest* r : live) {
+    CU(cudaMemcpyAsync(tmp + w, E->assignment + r->a0, (size_t)r->g.n * sizeof(uint32_t),
+                       cudaMemcpyDeviceToDevice, st));
+    r->a0 = w;
+    w += r->g.n;
+  }
+  if (w) {
+    CU(cudaMemcpyAsync(E->assignment, tmp, (size_t)w * sizeof(uint32_t),
+                       cudaMemcpyDeviceToDevice, st));
+  }
+  for (ServeRequest* r : live) CU(launch_fill_u32(E->graph0 + r->a0, r->g.n, r->slot, st));
+  S->arena_used = w;
+  E->n0 = w;
+  return LV_OK;
+}
+
+// Appends request r's graph to the union (rows after the current level's
+// last vertex) and gives it an arena range and a slot.
+lv_status serve_append(lv_server* S, ServeRequest* r) {
+  lv_engine* E = S->E;
+  cudaStream_t st = E->st;
+  const lv_graph& g = r->g;
+  if (S->arena_used + g.n > S->cap_n) LVTRY(serve_compact(S));
+  if (E->cur < 0) {  // first graph: the union lives in the contraction buffers
+    E->cur = 0;
+    E->n = 0;
+    E->e = 0;
+  }
+  const int c = E->cur;
+  const uint32_t vb = E->n;
+  const uint64_t eb = E->e;
+  CU(cudaMemcpyAsync(E->c_off[c] + vb, g.off.data(), ((size_t)g.n + 1) * sizeof(uint64_t),
+                     cudaMemcpyHostToDevice, st));
+  CU(launch_add_u64(E->c_off[c] + vb, (size_t)g.n + 1, eb, st));
+  if (g.nnz) {
+    CU(cudaMemcpyAsync(E->c_col[c] + eb, g.col.data(), g.nnz * sizeof(uint32_t),
+                       cudaMemcpyHostToDevice, st));
+    CU(launch_add_u32(E->c_col[c] + eb, g.nnz, vb, st));
+    CU(cudaMemcpyAsync(E->c_w[c] + eb, g.w.data(), g.nnz * sizeof(float),
+                       cudaMemcpyHostToDevice, st));
+  }
+  r->slot = S->free_slots.back();
+  S->free_slots.pop_back();
+  S->by_slot[r->slot] = r;
+  r->a0 = S->arena_used;
+  CU(launch_iota_from(E->assignment + r->a0, g.n, vb, st));
+  CU(launch_fill_u32(E->graph0 + r->a0, g.n, r->slot, st));
+  S->arena_used += g.n;
+  E->n0 = S->arena_used;
+  E->n += g.n;
+  E->e += g.nnz;
+  E->level_ready = false;
+  S->graphs.push_back(UnionGraph{r->slot, g.n, 0u, 0u, 0.0});
+  S->res_n += g.n;
+  S->res_e += g.nnz;
+  return LV_OK;
+}
+
+}  // namespace
 
 // ===========================================================================
 // C ABI
@@ -1620,6 +1772,209 @@ lv_status lv_batch_run(lv_engine* E, uint32_t n_graphs, const lv_graph* const* g
                      E->st));
   CU(cudaStreamSynchronize(E->st));
   return LV_OK;
+}
+
+// ---- served form ----------------------------------------------------------
+lv_status lv_serve_create(const lv_config* cfg, float min_gain, uint64_t budget_bytes,
+                          uint32_t max_graphs, lv_server** out) {
+  if (!out) return fail(LV_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  const uint64_t per_v = kServeBytesPerVertex, per_e = kServeBytesPerEntry;
+  if (budget_bytes < 64 * (per_v + per_e)) return fail(LV_ERR_ARG, "budget too small");
+  lv_server* S = new (std::nothrow) lv_server();
+  if (!S) return fail(LV_ERR_NOMEM, "server allocation failed");
+  lv_status st = lv_engine_create(cfg, &S->E);
+  if (st != LV_OK) {
+    delete S;
+    return st;
+  }
+  lv_engine* E = S->E;
+  // a fifth of the budget for per-vertex state, the rest for adjacency
+  uint64_t cap_n = budget_bytes / 5 / per_v;
+  cap_n = std::min<uint64_t>(cap_n, 0xFFFFFFF0ull);
+  S->cap_n = (uint32_t)cap_n;
+  S->cap_e = (budget_bytes - cap_n * per_v) / per_e;
+  S->slot_cap = max_graphs ? max_graphs : 4096;
+  S->budget = budget_bytes;
+  S->min_gain = min_gain;
+  auto setup = [&]() -> lv_status {
+    LVTRY(ensure_capacity(E, S->cap_n, S->cap_e, false));
+    LVTRY(batch_alloc(E, S->slot_cap));
+    CU(dalloc(&E->act_order, S->cap_n));
+    E->act_order_cap = S->cap_n;
+    CU(dalloc(&S->out, S->cap_n));
+    // every id a stale arena entry can hold stays a valid index: compose
+    // (cnew[assignment]) runs over the whole arena, holes included
+    CU(cudaMemsetAsync(E->cb.cnew, 0, (size_t)S->cap_n * sizeof(uint32_t), E->st));
+    CU(cudaMemsetAsync(E->sc, 0, sizeof(LevelScalars), E->st));
+    CU(cudaStreamSynchronize(E->st));
+    return LV_OK;
+  };
+  st = setup();
+  if (st != LV_OK) {
+    lv_serve_destroy(S);
+    return st;
+  }
+  E->loaded = true;
+  E->batch = true;
+  E->cur = -1;
+  E->n = 0;
+  E->e = 0;
+  E->n0 = 0;
+  S->by_slot.assign(S->slot_cap, nullptr);
+  for (uint32_t i = S->slot_cap; i > 0; i--) S->free_slots.push_back(i - 1);
+  S->t0 = std::chrono::steady_clock::now();
+  *out = S;
+  return LV_OK;
+}
+
+lv_status lv_serve_submit(lv_server* S, const lv_graph* g, uint64_t* ticket) {
+  if (!S || !g) return fail(LV_ERR_ARG, "NULL server or graph");
+  if (g->n > S->cap_n || g->nnz > S->cap_e)
+    return fail(LV_ERR_LIMIT, "graph exceeds the server's device budget");
+  ServeRequest* r = new (std::nothrow) ServeRequest();
+  if (!r) return fail(LV_ERR_NOMEM, "request allocation failed");
+  try {
+    r->g = *g;
+  } catch (const std::bad_alloc&) {
+    delete r;
+    return fail(LV_ERR_NOMEM, "request copy failed");
+  }
+  std::lock_guard<std::mutex> lock(S->mu);
+  r->ticket = S->next_ticket++;
+  r->t_submit = ms_since(S->t0);
+  if (g->n == 0) {  // nothing to run
+    r->t_admit = r->t_done = r->t_submit;
+    S->finished.push_back(r);
+  } else {
+    S->queue.push_back(r);
+  }
+  if (ticket) *ticket = r->ticket;
+  return LV_OK;
+}
+
+lv_status lv_serve_step(lv_server* S, uint32_t* resident, uint32_t* queued) {
+  if (!S) return fail(LV_ERR_ARG, "NULL server");
+  lv_engine* E = S->E;
+  cudaSetDevice(E->device);
+  // admissions, first come first served, while slots and budget last
+  std::vector<ServeRequest*> adm;
+  {
+    std::lock_guard<std::mutex> lock(S->mu);
+    uint64_t tn = S->res_n, te = S->res_e;
+    size_t slots = S->free_slots.size();
+    while (!S->queue.empty()) {
+      ServeRequest* r = S->queue.front();
+      if (!slots || tn + r->g.n > S->cap_n || te + r->g.nnz > S->cap_e) break;
+      adm.push_back(r);
+      S->queue.pop_front();
+      tn += r->g.n;
+      te += r->g.nnz;
+      slots--;
+    }
+  }
+  for (ServeRequest* r : adm) {
+    LVTRY(serve_append(S, r));
+    r->t_admit = ms_since(S->t0);
+    S->admitted++;
+  }
+  if (!S->graphs.empty()) {
+    std::vector<UnionGraph> done;
+    LVTRY(union_level(E, S->graphs, S->min_gain, S->out, done, nullptr));
+    E->levels.clear();
+    S->steps++;
+    for (const UnionGraph& u : done) {
+      ServeRequest* r = S->by_slot[u.slot];
+      r->assignment.resize(r->g.n);
+      CU(cudaMemcpyAsync(r->assignment.data(), S->out + r->a0, (size_t)r->g.n * sizeof(uint32_t),
+                         cudaMemcpyDeviceToHost, E->st));
+      r->q = u.q;
+      r->levels = u.levels;
+      r->n_comm = u.nv;
+    }
+    CU(cudaStreamSynchronize(E->st));
+    const double now = ms_since(S->t0);
+    for (const UnionGraph& u : done) {
+      ServeRequest* r = S->by_slot[u.slot];
+      r->t_done = now;
+      S->by_slot[u.slot] = nullptr;
+      S->free_slots.push_back(u.slot);
+      S->res_n -= r->g.n;
+      S->res_e -= r->g.nnz;
+      S->completed++;
+      std::lock_guard<std::mutex> lock(S->mu);
+      S->finished.push_back(r);
+    }
+    if (S->graphs.empty()) {  // every arena range is free
+      S->arena_used = 0;
+      E->n0 = 0;
+    }
+  }
+  std::lock_guard<std::mutex> lock(S->mu);
+  if (resident) *resident = (uint32_t)S->graphs.size();
+  if (queued) *queued = (uint32_t)S->queue.size();
+  return LV_OK;
+}
+
+lv_status lv_serve_poll(lv_server* S, lv_serve_result* res, uint32_t* assignment, size_t cap,
+                        int* got) {
+  if (!S || !got) return fail(LV_ERR_ARG, "NULL server or flag");
+  *got = 0;
+  ServeRequest* r = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(S->mu);
+    if (S->finished.empty()) return LV_OK;
+    r = S->finished.front();
+    if (assignment && cap < r->g.n) return fail(LV_ERR_ARG, "assignment buffer too small");
+    S->finished.pop_front();
+  }
+  if (res) {
+    memset(res, 0, sizeof(*res));
+    res->ticket = r->ticket;
+    res->modularity = r->q;
+    res->n_vertices = r->g.n;
+    res->n_communities = r->n_comm;
+    res->levels = r->levels;
+    res->submit_ms = r->t_submit;
+    res->admit_ms = r->t_admit;
+    res->done_ms = r->t_done;
+  }
+  if (assignment && r->g.n) memcpy(assignment, r->assignment.data(), r->g.n * sizeof(uint32_t));
+  delete r;
+  *got = 1;
+  return LV_OK;
+}
+
+lv_status lv_serve_get_stats(lv_server* S, lv_serve_stats* out) {
+  if (!S || !out) return fail(LV_ERR_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lock(S->mu);
+  memset(out, 0, sizeof(*out));
+  out->queued = (uint32_t)S->queue.size();
+  out->resident = (uint32_t)S->graphs.size();
+  out->finished = (uint32_t)S->finished.size();
+  out->slot_cap = S->slot_cap;
+  out->resident_vertices = S->res_n;
+  out->resident_entries = S->res_e;
+  out->cap_vertices = S->cap_n;
+  out->cap_entries = S->cap_e;
+  out->budget_bytes = S->budget;
+  out->steps = S->steps;
+  out->admitted = S->admitted;
+  out->completed = S->completed;
+  return LV_OK;
+}
+
+void lv_serve_destroy(lv_server* S) {
+  if (!S) return;
+  for (ServeRequest* r : S->queue) delete r;
+  for (ServeRequest* r : S->finished) delete r;
+  for (ServeRequest* r : S->by_slot) delete r;
+  if (S->E) {
+    cudaSetDevice(S->E->device);
+    dfree(S->out);
+    lv_engine_destroy(S->E);
+  }
+  delete S;
 }
 
 lv_status lv_get_launch_count(uint64_t* count) {

@@ -277,6 +277,11 @@ cudaError_t launch_compose(uint32_t* assignment, size_t n0,
 cudaError_t launch_gather(uint32_t* out, const uint32_t* in, size_t n,
                           const uint32_t* map, cudaStream_t st);
 cudaError_t launch_fill_iota(uint32_t* a, size_t n, cudaStream_t st);
+// Served form: a[i] = start + i; a[i] = v; a[i] += d.
+cudaError_t launch_iota_from(uint32_t* a, size_t n, uint32_t start, cudaStream_t st);
+cudaError_t launch_fill_u32(uint32_t* a, size_t n, uint32_t v, cudaStream_t st);
+cudaError_t launch_add_u32(uint32_t* a, size_t n, uint32_t d, cudaStream_t st);
+cudaError_t launch_add_u64(uint64_t* a, size_t n, uint64_t d, cudaStream_t st);
 // Recompute sizes and totals from comm (used when a caller sets comm).
 cudaError_t launch_recount(const LevelView& L, cudaStream_t st);
 // FP64 modularity of an arbitrary partition (one-off, not hot).

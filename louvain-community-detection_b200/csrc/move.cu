@@ -1278,6 +1278,27 @@ __global__ void iota_kernel(uint32_t* a, size_t n) {
        i += (size_t)gridDim.x * blockDim.x)
     a[i] = (uint32_t)i;
 }
+// Served form: arena and union-append helpers.
+__global__ void iota_from_kernel(uint32_t* a, size_t n, uint32_t start) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    a[i] = start + (uint32_t)i;
+}
+__global__ void fill_u32_kernel(uint32_t* a, size_t n, uint32_t v) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    a[i] = v;
+}
+__global__ void add_u32_kernel(uint32_t* a, size_t n, uint32_t d) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    a[i] += d;
+}
+__global__ void add_u64_kernel(uint64_t* a, size_t n, uint64_t d) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    a[i] += d;
+}
 __global__ void recount_zero_kernel(LevelView L) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n;
        i += gridDim.x * blockDim.x) {
@@ -1684,6 +1705,31 @@ cudaError_t launch_gather_u32(const uint32_t* src, const uint32_t* idx, uint32_t
   if (!n) return cudaSuccess;
   (count_launches(1), gather_u32_kernel<<<grid_for((n + 255) / 256, sm_count() * 8), 256, 0, st>>>(
       src, idx, n, out));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_iota_from(uint32_t* a, size_t n, uint32_t start, cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  (count_launches(1), iota_from_kernel<<<grid_for((n + 255) / 256, sm_count() * 8), 256, 0, st>>>(
+      a, n, start));
+  return cudaGetLastError();
+}
+cudaError_t launch_fill_u32(uint32_t* a, size_t n, uint32_t v, cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  (count_launches(1), fill_u32_kernel<<<grid_for((n + 255) / 256, sm_count() * 8), 256, 0, st>>>(
+      a, n, v));
+  return cudaGetLastError();
+}
+cudaError_t launch_add_u32(uint32_t* a, size_t n, uint32_t d, cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  (count_launches(1), add_u32_kernel<<<grid_for((n + 255) / 256, sm_count() * 8), 256, 0, st>>>(
+      a, n, d));
+  return cudaGetLastError();
+}
+cudaError_t launch_add_u64(uint64_t* a, size_t n, uint64_t d, cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  (count_launches(1), add_u64_kernel<<<grid_for((n + 255) / 256, sm_count() * 8), 256, 0, st>>>(
+      a, n, d));
   return cudaGetLastError();
 }
 

@@ -79,6 +79,23 @@ class KernelStat(ctypes.Structure):
     ]
 
 
+class ServeResult(ctypes.Structure):
+    _fields_ = [("ticket", ctypes.c_uint64), ("modularity", ctypes.c_double),
+                ("n_vertices", ctypes.c_uint32), ("n_communities", ctypes.c_uint32),
+                ("levels", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("submit_ms", ctypes.c_double), ("admit_ms", ctypes.c_double),
+                ("done_ms", ctypes.c_double)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("queued", ctypes.c_uint32), ("resident", ctypes.c_uint32),
+                ("finished", ctypes.c_uint32), ("slot_cap", ctypes.c_uint32),
+                ("resident_vertices", ctypes.c_uint64), ("resident_entries", ctypes.c_uint64),
+                ("cap_vertices", ctypes.c_uint64), ("cap_entries", ctypes.c_uint64),
+                ("budget_bytes", ctypes.c_uint64), ("steps", ctypes.c_uint64),
+                ("admitted", ctypes.c_uint64), ("completed", ctypes.c_uint64)]
+
+
 # symbol -> (restype, argtypes)
 _VP = ctypes.c_void_p
 _U32 = ctypes.c_uint32
@@ -126,6 +143,14 @@ _SIGS = {
                                            ctypes.POINTER(Result)]),
     "lv_batch_run": (ctypes.c_int, [_VP, _U32, _VP, ctypes.c_float, _VP, _VP, _VP,
                                     ctypes.POINTER(Result)]),
+    "lv_serve_create": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.c_float, _U64, _U32,
+                                       ctypes.POINTER(_VP)]),
+    "lv_serve_submit": (ctypes.c_int, [_VP, _VP, ctypes.POINTER(_U64)]),
+    "lv_serve_step": (ctypes.c_int, [_VP, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
+    "lv_serve_poll": (ctypes.c_int, [_VP, ctypes.POINTER(ServeResult), _VP, ctypes.c_size_t,
+                                     ctypes.POINTER(ctypes.c_int)]),
+    "lv_serve_get_stats": (ctypes.c_int, [_VP, ctypes.POINTER(ServeStats)]),
+    "lv_serve_destroy": (None, [_VP]),
 }
 
 NOALLOC_MAX_VERTICES = 1 << 20
@@ -459,3 +484,103 @@ class Engine:
         return {a.name.decode(): dict(launches=a.launches, total_ms=a.total_ms,
                                       bytes=a.bytes)
                 for a in arr[: cnt.value]}
+
+
+@dataclass
+class ServedGraph:
+    ticket: int
+    modularity: float
+    assignment: np.ndarray
+    n_communities: int
+    levels: int
+    submit_ms: float
+    admit_ms: float
+    done_ms: float
+
+
+class Server:
+    """Continuous-batching server (lv_serve_*).  submit() queues a graph;
+    step() admits what fits and runs one level for every resident graph;
+    poll() returns finished requests."""
+
+    def __init__(self, min_gain: float, budget_bytes: int, max_graphs: int = 0,
+                 device: int = 0, rule: str = "py", max_passes: int = 0,
+                 max_levels: int = 0, use_graphs: bool = True, stream: int = 0):
+        cfg = Config()
+        lib().lv_config_default(ctypes.byref(cfg))
+        cfg.device = device
+        cfg.rule = RULES[rule]
+        cfg.max_passes = max_passes
+        cfg.max_levels = max_levels
+        cfg.use_graphs = int(use_graphs)
+        cfg.stream = stream or None
+        h = ctypes.c_void_p()
+        _check(lib().lv_serve_create(ctypes.byref(cfg), min_gain, budget_bytes, max_graphs,
+                                     ctypes.byref(h)))
+        self._h = h
+        self._sizes = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lv_serve_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, g: Graph, n_vertices: int | None = None) -> int:
+        """Queues g; returns its ticket.  n_vertices (if known) saves a
+        look-up of the graph's size."""
+        t = _U64()
+        _check(lib().lv_serve_submit(self._h, g._h, ctypes.byref(t)))
+        self._sizes[t.value] = g.csr()[0] if n_vertices is None else n_vertices
+        return t.value
+
+    def step(self):
+        """One scheduling step; returns (resident, queued) graph counts."""
+        r, q = _U32(), _U32()
+        _check(lib().lv_serve_step(self._h, ctypes.byref(r), ctypes.byref(q)))
+        return r.value, q.value
+
+    def poll(self):
+        """The oldest finished request as a ServedGraph, or None."""
+        cap = max(self._sizes.values(), default=0)
+        buf = np.zeros(max(cap, 1), dtype=np.uint32)
+        res = ServeResult()
+        got = ctypes.c_int()
+        _check(lib().lv_serve_poll(self._h, ctypes.byref(res), _p(buf), buf.size,
+                                   ctypes.byref(got)))
+        if not got.value:
+            return None
+        self._sizes.pop(res.ticket, None)
+        return ServedGraph(res.ticket, res.modularity, buf[: res.n_vertices].copy(),
+                           res.n_communities, res.levels, res.submit_ms, res.admit_ms,
+                           res.done_ms)
+
+    def drain(self):
+        """Steps until nothing is queued or resident; returns the finished
+        requests by ticket."""
+        out = {}
+        while True:
+            r, q = self.step()
+            while (x := self.poll()) is not None:
+                out[x.ticket] = x
+            if r == 0 and q == 0:
+                break
+        while (x := self.poll()) is not None:
+            out[x.ticket] = x
+        return out
+
+    def stats(self) -> dict:
+        st = ServeStats()
+        _check(lib().lv_serve_get_stats(self._h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServeStats._fields_}
