@@ -23,6 +23,9 @@ does not shard); value = edges of all ranks / max-over-ranks time.
   batched    (N=1) the batched form on 4,096 SBM graphs against the plain
              engine looped over the same graphs: graphs/s of each, and whether
              every partition is identical
+  served     (N=1) the served form (continuous batching, 120 GB budget) on
+             Poisson arrivals of R-MAT / LFR-style requests: graphs/s and
+             p50/p99 latency against the plain engine run per request
 --impl reference: the reference's CPU implementation (oracle port) alone.
 """
 from __future__ import annotations
@@ -245,6 +248,126 @@ def batched_measure(stream, count: int, steps: int = 2):
     return res
 
 
+def served_requests(count: int, seed: int):
+    """The served workload's requests (seeded): half R-MAT graphs of scale
+    U{10..21} (1,024 .. 2,097,152 vertices), half LFR-style graphs with
+    log-uniform 1k .. 2M vertices and mixing mu ~ U(0.1, 0.5); unit FP32
+    weights.  Generated on the device, kept as host graphs (the requests
+    arrive from the host).  Returns [(graph, n, entries, kind)]."""
+    import torch
+
+    import lvb200
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        gseed = seed * 100_003 + i
+        if rng.random() < 0.5:
+            scale = int(rng.integers(10, 22))
+            n, off, col, w, _ = lvgen.rmat_device(scale, seed=gseed)
+            kind = f"rmat{scale}"
+        else:
+            n = int(np.exp(rng.uniform(np.log(1_000), np.log(2_000_000))))
+            mu = float(rng.uniform(0.1, 0.5))
+            (n, off, col, w, _), _ = lvgen.lfr_device(n, mu, seed=gseed)
+            kind = "lfr"
+        g = lvb200.Graph.from_csr(n, off.cpu().numpy().view(np.uint64),
+                                  col.cpu().numpy().view(np.uint32), w.cpu().numpy())
+        out.append((g, n, int(col.numel()), kind))
+        del off, col, w
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return out
+
+
+def served_measure(count: int, rate: float, budget: int, seed: int = 0):
+    """Served form under Poisson arrivals (rate per second): every request
+    is submitted to lv_serve at its arrival time (host clock), the loop
+    steps the server and polls results; latency = result time - arrival.
+    Against it, the plain engine runs the same requests one by one through
+    lv_run (host graphs, as the server's are): graphs/s from the summed
+    run times, and the latencies a first-come-first-served single engine
+    would give for the same arrivals."""
+    reqs = served_requests(count, seed)
+    arrivals = np.cumsum(np.random.default_rng(seed + 1).exponential(1.0 / rate, size=count))
+    return served_report(reqs, arrivals, rate, budget)
+
+
+def serve_run(reqs, arrivals, budget):
+    """Replays the arrivals against a server; returns (results by request,
+    completion times, steps, most graphs resident at once)."""
+    import lvb200
+
+    count = len(reqs)
+    with lvb200.Server(MIN_GAIN, budget) as server:
+        # warm-up request (kernel set-up, first graph instantiations)
+        server.submit(reqs[0][0], n_vertices=reqs[0][1])
+        server.drain()
+        ticket_of, done, done_t = {}, {}, np.zeros(count)
+        max_res, i = 0, 0
+        t0 = time.perf_counter()
+        while len(done) < count:
+            now = time.perf_counter() - t0
+            while i < count and arrivals[i] <= now:
+                ticket_of[server.submit(reqs[i][0], n_vertices=reqs[i][1])] = i
+                i += 1
+            r, q = server.step()
+            max_res = max(max_res, r)
+            t = time.perf_counter() - t0
+            while (x := server.poll()) is not None:
+                j = ticket_of[x.ticket]
+                done[j] = x
+                done_t[j] = t
+            if r == 0 and q == 0 and i < count:
+                time.sleep(max(0.0, arrivals[i] - (time.perf_counter() - t0)))
+        stats = server.stats()
+    return done, done_t, int(stats["steps"]), max_res
+
+
+def served_report(reqs, arrivals, rate, budget):
+    import lvb200
+
+    count = len(reqs)
+    done, done_t, steps, max_res = serve_run(reqs, arrivals, budget)
+    lat = (done_t - arrivals) * 1000.0
+    makespan = float(done_t.max() - arrivals[0])
+    # plain engine, one request at a time
+    eng = lvb200.Engine()
+    eng.run(reqs[0][0], MIN_GAIN)
+    svc = np.zeros(count)
+    same, dq = 0, 0.0
+    for j, (g, n, e, kind) in enumerate(reqs):
+        t = time.perf_counter()
+        res = eng.run(g, MIN_GAIN)
+        svc[j] = time.perf_counter() - t
+        same += int(np.array_equal(res.assignment, done[j].assignment))
+        dq = max(dq, abs(res.modularity - done[j].modularity))
+    eng.close()
+    end, plain_lat = 0.0, np.zeros(count)
+    for j in range(count):  # first come first served on one engine
+        end = max(end, arrivals[j]) + svc[j]
+        plain_lat[j] = (end - arrivals[j]) * 1000.0
+    kinds = {}
+    for _, _, _, k in reqs:
+        kinds[k] = kinds.get(k, 0) + 1
+    return {
+        "workload": "served requests", "requests": count, "arrivals": f"Poisson {rate}/s",
+        "mix": "50% R-MAT scale U{10..21}, 50% LFR-style n log-U[1k,2M] mu U(0.1,0.5)",
+        "kinds": kinds, "total_entries": int(sum(r[2] for r in reqs)),
+        "total_vertices": int(sum(r[1] for r in reqs)), "budget_gb": budget / 1e9,
+        "served": {"graphs_per_s": count / makespan, "makespan_s": makespan,
+                   "p50_ms": float(np.percentile(lat, 50)),
+                   "p99_ms": float(np.percentile(lat, 99)),
+                   "max_resident": int(max_res), "steps": steps},
+        "plain_looped": {"graphs_per_s": count / float(svc.sum()),
+                         "total_s": float(svc.sum()),
+                         "p50_ms": float(np.percentile(plain_lat, 50)),
+                         "p99_ms": float(np.percentile(plain_lat, 99))},
+        "speedup_graphs_per_s": float(svc.sum()) / makespan,
+        "partitions_identical": f"{same}/{count}", "max_abs_dq": dq,
+    }
+
+
 def run_reference(args, rank, world):
     n, off, col, ww, desc = workload(args.workload)
     if rank != 0:
@@ -369,9 +492,12 @@ def run_engine(args, rank, world):
             e2e_value = float(t.item())
 
     eng.close()
-    batched = None
+    batched = served = None
     if world == 1 and args.batch_graphs > 0:
         batched = batched_measure(stream, args.batch_graphs)
+    if world == 1 and args.serve_requests > 0:
+        served = served_measure(args.serve_requests, args.serve_rate,
+                                int(args.serve_budget_gb * 1e9))
     if rank != 0:
         return
     # roofline of the dominant kernel group
@@ -411,6 +537,8 @@ def run_engine(args, rank, world):
     }
     if batched:
         line["batched"] = batched
+    if served:
+        line["served"] = served
     if cpu:
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind",
                                                     "sample")}
@@ -427,6 +555,12 @@ def main():
     ap.add_argument("--workload", default="powerlaw")
     ap.add_argument("--batch-graphs", type=int, default=4096,
                     help="graphs of the batched-form measurement (0: skip)")
+    ap.add_argument("--serve-requests", type=int, default=200,
+                    help="requests of the served-form measurement (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=200.0,
+                    help="Poisson arrival rate of the served requests, per second")
+    ap.add_argument("--serve-budget-gb", type=float, default=120.0,
+                    help="device memory budget of the server")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -235,8 +235,9 @@ lv_status lv_batch_run(lv_engine *e, uint32_t n_graphs,
 
 /* ---- served form (no counterpart in the reference) ----------------------
  * Continuous batching of graph requests on one device.  lv_serve_submit
- * queues a copy of a graph and returns at once (thread-safe beside
- * lv_serve_step and lv_serve_poll).  Each lv_serve_step admits the queued
+ * queues a graph by reference and returns at once (thread-safe beside
+ * lv_serve_step and lv_serve_poll); the graph must stay alive and
+ * unchanged until lv_serve_poll has returned its result.  Each lv_serve_step admits the queued
  * graphs that fit (first come first served, while slots and the device
  * budget last), appends them to the resident union at the level boundary
  * and runs one level for every resident graph (the batched form's level);
@@ -283,6 +284,9 @@ lv_status lv_serve_step(lv_server *s, uint32_t *resident, uint32_t *queued);
 lv_status lv_serve_poll(lv_server *s, lv_serve_result *res,
                         uint32_t *assignment, size_t cap, int *got);
 lv_status lv_serve_get_stats(lv_server *s, lv_serve_stats *out);
+/* The server's engine, for lv_set_profiling / lv_get_kernel_stats only
+ * (owned by the server: never load, run or destroy it).                  */
+lv_status lv_serve_engine(lv_server *s, lv_engine **out);
 void lv_serve_destroy(lv_server *s);
 
 /* ---- kernel timing (no counterpart in the reference, whose only timers

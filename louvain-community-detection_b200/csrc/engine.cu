@@ -80,10 +80,19 @@ __global__ void class_degree_kernel(const uint64_t* off, uint32_t n,
   __shared__ unsigned long long s[kClasses];
   if (threadIdx.x < kClasses) s[threadIdx.x] = 0ull;
   __syncthreads();
+  unsigned long long local[kClasses] = {};  // per thread, then per warp
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n;
        v += gridDim.x * blockDim.x) {
     const uint64_t d = off[v + 1] - off[v];
-    atomicAdd(&s[move_class_of_degree(d)], (unsigned long long)d);
+    const int c = move_class_of_degree(d);
+#pragma unroll
+    for (int k = 0; k < kClasses; k++) local[k] += (k == c) ? d : 0ull;
+  }
+#pragma unroll
+  for (int k = 0; k < kClasses; k++) {
+    unsigned long long x = local[k];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0 && x) atomicAdd(&s[k], x);
   }
   __syncthreads();
   if (threadIdx.x < kClasses) atomicAdd(&out[threadIdx.x], s[threadIdx.x]);
@@ -664,6 +673,7 @@ lv_status prepare_level(lv_engine* E) {
       CU(cudaMemcpyAsync(E->act_order + hs, E->order + hs, hc * sizeof(uint32_t),
                          cudaMemcpyDeviceToDevice, st));
   }
+  g_trace.mark("  hub plan", (uint32_t)E->levels.size(), n);
   // entries per move class (byte counts of the kernel timings)
   if (!E->d_class_deg) CU(dalloc(&E->d_class_deg, kClasses));
   CU(cudaMemsetAsync(E->d_class_deg, 0, kClasses * sizeof(unsigned long long), st));
@@ -687,6 +697,7 @@ lv_status prepare_level(lv_engine* E) {
                      cudaMemcpyDeviceToHost, st));
   CU(cudaStreamSynchronize(st));
   prof_collect(E);
+  g_trace.mark("  level init + Q0", (uint32_t)E->levels.size(), n);
   // tables of E->n vertices (blocking host copies above must be done
   // before the vectors go out of scope: synchronised)
   E->level_ready = true;
@@ -804,7 +815,7 @@ lv_status issue_pass(lv_engine* E, const PassControl* ctl) {
   const uint32_t* ac = nullptr;
   if (E->batch) {
     CU(launch_compact_active(E->order, E->plan, E->cg, E->cg_new, E->gs, E->n_graphs,
-                             E->act_cnt, E->act_order, E->st));
+                             E->act_cnt, E->act_order, E->sc, E->st));
     ord = E->act_order;
     ac = E->act_cnt;
   }
@@ -971,7 +982,9 @@ lv_status union_level(lv_engine* E, std::vector<UnionGraph>& graphs, float min_g
     CU(cudaMemcpyAsync(E->goff_dev, goff.data(), (Gl + 1) * sizeof(uint32_t),
                        cudaMemcpyHostToDevice, st));
     CU(launch_graph_ids(E->goff_dev, Gl, E->n, E->gid, st));
+    g_trace.mark("union: level start", (uint32_t)E->levels.size(), E->n);
     LVTRY(batch_passes(E, min_gain));  // synchronises: init/goff may go
+    g_trace.mark("union: passes", (uint32_t)E->levels.size(), E->n);
   }
   std::vector<uint32_t> base(E->graph_cap, 0xFFFFFFFFu), drop(Gl, 0u);
   std::vector<uint8_t> last(Gl, 0);
@@ -1025,7 +1038,9 @@ lv_status union_level(lv_engine* E, std::vector<UnionGraph>& graphs, float min_g
   CU(cudaMemcpyAsync(E->gdrop, drop.data(), Gl * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
   CU(launch_drop_graphs(E->comm_sz, E->gid, E->n, E->gdrop, st));
   E->accepted = true;
+  g_trace.mark("union: finalize", (uint32_t)E->levels.size(), E->n);
   LVTRY(lv_phase_aggregate(E));  // synchronises
+  g_trace.mark("union: contract", (uint32_t)E->levels.size(), E->n);
   // new offsets: the new id of each kept graph's first vertex (flag_id is
   // the exclusive scan of non-empty communities in old-id order)
   std::vector<uint32_t> first;
@@ -1128,7 +1143,9 @@ constexpr uint64_t kServeBytesPerEntry = 40;
 
 struct ServeRequest {
   uint64_t ticket = 0;
-  lv_graph g;
+  const lv_graph* g = nullptr;  // the caller's graph, alive until polled
+  uint32_t n = 0;                // its sizes
+  uint64_t nnz = 0;
   double t_submit = 0.0, t_admit = -1.0, t_done = -1.0;
   uint32_t slot = 0, a0 = 0;  // slot and arena range while resident
   double q = 0.0;
@@ -1176,16 +1193,16 @@ lv_status serve_compact(lv_server* S) {
   uint32_t w = 0;
   uint32_t* tmp = E->cb.cursor;  // contraction scratch, idle between levels
   for (ServeRequest* r : live) {
-    CU(cudaMemcpyAsync(tmp + w, E->assignment + r->a0, (size_t)r->g.n * sizeof(uint32_t),
+    CU(cudaMemcpyAsync(tmp + w, E->assignment + r->a0, (size_t)r->n * sizeof(uint32_t),
                        cudaMemcpyDeviceToDevice, st));
     r->a0 = w;
-    w += r->g.n;
+    w += r->n;
   }
   if (w) {
     CU(cudaMemcpyAsync(E->assignment, tmp, (size_t)w * sizeof(uint32_t),
                        cudaMemcpyDeviceToDevice, st));
   }
-  for (ServeRequest* r : live) CU(launch_fill_u32(E->graph0 + r->a0, r->g.n, r->slot, st));
+  for (ServeRequest* r : live) CU(launch_fill_u32(E->graph0 + r->a0, r->n, r->slot, st));
   S->arena_used = w;
   E->n0 = w;
   return LV_OK;
@@ -1196,7 +1213,7 @@ lv_status serve_compact(lv_server* S) {
 lv_status serve_append(lv_server* S, ServeRequest* r) {
   lv_engine* E = S->E;
   cudaStream_t st = E->st;
-  const lv_graph& g = r->g;
+  const lv_graph& g = *r->g;
   if (S->arena_used + g.n > S->cap_n) LVTRY(serve_compact(S));
   if (E->cur < 0) {  // first graph: the union lives in the contraction buffers
     E->cur = 0;
@@ -1737,30 +1754,33 @@ lv_status lv_batch_run(lv_engine* E, uint32_t n_graphs, const lv_graph* const* g
     eoff[g + 1] = eoff[g] + graphs[g]->nnz;
   }
   if (goff[n_graphs] >= 0xFFFFFFFFull) return fail(LV_ERR_LIMIT, "too many vertices in the batch");
-  lv_graph u;
   const uint32_t N = (uint32_t)goff[n_graphs];
-  try {
-    u.n = N;
-    u.nnz = eoff[n_graphs];
-    for (uint32_t g = 0; g < n_graphs; g++) u.max_deg = std::max(u.max_deg, graphs[g]->max_deg);
-    u.off.resize((size_t)N + 1);
-    u.col.resize(u.nnz);
-    u.w.resize(u.nnz);
-    for (uint32_t g = 0; g < n_graphs; g++) {
-      const lv_graph* h = graphs[g];
-      const uint32_t vb = (uint32_t)goff[g];
-      const uint64_t eb = eoff[g];
-      for (uint32_t v = 0; v < h->n; v++) u.off[vb + v] = eb + h->off[v];
-      for (uint64_t j = 0; j < h->nnz; j++) {
-        u.col[eb + j] = vb + h->col[j];
-        u.w[eb + j] = h->w[j];
-      }
+  const uint64_t NNZ = eoff[n_graphs];
+  cudaSetDevice(E->device);
+  LVTRY(ensure_capacity(E, N, NNZ, true));
+  E->in_off = E->own_off;
+  E->in_col = E->own_col;
+  E->in_w = E->own_w;
+  // the union is assembled on the device: every graph's rows are copied
+  // into place and shifted by its vertex / entry offsets (a graph's last
+  // offset and the next graph's first are the same value)
+  cudaStream_t st = E->st;
+  for (uint32_t g = 0; g < n_graphs; g++) {
+    const lv_graph* h = graphs[g];
+    const uint32_t vb = (uint32_t)goff[g];
+    const uint64_t eb = eoff[g];
+    CU(cudaMemcpyAsync(E->own_off + vb, h->off.data(), ((size_t)h->n + 1) * sizeof(uint64_t),
+                       cudaMemcpyHostToDevice, st));
+    CU(launch_add_u64(E->own_off + vb, (size_t)h->n + 1, eb, st));
+    if (h->nnz) {
+      CU(cudaMemcpyAsync(E->own_col + eb, h->col.data(), h->nnz * sizeof(uint32_t),
+                         cudaMemcpyHostToDevice, st));
+      CU(launch_add_u32(E->own_col + eb, h->nnz, vb, st));
+      CU(cudaMemcpyAsync(E->own_w + eb, h->w.data(), h->nnz * sizeof(float),
+                         cudaMemcpyHostToDevice, st));
     }
-    u.off[N] = u.nnz;
-  } catch (const std::bad_alloc&) {
-    return fail(LV_ERR_NOMEM, "batch does not fit in host memory");
   }
-  LVTRY(lv_engine_load(E, &u));
+  LVTRY(load_common(E, N, NNZ));
   if (N > E->batch_out_cap) {
     dfree(E->batch_out);
     CU(dalloc(&E->batch_out, N));
@@ -1834,12 +1854,9 @@ lv_status lv_serve_submit(lv_server* S, const lv_graph* g, uint64_t* ticket) {
     return fail(LV_ERR_LIMIT, "graph exceeds the server's device budget");
   ServeRequest* r = new (std::nothrow) ServeRequest();
   if (!r) return fail(LV_ERR_NOMEM, "request allocation failed");
-  try {
-    r->g = *g;
-  } catch (const std::bad_alloc&) {
-    delete r;
-    return fail(LV_ERR_NOMEM, "request copy failed");
-  }
+  r->g = g;  // not copied: the caller keeps it alive until the result is polled
+  r->n = g->n;
+  r->nnz = g->nnz;
   std::lock_guard<std::mutex> lock(S->mu);
   r->ticket = S->next_ticket++;
   r->t_submit = ms_since(S->t0);
@@ -1865,19 +1882,21 @@ lv_status lv_serve_step(lv_server* S, uint32_t* resident, uint32_t* queued) {
     size_t slots = S->free_slots.size();
     while (!S->queue.empty()) {
       ServeRequest* r = S->queue.front();
-      if (!slots || tn + r->g.n > S->cap_n || te + r->g.nnz > S->cap_e) break;
+      if (!slots || tn + r->n > S->cap_n || te + r->nnz > S->cap_e) break;
       adm.push_back(r);
       S->queue.pop_front();
-      tn += r->g.n;
-      te += r->g.nnz;
+      tn += r->n;
+      te += r->nnz;
       slots--;
     }
   }
+  g_trace.reset();
   for (ServeRequest* r : adm) {
     LVTRY(serve_append(S, r));
     r->t_admit = ms_since(S->t0);
     S->admitted++;
   }
+  g_trace.mark("serve: admit + append", (uint32_t)adm.size(), E->n);
   if (!S->graphs.empty()) {
     std::vector<UnionGraph> done;
     LVTRY(union_level(E, S->graphs, S->min_gain, S->out, done, nullptr));
@@ -1885,8 +1904,8 @@ lv_status lv_serve_step(lv_server* S, uint32_t* resident, uint32_t* queued) {
     S->steps++;
     for (const UnionGraph& u : done) {
       ServeRequest* r = S->by_slot[u.slot];
-      r->assignment.resize(r->g.n);
-      CU(cudaMemcpyAsync(r->assignment.data(), S->out + r->a0, (size_t)r->g.n * sizeof(uint32_t),
+      r->assignment.resize(r->n);
+      CU(cudaMemcpyAsync(r->assignment.data(), S->out + r->a0, (size_t)r->n * sizeof(uint32_t),
                          cudaMemcpyDeviceToHost, E->st));
       r->q = u.q;
       r->levels = u.levels;
@@ -1899,8 +1918,8 @@ lv_status lv_serve_step(lv_server* S, uint32_t* resident, uint32_t* queued) {
       r->t_done = now;
       S->by_slot[u.slot] = nullptr;
       S->free_slots.push_back(u.slot);
-      S->res_n -= r->g.n;
-      S->res_e -= r->g.nnz;
+      S->res_n -= r->n;
+      S->res_e -= r->nnz;
       S->completed++;
       std::lock_guard<std::mutex> lock(S->mu);
       S->finished.push_back(r);
@@ -1925,21 +1944,21 @@ lv_status lv_serve_poll(lv_server* S, lv_serve_result* res, uint32_t* assignment
     std::lock_guard<std::mutex> lock(S->mu);
     if (S->finished.empty()) return LV_OK;
     r = S->finished.front();
-    if (assignment && cap < r->g.n) return fail(LV_ERR_ARG, "assignment buffer too small");
+    if (assignment && cap < r->n) return fail(LV_ERR_ARG, "assignment buffer too small");
     S->finished.pop_front();
   }
   if (res) {
     memset(res, 0, sizeof(*res));
     res->ticket = r->ticket;
     res->modularity = r->q;
-    res->n_vertices = r->g.n;
+    res->n_vertices = r->n;
     res->n_communities = r->n_comm;
     res->levels = r->levels;
     res->submit_ms = r->t_submit;
     res->admit_ms = r->t_admit;
     res->done_ms = r->t_done;
   }
-  if (assignment && r->g.n) memcpy(assignment, r->assignment.data(), r->g.n * sizeof(uint32_t));
+  if (assignment && r->n) memcpy(assignment, r->assignment.data(), r->n * sizeof(uint32_t));
   delete r;
   *got = 1;
   return LV_OK;
@@ -1961,6 +1980,12 @@ lv_status lv_serve_get_stats(lv_server* S, lv_serve_stats* out) {
   out->steps = S->steps;
   out->admitted = S->admitted;
   out->completed = S->completed;
+  return LV_OK;
+}
+
+lv_status lv_serve_engine(lv_server* S, lv_engine** out) {
+  if (!S || !out) return fail(LV_ERR_ARG, "NULL argument");
+  *out = S->E;
   return LV_OK;
 }
 

@@ -64,7 +64,8 @@ struct LevelScalars {
   double q_prev;         // Q after the previous pass
   double q_before;       // Q before the last pass
   uint32_t any_active;   // some graph's pass loop goes on
-  uint32_t pad;
+  uint32_t act_changed;  // batched form: a graph stopped moving in the last
+                         // pass, so the active lists must be compacted again
 };
 
 // Stop rule evaluated by the modularity sweep's last block when the pass
@@ -266,10 +267,12 @@ cudaError_t launch_class_graph_starts(const uint32_t* order, const DispatchPlan&
                                       cudaStream_t st);
 // Compacted lists of classes 1..7 holding only the vertices of graphs
 // still active (same class offsets as order), lengths into act_cnt[1..7].
+// Skipped on the device while sc->act_changed is 0 (no graph stopped in
+// the last pass).
 cudaError_t launch_compact_active(const uint32_t* order, const DispatchPlan& P,
                                   const uint32_t* cg, uint32_t* cg_new, const GraphState* gs,
                                   uint32_t G, uint32_t* act_cnt, uint32_t* act_order,
-                                  cudaStream_t st);
+                                  const LevelScalars* sc, cudaStream_t st);
 // assignment[i] = map[assignment[i]]
 cudaError_t launch_compose(uint32_t* assignment, size_t n0,
                            const uint32_t* map, cudaStream_t st);

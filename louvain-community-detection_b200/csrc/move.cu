@@ -1172,7 +1172,7 @@ __global__ void __launch_bounds__(kThreads)
   }
   // batched form: every graph's modularity and stop rule; the loop goes on
   // while any graph still gains
-  int any = 0;
+  int any = 0, stopped = 0;
   for (uint32_t g = threadIdx.x; g < L.n_graphs; g += kThreads) {
     GraphState& s = L.gs[g];
     const double gi = __ldcg(&s.intra_acc), gq = __ldcg(&s.asq_acc);
@@ -1192,13 +1192,16 @@ __global__ void __launch_bounds__(kThreads)
       s.q_prev = q;
       s.active = cont ? 1u : 0u;
       any |= cont ? 1 : 0;
+      stopped |= cont ? 0 : 1;
     }
   }
   any = __syncthreads_or(any);
+  stopped = __syncthreads_or(stopped);
   if (threadIdx.x == 0) {
     L.sc->done_blocks = 0u;
     if (ctl.enabled) {
       L.sc->any_active = any ? 1u : 0u;
+      L.sc->act_changed = stopped ? 1u : 0u;
       if (ctl.use_handle)
         cudaGraphSetConditional((cudaGraphConditionalHandle)ctl.handle, any ? 1u : 0u);
     }
@@ -1214,6 +1217,7 @@ __global__ void pass_control_init_kernel(LevelScalars* sc, GraphState* gs,
     sc->q_prev = sc->q;
     sc->q_before = sc->q;
     sc->any_active = 1u;
+    sc->act_changed = 1u;  // the first pass builds the active lists
   }
   for (uint32_t g = t; g < n_graphs; g += gridDim.x * blockDim.x) {
     GraphState& s = gs[g];
@@ -1573,10 +1577,12 @@ __global__ void class_graph_starts_kernel(const uint32_t* __restrict__ order, Cl
 
 // One block per class: exclusive scan over graphs of the active run
 // lengths -> each active run's place in the compacted list, and the
-// class's active count.
+// class's active count.  Skipped while the active set is unchanged.
 __global__ void __launch_bounds__(1024)
     compact_scan_kernel(const uint32_t* __restrict__ cg, const GraphState* __restrict__ gs,
-                        uint32_t G, uint32_t* __restrict__ cg_new, uint32_t* __restrict__ act_cnt) {
+                        uint32_t G, uint32_t* __restrict__ cg_new, uint32_t* __restrict__ act_cnt,
+                        const LevelScalars* __restrict__ sc) {
+  if (!sc->act_changed) return;  // block-uniform
   __shared__ uint32_t warp_tot[32];
   __shared__ uint32_t carry;
   const uint32_t per = G + 1, c = blockIdx.x;
@@ -1615,23 +1621,31 @@ __global__ void __launch_bounds__(1024)
   if (threadIdx.x == 0) act_cnt[1 + c] = carry;
 }
 
-// One warp per (class, graph): copies an active graph's run.
+// Fills the compacted lists: one thread per output position (blockIdx.y =
+// class), its graph found by binary search over the runs' new starts (an
+// inactive graph's empty run shares its start with the next graph, and the
+// search takes the last of equal starts).  Skipped while the active set is
+// unchanged.
 __global__ void compact_copy_kernel(const uint32_t* __restrict__ order, ClassStarts cs,
                                     const uint32_t* __restrict__ cg,
                                     const uint32_t* __restrict__ cg_new,
-                                    const GraphState* __restrict__ gs, uint32_t G,
-                                    uint32_t* __restrict__ act_order) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-  for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < kMoveClasses * G;
-       t += warps) {
-    const uint32_t ci = t / G, g = t % G;
-    if (!gs[g].active) continue;  // warp-uniform
-    const uint32_t per = G + 1;
-    const uint32_t a = cg[ci * per + g], e = cg[ci * per + g + 1];
-    const uint32_t base = cs.s[ci + 1];
-    const uint32_t dst = base + cg_new[ci * per + g];
-    for (uint32_t i = a + lane; i < e; i += 32) act_order[dst + (i - a)] = order[base + i];
+                                    const uint32_t* __restrict__ act_cnt, uint32_t G,
+                                    uint32_t* __restrict__ act_order,
+                                    const LevelScalars* __restrict__ sc) {
+  if (!sc->act_changed) return;
+  const uint32_t ci = blockIdx.y, per = G + 1;
+  const uint32_t total = act_cnt[1 + ci];
+  const uint32_t* row = cg + ci * per;
+  const uint32_t* row_new = cg_new + ci * per;
+  const uint32_t base = cs.s[ci + 1];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = G - 1;  // last g with row_new[g] <= i
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (row_new[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    act_order[base + i] = order[base + row[lo] + (i - row_new[lo])];
   }
 }
 
@@ -1650,14 +1664,21 @@ cudaError_t launch_class_graph_starts(const uint32_t* order, const DispatchPlan&
 cudaError_t launch_compact_active(const uint32_t* order, const DispatchPlan& P,
                                   const uint32_t* cg, uint32_t* cg_new, const GraphState* gs,
                                   uint32_t G, uint32_t* act_cnt, uint32_t* act_order,
-                                  cudaStream_t st) {
+                                  const LevelScalars* sc, cudaStream_t st) {
   ClassStarts cs;
   for (int c = 0; c <= kClasses; c++) cs.s[c] = P.cls_start[c];
   if (!G) return cudaSuccess;
-  (count_launches(1), compact_scan_kernel<<<kMoveClasses, 1024, 0, st>>>(cg, gs, G, cg_new, act_cnt));
-  const uint32_t warps = kMoveClasses * G;
-  (count_launches(1), compact_copy_kernel<<<grid_for((warps + 7) / 8, sm_count() * 8), 256, 0, st>>>(
-      order, cs, cg, cg_new, gs, G, act_order));
+  (count_launches(1), compact_scan_kernel<<<kMoveClasses, 1024, 0, st>>>(cg, gs, G, cg_new, act_cnt,
+                                                                         sc));
+  // grid sized for the largest class; each class's threads stop at its
+  // active count
+  uint32_t most = 0;
+  for (int c = 1; c <= kMoveClasses; c++) most = std::max(most, P.cls_start[c + 1] - P.cls_start[c]);
+  if (most) {
+    const dim3 grid(grid_for((most + 255) / 256, sm_count() * 2), kMoveClasses);
+    (count_launches(1), compact_copy_kernel<<<grid, 256, 0, st>>>(order, cs, cg, cg_new, act_cnt, G,
+                                                                  act_order, sc));
+  }
   return cudaGetLastError();
 }
 

@@ -151,6 +151,7 @@ _SIGS = {
                                      ctypes.POINTER(ctypes.c_int)]),
     "lv_serve_get_stats": (ctypes.c_int, [_VP, ctypes.POINTER(ServeStats)]),
     "lv_serve_destroy": (None, [_VP]),
+    "lv_serve_engine": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
 }
 
 NOALLOC_MAX_VERTICES = 1 << 20
@@ -519,6 +520,7 @@ class Server:
                                      ctypes.byref(h)))
         self._h = h
         self._sizes = {}
+        self._graphs = {}
 
     def close(self):
         if getattr(self, "_h", None):
@@ -543,6 +545,7 @@ class Server:
         t = _U64()
         _check(lib().lv_serve_submit(self._h, g._h, ctypes.byref(t)))
         self._sizes[t.value] = g.csr()[0] if n_vertices is None else n_vertices
+        self._graphs[t.value] = g  # the server reads it until the result is polled
         return t.value
 
     def step(self):
@@ -562,6 +565,7 @@ class Server:
         if not got.value:
             return None
         self._sizes.pop(res.ticket, None)
+        self._graphs.pop(res.ticket, None)
         return ServedGraph(res.ticket, res.modularity, buf[: res.n_vertices].copy(),
                            res.n_communities, res.levels, res.submit_ms, res.admit_ms,
                            res.done_ms)
@@ -579,6 +583,21 @@ class Server:
         while (x := self.poll()) is not None:
             out[x.ticket] = x
         return out
+
+    def set_profiling(self, on: bool = True):
+        _check(lib().lv_set_profiling(self._engine(), int(on)))
+
+    def kernel_stats(self) -> dict:
+        arr = (KernelStat * 32)()
+        cnt = _U32()
+        _check(lib().lv_get_kernel_stats(self._engine(), arr, 32, ctypes.byref(cnt)))
+        return {a.name.decode(): dict(launches=a.launches, total_ms=a.total_ms, bytes=a.bytes)
+                for a in arr[: cnt.value]}
+
+    def _engine(self):
+        e = ctypes.c_void_p()
+        _check(lib().lv_serve_engine(self._h, ctypes.byref(e)))
+        return e
 
     def stats(self) -> dict:
         st = ServeStats()

@@ -378,6 +378,89 @@ def sbm_batch_device(count: int, seed: int = 0, lo: int = 64, hi: int = 65_536,
     return goff, off, cols, ww, n_edges
 
 
+def _csr_device(n, a, b, device):
+    """Symmetric CSR (rows ascending, each row's entries in key order) of
+    the undirected edges a < b (int64 tensors), unit FP32 weights."""
+    import torch
+
+    rows = torch.cat([a, b])
+    cols = torch.cat([b, a])
+    rows, order = torch.sort(rows, stable=True)
+    cols = cols[order].to(torch.int32)
+    del order
+    counts = torch.bincount(rows, minlength=n)
+    del rows
+    off = torch.zeros(n + 1, dtype=torch.int64, device=device)
+    off[1:] = torch.cumsum(counts, 0)
+    w = torch.ones(cols.numel(), dtype=torch.float32, device=device)
+    return off, cols, w
+
+
+def lfr_device(n: int, mu: float, seed: int = 0, gamma: float = 2.3, beta: float = 1.5,
+               mean_deg: float = 16.0, cmin: int = 20, device: str = "cuda"):
+    """LFR-style benchmark graph generated on the device (torch): vertex
+    degrees from a power law (exponent gamma, mean about mean_deg, maximum
+    about 2 sqrt(n)), community sizes from a power law (exponent beta,
+    cmin .. n/10), a fraction mu of every vertex's edges to uniform random
+    vertices and the rest to uniform members of its own community (the
+    degree cap and merged duplicates leave a mean degree somewhat below
+    mean_deg).  Self-loops dropped, unit FP32 weights.  Returns
+    (n, off int64[n+1], col int32[E], w float32[E], n_edges) on `device`
+    and the community of every vertex (numpy)."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    # community sizes, then a random placement of vertices into them
+    cmax = max(cmin + 1, n // 10)
+    sizes = []
+    total = 0
+    while total < n:
+        u = rng.random()
+        lo_, hi_ = cmin ** (1 - beta), cmax ** (1 - beta)
+        s = int((lo_ + u * (hi_ - lo_)) ** (1 / (1 - beta)))
+        s = min(max(s, cmin), n - total) if n - total >= cmin else n - total
+        sizes.append(s)
+        total += s
+    sizes = np.array(sizes, dtype=np.int64)
+    starts = np.r_[0, np.cumsum(sizes)[:-1]]
+    perm = rng.permutation(n)  # position p of the community layout -> vertex id
+    comm_of_pos = np.repeat(np.arange(len(sizes)), sizes)
+    comm = np.empty(n, dtype=np.int64)
+    comm[perm] = comm_of_pos
+    # degrees (halved: every stub makes one edge, seen from both ends)
+    kmax = max(8.0, 2.0 * np.sqrt(n))
+    kmin = max(1.0, mean_deg * (gamma - 2) / (gamma - 1))
+    T = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(device)
+    u = torch.rand(n, generator=gen, device=device, dtype=torch.float64)
+    deg = kmin * (1 - u) ** (-1.0 / (gamma - 1))
+    deg = torch.clamp(deg, max=kmax)
+    stubs = torch.clamp((deg / 2).round().to(torch.int64), min=1)
+    pos_of_v = T(np.argsort(perm))  # vertex -> layout position
+    t_perm, t_sizes, t_starts = T(perm), T(sizes), T(starts)
+    t_comm = T(comm)
+    src = torch.repeat_interleave(torch.arange(n, device=device), stubs)
+    m = src.numel()
+    ext = torch.rand(m, generator=gen, device=device) < mu
+    c = t_comm[src]
+    r = torch.rand(m, generator=gen, device=device, dtype=torch.float64)
+    internal = t_perm[t_starts[c] + torch.minimum((r * t_sizes[c]).to(torch.int64), t_sizes[c] - 1)]
+    external = torch.minimum((r * n).to(torch.int64), torch.tensor(n - 1, device=device))
+    dst = torch.where(ext, external, internal)
+    del ext, c, r, internal, external, pos_of_v
+    keep = src != dst
+    a = torch.minimum(src, dst)[keep]
+    b = torch.maximum(src, dst)[keep]
+    del src, dst, keep
+    key = torch.unique(a * n + b)
+    a, b = key // n, key % n
+    del key
+    n_edges = int(a.numel())
+    off, col, w = _csr_device(n, a, b, device)
+    return (n, off, col, w, n_edges), comm
+
+
 def localize_batch(goff, off, col):
     """Per-graph CSR views of a block-diagonal union, for running the
     graphs one by one: returns (loff int64[N+G], lcol int32[E]) where graph
