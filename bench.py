@@ -418,7 +418,8 @@ def run_engine(args, rank, world):
     d_asg = torch.empty(n, dtype=torch.int32, device="cuda")
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB
     torch.cuda.synchronize()
-    eng = lvb200.Engine(device=dev, rule="py", stream=stream.cuda_stream)
+    eng = lvb200.Engine(device=dev, rule="py", stream=stream.cuda_stream,
+                        use_graphs=not args.no_graphs)
 
     def step():
         return eng.run_device(n, nnz, d_off.data_ptr(), d_col.data_ptr(),
@@ -514,7 +515,8 @@ def run_engine(args, rank, world):
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": dict(desc, parallelism="replicas only" if world > 1 else "single GPU",
-                       l2="flushed (256 MB write) between timed steps"),
+                       l2="flushed (256 MB write) between timed steps",
+                       pass_loop="host loop" if args.no_graphs else "CUDA graph WHILE node"),
         "final_q": q,
         "levels": [{"V": l["n_vertices"], "E": l["n_entries"], "passes": l["passes"],
                     "prepare_ms": round(l["prepare_ms"], 4),
@@ -553,6 +555,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="powerlaw")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="run each level's pass loop from the host instead of a CUDA graph "
+                         "WHILE node (same kernels; ncu cannot profile kernels inside "
+                         "graphs with conditional nodes)")
     ap.add_argument("--batch-graphs", type=int, default=4096,
                     help="graphs of the batched-form measurement (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=200,
