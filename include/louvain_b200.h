@@ -235,19 +235,42 @@ lv_status lv_batch_run(lv_engine *e, uint32_t n_graphs,
 
 /* ---- served form (no counterpart in the reference) ----------------------
  * Continuous batching of graph requests on one device.  lv_serve_submit
- * queues a graph by reference and returns at once (thread-safe beside
- * lv_serve_step and lv_serve_poll); the graph must stay alive and
- * unchanged until lv_serve_poll has returned its result.  Each lv_serve_step admits the queued
- * graphs that fit (first come first served, while slots and the device
- * budget last), appends them to the resident union at the level boundary
- * and runs one level for every resident graph (the batched form's level);
- * graphs whose run ends are finalised, copied out and leave, freeing their
- * slot and memory for the next admissions.  Every graph keeps its own m,
+ * queues a graph by reference and returns at once (thread-safe beside the
+ * other calls); the graph must stay alive and unchanged until
+ * lv_serve_poll has returned its result.  A request goes to the first lane
+ * whose size bound holds its entries; a lane is one union of resident
+ * graphs with its own engine, stream and share of the device budget.  A
+ * lane's step admits its queued graphs that fit (first come first served,
+ * while slots and budget last), appends them to its union at the level
+ * boundary and runs one level for every resident graph (the batched form's
+ * level); graphs whose run ends are finalised, copied out and leave,
+ * freeing their slot and memory for the next admissions.  Separate lanes
+ * keep small graphs from waiting on the levels of large ones, and with
+ * `background` set every lane is stepped by its own worker thread, so the
+ * lanes run concurrently on the device.  Every graph keeps its own m,
  * modularity, stop rule and levels, so its result equals lv_run on it
  * alone.  Times are milliseconds on the server's clock (from creation).
- * After an error other than LV_ERR_ARG / LV_ERR_LIMIT from submit, the
- * server should be destroyed.                                              */
+ * After an error other than LV_ERR_ARG / LV_ERR_LIMIT the server should be
+ * destroyed.                                                               */
 typedef struct lv_server lv_server;
+
+typedef struct {
+  float min_gain;
+  uint64_t budget_bytes;         /* device memory for all lanes */
+  uint32_t max_graphs;           /* resident graphs per lane (0: 4096) */
+  uint32_t n_lanes;              /* 1..4 */
+  uint64_t lane_max_entries[4];  /* lane i takes requests with at most this
+                                    many entries (ascending; the last lane
+                                    takes the rest) */
+  float lane_share[4];           /* share of the budget per lane */
+  int background;                /* step the lanes on worker threads */
+} lv_serve_config;
+
+/* 3 background lanes: <= 2^18 entries (15% of the budget), <= 2^23 (35%),
+ * larger (50%); budget 8 GiB; min_gain 1e-6.  Each lane holds a fifth of
+ * its budget for per-vertex state at 192 B a vertex and the rest for
+ * adjacency at 40 B an entry.                                              */
+void lv_serve_config_default(lv_serve_config *c);
 
 typedef struct {
   uint64_t ticket;
@@ -255,38 +278,38 @@ typedef struct {
   uint32_t n_vertices;
   uint32_t n_communities;
   uint32_t levels;
-  uint32_t reserved;
+  uint32_t lane;
   double submit_ms; /* lv_serve_submit */
-  double admit_ms;  /* joined the union */
+  double admit_ms;  /* joined a union */
   double done_ms;   /* result copied out */
 } lv_serve_result;
 
 typedef struct {
-  uint32_t queued, resident, finished, slot_cap;
+  uint32_t queued, resident, finished, slot_cap, n_lanes;
   uint64_t resident_vertices, resident_entries; /* input sizes, resident graphs */
   uint64_t cap_vertices, cap_entries, budget_bytes;
   uint64_t steps, admitted, completed;
 } lv_serve_stats;
 
-/* budget_bytes: device memory the server may hold (a fifth for per-vertex
- * state at 192 B a vertex, the rest for adjacency at 40 B an entry);
- * max_graphs: resident graphs at most (0: 4096).                           */
-lv_status lv_serve_create(const lv_config *cfg, float min_gain,
-                          uint64_t budget_bytes, uint32_t max_graphs,
+lv_status lv_serve_create(const lv_config *cfg, const lv_serve_config *scfg,
                           lv_server **out);
 lv_status lv_serve_submit(lv_server *s, const lv_graph *g, uint64_t *ticket);
-/* resident / queued (may be NULL): graphs resident and waiting after the
- * step.  With nothing resident or admissible the step returns at once.    */
+/* Without background workers: one step of every lane.  With them: nothing
+ * to do.  resident / queued (may be NULL): graphs resident and waiting.    */
 lv_status lv_serve_step(lv_server *s, uint32_t *resident, uint32_t *queued);
+/* Blocks (background mode) until a result is ready, nothing is queued or
+ * resident, or timeout_ms passes; *idle (may be NULL) = 1 when nothing is
+ * queued, resident or waiting to be polled.                                */
+lv_status lv_serve_wait(lv_server *s, uint32_t timeout_ms, int *idle);
 /* Pops the oldest finished request: *got = 1 and its result (assignment:
  * n_vertices local community ids, may be NULL; cap its capacity), or
  * *got = 0 when none is finished.                                          */
 lv_status lv_serve_poll(lv_server *s, lv_serve_result *res,
                         uint32_t *assignment, size_t cap, int *got);
 lv_status lv_serve_get_stats(lv_server *s, lv_serve_stats *out);
-/* The server's engine, for lv_set_profiling / lv_get_kernel_stats only
- * (owned by the server: never load, run or destroy it).                  */
-lv_status lv_serve_engine(lv_server *s, lv_engine **out);
+/* A lane's engine, for lv_set_profiling / lv_get_kernel_stats only (owned
+ * by the server: never load, run or destroy it).                           */
+lv_status lv_serve_engine(lv_server *s, uint32_t lane, lv_engine **out);
 void lv_serve_destroy(lv_server *s);
 
 /* ---- kernel timing (no counterpart in the reference, whose only timers

@@ -13,10 +13,13 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <condition_variable>
 #include <deque>
 #include <mutex>
+#include <thread>
 #include <new>
 #include <string>
+#include <system_error>
 #include <vector>
 
 #include "../../include/louvain_b200.h"
@@ -52,16 +55,32 @@ lv_status cuda_fail(cudaError_t e, const char* what) {
     if (s_ != LV_OK) return s_;       \
   } while (0)
 
+// Device buffers are stream-ordered allocations on the calling engine's
+// stream (set by AllocScope in every entry point), so growing a buffer never
+// synchronises the whole device -- several engines (the server's lanes)
+// run side by side.  Without a scope: plain cudaMalloc / cudaFree.
+thread_local cudaStream_t t_alloc_stream = nullptr;
+
+struct AllocScope {
+  cudaStream_t prev;
+  explicit AllocScope(cudaStream_t s) : prev(t_alloc_stream) { t_alloc_stream = s; }
+  ~AllocScope() { t_alloc_stream = prev; }
+};
+
 template <typename T>
 cudaError_t dalloc(T** p, size_t count) {
   *p = nullptr;
   if (count == 0) count = 1;
+  if (t_alloc_stream) return cudaMallocAsync((void**)p, count * sizeof(T), t_alloc_stream);
   return cudaMalloc((void**)p, count * sizeof(T));
 }
 
 template <typename T>
 void dfree(T*& p) {
-  if (p) cudaFree((void*)p);
+  if (p) {
+    if (t_alloc_stream) cudaFreeAsync((void*)p, t_alloc_stream);
+    else cudaFree((void*)p);
+  }
   p = nullptr;
 }
 
@@ -138,13 +157,15 @@ struct Trace {
   void mark(const char* what, uint32_t level, uint32_t n) {
     if (!on) return;
     const auto t = std::chrono::steady_clock::now();
-    fprintf(stderr, "[lvb200] level=%u V=%u %-28s %9.3f ms\n", level, n, what,
+    static std::atomic<int> next_id{0};
+    thread_local int id = next_id++;
+    fprintf(stderr, "[lvb200] t%d level=%u V=%u %-28s %9.3f ms\n", id, level, n, what,
             std::chrono::duration<double, std::milli>(t - t0).count());
     t0 = t;
   }
   void reset() { t0 = std::chrono::steady_clock::now(); }
 };
-Trace g_trace;
+thread_local Trace g_trace;  // per thread: server lanes step concurrently
 }  // namespace
 
 namespace lvb {
@@ -1125,13 +1146,18 @@ static lv_status batch_run(lv_engine* E, uint32_t G, const uint64_t* goff_in,
 }
 
 // ---------------------------------------------------------------------------
-// Served form: continuous batching.  Requests queue on submit; every step
-// admits the queued graphs that fit the device budget (FIFO), appends them
-// to the union at the level boundary -- so a new graph's level 0 runs
-// beside the resident graphs' later levels -- and runs one union level.
-// Graphs whose run ends are finalised, copied out and leave at once; their
-// slots and memory serve the next admissions.  A graph's kernels read only
-// its own rows and state, so its result equals a run of it alone.
+// Served form: continuous batching.  Requests queue on submit, routed by
+// size to one of up to four lanes; a lane is one union of resident graphs
+// on its own engine and stream.  Every step of a lane admits its queued
+// graphs that fit its share of the device budget (FIFO), appends them to
+// its union at the level boundary -- so a new graph's level 0 runs beside
+// the resident graphs' later levels -- and runs one union level; graphs
+// whose run ends are finalised, copied out and leave at once, freeing their
+// slots and memory.  Lanes keep small graphs from being paced by large
+// ones (a union level lasts as long as its slowest graph's pass loop) and,
+// stepped by worker threads, run concurrently on the device.  A graph's
+// kernels read only its own rows and state, so its result equals a run of
+// it alone.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -1144,10 +1170,10 @@ constexpr uint64_t kServeBytesPerEntry = 40;
 struct ServeRequest {
   uint64_t ticket = 0;
   const lv_graph* g = nullptr;  // the caller's graph, alive until polled
-  uint32_t n = 0;                // its sizes
+  uint32_t n = 0;               // its sizes
   uint64_t nnz = 0;
   double t_submit = 0.0, t_admit = -1.0, t_done = -1.0;
-  uint32_t slot = 0, a0 = 0;  // slot and arena range while resident
+  uint32_t lane = 0, slot = 0, a0 = 0;  // lane, slot and arena range while resident
   double q = 0.0;
   uint32_t levels = 0, n_comm = 0;
   std::vector<uint32_t> assignment;
@@ -1157,37 +1183,50 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// One union of resident graphs on its own engine (and stream).
+struct ServeLane {
+  lv_engine* E = nullptr;
+  uint64_t max_entries = 0;  // routing: requests with at most this many entries
+  uint32_t cap_n = 0, slot_cap = 0;
+  uint64_t cap_e = 0;
+  std::deque<ServeRequest*> queue;  // guarded by lv_server::mu
+  std::vector<ServeRequest*> by_slot;
+  std::vector<uint32_t> free_slots;
+  std::vector<UnionGraph> graphs;   // resident, in union order (lane thread only)
+  uint32_t arena_used = 0;          // input-vertex arena bump pointer
+  uint64_t res_n = 0, res_e = 0;    // input sizes of the resident graphs (under mu)
+  uint32_t n_res = 0;               // resident graphs (under mu)
+  uint32_t* out = nullptr;          // arena-indexed local ids
+  uint64_t steps = 0, admitted = 0, completed = 0;
+  std::thread worker;
+  cudaStream_t stream = nullptr;  // created for the lane (priority by size)
+};
+
 }  // namespace
 
 struct lv_server {
-  lv_engine* E = nullptr;
-  float min_gain = 0.0f;
-  uint64_t budget = 0;
-  uint32_t cap_n = 0, slot_cap = 0;
-  uint64_t cap_e = 0;
-  std::mutex mu;  // queue, finished, next_ticket (submit/poll may run beside step)
-  std::deque<ServeRequest*> queue;
+  lv_serve_config cfg{};
+  std::vector<ServeLane*> lanes;
+  std::mutex mu;  // queues, finished, counters shared with submit / poll
+  std::condition_variable cv_work, cv_done;
   std::deque<ServeRequest*> finished;
   uint64_t next_ticket = 1;
-  std::vector<ServeRequest*> by_slot;
-  std::vector<uint32_t> free_slots;
-  std::vector<UnionGraph> graphs;  // resident, in union order
-  uint32_t arena_used = 0;         // input-vertex arena bump pointer
-  uint64_t res_n = 0, res_e = 0;   // input sizes of the resident graphs
-  uint32_t* out = nullptr;         // arena-indexed local ids
+  uint32_t busy = 0;  // lanes in the middle of a step
+  bool stop = false;
+  lv_status bg_status = LV_OK;  // first failure of a lane worker
+  std::string bg_error;
   std::chrono::steady_clock::time_point t0;
-  uint64_t steps = 0, admitted = 0, completed = 0;
 };
 
 namespace {
 
 // Moves the resident graphs' arena ranges to the front (the arena is a bump
 // allocator; finished graphs leave holes).
-lv_status serve_compact(lv_server* S) {
-  lv_engine* E = S->E;
+lv_status serve_compact(ServeLane* L) {
+  lv_engine* E = L->E;
   cudaStream_t st = E->st;
   std::vector<ServeRequest*> live;
-  for (const UnionGraph& u : S->graphs) live.push_back(S->by_slot[u.slot]);
+  for (const UnionGraph& u : L->graphs) live.push_back(L->by_slot[u.slot]);
   std::sort(live.begin(), live.end(),
             [](const ServeRequest* a, const ServeRequest* b) { return a->a0 < b->a0; });
   uint32_t w = 0;
@@ -1203,18 +1242,18 @@ lv_status serve_compact(lv_server* S) {
                        cudaMemcpyDeviceToDevice, st));
   }
   for (ServeRequest* r : live) CU(launch_fill_u32(E->graph0 + r->a0, r->n, r->slot, st));
-  S->arena_used = w;
+  L->arena_used = w;
   E->n0 = w;
   return LV_OK;
 }
 
-// Appends request r's graph to the union (rows after the current level's
-// last vertex) and gives it an arena range and a slot.
-lv_status serve_append(lv_server* S, ServeRequest* r) {
-  lv_engine* E = S->E;
+// Appends request r's graph to the lane's union (rows after the current
+// level's last vertex) and gives it an arena range and a slot.
+lv_status serve_append(ServeLane* L, ServeRequest* r) {
+  lv_engine* E = L->E;
   cudaStream_t st = E->st;
   const lv_graph& g = *r->g;
-  if (S->arena_used + g.n > S->cap_n) LVTRY(serve_compact(S));
+  if (L->arena_used + g.n > L->cap_n) LVTRY(serve_compact(L));
   if (E->cur < 0) {  // first graph: the union lives in the contraction buffers
     E->cur = 0;
     E->n = 0;
@@ -1233,21 +1272,111 @@ lv_status serve_append(lv_server* S, ServeRequest* r) {
     CU(cudaMemcpyAsync(E->c_w[c] + eb, g.w.data(), g.nnz * sizeof(float),
                        cudaMemcpyHostToDevice, st));
   }
-  r->slot = S->free_slots.back();
-  S->free_slots.pop_back();
-  S->by_slot[r->slot] = r;
-  r->a0 = S->arena_used;
+  r->slot = L->free_slots.back();
+  L->free_slots.pop_back();
+  L->by_slot[r->slot] = r;
+  r->a0 = L->arena_used;
   CU(launch_iota_from(E->assignment + r->a0, g.n, vb, st));
   CU(launch_fill_u32(E->graph0 + r->a0, g.n, r->slot, st));
-  S->arena_used += g.n;
-  E->n0 = S->arena_used;
+  L->arena_used += g.n;
+  E->n0 = L->arena_used;
   E->n += g.n;
   E->e += g.nnz;
   E->level_ready = false;
-  S->graphs.push_back(UnionGraph{r->slot, g.n, 0u, 0u, 0.0});
-  S->res_n += g.n;
-  S->res_e += g.nnz;
+  L->graphs.push_back(UnionGraph{r->slot, g.n, 0u, 0u, 0.0});
   return LV_OK;
+}
+
+// One step of a lane: admissions, then one level of its union.
+lv_status lane_step(lv_server* S, ServeLane* L) {
+  lv_engine* E = L->E;
+  cudaSetDevice(E->device);
+  AllocScope alloc_scope(E->st);
+  std::vector<ServeRequest*> adm;
+  {
+    std::lock_guard<std::mutex> lock(S->mu);
+    uint64_t tn = L->res_n, te = L->res_e;
+    size_t slots = L->free_slots.size();
+    while (!L->queue.empty()) {
+      ServeRequest* r = L->queue.front();
+      if (!slots || tn + r->n > L->cap_n || te + r->nnz > L->cap_e) break;
+      adm.push_back(r);
+      L->queue.pop_front();
+      tn += r->n;
+      te += r->nnz;
+      slots--;
+    }
+    L->res_n = tn;  // reserved now, released when the graph leaves
+    L->res_e = te;
+    L->n_res += (uint32_t)adm.size();
+  }
+  g_trace.reset();
+  for (ServeRequest* r : adm) {
+    LVTRY(serve_append(L, r));
+    r->t_admit = ms_since(S->t0);
+    L->admitted++;
+  }
+  g_trace.mark("serve: admit + append", (uint32_t)adm.size(), E->n);
+  if (L->graphs.empty()) return LV_OK;
+  std::vector<UnionGraph> done;
+  LVTRY(union_level(E, L->graphs, S->cfg.min_gain, L->out, done, nullptr));
+  E->levels.clear();
+  L->steps++;
+  for (const UnionGraph& u : done) {
+    ServeRequest* r = L->by_slot[u.slot];
+    r->assignment.resize(r->n);
+    CU(cudaMemcpyAsync(r->assignment.data(), L->out + r->a0, (size_t)r->n * sizeof(uint32_t),
+                       cudaMemcpyDeviceToHost, E->st));
+    r->q = u.q;
+    r->levels = u.levels;
+    r->n_comm = u.nv;
+  }
+  CU(cudaStreamSynchronize(E->st));
+  const double now = ms_since(S->t0);
+  {
+    std::lock_guard<std::mutex> lock(S->mu);
+    for (const UnionGraph& u : done) {
+      ServeRequest* r = L->by_slot[u.slot];
+      r->t_done = now;
+      L->by_slot[u.slot] = nullptr;
+      L->free_slots.push_back(u.slot);
+      L->res_n -= r->n;
+      L->res_e -= r->nnz;
+      L->n_res--;
+      L->completed++;
+      S->finished.push_back(r);
+    }
+  }
+  if (!done.empty()) S->cv_done.notify_all();
+  if (L->graphs.empty()) {  // every arena range is free
+    L->arena_used = 0;
+    E->n0 = 0;
+  }
+  return LV_OK;
+}
+
+// Background mode: a lane steps while it has queued or resident graphs.
+void lane_worker(lv_server* S, ServeLane* L) {
+  for (;;) {
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      S->cv_work.wait(lk, [&] { return S->stop || !L->queue.empty() || !L->graphs.empty(); });
+      if (S->stop) return;
+      S->busy++;
+    }
+    const lv_status st = lane_step(S, L);
+    std::lock_guard<std::mutex> lock(S->mu);
+    S->busy--;
+    if (st != LV_OK) {
+      if (S->bg_status == LV_OK) {
+        S->bg_status = st;
+        S->bg_error = lv_last_error();
+      }
+      S->cv_done.notify_all();
+      return;  // the lane stops; the server reports the error from now on
+    }
+    S->cv_done.notify_all();
+  }
 }
 
 }  // namespace
@@ -1313,6 +1442,14 @@ lv_status lv_engine_create(const lv_config* cfg, lv_engine** out) {
     delete E;
     return cuda_fail(ce, "configure_kernels");
   }
+  {  // keep freed stream-ordered blocks in the pool for the next growth
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, E->device) == cudaSuccess) {
+      uint64_t keep = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+  }
   if (E->cfg.stream) {
     E->st = (cudaStream_t)E->cfg.stream;
   } else {
@@ -1338,6 +1475,7 @@ lv_status lv_engine_create(const lv_config* cfg, lv_engine** out) {
 
 void lv_engine_destroy(lv_engine* E) {
   if (!E) return;
+  AllocScope alloc_scope(E->st);
   cudaSetDevice(E->device);
   if (E->st) cudaStreamSynchronize(E->st);
   drop_pass_graph(E);
@@ -1366,6 +1504,7 @@ void lv_engine_destroy(lv_engine* E) {
 }
 
 lv_status lv_engine_load(lv_engine* E, const lv_graph* g) {
+  AllocScope alloc_scope(E ? E->st : nullptr);
   if (!E || !g) return fail(LV_ERR_ARG, "NULL engine or graph");
   LVTRY(validate_sizes(g->n, g->nnz));
   cudaSetDevice(E->device);
@@ -1387,6 +1526,7 @@ lv_status lv_engine_load(lv_engine* E, const lv_graph* g) {
 lv_status lv_engine_load_device(lv_engine* E, uint32_t n, uint64_t nnz,
                                 const uint64_t* d_off, const uint32_t* d_col,
                                 const float* d_w) {
+  AllocScope alloc_scope(E ? E->st : nullptr);
   if (!E || !d_off || (nnz && (!d_col || !d_w)))
     return fail(LV_ERR_ARG, "NULL engine or device buffer");
   LVTRY(validate_sizes(n, nnz));
@@ -1399,6 +1539,7 @@ lv_status lv_engine_load_device(lv_engine* E, uint32_t n, uint64_t nnz,
 }
 
 lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
+  AllocScope alloc_scope(E ? E->st : nullptr);
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   if (E->finished) return fail(LV_ERR_STATE, "the run has ended; load a graph again");
@@ -1468,6 +1609,7 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
 }
 
 lv_status lv_phase_aggregate(lv_engine* E) {
+  AllocScope alloc_scope(E ? E->st : nullptr);
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   if (!E->loaded || !E->level_ready) return fail(LV_ERR_STATE, "no move phase to aggregate");
   cudaSetDevice(E->device);
@@ -1489,7 +1631,8 @@ lv_status lv_phase_aggregate(lv_engine* E) {
   E->accepted = false;
   CU(cudaEventRecord(E->ev1, E->st));
   CU(cudaEventSynchronize(E->ev1));
-  CU(cudaMemcpy(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost));
+  CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost, E->st));
+  CU(cudaStreamSynchronize(E->st));
   LVTRY(check_device_error(E));
   prof_collect(E);
   float ms = 0.0f;
@@ -1555,6 +1698,7 @@ static lv_status run_loaded(lv_engine* E, float min_gain, lv_result* res) {
 }
 
 lv_status lv_run(lv_engine* E, const lv_graph* g, float min_gain, lv_result* res) {
+  AllocScope alloc_scope(E ? E->st : nullptr);
   if (!E || !g) return fail(LV_ERR_ARG, "NULL engine or graph");
   cudaSetDevice(E->device);
   cudaEvent_t c0, c1;
@@ -1581,6 +1725,7 @@ lv_status lv_run(lv_engine* E, const lv_graph* g, float min_gain, lv_result* res
 lv_status lv_run_device(lv_engine* E, uint32_t n, uint64_t nnz, const uint64_t* d_off,
                         const uint32_t* d_col, const float* d_w, float min_gain,
                         uint32_t* d_assignment, lv_result* res) {
+  AllocScope alloc_scope(E ? E->st : nullptr);
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   LVTRY(lv_engine_load_device(E, n, nnz, d_off, d_col, d_w));
   LVTRY(run_loaded(E, min_gain, res));
@@ -1598,6 +1743,7 @@ lv_status lv_run_device(lv_engine* E, uint32_t n, uint64_t nnz, const uint64_t* 
 }
 
 lv_status lv_get_assignment(lv_engine* E, uint32_t* out, size_t n) {
+  AllocScope alloc_scope(E ? E->st : nullptr);
   if (!E || (!out && n)) return fail(LV_ERR_ARG, "NULL argument");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   if (n != E->n0) return fail(LV_ERR_ARG, "buffer length must equal the input vertex count");
@@ -1632,6 +1778,7 @@ lv_status lv_get_level_size(lv_engine* E, uint32_t* n, uint64_t* e) {
 
 lv_status lv_get_level_state(lv_engine* E, uint32_t* comm, uint32_t* comm_size,
                              float* weighted_degree) {
+  AllocScope alloc_scope(E ? E->st : nullptr);
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   cudaSetDevice(E->device);
@@ -1650,6 +1797,7 @@ lv_status lv_get_level_state(lv_engine* E, uint32_t* comm, uint32_t* comm_size,
 
 lv_status lv_get_level_csr(lv_engine* E, uint64_t* offsets, uint32_t* cols,
                            float* weights) {
+  AllocScope alloc_scope(E ? E->st : nullptr);
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   cudaSetDevice(E->device);
@@ -1666,6 +1814,7 @@ lv_status lv_get_level_csr(lv_engine* E, uint64_t* offsets, uint32_t* cols,
 }
 
 lv_status lv_set_level_comm(lv_engine* E, const uint32_t* comm) {
+  AllocScope alloc_scope(E ? E->st : nullptr);
   if (!E || !comm) return fail(LV_ERR_ARG, "NULL argument");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   cudaSetDevice(E->device);
@@ -1684,6 +1833,7 @@ lv_status lv_set_level_comm(lv_engine* E, const uint32_t* comm) {
 }
 
 lv_status lv_modularity_fp64(lv_engine* E, const uint32_t* partition, double* q) {
+  AllocScope alloc_scope(E ? E->st : nullptr);
   if (!E || !partition || !q) return fail(LV_ERR_ARG, "NULL argument");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   cudaSetDevice(E->device);
@@ -1729,6 +1879,7 @@ lv_status lv_batch_run_device(lv_engine* E, uint32_t n_graphs, const uint64_t* g
                               const uint32_t* d_cols, const float* d_weights, float min_gain,
                               uint32_t* d_assignment, double* modularity, uint32_t* levels,
                               lv_result* res) {
+  AllocScope alloc_scope(E ? E->st : nullptr);
   if (!E || !graph_offsets || !d_assignment || (n_graphs && !modularity))
     return fail(LV_ERR_ARG, "NULL argument");
   if (n_graphs == 0) return fail(LV_ERR_ARG, "no graphs");
@@ -1744,6 +1895,7 @@ lv_status lv_batch_run_device(lv_engine* E, uint32_t n_graphs, const uint64_t* g
 lv_status lv_batch_run(lv_engine* E, uint32_t n_graphs, const lv_graph* const* graphs,
                        float min_gain, uint32_t* assignment, double* modularity,
                        uint32_t* levels, lv_result* res) {
+  AllocScope alloc_scope(E ? E->st : nullptr);
   if (!E || !graphs || !assignment || !modularity) return fail(LV_ERR_ARG, "NULL argument");
   if (n_graphs == 0) return fail(LV_ERR_ARG, "no graphs");
   // pack the graphs into one block-diagonal CSR (vertex ids offset per graph)
@@ -1795,143 +1947,195 @@ lv_status lv_batch_run(lv_engine* E, uint32_t n_graphs, const lv_graph* const* g
 }
 
 // ---- served form ----------------------------------------------------------
-lv_status lv_serve_create(const lv_config* cfg, float min_gain, uint64_t budget_bytes,
-                          uint32_t max_graphs, lv_server** out) {
-  if (!out) return fail(LV_ERR_ARG, "out is NULL");
+void lv_serve_config_default(lv_serve_config* c) {
+  if (!c) return;
+  memset(c, 0, sizeof(*c));
+  c->min_gain = 1e-6f;
+  c->budget_bytes = 8ull << 30;
+  c->max_graphs = 0;
+  c->n_lanes = 3;
+  c->lane_max_entries[0] = 1ull << 18;
+  c->lane_max_entries[1] = 1ull << 23;
+  c->lane_max_entries[2] = ~0ull;
+  c->lane_max_entries[3] = ~0ull;
+  c->lane_share[0] = 0.15f;
+  c->lane_share[1] = 0.35f;
+  c->lane_share[2] = 0.50f;
+  c->lane_share[3] = 0.0f;
+  c->background = 1;
+}
+
+lv_status lv_serve_create(const lv_config* cfg, const lv_serve_config* scfg, lv_server** out) {
+  if (!out || !scfg) return fail(LV_ERR_ARG, "NULL argument");
   *out = nullptr;
+  if (scfg->n_lanes < 1 || scfg->n_lanes > 4) return fail(LV_ERR_ARG, "n_lanes must be 1..4");
+  double share_sum = 0.0;
+  for (uint32_t i = 0; i < scfg->n_lanes; i++) {
+    if (!(scfg->lane_share[i] > 0.0f)) return fail(LV_ERR_ARG, "every lane needs a budget share");
+    if (i && scfg->lane_max_entries[i] < scfg->lane_max_entries[i - 1])
+      return fail(LV_ERR_ARG, "lane_max_entries must ascend");
+    share_sum += scfg->lane_share[i];
+  }
   const uint64_t per_v = kServeBytesPerVertex, per_e = kServeBytesPerEntry;
-  if (budget_bytes < 64 * (per_v + per_e)) return fail(LV_ERR_ARG, "budget too small");
   lv_server* S = new (std::nothrow) lv_server();
   if (!S) return fail(LV_ERR_NOMEM, "server allocation failed");
-  lv_status st = lv_engine_create(cfg, &S->E);
-  if (st != LV_OK) {
-    delete S;
-    return st;
+  S->cfg = *scfg;
+  S->cfg.lane_max_entries[scfg->n_lanes - 1] = ~0ull;  // the last lane takes the rest
+  for (uint32_t i = 0; i < scfg->n_lanes; i++) {
+    const uint64_t budget = (uint64_t)((double)scfg->budget_bytes * scfg->lane_share[i] / share_sum);
+    if (budget < 64 * (per_v + per_e)) {
+      lv_serve_destroy(S);
+      return fail(LV_ERR_ARG, "budget too small");
+    }
+    ServeLane* L = new (std::nothrow) ServeLane();
+    if (!L) {
+      lv_serve_destroy(S);
+      return fail(LV_ERR_NOMEM, "lane allocation failed");
+    }
+    S->lanes.push_back(L);
+    L->max_entries = S->cfg.lane_max_entries[i];
+    // lanes of smaller graphs get higher stream priority, so their short
+    // kernels are scheduled ahead of a large lane's blocks as SMs free up
+    lv_config lc;
+    if (cfg) lc = *cfg; else lv_config_default(&lc);
+    if (!lc.stream) {
+      int least = 0, greatest = 0;
+      cudaSetDevice(lc.device);
+      cudaDeviceGetStreamPriorityRange(&least, &greatest);
+      const int span = least - greatest;  // greatest is the numerically lower
+      const int prio = scfg->n_lanes > 1
+                           ? greatest + (int)((int64_t)span * i / (scfg->n_lanes - 1))
+                           : least;
+      cudaError_t ce = cudaStreamCreateWithPriority(&L->stream, cudaStreamNonBlocking, prio);
+      if (ce != cudaSuccess) {
+        lv_serve_destroy(S);
+        return cuda_fail(ce, "cudaStreamCreateWithPriority");
+      }
+      lc.stream = L->stream;
+    }
+    lv_status st = lv_engine_create(&lc, &L->E);
+    if (st != LV_OK) {
+      lv_serve_destroy(S);
+      return st;
+    }
+    lv_engine* E = L->E;
+    // a fifth of the lane's budget for per-vertex state, the rest for adjacency
+    uint64_t cap_n = std::min<uint64_t>(budget / 5 / per_v, 0xFFFFFFF0ull);
+    L->cap_n = (uint32_t)cap_n;
+    L->cap_e = (budget - cap_n * per_v) / per_e;
+    L->slot_cap = scfg->max_graphs ? scfg->max_graphs : 4096;
+    auto setup = [&]() -> lv_status {
+      AllocScope alloc_scope(E->st);
+      LVTRY(ensure_capacity(E, L->cap_n, L->cap_e, false));
+      LVTRY(batch_alloc(E, L->slot_cap));
+      CU(dalloc(&E->act_order, L->cap_n));
+      E->act_order_cap = L->cap_n;
+      CU(dalloc(&L->out, L->cap_n));
+      // every id a stale arena entry can hold stays a valid index: compose
+      // (cnew[assignment]) runs over the whole arena, holes included
+      CU(cudaMemsetAsync(E->cb.cnew, 0, (size_t)L->cap_n * sizeof(uint32_t), E->st));
+      CU(cudaMemsetAsync(E->sc, 0, sizeof(LevelScalars), E->st));
+      CU(cudaStreamSynchronize(E->st));
+      return LV_OK;
+    };
+    st = setup();
+    if (st != LV_OK) {
+      lv_serve_destroy(S);
+      return st;
+    }
+    E->loaded = true;
+    E->batch = true;
+    E->cur = -1;
+    E->n = 0;
+    E->e = 0;
+    E->n0 = 0;
+    L->by_slot.assign(L->slot_cap, nullptr);
+    for (uint32_t k = L->slot_cap; k > 0; k--) L->free_slots.push_back(k - 1);
   }
-  lv_engine* E = S->E;
-  // a fifth of the budget for per-vertex state, the rest for adjacency
-  uint64_t cap_n = budget_bytes / 5 / per_v;
-  cap_n = std::min<uint64_t>(cap_n, 0xFFFFFFF0ull);
-  S->cap_n = (uint32_t)cap_n;
-  S->cap_e = (budget_bytes - cap_n * per_v) / per_e;
-  S->slot_cap = max_graphs ? max_graphs : 4096;
-  S->budget = budget_bytes;
-  S->min_gain = min_gain;
-  auto setup = [&]() -> lv_status {
-    LVTRY(ensure_capacity(E, S->cap_n, S->cap_e, false));
-    LVTRY(batch_alloc(E, S->slot_cap));
-    CU(dalloc(&E->act_order, S->cap_n));
-    E->act_order_cap = S->cap_n;
-    CU(dalloc(&S->out, S->cap_n));
-    // every id a stale arena entry can hold stays a valid index: compose
-    // (cnew[assignment]) runs over the whole arena, holes included
-    CU(cudaMemsetAsync(E->cb.cnew, 0, (size_t)S->cap_n * sizeof(uint32_t), E->st));
-    CU(cudaMemsetAsync(E->sc, 0, sizeof(LevelScalars), E->st));
-    CU(cudaStreamSynchronize(E->st));
-    return LV_OK;
-  };
-  st = setup();
-  if (st != LV_OK) {
-    lv_serve_destroy(S);
-    return st;
-  }
-  E->loaded = true;
-  E->batch = true;
-  E->cur = -1;
-  E->n = 0;
-  E->e = 0;
-  E->n0 = 0;
-  S->by_slot.assign(S->slot_cap, nullptr);
-  for (uint32_t i = S->slot_cap; i > 0; i--) S->free_slots.push_back(i - 1);
   S->t0 = std::chrono::steady_clock::now();
+  if (scfg->background) {
+    try {
+      for (ServeLane* L : S->lanes) L->worker = std::thread(lane_worker, S, L);
+    } catch (const std::system_error&) {
+      lv_serve_destroy(S);
+      return fail(LV_ERR_NOMEM, "worker thread start failed");
+    }
+  }
   *out = S;
   return LV_OK;
 }
 
 lv_status lv_serve_submit(lv_server* S, const lv_graph* g, uint64_t* ticket) {
   if (!S || !g) return fail(LV_ERR_ARG, "NULL server or graph");
-  if (g->n > S->cap_n || g->nnz > S->cap_e)
-    return fail(LV_ERR_LIMIT, "graph exceeds the server's device budget");
+  uint32_t lane = ~0u;  // the first lane for the graph's size that can hold it
+  for (uint32_t i = 0; i < S->lanes.size(); i++) {
+    const ServeLane* L = S->lanes[i];
+    if (g->nnz <= L->max_entries && g->n <= L->cap_n && g->nnz <= L->cap_e) {
+      lane = i;
+      break;
+    }
+  }
+  if (lane == ~0u) return fail(LV_ERR_LIMIT, "graph exceeds the server's device budget");
   ServeRequest* r = new (std::nothrow) ServeRequest();
   if (!r) return fail(LV_ERR_NOMEM, "request allocation failed");
   r->g = g;  // not copied: the caller keeps it alive until the result is polled
   r->n = g->n;
   r->nnz = g->nnz;
-  std::lock_guard<std::mutex> lock(S->mu);
-  r->ticket = S->next_ticket++;
-  r->t_submit = ms_since(S->t0);
-  if (g->n == 0) {  // nothing to run
-    r->t_admit = r->t_done = r->t_submit;
-    S->finished.push_back(r);
-  } else {
-    S->queue.push_back(r);
+  r->lane = lane;
+  {
+    std::lock_guard<std::mutex> lock(S->mu);
+    r->ticket = S->next_ticket++;
+    r->t_submit = ms_since(S->t0);
+    if (g->n == 0) {  // nothing to run
+      r->t_admit = r->t_done = r->t_submit;
+      S->finished.push_back(r);
+    } else {
+      S->lanes[lane]->queue.push_back(r);
+    }
+    if (ticket) *ticket = r->ticket;
   }
-  if (ticket) *ticket = r->ticket;
+  S->cv_work.notify_all();
+  S->cv_done.notify_all();
   return LV_OK;
 }
 
+namespace {
+void serve_counts(lv_server* S, uint32_t* resident, uint32_t* queued) {
+  uint32_t r = 0, q = 0;
+  for (const ServeLane* L : S->lanes) {
+    r += L->n_res;
+    q += (uint32_t)L->queue.size();
+  }
+  if (resident) *resident = r;
+  if (queued) *queued = q;
+}
+}  // namespace
+
 lv_status lv_serve_step(lv_server* S, uint32_t* resident, uint32_t* queued) {
   if (!S) return fail(LV_ERR_ARG, "NULL server");
-  lv_engine* E = S->E;
-  cudaSetDevice(E->device);
-  // admissions, first come first served, while slots and budget last
-  std::vector<ServeRequest*> adm;
-  {
-    std::lock_guard<std::mutex> lock(S->mu);
-    uint64_t tn = S->res_n, te = S->res_e;
-    size_t slots = S->free_slots.size();
-    while (!S->queue.empty()) {
-      ServeRequest* r = S->queue.front();
-      if (!slots || tn + r->n > S->cap_n || te + r->nnz > S->cap_e) break;
-      adm.push_back(r);
-      S->queue.pop_front();
-      tn += r->n;
-      te += r->nnz;
-      slots--;
-    }
-  }
-  g_trace.reset();
-  for (ServeRequest* r : adm) {
-    LVTRY(serve_append(S, r));
-    r->t_admit = ms_since(S->t0);
-    S->admitted++;
-  }
-  g_trace.mark("serve: admit + append", (uint32_t)adm.size(), E->n);
-  if (!S->graphs.empty()) {
-    std::vector<UnionGraph> done;
-    LVTRY(union_level(E, S->graphs, S->min_gain, S->out, done, nullptr));
-    E->levels.clear();
-    S->steps++;
-    for (const UnionGraph& u : done) {
-      ServeRequest* r = S->by_slot[u.slot];
-      r->assignment.resize(r->n);
-      CU(cudaMemcpyAsync(r->assignment.data(), S->out + r->a0, (size_t)r->n * sizeof(uint32_t),
-                         cudaMemcpyDeviceToHost, E->st));
-      r->q = u.q;
-      r->levels = u.levels;
-      r->n_comm = u.nv;
-    }
-    CU(cudaStreamSynchronize(E->st));
-    const double now = ms_since(S->t0);
-    for (const UnionGraph& u : done) {
-      ServeRequest* r = S->by_slot[u.slot];
-      r->t_done = now;
-      S->by_slot[u.slot] = nullptr;
-      S->free_slots.push_back(u.slot);
-      S->res_n -= r->n;
-      S->res_e -= r->nnz;
-      S->completed++;
-      std::lock_guard<std::mutex> lock(S->mu);
-      S->finished.push_back(r);
-    }
-    if (S->graphs.empty()) {  // every arena range is free
-      S->arena_used = 0;
-      E->n0 = 0;
-    }
+  if (!S->cfg.background) {
+    for (ServeLane* L : S->lanes) LVTRY(lane_step(S, L));
   }
   std::lock_guard<std::mutex> lock(S->mu);
-  if (resident) *resident = (uint32_t)S->graphs.size();
-  if (queued) *queued = (uint32_t)S->queue.size();
+  if (S->bg_status != LV_OK) return fail(S->bg_status, S->bg_error);
+  serve_counts(S, resident, queued);
+  return LV_OK;
+}
+
+lv_status lv_serve_wait(lv_server* S, uint32_t timeout_ms, int* idle) {
+  if (!S) return fail(LV_ERR_ARG, "NULL server");
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto quiet = [&] {
+    uint32_t r = 0, q = 0;
+    serve_counts(S, &r, &q);
+    return r == 0 && q == 0 && S->busy == 0;
+  };
+  if (S->cfg.background)
+    S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] {
+      return !S->finished.empty() || quiet() || S->bg_status != LV_OK;
+    });
+  if (idle) *idle = quiet() && S->finished.empty() ? 1 : 0;
+  if (S->bg_status != LV_OK) return fail(S->bg_status, S->bg_error);
   return LV_OK;
 }
 
@@ -1942,7 +2146,10 @@ lv_status lv_serve_poll(lv_server* S, lv_serve_result* res, uint32_t* assignment
   ServeRequest* r = nullptr;
   {
     std::lock_guard<std::mutex> lock(S->mu);
-    if (S->finished.empty()) return LV_OK;
+    if (S->finished.empty()) {
+      if (S->bg_status != LV_OK) return fail(S->bg_status, S->bg_error);
+      return LV_OK;
+    }
     r = S->finished.front();
     if (assignment && cap < r->n) return fail(LV_ERR_ARG, "assignment buffer too small");
     S->finished.pop_front();
@@ -1954,6 +2161,7 @@ lv_status lv_serve_poll(lv_server* S, lv_serve_result* res, uint32_t* assignment
     res->n_vertices = r->n;
     res->n_communities = r->n_comm;
     res->levels = r->levels;
+    res->lane = r->lane;
     res->submit_ms = r->t_submit;
     res->admit_ms = r->t_admit;
     res->done_ms = r->t_done;
@@ -1968,36 +2176,52 @@ lv_status lv_serve_get_stats(lv_server* S, lv_serve_stats* out) {
   if (!S || !out) return fail(LV_ERR_ARG, "NULL argument");
   std::lock_guard<std::mutex> lock(S->mu);
   memset(out, 0, sizeof(*out));
-  out->queued = (uint32_t)S->queue.size();
-  out->resident = (uint32_t)S->graphs.size();
+  serve_counts(S, &out->resident, &out->queued);
   out->finished = (uint32_t)S->finished.size();
-  out->slot_cap = S->slot_cap;
-  out->resident_vertices = S->res_n;
-  out->resident_entries = S->res_e;
-  out->cap_vertices = S->cap_n;
-  out->cap_entries = S->cap_e;
-  out->budget_bytes = S->budget;
-  out->steps = S->steps;
-  out->admitted = S->admitted;
-  out->completed = S->completed;
+  out->n_lanes = (uint32_t)S->lanes.size();
+  for (const ServeLane* L : S->lanes) {
+    out->slot_cap += L->slot_cap;
+    out->resident_vertices += L->res_n;
+    out->resident_entries += L->res_e;
+    out->cap_vertices += L->cap_n;
+    out->cap_entries += L->cap_e;
+    out->steps += L->steps;
+    out->admitted += L->admitted;
+    out->completed += L->completed;
+  }
+  out->budget_bytes = S->cfg.budget_bytes;
   return LV_OK;
 }
 
-lv_status lv_serve_engine(lv_server* S, lv_engine** out) {
-  if (!S || !out) return fail(LV_ERR_ARG, "NULL argument");
-  *out = S->E;
+lv_status lv_serve_engine(lv_server* S, uint32_t lane, lv_engine** out) {
+  if (!S || !out || lane >= S->lanes.size()) return fail(LV_ERR_ARG, "bad server, lane or out");
+  *out = S->lanes[lane]->E;
   return LV_OK;
 }
 
 void lv_serve_destroy(lv_server* S) {
   if (!S) return;
-  for (ServeRequest* r : S->queue) delete r;
+  {
+    std::lock_guard<std::mutex> lock(S->mu);
+    S->stop = true;
+  }
+  S->cv_work.notify_all();
+  for (ServeLane* L : S->lanes)
+    if (L->worker.joinable()) L->worker.join();
   for (ServeRequest* r : S->finished) delete r;
-  for (ServeRequest* r : S->by_slot) delete r;
-  if (S->E) {
-    cudaSetDevice(S->E->device);
-    dfree(S->out);
-    lv_engine_destroy(S->E);
+  for (ServeLane* L : S->lanes) {
+    for (ServeRequest* r : L->queue) delete r;
+    for (ServeRequest* r : L->by_slot) delete r;
+    if (L->E) {
+      cudaSetDevice(L->E->device);
+      {
+        AllocScope alloc_scope(L->E->st);
+        dfree(L->out);
+      }
+      lv_engine_destroy(L->E);
+    }
+    if (L->stream) cudaStreamDestroy(L->stream);
+    delete L;
   }
   delete S;
 }
@@ -2015,6 +2239,7 @@ lv_status lv_reset_kernel_stats(lv_engine* E) {
 }
 
 lv_status lv_get_buckets(lv_engine* E, uint8_t* bucket_of, size_t n) {
+  AllocScope alloc_scope(E ? E->st : nullptr);
   if (!E || (!bucket_of && n)) return fail(LV_ERR_ARG, "NULL argument");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   if (n != E->n) return fail(LV_ERR_ARG, "buffer length must equal the level's vertex count");

@@ -79,10 +79,17 @@ class KernelStat(ctypes.Structure):
     ]
 
 
+class ServeConfig(ctypes.Structure):
+    _fields_ = [("min_gain", ctypes.c_float), ("budget_bytes", ctypes.c_uint64),
+                ("max_graphs", ctypes.c_uint32), ("n_lanes", ctypes.c_uint32),
+                ("lane_max_entries", ctypes.c_uint64 * 4), ("lane_share", ctypes.c_float * 4),
+                ("background", ctypes.c_int)]
+
+
 class ServeResult(ctypes.Structure):
     _fields_ = [("ticket", ctypes.c_uint64), ("modularity", ctypes.c_double),
                 ("n_vertices", ctypes.c_uint32), ("n_communities", ctypes.c_uint32),
-                ("levels", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("levels", ctypes.c_uint32), ("lane", ctypes.c_uint32),
                 ("submit_ms", ctypes.c_double), ("admit_ms", ctypes.c_double),
                 ("done_ms", ctypes.c_double)]
 
@@ -90,6 +97,7 @@ class ServeResult(ctypes.Structure):
 class ServeStats(ctypes.Structure):
     _fields_ = [("queued", ctypes.c_uint32), ("resident", ctypes.c_uint32),
                 ("finished", ctypes.c_uint32), ("slot_cap", ctypes.c_uint32),
+                ("n_lanes", ctypes.c_uint32),
                 ("resident_vertices", ctypes.c_uint64), ("resident_entries", ctypes.c_uint64),
                 ("cap_vertices", ctypes.c_uint64), ("cap_entries", ctypes.c_uint64),
                 ("budget_bytes", ctypes.c_uint64), ("steps", ctypes.c_uint64),
@@ -143,15 +151,17 @@ _SIGS = {
                                            ctypes.POINTER(Result)]),
     "lv_batch_run": (ctypes.c_int, [_VP, _U32, _VP, ctypes.c_float, _VP, _VP, _VP,
                                     ctypes.POINTER(Result)]),
-    "lv_serve_create": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.c_float, _U64, _U32,
+    "lv_serve_config_default": (None, [ctypes.POINTER(ServeConfig)]),
+    "lv_serve_create": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(ServeConfig),
                                        ctypes.POINTER(_VP)]),
+    "lv_serve_wait": (ctypes.c_int, [_VP, _U32, ctypes.POINTER(ctypes.c_int)]),
     "lv_serve_submit": (ctypes.c_int, [_VP, _VP, ctypes.POINTER(_U64)]),
     "lv_serve_step": (ctypes.c_int, [_VP, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
     "lv_serve_poll": (ctypes.c_int, [_VP, ctypes.POINTER(ServeResult), _VP, ctypes.c_size_t,
                                      ctypes.POINTER(ctypes.c_int)]),
     "lv_serve_get_stats": (ctypes.c_int, [_VP, ctypes.POINTER(ServeStats)]),
     "lv_serve_destroy": (None, [_VP]),
-    "lv_serve_engine": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
+    "lv_serve_engine": (ctypes.c_int, [_VP, _U32, ctypes.POINTER(_VP)]),
 }
 
 NOALLOC_MAX_VERTICES = 1 << 20
@@ -494,6 +504,7 @@ class ServedGraph:
     assignment: np.ndarray
     n_communities: int
     levels: int
+    lane: int
     submit_ms: float
     admit_ms: float
     done_ms: float
@@ -501,12 +512,16 @@ class ServedGraph:
 
 class Server:
     """Continuous-batching server (lv_serve_*).  submit() queues a graph;
-    step() admits what fits and runs one level for every resident graph;
-    poll() returns finished requests."""
+    without background workers step() admits what fits and runs one level
+    of every lane; poll() returns finished requests; drain() runs until
+    everything submitted is finished.  lanes > 1 routes requests by entry
+    count (lane_max_entries) to separate unions with their own budget share;
+    background=True steps every lane on its own worker thread."""
 
     def __init__(self, min_gain: float, budget_bytes: int, max_graphs: int = 0,
-                 device: int = 0, rule: str = "py", max_passes: int = 0,
-                 max_levels: int = 0, use_graphs: bool = True, stream: int = 0):
+                 lanes: int = 1, background: bool = False, lane_max_entries=None,
+                 lane_share=None, device: int = 0, rule: str = "py", max_passes: int = 0,
+                 max_levels: int = 0, use_graphs: bool = True):
         cfg = Config()
         lib().lv_config_default(ctypes.byref(cfg))
         cfg.device = device
@@ -514,11 +529,26 @@ class Server:
         cfg.max_passes = max_passes
         cfg.max_levels = max_levels
         cfg.use_graphs = int(use_graphs)
-        cfg.stream = stream or None
+        sc = ServeConfig()
+        lib().lv_serve_config_default(ctypes.byref(sc))
+        sc.min_gain = min_gain
+        sc.budget_bytes = budget_bytes
+        sc.max_graphs = max_graphs
+        sc.n_lanes = lanes
+        sc.background = int(background)
+        if lanes == 1:
+            sc.lane_share[0] = 1.0
+        if lane_max_entries is not None:
+            for i, x in enumerate(lane_max_entries):
+                sc.lane_max_entries[i] = x
+        if lane_share is not None:
+            for i, x in enumerate(lane_share):
+                sc.lane_share[i] = x
         h = ctypes.c_void_p()
-        _check(lib().lv_serve_create(ctypes.byref(cfg), min_gain, budget_bytes, max_graphs,
-                                     ctypes.byref(h)))
+        _check(lib().lv_serve_create(ctypes.byref(cfg), ctypes.byref(sc), ctypes.byref(h)))
         self._h = h
+        self.background = background
+        self.lanes = lanes
         self._sizes = {}
         self._graphs = {}
 
@@ -549,10 +579,18 @@ class Server:
         return t.value
 
     def step(self):
-        """One scheduling step; returns (resident, queued) graph counts."""
+        """One scheduling step of every lane (nothing with background
+        workers); returns (resident, queued) graph counts."""
         r, q = _U32(), _U32()
         _check(lib().lv_serve_step(self._h, ctypes.byref(r), ctypes.byref(q)))
         return r.value, q.value
+
+    def wait(self, timeout_ms: int = 50) -> bool:
+        """Background mode: blocks until a result is ready, the server is
+        idle or the timeout passes; returns True when idle."""
+        idle = ctypes.c_int()
+        _check(lib().lv_serve_wait(self._h, timeout_ms, ctypes.byref(idle)))
+        return bool(idle.value)
 
     def poll(self):
         """The oldest finished request as a ServedGraph, or None."""
@@ -567,15 +605,19 @@ class Server:
         self._sizes.pop(res.ticket, None)
         self._graphs.pop(res.ticket, None)
         return ServedGraph(res.ticket, res.modularity, buf[: res.n_vertices].copy(),
-                           res.n_communities, res.levels, res.submit_ms, res.admit_ms,
-                           res.done_ms)
+                           res.n_communities, res.levels, res.lane, res.submit_ms,
+                           res.admit_ms, res.done_ms)
 
     def drain(self):
-        """Steps until nothing is queued or resident; returns the finished
+        """Runs until nothing is queued or resident; returns the finished
         requests by ticket."""
         out = {}
         while True:
-            r, q = self.step()
+            if self.background:
+                idle = self.wait(50)
+                r = q = 0 if idle else 1
+            else:
+                r, q = self.step()
             while (x := self.poll()) is not None:
                 out[x.ticket] = x
             if r == 0 and q == 0:
@@ -584,19 +626,19 @@ class Server:
             out[x.ticket] = x
         return out
 
-    def set_profiling(self, on: bool = True):
-        _check(lib().lv_set_profiling(self._engine(), int(on)))
+    def set_profiling(self, on: bool = True, lane: int = 0):
+        _check(lib().lv_set_profiling(self._engine(lane), int(on)))
 
-    def kernel_stats(self) -> dict:
+    def kernel_stats(self, lane: int = 0) -> dict:
         arr = (KernelStat * 32)()
         cnt = _U32()
-        _check(lib().lv_get_kernel_stats(self._engine(), arr, 32, ctypes.byref(cnt)))
+        _check(lib().lv_get_kernel_stats(self._engine(lane), arr, 32, ctypes.byref(cnt)))
         return {a.name.decode(): dict(launches=a.launches, total_ms=a.total_ms, bytes=a.bytes)
                 for a in arr[: cnt.value]}
 
-    def _engine(self):
+    def _engine(self, lane: int = 0):
         e = ctypes.c_void_p()
-        _check(lib().lv_serve_engine(self._h, ctypes.byref(e)))
+        _check(lib().lv_serve_engine(self._h, lane, ctypes.byref(e)))
         return e
 
     def stats(self) -> dict:

@@ -135,3 +135,23 @@ def test_serve_slot_limit():
             if r == 0 and q == 0:
                 break
     _check(alone, served, tickets)
+
+
+@pytest.mark.parametrize("background", [False, True])
+def test_serve_lanes(background):
+    """Three lanes routed by entry count (tiny bounds so every lane gets
+    graphs), stepped by the caller or by worker threads: every result still
+    equals the lone run, and the lanes' unions are independent."""
+    graphs = _mix()
+    alone = _alone(graphs, 1e-6)
+    entries = [g.csr()[2].size for g in graphs]
+    with lvb200.Server(1e-6, 512 << 20, lanes=3, background=background,
+                       lane_max_entries=[2_000, 20_000], lane_share=[0.2, 0.3, 0.5]) as s:
+        tickets, served = _staggered(s, graphs)
+        st = s.stats()
+    assert st["n_lanes"] == 3 and st["completed"] == len(graphs)
+    _check(alone, served, tickets)
+    for t, e in zip(tickets, entries):
+        want = 0 if e <= 2_000 else (1 if e <= 20_000 else 2)
+        assert served[t].lane == want
+    assert len({served[t].lane for t in tickets}) == 3
