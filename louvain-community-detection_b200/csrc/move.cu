@@ -219,6 +219,14 @@ __device__ __forceinline__ uint32_t table_insert_fresh(uint32_t* keys, uint32_t 
 // Move kernels
 // ---------------------------------------------------------------------------
 
+// Candidate key from values already loaded (see candidate()).
+__device__ __forceinline__ unsigned long long candidate_loaded(const GainCtx& g,
+                                                               uint32_t c, double ec,
+                                                               uint32_t szc, double ac) {
+  if (g.szv == 1 && szc == 1 && !(c < g.cv)) return 0ull;
+  return pack_best(gain_of((float)ec, (float)ac, g), c);
+}
+
 // deg <= G: G lanes per vertex, one edge per lane.
 template <int G, int RULE>
 __global__ void __launch_bounds__(kThreads)
@@ -245,12 +253,18 @@ __global__ void __launch_bounds__(kThreads)
       act = vertex_active(L, v);
     }
     const bool has = act && gl < (int)d;
-    uint32_t u = 0, cu = 0;
+    // the vertex's own state is read alongside its row (no dependency)
+    GainCtx g;
+    if (vvalid) g = make_ctx(L, v, cv);
+    uint32_t u = 0, cu = 0, szc = 0;
     float wt = 0.0f;
+    double ac = 0.0;
     if (has) {
       u = L.col[s + gl];
       wt = L.w[s + gl];
       cu = L.comm[u];
+      szc = L.comm_sz[cu];  // the candidate's data, read before the grouping
+      ac = L.tot[cu];
     }
     // the own community's entries are summed with shuffles (its lowest
     // lane holds the sum); the others through one shared slot per distinct
@@ -273,23 +287,13 @@ __global__ void __launch_bounds__(kThreads)
     if (RULE == LV_RULE_CUDA_I && is_hot && u != v) own = (double)wt;
     __syncwarp();
     unsigned long long best = 0ull;
-    GainCtx g;
-    if (vvalid) g = make_ctx(L, v, cv);
     if ((ins && leader == lane) || lane == hot_leader)
-      best = candidate(L, g, cu, sums[wib][lane]);
+      best = candidate_loaded(g, cu, sums[wib][lane], szc, ac);
     best = group_max<G>(best);
     if (RULE == LV_RULE_CUDA_I) own = group_sum<G>(own);
     if (vvalid && gl == 0) prop[vidx] = decide<RULE>(best, own, g);
     __syncwarp();
   }
-}
-
-// Candidate key from values already loaded (see candidate()).
-__device__ __forceinline__ unsigned long long candidate_loaded(const GainCtx& g,
-                                                               uint32_t c, double ec,
-                                                               uint32_t szc, double ac) {
-  if (g.szv == 1 && szc == 1 && !(c < g.cv)) return 0ull;
-  return pack_best(gain_of((float)ec, (float)ac, g), c);
 }
 
 // Best candidate among the listed slots (nthr threads from tid, four per
@@ -363,6 +367,7 @@ __global__ void __launch_bounds__(kThreads)
       continue;
     }
     const uint32_t tv = table_size_for(d, T);
+    const GainCtx g = make_ctx(L, v, cv);
     uint32_t cu[MAXW];
     float wt[MAXW];
     unsigned self_mask = 0u;  // waves whose entry is the self-loop
@@ -413,7 +418,6 @@ __global__ void __launch_bounds__(kThreads)
       vals[slot] += hot;
     }
     __syncwarp();
-    const GainCtx g = make_ctx(L, v, cv);
     unsigned long long best =
         scan_fresh_and_clear(L, g, keys, vals, fresh, *n_fresh, lane, 32);
     best = group_max<32>(best);
@@ -540,6 +544,7 @@ __global__ void __launch_bounds__(kThreads)
       continue;
     }
     const uint32_t tv = table_size_for(d, T);
+    const GainCtx g = make_ctx(L, v, cv);
     double own = 0.0;
     double hot = 0.0;
     bool hot_seen = false;
@@ -552,7 +557,6 @@ __global__ void __launch_bounds__(kThreads)
       vals[slot] += hot;
     }
     __syncthreads();
-    const GainCtx g = make_ctx(L, v, cv);
     unsigned long long best =
         scan_fresh_and_clear(L, g, keys, vals, fresh, n_fresh, threadIdx.x, kThreads);
     best = block_max(best, red_best);
