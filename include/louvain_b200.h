@@ -312,6 +312,35 @@ lv_status lv_serve_get_stats(lv_server *s, lv_serve_stats *out);
 lv_status lv_serve_engine(lv_server *s, uint32_t lane, lv_engine **out);
 void lv_serve_destroy(lv_server *s);
 
+/* ---- autotuning (no counterpart in the reference) -----------------------
+ * Every degree bucket (1..7) can run on any move kernel variant whose
+ * shape holds its degrees; all variants give the same proposals, so the
+ * choice changes speed only.  Variants: G-lane groups with one entry per
+ * lane (LV_KERNEL_LANES4/8/16/32: degree <= G), a warp per vertex with a
+ * 128- or 512-slot shared table (LV_KERNEL_WARP128: <= 84, WARP512: <= 319)
+ * and a block per vertex with a 4096-slot table (LV_KERNEL_BLOCK: <= 2048).
+ * lv_autotune times every fitting variant of every non-empty bucket on the
+ * loaded graph's current level (proposals only; the state is unchanged)
+ * and keeps the fastest; the engine uses its tuning until changed.        */
+enum {
+  LV_KERNEL_LANES4 = 0,
+  LV_KERNEL_LANES8 = 1,
+  LV_KERNEL_LANES16 = 2,
+  LV_KERNEL_LANES32 = 3,
+  LV_KERNEL_WARP128 = 4,
+  LV_KERNEL_WARP512 = 5,
+  LV_KERNEL_BLOCK = 6
+};
+typedef struct lv_tuning {
+  uint8_t bucket_kernel[8]; /* [b] for buckets b = 1..7; [0] unused       */
+  float bucket_ms[8];       /* lv_autotune: time per launch of the choice */
+} lv_tuning;
+
+/* reps: timed launches per variant (0: 5). */
+lv_status lv_autotune(lv_engine *e, uint32_t reps, lv_tuning *out);
+lv_status lv_set_tuning(lv_engine *e, const lv_tuning *t);
+lv_status lv_get_tuning(lv_engine *e, lv_tuning *t);
+
 /* ---- kernel timing (no counterpart in the reference, whose only timers
  * are main.cu:19-56's two regions) --------------------------------------
  * With profiling on, every launch group is bracketed by CUDA events on the

@@ -278,6 +278,10 @@ struct lv_engine {
   unsigned long long pass_launches = 0;      // kernels per replay
   unsigned long long* d_class_deg = nullptr;
   uint64_t class_deg[kClasses] = {};
+  // move kernel variant of every bucket (1..7): defaults or lv_autotune's pick
+  uint8_t tune[8] = {kDefaultVariant[0], kDefaultVariant[1], kDefaultVariant[2],
+                     kDefaultVariant[3], kDefaultVariant[4], kDefaultVariant[5],
+                     kDefaultVariant[6], kDefaultVariant[7]};
 
   const uint64_t* off() const { return cur < 0 ? in_off : c_off[cur]; }
   const uint32_t* col() const { return cur < 0 ? in_col : c_col[cur]; }
@@ -849,7 +853,7 @@ lv_status issue_pass(lv_engine* E, const PassControl* ctl) {
     const double vb = (double)(e - s);
     const double v7 = (double)(E->plan.cls_start[b + 1] - s);
     cudaEvent_t t0 = prof_begin(E);
-    CU(launch_move_bucket(L, b, rule, ord, E->prop, E->plan, H, E->st, ac));
+    CU(launch_move_bucket(L, b, rule, ord, E->prop, E->plan, H, E->st, ac, nullptr, E->tune));
     prof_end(E, t0, K_MOVE1 + b - 1, (double)E->class_deg[b] * 12.0 + v7 * 32.0);
     if (b == 7 && E->plan.hub_count) {
       t0 = prof_begin(E);
@@ -2224,6 +2228,72 @@ void lv_serve_destroy(lv_server* S) {
     delete L;
   }
   delete S;
+}
+
+// ---- autotuning ------------------------------------------------------------
+lv_status lv_autotune(lv_engine* E, uint32_t reps, lv_tuning* out) {
+  if (!E) return fail(LV_ERR_ARG, "NULL engine");
+  if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
+  if (E->batch) return fail(LV_ERR_STATE, "a batched run is in progress");
+  AllocScope alloc_scope(E->st);
+  cudaSetDevice(E->device);
+  if (!reps) reps = 5;
+  if (!E->level_ready) LVTRY(prepare_level(E));
+  drop_pass_graph(E);  // a captured pass would keep the old kernels
+  const LevelView L = E->view();
+  const int rule = (E->cfg.rule == LV_RULE_CUDA) ? LV_RULE_CUDA_I : LV_RULE_PY_I;
+  lv_tuning t{};
+  for (int b = 1; b <= kBuckets; b++) {
+    t.bucket_kernel[b] = E->tune[b];
+    const uint32_t cnt = E->plan.cls_start[b + 1] - E->plan.cls_start[b];
+    if (!cnt) continue;
+    // proposals only (no apply), so every launch sees the same state
+    float best_ms = 1e30f;
+    for (int v = 0; v < KV_COUNT; v++) {
+      if (!variant_fits(v, b)) continue;
+      uint8_t kv[8];
+      memcpy(kv, E->tune, sizeof(kv));
+      kv[b] = (uint8_t)v;
+      CU(launch_move_bucket(L, b, rule, E->order, E->prop, E->plan, E->hub, E->st, nullptr,
+                            nullptr, kv));
+      CU(cudaEventRecord(E->ev0, E->st));
+      for (uint32_t r = 0; r < reps; r++)
+        CU(launch_move_bucket(L, b, rule, E->order, E->prop, E->plan, E->hub, E->st, nullptr,
+                              nullptr, kv));
+      CU(cudaEventRecord(E->ev1, E->st));
+      CU(cudaEventSynchronize(E->ev1));
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, E->ev0, E->ev1);
+      ms /= (float)reps;
+      if (ms < best_ms) {
+        best_ms = ms;
+        t.bucket_kernel[b] = (uint8_t)v;
+      }
+    }
+    t.bucket_ms[b] = best_ms;
+    E->tune[b] = t.bucket_kernel[b];
+  }
+  LVTRY(check_device_error(E));
+  if (out) *out = t;
+  return LV_OK;
+}
+
+lv_status lv_set_tuning(lv_engine* E, const lv_tuning* t) {
+  if (!E || !t) return fail(LV_ERR_ARG, "NULL argument");
+  for (int b = 1; b <= kBuckets; b++)
+    if (!variant_fits(t->bucket_kernel[b], b))
+      return fail(LV_ERR_ARG, "kernel variant cannot hold bucket " + std::to_string(b) +
+                                  "'s degrees");
+  for (int b = 1; b <= kBuckets; b++) E->tune[b] = t->bucket_kernel[b];
+  drop_pass_graph(E);
+  return LV_OK;
+}
+
+lv_status lv_get_tuning(lv_engine* E, lv_tuning* t) {
+  if (!E || !t) return fail(LV_ERR_ARG, "NULL argument");
+  memset(t, 0, sizeof(*t));
+  for (int b = 1; b <= kBuckets; b++) t->bucket_kernel[b] = E->tune[b];
+  return LV_OK;
 }
 
 lv_status lv_get_launch_count(uint64_t* count) {

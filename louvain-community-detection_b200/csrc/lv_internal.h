@@ -250,11 +250,42 @@ constexpr uint32_t kHubMaxParts = 8192;
 // act_cnt: as for launch_modularity (null: whole classes).
 // Bucket 8 (hubs) also needs the hub dispatch map (hub index | chunk of
 // every kHubChunk-entry block, P.hub_blocks of each).
+// variant[b] (b = 1..7; null: the defaults) picks the kernel of bucket b.
 cudaError_t launch_move_bucket(const LevelView& L, int bucket, int rule,
                                const uint32_t* order, uint32_t* proposal,
                                const DispatchPlan& P, const HubArena& H,
                                cudaStream_t st, const uint32_t* act_cnt = nullptr,
-                               const uint32_t* hub_map = nullptr);
+                               const uint32_t* hub_map = nullptr,
+                               const uint8_t* variant = nullptr);
+
+// Move kernel variants a bucket can run on: G-lane groups (one entry per
+// lane, degree <= G), a warp with a 128- or 512-slot shared table, a block
+// with a 4096-slot table.  All give the same proposals; they differ in how
+// the work maps onto the SMs, which the autotuner measures.
+enum MoveVariant : uint8_t {
+  KV_SMALL4 = 0,
+  KV_SMALL8 = 1,
+  KV_SMALL16 = 2,
+  KV_SMALL32 = 3,
+  KV_WARP128 = 4,
+  KV_WARP512 = 5,
+  KV_BLOCK = 6,
+  KV_COUNT = 7
+};
+// Largest degree a variant handles / a bucket holds (bucket 7: its shared
+// table class, degree <= kHubSmemMaxDeg).
+constexpr uint64_t variant_max_degree(int v) {
+  return v == KV_SMALL4 ? 4 : v == KV_SMALL8 ? 8 : v == KV_SMALL16 ? 16 : v == KV_SMALL32 ? 32
+       : v == KV_WARP128 ? 84 : v == KV_WARP512 ? 319 : kHubSmemMaxDeg;
+}
+constexpr uint64_t bucket_max_degree(int b) {
+  return b == 7 ? kHubSmemMaxDeg : kBucketHi[b];
+}
+constexpr bool variant_fits(int v, int b) {
+  return v >= 0 && v < KV_COUNT && b >= 1 && b <= 7 && variant_max_degree(v) >= bucket_max_degree(b);
+}
+constexpr uint8_t kDefaultVariant[8] = {0, KV_SMALL4, KV_SMALL8, KV_SMALL16, KV_SMALL32,
+                                        KV_WARP128, KV_WARP512, KV_BLOCK};
 cudaError_t launch_apply_bucket(const LevelView& L, int bucket,
                                 const uint32_t* order,
                                 const uint32_t* proposal,

@@ -1451,69 +1451,72 @@ cudaError_t launch_pass_control_init(LevelScalars* sc, GraphState* gs,
   return cudaGetLastError();
 }
 
+// One launch of a move kernel variant over `cnt` vertices of a class list.
+template <int RULE>
+static void launch_variant(int kv, const LevelView& L, const uint32_t* verts, uint32_t cnt,
+                           uint32_t* pr, const uint32_t* dc, cudaStream_t st) {
+  const unsigned cap = sm_count() * 8;
+  switch (kv) {
+    case KV_SMALL4:
+      (count_launches(1), move_small_kernel<4, RULE><<<grid_for((cnt + 63) / 64, cap), kThreads, 0, st>>>(L, verts, cnt, pr, dc));
+      break;
+    case KV_SMALL8:
+      (count_launches(1), move_small_kernel<8, RULE><<<grid_for((cnt + 31) / 32, cap), kThreads, 0, st>>>(L, verts, cnt, pr, dc));
+      break;
+    case KV_SMALL16:
+      (count_launches(1), move_small_kernel<16, RULE><<<grid_for((cnt + 15) / 16, cap), kThreads, 0, st>>>(L, verts, cnt, pr, dc));
+      break;
+    case KV_SMALL32:
+      (count_launches(1), move_small_kernel<32, RULE><<<grid_for((cnt + 7) / 8, cap), kThreads, 0, st>>>(L, verts, cnt, pr, dc));
+      break;
+    case KV_WARP128: {
+      constexpr int T = 128;
+      (count_launches(1), move_warp_kernel<T, 3, RULE><<<grid_for((cnt + 7) / 8, cap), kThreads,
+                                  kWarps * T * kSlotBytes, st>>>(L, verts, cnt, pr, dc));
+      break;
+    }
+    case KV_WARP512: {
+      constexpr int T = 512;
+      (count_launches(1), move_warp_kernel<T, 10, RULE><<<grid_for((cnt + 7) / 8, sm_count() * 4), kThreads,
+                                  kWarps * T * kSlotBytes, st>>>(L, verts, cnt, pr, dc));
+      break;
+    }
+    default:  // KV_BLOCK: shared table, one block per vertex
+      (count_launches(1), move_block_kernel<RULE><<<grid_for(cnt, sm_count() * 4), kThreads,
+                                kBlockTabSmem, st>>>(L, verts, cnt, pr, dc));
+      break;
+  }
+}
+
 template <int RULE>
 static cudaError_t move_bucket_impl(const LevelView& L, int bucket,
                                     const uint32_t* order, uint32_t* prop,
                                     const DispatchPlan& P, const HubArena& H,
                                     const uint32_t* act_cnt, const uint32_t* hub_map,
-                                    cudaStream_t st) {
-  const unsigned cap = sm_count() * 8;
+                                    const uint8_t* kv, cudaStream_t st) {
   const uint32_t s = P.cls_start[bucket];
   const uint32_t cnt = P.cls_start[bucket + 1] - s;
-  const uint32_t* verts = order + s;
-  uint32_t* pr = prop + s;
   // grids are sized for the whole class; with act_cnt the kernels read the
   // active count and their grid-stride loops end early
   const uint32_t* dc = (act_cnt && bucket <= 7) ? act_cnt + bucket : nullptr;
-  switch (bucket) {
-    case 1:
-      if (cnt) (count_launches(1), move_small_kernel<4, RULE><<<grid_for((cnt + 63) / 64, cap), kThreads, 0, st>>>(L, verts, cnt, pr, dc));
-      break;
-    case 2:
-      if (cnt) (count_launches(1), move_small_kernel<8, RULE><<<grid_for((cnt + 31) / 32, cap), kThreads, 0, st>>>(L, verts, cnt, pr, dc));
-      break;
-    case 3:
-      if (cnt) (count_launches(1), move_small_kernel<16, RULE><<<grid_for((cnt + 15) / 16, cap), kThreads, 0, st>>>(L, verts, cnt, pr, dc));
-      break;
-    case 4:
-      if (cnt) (count_launches(1), move_small_kernel<32, RULE><<<grid_for((cnt + 7) / 8, cap), kThreads, 0, st>>>(L, verts, cnt, pr, dc));
-      break;
-    case 5:
-      if (cnt) {
-        constexpr int T = 128;
-        (count_launches(1), move_warp_kernel<T, 3, RULE><<<grid_for((cnt + 7) / 8, cap), kThreads,
-                                    kWarps * T * kSlotBytes, st>>>(L, verts, cnt, pr, dc));
-      }
-      break;
-    case 6:
-      if (cnt) {
-        constexpr int T = 512;
-        (count_launches(1), move_warp_kernel<T, 10, RULE><<<grid_for((cnt + 7) / 8, sm_count() * 4), kThreads,
-                                    kWarps * T * kSlotBytes, st>>>(L, verts, cnt, pr, dc));
-      }
-      break;
-    case 7:  // class 7 of bucket 7: shared table, one block per vertex
-      if (cnt) {
-        (count_launches(1), move_block_kernel<RULE><<<grid_for(cnt, sm_count() * 4), kThreads,
-                                  kBlockTabSmem, st>>>(L, verts, cnt, pr, dc));
-      }
-      break;
-    case 8: {  // class 8 of bucket 7: split chunks, merge (hub, partition)
-      const uint32_t hs = P.cls_start[8];
-      const uint32_t hc = P.cls_start[9] - hs;
-      if (hc) {
-        const uint32_t hb = P.hub_blocks;
-        (count_launches(1), hub_split_kernel<RULE><<<grid_for(hb, sm_count() * 6), kThreads, 0, st>>>(
-            L, order + hs, H, hub_map, hub_map + hb, hb));
-        (count_launches(1), hub_merge_kernel<RULE><<<grid_for(H.units, sm_count() * 3), kThreads,
-                                                   kHubPartSmem, st>>>(L, order + hs, H, H.units));
-        (count_launches(1), hub_decide_kernel<RULE><<<(hc + 127) / 128, 128, 0, st>>>(
-            L, order + hs, H, hc, prop + hs));
-      }
-      break;
-    }
-    default:
-      return cudaErrorInvalidValue;
+  if (bucket >= 1 && bucket <= 7) {
+    const int v = kv ? kv[bucket] : kDefaultVariant[bucket];
+    if (!variant_fits(v, bucket)) return cudaErrorInvalidValue;
+    if (cnt) launch_variant<RULE>(v, L, order + s, cnt, prop + s, dc, st);
+    return cudaGetLastError();
+  }
+  if (bucket != 8) return cudaErrorInvalidValue;
+  // class 8 of bucket 7: split chunks, merge (hub, partition)
+  const uint32_t hs = P.cls_start[8];
+  const uint32_t hc = P.cls_start[9] - hs;
+  if (hc) {
+    const uint32_t hb = P.hub_blocks;
+    (count_launches(1), hub_split_kernel<RULE><<<grid_for(hb, sm_count() * 6), kThreads, 0, st>>>(
+        L, order + hs, H, hub_map, hub_map + hb, hb));
+    (count_launches(1), hub_merge_kernel<RULE><<<grid_for(H.units, sm_count() * 3), kThreads,
+                                               kHubPartSmem, st>>>(L, order + hs, H, H.units));
+    (count_launches(1), hub_decide_kernel<RULE><<<(hc + 127) / 128, 128, 0, st>>>(
+        L, order + hs, H, hc, prop + hs));
   }
   return cudaGetLastError();
 }
@@ -1522,12 +1525,13 @@ cudaError_t launch_move_bucket(const LevelView& L, int bucket, int rule,
                                const uint32_t* order, uint32_t* proposal,
                                const DispatchPlan& P, const HubArena& H,
                                cudaStream_t st, const uint32_t* act_cnt,
-                               const uint32_t* hub_map) {
+                               const uint32_t* hub_map, const uint8_t* variant) {
   if (bucket == 8 && !hub_map) return cudaErrorInvalidValue;
   if (rule == LV_RULE_CUDA_I)
     return move_bucket_impl<LV_RULE_CUDA_I>(L, bucket, order, proposal, P, H, act_cnt, hub_map,
-                                            st);
-  return move_bucket_impl<LV_RULE_PY_I>(L, bucket, order, proposal, P, H, act_cnt, hub_map, st);
+                                            variant, st);
+  return move_bucket_impl<LV_RULE_PY_I>(L, bucket, order, proposal, P, H, act_cnt, hub_map,
+                                        variant, st);
 }
 
 cudaError_t launch_apply_bucket(const LevelView& L, int bucket,

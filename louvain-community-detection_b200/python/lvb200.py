@@ -79,6 +79,15 @@ class KernelStat(ctypes.Structure):
     ]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("bucket_kernel", ctypes.c_uint8 * 8), ("bucket_ms", ctypes.c_float * 8)]
+
+
+KERNELS = ["lanes4", "lanes8", "lanes16", "lanes32", "warp128", "warp512", "block"]
+KERNEL_MAX_DEGREE = [4, 8, 16, 32, 84, 319, 2048]
+BUCKET_MAX_DEGREE = [0, 4, 8, 16, 32, 84, 319, 2048]
+
+
 class ServeConfig(ctypes.Structure):
     _fields_ = [("min_gain", ctypes.c_float), ("budget_bytes", ctypes.c_uint64),
                 ("max_graphs", ctypes.c_uint32), ("n_lanes", ctypes.c_uint32),
@@ -152,6 +161,9 @@ _SIGS = {
     "lv_batch_run": (ctypes.c_int, [_VP, _U32, _VP, ctypes.c_float, _VP, _VP, _VP,
                                     ctypes.POINTER(Result)]),
     "lv_serve_config_default": (None, [ctypes.POINTER(ServeConfig)]),
+    "lv_autotune": (ctypes.c_int, [_VP, _U32, ctypes.POINTER(Tuning)]),
+    "lv_set_tuning": (ctypes.c_int, [_VP, ctypes.POINTER(Tuning)]),
+    "lv_get_tuning": (ctypes.c_int, [_VP, ctypes.POINTER(Tuning)]),
     "lv_serve_create": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(ServeConfig),
                                        ctypes.POINTER(_VP)]),
     "lv_serve_wait": (ctypes.c_int, [_VP, _U32, ctypes.POINTER(ctypes.c_int)]),
@@ -382,6 +394,28 @@ class Engine:
                                    d_assignment or None, ctypes.byref(r)))
         self.n0 = n
         return r
+
+    # -- autotuning ------------------------------------------------------
+    def autotune(self, reps: int = 5) -> dict:
+        """Times every fitting kernel variant of every bucket on the loaded
+        graph's current level and keeps the fastest.  Returns {bucket:
+        (kernel name, ms per launch)} for the non-empty buckets."""
+        t = Tuning()
+        _check(lib().lv_autotune(self._h, reps, ctypes.byref(t)))
+        return {b: (KERNELS[t.bucket_kernel[b]], t.bucket_ms[b])
+                for b in range(1, 8) if t.bucket_ms[b] > 0}
+
+    def set_tuning(self, kernels):
+        """kernels: 7 names or ids, buckets 1..7."""
+        t = Tuning()
+        for b, k in enumerate(kernels, start=1):
+            t.bucket_kernel[b] = KERNELS.index(k) if isinstance(k, str) else int(k)
+        _check(lib().lv_set_tuning(self._h, ctypes.byref(t)))
+
+    def tuning(self) -> list:
+        t = Tuning()
+        _check(lib().lv_get_tuning(self._h, ctypes.byref(t)))
+        return [KERNELS[t.bucket_kernel[b]] for b in range(1, 8)]
 
     def batch_run(self, graphs, min_gain: float):
         """Runs every graph of `graphs` (Graph objects) in one batched run.
