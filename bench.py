@@ -196,6 +196,9 @@ def batched_measure(stream, count: int, steps: int = 2):
            "weights": "U(0.5,1.5) FP32", "seed": 0}
     with torch.cuda.stream(stream):
         eng = lvb200.Engine(stream=stream.cuda_stream)
+        # kernel variants tuned on the union's level 0 (untimed)
+        eng.load_device(N, E, off.data_ptr(), col.data_ptr(), w.data_ptr())
+        res["tuning"] = {str(b): k for b, (k, _) in eng.autotune().items()}
 
         def batch_step():
             return eng.batch_run_device(goff, N, E, off.data_ptr(), col.data_ptr(),
@@ -446,6 +449,11 @@ def run_engine(args, rank, world):
     torch.cuda.synchronize()
     eng = lvb200.Engine(device=dev, rule="py", stream=stream.cuda_stream,
                         use_graphs=not args.no_graphs)
+    tuning = None
+    if not args.no_tune:  # kernel variant per bucket, timed on level 0 (untimed)
+        with torch.cuda.stream(stream):
+            eng.load_device(n, nnz, d_off.data_ptr(), d_col.data_ptr(), d_w.data_ptr())
+            tuning = {str(b): k for b, (k, _) in eng.autotune().items()}
 
     def step():
         return eng.run_device(n, nnz, d_off.data_ptr(), d_col.data_ptr(),
@@ -542,7 +550,8 @@ def run_engine(args, rank, world):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": dict(desc, parallelism="replicas only" if world > 1 else "single GPU",
                        l2="flushed (256 MB write) between timed steps",
-                       pass_loop="host loop" if args.no_graphs else "CUDA graph WHILE node"),
+                       pass_loop="host loop" if args.no_graphs else "CUDA graph WHILE node",
+                       tuning=tuning or "defaults"),
         "final_q": q,
         "levels": [{"V": l["n_vertices"], "E": l["n_entries"], "passes": l["passes"],
                     "prepare_ms": round(l["prepare_ms"], 4),
@@ -581,6 +590,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="powerlaw")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default move kernel of every bucket (no lv_autotune)")
     ap.add_argument("--no-graphs", action="store_true",
                     help="run each level's pass loop from the host instead of a CUDA graph "
                          "WHILE node (same kernels; ncu cannot profile kernels inside "
