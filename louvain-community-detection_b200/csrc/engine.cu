@@ -170,7 +170,17 @@ thread_local Trace g_trace;  // per thread: server lanes step concurrently
 
 namespace lvb {
 static std::atomic<unsigned long long> g_launches{0};
-void count_launches(unsigned k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+// Launches recorded while a stream is captured only tally the graph's
+// kernels (t_tally); the graph's launches count them when it runs.
+thread_local bool t_capturing = false;
+thread_local unsigned long long t_tally = 0;
+void count_launches(unsigned k) {
+  if (t_capturing) {
+    t_tally += k;
+    return;
+  }
+  g_launches.fetch_add(k, std::memory_order_relaxed);
+}
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 }  // namespace lvb
 
@@ -275,10 +285,15 @@ struct lv_engine {
   cudaGraphExec_t pass_exec = nullptr;
   bool capturing = false;
   std::vector<PendingTiming> graph_timings;  // event pairs inside the graph
-  unsigned long long pass_launches = 0;      // kernels per replay
+  unsigned long long pass_launches = 0;      // kernels per replay (timing mode)
+  unsigned long long level_launches = 0;     // kernels per pass of the level graph
   unsigned long long* d_class_deg = nullptr;
   uint64_t class_deg[kClasses] = {};
   // move kernel variant of every bucket (1..7): defaults or lv_autotune's pick
+  // the pass descriptor (device) and the level graph built on it, kept
+  // across levels and runs while the key (form, rule, tuning) holds
+  PassDesc* d_desc = nullptr;
+  uint64_t level_key = ~0ull;
   uint8_t tune[8] = {kDefaultVariant[0], kDefaultVariant[1], kDefaultVariant[2],
                      kDefaultVariant[3], kDefaultVariant[4], kDefaultVariant[5],
                      kDefaultVariant[6], kDefaultVariant[7]};
@@ -355,11 +370,11 @@ void prof_collect_graph(lv_engine* E) {
   cudaGetLastError();
 }
 
+// Drops the per-level pass graph of the timing mode (the level graph of
+// the WHILE loop is kept: it reads the level from the descriptor).
 void drop_pass_graph(lv_engine* E) {
   if (E->pass_exec) cudaGraphExecDestroy(E->pass_exec);
   E->pass_exec = nullptr;
-  if (E->level_exec) cudaGraphExecDestroy(E->level_exec);
-  E->level_exec = nullptr;
   for (const PendingTiming& p : E->graph_timings) {
     E->ev_free.push_back(p.a);
     E->ev_free.push_back(p.b);
@@ -630,7 +645,8 @@ lv_status prepare_level(lv_engine* E) {
   P.blk_start[9] = u;
   P.total_blocks = u;
   // partials: hub accumulators + 2 per dispatch block
-  const size_t need_partials = hc + 2 * (size_t)dispatch_grid(P) + 16;
+  const size_t need_partials =
+      hc + 2 * (size_t)std::max(dispatch_grid(P), pass_dispatch_grid()) + 16;
   if (need_partials > E->partials_cap) {
     dfree(E->partials);
     CU(dalloc(&E->partials, need_partials));
@@ -731,26 +747,66 @@ lv_status prepare_level(lv_engine* E) {
 
 lv_status issue_pass(lv_engine* E, const PassControl* ctl);
 
+// Writes the current level into the device pass descriptor (every pass
+// kernel reads it at launch).
+lv_status upload_desc(lv_engine* E, float min_gain) {
+  PassDesc d{};
+  d.L = E->view();
+  const uint32_t* ord = E->batch ? E->act_order : E->order;
+  d.A = dispatch_args(ord, E->plan, E->plan.hub_count ? E->hub_map : nullptr, E->partials);
+  d.A.act_cnt = E->batch ? E->act_cnt : nullptr;
+  d.prop = E->prop;
+  d.full_order = E->order;
+  d.H = E->hub;
+  d.act_cnt = E->batch ? E->act_cnt : nullptr;
+  d.act_order = E->act_order;
+  d.cg = E->cg;
+  d.cg_new = E->cg_new;
+  d.n_graphs = E->batch ? E->n_graphs : 0u;
+  d.min_gain = (double)min_gain;
+  d.max_passes = E->cfg.max_passes;
+  CU(cudaMemcpyAsync(E->d_desc, &d, sizeof(d), cudaMemcpyHostToDevice, E->st));
+  return LV_OK;
+}
+
+// What a captured pass depends on besides the descriptor: the form
+// (batched passes compact their lists), the rule and the tuning.
+uint64_t level_key(const lv_engine* E) {
+  uint64_t k = (E->batch ? 1u : 0u) | ((uint64_t)(E->cfg.rule == LV_RULE_CUDA) << 1);
+  for (int b = 1; b <= kBuckets; b++) k |= (uint64_t)E->tune[b] << (4 * b);
+  return k;
+}
+
+void drop_level_exec(lv_engine* E) {
+  if (E->level_exec) cudaGraphExecDestroy(E->level_exec);
+  E->level_exec = nullptr;
+  E->level_key = ~0ull;
+}
+
 // Every pass of a level in one graph launch: [control init] -> WHILE
-// { 7 Jacobi steps; modularity sweep + stop rule }.  The body is captured
-// once per level; the modularity kernel's last block evaluates the stop
-// rule (modularity.cu:501-508) and sets the loop condition, so the host
-// waits once per level instead of once per pass.
+// { 7 Jacobi steps; modularity sweep + stop rule }.  The modularity
+// kernel's last block evaluates the stop rule (modularity.cu:501-508) and
+// sets the loop condition, so the host waits once per level instead of
+// once per pass.  The kernels read the level from the descriptor, so the
+// graph is captured once and replayed on every later level and run.
 lv_status run_level_graph(lv_engine* E, float min_gain) {
+  LVTRY(upload_desc(E, min_gain));
+  if (E->level_exec && E->level_key != level_key(E)) drop_level_exec(E);
   if (!E->level_exec) {
-    const unsigned long long l0 = launch_count();
     cudaGraph_t g = nullptr;
     CU(cudaGraphCreate(&g, 0));
     struct GraphGuard {
       cudaGraph_t g;
       ~GraphGuard() { if (g) cudaGraphDestroy(g); }
     } guard{g};
+    t_capturing = true;
+    t_tally = 0;
     CU(cudaStreamBeginCaptureToGraph(E->st, g, nullptr, nullptr, 0,
                                      cudaStreamCaptureModeThreadLocal));
-    cudaError_t ce = launch_pass_control_init(E->sc, E->batch ? E->gs : nullptr,
-                                              E->batch ? E->n_graphs : 0u, E->st);
+    cudaError_t ce = launch_pass_control_init(E->d_desc, E->st);
     cudaGraph_t cap = nullptr;
     cudaError_t ce2 = cudaStreamEndCapture(E->st, &cap);
+    t_capturing = false;
     CU(ce);
     CU(ce2);
     cudaGraphNode_t init_node = nullptr;
@@ -770,24 +826,22 @@ lv_status run_level_graph(lv_engine* E, float min_gain) {
     ctl.enabled = 1;
     ctl.use_handle = 1;
     ctl.handle = (unsigned long long)h;
-    ctl.min_gain = (double)min_gain;
-    ctl.max_passes = E->cfg.max_passes;
+    t_capturing = true;
+    t_tally = 0;
     CU(cudaStreamBeginCaptureToGraph(E->st, body, nullptr, nullptr, 0,
                                      cudaStreamCaptureModeThreadLocal));
     E->capturing = true;
-    const unsigned long long lb = launch_count();
     lv_status s = issue_pass(E, &ctl);
-    E->pass_launches = launch_count() - lb;
+    E->level_launches = t_tally;
     cudaGraph_t bcap = nullptr;
     ce = cudaStreamEndCapture(E->st, &bcap);
+    t_capturing = false;
     E->capturing = false;
     E->pending.clear();
     if (s != LV_OK) return s;
     CU(ce);
     CU(cudaGraphInstantiate(&E->level_exec, g, 0));
-    // capture counted the init kernel and one pass; lv_phase_move adds the
-    // kernels of the further passes once their number is known
-    (void)l0;
+    E->level_key = level_key(E);
     g_trace.mark("capture+instantiate", (uint32_t)E->levels.size(), E->n);
   }
   CU(cudaGraphLaunch(E->level_exec, E->st));
@@ -804,13 +858,15 @@ lv_status run_level_graph(lv_engine* E, float min_gain) {
 lv_status run_pass(lv_engine* E, const PassControl* ctl = nullptr) {
   if (!E->cfg.use_graphs) return issue_pass(E, ctl);
   if (!E->pass_exec) {
-    const unsigned long long l0 = launch_count();
+    t_capturing = true;
+    t_tally = 0;
     CU(cudaStreamBeginCapture(E->st, cudaStreamCaptureModeThreadLocal));
     E->capturing = true;
     lv_status s = issue_pass(E, ctl);
     cudaGraph_t g = nullptr;
     cudaError_t ce = cudaStreamEndCapture(E->st, &g);
     E->capturing = false;
+    t_capturing = false;
     if (s != LV_OK) {
       if (g) cudaGraphDestroy(g);
       return s;
@@ -819,12 +875,9 @@ lv_status run_pass(lv_engine* E, const PassControl* ctl = nullptr) {
     ce = cudaGraphInstantiate(&E->pass_exec, g, 0);
     cudaGraphDestroy(g);
     CU(ce);
-    E->pass_launches = launch_count() - l0;
+    E->pass_launches = t_tally;
     E->graph_timings.swap(E->pending);
     E->pending.clear();
-    // the capture counted its kernels once, which stands for this launch
-    CU(cudaGraphLaunch(E->pass_exec, E->st));
-    return LV_OK;
   }
   CU(cudaGraphLaunch(E->pass_exec, E->st));
   count_launches((unsigned)E->pass_launches);
@@ -832,42 +885,35 @@ lv_status run_pass(lv_engine* E, const PassControl* ctl = nullptr) {
 }
 
 lv_status issue_pass(lv_engine* E, const PassControl* ctl) {
-  const LevelView L = E->view();
   const int rule = (E->cfg.rule == LV_RULE_CUDA) ? LV_RULE_CUDA_I : LV_RULE_PY_I;
-  HubArena H = E->hub;
+  const PassDesc* D = E->d_desc;
+  cudaStream_t st = E->st;
   // batched form: this pass visits only the graphs still moving
-  const uint32_t* ord = E->order;
-  const uint32_t* ac = nullptr;
-  if (E->batch) {
-    CU(launch_compact_active(E->order, E->plan, E->cg, E->cg_new, E->gs, E->n_graphs,
-                             E->act_cnt, E->act_order, E->sc, E->st));
-    ord = E->act_order;
-    ac = E->act_cnt;
-  }
+  if (E->batch) CU(launch_compact_active(D, st));
+  // every bucket's kernels are issued, empty or not, so the pass has the
+  // same shape on every level
   for (int b = 1; b <= kBuckets; b++) {
     const uint32_t s = E->plan.cls_start[b];
     const uint32_t e = (b == 7) ? E->plan.cls_start[9] : E->plan.cls_start[b + 1];
-    if (e == s) continue;
     // algorithmic bytes: every entry's (col, w, comm[col]) and, per vertex,
     // order id, offset, comm, k, a_C(v) (FP64) and the proposal
     const double vb = (double)(e - s);
     const double v7 = (double)(E->plan.cls_start[b + 1] - s);
     cudaEvent_t t0 = prof_begin(E);
-    CU(launch_move_bucket(L, b, rule, ord, E->prop, E->plan, H, E->st, ac, nullptr, E->tune));
+    CU(launch_move_bucket(D, b, rule, E->tune, st));
     prof_end(E, t0, K_MOVE1 + b - 1, (double)E->class_deg[b] * 12.0 + v7 * 32.0);
-    if (b == 7 && E->plan.hub_count) {
+    if (b == 7) {
       t0 = prof_begin(E);
-      CU(launch_move_bucket(L, 8, rule, ord, E->prop, E->plan, H, E->st, ac, E->hub_map));
+      CU(launch_move_bucket(D, 8, rule, nullptr, st));
       prof_end(E, t0, K_HUB,
                (double)E->class_deg[8] * 12.0 + (double)E->plan.hub_count * 32.0);
     }
     t0 = prof_begin(E);
-    CU(launch_apply_bucket(L, b, ord, E->prop, E->plan, E->st, ac));
+    CU(launch_apply_bucket(D, b, E->batch, st));
     prof_end(E, t0, K_APPLY, vb * 12.0);
   }
   cudaEvent_t t0 = prof_begin(E);
-  CU(launch_modularity(L, ord, E->plan, E->plan.hub_count ? E->hub_map : nullptr,
-                       E->partials, E->st, ctl, ac));
+  CU(launch_modularity_pass(D, ctl, st));
   prof_end(E, t0, K_MODULARITY, (double)E->e * 12.0 + (double)E->n * 24.0);
   return LV_OK;
 }
@@ -941,12 +987,11 @@ lv_status batch_passes(lv_engine* E, float min_gain) {
   if (E->cfg.use_graphs && !E->profiling) {
     LVTRY(run_level_graph(E, min_gain));
   } else {
-    CU(launch_pass_control_init(E->sc, E->gs, E->n_graphs, E->st));
+    LVTRY(upload_desc(E, min_gain));
+    CU(launch_pass_control_init(E->d_desc, E->st));
     PassControl ctl{};
     ctl.enabled = 1;
     ctl.use_handle = 0;
-    ctl.min_gain = (double)min_gain;
-    ctl.max_passes = E->cfg.max_passes;
     for (;;) {
       LVTRY(run_pass(E, &ctl));
       CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost,
@@ -963,7 +1008,7 @@ lv_status batch_passes(lv_engine* E, float min_gain) {
   if (E->cfg.use_graphs && !E->profiling) {  // replays of the WHILE body
     uint32_t maxp = 0;
     for (uint32_t g = 0; g < E->n_graphs; g++) maxp = std::max(maxp, E->gs_host[g].passes);
-    if (maxp > 1) count_launches((unsigned)((maxp - 1) * E->pass_launches));
+    count_launches((unsigned)(1 + maxp * E->level_launches));
   }
   return check_device_error(E);
 }
@@ -1465,6 +1510,7 @@ lv_status lv_engine_create(const lv_config* cfg, lv_engine** out) {
     E->own_stream = true;
   }
   if ((ce = cudaMalloc(&E->sc, sizeof(LevelScalars))) != cudaSuccess ||
+      (ce = cudaMalloc(&E->d_desc, sizeof(PassDesc))) != cudaSuccess ||
       (ce = cudaMallocHost(&E->sc_host, sizeof(LevelScalars))) != cudaSuccess ||
       (ce = cudaMallocHost(&E->h_counts, 32 * sizeof(uint32_t))) != cudaSuccess ||
       (ce = cudaEventCreate(&E->ev0)) != cudaSuccess ||
@@ -1483,6 +1529,7 @@ void lv_engine_destroy(lv_engine* E) {
   cudaSetDevice(E->device);
   if (E->st) cudaStreamSynchronize(E->st);
   drop_pass_graph(E);
+  drop_level_exec(E);
   free_state(E);
   dfree(E->gs);
   dfree(E->goff_dev);
@@ -1499,6 +1546,7 @@ void lv_engine_destroy(lv_engine* E) {
   E->ev_free.clear();
   dfree(E->d_class_deg);
   if (E->sc) cudaFree(E->sc);
+  if (E->d_desc) cudaFree(E->d_desc);
   if (E->sc_host) cudaFreeHost(E->sc_host);
   if (E->h_counts) cudaFreeHost(E->h_counts);
   if (E->ev0) cudaEventDestroy(E->ev0);
@@ -1574,8 +1622,9 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
     ret = E->sc_host->first_fail ? 0 : 1;
     act = E->sc_host->q;
     old = E->sc_host->q_before;
-    if (passes > 1) count_launches((unsigned)((passes - 1) * E->pass_launches));
+    count_launches((unsigned)(1 + passes * E->level_launches));
   } else {
+    LVTRY(upload_desc(E, min_gain));
     bool first = true;
     do {
       LVTRY(run_pass(E));
@@ -2240,7 +2289,7 @@ lv_status lv_autotune(lv_engine* E, uint32_t reps, lv_tuning* out) {
   if (!reps) reps = 5;
   if (!E->level_ready) LVTRY(prepare_level(E));
   drop_pass_graph(E);  // a captured pass would keep the old kernels
-  const LevelView L = E->view();
+  LVTRY(upload_desc(E, 0.0f));
   const int rule = (E->cfg.rule == LV_RULE_CUDA) ? LV_RULE_CUDA_I : LV_RULE_PY_I;
   lv_tuning t{};
   for (int b = 1; b <= kBuckets; b++) {
@@ -2254,12 +2303,9 @@ lv_status lv_autotune(lv_engine* E, uint32_t reps, lv_tuning* out) {
       uint8_t kv[8];
       memcpy(kv, E->tune, sizeof(kv));
       kv[b] = (uint8_t)v;
-      CU(launch_move_bucket(L, b, rule, E->order, E->prop, E->plan, E->hub, E->st, nullptr,
-                            nullptr, kv));
+      CU(launch_move_bucket(E->d_desc, b, rule, kv, E->st));
       CU(cudaEventRecord(E->ev0, E->st));
-      for (uint32_t r = 0; r < reps; r++)
-        CU(launch_move_bucket(L, b, rule, E->order, E->prop, E->plan, E->hub, E->st, nullptr,
-                              nullptr, kv));
+      for (uint32_t r = 0; r < reps; r++) CU(launch_move_bucket(E->d_desc, b, rule, kv, E->st));
       CU(cudaEventRecord(E->ev1, E->st));
       CU(cudaEventSynchronize(E->ev1));
       float ms = 0.0f;

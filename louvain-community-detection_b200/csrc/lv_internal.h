@@ -206,13 +206,8 @@ cudaError_t launch_level_init(const LevelView& L, const uint32_t* order,
 // modularity then comes from its own vertices' rows and totals.
 cudaError_t launch_modularity(const LevelView& L, const uint32_t* order,
                               const DispatchPlan& P, const uint32_t* hub_map,
-                              double* partials, cudaStream_t st,
-                              const PassControl* ctl = nullptr,
-                              const uint32_t* act_cnt = nullptr);
-// passes = 0, first_fail = 0, q_prev = q (start of a level's pass loop),
-// for the single graph and for every graph of a batch
-cudaError_t launch_pass_control_init(LevelScalars* sc, GraphState* gs,
-                                     uint32_t n_graphs, cudaStream_t st);
+                              double* partials, cudaStream_t st);
+
 // Hubs (class 8).  A split pass reads every hub row once in chunks of
 // kHubChunk entries and writes each chunk's (community, weight) pairs
 // grouped by hash partition of the community (partitions of about
@@ -244,20 +239,66 @@ struct HubArena {
 constexpr int kHubPartSlots = 4096;
 constexpr uint32_t kHubPartKeys = 2048;
 constexpr uint32_t kHubMaxParts = 8192;
+
+// Work units of the class-dispatch kernels (row sums, modularity sweep).
+struct DispatchArgs {
+  DispatchPlan P;
+  const uint32_t* order;
+  const uint32_t* hub_blk_vertex;
+  const uint32_t* hub_blk_chunk;
+  double* hub_acc;
+  double* partials;         // [2 * gridDim.x]
+  const uint32_t* act_cnt;  // batched form: active lengths of classes 1..7
+};
+
+// Everything a pass's kernels need about the current level, in device
+// memory: the kernels of a pass read it at launch, so one captured pass
+// graph serves every level and every run (only this block is rewritten
+// between levels), and its grids are fixed.
+struct PassDesc {
+  LevelView L;
+  DispatchArgs A;              // class lists, plan, hub chunks, partials
+  uint32_t* prop;              // proposals, parallel to A.order
+  const uint32_t* full_order;  // batched form: the uncompacted class lists
+  HubArena H;
+  // batched form: active lists and their per-graph runs
+  uint32_t* act_cnt;
+  uint32_t* act_order;
+  const uint32_t* cg;
+  uint32_t* cg_new;
+  uint32_t n_graphs;
+  // device-side pass loop
+  double min_gain;
+  uint32_t max_passes;
+};
+
+// Pass kernels: every launch reads the level from D (device memory) and
+// uses a fixed grid, so a pass captured once replays on every level.
+// passes = 0, first_fail = 0, q_prev = q (start of a level's pass loop),
+// for the single graph and for every graph of a batch.
+cudaError_t launch_pass_control_init(const PassDesc* D, cudaStream_t st);
+// Proposals of bucket 1..7 (variant[b]: the kernel, null = defaults), or of
+// the hubs (bucket 8).
+cudaError_t launch_move_bucket(const PassDesc* D, int bucket, int rule, const uint8_t* variant,
+                               cudaStream_t st);
+// Applies bucket b's proposals (bucket 7: classes 7 and 8; `compacted`:
+// the batched form's active lists, where they are not adjacent).
+cudaError_t launch_apply_bucket(const PassDesc* D, int bucket, bool compacted, cudaStream_t st);
+// Modularity sweep of the pass; with ctl->enabled also the stop rule
+// (limits from D), with ctl->use_handle the WHILE node's condition.
+cudaError_t launch_modularity_pass(const PassDesc* D, const PassControl* ctl, cudaStream_t st);
+// Batched form: compacts the class lists to the graphs still moving
+// (skipped on the device while no graph stopped in the last pass).
+cudaError_t launch_compact_active(const PassDesc* D, cudaStream_t st);
+// Blocks of the pass's modularity sweep (its partials need 2 per block).
+unsigned pass_dispatch_grid();
+// Class-dispatch work units of a level (row sums, modularity sweeps).
+DispatchArgs dispatch_args(const uint32_t* order, const DispatchPlan& P, const uint32_t* hub_map,
+                           double* partials);
 // Proposals for the vertices of kernel class c (1..8; bucket 7 is classes 7
 // and 8, both launched before its apply).  proposal[] is parallel to
 // order[].
 // act_cnt: as for launch_modularity (null: whole classes).
-// Bucket 8 (hubs) also needs the hub dispatch map (hub index | chunk of
-// every kHubChunk-entry block, P.hub_blocks of each).
-// variant[b] (b = 1..7; null: the defaults) picks the kernel of bucket b.
-cudaError_t launch_move_bucket(const LevelView& L, int bucket, int rule,
-                               const uint32_t* order, uint32_t* proposal,
-                               const DispatchPlan& P, const HubArena& H,
-                               cudaStream_t st, const uint32_t* act_cnt = nullptr,
-                               const uint32_t* hub_map = nullptr,
-                               const uint8_t* variant = nullptr);
-
 // Move kernel variants a bucket can run on: G-lane groups (one entry per
 // lane, degree <= G), a warp with a 128- or 512-slot shared table, a block
 // with a 4096-slot table.  All give the same proposals; they differ in how
@@ -286,11 +327,7 @@ constexpr bool variant_fits(int v, int b) {
 }
 constexpr uint8_t kDefaultVariant[8] = {0, KV_SMALL4, KV_SMALL8, KV_SMALL16, KV_SMALL32,
                                         KV_WARP128, KV_WARP512, KV_BLOCK};
-cudaError_t launch_apply_bucket(const LevelView& L, int bucket,
-                                const uint32_t* order,
-                                const uint32_t* proposal,
-                                const DispatchPlan& P, cudaStream_t st,
-                                const uint32_t* act_cnt = nullptr);
+
 // Batched form.  cg[(c-1)*(G+1) + g] = first index of class c's list
 // holding a vertex of graph g (goff: the G+1 graph offsets of the level).
 cudaError_t launch_class_graph_starts(const uint32_t* order, const DispatchPlan& P,
@@ -298,12 +335,7 @@ cudaError_t launch_class_graph_starts(const uint32_t* order, const DispatchPlan&
                                       cudaStream_t st);
 // Compacted lists of classes 1..7 holding only the vertices of graphs
 // still active (same class offsets as order), lengths into act_cnt[1..7].
-// Skipped on the device while sc->act_changed is 0 (no graph stopped in
-// the last pass).
-cudaError_t launch_compact_active(const uint32_t* order, const DispatchPlan& P,
-                                  const uint32_t* cg, uint32_t* cg_new, const GraphState* gs,
-                                  uint32_t G, uint32_t* act_cnt, uint32_t* act_order,
-                                  const LevelScalars* sc, cudaStream_t st);
+
 // assignment[i] = map[assignment[i]]
 cudaError_t launch_compose(uint32_t* assignment, size_t n0,
                            const uint32_t* map, cudaStream_t st);

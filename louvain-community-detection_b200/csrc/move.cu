@@ -230,10 +230,13 @@ __device__ __forceinline__ unsigned long long candidate_loaded(const GainCtx& g,
 // deg <= G: G lanes per vertex, one edge per lane.
 template <int G, int RULE>
 __global__ void __launch_bounds__(kThreads)
-    move_small_kernel(LevelView L, const uint32_t* __restrict__ verts,
-                      uint32_t count, uint32_t* __restrict__ prop,
-                      const uint32_t* __restrict__ dcnt) {
-  if (dcnt) count = *dcnt;  // batched form: active vertices of the class
+    move_small_kernel(const PassDesc* __restrict__ D, int cls) {
+  const LevelView L = D->L;
+  const uint32_t s0 = D->A.P.cls_start[cls];
+  const uint32_t* __restrict__ verts = D->A.order + s0;
+  uint32_t* __restrict__ prop = D->prop + s0;
+  // batched form: the class's active vertices
+  const uint32_t count = D->act_cnt ? D->act_cnt[cls] : D->A.P.cls_start[cls + 1] - s0;
   __shared__ double sums[kWarps][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int gl = lane & (G - 1);
@@ -337,10 +340,12 @@ __device__ __forceinline__ unsigned long long scan_fresh_and_clear(
 // so a vertex costs one memory latency chain instead of one per wave.
 template <int T, int MAXW, int RULE>
 __global__ void __launch_bounds__(kThreads)
-    move_warp_kernel(LevelView L, const uint32_t* __restrict__ verts,
-                     uint32_t count, uint32_t* __restrict__ prop,
-                      const uint32_t* __restrict__ dcnt) {
-  if (dcnt) count = *dcnt;  // batched form: active vertices of the class
+    move_warp_kernel(const PassDesc* __restrict__ D, int cls) {
+  const LevelView L = D->L;
+  const uint32_t s0 = D->A.P.cls_start[cls];
+  const uint32_t* __restrict__ verts = D->A.order + s0;
+  uint32_t* __restrict__ prop = D->prop + s0;
+  const uint32_t count = D->act_cnt ? D->act_cnt[cls] : D->A.P.cls_start[cls + 1] - s0;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t n_fresh_sm[kWarps];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -515,10 +520,12 @@ __device__ __forceinline__ void insert_block_range(const LevelView& L, uint64_t 
 // 319 < deg <= 2048: one block per vertex, shared 4096-slot table.
 template <int RULE>
 __global__ void __launch_bounds__(kThreads)
-    move_block_kernel(LevelView L, const uint32_t* __restrict__ verts,
-                      uint32_t count, uint32_t* __restrict__ prop,
-                      const uint32_t* __restrict__ dcnt) {
-  if (dcnt) count = *dcnt;  // batched form: active vertices of the class
+    move_block_kernel(const PassDesc* __restrict__ D, int cls) {
+  const LevelView L = D->L;
+  const uint32_t s0 = D->A.P.cls_start[cls];
+  const uint32_t* __restrict__ verts = D->A.order + s0;
+  uint32_t* __restrict__ prop = D->prop + s0;
+  const uint32_t count = D->act_cnt ? D->act_cnt[cls] : D->A.P.cls_start[cls + 1] - s0;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int T = kHubSmemSlots;
   constexpr int MAXW = (int)(kHubSmemMaxDeg / kThreads);
@@ -621,9 +628,13 @@ __device__ __forceinline__ uint32_t block_scan_inplace(uint32_t* a, uint32_t n,
 
 template <int RULE>
 __global__ void __launch_bounds__(kThreads)
-    hub_split_kernel(LevelView L, const uint32_t* __restrict__ hubs, HubArena H,
-                     const uint32_t* __restrict__ blk_hub,
-                     const uint32_t* __restrict__ blk_ch, uint32_t nblocks) {
+    hub_split_kernel(const PassDesc* __restrict__ D) {
+  const LevelView L = D->L;
+  const uint32_t* __restrict__ hubs = D->A.order + D->A.P.cls_start[8];
+  const HubArena H = D->H;
+  const uint32_t nblocks = D->A.P.hub_blocks;
+  const uint32_t* __restrict__ blk_hub = D->A.hub_blk_vertex;
+  const uint32_t* __restrict__ blk_ch = D->A.hub_blk_chunk;
   constexpr int EPT = kHubChunk / kThreads;  // entries per thread
   static_assert(EPT * kThreads == (int)kHubChunk, "chunk = whole waves");
   __shared__ uint32_t cnt[kHubMaxParts];
@@ -706,8 +717,11 @@ __global__ void __launch_bounds__(kThreads)
 
 template <int RULE>
 __global__ void __launch_bounds__(kThreads)
-    hub_merge_kernel(LevelView L, const uint32_t* __restrict__ hubs, HubArena H,
-                     uint32_t units) {
+    hub_merge_kernel(const PassDesc* __restrict__ D) {
+  const LevelView L = D->L;
+  const uint32_t* __restrict__ hubs = D->A.order + D->A.P.cls_start[8];
+  const HubArena H = D->H;
+  const uint32_t units = H.units;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int T = kHubPartSlots;
   double* vals = reinterpret_cast<double*>(smem_raw);
@@ -785,9 +799,12 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 template <int RULE>
-__global__ void hub_decide_kernel(LevelView L, const uint32_t* __restrict__ hubs,
-                                  HubArena H, uint32_t hub_count,
-                                  uint32_t* __restrict__ prop) {
+__global__ void hub_decide_kernel(const PassDesc* __restrict__ D) {
+  const LevelView L = D->L;
+  const uint32_t* __restrict__ hubs = D->A.order + D->A.P.cls_start[8];
+  const HubArena H = D->H;
+  const uint32_t hub_count = D->A.P.hub_count;
+  uint32_t* __restrict__ prop = D->prop + D->A.P.cls_start[8];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < hub_count;
        i += gridDim.x * blockDim.x) {
     const uint32_t v = hubs[i];
@@ -805,10 +822,16 @@ __global__ void hub_decide_kernel(LevelView L, const uint32_t* __restrict__ hubs
 
 // Applies a bucket's proposals (assignCommunity + incremental totals).
 __global__ void __launch_bounds__(kThreads)
-    apply_kernel(LevelView L, const uint32_t* __restrict__ verts,
-                 const uint32_t* __restrict__ prop, uint32_t count,
-                 const uint32_t* __restrict__ dcnt) {
-  if (dcnt) count = *dcnt;
+    apply_kernel(const PassDesc* __restrict__ D, int lo_cls, int hi_cls) {
+  // classes lo..hi are adjacent in the lists (bucket 7 without compaction:
+  // classes 7 and 8); with compaction a class's active prefix
+  const LevelView L = D->L;
+  const uint32_t s0 = D->A.P.cls_start[lo_cls];
+  const uint32_t* __restrict__ verts = D->A.order + s0;
+  const uint32_t* __restrict__ prop = D->prop + s0;
+  const uint32_t count = (D->act_cnt && lo_cls <= kMoveClasses)
+                             ? D->act_cnt[lo_cls]
+                             : D->A.P.cls_start[hi_cls + 1] - s0;
   for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < count;
        i += gridDim.x * kThreads) {
     const uint32_t v = verts[i];
@@ -828,16 +851,6 @@ __global__ void __launch_bounds__(kThreads)
 // ---------------------------------------------------------------------------
 // Class-dispatch row reductions (row sums at level start, modularity sweep)
 // ---------------------------------------------------------------------------
-struct DispatchArgs {
-  DispatchPlan P;
-  const uint32_t* order;
-  const uint32_t* hub_blk_vertex;
-  const uint32_t* hub_blk_chunk;
-  double* hub_acc;
-  double* partials;  // [2 * gridDim.x]
-  const uint32_t* act_cnt;  // batched form: active lengths of classes 1..7
-};
-
 // Row sum: k_v = (float) sum_j w_vj.  vertex() returns the vertex's share
 // of its graph's accumulator (batched form).
 struct RowSumOp {
@@ -1132,8 +1145,8 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-__global__ void __launch_bounds__(kThreads)
-    modularity_kernel(LevelView L, DispatchArgs A, PassControl ctl) {
+__device__ __forceinline__ void modularity_body(const LevelView& L, const DispatchArgs& A,
+                                                const PassControl& ctl) {
   __shared__ double red[kWarps];
   double part = 0.0;
   dispatch_units(L, A, IntraOp{}, part, red);
@@ -1212,8 +1225,25 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-__global__ void pass_control_init_kernel(LevelScalars* sc, GraphState* gs,
-                                         uint32_t n_graphs) {
+__global__ void __launch_bounds__(kThreads)
+    modularity_kernel(LevelView L, DispatchArgs A, PassControl ctl) {
+  modularity_body(L, A, ctl);
+}
+
+// The modularity sweep of a pass (level and stop-rule limits from the
+// descriptor).
+__global__ void __launch_bounds__(kThreads)
+    modularity_pass_kernel(const PassDesc* __restrict__ D, PassControl ctl) {
+  ctl.min_gain = D->min_gain;
+  ctl.max_passes = D->max_passes;
+  const LevelView L = D->L;
+  modularity_body(L, D->A, ctl);
+}
+
+__global__ void pass_control_init_kernel(const PassDesc* __restrict__ D) {
+  LevelScalars* sc = D->L.sc;
+  GraphState* gs = D->L.gid ? D->L.gs : nullptr;
+  const uint32_t n_graphs = D->L.gid ? D->n_graphs : 0u;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t == 0) {
     sc->passes = 0u;
@@ -1385,6 +1415,11 @@ DispatchArgs make_args(const uint32_t* order, const DispatchPlan& P,
 
 }  // namespace
 
+DispatchArgs dispatch_args(const uint32_t* order, const DispatchPlan& P, const uint32_t* hub_map,
+                           double* partials) {
+  return make_args(order, P, hub_map, partials);
+}
+
 unsigned sm_count_cached() {
   static int num_sms = 0;
   if (!num_sms) {
@@ -1434,126 +1469,98 @@ cudaError_t launch_level_init(const LevelView& L, const uint32_t* order,
 
 cudaError_t launch_modularity(const LevelView& L, const uint32_t* order,
                               const DispatchPlan& P, const uint32_t* hub_map,
-                              double* partials, cudaStream_t st,
-                              const PassControl* ctl, const uint32_t* act_cnt) {
+                              double* partials, cudaStream_t st) {
   DispatchArgs A = make_args(order, P, hub_map, partials);
-  A.act_cnt = act_cnt;
   PassControl c{};
-  if (ctl) c = *ctl;
   (count_launches(1), modularity_kernel<<<dispatch_grid(P), kThreads, 0, st>>>(L, A, c));
   return cudaGetLastError();
 }
 
-cudaError_t launch_pass_control_init(LevelScalars* sc, GraphState* gs,
-                                     uint32_t n_graphs, cudaStream_t st) {
-  const unsigned g = n_graphs ? (n_graphs + 255) / 256 : 1;
-  (count_launches(1), pass_control_init_kernel<<<g, 256, 0, st>>>(sc, gs, n_graphs));
+// ---------------------------------------------------------------------------
+// Pass kernels.  Every launch reads the level from the descriptor and uses
+// a fixed grid (grid-stride loops end at the level's counts), so a pass
+// captured once replays on any level.
+// ---------------------------------------------------------------------------
+cudaError_t launch_pass_control_init(const PassDesc* D, cudaStream_t st) {
+  (count_launches(1), pass_control_init_kernel<<<sm_count(), 256, 0, st>>>(D));
   return cudaGetLastError();
 }
 
-// One launch of a move kernel variant over `cnt` vertices of a class list.
+cudaError_t launch_modularity_pass(const PassDesc* D, const PassControl* ctl, cudaStream_t st) {
+  PassControl c{};
+  if (ctl) c = *ctl;
+  (count_launches(1), modularity_pass_kernel<<<sm_count() * 8, kThreads, 0, st>>>(D, c));
+  return cudaGetLastError();
+}
+
+unsigned pass_dispatch_grid() { return sm_count() * 8; }
+
+// One launch of a move kernel variant over class `cls`.
 template <int RULE>
-static void launch_variant(int kv, const LevelView& L, const uint32_t* verts, uint32_t cnt,
-                           uint32_t* pr, const uint32_t* dc, cudaStream_t st) {
+static void launch_variant(int kv, const PassDesc* D, int cls, cudaStream_t st) {
   const unsigned cap = sm_count() * 8;
   switch (kv) {
     case KV_SMALL4:
-      (count_launches(1), move_small_kernel<4, RULE><<<grid_for((cnt + 63) / 64, cap), kThreads, 0, st>>>(L, verts, cnt, pr, dc));
+      (count_launches(1), move_small_kernel<4, RULE><<<cap, kThreads, 0, st>>>(D, cls));
       break;
     case KV_SMALL8:
-      (count_launches(1), move_small_kernel<8, RULE><<<grid_for((cnt + 31) / 32, cap), kThreads, 0, st>>>(L, verts, cnt, pr, dc));
+      (count_launches(1), move_small_kernel<8, RULE><<<cap, kThreads, 0, st>>>(D, cls));
       break;
     case KV_SMALL16:
-      (count_launches(1), move_small_kernel<16, RULE><<<grid_for((cnt + 15) / 16, cap), kThreads, 0, st>>>(L, verts, cnt, pr, dc));
+      (count_launches(1), move_small_kernel<16, RULE><<<cap, kThreads, 0, st>>>(D, cls));
       break;
     case KV_SMALL32:
-      (count_launches(1), move_small_kernel<32, RULE><<<grid_for((cnt + 7) / 8, cap), kThreads, 0, st>>>(L, verts, cnt, pr, dc));
+      (count_launches(1), move_small_kernel<32, RULE><<<cap, kThreads, 0, st>>>(D, cls));
       break;
     case KV_WARP128: {
       constexpr int T = 128;
-      (count_launches(1), move_warp_kernel<T, 3, RULE><<<grid_for((cnt + 7) / 8, cap), kThreads,
-                                  kWarps * T * kSlotBytes, st>>>(L, verts, cnt, pr, dc));
+      (count_launches(1), move_warp_kernel<T, 3, RULE><<<cap, kThreads, kWarps * T * kSlotBytes, st>>>(D, cls));
       break;
     }
     case KV_WARP512: {
       constexpr int T = 512;
-      (count_launches(1), move_warp_kernel<T, 10, RULE><<<grid_for((cnt + 7) / 8, sm_count() * 4), kThreads,
-                                  kWarps * T * kSlotBytes, st>>>(L, verts, cnt, pr, dc));
+      (count_launches(1), move_warp_kernel<T, 10, RULE><<<sm_count() * 4, kThreads,
+                                                        kWarps * T * kSlotBytes, st>>>(D, cls));
       break;
     }
     default:  // KV_BLOCK: shared table, one block per vertex
-      (count_launches(1), move_block_kernel<RULE><<<grid_for(cnt, sm_count() * 4), kThreads,
-                                kBlockTabSmem, st>>>(L, verts, cnt, pr, dc));
+      (count_launches(1), move_block_kernel<RULE><<<sm_count() * 4, kThreads, kBlockTabSmem, st>>>(D, cls));
       break;
   }
 }
 
 template <int RULE>
-static cudaError_t move_bucket_impl(const LevelView& L, int bucket,
-                                    const uint32_t* order, uint32_t* prop,
-                                    const DispatchPlan& P, const HubArena& H,
-                                    const uint32_t* act_cnt, const uint32_t* hub_map,
-                                    const uint8_t* kv, cudaStream_t st) {
-  const uint32_t s = P.cls_start[bucket];
-  const uint32_t cnt = P.cls_start[bucket + 1] - s;
-  // grids are sized for the whole class; with act_cnt the kernels read the
-  // active count and their grid-stride loops end early
-  const uint32_t* dc = (act_cnt && bucket <= 7) ? act_cnt + bucket : nullptr;
+static cudaError_t move_bucket_impl(const PassDesc* D, int bucket, const uint8_t* kv,
+                                    cudaStream_t st) {
   if (bucket >= 1 && bucket <= 7) {
     const int v = kv ? kv[bucket] : kDefaultVariant[bucket];
     if (!variant_fits(v, bucket)) return cudaErrorInvalidValue;
-    if (cnt) launch_variant<RULE>(v, L, order + s, cnt, prop + s, dc, st);
+    launch_variant<RULE>(v, D, bucket, st);
     return cudaGetLastError();
   }
   if (bucket != 8) return cudaErrorInvalidValue;
-  // class 8 of bucket 7: split chunks, merge (hub, partition)
-  const uint32_t hs = P.cls_start[8];
-  const uint32_t hc = P.cls_start[9] - hs;
-  if (hc) {
-    const uint32_t hb = P.hub_blocks;
-    (count_launches(1), hub_split_kernel<RULE><<<grid_for(hb, sm_count() * 6), kThreads, 0, st>>>(
-        L, order + hs, H, hub_map, hub_map + hb, hb));
-    (count_launches(1), hub_merge_kernel<RULE><<<grid_for(H.units, sm_count() * 3), kThreads,
-                                               kHubPartSmem, st>>>(L, order + hs, H, H.units));
-    (count_launches(1), hub_decide_kernel<RULE><<<(hc + 127) / 128, 128, 0, st>>>(
-        L, order + hs, H, hc, prop + hs));
-  }
+  // class 8 of bucket 7: split chunks, merge (hub, partition), decide
+  (count_launches(1), hub_split_kernel<RULE><<<sm_count() * 6, kThreads, 0, st>>>(D));
+  (count_launches(1), hub_merge_kernel<RULE><<<sm_count() * 3, kThreads, kHubPartSmem, st>>>(D));
+  (count_launches(1), hub_decide_kernel<RULE><<<sm_count() * 2, 128, 0, st>>>(D));
   return cudaGetLastError();
 }
 
-cudaError_t launch_move_bucket(const LevelView& L, int bucket, int rule,
-                               const uint32_t* order, uint32_t* proposal,
-                               const DispatchPlan& P, const HubArena& H,
-                               cudaStream_t st, const uint32_t* act_cnt,
-                               const uint32_t* hub_map, const uint8_t* variant) {
-  if (bucket == 8 && !hub_map) return cudaErrorInvalidValue;
-  if (rule == LV_RULE_CUDA_I)
-    return move_bucket_impl<LV_RULE_CUDA_I>(L, bucket, order, proposal, P, H, act_cnt, hub_map,
-                                            variant, st);
-  return move_bucket_impl<LV_RULE_PY_I>(L, bucket, order, proposal, P, H, act_cnt, hub_map,
-                                        variant, st);
+cudaError_t launch_move_bucket(const PassDesc* D, int bucket, int rule, const uint8_t* variant,
+                               cudaStream_t st) {
+  if (rule == LV_RULE_CUDA_I) return move_bucket_impl<LV_RULE_CUDA_I>(D, bucket, variant, st);
+  return move_bucket_impl<LV_RULE_PY_I>(D, bucket, variant, st);
 }
 
-cudaError_t launch_apply_bucket(const LevelView& L, int bucket,
-                                const uint32_t* order,
-                                const uint32_t* proposal,
-                                const DispatchPlan& P, cudaStream_t st,
-                                const uint32_t* act_cnt) {
-  const uint32_t s = P.cls_start[bucket];
-  // bucket 7 applies classes 7 and 8 (hubs); with compacted lists class 7's
-  // active part and the hubs are not adjacent, so they go separately
-  const bool split = act_cnt && bucket == 7;
-  const uint32_t e = (bucket == 7 && !split) ? P.cls_start[9] : P.cls_start[bucket + 1];
-  const uint32_t cnt = e - s;
+cudaError_t launch_apply_bucket(const PassDesc* D, int bucket, bool compacted, cudaStream_t st) {
   const unsigned cap = sm_count() * 8;
-  if (cnt)
-    (count_launches(1), apply_kernel<<<grid_for((cnt + kThreads - 1) / kThreads, cap), kThreads, 0, st>>>(
-        L, order + s, proposal + s, cnt, act_cnt ? act_cnt + bucket : nullptr));
-  if (split) {
-    const uint32_t hs = P.cls_start[8], hc = P.cls_start[9] - hs;
-    if (hc)
-      (count_launches(1), apply_kernel<<<grid_for((hc + kThreads - 1) / kThreads, cap), kThreads, 0, st>>>(
-          L, order + hs, proposal + hs, hc, nullptr));
+  if (bucket == 7 && !compacted) {  // classes 7 and 8 are adjacent
+    (count_launches(1), apply_kernel<<<cap, kThreads, 0, st>>>(D, 7, 8));
+  } else if (bucket == 7) {  // class 7's active prefix, then the hubs
+    (count_launches(1), apply_kernel<<<cap, kThreads, 0, st>>>(D, 7, 7));
+    (count_launches(1), apply_kernel<<<cap, kThreads, 0, st>>>(D, 8, 8));
+  } else {
+    (count_launches(1), apply_kernel<<<cap, kThreads, 0, st>>>(D, bucket, bucket));
   }
   return cudaGetLastError();
 }
@@ -1587,10 +1594,13 @@ __global__ void class_graph_starts_kernel(const uint32_t* __restrict__ order, Cl
 // lengths -> each active run's place in the compacted list, and the
 // class's active count.  Skipped while the active set is unchanged.
 __global__ void __launch_bounds__(1024)
-    compact_scan_kernel(const uint32_t* __restrict__ cg, const GraphState* __restrict__ gs,
-                        uint32_t G, uint32_t* __restrict__ cg_new, uint32_t* __restrict__ act_cnt,
-                        const LevelScalars* __restrict__ sc) {
-  if (!sc->act_changed) return;  // block-uniform
+    compact_scan_kernel(const PassDesc* __restrict__ D) {
+  const uint32_t* __restrict__ cg = D->cg;
+  const GraphState* __restrict__ gs = D->L.gs;
+  const uint32_t G = D->n_graphs;
+  uint32_t* __restrict__ cg_new = D->cg_new;
+  uint32_t* __restrict__ act_cnt = D->act_cnt;
+  if (!D->L.sc->act_changed) return;  // block-uniform
   __shared__ uint32_t warp_tot[32];
   __shared__ uint32_t carry;
   const uint32_t per = G + 1, c = blockIdx.x;
@@ -1634,18 +1644,16 @@ __global__ void __launch_bounds__(1024)
 // inactive graph's empty run shares its start with the next graph, and the
 // search takes the last of equal starts).  Skipped while the active set is
 // unchanged.
-__global__ void compact_copy_kernel(const uint32_t* __restrict__ order, ClassStarts cs,
-                                    const uint32_t* __restrict__ cg,
-                                    const uint32_t* __restrict__ cg_new,
-                                    const uint32_t* __restrict__ act_cnt, uint32_t G,
-                                    uint32_t* __restrict__ act_order,
-                                    const LevelScalars* __restrict__ sc) {
-  if (!sc->act_changed) return;
+__global__ void compact_copy_kernel(const PassDesc* __restrict__ D) {
+  if (!D->L.sc->act_changed) return;
+  const uint32_t* __restrict__ order = D->full_order;
+  uint32_t* __restrict__ act_order = D->act_order;
+  const uint32_t G = D->n_graphs;
   const uint32_t ci = blockIdx.y, per = G + 1;
-  const uint32_t total = act_cnt[1 + ci];
-  const uint32_t* row = cg + ci * per;
-  const uint32_t* row_new = cg_new + ci * per;
-  const uint32_t base = cs.s[ci + 1];
+  const uint32_t total = D->act_cnt[1 + ci];
+  const uint32_t* row = D->cg + ci * per;
+  const uint32_t* row_new = D->cg_new + ci * per;
+  const uint32_t base = D->A.P.cls_start[ci + 1];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += gridDim.x * blockDim.x) {
     uint32_t lo = 0, hi = G - 1;  // last g with row_new[g] <= i
@@ -1669,24 +1677,10 @@ cudaError_t launch_class_graph_starts(const uint32_t* order, const DispatchPlan&
   return cudaGetLastError();
 }
 
-cudaError_t launch_compact_active(const uint32_t* order, const DispatchPlan& P,
-                                  const uint32_t* cg, uint32_t* cg_new, const GraphState* gs,
-                                  uint32_t G, uint32_t* act_cnt, uint32_t* act_order,
-                                  const LevelScalars* sc, cudaStream_t st) {
-  ClassStarts cs;
-  for (int c = 0; c <= kClasses; c++) cs.s[c] = P.cls_start[c];
-  if (!G) return cudaSuccess;
-  (count_launches(1), compact_scan_kernel<<<kMoveClasses, 1024, 0, st>>>(cg, gs, G, cg_new, act_cnt,
-                                                                         sc));
-  // grid sized for the largest class; each class's threads stop at its
-  // active count
-  uint32_t most = 0;
-  for (int c = 1; c <= kMoveClasses; c++) most = std::max(most, P.cls_start[c + 1] - P.cls_start[c]);
-  if (most) {
-    const dim3 grid(grid_for((most + 255) / 256, sm_count() * 2), kMoveClasses);
-    (count_launches(1), compact_copy_kernel<<<grid, 256, 0, st>>>(order, cs, cg, cg_new, act_cnt, G,
-                                                                  act_order, sc));
-  }
+cudaError_t launch_compact_active(const PassDesc* D, cudaStream_t st) {
+  (count_launches(1), compact_scan_kernel<<<kMoveClasses, 1024, 0, st>>>(D));
+  const dim3 grid(sm_count() * 2, kMoveClasses);
+  (count_launches(1), compact_copy_kernel<<<grid, 256, 0, st>>>(D));
   return cudaGetLastError();
 }
 
