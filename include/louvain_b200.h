@@ -127,6 +127,14 @@ lv_status lv_graph_view(const lv_graph *g, uint32_t *n_vertices,
                         uint32_t *max_degree);
 void lv_graph_destroy(lv_graph *g);
 
+/* Binary CSR files (no counterpart in the reference): this library's own
+ * format ("LVBCSR01", n, max degree, nnz, offsets, cols, weights;
+ * little-endian), so a parsed graph reloads without the text parse
+ * (the CLI's --cache keeps one beside the .mtx).  Loading checks that the
+ * file is a consistent CSR.                                               */
+lv_status lv_graph_save(const lv_graph *g, const char *path);
+lv_status lv_graph_load(const char *path, lv_graph **out);
+
 /* ---- engine ----------------------------------------------------------- */
 lv_status lv_engine_create(const lv_config *cfg, lv_engine **out);
 void lv_engine_destroy(lv_engine *e);

@@ -19,8 +19,10 @@
 #include <algorithm>
 #include <cstring>
 #include <new>
-#include <vector>
 #include <string>
+#include <system_error>
+#include <thread>
+#include <vector>
 
 #include "../../include/louvain_b200.h"
 #include "lv_graph.h"
@@ -179,26 +181,118 @@ lv_status lv_graph_load_mtx(const char* path, lv_graph** out) {
   } catch (const std::bad_alloc&) {
     return io_fail(LV_ERR_NOMEM, "entry count too large for host memory");
   }
-  bool zero_based = false;
-  float wprev = 1.0f;
-  for (uint64_t i = 0; i < nnz; i++) {
-    if (!next_line(ls, le))
+  // Entry lines are parsed in parallel: the body is cut at line ends into
+  // chunks, a first sweep counts each chunk's lines (global line numbers),
+  // a second parses the first nnz lines in place.  A line without a weight
+  // repeats the previous line's (the reference's stream leaves `weight` as
+  // it was), so each chunk's leading weightless lines are fixed up after.
+  const char* body = p;
+  const size_t body_len = (size_t)(end - body);
+  unsigned hw = std::thread::hardware_concurrency();
+  const unsigned nt = (unsigned)std::max<size_t>(
+      1, std::min<size_t>({(size_t)std::min(hw ? hw : 1u, 32u), body_len / (1u << 22) + 1}));
+  std::vector<const char*> cb(nt + 1);
+  cb[0] = body;
+  cb[nt] = end;
+  for (unsigned t = 1; t < nt; t++) {
+    const char* c = body + body_len * t / nt;
+    if (c < cb[t - 1]) c = cb[t - 1];
+    const char* nl = (const char*)memchr(c, '\n', (size_t)(end - c));
+    cb[t] = nl ? nl + 1 : end;
+  }
+  std::vector<uint64_t> lines(nt + 1, 0);
+  auto count_lines = [&](unsigned t) {
+    uint64_t c = 0;
+    const char* q = cb[t];
+    while (q < cb[t + 1]) {
+      const char* nl = (const char*)memchr(q, '\n', (size_t)(cb[t + 1] - q));
+      c++;
+      q = nl ? nl + 1 : cb[t + 1];
+    }
+    lines[t + 1] = c;
+  };
+  struct ChunkOut {
+    bool zero = false;
+    bool any_weight = false;
+    uint64_t lead = 0;   // leading lines without a weight
+    float last = 1.0f;   // last explicit weight of the chunk
+    uint64_t bad = UINT64_MAX;  // first malformed line (global index)
+    lv_status bad_status = LV_OK;
+    std::string bad_what;
+  };
+  std::vector<ChunkOut> co(nt);
+  auto parse_chunk = [&](unsigned t) {
+    ChunkOut& o = co[t];
+    uint64_t idx = lines[t];
+    const char* q0 = cb[t];
+    float wprev = 1.0f;
+    while (q0 < cb[t + 1] && idx < nnz) {
+      const char* nl = (const char*)memchr(q0, '\n', (size_t)(cb[t + 1] - q0));
+      const char* le2 = nl ? nl : cb[t + 1];
+      const char* q = q0;
+      uint64_t a, b;
+      if (!parse_u64(q, le2, &a) || !parse_u64(q, le2, &b)) {
+        o.bad = idx;
+        o.bad_status = LV_ERR_PARSE;
+        o.bad_what = "bad entry line";
+        return;
+      }
+      if (a > 0xFFFFFFFFull || b > 0xFFFFFFFFull) {
+        o.bad = idx;
+        o.bad_status = LV_ERR_PARSE;
+        o.bad_what = "vertex index out of range";
+        return;
+      }
+      float x;
+      const int r = parse_weight(q, le2, &x);
+      if (r < 0) {
+        o.bad = idx;
+        o.bad_status = LV_ERR_PARSE;
+        o.bad_what = "bad weight";
+        return;
+      }
+      if (r > 0) {
+        wprev = std::fabs(x);
+        o.any_weight = true;
+        o.last = wprev;
+      } else if (!o.any_weight) {
+        o.lead++;
+      }
+      if (a == 0 || b == 0) o.zero = true;
+      src[idx] = (uint32_t)a;
+      dst[idx] = (uint32_t)b;
+      ws[idx] = wprev;
+      idx++;
+      q0 = nl ? nl + 1 : cb[t + 1];
+    }
+  };
+  auto run = [&](auto&& fn) {
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; t++) th.emplace_back(fn, t);
+    fn(0u);
+    for (auto& x : th) x.join();
+  };
+  try {
+    run(count_lines);
+    for (unsigned t = 0; t < nt; t++) lines[t + 1] += lines[t];
+    if (lines[nt] < nnz)
       return io_fail(LV_ERR_PARSE, "fewer entry lines than the size line's count");
-    lineno++;
-    const char* q = ls;
-    uint64_t a, b;
-    if (!parse_u64(q, le, &a) || !parse_u64(q, le, &b))
-      return io_fail(LV_ERR_PARSE, "bad entry line (line " + std::to_string(lineno) + ")");
-    if (a > 0xFFFFFFFFull || b > 0xFFFFFFFFull)
-      return io_fail(LV_ERR_PARSE, "vertex index out of range (line " + std::to_string(lineno) + ")");
-    float x;
-    int r = parse_weight(q, le, &x);
-    if (r < 0) return io_fail(LV_ERR_PARSE, "bad weight (line " + std::to_string(lineno) + ")");
-    if (r > 0) wprev = std::fabs(x);
-    if (a == 0 || b == 0) zero_based = true;
-    src[i] = (uint32_t)a;
-    dst[i] = (uint32_t)b;
-    ws[i] = wprev;
+    run(parse_chunk);
+  } catch (const std::system_error&) {
+    return io_fail(LV_ERR_NOMEM, "parser threads could not start");
+  }
+  bool zero_based = false;
+  float carry = 1.0f;
+  for (unsigned t = 0; t < nt; t++) {
+    const ChunkOut& o = co[t];
+    if (o.bad != UINT64_MAX)  // the first failure in file order
+      return io_fail(o.bad_status, o.bad_what + " (line " +
+                                       std::to_string(lineno + o.bad + 1) + ")");
+    zero_based = zero_based || o.zero;
+    const uint64_t first = lines[t];
+    const uint64_t stop = std::min<uint64_t>(first + o.lead, nnz);
+    for (uint64_t k = first; k < stop; k++) ws[k] = carry;
+    if (o.any_weight) carry = o.last;
   }
   const uint32_t n = (uint32_t)cols;
   for (uint64_t i = 0; i < nnz; i++) {
@@ -277,6 +371,71 @@ lv_status lv_graph_view(const lv_graph* g, uint32_t* n, uint64_t* nnz,
   if (col) *col = g->col.data();
   if (w) *w = g->w.data();
   if (max_deg) *max_deg = g->max_deg;
+  return LV_OK;
+}
+
+// Binary CSR file: "LVBCSR01", n (u32), max degree (u32), nnz (u64), then
+// offsets (u64, n+1), cols (u32, nnz), weights (f32, nnz); little-endian.
+static const char kCsrMagic[8] = {'L', 'V', 'B', 'C', 'S', 'R', '0', '1'};
+
+lv_status lv_graph_save(const lv_graph* g, const char* path) {
+  if (!g || !path) return io_fail(LV_ERR_ARG, "NULL argument");
+  FILE* f = fopen(path, "wb");
+  if (!f) return io_fail(LV_ERR_IO, "cannot open file for writing");
+  const uint32_t hdr32[2] = {g->n, g->max_deg};
+  const uint64_t nnz = g->nnz;
+  bool ok = fwrite(kCsrMagic, 1, 8, f) == 8 && fwrite(hdr32, 4, 2, f) == 2 &&
+            fwrite(&nnz, 8, 1, f) == 1 &&
+            fwrite(g->off.data(), 8, (size_t)g->n + 1, f) == (size_t)g->n + 1 &&
+            fwrite(g->col.data(), 4, nnz, f) == nnz && fwrite(g->w.data(), 4, nnz, f) == nnz;
+  ok = (fclose(f) == 0) && ok;
+  if (!ok) return io_fail(LV_ERR_IO, "write failed");
+  return LV_OK;
+}
+
+lv_status lv_graph_load(const char* path, lv_graph** out) {
+  if (!path || !out) return io_fail(LV_ERR_ARG, "NULL argument");
+  *out = nullptr;
+  FILE* f = fopen(path, "rb");
+  if (!f) return io_fail(LV_ERR_IO, "Error opening file");
+  char magic[8];
+  uint32_t hdr32[2];
+  uint64_t nnz = 0;
+  if (fread(magic, 1, 8, f) != 8 || memcmp(magic, kCsrMagic, 8) != 0 ||
+      fread(hdr32, 4, 2, f) != 2 || fread(&nnz, 8, 1, f) != 1 || hdr32[0] == 0xFFFFFFFFu) {
+    fclose(f);
+    return io_fail(LV_ERR_PARSE, "not a binary CSR file");
+  }
+  lv_graph* g = new (std::nothrow) lv_graph();
+  if (!g) {
+    fclose(f);
+    return io_fail(LV_ERR_NOMEM, "graph allocation failed");
+  }
+  const uint32_t n = hdr32[0];
+  try {
+    g->n = n;
+    g->max_deg = hdr32[1];
+    g->nnz = nnz;
+    g->off.resize((size_t)n + 1);
+    g->col.resize(nnz);
+    g->w.resize(nnz);
+  } catch (const std::bad_alloc&) {
+    fclose(f);
+    delete g;
+    return io_fail(LV_ERR_NOMEM, "graph too large for host memory");
+  }
+  bool ok = fread(g->off.data(), 8, (size_t)n + 1, f) == (size_t)n + 1 &&
+            fread(g->col.data(), 4, nnz, f) == nnz && fread(g->w.data(), 4, nnz, f) == nnz;
+  fclose(f);
+  // the structure must be a valid CSR of n vertices
+  ok = ok && g->off[0] == 0 && g->off[n] == nnz;
+  for (uint32_t v = 0; ok && v < n; v++) ok = g->off[v] <= g->off[(size_t)v + 1];
+  for (uint64_t j = 0; ok && j < nnz; j++) ok = g->col[j] < n;
+  if (!ok) {
+    delete g;
+    return io_fail(LV_ERR_PARSE, "truncated or inconsistent binary CSR file");
+  }
+  *out = g;
   return LV_OK;
 }
 

@@ -2,10 +2,12 @@
 #include "louvain_host.h"
 
 #include <getopt.h>
+#include <sys/stat.h>
 
 #include <cstdlib>
 #include <iostream>
 #include <iterator>
+#include <string>
 
 namespace lvb_host {
 
@@ -13,9 +15,22 @@ static void check(lv_status s) {
   if (s != LV_OK) throw Error(s, lv_last_error());
 }
 
+static bool g_use_cache = false;
+void setCsrCache(bool on) { g_use_cache = on; }
+
+// With the cache on, `<file>.lvbcsr` (a binary CSR newer than the file)
+// replaces the text parse, and is written after a parse.
 void parseGraph(Graph& graph, const char* filename) {
   lv_graph* g = nullptr;
-  check(lv_graph_load_mtx(filename, &g));
+  const std::string cache = std::string(filename) + ".lvbcsr";
+  struct stat sm {}, sc {};
+  const bool fresh = g_use_cache && stat(filename, &sm) == 0 && stat(cache.c_str(), &sc) == 0 &&
+                     sc.st_mtime >= sm.st_mtime;
+  if (!fresh || lv_graph_load(cache.c_str(), &g) != LV_OK) {
+    g = nullptr;
+    check(lv_graph_load_mtx(filename, &g));
+    if (g_use_cache) lv_graph_save(g, cache.c_str());  // best effort
+  }
   graph.host = g;
   uint32_t n = 0, md = 0;
   uint64_t e = 0;
@@ -88,6 +103,7 @@ void parseArgs(int argc, char** argv, float& threshold, bool& verbose,
   static const struct option longopts[] = {
       {"rule", required_argument, nullptr, 'r'},
       {"timing", no_argument, nullptr, 't'},
+      {"cache", no_argument, nullptr, 'c'},
       {nullptr, 0, nullptr, 0}};
   const char* usage = "Usage: ./gpulouvain -f mtx-matrix-file -g min-gain [-v]";
   bool fopt = false, gopt = false;
@@ -125,6 +141,9 @@ void parseArgs(int argc, char** argv, float& threshold, bool& verbose,
         break;
       case 't':
         timing = true;
+        break;
+      case 'c':
+        setCsrCache(true);
         break;
       case '?':
         std::cout << usage << std::endl;

@@ -35,6 +35,8 @@ struct Graph {
 
 // parseGraph (utils.cu:168-229): Matrix Market file -> host CSR.
 void parseGraph(Graph& graph, const char* filename);
+// This build's --cache: parseGraph keeps a binary CSR beside the file.
+void setCsrCache(bool on);
 
 // initDevGraph + copyToDevice + initCommAggr + setInitComm
 // (utils.cu:66-108): create the engine and upload the graph.
@@ -53,7 +55,7 @@ void aggregation(Graph& dev_graph);
 void printCommunities(Graph& dev_graph);
 
 // parseArgs (utils.cu:231-267): -f file -g min_gain [-v]; this build adds
-// --rule py|cuda and --timing (per-level times on stderr).
+// --rule py|cuda, --timing (per-level times on stderr) and --cache.
 void parseArgs(int argc, char** argv, float& threshold, bool& verbose,
                char*& filename, lv_rule& rule, bool& timing);
 

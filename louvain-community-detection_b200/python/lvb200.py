@@ -129,6 +129,8 @@ _SIGS = {
                                      ctypes.POINTER(_VP), ctypes.POINTER(_VP),
                                      ctypes.POINTER(_VP), ctypes.POINTER(_U32)]),
     "lv_graph_destroy": (None, [_VP]),
+    "lv_graph_save": (ctypes.c_int, [_VP, ctypes.c_char_p]),
+    "lv_graph_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_VP)]),
     "lv_engine_create": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(_VP)]),
     "lv_engine_destroy": (None, [_VP]),
     "lv_engine_load": (ctypes.c_int, [_VP, _VP]),
@@ -290,6 +292,16 @@ class Graph:
         h = ctypes.c_void_p()
         _check(lib().lv_graph_from_csr(n, _p(off), _p(col), _p(w), ctypes.byref(h)))
         return cls(h)
+
+    @classmethod
+    def load(cls, path: str) -> "Graph":
+        """A graph saved with save() (binary CSR)."""
+        h = ctypes.c_void_p()
+        _check(lib().lv_graph_load(path.encode(), ctypes.byref(h)))
+        return cls(h)
+
+    def save(self, path: str):
+        _check(lib().lv_graph_save(self._h, path.encode()))
 
     def csr(self):
         n = _U32()

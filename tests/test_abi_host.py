@@ -162,3 +162,50 @@ def test_pack_graphs_block_diagonal():
         assert np.array_equal(col[seg], c.astype(np.uint32) + vb)
         assert np.array_equal(w[seg], x)
         assert (col[seg] >= vb).all() and (col[seg] < vb + n).all()
+
+
+def test_binary_csr_round_trip(tmp_path):
+    """lv_graph_save / lv_graph_load give back the same CSR; damaged files
+    are rejected."""
+    n, s, d, w = lvgen.planted_powerlaw(n=3000, target_edges=9000, seed=5, unit=False)
+    mtx = str(tmp_path / "g.mtx")
+    lvgen.write_mtx(mtx, n, s, d, w)
+    g = lvb200.Graph.load_mtx(mtx)
+    path = str(tmp_path / "g.lvbcsr")
+    g.save(path)
+    h = lvb200.Graph.load(path)
+    a, b = g.csr(), h.csr()
+    assert a[0] == b[0] and a[4] == b[4]
+    for x, y in zip(a[1:4], b[1:4]):
+        assert np.array_equal(x, y)
+    raw = open(path, "rb").read()
+    bad = str(tmp_path / "bad.lvbcsr")
+    for blob in (raw[:40], b"XXXXXXXX" + raw[8:], raw[:-4]):
+        open(bad, "wb").write(blob)
+        with pytest.raises(lvb200.LouvainError):
+            lvb200.Graph.load(bad)
+
+
+def test_parallel_reader_weights_carry_across_chunks(tmp_path):
+    """A multi-chunk file (the reader splits large files across threads)
+    whose lines alternate between explicit and missing weights reads the
+    same as the oracle's serial reader."""
+    rng = np.random.default_rng(1)
+    n, m = 50_000, 400_000
+    src = rng.integers(1, n + 1, m)
+    dst = rng.integers(1, n + 1, m)
+    path = str(tmp_path / "big.mtx")
+    with open(path, "w") as f:
+        f.write(f"{n} {n} {m}\n")
+        for i in range(m):
+            if (i // 7) % 3 == 0:
+                f.write(f"{src[i]} {dst[i]}\n")
+            else:
+                f.write(f"{src[i]} {dst[i]} {rng.uniform(-2, 2):.6f}\n")
+    g = lvb200.Graph.load_mtx(path)
+    o = pyoracle.read_mtx(path, as_float=True)
+    n2, off, col, w, _ = g.csr()
+    assert n2 == o.n
+    assert np.array_equal(off, np.asarray(o.off))
+    assert np.array_equal(col, np.asarray(o.col))
+    assert np.array_equal(w, np.asarray(o.w).astype(np.float32))

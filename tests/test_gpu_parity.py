@@ -261,3 +261,22 @@ def test_cli_matches_reference_output_format(tmp_path):
         seen.extend(int(x) for x in parts[1:])
     assert len(lines) - 3 == ncomm
     assert sorted(seen) == list(range(1, gold["n_vertices"] + 1))
+
+
+def test_cli_cache_gives_the_same_output(tmp_path):
+    """--cache: the first run parses and writes <file>.lvbcsr, the second
+    loads it; both print the same modularity and communities."""
+    import shutil
+
+    cli = os.path.join(lvb200.PKG_DIR, "bin", "louvain")
+    mtx = str(tmp_path / "g.mtx")
+    shutil.copy(golden_mtx("planted_weighted"), mtx)
+    outs = []
+    for _ in range(2):
+        r = subprocess.run([cli, "-f", mtx, "-g", "1e-6", "-v", "--cache"],
+                           capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stdout + r.stderr
+        lines = r.stdout.splitlines()
+        outs.append([lines[0]] + lines[2:])  # line 2 holds times
+        assert os.path.exists(mtx + ".lvbcsr")
+    assert outs[0] == outs[1]
