@@ -78,24 +78,50 @@ void aggregation(Graph& dev_graph) {
   dev_graph.edges_sz = e;
 }
 
+// Groups the vertices by community with one counting sort (vertex ids stay
+// ascending inside a community, as the reference's push_back order leaves
+// them) and writes the listing through one buffer.
 void printCommunities(Graph& dev_graph) {
-  std::vector<uint32_t> comm(dev_graph.init_sz);
+  const size_t n0 = dev_graph.init_sz;
+  const size_t nc = dev_graph.vert_sz;
+  std::vector<uint32_t> comm(n0);
   check(lv_get_assignment(dev_graph.dev, comm.data(), comm.size()));
-  std::vector<std::vector<unsigned int>> comm_vert(dev_graph.vert_sz);
-  for (size_t i = 0; i < dev_graph.init_sz; i++) {
-    if (comm[i] < comm_vert.size()) comm_vert[comm[i]].push_back((unsigned)i + 1);
+  std::vector<uint64_t> start(nc + 1, 0);
+  for (size_t i = 0; i < n0; i++)
+    if (comm[i] < nc) start[(size_t)comm[i] + 1]++;
+  for (size_t c = 0; c < nc; c++) start[c + 1] += start[c];
+  std::vector<uint32_t> members(start[nc]);
+  {
+    std::vector<uint64_t> cur(start.begin(), start.end() - 1);
+    for (size_t i = 0; i < n0; i++)
+      if (comm[i] < nc) members[cur[comm[i]]++] = (uint32_t)i + 1;
   }
-  unsigned int comm_n = 1;
-  std::cout << dev_graph.vert_sz << std::endl;
-  for (size_t i = 0; i < dev_graph.vert_sz; i++) {
-    if (!comm_vert[i].empty()) {
-      std::cout << comm_n << " ";
-      std::copy(comm_vert[i].begin(), comm_vert[i].end(),
-                std::ostream_iterator<unsigned int>(std::cout, " "));
-      std::cout << std::endl;
-      comm_n++;
+  std::string out;
+  out.reserve(16 * (n0 + nc) + 32);
+  char num[24];
+  auto put = [&](uint64_t v) {
+    int k = 0;
+    do {
+      num[k++] = (char)('0' + v % 10);
+      v /= 10;
+    } while (v);
+    while (k) out.push_back(num[--k]);
+  };
+  put(nc);
+  out.push_back('\n');
+  uint64_t comm_n = 1;
+  for (size_t c = 0; c < nc; c++) {
+    if (start[c] == start[c + 1]) continue;
+    put(comm_n++);
+    out.push_back(' ');
+    for (uint64_t k = start[c]; k < start[c + 1]; k++) {
+      put(members[k]);
+      out.push_back(' ');
     }
+    out.push_back('\n');
   }
+  std::cout.write(out.data(), (std::streamsize)out.size());
+  std::cout.flush();
 }
 
 void parseArgs(int argc, char** argv, float& threshold, bool& verbose,
