@@ -296,7 +296,7 @@ def served_measure(count: int, rate: float, budget: int, seed: int = 0):
     return served_report(reqs, arrivals, rate, budget)
 
 
-def serve_run(reqs, arrivals, budget, lanes=3):
+def serve_run(reqs, arrivals, budget, lanes=4):
     """Replays the arrivals against a server (lanes > 1: the default size
     lanes stepped by worker threads; 1: one union stepped by this loop);
     returns (results by request, completion times, steps, most graphs
@@ -343,7 +343,7 @@ def served_report(reqs, arrivals, rate, budget):
     done1, done_t1, _, _ = serve_run(reqs, arrivals, budget, lanes=1)
     lat1 = (done_t1 - arrivals) * 1000.0
     makespan1 = float(done_t1.max() - arrivals[0])
-    done, done_t, steps, max_res = serve_run(reqs, arrivals, budget, lanes=3)
+    done, done_t, steps, max_res = serve_run(reqs, arrivals, budget, lanes=4)
     lat = (done_t - arrivals) * 1000.0
     makespan = float(done_t.max() - arrivals[0])
     # plain engine, one request at a time
@@ -378,8 +378,8 @@ def served_report(reqs, arrivals, rate, budget):
         "mix": "50% R-MAT scale U{10..21}, 50% LFR-style n log-U[1k,2M] mu U(0.1,0.5)",
         "kinds": kinds, "total_entries": int(sum(r[2] for r in reqs)),
         "total_vertices": int(sum(r[1] for r in reqs)), "budget_gb": budget / 1e9,
-        "served": {"lanes": "3 (<= 2^18, <= 2^23, larger entries; 15/35/50% of the budget), "
-                            "worker threads",
+        "served": {"lanes": "4 (<= 2^18, <= 2^23 entries, two for larger ones; "
+                            "10/30/30/30% of the budget), worker threads",
                    "graphs_per_s": count / makespan, "makespan_s": makespan,
                    "p50_ms": float(np.percentile(lat, 50)),
                    "p99_ms": float(np.percentile(lat, 99)),

@@ -274,10 +274,12 @@ typedef struct {
   int background;                /* step the lanes on worker threads */
 } lv_serve_config;
 
-/* 3 background lanes: <= 2^18 entries (15% of the budget), <= 2^23 (35%),
- * larger (50%); budget 8 GiB; min_gain 1e-6.  Each lane holds a fifth of
- * its budget for per-vertex state at 192 B a vertex and the rest for
- * adjacency at 40 B an entry.                                              */
+/* 4 background lanes: <= 2^18 entries (10% of the budget), <= 2^23 (30%),
+ * and two for larger graphs (30% each); budget 8 GiB; min_gain 1e-6.
+ * Lanes with the same bound form a group: a request goes to the group's
+ * lane with the fewest entries resident or queued.  Each lane holds a
+ * fifth of its budget for per-vertex state at 192 B a vertex and the rest
+ * for adjacency at 40 B an entry.                                          */
 void lv_serve_config_default(lv_serve_config *c);
 
 typedef struct {

@@ -2006,15 +2006,15 @@ void lv_serve_config_default(lv_serve_config* c) {
   c->min_gain = 1e-6f;
   c->budget_bytes = 8ull << 30;
   c->max_graphs = 0;
-  c->n_lanes = 3;
+  c->n_lanes = 4;
   c->lane_max_entries[0] = 1ull << 18;
   c->lane_max_entries[1] = 1ull << 23;
   c->lane_max_entries[2] = ~0ull;
   c->lane_max_entries[3] = ~0ull;
-  c->lane_share[0] = 0.15f;
-  c->lane_share[1] = 0.35f;
-  c->lane_share[2] = 0.50f;
-  c->lane_share[3] = 0.0f;
+  c->lane_share[0] = 0.10f;
+  c->lane_share[1] = 0.30f;
+  c->lane_share[2] = 0.30f;
+  c->lane_share[3] = 0.30f;
   c->background = 1;
 }
 
@@ -2034,6 +2034,9 @@ lv_status lv_serve_create(const lv_config* cfg, const lv_serve_config* scfg, lv_
   if (!S) return fail(LV_ERR_NOMEM, "server allocation failed");
   S->cfg = *scfg;
   S->cfg.lane_max_entries[scfg->n_lanes - 1] = ~0ull;  // the last lane takes the rest
+  for (uint32_t i = scfg->n_lanes - 1; i > 0; i--)  // so do lanes with the same bound
+    if (scfg->lane_max_entries[i - 1] == scfg->lane_max_entries[scfg->n_lanes - 1])
+      S->cfg.lane_max_entries[i - 1] = ~0ull;
   for (uint32_t i = 0; i < scfg->n_lanes; i++) {
     const uint64_t budget = (uint64_t)((double)scfg->budget_bytes * scfg->lane_share[i] / share_sum);
     if (budget < 64 * (per_v + per_e)) {
@@ -2120,12 +2123,23 @@ lv_status lv_serve_create(const lv_config* cfg, const lv_serve_config* scfg, lv_
 
 lv_status lv_serve_submit(lv_server* S, const lv_graph* g, uint64_t* ticket) {
   if (!S || !g) return fail(LV_ERR_ARG, "NULL server or graph");
-  uint32_t lane = ~0u;  // the first lane for the graph's size that can hold it
-  for (uint32_t i = 0; i < S->lanes.size(); i++) {
-    const ServeLane* L = S->lanes[i];
-    if (g->nnz <= L->max_entries && g->n <= L->cap_n && g->nnz <= L->cap_e) {
-      lane = i;
-      break;
+  // the first size bound that holds the graph; among the lanes sharing that
+  // bound (a group), the one with the fewest entries resident or queued
+  uint32_t lane = ~0u;
+  {
+    std::lock_guard<std::mutex> lock(S->mu);
+    uint64_t bound = 0, best_load = ~0ull;
+    for (uint32_t i = 0; i < S->lanes.size(); i++) {
+      const ServeLane* L = S->lanes[i];
+      if (g->nnz > L->max_entries || g->n > L->cap_n || g->nnz > L->cap_e) continue;
+      if (lane != ~0u && L->max_entries != bound) break;
+      uint64_t load = L->res_e;
+      for (const ServeRequest* q : L->queue) load += q->nnz;
+      if (lane == ~0u || load < best_load) {
+        lane = i;
+        bound = L->max_entries;
+        best_load = load;
+      }
     }
   }
   if (lane == ~0u) return fail(LV_ERR_LIMIT, "graph exceeds the server's device budget");
