@@ -55,22 +55,32 @@ lv_status cuda_fail(cudaError_t e, const char* what) {
     if (s_ != LV_OK) return s_;       \
   } while (0)
 
-// Device buffers are stream-ordered allocations on the calling engine's
-// stream (set by AllocScope in every entry point), so growing a buffer never
-// synchronises the whole device -- several engines (the server's lanes)
-// run side by side.  Without a scope: plain cudaMalloc / cudaFree.
+// Device buffers are stream-ordered allocations from the calling engine's
+// own memory pool on its stream (set by AllocScope in every entry point), so
+// growing a buffer never synchronises the whole device -- several engines
+// (the server's lanes) run side by side.  A pool per engine also keeps one
+// engine's allocation from reusing a block another engine freed on its
+// stream, which would make the first wait for the second's queued work.
+// Without a scope: plain cudaMalloc / cudaFree.
 thread_local cudaStream_t t_alloc_stream = nullptr;
+thread_local cudaMemPool_t t_alloc_pool = nullptr;
 
 struct AllocScope {
   cudaStream_t prev;
-  explicit AllocScope(cudaStream_t s) : prev(t_alloc_stream) { t_alloc_stream = s; }
-  ~AllocScope() { t_alloc_stream = prev; }
+  cudaMemPool_t prev_pool;
+  explicit AllocScope(const lv_engine* E);
+  ~AllocScope() {
+    t_alloc_stream = prev;
+    t_alloc_pool = prev_pool;
+  }
 };
 
 template <typename T>
 cudaError_t dalloc(T** p, size_t count) {
   *p = nullptr;
   if (count == 0) count = 1;
+  if (t_alloc_stream && t_alloc_pool)
+    return cudaMallocFromPoolAsync((void**)p, count * sizeof(T), t_alloc_pool, t_alloc_stream);
   if (t_alloc_stream) return cudaMallocAsync((void**)p, count * sizeof(T), t_alloc_stream);
   return cudaMalloc((void**)p, count * sizeof(T));
 }
@@ -188,6 +198,7 @@ struct lv_engine {
   lv_config cfg;
   cudaStream_t st = nullptr;
   bool own_stream = false;
+  cudaMemPool_t pool = nullptr;  // this engine's stream-ordered allocations
   int device = 0;
 
   // capacities of the allocations below
@@ -321,6 +332,11 @@ struct lv_engine {
 };
 
 namespace {
+
+AllocScope::AllocScope(const lv_engine* E) : prev(t_alloc_stream), prev_pool(t_alloc_pool) {
+  t_alloc_stream = E ? E->st : nullptr;
+  t_alloc_pool = E ? E->pool : nullptr;
+}
 
 cudaEvent_t take_event(lv_engine* E) {
   if (!E->ev_free.empty()) {
@@ -1340,7 +1356,7 @@ lv_status serve_append(ServeLane* L, ServeRequest* r) {
 lv_status lane_step(lv_server* S, ServeLane* L) {
   lv_engine* E = L->E;
   cudaSetDevice(E->device);
-  AllocScope alloc_scope(E->st);
+  AllocScope alloc_scope(E);
   std::vector<ServeRequest*> adm;
   {
     std::lock_guard<std::mutex> lock(S->mu);
@@ -1491,19 +1507,26 @@ lv_status lv_engine_create(const lv_config* cfg, lv_engine** out) {
     delete E;
     return cuda_fail(ce, "configure_kernels");
   }
-  {  // keep freed stream-ordered blocks in the pool for the next growth
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, E->device) == cudaSuccess) {
-      uint64_t keep = ~0ull;
-      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  {  // the engine's own pool; freed blocks stay in it for the next growth
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = E->device;
+    ce = cudaMemPoolCreate(&E->pool, &props);
+    if (ce != cudaSuccess) {
+      delete E;
+      return cuda_fail(ce, "cudaMemPoolCreate");
     }
-    cudaGetLastError();
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(E->pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
   if (E->cfg.stream) {
     E->st = (cudaStream_t)E->cfg.stream;
   } else {
     ce = cudaStreamCreateWithFlags(&E->st, cudaStreamNonBlocking);
     if (ce != cudaSuccess) {
+      cudaMemPoolDestroy(E->pool);
       delete E;
       return cuda_fail(ce, "cudaStreamCreate");
     }
@@ -1525,7 +1548,7 @@ lv_status lv_engine_create(const lv_config* cfg, lv_engine** out) {
 
 void lv_engine_destroy(lv_engine* E) {
   if (!E) return;
-  AllocScope alloc_scope(E->st);
+  AllocScope alloc_scope(E);
   cudaSetDevice(E->device);
   if (E->st) cudaStreamSynchronize(E->st);
   drop_pass_graph(E);
@@ -1551,12 +1574,14 @@ void lv_engine_destroy(lv_engine* E) {
   if (E->h_counts) cudaFreeHost(E->h_counts);
   if (E->ev0) cudaEventDestroy(E->ev0);
   if (E->ev1) cudaEventDestroy(E->ev1);
+  if (E->st) cudaStreamSynchronize(E->st);  // the frees above are stream-ordered
+  if (E->pool) cudaMemPoolDestroy(E->pool);
   if (E->own_stream && E->st) cudaStreamDestroy(E->st);
   delete E;
 }
 
 lv_status lv_engine_load(lv_engine* E, const lv_graph* g) {
-  AllocScope alloc_scope(E ? E->st : nullptr);
+  AllocScope alloc_scope(E);
   if (!E || !g) return fail(LV_ERR_ARG, "NULL engine or graph");
   LVTRY(validate_sizes(g->n, g->nnz));
   cudaSetDevice(E->device);
@@ -1578,7 +1603,7 @@ lv_status lv_engine_load(lv_engine* E, const lv_graph* g) {
 lv_status lv_engine_load_device(lv_engine* E, uint32_t n, uint64_t nnz,
                                 const uint64_t* d_off, const uint32_t* d_col,
                                 const float* d_w) {
-  AllocScope alloc_scope(E ? E->st : nullptr);
+  AllocScope alloc_scope(E);
   if (!E || !d_off || (nnz && (!d_col || !d_w)))
     return fail(LV_ERR_ARG, "NULL engine or device buffer");
   LVTRY(validate_sizes(n, nnz));
@@ -1591,7 +1616,7 @@ lv_status lv_engine_load_device(lv_engine* E, uint32_t n, uint64_t nnz,
 }
 
 lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
-  AllocScope alloc_scope(E ? E->st : nullptr);
+  AllocScope alloc_scope(E);
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   if (E->finished) return fail(LV_ERR_STATE, "the run has ended; load a graph again");
@@ -1662,7 +1687,7 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
 }
 
 lv_status lv_phase_aggregate(lv_engine* E) {
-  AllocScope alloc_scope(E ? E->st : nullptr);
+  AllocScope alloc_scope(E);
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   if (!E->loaded || !E->level_ready) return fail(LV_ERR_STATE, "no move phase to aggregate");
   cudaSetDevice(E->device);
@@ -1751,7 +1776,7 @@ static lv_status run_loaded(lv_engine* E, float min_gain, lv_result* res) {
 }
 
 lv_status lv_run(lv_engine* E, const lv_graph* g, float min_gain, lv_result* res) {
-  AllocScope alloc_scope(E ? E->st : nullptr);
+  AllocScope alloc_scope(E);
   if (!E || !g) return fail(LV_ERR_ARG, "NULL engine or graph");
   cudaSetDevice(E->device);
   cudaEvent_t c0, c1;
@@ -1778,7 +1803,7 @@ lv_status lv_run(lv_engine* E, const lv_graph* g, float min_gain, lv_result* res
 lv_status lv_run_device(lv_engine* E, uint32_t n, uint64_t nnz, const uint64_t* d_off,
                         const uint32_t* d_col, const float* d_w, float min_gain,
                         uint32_t* d_assignment, lv_result* res) {
-  AllocScope alloc_scope(E ? E->st : nullptr);
+  AllocScope alloc_scope(E);
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   LVTRY(lv_engine_load_device(E, n, nnz, d_off, d_col, d_w));
   LVTRY(run_loaded(E, min_gain, res));
@@ -1796,7 +1821,7 @@ lv_status lv_run_device(lv_engine* E, uint32_t n, uint64_t nnz, const uint64_t* 
 }
 
 lv_status lv_get_assignment(lv_engine* E, uint32_t* out, size_t n) {
-  AllocScope alloc_scope(E ? E->st : nullptr);
+  AllocScope alloc_scope(E);
   if (!E || (!out && n)) return fail(LV_ERR_ARG, "NULL argument");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   if (n != E->n0) return fail(LV_ERR_ARG, "buffer length must equal the input vertex count");
@@ -1831,7 +1856,7 @@ lv_status lv_get_level_size(lv_engine* E, uint32_t* n, uint64_t* e) {
 
 lv_status lv_get_level_state(lv_engine* E, uint32_t* comm, uint32_t* comm_size,
                              float* weighted_degree) {
-  AllocScope alloc_scope(E ? E->st : nullptr);
+  AllocScope alloc_scope(E);
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   cudaSetDevice(E->device);
@@ -1850,7 +1875,7 @@ lv_status lv_get_level_state(lv_engine* E, uint32_t* comm, uint32_t* comm_size,
 
 lv_status lv_get_level_csr(lv_engine* E, uint64_t* offsets, uint32_t* cols,
                            float* weights) {
-  AllocScope alloc_scope(E ? E->st : nullptr);
+  AllocScope alloc_scope(E);
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   cudaSetDevice(E->device);
@@ -1867,7 +1892,7 @@ lv_status lv_get_level_csr(lv_engine* E, uint64_t* offsets, uint32_t* cols,
 }
 
 lv_status lv_set_level_comm(lv_engine* E, const uint32_t* comm) {
-  AllocScope alloc_scope(E ? E->st : nullptr);
+  AllocScope alloc_scope(E);
   if (!E || !comm) return fail(LV_ERR_ARG, "NULL argument");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   cudaSetDevice(E->device);
@@ -1886,7 +1911,7 @@ lv_status lv_set_level_comm(lv_engine* E, const uint32_t* comm) {
 }
 
 lv_status lv_modularity_fp64(lv_engine* E, const uint32_t* partition, double* q) {
-  AllocScope alloc_scope(E ? E->st : nullptr);
+  AllocScope alloc_scope(E);
   if (!E || !partition || !q) return fail(LV_ERR_ARG, "NULL argument");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   cudaSetDevice(E->device);
@@ -1932,7 +1957,7 @@ lv_status lv_batch_run_device(lv_engine* E, uint32_t n_graphs, const uint64_t* g
                               const uint32_t* d_cols, const float* d_weights, float min_gain,
                               uint32_t* d_assignment, double* modularity, uint32_t* levels,
                               lv_result* res) {
-  AllocScope alloc_scope(E ? E->st : nullptr);
+  AllocScope alloc_scope(E);
   if (!E || !graph_offsets || !d_assignment || (n_graphs && !modularity))
     return fail(LV_ERR_ARG, "NULL argument");
   if (n_graphs == 0) return fail(LV_ERR_ARG, "no graphs");
@@ -1948,7 +1973,7 @@ lv_status lv_batch_run_device(lv_engine* E, uint32_t n_graphs, const uint64_t* g
 lv_status lv_batch_run(lv_engine* E, uint32_t n_graphs, const lv_graph* const* graphs,
                        float min_gain, uint32_t* assignment, double* modularity,
                        uint32_t* levels, lv_result* res) {
-  AllocScope alloc_scope(E ? E->st : nullptr);
+  AllocScope alloc_scope(E);
   if (!E || !graphs || !assignment || !modularity) return fail(LV_ERR_ARG, "NULL argument");
   if (n_graphs == 0) return fail(LV_ERR_ARG, "no graphs");
   // pack the graphs into one block-diagonal CSR (vertex ids offset per graph)
@@ -2081,7 +2106,7 @@ lv_status lv_serve_create(const lv_config* cfg, const lv_serve_config* scfg, lv_
     L->cap_e = (budget - cap_n * per_v) / per_e;
     L->slot_cap = scfg->max_graphs ? scfg->max_graphs : 4096;
     auto setup = [&]() -> lv_status {
-      AllocScope alloc_scope(E->st);
+      AllocScope alloc_scope(E);
       LVTRY(ensure_capacity(E, L->cap_n, L->cap_e, false));
       LVTRY(batch_alloc(E, L->slot_cap));
       CU(dalloc(&E->act_order, L->cap_n));
@@ -2282,7 +2307,7 @@ void lv_serve_destroy(lv_server* S) {
     if (L->E) {
       cudaSetDevice(L->E->device);
       {
-        AllocScope alloc_scope(L->E->st);
+        AllocScope alloc_scope(L->E);
         dfree(L->out);
       }
       lv_engine_destroy(L->E);
@@ -2298,7 +2323,7 @@ lv_status lv_autotune(lv_engine* E, uint32_t reps, lv_tuning* out) {
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   if (E->batch) return fail(LV_ERR_STATE, "a batched run is in progress");
-  AllocScope alloc_scope(E->st);
+  AllocScope alloc_scope(E);
   cudaSetDevice(E->device);
   if (!reps) reps = 5;
   if (!E->level_ready) LVTRY(prepare_level(E));
@@ -2369,7 +2394,7 @@ lv_status lv_reset_kernel_stats(lv_engine* E) {
 }
 
 lv_status lv_get_buckets(lv_engine* E, uint8_t* bucket_of, size_t n) {
-  AllocScope alloc_scope(E ? E->st : nullptr);
+  AllocScope alloc_scope(E);
   if (!E || (!bucket_of && n)) return fail(LV_ERR_ARG, "NULL argument");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   if (n != E->n) return fail(LV_ERR_ARG, "buffer length must equal the level's vertex count");

@@ -155,3 +155,22 @@ def test_serve_lanes(background):
         want = 0 if e <= 2_000 else (1 if e <= 20_000 else 2)
         assert served[t].lane == want
     assert len({served[t].lane for t in tickets}) == 3
+
+
+def test_serve_lane_group():
+    """Two unbounded lanes form a group: requests too large for lane 0 go
+    to whichever of lanes 1 and 2 holds fewer entries, so both take work;
+    results still equal the lone runs."""
+    graphs = _mix()
+    alone = _alone(graphs, 1e-6)
+    entries = [g.csr()[2].size for g in graphs]
+    unbounded = 2**64 - 1
+    with lvb200.Server(1e-6, 512 << 20, lanes=3, background=True,
+                       lane_max_entries=[2_000, unbounded, unbounded],
+                       lane_share=[0.2, 0.4, 0.4]) as s:
+        tickets = [s.submit(g) for g in graphs]
+        served = s.drain()
+    _check(alone, served, tickets)
+    big = [served[t].lane for t, e in zip(tickets, entries) if e > 2_000]
+    assert all(served[t].lane == 0 for t, e in zip(tickets, entries) if e <= 2_000)
+    assert set(big) == {1, 2}
