@@ -30,10 +30,11 @@
 //     32 < deg <= 319: one warp per vertex, open-addressing table in shared
 //     memory.  319 < deg <= 2048: one block per vertex, 4096-slot shared
 //     table.  deg > 2048: one block per (vertex, hash partition of its
-//     neighbour communities), 8192-slot shared table, the partitions' best
+//     neighbour communities), 4096-slot shared table, the partitions' best
 //     candidates merged with one 64-bit atomicMax each -- no global hash
-//     table, whatever the degree.  Shared tables are self-cleaning: taken
-//     slots are listed, and only they are scanned and cleared.
+//     table, whatever the degree.  Shared tables are self-cleaning: a row
+//     uses the first slots of its table (a power of two >= 1.5 x its
+//     degree), and the candidate scan clears the slots it reads.
 //   * Community totals are updated incrementally by the moved vertices
 //     only (FP64 atomics), instead of a full recount after every bucket.
 #include "lv_internal.h"
@@ -46,10 +47,21 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+// Blocks per SM each pass kernel is compiled for (__launch_bounds__) and
+// launched with: the grid-stride kernels run as exactly one resident wave
+// (a grid above residency would run a partial second wave of blocks).
+constexpr int kSmallPerSM = 8;     // 32 registers
+constexpr int kWarp128PerSM = 5;   // 48 registers, 12 KB tables
+constexpr int kWarp512PerSM = 4;   // 64 registers, 48 KB tables
+constexpr int kBlockPerSM = 4;     // 64 registers, 48 KB table
+constexpr int kSplitPerSM = 4;
+constexpr int kMergePerSM = 3;
+constexpr int kSweepPerSM = 8;     // apply
+constexpr int kModPerSM = 6;       // modularity sweep, 40 registers
 static_assert(class_per_unit(1) * 4 == kThreads && class_per_unit(5) == kWarps,
               "dispatch units assume 256-thread blocks");
-// shared tables: FP64 values + u32 keys + u16 list of taken slots
-constexpr int kSlotBytes = 14;
+// shared tables: FP64 values + u32 keys
+constexpr int kSlotBytes = 12;
 constexpr int kHubPartSmem = kHubPartSlots * kSlotBytes;
 constexpr int kBlockTabSmem = kHubSmemSlots * kSlotBytes;
 
@@ -189,25 +201,20 @@ __device__ __forceinline__ uint32_t table_size_for(uint32_t d, uint32_t tmax) {
   return t < tmax ? t : tmax;
 }
 
-// Self-cleaning shared tables: a slot taken for the first time is appended
-// to `fresh`, so the candidates are read from the list (O(distinct), not
-// O(table)) and only listed slots are cleared afterwards.  The table is
-// cleared in full once, when a warp or block starts.
-__device__ __forceinline__ uint32_t table_insert_fresh(uint32_t* keys, uint32_t mask,
-                                                       uint32_t key, uint16_t* fresh,
-                                                       uint32_t* n_fresh,
-                                                       LevelScalars* sc) {
+// Slot of key in a shared table of mask + 1 slots (inserted if absent).
+// The table is cleared in full once, when a warp or block starts; after a
+// row, the candidate scan (scan_table_and_clear) empties the slots it used.
+// No shared counter: keeping a list of taken slots cost one same-address
+// atomic per distinct key, which serialised whole warps.
+__device__ __forceinline__ uint32_t table_insert(uint32_t* keys, uint32_t mask,
+                                                 uint32_t key, LevelScalars* sc) {
   uint32_t h = hash_slot(key, mask);
   for (uint32_t it = 0; it <= mask; it++) {
     uint32_t cur = keys[h];
     if (cur == key) return h;
     if (cur == kEmptyKey) {
       uint32_t prev = atomicCAS(&keys[h], kEmptyKey, key);
-      if (prev == kEmptyKey) {
-        fresh[atomicAdd(n_fresh, 1u)] = (uint16_t)h;
-        return h;
-      }
-      if (prev == key) return h;
+      if (prev == kEmptyKey || prev == key) return h;
     }
     h = (h + 1) & mask;
   }
@@ -229,7 +236,7 @@ __device__ __forceinline__ unsigned long long candidate_loaded(const GainCtx& g,
 
 // deg <= G: G lanes per vertex, one edge per lane.
 template <int G, int RULE>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, kSmallPerSM)
     move_small_kernel(const PassDesc* __restrict__ D, int cls) {
   const LevelView L = D->L;
   const uint32_t s0 = D->A.P.cls_start[cls];
@@ -299,22 +306,23 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// Best candidate among the listed slots (nthr threads from tid, four per
-// thread at a time so the gathers overlap); each thread then clears the
-// slots it read, leaving the table clean.
-__device__ __forceinline__ unsigned long long scan_fresh_and_clear(
+// Best candidate among the taken slots of the first tv slots (nthr
+// threads from tid, four slots per thread at a time so the gathers
+// overlap); each thread empties the taken slots it read, leaving the table
+// clean.
+__device__ __forceinline__ unsigned long long scan_table_and_clear(
     const LevelView& L, const GainCtx& g, uint32_t* keys, double* vals,
-    const uint16_t* fresh, uint32_t cnt, uint32_t tid, uint32_t nthr) {
+    uint32_t tv, uint32_t tid, uint32_t nthr) {
   unsigned long long best = 0ull;
-  for (uint32_t i0 = tid; i0 < cnt; i0 += 4 * nthr) {
-    uint32_t sl[4], c[4], szc[4];
+#pragma unroll 1
+  for (uint32_t i0 = tid; i0 < tv; i0 += 4 * nthr) {
+    uint32_t c[4], szc[4];
     double ec[4], ac[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const uint32_t i = i0 + q * nthr;
-      sl[q] = i < cnt ? fresh[i] : 0u;
-      c[q] = i < cnt ? keys[sl[q]] : kEmptyKey;
-      ec[q] = i < cnt ? vals[sl[q]] : 0.0;
+      c[q] = i < tv ? keys[i] : kEmptyKey;
+      ec[q] = c[q] != kEmptyKey ? vals[i] : 0.0;
     }
 #pragma unroll
     for (int q = 0; q < 4; q++) {
@@ -327,8 +335,9 @@ __device__ __forceinline__ unsigned long long scan_fresh_and_clear(
     for (int q = 0; q < 4; q++) {
       if (c[q] != kEmptyKey) {
         best = umax64(best, candidate_loaded(g, c[q], ec[q], szc[q], ac[q]));
-        keys[sl[q]] = kEmptyKey;
-        vals[sl[q]] = 0.0;
+        const uint32_t i = i0 + q * nthr;
+        keys[i] = kEmptyKey;
+        vals[i] = 0.0;
       }
     }
   }
@@ -339,7 +348,7 @@ __device__ __forceinline__ unsigned long long scan_fresh_and_clear(
 // row's loads (at most MAXW waves of 32) are issued before any insertion,
 // so a vertex costs one memory latency chain instead of one per wave.
 template <int T, int MAXW, int RULE>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, T == 128 ? kWarp128PerSM : kWarp512PerSM)
     move_warp_kernel(const PassDesc* __restrict__ D, int cls) {
   const LevelView L = D->L;
   const uint32_t s0 = D->A.P.cls_start[cls];
@@ -347,20 +356,11 @@ __global__ void __launch_bounds__(kThreads)
   uint32_t* __restrict__ prop = D->prop + s0;
   const uint32_t count = D->act_cnt ? D->act_cnt[cls] : D->A.P.cls_start[cls + 1] - s0;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ uint32_t n_fresh_sm[kWarps];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   double* vals = reinterpret_cast<double*>(smem_raw) + wib * T;
   uint32_t* keys =
       reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T * kWarps) + wib * T;
-  uint16_t* fresh =
-      reinterpret_cast<uint16_t*>(smem_raw + 12 * T * kWarps) + wib * T;
-  uint32_t* n_fresh = &n_fresh_sm[wib];
-  for (uint32_t i = lane; i < T; i += 32) {
-    keys[i] = kEmptyKey;
-    vals[i] = 0.0;
-  }
-  if (lane == 0) *n_fresh = 0u;
-  __syncwarp();
+  uint32_t clean = 0;  // leading table slots known to be empty
   for (uint32_t vidx = blockIdx.x * kWarps + wib; vidx < count;
        vidx += gridDim.x * kWarps) {
     const uint32_t v = verts[vidx];
@@ -372,6 +372,14 @@ __global__ void __launch_bounds__(kThreads)
       continue;
     }
     const uint32_t tv = table_size_for(d, T);
+    if (tv > clean) {  // warp-uniform; the scan empties what a row used
+      for (uint32_t i = clean + lane; i < tv; i += 32) {
+        keys[i] = kEmptyKey;
+        vals[i] = 0.0;
+      }
+      clean = tv;
+      __syncwarp();
+    }
     const GainCtx g = make_ctx(L, v, cv);
     uint32_t cu[MAXW];
     float wt[MAXW];
@@ -413,24 +421,20 @@ __global__ void __launch_bounds__(kThreads)
       const int leader = __ffs(peers) - 1;
       uint32_t slot = 0;
       if (ins && lane == leader)
-        slot = table_insert_fresh(keys, tv - 1, cu[k], fresh, n_fresh, L.sc);
+        slot = table_insert(keys, tv - 1, cu[k], L.sc);
       slot = __shfl_sync(kFull, slot, leader);
       if (ins) atomicAdd(&vals[slot], (double)wt[k]);
     }
     hot = group_sum<32>(hot);
     if (__any_sync(kFull, hot_seen) && lane == 0) {
-      const uint32_t slot = table_insert_fresh(keys, tv - 1, cv, fresh, n_fresh, L.sc);
+      const uint32_t slot = table_insert(keys, tv - 1, cv, L.sc);
       vals[slot] += hot;
     }
     __syncwarp();
-    unsigned long long best =
-        scan_fresh_and_clear(L, g, keys, vals, fresh, *n_fresh, lane, 32);
+    unsigned long long best = scan_table_and_clear(L, g, keys, vals, tv, lane, 32);
     best = group_max<32>(best);
     if (RULE == LV_RULE_CUDA_I) own = group_sum<32>(own);
-    if (lane == 0) {
-      prop[vidx] = decide<RULE>(best, own, g);
-      *n_fresh = 0u;
-    }
+    if (lane == 0) prop[vidx] = decide<RULE>(best, own, g);
     __syncwarp();
   }
 }
@@ -471,7 +475,6 @@ __device__ __forceinline__ void insert_block_range(const LevelView& L, uint64_t 
                                                    uint32_t v, uint32_t cv,
                                                    uint32_t* keys, double* vals,
                                                    uint32_t mask, double& own,
-                                                   uint16_t* fresh, uint32_t* n_fresh,
                                                    double& hot, bool& hot_seen) {
   const int lane = threadIdx.x & 31;
   uint32_t cu[MAXW];
@@ -511,7 +514,7 @@ __device__ __forceinline__ void insert_block_range(const LevelView& L, uint64_t 
     const int leader = __ffs(peers) - 1;
     uint32_t slot = 0;
     if (ins && lane == leader)
-      slot = table_insert_fresh(keys, mask, cu[k], fresh, n_fresh, L.sc);
+      slot = table_insert(keys, mask, cu[k], L.sc);
     slot = __shfl_sync(kFull, slot, leader);
     if (ins) atomicAdd(&vals[slot], (double)wt[k]);
   }
@@ -519,7 +522,7 @@ __device__ __forceinline__ void insert_block_range(const LevelView& L, uint64_t 
 
 // 319 < deg <= 2048: one block per vertex, shared 4096-slot table.
 template <int RULE>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, kBlockPerSM)
     move_block_kernel(const PassDesc* __restrict__ D, int cls) {
   const LevelView L = D->L;
   const uint32_t s0 = D->A.P.cls_start[cls];
@@ -531,16 +534,9 @@ __global__ void __launch_bounds__(kThreads)
   constexpr int MAXW = (int)(kHubSmemMaxDeg / kThreads);
   double* vals = reinterpret_cast<double*>(smem_raw);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T);
-  uint16_t* fresh = reinterpret_cast<uint16_t*>(smem_raw + 12 * T);
   __shared__ unsigned long long red_best[kWarps];
   __shared__ double red_own[kWarps];
-  __shared__ uint32_t n_fresh;
-  for (uint32_t i = threadIdx.x; i < T; i += kThreads) {
-    keys[i] = kEmptyKey;
-    vals[i] = 0.0;
-  }
-  if (threadIdx.x == 0) n_fresh = 0u;
-  __syncthreads();
+  uint32_t clean = 0;  // leading table slots known to be empty
   for (uint32_t vidx = blockIdx.x; vidx < count; vidx += gridDim.x) {
     const uint32_t v = verts[vidx];
     const uint64_t s = L.off[v];
@@ -551,27 +547,32 @@ __global__ void __launch_bounds__(kThreads)
       continue;
     }
     const uint32_t tv = table_size_for(d, T);
+    if (tv > clean) {  // block-uniform; the scan empties what a row used
+      for (uint32_t i = clean + threadIdx.x; i < tv; i += kThreads) {
+        keys[i] = kEmptyKey;
+        vals[i] = 0.0;
+      }
+      clean = tv;
+      __syncthreads();
+    }
     const GainCtx g = make_ctx(L, v, cv);
     double own = 0.0;
     double hot = 0.0;
     bool hot_seen = false;
-    insert_block_range<MAXW, RULE>(L, s, 0, d, v, cv, keys, vals, tv - 1, own,
-                                   fresh, &n_fresh, hot, hot_seen);
+    insert_block_range<MAXW, RULE>(L, s, 0, d, v, cv, keys, vals, tv - 1, own, hot,
+                                   hot_seen);
     const int any_hot = __syncthreads_or(hot_seen);
     hot = block_sum(hot, red_own);  // thread 0
     if (threadIdx.x == 0 && any_hot) {
-      const uint32_t slot = table_insert_fresh(keys, tv - 1, cv, fresh, &n_fresh, L.sc);
+      const uint32_t slot = table_insert(keys, tv - 1, cv, L.sc);
       vals[slot] += hot;
     }
     __syncthreads();
     unsigned long long best =
-        scan_fresh_and_clear(L, g, keys, vals, fresh, n_fresh, threadIdx.x, kThreads);
+        scan_table_and_clear(L, g, keys, vals, tv, threadIdx.x, kThreads);
     best = block_max(best, red_best);
     if (RULE == LV_RULE_CUDA_I) own = block_sum(own, red_own);
-    if (threadIdx.x == 0) {
-      prop[vidx] = decide<RULE>(best, own, g);
-      n_fresh = 0u;  // every thread read it before block_max's barriers
-    }
+    if (threadIdx.x == 0) prop[vidx] = decide<RULE>(best, own, g);
     __syncthreads();
   }
 }
@@ -627,7 +628,7 @@ __device__ __forceinline__ uint32_t block_scan_inplace(uint32_t* a, uint32_t n,
 }
 
 template <int RULE>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, kSplitPerSM)
     hub_split_kernel(const PassDesc* __restrict__ D) {
   const LevelView L = D->L;
   const uint32_t* __restrict__ hubs = D->A.order + D->A.P.cls_start[8];
@@ -716,7 +717,7 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 template <int RULE>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, kMergePerSM)
     hub_merge_kernel(const PassDesc* __restrict__ D) {
   const LevelView L = D->L;
   const uint32_t* __restrict__ hubs = D->A.order + D->A.P.cls_start[8];
@@ -726,16 +727,13 @@ __global__ void __launch_bounds__(kThreads)
   constexpr int T = kHubPartSlots;
   double* vals = reinterpret_cast<double*>(smem_raw);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T);
-  uint16_t* fresh = reinterpret_cast<uint16_t*>(smem_raw + 12 * T);
   __shared__ unsigned long long red_best[kWarps];
-  __shared__ uint32_t n_fresh;
   __shared__ uint32_t seg_a[kThreads], seg_pre[kThreads], wsum[kWarps];
   const int lane = threadIdx.x & 31;
   for (uint32_t i = threadIdx.x; i < T; i += kThreads) {
     keys[i] = kEmptyKey;
     vals[i] = 0.0;
   }
-  if (threadIdx.x == 0) n_fresh = 0u;
   __syncthreads();
   for (uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
     const uint32_t hi = H.blk_vertex[u], part = H.blk_chunk[u];
@@ -780,20 +778,16 @@ __global__ void __launch_bounds__(kThreads)
         const int leader = __ffs(peers) - 1;
         uint32_t slot = 0;
         if (has && lane == leader)
-          slot = table_insert_fresh(keys, T - 1, c, fresh, &n_fresh, L.sc);
+          slot = table_insert(keys, T - 1, c, L.sc);
         slot = __shfl_sync(kFull, slot, leader);
         if (has) atomicAdd(&vals[slot], (double)w);
       }
       __syncthreads();  // seg_a / seg_pre are refilled
     }
     const GainCtx g = make_ctx(L, v, L.comm[v]);
-    unsigned long long best =
-        scan_fresh_and_clear(L, g, keys, vals, fresh, n_fresh, threadIdx.x, kThreads);
+    unsigned long long best = scan_table_and_clear(L, g, keys, vals, T, threadIdx.x, kThreads);
     best = block_max(best, red_best);
-    if (threadIdx.x == 0) {
-      if (best) atomicMax(&H.best[hi], best);
-      n_fresh = 0u;
-    }
+    if (threadIdx.x == 0 && best) atomicMax(&H.best[hi], best);
     __syncthreads();
   }
 }
@@ -821,7 +815,7 @@ __global__ void hub_decide_kernel(const PassDesc* __restrict__ D) {
 }
 
 // Applies a bucket's proposals (assignCommunity + incremental totals).
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, kSweepPerSM)
     apply_kernel(const PassDesc* __restrict__ D, int lo_cls, int hi_cls) {
   // classes lo..hi are adjacent in the lists (bucket 7 without compaction:
   // classes 7 and 8); with compaction a class's active prefix
@@ -1232,7 +1226,7 @@ __global__ void __launch_bounds__(kThreads)
 
 // The modularity sweep of a pass (level and stop-rule limits from the
 // descriptor).
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, kModPerSM)
     modularity_pass_kernel(const PassDesc* __restrict__ D, PassControl ctl) {
   ctl.min_gain = D->min_gain;
   ctl.max_passes = D->max_passes;
@@ -1489,16 +1483,16 @@ cudaError_t launch_pass_control_init(const PassDesc* D, cudaStream_t st) {
 cudaError_t launch_modularity_pass(const PassDesc* D, const PassControl* ctl, cudaStream_t st) {
   PassControl c{};
   if (ctl) c = *ctl;
-  (count_launches(1), modularity_pass_kernel<<<sm_count() * 8, kThreads, 0, st>>>(D, c));
+  (count_launches(1), modularity_pass_kernel<<<sm_count() * kModPerSM, kThreads, 0, st>>>(D, c));
   return cudaGetLastError();
 }
 
-unsigned pass_dispatch_grid() { return sm_count() * 8; }
+unsigned pass_dispatch_grid() { return sm_count() * kModPerSM; }
 
 // One launch of a move kernel variant over class `cls`.
 template <int RULE>
 static void launch_variant(int kv, const PassDesc* D, int cls, cudaStream_t st) {
-  const unsigned cap = sm_count() * 8;
+  const unsigned cap = sm_count() * kSmallPerSM;
   switch (kv) {
     case KV_SMALL4:
       (count_launches(1), move_small_kernel<4, RULE><<<cap, kThreads, 0, st>>>(D, cls));
@@ -1514,17 +1508,19 @@ static void launch_variant(int kv, const PassDesc* D, int cls, cudaStream_t st) 
       break;
     case KV_WARP128: {
       constexpr int T = 128;
-      (count_launches(1), move_warp_kernel<T, 3, RULE><<<cap, kThreads, kWarps * T * kSlotBytes, st>>>(D, cls));
+      (count_launches(1), move_warp_kernel<T, 3, RULE><<<sm_count() * kWarp128PerSM, kThreads,
+                                                       kWarps * T * kSlotBytes, st>>>(D, cls));
       break;
     }
     case KV_WARP512: {
       constexpr int T = 512;
-      (count_launches(1), move_warp_kernel<T, 10, RULE><<<sm_count() * 4, kThreads,
+      (count_launches(1), move_warp_kernel<T, 10, RULE><<<sm_count() * kWarp512PerSM, kThreads,
                                                         kWarps * T * kSlotBytes, st>>>(D, cls));
       break;
     }
     default:  // KV_BLOCK: shared table, one block per vertex
-      (count_launches(1), move_block_kernel<RULE><<<sm_count() * 4, kThreads, kBlockTabSmem, st>>>(D, cls));
+      (count_launches(1), move_block_kernel<RULE><<<sm_count() * kBlockPerSM, kThreads,
+                                                   kBlockTabSmem, st>>>(D, cls));
       break;
   }
 }
@@ -1540,8 +1536,9 @@ static cudaError_t move_bucket_impl(const PassDesc* D, int bucket, const uint8_t
   }
   if (bucket != 8) return cudaErrorInvalidValue;
   // class 8 of bucket 7: split chunks, merge (hub, partition), decide
-  (count_launches(1), hub_split_kernel<RULE><<<sm_count() * 6, kThreads, 0, st>>>(D));
-  (count_launches(1), hub_merge_kernel<RULE><<<sm_count() * 3, kThreads, kHubPartSmem, st>>>(D));
+  (count_launches(1), hub_split_kernel<RULE><<<sm_count() * kSplitPerSM, kThreads, 0, st>>>(D));
+  (count_launches(1), hub_merge_kernel<RULE><<<sm_count() * kMergePerSM, kThreads, kHubPartSmem,
+                                               st>>>(D));
   (count_launches(1), hub_decide_kernel<RULE><<<sm_count() * 2, 128, 0, st>>>(D));
   return cudaGetLastError();
 }
@@ -1553,7 +1550,7 @@ cudaError_t launch_move_bucket(const PassDesc* D, int bucket, int rule, const ui
 }
 
 cudaError_t launch_apply_bucket(const PassDesc* D, int bucket, bool compacted, cudaStream_t st) {
-  const unsigned cap = sm_count() * 8;
+  const unsigned cap = sm_count() * kSweepPerSM;
   if (bucket == 7 && !compacted) {  // classes 7 and 8 are adjacent
     (count_launches(1), apply_kernel<<<cap, kThreads, 0, st>>>(D, 7, 8));
   } else if (bucket == 7) {  // class 7's active prefix, then the hubs
