@@ -254,14 +254,8 @@ __global__ void __launch_bounds__(kThreads)
             ins = true;
           }
         }
-        const unsigned long long mk =
-            ins ? (unsigned long long)key : (0x100000000ull | (unsigned)lane);
-        const unsigned peers = __match_any_sync(kFull, mk);
-        const int leader = __ffs(peers) - 1;
-        uint32_t slot = 0;
-        if (ins && lane == leader) slot = table_insert(keys, mask, key, C.err);
-        slot = __shfl_sync(kFull, slot, leader);
-        if (ins) atomicAdd(&vals[slot], (double)wt);
+        // every lane inserts its own entry: equal keys meet in the CAS
+        if (ins) atomicAdd(&vals[table_insert(keys, mask, key, C.err)], (double)wt);
       }
     }
     hot_acc = warp_sum(hot_acc);
@@ -326,7 +320,6 @@ __device__ __forceinline__ void insert_range(const Ctx& C, uint32_t m0,
                                              uint64_t* s_start,
                                              uint64_t* s_off, uint32_t hot,
                                              double& hot_acc, bool& hot_seen) {
-  const int lane = threadIdx.x & 31;
   // first member whose range contains lo: largest k with start_k <= lo
   __shared__ uint32_t s_k;
   if (threadIdx.x == 0) {
@@ -375,14 +368,7 @@ __device__ __forceinline__ void insert_range(const Ctx& C, uint32_t m0,
           ins = true;
         }
       }
-      const unsigned long long mk =
-          ins ? (unsigned long long)key : (0x100000000ull | (unsigned)lane);
-      const unsigned peers = __match_any_sync(kFull, mk);
-      const int leader = __ffs(peers) - 1;
-      uint32_t slot = 0;
-      if (ins && lane == leader) slot = table_insert(keys, mask, key, C.err);
-      slot = __shfl_sync(kFull, slot, leader);
-      if (ins) atomicAdd(&vals[slot], (double)wt);
+      if (ins) atomicAdd(&vals[table_insert(keys, mask, key, C.err)], (double)wt);
     }
     pos = chunk_end;
     k0 += kThreads;

@@ -25,8 +25,10 @@
 //   * A candidate is evaluated once per distinct neighbour community, and
 //     the argmax is a max over packed (gain, ~community) 64-bit keys, so
 //     the lowest community id wins ties deterministically.
-//   * deg <= 32: G lanes per vertex (G = 4, 8, 16, 32), one edge per lane,
-//     __match_any_sync groups equal communities, no hash table at all.
+//   * deg <= 32: G lanes per vertex (G = 4, 8, 16, 32), one edge per lane;
+//     equal communities in a group are found with G - 1 shuffles, no hash
+//     table at all.  (__match_any_sync costs about one step per distinct
+//     value in the warp, and at level 0 all 32 values are distinct.)
 //     32 < deg <= 319: one warp per vertex, open-addressing table in shared
 //     memory.  319 < deg <= 2048: one block per vertex, 4096-slot shared
 //     table.  deg > 2048: one block per (vertex, hash partition of its
@@ -285,11 +287,17 @@ __global__ void __launch_bounds__(kThreads, kSmallPerSM)
     const unsigned gmask = (G == 32) ? kFull : (((1u << G) - 1u) << (lane & ~(G - 1)));
     const unsigned hmask = __ballot_sync(kFull, is_hot) & gmask;
     const int hot_leader = hmask ? __ffs(hmask) - 1 : -1;
-    const unsigned long long mk =
-        ins ? (((unsigned long long)(lane / G) << 32) | cu)
-            : (0xFFFFFFFF00000000ull | (unsigned)lane);
-    const unsigned peers = __match_any_sync(kFull, mk);
-    const int leader = __ffs(peers) - 1;
+    // leader of an entry: the group's lowest lane holding the same community
+    const uint32_t gbase = lane & ~(G - 1);
+    const uint32_t mykey = ins ? cu : kEmptyKey;
+    uint32_t first = gl;
+#pragma unroll
+    for (int o = 1; o < G; o++) {
+      const uint32_t src = (gl + o) & (G - 1);
+      const uint32_t ok = __shfl_sync(kFull, mykey, gbase | src);
+      if (ins && ok == cu && src < first) first = src;
+    }
+    const int leader = (int)(gbase | first);
     sums[wib][lane] = (lane == hot_leader) ? hv : 0.0;
     __syncwarp();
     if (ins) atomicAdd(&sums[wib][leader], (double)wt);
@@ -415,15 +423,8 @@ __global__ void __launch_bounds__(kThreads, T == 128 ? kWarp128PerSM : kWarp512P
         hot_seen = true;
         if (RULE == LV_RULE_CUDA_I && !(self_mask >> k & 1u)) own += (double)wt[k];
       }
-      const unsigned long long mk =
-          ins ? (unsigned long long)cu[k] : (0x100000000ull | (unsigned)lane);
-      const unsigned peers = __match_any_sync(kFull, mk);
-      const int leader = __ffs(peers) - 1;
-      uint32_t slot = 0;
-      if (ins && lane == leader)
-        slot = table_insert(keys, tv - 1, cu[k], L.sc);
-      slot = __shfl_sync(kFull, slot, leader);
-      if (ins) atomicAdd(&vals[slot], (double)wt[k]);
+      // every lane inserts its own entry: equal keys meet in the CAS
+      if (ins) atomicAdd(&vals[table_insert(keys, tv - 1, cu[k], L.sc)], (double)wt[k]);
     }
     hot = group_sum<32>(hot);
     if (__any_sync(kFull, hot_seen) && lane == 0) {
@@ -476,7 +477,6 @@ __device__ __forceinline__ void insert_block_range(const LevelView& L, uint64_t 
                                                    uint32_t* keys, double* vals,
                                                    uint32_t mask, double& own,
                                                    double& hot, bool& hot_seen) {
-  const int lane = threadIdx.x & 31;
   uint32_t cu[MAXW];
   float wt[MAXW];
   unsigned self_mask = 0u;
@@ -508,15 +508,7 @@ __device__ __forceinline__ void insert_block_range(const LevelView& L, uint64_t 
       hot_seen = true;
       if (RULE == LV_RULE_CUDA_I && !(self_mask >> k & 1u)) own += (double)wt[k];
     }
-    const unsigned long long mk =
-        ins ? (unsigned long long)cu[k] : (0x100000000ull | (unsigned)lane);
-    const unsigned peers = __match_any_sync(kFull, mk);
-    const int leader = __ffs(peers) - 1;
-    uint32_t slot = 0;
-    if (ins && lane == leader)
-      slot = table_insert(keys, mask, cu[k], L.sc);
-    slot = __shfl_sync(kFull, slot, leader);
-    if (ins) atomicAdd(&vals[slot], (double)wt[k]);
+    if (ins) atomicAdd(&vals[table_insert(keys, mask, cu[k], L.sc)], (double)wt[k]);
   }
 }
 
@@ -729,7 +721,6 @@ __global__ void __launch_bounds__(kThreads, kMergePerSM)
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T);
   __shared__ unsigned long long red_best[kWarps];
   __shared__ uint32_t seg_a[kThreads], seg_pre[kThreads], wsum[kWarps];
-  const int lane = threadIdx.x & 31;
   for (uint32_t i = threadIdx.x; i < T; i += kThreads) {
     keys[i] = kEmptyKey;
     vals[i] = 0.0;
@@ -772,15 +763,7 @@ __global__ void __launch_bounds__(kThreads, kMergePerSM)
           c = H.stage_c[pos];
           w = H.stage_w[pos];
         }
-        const unsigned long long mk =
-            has ? (unsigned long long)c : (0x100000000ull | (unsigned)lane);
-        const unsigned peers = __match_any_sync(kFull, mk);
-        const int leader = __ffs(peers) - 1;
-        uint32_t slot = 0;
-        if (has && lane == leader)
-          slot = table_insert(keys, T - 1, c, L.sc);
-        slot = __shfl_sync(kFull, slot, leader);
-        if (has) atomicAdd(&vals[slot], (double)w);
+        if (has) atomicAdd(&vals[table_insert(keys, T - 1, c, L.sc)], (double)w);
       }
       __syncthreads();  // seg_a / seg_pre are refilled
     }
