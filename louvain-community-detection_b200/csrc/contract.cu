@@ -48,8 +48,11 @@ static_assert(kMergeMidMax * 3 / 2 + 1 <= kMidSlots &&
                   kMergeBlockMax * 3 / 2 + 1 <= kBlockSlots,
               "tables keep load factor <= 2/3");
 
+// Slot from the top bits of a multiplicative (Fibonacci) hash: the low bits
+// of key * odd depend only on the key's low bits, and vertex ids such as
+// R-MAT's share low-bit patterns, which piled them into a few probe chains.
 __device__ __forceinline__ uint32_t hash_slot(uint32_t key, uint32_t mask) {
-  return (key * 2654435761u) & mask;
+  return __umulhi(key * 2654435761u, mask + 1u);  // mask + 1: a power of two
 }
 
 // Table slots used for a row of d entries: a power of two >= 1.5 d (load

@@ -188,11 +188,14 @@ __device__ __forceinline__ void warp_graph_add(GraphState* gs, GraphField field,
     atomicAdd(&(gs[key].*field), val);
 }
 
-// Open addressing with linear probing; multiplicative hash.  Probe counts
-// are bounded by the table size; a full table (impossible while a table
-// holds more slots than the row has entries) sets the error flag.
+// Open addressing with linear probing.  Probe counts are bounded by the
+// table size; a full table (impossible while a table holds more slots than
+// the row has entries) sets the error flag.
+// Slot from the top bits of a multiplicative (Fibonacci) hash: the low bits
+// of key * odd depend only on the key's low bits, and vertex ids such as
+// R-MAT's share low-bit patterns, which piled them into a few probe chains.
 __device__ __forceinline__ uint32_t hash_slot(uint32_t key, uint32_t mask) {
-  return (key * 2654435761u) & mask;
+  return __umulhi(key * 2654435761u, mask + 1u);  // mask + 1: a power of two
 }
 // Table slots used for a row of d entries: a power of two >= 1.5 d (load
 // factor <= 2/3), at most tmax (the class's shared-memory table).
