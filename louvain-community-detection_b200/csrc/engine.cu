@@ -290,8 +290,14 @@ struct lv_engine {
   uint32_t* cg = nullptr;       // [kMoveClasses * (graph cap + 1)]
   uint32_t* cg_new = nullptr;
 
-  // all passes of the current level as one graph (WHILE node)
-  cudaGraphExec_t level_exec = nullptr;
+  // all passes of a level as one graph (WHILE node), one per key (form,
+  // rule, tuning, which kernel classes are non-empty), most recent last
+  struct LevelExec {
+    uint64_t key;
+    cudaGraphExec_t exec;
+    unsigned long long launches;  // kernels per pass
+  };
+  std::vector<LevelExec> level_execs;
   // one pass of the current level captured as a CUDA graph (timing mode)
   cudaGraphExec_t pass_exec = nullptr;
   bool capturing = false;
@@ -301,10 +307,9 @@ struct lv_engine {
   unsigned long long* d_class_deg = nullptr;
   uint64_t class_deg[kClasses] = {};
   // move kernel variant of every bucket (1..7): defaults or lv_autotune's pick
-  // the pass descriptor (device) and the level graph built on it, kept
-  // across levels and runs while the key (form, rule, tuning) holds
+  // the pass descriptor (device); the level graphs built on it are kept
+  // across levels and runs
   PassDesc* d_desc = nullptr;
-  uint64_t level_key = ~0ull;
   uint8_t tune[8] = {kDefaultVariant[0], kDefaultVariant[1], kDefaultVariant[2],
                      kDefaultVariant[3], kDefaultVariant[4], kDefaultVariant[5],
                      kDefaultVariant[6], kDefaultVariant[7]};
@@ -785,18 +790,28 @@ lv_status upload_desc(lv_engine* E, float min_gain) {
   return LV_OK;
 }
 
+// Kernel class c (1..8) has vertices on this level.  A class empty at a
+// level's start stays empty through its passes (the batched form's
+// per-pass lists only shrink), so its kernels are left out of the pass.
+bool class_nonempty(const lv_engine* E, int c) {
+  return c == 8 ? E->plan.hub_count > 0 : E->plan.cls_start[c + 1] > E->plan.cls_start[c];
+}
+
 // What a captured pass depends on besides the descriptor: the form
-// (batched passes compact their lists), the rule and the tuning.
+// (batched passes compact their lists), the rule, the tuning and which
+// classes are non-empty.
 uint64_t level_key(const lv_engine* E) {
   uint64_t k = (E->batch ? 1u : 0u) | ((uint64_t)(E->cfg.rule == LV_RULE_CUDA) << 1);
   for (int b = 1; b <= kBuckets; b++) k |= (uint64_t)E->tune[b] << (4 * b);
+  for (int c = 1; c <= 8; c++) k |= (uint64_t)class_nonempty(E, c) << (39 + c);
   return k;
 }
 
+constexpr size_t kLevelExecCache = 8;
+
 void drop_level_exec(lv_engine* E) {
-  if (E->level_exec) cudaGraphExecDestroy(E->level_exec);
-  E->level_exec = nullptr;
-  E->level_key = ~0ull;
+  for (const lv_engine::LevelExec& x : E->level_execs) cudaGraphExecDestroy(x.exec);
+  E->level_execs.clear();
 }
 
 // Every pass of a level in one graph launch: [control init] -> WHILE
@@ -807,8 +822,18 @@ void drop_level_exec(lv_engine* E) {
 // graph is captured once and replayed on every later level and run.
 lv_status run_level_graph(lv_engine* E, float min_gain) {
   LVTRY(upload_desc(E, min_gain));
-  if (E->level_exec && E->level_key != level_key(E)) drop_level_exec(E);
-  if (!E->level_exec) {
+  const uint64_t key = level_key(E);
+  cudaGraphExec_t exec = nullptr;
+  for (size_t i = 0; i < E->level_execs.size(); i++) {
+    if (E->level_execs[i].key != key) continue;
+    lv_engine::LevelExec hit = E->level_execs[i];  // most recently used goes last
+    E->level_execs.erase(E->level_execs.begin() + (long)i);
+    E->level_execs.push_back(hit);
+    exec = hit.exec;
+    E->level_launches = hit.launches;
+    break;
+  }
+  if (!exec) {
     cudaGraph_t g = nullptr;
     CU(cudaGraphCreate(&g, 0));
     struct GraphGuard {
@@ -856,11 +881,15 @@ lv_status run_level_graph(lv_engine* E, float min_gain) {
     E->pending.clear();
     if (s != LV_OK) return s;
     CU(ce);
-    CU(cudaGraphInstantiate(&E->level_exec, g, 0));
-    E->level_key = level_key(E);
+    CU(cudaGraphInstantiate(&exec, g, 0));
+    if (E->level_execs.size() >= kLevelExecCache) {
+      cudaGraphExecDestroy(E->level_execs.front().exec);
+      E->level_execs.erase(E->level_execs.begin());
+    }
+    E->level_execs.push_back({key, exec, E->level_launches});
     g_trace.mark("capture+instantiate", (uint32_t)E->levels.size(), E->n);
   }
-  CU(cudaGraphLaunch(E->level_exec, E->st));
+  CU(cudaGraphLaunch(exec, E->st));
   CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost,
                      E->st));
   CU(cudaStreamSynchronize(E->st));
@@ -906,19 +935,24 @@ lv_status issue_pass(lv_engine* E, const PassControl* ctl) {
   cudaStream_t st = E->st;
   // batched form: this pass visits only the graphs still moving
   if (E->batch) CU(launch_compact_active(D, st));
-  // every bucket's kernels are issued, empty or not, so the pass has the
-  // same shape on every level
+  // the kernels of classes empty on this level are left out (the level
+  // graph is keyed by which classes are non-empty)
   for (int b = 1; b <= kBuckets; b++) {
+    const bool hubs = b == 7 && class_nonempty(E, 8);
+    if (!class_nonempty(E, b) && !hubs) continue;
     const uint32_t s = E->plan.cls_start[b];
     const uint32_t e = (b == 7) ? E->plan.cls_start[9] : E->plan.cls_start[b + 1];
     // algorithmic bytes: every entry's (col, w, comm[col]) and, per vertex,
     // order id, offset, comm, k, a_C(v) (FP64) and the proposal
     const double vb = (double)(e - s);
     const double v7 = (double)(E->plan.cls_start[b + 1] - s);
-    cudaEvent_t t0 = prof_begin(E);
-    CU(launch_move_bucket(D, b, rule, E->tune, st));
-    prof_end(E, t0, K_MOVE1 + b - 1, (double)E->class_deg[b] * 12.0 + v7 * 32.0);
-    if (b == 7) {
+    cudaEvent_t t0;
+    if (class_nonempty(E, b)) {
+      t0 = prof_begin(E);
+      CU(launch_move_bucket(D, b, rule, E->tune, st));
+      prof_end(E, t0, K_MOVE1 + b - 1, (double)E->class_deg[b] * 12.0 + v7 * 32.0);
+    }
+    if (hubs) {
       t0 = prof_begin(E);
       CU(launch_move_bucket(D, 8, rule, nullptr, st));
       prof_end(E, t0, K_HUB,
