@@ -746,6 +746,9 @@ lv_status prepare_level(lv_engine* E) {
   }
   CU(cudaMemcpyAsync(E->class_deg, E->d_class_deg, kClasses * sizeof(uint64_t),
                      cudaMemcpyDeviceToHost, st));
+  // single graph: the row of every entry, for the pass loop's modularity
+  // sweep (kept in the contraction's column scratch until the level ends)
+  if (!E->batch) CU(launch_row_ids(E->off(), n, E->e, E->cb.tcol, st));
   // row sums, singleton state, m; then Q of the singleton partition
   const LevelView L = E->view();
   const double Vd = (double)n, Ed = (double)E->e;
@@ -784,6 +787,10 @@ lv_status upload_desc(lv_engine* E, float min_gain) {
   d.cg = E->cg;
   d.cg_new = E->cg_new;
   d.n_graphs = E->batch ? E->n_graphs : 0u;
+  // single graph: row ids built by prepare_level in the contraction's
+  // column scratch, which is idle until the level's pass loop ends
+  d.rowid = E->batch ? nullptr : E->cb.tcol;
+  d.nnz = E->e;
   d.min_gain = (double)min_gain;
   d.max_passes = E->cfg.max_passes;
   CU(cudaMemcpyAsync(E->d_desc, &d, sizeof(d), cudaMemcpyHostToDevice, E->st));

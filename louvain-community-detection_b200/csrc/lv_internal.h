@@ -267,10 +267,18 @@ struct PassDesc {
   const uint32_t* cg;
   uint32_t* cg_new;
   uint32_t n_graphs;
+  // single graph: the row of every entry (the modularity sweep runs over
+  // the entries, not the class lists); nullptr in the batched form
+  const uint32_t* rowid;
+  uint64_t nnz;
   // device-side pass loop
   double min_gain;
   uint32_t max_passes;
 };
+
+// rowid[j] = the row holding entry j of a CSR of n rows and nnz entries.
+cudaError_t launch_row_ids(const uint64_t* off, uint32_t n, uint64_t nnz, uint32_t* rowid,
+                           cudaStream_t st);
 
 // Pass kernels: every launch reads the level from D (device memory) and
 // uses a fixed grid, so a pass captured once replays on every level.

@@ -1125,11 +1125,47 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// Single graph with row ids: the intra-community weight over the entries
+// themselves -- every load coalesced but the two community gathers, four
+// independent entries per thread in flight.
+__device__ __forceinline__ double intra_sweep(const LevelView& L, const uint32_t* rowid,
+                                             uint64_t nnz) {
+  double part = 0.0;
+  const uint64_t stride = (uint64_t)gridDim.x * kThreads * 4;
+  for (uint64_t b = (uint64_t)blockIdx.x * kThreads * 4 + threadIdx.x; b < nnz; b += stride) {
+    uint32_t r[4], c[4];
+    float w[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint64_t j = b + (uint64_t)k * kThreads;
+      r[k] = c[k] = 0u;
+      w[k] = 0.0f;
+      if (j < nnz) {
+        r[k] = rowid[j];
+        c[k] = L.col[j];
+        w[k] = L.w[j];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (L.comm[r[k]] == L.comm[c[k]]) part += (double)w[k];
+  }
+  return part;
+}
+
+// Modularity of the current partition (modularity.cu:400-436): the
+// intra-community weight (over the entries with row ids, else over the
+// class lists) and the sum of squared community totals.
 __device__ __forceinline__ void modularity_body(const LevelView& L, const DispatchArgs& A,
-                                                const PassControl& ctl) {
+                                                const PassControl& ctl,
+                                                const uint32_t* rowid, uint64_t nnz) {
   __shared__ double red[kWarps];
   double part = 0.0;
-  dispatch_units(L, A, IntraOp{}, part, red);
+  if (rowid && !L.gid) {
+    part = intra_sweep(L, rowid, nnz);
+  } else {
+    dispatch_units(L, A, IntraOp{}, part, red);
+  }
   const uint32_t chunk = (L.n + gridDim.x - 1) / gridDim.x;
   const uint32_t c0 = blockIdx.x * chunk;
   const uint32_t c1 = min(L.n, c0 + chunk);
@@ -1207,7 +1243,7 @@ __device__ __forceinline__ void modularity_body(const LevelView& L, const Dispat
 
 __global__ void __launch_bounds__(kThreads)
     modularity_kernel(LevelView L, DispatchArgs A, PassControl ctl) {
-  modularity_body(L, A, ctl);
+  modularity_body(L, A, ctl, nullptr, 0);
 }
 
 // The modularity sweep of a pass (level and stop-rule limits from the
@@ -1217,7 +1253,7 @@ __global__ void __launch_bounds__(kThreads, kModPerSM)
   ctl.min_gain = D->min_gain;
   ctl.max_passes = D->max_passes;
   const LevelView L = D->L;
-  modularity_body(L, D->A, ctl);
+  modularity_body(L, D->A, ctl, D->rowid, D->nnz);
 }
 
 __global__ void pass_control_init_kernel(const PassDesc* __restrict__ D) {
@@ -1456,11 +1492,43 @@ cudaError_t launch_modularity(const LevelView& L, const uint32_t* order,
   return cudaGetLastError();
 }
 
+// Row of every entry.  A warp takes 32 consecutive rows: each lane loads
+// one row's bounds, then the warp writes the 32 rows one after another,
+// 32 entries per store (coalesced).  O(rows / 32 + entries / 32) steps per
+// warp, whether the rows are long (hubs) or mostly empty (late levels).
+__global__ void row_ids_kernel(const uint64_t* __restrict__ off, uint32_t n,
+                               uint32_t* __restrict__ rowid) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t step = (uint64_t)gridDim.x * (blockDim.x / 32) * 32;
+  for (uint64_t v0 = ((uint64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5)) * 32; v0 < n;
+       v0 += step) {
+    const uint64_t v = v0 + lane;
+    uint64_t s = 0, e = 0;
+    if (v < n) {
+      s = off[v];
+      e = off[v + 1];
+    }
+    for (int i = 0; i < 32; i++) {
+      const uint64_t si = __shfl_sync(kFull, s, i), ei = __shfl_sync(kFull, e, i);
+      for (uint64_t j = si + lane; j < ei; j += 32) rowid[j] = (uint32_t)(v0 + i);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Pass kernels.  Every launch reads the level from the descriptor and uses
 // a fixed grid (grid-stride loops end at the level's counts), so a pass
 // captured once replays on any level.
 // ---------------------------------------------------------------------------
+cudaError_t launch_row_ids(const uint64_t* off, uint32_t n, uint64_t nnz, uint32_t* rowid,
+                           cudaStream_t st) {
+  if (nnz == 0 || n == 0) return cudaSuccess;
+  const uint64_t groups = ((uint64_t)n + 31) / 32;  // a warp per 32 rows
+  const unsigned grid = grid_for((groups + 7) / 8, sm_count() * 8);
+  (count_launches(1), row_ids_kernel<<<grid, 256, 0, st>>>(off, n, rowid));
+  return cudaGetLastError();
+}
+
 cudaError_t launch_pass_control_init(const PassDesc* D, cudaStream_t st) {
   (count_launches(1), pass_control_init_kernel<<<sm_count(), 256, 0, st>>>(D));
   return cudaGetLastError();
