@@ -26,6 +26,9 @@ does not shard); value = edges of all ranks / max-over-ranks time.
   served     (N=1) the served form (continuous batching, 120 GB budget) on
              Poisson arrivals of R-MAT / LFR-style requests: graphs/s and
              p50/p99 latency against the plain engine run per request
+  hbm_scale  (N=1) the plain engine on R-MAT scale 24 (16.8 M vertices,
+             521 M entries): ms per run, edges/s per pass and the dominant
+             move group's roofline
 --impl reference: the reference's CPU implementation (oracle port) alone.
 """
 from __future__ import annotations
@@ -247,6 +250,72 @@ def batched_measure(stream, count: int, steps: int = 2):
         "partitions_identical": bool(np.array_equal(o1, o2)),
         "max_abs_dq": float(np.max(np.abs(q_b - q_p))),
         "levels_max": int(lv_b.max()), "mean_q": float(q_b.mean()),
+    })
+    return res
+
+
+def hbm_scale_measure(stream, scale: int, steps: int = 2):
+    """The plain engine at HBM scale: R-MAT (a, b, c, d = 0.57, 0.19, 0.19,
+    0.05, edge factor 16, duplicates merged, unit weights) generated on the
+    device; edges/s per pass over `steps` device-timed runs after one
+    warm-up, then one run with a CUDA event pair around every launch group
+    for the dominant move group's algorithmic GB/s against the HBM peak."""
+    import torch
+
+    import lvb200
+
+    n, off, col, w, m = lvgen.rmat_device(scale, seed=0)
+    nnz = int(col.numel())
+    asg = torch.empty(n, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    res = {"workload": f"R-MAT scale {scale}", "n_vertices": n, "n_edges": int(m),
+           "n_entries": nnz, "abcd": [0.57, 0.19, 0.19, 0.05], "weights": "unit FP32",
+           "seed": 0}
+    with torch.cuda.stream(stream):
+        eng = lvb200.Engine(stream=stream.cuda_stream)
+        eng.load_device(n, nnz, off.data_ptr(), col.data_ptr(), w.data_ptr())
+        res["tuning"] = {str(b): k for b, (k, _) in eng.autotune().items()}
+
+        def step():
+            return eng.run_device(n, nnz, off.data_ptr(), col.data_ptr(), w.data_ptr(),
+                                  MIN_GAIN, asg.data_ptr())
+
+        step()
+        torch.cuda.synchronize()
+        ms, edges, r = [], 0, None
+        for _ in range(steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            r = step()
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+            edges += r.edges_processed
+        levels = eng.levels()
+        eng.set_profiling(True)
+        eng.reset_kernel_stats()
+        step()
+        torch.cuda.synchronize()
+        eng.set_profiling(False)
+        kstats = eng.kernel_stats()
+        eng.close()
+    del off, col, w, asg
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    peak, peak_kind = measured_peak()
+    moves = {k: v for k, v in kstats.items() if k.startswith("move") or k == "modularity"}
+    name, st = max(moves.items(), key=lambda kv: kv[1]["total_ms"])
+    launches_k = max(st["launches"], 1)
+    achieved = (st["bytes"] / launches_k) / (st["total_ms"] / launches_k / 1000.0) / 1e9
+    res.update({
+        "ms_per_run": sum(ms) / len(ms), "edges_per_s_per_pass": edges / (sum(ms) / 1000.0),
+        "final_q": r.modularity, "levels": len(levels),
+        "passes": [l["passes"] for l in levels],
+        "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "bytes_per_launch": st["bytes"] / launches_k,
+                     "ms_per_launch": st["total_ms"] / launches_k},
+        "kernel_ms": {k: round(v["total_ms"], 3) for k, v in kstats.items()},
     })
     return res
 
@@ -527,12 +596,14 @@ def run_engine(args, rank, world):
             e2e_value = float(t.item())
 
     eng.close()
-    batched = served = None
+    batched = served = hbm = None
     if world == 1 and args.batch_graphs > 0:
         batched = batched_measure(stream, args.batch_graphs)
     if world == 1 and args.serve_requests > 0:
         served = served_measure(args.serve_requests, args.serve_rate,
                                 int(args.serve_budget_gb * 1e9))
+    if world == 1 and args.hbm_scale > 0:
+        hbm = hbm_scale_measure(stream, args.hbm_scale)
     if rank != 0:
         return
     # roofline of the dominant kernel group
@@ -576,6 +647,8 @@ def run_engine(args, rank, world):
         line["batched"] = batched
     if served:
         line["served"] = served
+    if hbm:
+        line["hbm_scale"] = hbm
     if cpu:
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind",
                                                     "sample")}
@@ -596,6 +669,8 @@ def main():
                     help="run each level's pass loop from the host instead of a CUDA graph "
                          "WHILE node (same kernels; ncu cannot profile kernels inside "
                          "graphs with conditional nodes)")
+    ap.add_argument("--hbm-scale", type=int, default=24,
+                    help="R-MAT scale of the HBM-scale plain-engine measurement (0: skip)")
     ap.add_argument("--batch-graphs", type=int, default=4096,
                     help="graphs of the batched-form measurement (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=200,
