@@ -500,6 +500,25 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def combine_replicas(ms: float, edges: float, device: str):
+    """Replicas on N ranks: the job's time is the slowest rank's (max over
+    ranks), its work the edges every rank processed (sum).  Every rank
+    calls it at the same point."""
+    import torch
+
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item()), sum_over_ranks(float(edges), device)
+
+
+def sum_over_ranks(x: float, device: str) -> float:
+    import torch
+
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t)
+    return float(t.item())
+
+
 def run_engine(args, rank, world):
     import torch
 
@@ -570,11 +589,7 @@ def run_engine(args, rank, world):
         prof_ms = prof_ev[0].elapsed_time(prof_ev[1]) / args.steps
         if world > 1:
             torch.distributed.barrier()
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e = torch.tensor([edges], device="cuda", dtype=torch.float64)
-            torch.distributed.all_reduce(e)
-            ms, edges_all = float(t.item()), float(e.item())
+            ms, edges_all = combine_replicas(ms, edges, "cuda")
         else:
             edges_all = float(edges)
         value = edges_all / (ms / 1000.0)
@@ -591,9 +606,7 @@ def run_engine(args, rank, world):
             e2e_edges += rr.edges_processed
         e2e_value = e2e_edges / sum(e2e_times)
         if world > 1:
-            t = torch.tensor([e2e_value], device="cuda", dtype=torch.float64)
-            torch.distributed.all_reduce(t)  # replicas: throughputs add up
-            e2e_value = float(t.item())
+            e2e_value = sum_over_ranks(e2e_value, "cuda")  # replicas: throughputs add up
 
     eng.close()
     batched = served = hbm = None
