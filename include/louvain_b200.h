@@ -376,16 +376,18 @@ lv_status lv_get_launch_count(uint64_t *count);
 /* ---- modularity without allocation (no counterpart in the reference) ----
  * The FP64 modularity of lv_modularity_fp64 for a graph and partition that
  * the caller keeps in device memory, for callers that must not allocate on
- * the call path: code running under CUDA-graph stream capture (cudaMalloc
- * and cudaFree cannot be captured, and cudaFree synchronises the device),
- * latency-bound serving loops, and processes whose device memory belongs to
- * another allocator.  It allocates nothing: its scratch is a fixed array in
- * the library's device memory (8 MiB per device that loads the library,
- * held until the process exits).
- *   n_vertices <= 1048576 (else LV_ERR_LIMIT); partition ids must be
- *   < n_vertices (else LV_ERR_ARG); *d_q receives Q, and *q_host too when
- *   q_host is not NULL.  Runs on `stream` (a cudaStream_t, NULL = legacy
- *   default stream) and returns after the stream has finished the work.
+ * the call path: latency-bound serving loops that cannot stall in the
+ * allocator (or on the device-wide synchronisation of a cudaFree), and
+ * processes whose device memory belongs to another allocator (a caching
+ * allocator, a budget carved out at start-up).  It allocates nothing: its
+ * scratch is a fixed array in the library's device memory (8 MiB per device
+ * that loads the library, held until the process exits).
+ *   n_vertices <= 1048576 (else LV_ERR_LIMIT); d_cols and d_weights must
+ *   not be NULL when n_vertices > 0 (else LV_ERR_ARG); partition ids must be
+ *   < n_vertices (else LV_ERR_ARG, and *d_q is set to NaN); otherwise *d_q
+ *   receives Q, and *q_host too when q_host is not NULL.  Runs on `stream`
+ *   (a cudaStream_t, NULL = legacy default stream) and returns after the
+ *   stream has finished the work.
  * Every call shares the one array (cleared at the start of each call), so
  * calls that overlap on the GPU race.  The first call on a device looks up
  * the array's address with that device current: make it before any stream

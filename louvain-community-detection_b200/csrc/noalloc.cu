@@ -1,11 +1,11 @@
 // noalloc.cu -- FP64 modularity of a partition without any allocation.
 //
-// Some callers cannot allocate device memory on the call path: code that
-// runs while a CUDA graph is being captured (cudaMalloc/cudaFree are not
-// capturable and cudaFree synchronises the device), serving loops with a
-// latency budget that must not stall on the allocator, and processes whose
-// device memory is owned by another allocator (a framework's caching
-// allocator, a fixed budget carved out at start-up).  For them,
+// Some callers cannot allocate device memory on the call path: serving
+// loops with a latency budget that must not stall on the allocator (and
+// cannot afford the device-wide synchronisation of a cudaFree), and
+// processes whose device memory is owned by another allocator (a
+// framework's caching allocator, a fixed budget carved out at start-up)
+// and so cannot be grown behind that allocator's back.  For them,
 // lv_modularity_noalloc computes what lv_modularity_fp64 computes, with
 // its scratch (one FP64 total per community plus four accumulators) in a
 // file-scope __device__ array of fixed size instead of engine buffers.
@@ -18,6 +18,8 @@
 //     8 MiB, plus a few accumulators);
 //   * every call uses the same array and clears it first; calls whose work
 //     overlaps on the GPU (other host threads, or other streams) race on it;
+//   * every call waits for its stream to finish the work (it reads back
+//     whether any community id was invalid);
 //   * the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
 //     before any stream capture begins.
@@ -106,7 +108,13 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Q, or NaN when some community id was out of range (the sums then miss
+// those vertices, so no Q is meaningful).
 __global__ void na_final_kernel(const double* s, double* q) {
+  if (s[kAcc + 3] != 0.0) {
+    *q = __longlong_as_double(0x7ff8000000000000ll);
+    return;
+  }
   const double m = s[kAcc + 2] / 2.0;
   *q = (m > 0.0) ? s[kAcc + 0] / (2.0 * m) - s[kAcc + 1] / (4.0 * m * m) : 0.0;
 }
@@ -148,6 +156,10 @@ extern "C" lv_status lv_modularity_noalloc(uint32_t n_vertices, const uint64_t* 
                                            double* q_host, void* stream) {
   if (!d_offsets || !d_partition || !d_q) {
     lvb_set_error("NULL device pointer");
+    return LV_ERR_ARG;
+  }
+  if (n_vertices > 0 && (!d_cols || !d_weights)) {
+    lvb_set_error("lv_modularity_noalloc: NULL columns or weights for a non-empty graph");
     return LV_ERR_ARG;
   }
   if (n_vertices > kNoAllocMaxVertices) {

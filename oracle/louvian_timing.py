@@ -4,7 +4,7 @@ not on the GPU box; bench.py's CPU baseline there is the oracle's
 restatement, which this script also times on the same graph for the
 ratio between the two).
 
-    python oracle/louvian_timing.py --ref /root/reference/louvian.py \
+    python oracle/louvian_timing.py --ref $LOUVAIN_REFERENCE_DIR/louvian.py \
         [--workload banded|powerlaw-small] [--min-gain 1e-6]
 
 louvian.py is imported unmodified; its Graph.modularity_optimization and
@@ -92,7 +92,8 @@ def time_louvian(mod, path, min_gain):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference/louvian.py")
+    ap.add_argument("--ref", default=os.path.join(
+        os.environ.get("LOUVAIN_REFERENCE_DIR", "/root/reference"), "louvian.py"))
     ap.add_argument("--workload", default="banded")
     ap.add_argument("--min-gain", type=float, default=1e-6)
     args = ap.parse_args()

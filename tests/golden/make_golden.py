@@ -3,7 +3,7 @@ reference's own CPU implementation (louvian.py, imported unmodified from the
 reference checkout) on small seeded graphs.
 
 Run in a checkout where the reference is present:
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref $LOUVAIN_REFERENCE_DIR]
 
 For every graph it writes `<name>.mtx` (the input, readable by both the
 reference CLI and louvian.py) and `<name>.json` with what louvian.py
@@ -112,7 +112,7 @@ def run_louvian(louvian, path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("LOUVAIN_REFERENCE_DIR", "/root/reference"))
     args = ap.parse_args()
     sys.path.insert(0, args.ref)
     import louvian  # the reference's CPU path, unmodified

@@ -10,7 +10,8 @@ import pytest
 import pyoracle
 from conftest import golden_mtx, golden_names, load_golden
 
-REF_FIXTURE = "/root/reference/tests/bcsstk16.mtx"
+REF_FIXTURE = os.path.join(os.environ.get("LOUVAIN_REFERENCE_DIR", "/root/reference"),
+                           "tests", "bcsstk16.mtx")
 
 
 @pytest.mark.parametrize("name", golden_names())
