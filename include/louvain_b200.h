@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define LV_ABI_VERSION 1
+#define LV_ABI_VERSION 2
 
 typedef enum lv_status {
     LV_OK = 0,
@@ -56,6 +56,16 @@ typedef enum lv_status {
  *                                                      278, 374)          */
 typedef enum lv_rule { LV_RULE_PY = 0, LV_RULE_CUDA = 1 } lv_rule;
 
+/* Arithmetic of the move gains (modularity.cu:149-152 and
+ * louvian.py:135-138 evaluate the same expression).
+ * LV_GAIN_FP32: FP32, operation by operation, as the reference CUDA program
+ *               (the default).
+ * LV_GAIN_FP64: FP64, operation by operation, as louvian.py.  With every
+ *               weight sum exact in FP32 (integer weights, sums below 2^24)
+ *               the runs equal louvian.py's; with large m (above ~1e7) the
+ *               two modes can break near-ties differently.                */
+typedef enum lv_gain { LV_GAIN_FP32 = 0, LV_GAIN_FP64 = 1 } lv_gain;
+
 typedef struct lv_config {
     int device;             /* CUDA device ordinal                          */
     lv_rule rule;           /* decision rule, default LV_RULE_PY            */
@@ -64,6 +74,7 @@ typedef struct lv_config {
     int use_graphs;         /* capture each level's pass in a CUDA graph
                                and replay it (default 1)                    */
     void *stream;           /* cudaStream_t to run on; NULL = own stream    */
+    lv_gain gain;           /* gain arithmetic, default LV_GAIN_FP32        */
 } lv_config;
 
 /* Per-level record (the reference prints none of this; -v here adds it). */

@@ -455,6 +455,9 @@ void free_state(lv_engine* E) {
   dfree(E->hub.blk_vertex);
   dfree(E->hub.blk_chunk);
   dfree(E->hub.blk_nchunks);
+  dfree(E->hub.unit_g);
+  dfree(E->hub.unit_c);
+  dfree(E->hub.unit_start);
   dfree(E->hub_deg);
   ContractBuffers& B = E->cb;
   dfree(B.flag_id);
@@ -600,6 +603,7 @@ lv_status prepare_level(lv_engine* E) {
   std::vector<uint32_t> blk_vertex, blk_chunk;            // dispatch chunks
   std::vector<uint32_t> unit_vertex, unit_part, unit_np;  // move units
   std::vector<uint32_t> hub_np;                           // partitions per hub
+  std::vector<uint32_t> hub_u0;                           // first move unit per hub
   std::vector<uint64_t> hub_stage, hub_ct;                // staging / chunk-table offsets
   uint64_t stage_total = 0, ct_total = 0;
   if (hc) {
@@ -613,7 +617,9 @@ lv_status prepare_level(lv_engine* E) {
       dfree(H.nparts);
       dfree(H.stage_off);
       dfree(H.ct_off);
+      dfree(H.unit_start);
       CU(dalloc(&E->hub_deg, hc));
+      CU(dalloc(&H.unit_start, (size_t)hc + 1));
       CU(dalloc(&H.best, hc));
       CU(dalloc(&H.own, hc));
       CU(dalloc(&H.hot, hc));
@@ -645,6 +651,7 @@ lv_status prepare_level(lv_engine* E) {
         unit_np.push_back(np);
       }
       hub_np.push_back(np);
+      hub_u0.push_back((uint32_t)(unit_vertex.size() - np));
       hub_stage.push_back(stage_total);
       hub_ct.push_back(ct_total);
       stage_total += deg[i];
@@ -685,9 +692,13 @@ lv_status prepare_level(lv_engine* E) {
       dfree(E->hub.blk_vertex);
       dfree(E->hub.blk_chunk);
       dfree(E->hub.blk_nchunks);
+      dfree(E->hub.unit_g);
+      dfree(E->hub.unit_c);
       CU(dalloc(&E->hub.blk_vertex, hu));
       CU(dalloc(&E->hub.blk_chunk, hu));
       CU(dalloc(&E->hub.blk_nchunks, hu));
+      CU(dalloc(&E->hub.unit_g, hu));
+      CU(dalloc(&E->hub.unit_c, hu));
       E->hub_units_cap = hu;
     }
     std::vector<uint32_t> map(2 * hb);
@@ -717,6 +728,9 @@ lv_status prepare_level(lv_engine* E) {
     }
     CU(cudaMemcpyAsync(H.nparts, hub_np.data(), hc * sizeof(uint32_t), cudaMemcpyHostToDevice,
                        st));
+    hub_u0.push_back((uint32_t)hu);
+    CU(cudaMemcpyAsync(H.unit_start, hub_u0.data(), ((size_t)hc + 1) * sizeof(uint32_t),
+                       cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync(H.stage_off, hub_stage.data(), hc * sizeof(uint64_t),
                        cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync(H.ct_off, hub_ct.data(), hc * sizeof(uint64_t), cudaMemcpyHostToDevice,
@@ -813,7 +827,8 @@ bool class_nonempty(const lv_engine* E, int c) {
 // (batched passes compact their lists), the rule, the tuning and which
 // classes are non-empty.
 uint64_t level_key(const lv_engine* E) {
-  uint64_t k = (E->batch ? 1u : 0u) | ((uint64_t)(E->cfg.rule == LV_RULE_CUDA) << 1);
+  uint64_t k = (E->batch ? 1u : 0u) | ((uint64_t)(E->cfg.rule == LV_RULE_CUDA) << 1) |
+               ((uint64_t)(E->cfg.gain == LV_GAIN_FP64) << 2);
   for (int b = 1; b <= kBuckets; b++) k |= (uint64_t)E->tune[b] << (4 * b);
   for (int c = 1; c <= 8; c++) k |= (uint64_t)class_nonempty(E, c) << (39 + c);
   return k;
@@ -941,8 +956,13 @@ lv_status run_pass(lv_engine* E, const PassControl* ctl = nullptr) {
   return LV_OK;
 }
 
+int engine_mode(const lv_engine* E) {
+  return move_mode(E->cfg.rule == LV_RULE_CUDA ? LV_RULE_CUDA_I : LV_RULE_PY_I,
+                   E->cfg.gain == LV_GAIN_FP64 ? 1 : 0);
+}
+
 lv_status issue_pass(lv_engine* E, const PassControl* ctl) {
-  const int rule = (E->cfg.rule == LV_RULE_CUDA) ? LV_RULE_CUDA_I : LV_RULE_PY_I;
+  const int rule = engine_mode(E);
   const PassDesc* D = E->d_desc;
   cudaStream_t st = E->st;
   // batched form: this pass visits only the graphs still moving
@@ -1525,6 +1545,7 @@ void lv_config_default(lv_config* cfg) {
   cfg->max_levels = 0;
   cfg->use_graphs = 1;
   cfg->stream = nullptr;
+  cfg->gain = LV_GAIN_FP32;
 }
 
 lv_status lv_engine_create(const lv_config* cfg, lv_engine** out) {
@@ -1540,6 +1561,10 @@ lv_status lv_engine_create(const lv_config* cfg, lv_engine** out) {
   if (E->cfg.rule != LV_RULE_PY && E->cfg.rule != LV_RULE_CUDA) {
     delete E;
     return fail(LV_ERR_ARG, "unknown rule");
+  }
+  if (E->cfg.gain != LV_GAIN_FP32 && E->cfg.gain != LV_GAIN_FP64) {
+    delete E;
+    return fail(LV_ERR_ARG, "unknown gain arithmetic");
   }
   if (E->cfg.max_passes == 0) E->cfg.max_passes = 100000;
   E->device = E->cfg.device;
@@ -2375,7 +2400,7 @@ lv_status lv_autotune(lv_engine* E, uint32_t reps, lv_tuning* out) {
   if (!E->level_ready) LVTRY(prepare_level(E));
   drop_pass_graph(E);  // a captured pass would keep the old kernels
   LVTRY(upload_desc(E, 0.0f));
-  const int rule = (E->cfg.rule == LV_RULE_CUDA) ? LV_RULE_CUDA_I : LV_RULE_PY_I;
+  const int rule = engine_mode(E);
   lv_tuning t{};
   for (int b = 1; b <= kBuckets; b++) {
     t.bucket_kernel[b] = E->tune[b];

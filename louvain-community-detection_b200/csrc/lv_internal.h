@@ -46,6 +46,9 @@ constexpr uint32_t kEmptyKey = 0xFFFFFFFFu;
 // Decision rules, numbered as lv_rule in the C ABI.
 constexpr int LV_RULE_PY_I = 0;    // louvian.py:148-151
 constexpr int LV_RULE_CUDA_I = 1;  // modularity.cu:182,278,374
+// Move mode of the kernels: rule | (gain precision << 1), precision 0 =
+// FP32 gains (modularity.cu:149-152), 1 = FP64 gains (louvian.py:135-138).
+constexpr int move_mode(int rule, int fp64) { return (rule & 1) | ((fp64 & 1) << 1); }
 
 // Scalars of the current level, resident in device memory so no kernel
 // needs a host round trip to learn them.
@@ -230,6 +233,11 @@ struct HubArena {
   uint32_t* blk_vertex = nullptr;  // [units] hub index of each merge unit
   uint32_t* blk_chunk = nullptr;   // [units] partition of the unit
   uint32_t* blk_nchunks = nullptr; // [units] partitions of that hub
+  // FP64 gains: every merge unit's best (gain key, ~community), reduced by
+  // the decide kernel over the hub's units [unit_start[i], unit_start[i+1])
+  unsigned long long* unit_g = nullptr;  // [units]
+  uint32_t* unit_c = nullptr;            // [units]
+  uint32_t* unit_start = nullptr;        // [hub_count + 1]
   uint32_t units = 0;
 };
 // Shared table of a hub merge unit (4096 slots, about kHubPartKeys
@@ -286,8 +294,8 @@ cudaError_t launch_row_ids(const uint64_t* off, uint32_t n, uint64_t nnz, uint32
 // for the single graph and for every graph of a batch.
 cudaError_t launch_pass_control_init(const PassDesc* D, cudaStream_t st);
 // Proposals of bucket 1..7 (variant[b]: the kernel, null = defaults), or of
-// the hubs (bucket 8).
-cudaError_t launch_move_bucket(const PassDesc* D, int bucket, int rule, const uint8_t* variant,
+// the hubs (bucket 8); mode = move_mode(rule, fp64 gains).
+cudaError_t launch_move_bucket(const PassDesc* D, int bucket, int mode, const uint8_t* variant,
                                cudaStream_t st);
 // Applies bucket b's proposals (bucket 7: classes 7 and 8; `compacted`:
 // the batched form's active lists, where they are not adjacent).

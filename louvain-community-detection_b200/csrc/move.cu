@@ -10,6 +10,9 @@
 //   argmax, ties -> lower community ... modularity.cu:169-179,359-368
 //   decision .......................... louvian.py:148-151 (LV_RULE_PY),
 //                                       modularity.cu:182,278,374 (LV_RULE_CUDA)
+//   gain arithmetic ................... FP32 as modularity.cu:149-152
+//                                       (LV_GAIN_FP32), FP64 as
+//                                       louvian.py:135-138 (LV_GAIN_FP64)
 //   apply moves + community totals .... modularity.cu:382-398
 //   modularity ........................ modularity.cu:400-436
 //
@@ -86,8 +89,56 @@ __device__ __forceinline__ unsigned long long pack_best(float gain,
   return ((unsigned long long)float_key(gain) << 32) | (uint32_t)(~c);
 }
 
+// FP64 gains: the argmax key is the pair (order-preserving bits of the
+// double gain, ~community), compared lexicographically -- max gain, then
+// lowest community id, as the packed FP32 key.  g == 0: no candidate.
+struct Best64 {
+  unsigned long long g;
+  uint32_t c;
+};
+__device__ __forceinline__ unsigned long long double_key(double d) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(d);
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double key_double(unsigned long long k) {
+  return __longlong_as_double(
+      (long long)((k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k));
+}
+// Kernels are instantiated per mode: bit 0 the decision rule, bit 1 the
+// gain precision.
+template <int MODE>
+struct ModeOf {
+  static constexpr int kRule = MODE & 1;
+  static constexpr int kPrec = MODE >> 1;
+};
+template <int PREC>
+struct BestOf {
+  using T = unsigned long long;
+};
+template <>
+struct BestOf<1> {
+  using T = Best64;
+};
+__device__ __forceinline__ unsigned long long best_max(unsigned long long a,
+                                                       unsigned long long b) {
+  return umax64(a, b);
+}
+__device__ __forceinline__ Best64 best_max(const Best64& a, const Best64& b) {
+  return (a.g > b.g || (a.g == b.g && a.c > b.c)) ? a : b;
+}
+__device__ __forceinline__ unsigned long long shfl_xor_best(unsigned long long x, int o) {
+  return __shfl_xor_sync(0xffffffffu, x, o);
+}
+__device__ __forceinline__ Best64 shfl_xor_best(const Best64& x, int o) {
+  Best64 y;
+  y.g = __shfl_xor_sync(0xffffffffu, x.g, o);
+  y.c = __shfl_xor_sync(0xffffffffu, x.c, o);
+  return y;
+}
+
 struct GainCtx {
   float m, den, kv, aown_minus_kv;
+  double m64, den64, kv64, aown_minus_kv64;  // FP64 gains
   uint32_t cv, szv;
   bool active;  // the vertex's graph still moves (batched form)
 };
@@ -97,6 +148,7 @@ __device__ __forceinline__ bool vertex_active(const LevelView& L, uint32_t v) {
   return !L.gid || L.gs[L.gid[v]].active;
 }
 
+template <int PREC>
 __device__ __forceinline__ GainCtx make_ctx(const LevelView& L, uint32_t v,
                                             uint32_t cv) {
   GainCtx g;
@@ -104,14 +156,23 @@ __device__ __forceinline__ GainCtx make_ctx(const LevelView& L, uint32_t v,
     const GraphState& gs = L.gs[L.gid[v]];
     g.m = gs.m;
     g.den = gs.den;
+    g.m64 = gs.m64;
     g.active = gs.active != 0u;
   } else {
     g.m = L.sc->m;
     g.den = L.sc->den;
+    g.m64 = L.sc->m64;
     g.active = true;
   }
   g.kv = L.k[v];
-  g.aown_minus_kv = __fsub_rn((float)L.tot[cv], g.kv);
+  const double acv = L.tot[cv];
+  if (PREC) {  // louvian.py:135-138: kv * ((a_own - kv) - a_c) / (2 * (m * m))
+    g.kv64 = (double)g.kv;
+    g.aown_minus_kv64 = __dsub_rn(acv, g.kv64);
+    g.den64 = __dmul_rn(2.0, __dmul_rn(g.m64, g.m64));
+  } else {
+    g.aown_minus_kv = __fsub_rn((float)acv, g.kv);
+  }
   g.cv = cv;
   g.szv = L.comm_sz[cv];
   return g;
@@ -125,17 +186,35 @@ __device__ __forceinline__ float gain_of(float ec, float ac, const GainCtx& g) {
   float t4 = __fdiv_rn(t3, g.den);
   return __fadd_rn(t1, t4);
 }
+// The same expression in FP64, operation by operation (louvian.py:135-138).
+__device__ __forceinline__ double gain_of64(double ec, double ac, const GainCtx& g) {
+  const double t1 = __ddiv_rn(ec, g.m64);
+  const double t2 = __dsub_rn(g.aown_minus_kv64, ac);
+  const double t3 = __dmul_rn(g.kv64, t2);
+  const double t4 = __ddiv_rn(t3, g.den64);
+  return __dadd_rn(t1, t4);
+}
 
-// Candidate key of neighbour community c with summed weight ec (0 if c is
-// not eligible under isLowerIdx, modularity.cu:85-93).
-__device__ __forceinline__ unsigned long long candidate(const LevelView& L,
-                                                        const GainCtx& g,
-                                                        uint32_t c,
-                                                        double ec) {
-  const uint32_t szc = L.comm_sz[c];
-  if (g.szv == 1 && szc == 1 && !(c < g.cv)) return 0ull;
-  const float gain = gain_of((float)ec, (float)L.tot[c], g);
-  return pack_best(gain, c);
+// Candidate key of neighbour community c (summed weight ec, total ac, size
+// szc); none if c is not eligible under isLowerIdx (modularity.cu:85-93).
+template <int PREC>
+__device__ __forceinline__ typename BestOf<PREC>::T candidate_loaded(const GainCtx& g,
+                                                                     uint32_t c, double ec,
+                                                                     uint32_t szc, double ac) {
+  using K = typename BestOf<PREC>::T;
+  if (g.szv == 1 && szc == 1 && !(c < g.cv)) return K{};
+  if constexpr (PREC) {
+    return Best64{double_key(gain_of64(ec, ac, g)), ~c};
+  } else {
+    return pack_best(gain_of((float)ec, (float)ac, g), c);
+  }
+}
+
+template <int PREC>
+__device__ __forceinline__ typename BestOf<PREC>::T candidate(const LevelView& L,
+                                                              const GainCtx& g, uint32_t c,
+                                                              double ec) {
+  return candidate_loaded<PREC>(g, c, ec, L.comm_sz[c], L.tot[c]);
 }
 
 template <int RULE>
@@ -152,11 +231,24 @@ __device__ __forceinline__ uint32_t decide(unsigned long long best, double own,
   }
   return move ? bc : g.cv;
 }
+template <int RULE>
+__device__ __forceinline__ uint32_t decide(const Best64& best, double own, const GainCtx& g) {
+  if (best.g == 0ull || !g.active) return g.cv;
+  const double bg = key_double(best.g);
+  const uint32_t bc = ~best.c;
+  bool move;
+  if (RULE == LV_RULE_CUDA_I) {  // max_gain - e_own / m > 0 in FP64
+    move = __dsub_rn(bg, __ddiv_rn(own, g.m64)) > 0.0;
+  } else {
+    move = bg > 0.0;
+  }
+  return move ? bc : g.cv;
+}
 
-template <int G>
-__device__ __forceinline__ unsigned long long group_max(unsigned long long x) {
+template <int G, class K>
+__device__ __forceinline__ K group_max(K x) {
 #pragma unroll
-  for (int o = G / 2; o > 0; o >>= 1) x = umax64(x, __shfl_xor_sync(kFull, x, o));
+  for (int o = G / 2; o > 0; o >>= 1) x = best_max(x, shfl_xor_best(x, o));
   return x;
 }
 template <int G>
@@ -231,18 +323,12 @@ __device__ __forceinline__ uint32_t table_insert(uint32_t* keys, uint32_t mask,
 // Move kernels
 // ---------------------------------------------------------------------------
 
-// Candidate key from values already loaded (see candidate()).
-__device__ __forceinline__ unsigned long long candidate_loaded(const GainCtx& g,
-                                                               uint32_t c, double ec,
-                                                               uint32_t szc, double ac) {
-  if (g.szv == 1 && szc == 1 && !(c < g.cv)) return 0ull;
-  return pack_best(gain_of((float)ec, (float)ac, g), c);
-}
-
 // deg <= G: G lanes per vertex, one edge per lane.
-template <int G, int RULE>
+template <int G, int MODE>
 __global__ void __launch_bounds__(kThreads, kSmallPerSM)
     move_small_kernel(const PassDesc* __restrict__ D, int cls) {
+  constexpr int RULE = ModeOf<MODE>::kRule, PREC = ModeOf<MODE>::kPrec;
+  using K = typename BestOf<PREC>::T;
   const LevelView L = D->L;
   const uint32_t s0 = D->A.P.cls_start[cls];
   const uint32_t* __restrict__ verts = D->A.order + s0;
@@ -270,7 +356,7 @@ __global__ void __launch_bounds__(kThreads, kSmallPerSM)
     const bool has = act && gl < (int)d;
     // the vertex's own state is read alongside its row (no dependency)
     GainCtx g;
-    if (vvalid) g = make_ctx(L, v, cv);
+    if (vvalid) g = make_ctx<PREC>(L, v, cv);
     uint32_t u = 0, cu = 0, szc = 0;
     float wt = 0.0f;
     double ac = 0.0;
@@ -307,9 +393,9 @@ __global__ void __launch_bounds__(kThreads, kSmallPerSM)
     double own = 0.0;
     if (RULE == LV_RULE_CUDA_I && is_hot && u != v) own = (double)wt;
     __syncwarp();
-    unsigned long long best = 0ull;
+    K best{};
     if ((ins && leader == lane) || lane == hot_leader)
-      best = candidate_loaded(g, cu, sums[wib][lane], szc, ac);
+      best = candidate_loaded<PREC>(g, cu, sums[wib][lane], szc, ac);
     best = group_max<G>(best);
     if (RULE == LV_RULE_CUDA_I) own = group_sum<G>(own);
     if (vvalid && gl == 0) prop[vidx] = decide<RULE>(best, own, g);
@@ -321,10 +407,11 @@ __global__ void __launch_bounds__(kThreads, kSmallPerSM)
 // threads from tid, four slots per thread at a time so the gathers
 // overlap); each thread empties the taken slots it read, leaving the table
 // clean.
-__device__ __forceinline__ unsigned long long scan_table_and_clear(
+template <int PREC>
+__device__ __forceinline__ typename BestOf<PREC>::T scan_table_and_clear(
     const LevelView& L, const GainCtx& g, uint32_t* keys, double* vals,
     uint32_t tv, uint32_t tid, uint32_t nthr) {
-  unsigned long long best = 0ull;
+  typename BestOf<PREC>::T best{};
 #pragma unroll 1
   for (uint32_t i0 = tid; i0 < tv; i0 += 4 * nthr) {
     uint32_t c[4], szc[4];
@@ -345,7 +432,7 @@ __device__ __forceinline__ unsigned long long scan_table_and_clear(
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       if (c[q] != kEmptyKey) {
-        best = umax64(best, candidate_loaded(g, c[q], ec[q], szc[q], ac[q]));
+        best = best_max(best, candidate_loaded<PREC>(g, c[q], ec[q], szc[q], ac[q]));
         const uint32_t i = i0 + q * nthr;
         keys[i] = kEmptyKey;
         vals[i] = 0.0;
@@ -358,9 +445,10 @@ __device__ __forceinline__ unsigned long long scan_table_and_clear(
 // 32 < deg <= 319: one warp per vertex, T-slot table per warp.  All of a
 // row's loads (at most MAXW waves of 32) are issued before any insertion,
 // so a vertex costs one memory latency chain instead of one per wave.
-template <int T, int MAXW, int RULE>
+template <int T, int MAXW, int MODE>
 __global__ void __launch_bounds__(kThreads, T == 128 ? kWarp128PerSM : kWarp512PerSM)
     move_warp_kernel(const PassDesc* __restrict__ D, int cls) {
+  constexpr int RULE = ModeOf<MODE>::kRule, PREC = ModeOf<MODE>::kPrec;
   const LevelView L = D->L;
   const uint32_t s0 = D->A.P.cls_start[cls];
   const uint32_t* __restrict__ verts = D->A.order + s0;
@@ -391,7 +479,7 @@ __global__ void __launch_bounds__(kThreads, T == 128 ? kWarp128PerSM : kWarp512P
       clean = tv;
       __syncwarp();
     }
-    const GainCtx g = make_ctx(L, v, cv);
+    const GainCtx g = make_ctx<PREC>(L, v, cv);
     uint32_t cu[MAXW];
     float wt[MAXW];
     unsigned self_mask = 0u;  // waves whose entry is the self-loop
@@ -435,7 +523,7 @@ __global__ void __launch_bounds__(kThreads, T == 128 ? kWarp128PerSM : kWarp512P
       vals[slot] += hot;
     }
     __syncwarp();
-    unsigned long long best = scan_table_and_clear(L, g, keys, vals, tv, lane, 32);
+    auto best = scan_table_and_clear<PREC>(L, g, keys, vals, tv, lane, 32);
     best = group_max<32>(best);
     if (RULE == LV_RULE_CUDA_I) own = group_sum<32>(own);
     if (lane == 0) prop[vidx] = decide<RULE>(best, own, g);
@@ -443,15 +531,15 @@ __global__ void __launch_bounds__(kThreads, T == 128 ? kWarp128PerSM : kWarp512P
   }
 }
 
-__device__ __forceinline__ unsigned long long block_max(unsigned long long x,
-                                                        unsigned long long* red) {
+template <class K>
+__device__ __forceinline__ K block_max(K x, K* red) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   x = group_max<32>(x);
   if (lane == 0) red[wib] = x;
   __syncthreads();
-  unsigned long long r = 0ull;
+  K r{};
   if (threadIdx.x == 0) {
-    for (int i = 0; i < kWarps; i++) r = umax64(r, red[i]);
+    for (int i = 0; i < kWarps; i++) r = best_max(r, red[i]);
   }
   __syncthreads();
   return r;  // valid in thread 0
@@ -516,9 +604,11 @@ __device__ __forceinline__ void insert_block_range(const LevelView& L, uint64_t 
 }
 
 // 319 < deg <= 2048: one block per vertex, shared 4096-slot table.
-template <int RULE>
+template <int MODE>
 __global__ void __launch_bounds__(kThreads, kBlockPerSM)
     move_block_kernel(const PassDesc* __restrict__ D, int cls) {
+  constexpr int RULE = ModeOf<MODE>::kRule, PREC = ModeOf<MODE>::kPrec;
+  using K = typename BestOf<PREC>::T;
   const LevelView L = D->L;
   const uint32_t s0 = D->A.P.cls_start[cls];
   const uint32_t* __restrict__ verts = D->A.order + s0;
@@ -529,7 +619,7 @@ __global__ void __launch_bounds__(kThreads, kBlockPerSM)
   constexpr int MAXW = (int)(kHubSmemMaxDeg / kThreads);
   double* vals = reinterpret_cast<double*>(smem_raw);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T);
-  __shared__ unsigned long long red_best[kWarps];
+  __shared__ K red_best[kWarps];
   __shared__ double red_own[kWarps];
   uint32_t clean = 0;  // leading table slots known to be empty
   for (uint32_t vidx = blockIdx.x; vidx < count; vidx += gridDim.x) {
@@ -550,7 +640,7 @@ __global__ void __launch_bounds__(kThreads, kBlockPerSM)
       clean = tv;
       __syncthreads();
     }
-    const GainCtx g = make_ctx(L, v, cv);
+    const GainCtx g = make_ctx<PREC>(L, v, cv);
     double own = 0.0;
     double hot = 0.0;
     bool hot_seen = false;
@@ -563,8 +653,7 @@ __global__ void __launch_bounds__(kThreads, kBlockPerSM)
       vals[slot] += hot;
     }
     __syncthreads();
-    unsigned long long best =
-        scan_table_and_clear(L, g, keys, vals, tv, threadIdx.x, kThreads);
+    K best = scan_table_and_clear<PREC>(L, g, keys, vals, tv, threadIdx.x, kThreads);
     best = block_max(best, red_best);
     if (RULE == LV_RULE_CUDA_I) own = block_sum(own, red_own);
     if (threadIdx.x == 0) prop[vidx] = decide<RULE>(best, own, g);
@@ -622,9 +711,10 @@ __device__ __forceinline__ uint32_t block_scan_inplace(uint32_t* a, uint32_t n,
   return total;
 }
 
-template <int RULE>
+template <int MODE>
 __global__ void __launch_bounds__(kThreads, kSplitPerSM)
     hub_split_kernel(const PassDesc* __restrict__ D) {
+  constexpr int RULE = ModeOf<MODE>::kRule;
   const LevelView L = D->L;
   const uint32_t* __restrict__ hubs = D->A.order + D->A.P.cls_start[8];
   const HubArena H = D->H;
@@ -711,9 +801,11 @@ __global__ void __launch_bounds__(kThreads, kSplitPerSM)
   }
 }
 
-template <int RULE>
+template <int MODE>
 __global__ void __launch_bounds__(kThreads, kMergePerSM)
     hub_merge_kernel(const PassDesc* __restrict__ D) {
+  constexpr int PREC = ModeOf<MODE>::kPrec;
+  using K = typename BestOf<PREC>::T;
   const LevelView L = D->L;
   const uint32_t* __restrict__ hubs = D->A.order + D->A.P.cls_start[8];
   const HubArena H = D->H;
@@ -722,7 +814,7 @@ __global__ void __launch_bounds__(kThreads, kMergePerSM)
   constexpr int T = kHubPartSlots;
   double* vals = reinterpret_cast<double*>(smem_raw);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T);
-  __shared__ unsigned long long red_best[kWarps];
+  __shared__ K red_best[kWarps];
   __shared__ uint32_t seg_a[kThreads], seg_pre[kThreads], wsum[kWarps];
   for (uint32_t i = threadIdx.x; i < T; i += kThreads) {
     keys[i] = kEmptyKey;
@@ -770,16 +862,25 @@ __global__ void __launch_bounds__(kThreads, kMergePerSM)
       }
       __syncthreads();  // seg_a / seg_pre are refilled
     }
-    const GainCtx g = make_ctx(L, v, L.comm[v]);
-    unsigned long long best = scan_table_and_clear(L, g, keys, vals, T, threadIdx.x, kThreads);
+    const GainCtx g = make_ctx<PREC>(L, v, L.comm[v]);
+    K best = scan_table_and_clear<PREC>(L, g, keys, vals, T, threadIdx.x, kThreads);
     best = block_max(best, red_best);
-    if (threadIdx.x == 0 && best) atomicMax(&H.best[hi], best);
+    if (threadIdx.x == 0) {
+      if constexpr (PREC) {  // no 96-bit atomic: the decide kernel reduces the units
+        H.unit_g[u] = best.g;
+        H.unit_c[u] = best.c;
+      } else if (best) {
+        atomicMax(&H.best[hi], best);
+      }
+    }
     __syncthreads();
   }
 }
 
-template <int RULE>
+template <int MODE>
 __global__ void hub_decide_kernel(const PassDesc* __restrict__ D) {
+  constexpr int RULE = ModeOf<MODE>::kRule, PREC = ModeOf<MODE>::kPrec;
+  using K = typename BestOf<PREC>::T;
   const LevelView L = D->L;
   const uint32_t* __restrict__ hubs = D->A.order + D->A.P.cls_start[8];
   const HubArena H = D->H;
@@ -788,10 +889,16 @@ __global__ void hub_decide_kernel(const PassDesc* __restrict__ D) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < hub_count;
        i += gridDim.x * blockDim.x) {
     const uint32_t v = hubs[i];
-    const GainCtx g = make_ctx(L, v, L.comm[v]);
-    unsigned long long best = H.best[i];
+    const GainCtx g = make_ctx<PREC>(L, v, L.comm[v]);
+    K best{};
+    if constexpr (PREC) {  // the hub's merge units, adjacent from unit_start[i]
+      for (uint32_t u = H.unit_start[i]; u < H.unit_start[i + 1]; u++)
+        best = best_max(best, Best64{H.unit_g[u], H.unit_c[u]});
+    } else {
+      best = H.best[i];
+    }
     // the own community's candidate from the split pass's sums
-    if (H.hot_any[i]) best = umax64(best, candidate(L, g, g.cv, H.hot[i]));
+    if (H.hot_any[i]) best = best_max(best, candidate<PREC>(L, g, g.cv, H.hot[i]));
     prop[i] = decide<RULE>(best, H.own[i], g);
     H.best[i] = 0ull;
     H.own[i] = 0.0;
@@ -1447,27 +1554,25 @@ unsigned sm_count_cached() {
   return (unsigned)num_sms;
 }
 
+template <int MODE>
+static cudaError_t configure_mode() {
+  const int warp512 = kWarps * 512 * kSlotBytes;
+  cudaError_t e = cudaFuncSetAttribute(move_warp_kernel<512, 10, MODE>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, warp512);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(move_block_kernel<MODE>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, kBlockTabSmem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(hub_merge_kernel<MODE>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, kHubPartSmem);
+}
+
 cudaError_t configure_kernels() {
   cudaError_t e;
-  const int warp512 = kWarps * 512 * kSlotBytes;
-  e = cudaFuncSetAttribute(move_warp_kernel<512, 10, LV_RULE_PY_I>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, warp512);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(move_warp_kernel<512, 10, LV_RULE_CUDA_I>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, warp512);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(move_block_kernel<LV_RULE_PY_I>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, kBlockTabSmem);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(move_block_kernel<LV_RULE_CUDA_I>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, kBlockTabSmem);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(hub_merge_kernel<LV_RULE_PY_I>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, kHubPartSmem);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(hub_merge_kernel<LV_RULE_CUDA_I>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, kHubPartSmem);
-  if (e != cudaSuccess) return e;
+  if ((e = configure_mode<0>()) != cudaSuccess) return e;
+  if ((e = configure_mode<1>()) != cudaSuccess) return e;
+  if ((e = configure_mode<2>()) != cudaSuccess) return e;
+  if ((e = configure_mode<3>()) != cudaSuccess) return e;
   return configure_contract_kernels();
 }
 
@@ -1544,63 +1649,68 @@ cudaError_t launch_modularity_pass(const PassDesc* D, const PassControl* ctl, cu
 unsigned pass_dispatch_grid() { return sm_count() * kModPerSM; }
 
 // One launch of a move kernel variant over class `cls`.
-template <int RULE>
+template <int MODE>
 static void launch_variant(int kv, const PassDesc* D, int cls, cudaStream_t st) {
   const unsigned cap = sm_count() * kSmallPerSM;
   switch (kv) {
     case KV_SMALL4:
-      (count_launches(1), move_small_kernel<4, RULE><<<cap, kThreads, 0, st>>>(D, cls));
+      (count_launches(1), move_small_kernel<4, MODE><<<cap, kThreads, 0, st>>>(D, cls));
       break;
     case KV_SMALL8:
-      (count_launches(1), move_small_kernel<8, RULE><<<cap, kThreads, 0, st>>>(D, cls));
+      (count_launches(1), move_small_kernel<8, MODE><<<cap, kThreads, 0, st>>>(D, cls));
       break;
     case KV_SMALL16:
-      (count_launches(1), move_small_kernel<16, RULE><<<cap, kThreads, 0, st>>>(D, cls));
+      (count_launches(1), move_small_kernel<16, MODE><<<cap, kThreads, 0, st>>>(D, cls));
       break;
     case KV_SMALL32:
-      (count_launches(1), move_small_kernel<32, RULE><<<cap, kThreads, 0, st>>>(D, cls));
+      (count_launches(1), move_small_kernel<32, MODE><<<cap, kThreads, 0, st>>>(D, cls));
       break;
     case KV_WARP128: {
       constexpr int T = 128;
-      (count_launches(1), move_warp_kernel<T, 3, RULE><<<sm_count() * kWarp128PerSM, kThreads,
+      (count_launches(1), move_warp_kernel<T, 3, MODE><<<sm_count() * kWarp128PerSM, kThreads,
                                                        kWarps * T * kSlotBytes, st>>>(D, cls));
       break;
     }
     case KV_WARP512: {
       constexpr int T = 512;
-      (count_launches(1), move_warp_kernel<T, 10, RULE><<<sm_count() * kWarp512PerSM, kThreads,
+      (count_launches(1), move_warp_kernel<T, 10, MODE><<<sm_count() * kWarp512PerSM, kThreads,
                                                         kWarps * T * kSlotBytes, st>>>(D, cls));
       break;
     }
     default:  // KV_BLOCK: shared table, one block per vertex
-      (count_launches(1), move_block_kernel<RULE><<<sm_count() * kBlockPerSM, kThreads,
+      (count_launches(1), move_block_kernel<MODE><<<sm_count() * kBlockPerSM, kThreads,
                                                    kBlockTabSmem, st>>>(D, cls));
       break;
   }
 }
 
-template <int RULE>
+template <int MODE>
 static cudaError_t move_bucket_impl(const PassDesc* D, int bucket, const uint8_t* kv,
                                     cudaStream_t st) {
   if (bucket >= 1 && bucket <= 7) {
     const int v = kv ? kv[bucket] : kDefaultVariant[bucket];
     if (!variant_fits(v, bucket)) return cudaErrorInvalidValue;
-    launch_variant<RULE>(v, D, bucket, st);
+    launch_variant<MODE>(v, D, bucket, st);
     return cudaGetLastError();
   }
   if (bucket != 8) return cudaErrorInvalidValue;
   // class 8 of bucket 7: split chunks, merge (hub, partition), decide
-  (count_launches(1), hub_split_kernel<RULE><<<sm_count() * kSplitPerSM, kThreads, 0, st>>>(D));
-  (count_launches(1), hub_merge_kernel<RULE><<<sm_count() * kMergePerSM, kThreads, kHubPartSmem,
+  (count_launches(1), hub_split_kernel<MODE><<<sm_count() * kSplitPerSM, kThreads, 0, st>>>(D));
+  (count_launches(1), hub_merge_kernel<MODE><<<sm_count() * kMergePerSM, kThreads, kHubPartSmem,
                                                st>>>(D));
-  (count_launches(1), hub_decide_kernel<RULE><<<sm_count() * 2, 128, 0, st>>>(D));
+  (count_launches(1), hub_decide_kernel<MODE><<<sm_count() * 2, 128, 0, st>>>(D));
   return cudaGetLastError();
 }
 
-cudaError_t launch_move_bucket(const PassDesc* D, int bucket, int rule, const uint8_t* variant,
+cudaError_t launch_move_bucket(const PassDesc* D, int bucket, int mode, const uint8_t* variant,
                                cudaStream_t st) {
-  if (rule == LV_RULE_CUDA_I) return move_bucket_impl<LV_RULE_CUDA_I>(D, bucket, variant, st);
-  return move_bucket_impl<LV_RULE_PY_I>(D, bucket, variant, st);
+  switch (mode) {
+    case 0: return move_bucket_impl<0>(D, bucket, variant, st);
+    case 1: return move_bucket_impl<1>(D, bucket, variant, st);
+    case 2: return move_bucket_impl<2>(D, bucket, variant, st);
+    case 3: return move_bucket_impl<3>(D, bucket, variant, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_apply_bucket(const PassDesc* D, int bucket, bool compacted, cudaStream_t st) {

@@ -125,9 +125,10 @@ void printCommunities(Graph& dev_graph) {
 }
 
 void parseArgs(int argc, char** argv, float& threshold, bool& verbose,
-               char*& filename, lv_rule& rule, bool& timing) {
+               char*& filename, lv_rule& rule, bool& timing, lv_gain& gain) {
   static const struct option longopts[] = {
       {"rule", required_argument, nullptr, 'r'},
+      {"gain", required_argument, nullptr, 'p'},
       {"timing", no_argument, nullptr, 't'},
       {"cache", no_argument, nullptr, 'c'},
       {nullptr, 0, nullptr, 0}};
@@ -162,6 +163,16 @@ void parseArgs(int argc, char** argv, float& threshold, bool& verbose,
           rule = LV_RULE_CUDA;
         } else {
           std::cout << "--rule must be py or cuda" << std::endl;
+          exit(1);
+        }
+        break;
+      case 'p':
+        if (std::string(optarg) == "fp32") {
+          gain = LV_GAIN_FP32;
+        } else if (std::string(optarg) == "fp64") {
+          gain = LV_GAIN_FP64;
+        } else {
+          std::cout << "--gain must be fp32 or fp64" << std::endl;
           exit(1);
         }
         break;

@@ -55,9 +55,10 @@ void aggregation(Graph& dev_graph);
 void printCommunities(Graph& dev_graph);
 
 // parseArgs (utils.cu:231-267): -f file -g min_gain [-v]; this build adds
-// --rule py|cuda, --timing (per-level times on stderr) and --cache.
+// --rule py|cuda, --gain fp32|fp64, --timing (per-level times on stderr)
+// and --cache.
 void parseArgs(int argc, char** argv, float& threshold, bool& verbose,
-               char*& filename, lv_rule& rule, bool& timing);
+               char*& filename, lv_rule& rule, bool& timing, lv_gain& gain);
 
 // deleteDevGraph / deleteHostGraph (utils.cu:30-64).
 void deleteDevGraph(Graph& dev_graph);

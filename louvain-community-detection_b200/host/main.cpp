@@ -1,5 +1,6 @@
 // main.cpp -- CLI with the reference's interface (main.cu:5-70):
-//   louvain -f <file.mtx> -g <min_gain> [-v] [--rule py|cuda] [--timing]
+//   louvain -f <file.mtx> -g <min_gain> [-v] [--rule py|cuda] [--gain fp32|fp64]
+//           [--timing] [--cache]
 // stdout: final modularity (6 significant digits), then "alg_ms total_ms";
 // with -v the community count and one "k v1 v2 ..." line per community.
 // --timing adds a per-level table on stderr (stdout stays as the
@@ -17,7 +18,8 @@ int main(int argc, char** argv) {
   float threshold = 0.0f;
   bool verbose = false, timing = false;
   lv_rule rule = LV_RULE_PY;
-  parseArgs(argc, argv, threshold, verbose, filename, rule, timing);
+  lv_gain gain = LV_GAIN_FP32;
+  parseArgs(argc, argv, threshold, verbose, filename, rule, timing, gain);
 
   Graph host_graph, dev_graph;
   try {
@@ -34,6 +36,7 @@ int main(int argc, char** argv) {
     lv_config cfg;
     lv_config_default(&cfg);
     cfg.rule = rule;
+    cfg.gain = gain;
     // "copy" region (main.cu:19-35): engine set-up and upload
     auto c0 = std::chrono::steady_clock::now();
     initDevGraph(dev_graph, host_graph, &cfg);

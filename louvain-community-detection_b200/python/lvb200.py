@@ -19,6 +19,7 @@ HEADER_PATH = os.path.join(os.path.dirname(PKG_DIR), "include", "louvain_b200.h"
 RULE_PY = 0
 RULE_CUDA = 1
 RULES = {"py": RULE_PY, "cuda": RULE_CUDA}
+GAINS = {"fp32": 0, "fp64": 1}  # lv_gain
 
 STATUS = {
     0: "LV_OK", 1: "LV_ERR_ARG", 2: "LV_ERR_IO", 3: "LV_ERR_PARSE",
@@ -41,6 +42,7 @@ class Config(ctypes.Structure):
         ("max_levels", ctypes.c_uint32),
         ("use_graphs", ctypes.c_int),
         ("stream", ctypes.c_void_p),
+        ("gain", ctypes.c_int),
     ]
 
 
@@ -343,11 +345,13 @@ class RunResult:
 
 class Engine:
     def __init__(self, device: int = 0, rule: str = "py", max_passes: int = 0,
-                 max_levels: int = 0, use_graphs: bool = True, stream: int = 0):
+                 max_levels: int = 0, use_graphs: bool = True, stream: int = 0,
+                 gain: str = "fp32"):
         cfg = Config()
         lib().lv_config_default(ctypes.byref(cfg))
         cfg.device = device
         cfg.rule = RULES[rule]
+        cfg.gain = GAINS[gain]
         cfg.max_passes = max_passes
         cfg.max_levels = max_levels
         cfg.use_graphs = int(use_graphs)
@@ -567,11 +571,12 @@ class Server:
     def __init__(self, min_gain: float, budget_bytes: int, max_graphs: int = 0,
                  lanes: int = 1, background: bool = False, lane_max_entries=None,
                  lane_share=None, device: int = 0, rule: str = "py", max_passes: int = 0,
-                 max_levels: int = 0, use_graphs: bool = True):
+                 max_levels: int = 0, use_graphs: bool = True, gain: str = "fp32"):
         cfg = Config()
         lib().lv_config_default(ctypes.byref(cfg))
         cfg.device = device
         cfg.rule = RULES[rule]
+        cfg.gain = GAINS[gain]
         cfg.max_passes = max_passes
         cfg.max_levels = max_levels
         cfg.use_graphs = int(use_graphs)

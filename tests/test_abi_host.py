@@ -25,7 +25,7 @@ def test_library_exports_every_header_symbol():
 
 def test_abi_version_and_status_strings():
     L = lvb200.lib()
-    assert L.lv_abi_version() == 1
+    assert L.lv_abi_version() == 2
     assert L.lv_status_string(0) == b"ok"
     assert L.lv_status_string(2) == b"Error opening file"
 
