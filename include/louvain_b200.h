@@ -75,6 +75,9 @@ typedef struct lv_config {
                                and replay it (default 1)                    */
     void *stream;           /* cudaStream_t to run on; NULL = own stream    */
     lv_gain gain;           /* gain arithmetic, default LV_GAIN_FP32        */
+    int level_kernel;       /* run a single graph's pass loop as one
+                               persistent kernel per level (default 1); 0:
+                               per-kernel launches, as use_graphs says      */
 } lv_config;
 
 /* Per-level record (the reference prints none of this; -v here adds it). */

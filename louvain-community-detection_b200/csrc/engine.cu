@@ -310,6 +310,10 @@ struct lv_engine {
   // the pass descriptor (device); the level graphs built on it are kept
   // across levels and runs
   PassDesc* d_desc = nullptr;
+  // persistent level kernel: barrier / timer state (device) and its pinned
+  // host mirror
+  LevelLoopState* loop_state = nullptr;
+  LevelLoopState* loop_host = nullptr;
   uint8_t tune[8] = {kDefaultVariant[0], kDefaultVariant[1], kDefaultVariant[2],
                      kDefaultVariant[3], kDefaultVariant[4], kDefaultVariant[5],
                      kDefaultVariant[6], kDefaultVariant[7]};
@@ -807,6 +811,8 @@ lv_status upload_desc(lv_engine* E, float min_gain) {
   d.nnz = E->e;
   d.min_gain = (double)min_gain;
   d.max_passes = E->cfg.max_passes;
+  for (int b = 0; b < 8; b++) d.tune[b] = E->tune[b];
+  d.loop = E->loop_state;
   CU(cudaMemcpyAsync(E->d_desc, &d, sizeof(d), cudaMemcpyHostToDevice, E->st));
   return LV_OK;
 }
@@ -1001,9 +1007,60 @@ lv_status issue_pass(lv_engine* E, const PassControl* ctl) {
 }
 
 lv_status check_device_error(lv_engine* E) {
+  if (E->sc_host->error == kErrBarrierTimeout) {
+    return fail(LV_ERR_TIMEOUT, "a grid barrier wait of the level kernel gave up");
+  }
   if (E->sc_host->error) {
     return fail(LV_ERR_LIMIT, "a device hash table overflowed (bounded probe gave up)");
   }
+  return LV_OK;
+}
+
+// A single graph's level runs as one persistent kernel (the batched and
+// served forms keep the per-kernel level graph: their passes compact the
+// lists of graphs still moving).
+bool use_level_kernel(const lv_engine* E) { return !E->batch && E->cfg.level_kernel; }
+
+// Algorithmic bytes of one pass per timing group (as issue_pass counts them).
+void pass_group_bytes(const lv_engine* E, double* out /*[K_COUNT]*/) {
+  for (int i = 0; i < K_COUNT; i++) out[i] = 0.0;
+  for (int b = 1; b <= kBuckets; b++) {
+    const uint32_t s = E->plan.cls_start[b];
+    const uint32_t e = (b == 7) ? E->plan.cls_start[9] : E->plan.cls_start[b + 1];
+    const double v7 = (double)(E->plan.cls_start[b + 1] - s);
+    out[K_MOVE1 + b - 1] = (double)E->class_deg[b] * 12.0 + v7 * 32.0;
+    out[K_APPLY] += (double)(e - s) * 12.0;
+  }
+  out[K_HUB] = (double)E->class_deg[8] * 12.0 + (double)E->plan.hub_count * 32.0;
+  out[K_MODULARITY] = (double)E->e * 12.0 + (double)E->n * 24.0;
+}
+
+// The level's pass loop in one cooperative launch of the persistent level
+// kernel; the host waits once, for the level's result.
+lv_status run_level_loop(lv_engine* E, float min_gain) {
+  LVTRY(upload_desc(E, min_gain));
+  memset(E->loop_host, 0, sizeof(LevelLoopState));
+  E->loop_host->timing = E->profiling ? 1u : 0u;
+  CU(cudaMemcpyAsync(E->loop_state, E->loop_host, sizeof(LevelLoopState),
+                     cudaMemcpyHostToDevice, E->st));
+  CU(launch_level_loop(E->d_desc, engine_mode(E), E->st));
+  CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost, E->st));
+  if (E->profiling)
+    CU(cudaMemcpyAsync(E->loop_host, E->loop_state, sizeof(LevelLoopState),
+                       cudaMemcpyDeviceToHost, E->st));
+  CU(cudaStreamSynchronize(E->st));
+  if (E->profiling) {  // per-phase device time, as block 0 saw the barriers
+    double bytes[K_COUNT];
+    pass_group_bytes(E, bytes);
+    const double passes = (double)E->sc_host->passes;
+    for (int k = 0; k < kPhaseKinds; k++) {
+      if (!E->loop_host->phase_cnt[k]) continue;
+      E->kst[k].launches += E->loop_host->phase_cnt[k];
+      E->kst[k].ms += (double)E->loop_host->phase_ns[k] * 1e-6;
+      E->kst[k].bytes += bytes[k] * passes;
+    }
+  }
+  g_trace.mark("level kernel (all passes)", (uint32_t)E->levels.size(), E->n);
   return LV_OK;
 }
 
@@ -1546,6 +1603,7 @@ void lv_config_default(lv_config* cfg) {
   cfg->use_graphs = 1;
   cfg->stream = nullptr;
   cfg->gain = LV_GAIN_FP32;
+  cfg->level_kernel = 1;
 }
 
 lv_status lv_engine_create(const lv_config* cfg, lv_engine** out) {
@@ -1605,6 +1663,8 @@ lv_status lv_engine_create(const lv_config* cfg, lv_engine** out) {
   }
   if ((ce = cudaMalloc(&E->sc, sizeof(LevelScalars))) != cudaSuccess ||
       (ce = cudaMalloc(&E->d_desc, sizeof(PassDesc))) != cudaSuccess ||
+      (ce = cudaMalloc(&E->loop_state, sizeof(LevelLoopState))) != cudaSuccess ||
+      (ce = cudaMallocHost(&E->loop_host, sizeof(LevelLoopState))) != cudaSuccess ||
       (ce = cudaMallocHost(&E->sc_host, sizeof(LevelScalars))) != cudaSuccess ||
       (ce = cudaMallocHost(&E->h_counts, 32 * sizeof(uint32_t))) != cudaSuccess ||
       (ce = cudaEventCreate(&E->ev0)) != cudaSuccess ||
@@ -1641,6 +1701,8 @@ void lv_engine_destroy(lv_engine* E) {
   dfree(E->d_class_deg);
   if (E->sc) cudaFree(E->sc);
   if (E->d_desc) cudaFree(E->d_desc);
+  if (E->loop_state) cudaFree(E->loop_state);
+  if (E->loop_host) cudaFreeHost(E->loop_host);
   if (E->sc_host) cudaFreeHost(E->sc_host);
   if (E->h_counts) cudaFreeHost(E->h_counts);
   if (E->ev0) cudaEventDestroy(E->ev0);
@@ -1711,6 +1773,13 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
     ret = 0;
     act = old = 0.0;
     info.q_start = 0.0;
+  } else if (use_level_kernel(E)) {
+    LVTRY(run_level_loop(E, min_gain));
+    LVTRY(check_device_error(E));
+    passes = E->sc_host->passes;
+    ret = E->sc_host->first_fail ? 0 : 1;
+    act = E->sc_host->q;
+    old = E->sc_host->q_before;
   } else if (E->cfg.use_graphs && !E->profiling) {
     LVTRY(run_level_graph(E, min_gain));
     LVTRY(check_device_error(E));

@@ -263,6 +263,24 @@ struct DispatchArgs {
 // memory: the kernels of a pass read it at launch, so one captured pass
 // graph serves every level and every run (only this block is rewritten
 // between levels), and its grids are fixed.
+// Persistent level kernel (single graph): its grid barrier and per-phase
+// timers, in device memory, reset before every launch.  Phase kinds are
+// numbered as the engine's timing groups: 0..6 the moves of buckets 1..7
+// (bucket 7's phase includes the hubs' split pass), 7 the hubs' merge and
+// decide passes, 8 apply, 9 the modularity sweep.
+constexpr int kPhaseKinds = 10;
+struct LevelLoopState {
+  unsigned long long arrived;  // barrier arrivals of this launch (monotonic)
+  uint32_t abort;              // a barrier wait gave up: every block leaves
+  uint32_t timing;             // record per-phase device time
+  unsigned long long phase_ns[kPhaseKinds];
+  unsigned long long phase_cnt[kPhaseKinds];
+};
+// LevelScalars::error values: a bounded hash probe gave up / a barrier wait
+// of the persistent level kernel gave up.
+constexpr uint32_t kErrTableFull = 1u;
+constexpr uint32_t kErrBarrierTimeout = 2u;
+
 struct PassDesc {
   LevelView L;
   DispatchArgs A;              // class lists, plan, hub chunks, partials
@@ -282,6 +300,10 @@ struct PassDesc {
   // device-side pass loop
   double min_gain;
   uint32_t max_passes;
+  // persistent level kernel: move kernel variant of every bucket, and its
+  // barrier / timer state
+  uint8_t tune[8];
+  LevelLoopState* loop;
 };
 
 // rowid[j] = the row holding entry j of a CSR of n rows and nnz entries.
@@ -303,6 +325,15 @@ cudaError_t launch_apply_bucket(const PassDesc* D, int bucket, bool compacted, c
 // Modularity sweep of the pass; with ctl->enabled also the stop rule
 // (limits from D), with ctl->use_handle the WHILE node's condition.
 cudaError_t launch_modularity_pass(const PassDesc* D, const PassControl* ctl, cudaStream_t st);
+// The whole pass loop of a single graph's level (modularity.cu:466-508) in
+// one cooperative launch of a persistent kernel: every bucket step, apply
+// and modularity sweep separated by grid-wide barriers (waits bounded in
+// time; a wait that gives up sets kErrBarrierTimeout and ends the kernel),
+// the stop rule evaluated identically by every block.  D->loop must be
+// zeroed (timing flag aside) before the launch.
+cudaError_t launch_level_loop(const PassDesc* D, int mode, cudaStream_t st);
+// Blocks of that launch (co-resident: a multiple of the SM count).
+unsigned level_loop_grid(int mode);
 // Batched form: compacts the class lists to the graphs still moving
 // (skipped on the device while no graph stopped in the last pass).
 cudaError_t launch_compact_active(const PassDesc* D, cudaStream_t st);

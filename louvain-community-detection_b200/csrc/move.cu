@@ -44,6 +44,7 @@
 //     only (FP64 atomics), instead of a full recount after every bucket.
 #include "lv_internal.h"
 
+#include <algorithm>
 #include <cfloat>
 
 namespace lvb {
@@ -323,10 +324,14 @@ __device__ __forceinline__ uint32_t table_insert(uint32_t* keys, uint32_t mask,
 // Move kernels
 // ---------------------------------------------------------------------------
 
-// deg <= G: G lanes per vertex, one edge per lane.
+// Every kernel body below takes its block's index and the number of blocks
+// sharing the work (a grid-stride loop over work units), and its shared
+// memory from the caller: the standalone kernels pass blockIdx/gridDim and
+// their own shared arrays, the persistent level kernel the same body with
+// its one shared-memory arena.
 template <int G, int MODE>
-__global__ void __launch_bounds__(kThreads, kSmallPerSM)
-    move_small_kernel(const PassDesc* __restrict__ D, int cls) {
+__device__ __forceinline__ void small_body(const PassDesc* __restrict__ D, int cls,
+                                           uint32_t bid, uint32_t nblk, double (*sums)[32]) {
   constexpr int RULE = ModeOf<MODE>::kRule, PREC = ModeOf<MODE>::kPrec;
   using K = typename BestOf<PREC>::T;
   const LevelView L = D->L;
@@ -335,12 +340,10 @@ __global__ void __launch_bounds__(kThreads, kSmallPerSM)
   uint32_t* __restrict__ prop = D->prop + s0;
   // batched form: the class's active vertices
   const uint32_t count = D->act_cnt ? D->act_cnt[cls] : D->A.P.cls_start[cls + 1] - s0;
-  __shared__ double sums[kWarps][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int gl = lane & (G - 1);
   const uint32_t per_block = kThreads / G;
-  for (uint32_t base = blockIdx.x * per_block; base < count;
-       base += gridDim.x * per_block) {
+  for (uint32_t base = bid * per_block; base < count; base += nblk * per_block) {
     const uint32_t vidx = base + threadIdx.x / G;
     const bool vvalid = vidx < count;
     uint32_t v = 0, d = 0, cv = 0;
@@ -403,6 +406,14 @@ __global__ void __launch_bounds__(kThreads, kSmallPerSM)
   }
 }
 
+// deg <= G: G lanes per vertex, one edge per lane.
+template <int G, int MODE>
+__global__ void __launch_bounds__(kThreads, kSmallPerSM)
+    move_small_kernel(const PassDesc* __restrict__ D, int cls) {
+  __shared__ double sums[kWarps][32];
+  small_body<G, MODE>(D, cls, blockIdx.x, gridDim.x, sums);
+}
+
 // Best candidate among the taken slots of the first tv slots (nthr
 // threads from tid, four slots per thread at a time so the gathers
 // overlap); each thread empties the taken slots it read, leaving the table
@@ -446,22 +457,20 @@ __device__ __forceinline__ typename BestOf<PREC>::T scan_table_and_clear(
 // row's loads (at most MAXW waves of 32) are issued before any insertion,
 // so a vertex costs one memory latency chain instead of one per wave.
 template <int T, int MAXW, int MODE>
-__global__ void __launch_bounds__(kThreads, T == 128 ? kWarp128PerSM : kWarp512PerSM)
-    move_warp_kernel(const PassDesc* __restrict__ D, int cls) {
+__device__ __forceinline__ void warp_body(const PassDesc* __restrict__ D, int cls, uint32_t bid,
+                                          uint32_t nblk, unsigned char* smem_raw) {
   constexpr int RULE = ModeOf<MODE>::kRule, PREC = ModeOf<MODE>::kPrec;
   const LevelView L = D->L;
   const uint32_t s0 = D->A.P.cls_start[cls];
   const uint32_t* __restrict__ verts = D->A.order + s0;
   uint32_t* __restrict__ prop = D->prop + s0;
   const uint32_t count = D->act_cnt ? D->act_cnt[cls] : D->A.P.cls_start[cls + 1] - s0;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   double* vals = reinterpret_cast<double*>(smem_raw) + wib * T;
   uint32_t* keys =
       reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T * kWarps) + wib * T;
   uint32_t clean = 0;  // leading table slots known to be empty
-  for (uint32_t vidx = blockIdx.x * kWarps + wib; vidx < count;
-       vidx += gridDim.x * kWarps) {
+  for (uint32_t vidx = bid * kWarps + wib; vidx < count; vidx += nblk * kWarps) {
     const uint32_t v = verts[vidx];
     const uint64_t s = L.off[v];
     const uint32_t d = (uint32_t)(L.off[v + 1] - s);
@@ -529,6 +538,13 @@ __global__ void __launch_bounds__(kThreads, T == 128 ? kWarp128PerSM : kWarp512P
     if (lane == 0) prop[vidx] = decide<RULE>(best, own, g);
     __syncwarp();
   }
+}
+
+template <int T, int MAXW, int MODE>
+__global__ void __launch_bounds__(kThreads, T == 128 ? kWarp128PerSM : kWarp512PerSM)
+    move_warp_kernel(const PassDesc* __restrict__ D, int cls) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  warp_body<T, MAXW, MODE>(D, cls, blockIdx.x, gridDim.x, smem_raw);
 }
 
 template <class K>
@@ -603,10 +619,11 @@ __device__ __forceinline__ void insert_block_range(const LevelView& L, uint64_t 
   }
 }
 
-// 319 < deg <= 2048: one block per vertex, shared 4096-slot table.
 template <int MODE>
-__global__ void __launch_bounds__(kThreads, kBlockPerSM)
-    move_block_kernel(const PassDesc* __restrict__ D, int cls) {
+__device__ __forceinline__ void block_body(const PassDesc* __restrict__ D, int cls, uint32_t bid,
+                                           uint32_t nblk, unsigned char* smem_raw,
+                                           typename BestOf<ModeOf<MODE>::kPrec>::T* red_best,
+                                           double* red_own) {
   constexpr int RULE = ModeOf<MODE>::kRule, PREC = ModeOf<MODE>::kPrec;
   using K = typename BestOf<PREC>::T;
   const LevelView L = D->L;
@@ -614,15 +631,12 @@ __global__ void __launch_bounds__(kThreads, kBlockPerSM)
   const uint32_t* __restrict__ verts = D->A.order + s0;
   uint32_t* __restrict__ prop = D->prop + s0;
   const uint32_t count = D->act_cnt ? D->act_cnt[cls] : D->A.P.cls_start[cls + 1] - s0;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int T = kHubSmemSlots;
   constexpr int MAXW = (int)(kHubSmemMaxDeg / kThreads);
   double* vals = reinterpret_cast<double*>(smem_raw);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T);
-  __shared__ K red_best[kWarps];
-  __shared__ double red_own[kWarps];
   uint32_t clean = 0;  // leading table slots known to be empty
-  for (uint32_t vidx = blockIdx.x; vidx < count; vidx += gridDim.x) {
+  for (uint32_t vidx = bid; vidx < count; vidx += nblk) {
     const uint32_t v = verts[vidx];
     const uint64_t s = L.off[v];
     const uint32_t d = (uint32_t)(L.off[v + 1] - s);
@@ -659,6 +673,16 @@ __global__ void __launch_bounds__(kThreads, kBlockPerSM)
     if (threadIdx.x == 0) prop[vidx] = decide<RULE>(best, own, g);
     __syncthreads();
   }
+}
+
+// 319 < deg <= 2048: one block per vertex, shared 4096-slot table.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, kBlockPerSM)
+    move_block_kernel(const PassDesc* __restrict__ D, int cls) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ typename BestOf<ModeOf<MODE>::kPrec>::T red_best[kWarps];
+  __shared__ double red_own[kWarps];
+  block_body<MODE>(D, cls, blockIdx.x, gridDim.x, smem_raw, red_best, red_own);
 }
 
 // deg > 2048 (hubs).  The neighbour communities of a hub are split into P
@@ -712,8 +736,9 @@ __device__ __forceinline__ uint32_t block_scan_inplace(uint32_t* a, uint32_t n,
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kThreads, kSplitPerSM)
-    hub_split_kernel(const PassDesc* __restrict__ D) {
+__device__ __forceinline__ void split_body(const PassDesc* __restrict__ D, uint32_t bid,
+                                           uint32_t nblk, uint32_t* cnt, uint32_t* wsum,
+                                           double* red) {
   constexpr int RULE = ModeOf<MODE>::kRule;
   const LevelView L = D->L;
   const uint32_t* __restrict__ hubs = D->A.order + D->A.P.cls_start[8];
@@ -723,10 +748,7 @@ __global__ void __launch_bounds__(kThreads, kSplitPerSM)
   const uint32_t* __restrict__ blk_ch = D->A.hub_blk_chunk;
   constexpr int EPT = kHubChunk / kThreads;  // entries per thread
   static_assert(EPT * kThreads == (int)kHubChunk, "chunk = whole waves");
-  __shared__ uint32_t cnt[kHubMaxParts];
-  __shared__ uint32_t wsum[kWarps];
-  __shared__ double red[kWarps];
-  for (uint32_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
+  for (uint32_t b = bid; b < nblocks; b += nblk) {
     const uint32_t hi = blk_hub[b], ch = blk_ch[b];
     const uint32_t v = hubs[hi];
     if (!vertex_active(L, v)) continue;  // block-uniform
@@ -802,26 +824,34 @@ __global__ void __launch_bounds__(kThreads, kSplitPerSM)
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kThreads, kMergePerSM)
-    hub_merge_kernel(const PassDesc* __restrict__ D) {
+__global__ void __launch_bounds__(kThreads, kSplitPerSM)
+    hub_split_kernel(const PassDesc* __restrict__ D) {
+  __shared__ uint32_t cnt[kHubMaxParts];
+  __shared__ uint32_t wsum[kWarps];
+  __shared__ double red[kWarps];
+  split_body<MODE>(D, blockIdx.x, gridDim.x, cnt, wsum, red);
+}
+
+template <int MODE>
+__device__ __forceinline__ void merge_body(const PassDesc* __restrict__ D, uint32_t bid,
+                                           uint32_t nblk, unsigned char* smem_raw,
+                                           typename BestOf<ModeOf<MODE>::kPrec>::T* red_best,
+                                           uint32_t* seg_a, uint32_t* seg_pre, uint32_t* wsum) {
   constexpr int PREC = ModeOf<MODE>::kPrec;
   using K = typename BestOf<PREC>::T;
   const LevelView L = D->L;
   const uint32_t* __restrict__ hubs = D->A.order + D->A.P.cls_start[8];
   const HubArena H = D->H;
   const uint32_t units = H.units;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int T = kHubPartSlots;
   double* vals = reinterpret_cast<double*>(smem_raw);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T);
-  __shared__ K red_best[kWarps];
-  __shared__ uint32_t seg_a[kThreads], seg_pre[kThreads], wsum[kWarps];
   for (uint32_t i = threadIdx.x; i < T; i += kThreads) {
     keys[i] = kEmptyKey;
     vals[i] = 0.0;
   }
   __syncthreads();
-  for (uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
+  for (uint32_t u = bid; u < units; u += nblk) {
     const uint32_t hi = H.blk_vertex[u], part = H.blk_chunk[u];
     const uint32_t P = H.blk_nchunks[u];
     const uint32_t v = hubs[hi];
@@ -878,7 +908,17 @@ __global__ void __launch_bounds__(kThreads, kMergePerSM)
 }
 
 template <int MODE>
-__global__ void hub_decide_kernel(const PassDesc* __restrict__ D) {
+__global__ void __launch_bounds__(kThreads, kMergePerSM)
+    hub_merge_kernel(const PassDesc* __restrict__ D) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ typename BestOf<ModeOf<MODE>::kPrec>::T red_best[kWarps];
+  __shared__ uint32_t seg_a[kThreads], seg_pre[kThreads], wsum[kWarps];
+  merge_body<MODE>(D, blockIdx.x, gridDim.x, smem_raw, red_best, seg_a, seg_pre, wsum);
+}
+
+template <int MODE>
+__device__ __forceinline__ void decide_body(const PassDesc* __restrict__ D, uint32_t bid,
+                                            uint32_t nblk) {
   constexpr int RULE = ModeOf<MODE>::kRule, PREC = ModeOf<MODE>::kPrec;
   using K = typename BestOf<PREC>::T;
   const LevelView L = D->L;
@@ -886,8 +926,7 @@ __global__ void hub_decide_kernel(const PassDesc* __restrict__ D) {
   const HubArena H = D->H;
   const uint32_t hub_count = D->A.P.hub_count;
   uint32_t* __restrict__ prop = D->prop + D->A.P.cls_start[8];
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < hub_count;
-       i += gridDim.x * blockDim.x) {
+  for (uint32_t i = bid * blockDim.x + threadIdx.x; i < hub_count; i += nblk * blockDim.x) {
     const uint32_t v = hubs[i];
     const GainCtx g = make_ctx<PREC>(L, v, L.comm[v]);
     K best{};
@@ -907,20 +946,26 @@ __global__ void hub_decide_kernel(const PassDesc* __restrict__ D) {
   }
 }
 
+template <int MODE>
+__global__ void hub_decide_kernel(const PassDesc* __restrict__ D) {
+  decide_body<MODE>(D, blockIdx.x, gridDim.x);
+}
+
 // Applies a bucket's proposals (assignCommunity + incremental totals).
-__global__ void __launch_bounds__(kThreads, kSweepPerSM)
-    apply_kernel(const PassDesc* __restrict__ D, int lo_cls, int hi_cls) {
+__device__ __forceinline__ void apply_body(const PassDesc* __restrict__ D, int lo_cls,
+                                           int hi_cls, uint32_t bid, uint32_t nblk) {
   // classes lo..hi are adjacent in the lists (bucket 7 without compaction:
   // classes 7 and 8); with compaction a class's active prefix
   const LevelView L = D->L;
   const uint32_t s0 = D->A.P.cls_start[lo_cls];
   const uint32_t* __restrict__ verts = D->A.order + s0;
-  const uint32_t* __restrict__ prop = D->prop + s0;
+  // written by the move phase of the same persistent launch: a plain
+  // (coherent) load, never the read-only path
+  const uint32_t* prop = D->prop + s0;
   const uint32_t count = (D->act_cnt && lo_cls <= kMoveClasses)
                              ? D->act_cnt[lo_cls]
                              : D->A.P.cls_start[hi_cls + 1] - s0;
-  for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < count;
-       i += gridDim.x * kThreads) {
+  for (uint32_t i = bid * kThreads + threadIdx.x; i < count; i += nblk * kThreads) {
     const uint32_t v = verts[i];
     const uint32_t nc = prop[i];
     const uint32_t oc = L.comm[v];
@@ -933,6 +978,11 @@ __global__ void __launch_bounds__(kThreads, kSweepPerSM)
       L.comm[v] = nc;
     }
   }
+}
+
+__global__ void __launch_bounds__(kThreads, kSweepPerSM)
+    apply_kernel(const PassDesc* __restrict__ D, int lo_cls, int hi_cls) {
+  apply_body(D, lo_cls, hi_cls, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1236,10 +1286,10 @@ __global__ void __launch_bounds__(kThreads)
 // themselves -- every load coalesced but the two community gathers, four
 // independent entries per thread in flight.
 __device__ __forceinline__ double intra_sweep(const LevelView& L, const uint32_t* rowid,
-                                             uint64_t nnz) {
+                                             uint64_t nnz, uint32_t bid, uint32_t nblk) {
   double part = 0.0;
-  const uint64_t stride = (uint64_t)gridDim.x * kThreads * 4;
-  for (uint64_t b = (uint64_t)blockIdx.x * kThreads * 4 + threadIdx.x; b < nnz; b += stride) {
+  const uint64_t stride = (uint64_t)nblk * kThreads * 4;
+  for (uint64_t b = (uint64_t)bid * kThreads * 4 + threadIdx.x; b < nnz; b += stride) {
     uint32_t r[4], c[4];
     float w[4];
 #pragma unroll
@@ -1269,7 +1319,7 @@ __device__ __forceinline__ void modularity_body(const LevelView& L, const Dispat
   __shared__ double red[kWarps];
   double part = 0.0;
   if (rowid && !L.gid) {
-    part = intra_sweep(L, rowid, nnz);
+    part = intra_sweep(L, rowid, nnz, blockIdx.x, gridDim.x);
   } else {
     dispatch_units(L, A, IntraOp{}, part, red);
   }
@@ -1384,6 +1434,245 @@ __global__ void pass_control_init_kernel(const PassDesc* __restrict__ D) {
     s.q_before = s.q;
     // nothing moves in an edgeless graph, nor in one the host froze
     s.active = (s.m64 > 0.0 && !s.frozen) ? 1u : 0u;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent level kernel: a single graph's whole pass loop in one launch.
+// The reference runs every bucket step, community update and modularity
+// reduction as separate launches with host round trips
+// (modularity.cu:466-508); here they are phases of one cooperative kernel
+// separated by grid-wide barriers, so a pass costs no launch at all.  The
+// phases run the same bodies as the standalone kernels, on one shared-memory
+// arena sized for the largest table (the G-lane sums and the hub split's
+// partition counters alias it).
+// ---------------------------------------------------------------------------
+constexpr int kLoopPerSM = 4;
+constexpr int kLoopSmem = kBlockTabSmem;
+static_assert(kLoopSmem >= kWarps * 512 * kSlotBytes && kLoopSmem >= kHubPartSmem &&
+                  kLoopSmem >= (int)(kHubMaxParts * sizeof(uint32_t)) &&
+                  kLoopSmem >= (int)(kWarps * 32 * sizeof(double)),
+              "every phase's shared memory fits the arena");
+// A barrier wait longer than this is a fault (a phase of the largest graphs
+// lasts milliseconds): the block sets the abort flag and the kernel ends.
+constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid-wide barrier (every block is co-resident: cooperative launch).
+// `epoch` counts the barriers this block has passed, so barrier k completes
+// when k * nblk arrivals have been counted.  Returns false when the kernel
+// must end: this block's wait gave up (it sets the abort flag and the error)
+// or another block's did.
+__device__ __forceinline__ bool grid_barrier(LevelLoopState* S, uint32_t nblk,
+                                             unsigned long long& epoch, uint32_t* err,
+                                             int* ok_sm) {
+  __syncthreads();
+  epoch++;
+  if (threadIdx.x == 0) {
+    const unsigned long long target = epoch * nblk;
+    __threadfence();  // this block's writes before its arrival
+    atomicAdd(&S->arrived, 1ull);
+    int ok = 1;
+    const unsigned long long t0 = global_ns();
+    while (ld_acquire_u64(&S->arrived) < target) {
+      if (*(volatile uint32_t*)&S->abort) {
+        ok = 0;
+        break;
+      }
+      if (global_ns() - t0 > kBarrierTimeoutNs) {
+        atomicExch(&S->abort, 1u);
+        atomicExch(err, kErrBarrierTimeout);
+        ok = 0;
+        break;
+      }
+      __nanosleep(32);
+    }
+    __threadfence();
+    *ok_sm = ok;
+  }
+  __syncthreads();
+  return *ok_sm != 0;
+}
+
+// The phases are called, not inlined: each body gets the register budget
+// to itself instead of sharing one allocation across the whole loop.
+template <int G, int MODE>
+__device__ __noinline__ void small_phase(const PassDesc* __restrict__ D, int cls, uint32_t bid,
+                                         uint32_t nblk, unsigned char* smem) {
+  small_body<G, MODE>(D, cls, bid, nblk, reinterpret_cast<double(*)[32]>(smem));
+}
+template <int T, int MAXW, int MODE>
+__device__ __noinline__ void warp_phase(const PassDesc* __restrict__ D, int cls, uint32_t bid,
+                                        uint32_t nblk, unsigned char* smem) {
+  warp_body<T, MAXW, MODE>(D, cls, bid, nblk, smem);
+}
+template <int MODE>
+__device__ __noinline__ void block_phase(const PassDesc* __restrict__ D, int cls, uint32_t bid,
+                                         uint32_t nblk, unsigned char* smem,
+                                         typename BestOf<ModeOf<MODE>::kPrec>::T* red_best,
+                                         double* red_d) {
+  block_body<MODE>(D, cls, bid, nblk, smem, red_best, red_d);
+}
+template <int MODE>
+__device__ __noinline__ void split_phase(const PassDesc* __restrict__ D, uint32_t bid,
+                                         uint32_t nblk, unsigned char* smem, uint32_t* wsum,
+                                         double* red_d) {
+  split_body<MODE>(D, bid, nblk, reinterpret_cast<uint32_t*>(smem), wsum, red_d);
+}
+template <int MODE>
+__device__ __noinline__ void merge_phase(const PassDesc* __restrict__ D, uint32_t bid,
+                                         uint32_t nblk, unsigned char* smem,
+                                         typename BestOf<ModeOf<MODE>::kPrec>::T* red_best,
+                                         uint32_t* seg_a, uint32_t* seg_pre, uint32_t* wsum) {
+  merge_body<MODE>(D, bid, nblk, smem, red_best, seg_a, seg_pre, wsum);
+}
+template <int MODE>
+__device__ __noinline__ void decide_phase(const PassDesc* __restrict__ D, uint32_t bid,
+                                          uint32_t nblk) {
+  decide_body<MODE>(D, bid, nblk);
+}
+__device__ __noinline__ void apply_phase(const PassDesc* __restrict__ D, int lo, int hi,
+                                         uint32_t bid, uint32_t nblk) {
+  apply_body(D, lo, hi, bid, nblk);
+}
+// This block's shares of the intra-community weight and of the squared
+// community totals (modularity.cu:400-436), in partials[bid] and
+// partials[nblk + bid].
+__device__ __noinline__ void modularity_share_phase(const PassDesc* __restrict__ D, uint32_t bid,
+                                                    uint32_t nblk, double* red_d) {
+  const LevelView L = D->L;
+  double part = intra_sweep(L, D->rowid, D->nnz, bid, nblk);
+  const uint32_t chunk = (L.n + nblk - 1) / nblk;
+  const uint32_t c0 = bid * chunk, c1 = min(L.n, c0 + chunk);
+  double asq = 0.0;
+  for (uint32_t c = c0 + threadIdx.x; c < c1; c += kThreads) {
+    const double a = L.tot[c];
+    asq += a * a;
+  }
+  part = block_sum(part, red_d);
+  asq = block_sum(asq, red_d);
+  if (threadIdx.x == 0) {
+    D->A.partials[bid] = part;
+    D->A.partials[nblk + bid] = asq;
+  }
+}
+
+template <int MODE>
+__device__ __forceinline__ void run_variant(int kv, const PassDesc* __restrict__ D, int cls,
+                                            uint32_t bid, uint32_t nblk, unsigned char* smem,
+                                            typename BestOf<ModeOf<MODE>::kPrec>::T* red_best,
+                                            double* red_d) {
+  switch (kv) {
+    case KV_SMALL4: small_phase<4, MODE>(D, cls, bid, nblk, smem); break;
+    case KV_SMALL8: small_phase<8, MODE>(D, cls, bid, nblk, smem); break;
+    case KV_SMALL16: small_phase<16, MODE>(D, cls, bid, nblk, smem); break;
+    case KV_SMALL32: small_phase<32, MODE>(D, cls, bid, nblk, smem); break;
+    case KV_WARP128: warp_phase<128, 3, MODE>(D, cls, bid, nblk, smem); break;
+    case KV_WARP512: warp_phase<512, 10, MODE>(D, cls, bid, nblk, smem); break;
+    default: block_phase<MODE>(D, cls, bid, nblk, smem, red_best, red_d); break;
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, kLoopPerSM)
+    level_loop_kernel(const PassDesc* __restrict__ D) {
+  using K = typename BestOf<ModeOf<MODE>::kPrec>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ K red_best[kWarps];
+  __shared__ double red_d[kWarps];
+  __shared__ uint32_t seg_a[kThreads], seg_pre[kThreads], wsum[kWarps];
+  __shared__ int ok_sm;
+  __shared__ double q_sm[3];
+  const uint32_t bid = blockIdx.x, nblk = gridDim.x;
+  LevelLoopState* S = D->loop;
+  const LevelView L = D->L;
+  LevelScalars* sc = L.sc;
+  const DispatchArgs& A = D->A;
+  const bool timer = S->timing && bid == 0 && threadIdx.x == 0;
+  unsigned long long epoch = 0, t_prev = timer ? global_ns() : 0ull;
+  // ends a phase: barrier, then (timing) the phase's device time as block 0
+  // saw it -- from the previous barrier's exit to this one's
+  auto phase_end = [&](int kind) -> bool {
+    if (!grid_barrier(S, nblk, epoch, &sc->error, &ok_sm)) return false;
+    if (timer) {
+      const unsigned long long t = global_ns();
+      S->phase_ns[kind] += t - t_prev;
+      S->phase_cnt[kind] += 1ull;
+      t_prev = t;
+    }
+    return true;
+  };
+  // pass control (modularity.cu:466-508); every block holds the same copy
+  double q_prev = sc->q;
+  uint32_t passes = 0, first_fail = 0;
+  const double min_gain = D->min_gain;
+  const uint32_t max_passes = D->max_passes;
+  const bool hubs = A.P.hub_count > 0;
+  for (;;) {
+    for (int b = 1; b <= kBuckets; b++) {
+      const bool has = A.P.cls_start[b + 1] > A.P.cls_start[b];
+      const bool hb = b == kBuckets && hubs;
+      if (!has && !hb) continue;  // uniform: the plan is the level's
+      if (has) run_variant<MODE>(D->tune[b], D, b, bid, nblk, smem_raw, red_best, red_d);
+      if (hb) {
+        split_phase<MODE>(D, bid, nblk, smem_raw, wsum, red_d);
+        if (!phase_end(b - 1)) return;
+        merge_phase<MODE>(D, bid, nblk, smem_raw, red_best, seg_a, seg_pre, wsum);
+        if (!phase_end(7)) return;
+        decide_phase<MODE>(D, bid, nblk);
+        if (!phase_end(7)) return;
+      } else if (!phase_end(b - 1)) {
+        return;
+      }
+      apply_phase(D, b, hb ? 8 : b, bid, nblk);
+      if (!phase_end(8)) return;
+    }
+    // modularity of the pass: this block's shares ...
+    modularity_share_phase(D, bid, nblk, red_d);
+    if (!phase_end(9)) return;
+    // ... then every block sums all shares in the same fixed order, so all
+    // blocks hold the same Q and take the same stop decision
+    double x = 0.0, y = 0.0;
+    for (uint32_t i = threadIdx.x; i < nblk; i += kThreads) {
+      x += __ldcg(&A.partials[i]);
+      y += __ldcg(&A.partials[nblk + i]);
+    }
+    x = block_sum(x, red_d);
+    y = block_sum(y, red_d);
+    if (threadIdx.x == 0) {
+      const double m = sc->m64;
+      q_sm[0] = (m > 0.0) ? (x / (2.0 * m)) - (y / (4.0 * m * m)) : 0.0;
+      q_sm[1] = x;
+      q_sm[2] = y;
+    }
+    __syncthreads();
+    const double q = q_sm[0];
+    // stop rule of modularity.cu:501-508 / louvian.py:91-99
+    passes++;
+    if (passes == 1 && q - q_prev < min_gain) first_fail = 1u;
+    const bool cont = (q - q_prev >= min_gain) && passes < max_passes;
+    if (bid == 0 && threadIdx.x == 0) {
+      sc->q = q;
+      sc->intra = q_sm[1];
+      sc->asq = q_sm[2];
+      sc->passes = passes;
+      sc->first_fail = first_fail;
+      sc->q_before = q_prev;
+      sc->q_prev = q;
+      sc->any_active = cont ? 1u : 0u;
+    }
+    q_prev = q;
+    if (!cont) break;
   }
 }
 
@@ -1567,8 +1856,18 @@ static cudaError_t configure_mode() {
                               cudaFuncAttributeMaxDynamicSharedMemorySize, kHubPartSmem);
 }
 
+template <int MODE>
+static cudaError_t configure_loop() {
+  return cudaFuncSetAttribute(level_loop_kernel<MODE>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, kLoopSmem);
+}
+
 cudaError_t configure_kernels() {
   cudaError_t e;
+  if ((e = configure_loop<0>()) != cudaSuccess) return e;
+  if ((e = configure_loop<1>()) != cudaSuccess) return e;
+  if ((e = configure_loop<2>()) != cudaSuccess) return e;
+  if ((e = configure_loop<3>()) != cudaSuccess) return e;
   if ((e = configure_mode<0>()) != cudaSuccess) return e;
   if ((e = configure_mode<1>()) != cudaSuccess) return e;
   if ((e = configure_mode<2>()) != cudaSuccess) return e;
@@ -1709,6 +2008,49 @@ cudaError_t launch_move_bucket(const PassDesc* D, int bucket, int mode, const ui
     case 1: return move_bucket_impl<1>(D, bucket, variant, st);
     case 2: return move_bucket_impl<2>(D, bucket, variant, st);
     case 3: return move_bucket_impl<3>(D, bucket, variant, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int MODE>
+static unsigned loop_grid_impl() {
+  static int per_sm = -1;  // co-resident blocks of the kernel, once per process
+  if (per_sm < 0) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, level_loop_kernel<MODE>, kThreads,
+                                                      kLoopSmem) != cudaSuccess)
+      b = 0;
+    per_sm = std::min(b, kLoopPerSM);
+  }
+  return (unsigned)per_sm * sm_count();
+}
+
+unsigned level_loop_grid(int mode) {
+  switch (mode) {
+    case 0: return loop_grid_impl<0>();
+    case 1: return loop_grid_impl<1>();
+    case 2: return loop_grid_impl<2>();
+    case 3: return loop_grid_impl<3>();
+    default: return 0;
+  }
+}
+
+template <int MODE>
+static cudaError_t launch_loop_impl(const PassDesc* D, cudaStream_t st) {
+  const unsigned grid = loop_grid_impl<MODE>();
+  if (!grid) return cudaErrorCooperativeLaunchTooLarge;
+  void* args[] = {(void*)&D};
+  count_launches(1);
+  return cudaLaunchCooperativeKernel((const void*)level_loop_kernel<MODE>, dim3(grid),
+                                     dim3(kThreads), args, kLoopSmem, st);
+}
+
+cudaError_t launch_level_loop(const PassDesc* D, int mode, cudaStream_t st) {
+  switch (mode) {
+    case 0: return launch_loop_impl<0>(D, st);
+    case 1: return launch_loop_impl<1>(D, st);
+    case 2: return launch_loop_impl<2>(D, st);
+    case 3: return launch_loop_impl<3>(D, st);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -43,6 +43,7 @@ class Config(ctypes.Structure):
         ("use_graphs", ctypes.c_int),
         ("stream", ctypes.c_void_p),
         ("gain", ctypes.c_int),
+        ("level_kernel", ctypes.c_int),
     ]
 
 
@@ -346,12 +347,13 @@ class RunResult:
 class Engine:
     def __init__(self, device: int = 0, rule: str = "py", max_passes: int = 0,
                  max_levels: int = 0, use_graphs: bool = True, stream: int = 0,
-                 gain: str = "fp32"):
+                 gain: str = "fp32", level_kernel: bool = True):
         cfg = Config()
         lib().lv_config_default(ctypes.byref(cfg))
         cfg.device = device
         cfg.rule = RULES[rule]
         cfg.gain = GAINS[gain]
+        cfg.level_kernel = int(level_kernel)
         cfg.max_passes = max_passes
         cfg.max_levels = max_levels
         cfg.use_graphs = int(use_graphs)

@@ -227,14 +227,16 @@ def test_run_device_equals_run():
     assert np.array_equal(d_asg.cpu().numpy().view(np.uint32), ref.assignment)
 
 
-@pytest.mark.parametrize("name", ["planted_small", "rmat11", "hub3000"])
-def test_graph_replay_equals_direct_launches(name):
-    """Capturing a level's pass in a CUDA graph changes nothing."""
+@pytest.mark.parametrize("name", ["planted_small", "rmat11", "hub3000", "star1000"])
+def test_pass_loop_forms_agree(name):
+    """Every way of running a level's pass loop gives the same run: the
+    persistent level kernel (default) with and without its phase timers,
+    the level graph (WHILE node), the host loop, and the per-pass replay of
+    a captured pass (the mode kernel timing uses without the level kernel)."""
     out = []
-    # host pass loop; device pass loop (graph WHILE node); per-pass replay
-    # of a captured pass (the mode kernel timing uses)
-    for ug, prof in ((False, False), (True, False), (True, True)):
-        with lvb200.Engine(rule="py", use_graphs=ug) as e:
+    for lk, ug, prof in ((True, True, False), (True, True, True), (False, True, False),
+                         (False, False, False), (False, True, True)):
+        with lvb200.Engine(rule="py", use_graphs=ug, level_kernel=lk) as e:
             e.set_profiling(prof)
             out.append(e.run(lvb200.Graph.load_mtx(golden_mtx(name)), 1e-6))
     for o in out[1:]:
@@ -242,6 +244,43 @@ def test_graph_replay_equals_direct_launches(name):
         assert np.array_equal(o.assignment, out[0].assignment)
         assert [l["passes"] for l in o.levels] == [l["passes"] for l in out[0].levels]
         assert [l["q_end"] for l in o.levels] == [l["q_end"] for l in out[0].levels]
+
+
+@pytest.mark.parametrize("rule", ["py", "cuda"])
+@pytest.mark.parametrize("gain", ["fp32", "fp64"])
+def test_level_kernel_equals_level_graph_at_scale(rule, gain):
+    """The power-law workload (every degree class) and an R-MAT graph with
+    hubs, under both rules and both gain arithmetics."""
+    for kind in ("planted", "rmat"):
+        if kind == "planted":
+            n, s, d, w = lvgen.planted_powerlaw(n=60000, target_edges=200000, seed=5)
+        else:
+            n, s, d, w = lvgen.rmat(15, edge_factor=16, seed=2)
+        off, col, ww = lvgen.csr_from_edges(n, s, d, w)
+        g = lvb200.Graph.from_csr(n, off, col, ww)
+        res = []
+        for lk in (True, False):
+            with lvb200.Engine(rule=rule, gain=gain, level_kernel=lk) as e:
+                res.append(e.run(g, 1e-6))
+        assert res[0].modularity == res[1].modularity
+        assert np.array_equal(res[0].assignment, res[1].assignment)
+        assert [l["passes"] for l in res[0].levels] == [l["passes"] for l in res[1].levels]
+
+
+def test_level_kernel_phase_timers(eng):
+    """With profiling on, the level kernel's barrier timestamps give every
+    phase kind a device time and a count."""
+    eng.set_profiling(True)
+    eng.reset_kernel_stats()
+    res = eng.run(lvb200.Graph.load_mtx(golden_mtx("hub3000")), 1e-6)
+    st = eng.kernel_stats()
+    eng.set_profiling(False)
+    passes = sum(l["passes"] for l in res.levels)
+    assert st["modularity"]["launches"] == passes
+    assert st["apply"]["launches"] >= passes
+    assert st["move_hub"]["launches"] >= 2
+    assert all(v["total_ms"] >= 0.0 for v in st.values())
+    assert st["modularity"]["total_ms"] > 0.0
 
 
 def test_kernel_profiling_counts(eng):
