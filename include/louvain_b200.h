@@ -75,9 +75,10 @@ typedef struct lv_config {
                                and replay it (default 1)                    */
     void *stream;           /* cudaStream_t to run on; NULL = own stream    */
     lv_gain gain;           /* gain arithmetic, default LV_GAIN_FP32        */
-    int level_kernel;       /* run a single graph's pass loop as one
-                               persistent kernel per level (default 1); 0:
-                               per-kernel launches, as use_graphs says      */
+    int level_kernel;       /* 1: run a single graph's pass loop as one
+                               persistent cooperative kernel per level; 0
+                               (default): per-kernel launches, in a level
+                               graph or from the host as use_graphs says    */
 } lv_config;
 
 /* Per-level record (the reference prints none of this; -v here adds it). */
@@ -386,6 +387,14 @@ lv_status lv_reset_kernel_stats(lv_engine *e);
 
 /* Kernels this library has launched in the process so far (all engines). */
 lv_status lv_get_launch_count(uint64_t *count);
+
+/* ---- fault injection, for tests (no counterpart in the reference, which
+ * exits on any CUDA error, utils.cuh:95-100) -------------------------------
+ * From this call on, the nth device allocation the library makes (n >= 1)
+ * fails as if the device were out of memory: the entry point that needed
+ * it returns LV_ERR_NOMEM and the engine stays usable (the next run
+ * allocates again).  n = 0 switches the injection off.  Process-wide.      */
+lv_status lv_debug_fail_device_alloc(uint64_t n);
 
 /* ---- modularity without allocation (no counterpart in the reference) ----
  * The FP64 modularity of lv_modularity_fp64 for a graph and partition that

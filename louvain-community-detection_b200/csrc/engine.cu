@@ -75,9 +75,17 @@ struct AllocScope {
   }
 };
 
+// Fault injection for tests (lv_debug_fail_device_alloc): the nth device
+// allocation after the hook is set fails as if the device were full.
+std::atomic<unsigned long long> g_alloc_count{0};
+std::atomic<unsigned long long> g_alloc_fail_at{0};
+
 template <typename T>
 cudaError_t dalloc(T** p, size_t count) {
   *p = nullptr;
+  const unsigned long long fail_at = g_alloc_fail_at.load(std::memory_order_relaxed);
+  if (fail_at && g_alloc_count.fetch_add(1, std::memory_order_relaxed) + 1 == fail_at)
+    return cudaErrorMemoryAllocation;
   if (count == 0) count = 1;
   if (t_alloc_stream && t_alloc_pool)
     return cudaMallocFromPoolAsync((void**)p, count * sizeof(T), t_alloc_pool, t_alloc_stream);
@@ -503,7 +511,10 @@ void free_state(lv_engine* E) {
 cudaError_t grow_tables(void* ctx, size_t slots, size_t entries) {
   lv_engine* E = static_cast<lv_engine*>(ctx);
   ContractBuffers& B = E->cb;
+  // a capacity is zeroed before its buffers are freed, so a failed
+  // allocation never leaves a freed buffer behind a stale capacity
   if (slots > B.table_cap) {
+    B.table_cap = 0;
     dfree(B.keys);
     dfree(B.vals);
     size_t cap = std::max<size_t>(slots, 1 << 16);
@@ -514,6 +525,7 @@ cudaError_t grow_tables(void* ctx, size_t slots, size_t entries) {
     B.table_cap = cap;
   }
   if (entries > B.g_cap) {
+    B.g_cap = 0;
     dfree(B.g_tab_off);
     dfree(B.g_tab_size);
     dfree(B.g_blk_comm);
@@ -612,6 +624,7 @@ lv_status prepare_level(lv_engine* E) {
   uint64_t stage_total = 0, ct_total = 0;
   if (hc) {
     if (hc > E->hub_count_cap) {
+      E->hub_count_cap = 0;  // zeroed before the frees (see grow_tables)
       HubArena& H = E->hub;
       dfree(E->hub_deg);
       dfree(H.best);
@@ -680,6 +693,7 @@ lv_status prepare_level(lv_engine* E) {
   const size_t need_partials =
       hc + 2 * (size_t)std::max(dispatch_grid(P), pass_dispatch_grid()) + 16;
   if (need_partials > E->partials_cap) {
+    E->partials_cap = 0;
     dfree(E->partials);
     CU(dalloc(&E->partials, need_partials));
     E->partials_cap = need_partials;
@@ -688,11 +702,13 @@ lv_status prepare_level(lv_engine* E) {
     const size_t hb = P.hub_blocks;
     const size_t hu = E->hub.units;
     if (hb > E->hub_blocks_cap) {
+      E->hub_blocks_cap = 0;
       dfree(E->hub_map);
       CU(dalloc(&E->hub_map, 2 * hb));
       E->hub_blocks_cap = hb;
     }
     if (hu > E->hub_units_cap) {
+      E->hub_units_cap = 0;
       dfree(E->hub.blk_vertex);
       dfree(E->hub.blk_chunk);
       dfree(E->hub.blk_nchunks);
@@ -719,6 +735,7 @@ lv_status prepare_level(lv_engine* E) {
     // split/merge plan: partitions, staging copy of the hub rows, chunk table
     HubArena& H = E->hub;
     if (stage_total > E->hub_stage_cap) {
+      E->hub_stage_cap = 0;
       dfree(H.stage_c);
       dfree(H.stage_w);
       CU(dalloc(&H.stage_c, stage_total));
@@ -726,6 +743,7 @@ lv_status prepare_level(lv_engine* E) {
       E->hub_stage_cap = stage_total;
     }
     if (ct_total > E->hub_ct_cap) {
+      E->hub_ct_cap = 0;
       dfree(H.ct);
       CU(dalloc(&H.ct, ct_total));
       E->hub_ct_cap = ct_total;
@@ -1098,6 +1116,7 @@ lv_status validate_sizes(uint32_t n, uint64_t e) {
 // ---------------------------------------------------------------------------
 lv_status batch_alloc(lv_engine* E, uint32_t G) {
   if (G <= E->graph_cap && E->gs) return LV_OK;
+  E->graph_cap = 0;
   dfree(E->gs);
   dfree(E->goff_dev);
   dfree(E->gbase);
@@ -1285,6 +1304,7 @@ static lv_status batch_run(lv_engine* E, uint32_t G, const uint64_t* goff_in,
   cudaStream_t st = E->st;
   const uint32_t n0 = E->n0;
   if (n0 > E->act_order_cap) {
+    E->act_order_cap = 0;
     dfree(E->act_order);
     CU(dalloc(&E->act_order, n0));
     E->act_order_cap = n0;
@@ -1603,7 +1623,7 @@ void lv_config_default(lv_config* cfg) {
   cfg->use_graphs = 1;
   cfg->stream = nullptr;
   cfg->gain = LV_GAIN_FP32;
-  cfg->level_kernel = 1;
+  cfg->level_kernel = 0;
 }
 
 lv_status lv_engine_create(const lv_config* cfg, lv_engine** out) {
@@ -2152,6 +2172,7 @@ lv_status lv_batch_run(lv_engine* E, uint32_t n_graphs, const lv_graph* const* g
   }
   LVTRY(load_common(E, N, NNZ));
   if (N > E->batch_out_cap) {
+    E->batch_out_cap = 0;
     dfree(E->batch_out);
     CU(dalloc(&E->batch_out, N));
     E->batch_out_cap = N;
@@ -2518,6 +2539,13 @@ lv_status lv_get_tuning(lv_engine* E, lv_tuning* t) {
   if (!E || !t) return fail(LV_ERR_ARG, "NULL argument");
   memset(t, 0, sizeof(*t));
   for (int b = 1; b <= kBuckets; b++) t->bucket_kernel[b] = E->tune[b];
+  return LV_OK;
+}
+
+lv_status lv_debug_fail_device_alloc(uint64_t n) {
+  g_alloc_fail_at.store(0, std::memory_order_relaxed);
+  g_alloc_count.store(0, std::memory_order_relaxed);
+  g_alloc_fail_at.store(n, std::memory_order_relaxed);
   return LV_OK;
 }
 

@@ -158,6 +158,7 @@ _SIGS = {
                                            ctypes.POINTER(_U32)]),
     "lv_reset_kernel_stats": (ctypes.c_int, [_VP]),
     "lv_get_launch_count": (ctypes.c_int, [ctypes.POINTER(_U64)]),
+    "lv_debug_fail_device_alloc": (ctypes.c_int, [_U64]),
     "lv_modularity_noalloc": (ctypes.c_int, [_U32, _VP, _VP, _VP, _VP, _VP,
                                              ctypes.POINTER(ctypes.c_double), _VP]),
     "lv_batch_run_device": (ctypes.c_int, [_VP, _U32, _VP, _U32, _U64, _VP, _VP, _VP,
@@ -244,6 +245,12 @@ def lib() -> ctypes.CDLL:
             f.argtypes = args
         _lib = L
     return _lib
+
+
+def fail_device_alloc(n: int):
+    """Fault injection for tests: the nth device allocation from now on
+    fails as out-of-memory (0 switches it off)."""
+    _check(lib().lv_debug_fail_device_alloc(n))
 
 
 def launch_count() -> int:
@@ -347,7 +354,7 @@ class RunResult:
 class Engine:
     def __init__(self, device: int = 0, rule: str = "py", max_passes: int = 0,
                  max_levels: int = 0, use_graphs: bool = True, stream: int = 0,
-                 gain: str = "fp32", level_kernel: bool = True):
+                 gain: str = "fp32", level_kernel: bool = False):
         cfg = Config()
         lib().lv_config_default(ctypes.byref(cfg))
         cfg.device = device

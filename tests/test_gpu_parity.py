@@ -230,20 +230,23 @@ def test_run_device_equals_run():
 @pytest.mark.parametrize("name", ["planted_small", "rmat11", "hub3000", "star1000"])
 def test_pass_loop_forms_agree(name):
     """Every way of running a level's pass loop gives the same run: the
-    persistent level kernel (default) with and without its phase timers,
-    the level graph (WHILE node), the host loop, and the per-pass replay of
-    a captured pass (the mode kernel timing uses without the level kernel)."""
+    level graph (WHILE node, the default), the persistent level kernel with
+    and without its phase timers, the host loop, and the per-pass replay of
+    a captured pass (the mode kernel timing uses)."""
     out = []
-    for lk, ug, prof in ((True, True, False), (True, True, True), (False, True, False),
+    for lk, ug, prof in ((False, True, False), (True, True, False), (True, True, True),
                          (False, False, False), (False, True, True)):
         with lvb200.Engine(rule="py", use_graphs=ug, level_kernel=lk) as e:
             e.set_profiling(prof)
             out.append(e.run(lvb200.Graph.load_mtx(golden_mtx(name)), 1e-6))
+    # identical runs; Q values to the last bits only, since the level
+    # kernel's modularity reduction splits the sum over a different grid
     for o in out[1:]:
-        assert o.modularity == out[0].modularity
+        assert abs(o.modularity - out[0].modularity) < 1e-12
         assert np.array_equal(o.assignment, out[0].assignment)
         assert [l["passes"] for l in o.levels] == [l["passes"] for l in out[0].levels]
-        assert [l["q_end"] for l in o.levels] == [l["q_end"] for l in out[0].levels]
+        assert np.allclose([l["q_end"] for l in o.levels], [l["q_end"] for l in out[0].levels],
+                           rtol=0, atol=1e-12)
 
 
 @pytest.mark.parametrize("rule", ["py", "cuda"])
@@ -262,21 +265,22 @@ def test_level_kernel_equals_level_graph_at_scale(rule, gain):
         for lk in (True, False):
             with lvb200.Engine(rule=rule, gain=gain, level_kernel=lk) as e:
                 res.append(e.run(g, 1e-6))
-        assert res[0].modularity == res[1].modularity
+        assert abs(res[0].modularity - res[1].modularity) < 1e-12
         assert np.array_equal(res[0].assignment, res[1].assignment)
         assert [l["passes"] for l in res[0].levels] == [l["passes"] for l in res[1].levels]
 
 
-def test_level_kernel_phase_timers(eng):
+def test_level_kernel_phase_timers():
     """With profiling on, the level kernel's barrier timestamps give every
     phase kind a device time and a count."""
-    eng.set_profiling(True)
-    eng.reset_kernel_stats()
-    res = eng.run(lvb200.Graph.load_mtx(golden_mtx("hub3000")), 1e-6)
-    st = eng.kernel_stats()
-    eng.set_profiling(False)
+    with lvb200.Engine(rule="py", level_kernel=True) as eng:
+        eng.set_profiling(True)
+        eng.reset_kernel_stats()
+        res = eng.run(lvb200.Graph.load_mtx(golden_mtx("hub3000")), 1e-6)
+        st = eng.kernel_stats()
     passes = sum(l["passes"] for l in res.levels)
-    assert st["modularity"]["launches"] == passes
+    # one sweep per pass, plus each level's initial one
+    assert st["modularity"]["launches"] == passes + len(res.levels)
     assert st["apply"]["launches"] >= passes
     assert st["move_hub"]["launches"] >= 2
     assert all(v["total_ms"] >= 0.0 for v in st.values())
