@@ -28,13 +28,15 @@ def _same(a, b):
 
 @pytest.mark.parametrize("name", ["hub3000", "rmat11"])
 def test_injected_allocation_failure_then_clean_run(name):
+    """A fresh engine per position n (a warm engine reuses its buffers and
+    allocates nothing), so every allocation of a whole run is reached."""
     g = lvb200.Graph.load_mtx(golden_mtx(name))
     with lvb200.Engine(rule="py") as e:
         ref = e.run(g, 1e-6)
     failed = 0
     try:
-        with lvb200.Engine(rule="py") as e:
-            for n in range(1, 120):
+        for n in range(1, 200):
+            with lvb200.Engine(rule="py") as e:
                 lvb200.fail_device_alloc(n)
                 try:
                     e.run(g, 1e-6)
@@ -43,9 +45,11 @@ def test_injected_allocation_failure_then_clean_run(name):
                     failed += 1
                 lvb200.fail_device_alloc(0)
                 _same(e.run(g, 1e-6), ref)  # the same engine, afterwards
+            if failed < n:  # the run needed fewer than n allocations
+                break
     finally:
         lvb200.fail_device_alloc(0)
-    assert failed >= 10  # the hook reached allocations of several stages
+    assert failed >= 20  # allocations of loading, level set-up and contraction
 
 
 def test_injected_allocation_failure_in_batched_form():
@@ -55,8 +59,8 @@ def test_injected_allocation_failure_in_batched_form():
         ref = e.batch_run(graphs, 1e-6)
     failed = 0
     try:
-        with lvb200.Engine(rule="py") as e:
-            for n in range(1, 80):
+        for n in range(1, 200):
+            with lvb200.Engine(rule="py") as e:
                 lvb200.fail_device_alloc(n)
                 try:
                     e.batch_run(graphs, 1e-6)
@@ -68,6 +72,8 @@ def test_injected_allocation_failure_in_batched_form():
                 for a, b in zip(got[0], ref[0]):
                     assert np.array_equal(a, b)
                 assert np.allclose(got[1], ref[1], rtol=0, atol=1e-12)
+            if failed < n:
+                break
     finally:
         lvb200.fail_device_alloc(0)
-    assert failed >= 5
+    assert failed >= 20
