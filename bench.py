@@ -17,7 +17,9 @@ pass's stored adjacency entries / time.
              (on the engine's stream): algorithmic bytes / event time,
              against the measured HBM copy bandwidth
   cpu_baseline  the reference's CPU path (louvian.py restated in C by the
-             oracle, FP64, single thread) on the same graph
+             oracle, FP64; its move decisions spread over all host
+             threads -- every bucket is one Jacobi step -- with results
+             identical to the single-threaded restatement) on the same graph
 N > 1 (torchrun): every rank runs its own replica (the single-graph path
 does not shard); value = edges of all ranks / max-over-ranks time.
   batched    (N=1) the batched form on 4,096 SBM graphs against the plain
@@ -28,7 +30,9 @@ does not shard); value = edges of all ranks / max-over-ranks time.
              p50/p99 latency against the plain engine run per request
   hbm_scale  (N=1) the plain engine on R-MAT scale 24 (16.8 M vertices,
              521 M entries): ms per run, edges/s per pass and the dominant
-             move group's roofline
+             move group's roofline; then, untimed, one run with FP64 gains
+             and the oracle's louvian.py restatement on the same graph (its
+             final Q, and how far each engine mode is from it)
 --impl reference: the reference's CPU implementation (oracle port) alone.
 """
 from __future__ import annotations
@@ -154,12 +158,21 @@ def ncu_traffic(kernel_group: str):
     return d.get(kernel_group, {}).get("dram_bytes_per_launch")
 
 
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def cpu_baseline(n, off, col, ww, budget_s=12.0):
     """The reference's CPU path (louvian.py's algorithm, restated in C by the
-    oracle: FP64, first-seen row order), single thread, on the same graph,
-    repeated until about `budget_s` seconds of CPU work."""
+    oracle: FP64, first-seen row order), on every host thread, on the same
+    graph, repeated until about `budget_s` seconds of CPU work."""
     import pyoracle
 
+    threads = host_threads()
+    pyoracle.set_threads(threads)
     g = pyoracle.CSR(n, off, col, ww.astype(np.float64))
     runs, t_tot, edges = 0, 0.0, 0
     q = None
@@ -172,8 +185,11 @@ def cpu_baseline(n, off, col, ww, budget_s=12.0):
         runs += 1
         if runs >= 50:
             break
-    return {"value": edges / t_tot, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"full workload, {runs} complete runs ({t_tot:.1f} s)",
+    pyoracle.set_threads(1)
+    return {"value": edges / t_tot, "unit": UNIT, "cores": threads, "kind": "port",
+            "host_threads": os.cpu_count(),
+            "sample": f"full workload, {runs} complete runs ({t_tot:.1f} s) on {threads} of "
+                      f"{os.cpu_count()} host threads",
             "final_q": q}
 
 
@@ -254,7 +270,7 @@ def batched_measure(stream, count: int, steps: int = 2):
     return res
 
 
-def hbm_scale_measure(stream, scale: int, steps: int = 2):
+def hbm_scale_measure(stream, scale: int, steps: int = 2, oracle_check: bool = True):
     """The plain engine at HBM scale: R-MAT (a, b, c, d = 0.57, 0.19, 0.19,
     0.05, edge factor 16, duplicates merged, unit weights) generated on the
     device; edges/s per pass over `steps` device-timed runs after one
@@ -299,9 +315,41 @@ def hbm_scale_measure(stream, scale: int, steps: int = 2):
         eng.set_profiling(False)
         kstats = eng.kernel_stats()
         eng.close()
+        check = None
+        if oracle_check:  # untimed: FP64 gains, then the oracle on the host
+            eng64 = lvb200.Engine(stream=stream.cuda_stream, gain="fp64")
+            r64 = eng64.run_device(n, nnz, off.data_ptr(), col.data_ptr(), w.data_ptr(),
+                                   MIN_GAIN, asg.data_ptr())
+            torch.cuda.synchronize()
+            asg64 = asg.cpu().numpy().view(np.uint32).copy()
+            eng64.close()
+            check = {"engine_fp64_q": r64.modularity}
+            h_off = off.cpu().numpy().view(np.uint64)
+            h_col = col.cpu().numpy().view(np.uint32)
+            h_w = w.cpu().numpy()
     del off, col, w, asg
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
+    if check is not None:
+        import pyoracle
+
+        threads = host_threads()
+        pyoracle.set_threads(threads)
+        t0 = time.perf_counter()
+        g = pyoracle.CSR(n, h_off, h_col, h_w.astype(np.float64))
+        del h_w
+        ref = pyoracle.louvain(g, MIN_GAIN, rule="py", prec="fp64", rows="first_seen")
+        pyoracle.set_threads(1)
+        check.update({
+            "oracle": "louvian.py restated (FP64 gains, louvian.py's stop rule)",
+            "oracle_q": ref.q, "oracle_s": time.perf_counter() - t0,
+            "oracle_threads": threads,
+            "abs_dq_fp32_mode": abs(r.modularity - ref.q),
+            "abs_dq_fp64_mode": abs(check["engine_fp64_q"] - ref.q),
+            "fp64_mode_partition_identical": bool(np.array_equal(asg64, ref.assignment)),
+            "oracle_passes": [l.passes for l in ref.levels],
+        })
+        del g
     peak, peak_kind = measured_peak()
     moves = {k: v for k, v in kstats.items() if k.startswith("move") or k == "modularity"}
     name, st = max(moves.items(), key=lambda kv: kv[1]["total_ms"])
@@ -317,6 +365,8 @@ def hbm_scale_measure(stream, scale: int, steps: int = 2):
                      "ms_per_launch": st["total_ms"] / launches_k},
         "kernel_ms": {k: round(v["total_ms"], 3) for k, v in kstats.items()},
     })
+    if check is not None:
+        res["oracle_check"] = check
     return res
 
 
@@ -472,6 +522,8 @@ def run_reference(args, rank, world):
         return
     import pyoracle
 
+    threads = host_threads()
+    pyoracle.set_threads(threads)
     g = pyoracle.CSR(n, off, col, ww.astype(np.float64))
     for _ in range(args.warmup):
         pyoracle.louvain(g, MIN_GAIN, rule="py", prec="fp64", rows="first_seen")
@@ -489,11 +541,13 @@ def run_reference(args, rank, world):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(desc, parallelism="replicas only (1 CPU thread)",
+        "config": dict(desc, parallelism=f"replicas only ({threads} CPU threads)",
                        l2="n/a (CPU)"),
         "final_q": q,
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
-                         "sample": f"full workload, {args.steps} timed runs"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "host_threads": os.cpu_count(),
+                         "sample": f"full workload, {args.steps} timed runs on {threads} of "
+                                   f"{os.cpu_count()} host threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -616,7 +670,7 @@ def run_engine(args, rank, world):
         served = served_measure(args.serve_requests, args.serve_rate,
                                 int(args.serve_budget_gb * 1e9))
     if world == 1 and args.hbm_scale > 0:
-        hbm = hbm_scale_measure(stream, args.hbm_scale)
+        hbm = hbm_scale_measure(stream, args.hbm_scale, oracle_check=not args.no_oracle_check)
     if rank != 0:
         return
     # roofline of the dominant kernel group
@@ -664,7 +718,7 @@ def run_engine(args, rank, world):
         line["hbm_scale"] = hbm
     if cpu:
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind",
-                                                    "sample")}
+                                                    "host_threads", "sample")}
         line["cpu_baseline"]["final_q"] = cpu["final_q"]
     print(json.dumps(line), flush=True)
 
@@ -684,6 +738,8 @@ def main():
                          "graphs with conditional nodes)")
     ap.add_argument("--hbm-scale", type=int, default=24,
                     help="R-MAT scale of the HBM-scale plain-engine measurement (0: skip)")
+    ap.add_argument("--no-oracle-check", action="store_true",
+                    help="skip the untimed FP64-gain run and host oracle on the HBM-scale graph")
     ap.add_argument("--batch-graphs", type=int, default=4096,
                     help="graphs of the batched-form measurement (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=200,

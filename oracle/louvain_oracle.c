@@ -28,6 +28,7 @@
 
 #include <errno.h>
 #include <math.h>
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -37,6 +38,12 @@ static const uint64_t kBucketHi[NBUCKETS + 1] = {0, 4, 8, 16, 32, 84, 319,
                                                  UINT64_MAX};
 
 void orc_free(void *p) { free(p); }
+
+/* Host threads for the move decisions and the intra-weight sum (1: the
+ * plain sequential restatement). */
+static int g_threads = 1;
+void orc_set_threads(int t) { g_threads = t < 1 ? 1 : (t > 256 ? 256 : t); }
+int orc_get_threads(void) { return g_threads; }
 
 static void set_err(char *err, int errlen, const char *msg, long line) {
     if (!err || errlen <= 0) return;
@@ -324,15 +331,57 @@ typedef struct {
     uint32_t *touched;
 } mstate;
 
-static double state_modularity(const mstate *s) {
-    /* louvian.py:101-113 (FP64 mode): sum of squares with builtin sum()
-     * over communities in ascending order, intra weight in plain order. */
+static double intra_range(const mstate *s, uint32_t v0, uint32_t v1) {
     double intra = 0.0;
-    for (uint32_t v = 0; v < s->n; v++) {
+    for (uint32_t v = v0; v < v1; v++) {
         uint32_t cv = s->comm[v];
         for (uint64_t j = s->off[v]; j < s->off[v + 1]; j++)
             if (s->comm[s->col[j]] == cv) intra += s->w[j];
     }
+    return intra;
+}
+
+typedef struct {
+    const mstate *s;
+    uint32_t v0, v1;
+    double out;
+} intra_job;
+
+static void *intra_worker(void *arg) {
+    intra_job *j = (intra_job *)arg;
+    j->out = intra_range(j->s, j->v0, j->v1);
+    return NULL;
+}
+
+/* Intra-community weight: in vertex order on one thread (louvian.py's
+ * order); with several threads, per-range partial sums added in range
+ * order (equal whenever the sums are exact, e.g. integer weights). */
+static double intra_weight(const mstate *s) {
+    const int T = g_threads;
+    if (T <= 1 || s->n < 65536) return intra_range(s, 0, s->n);
+    pthread_t th[256];
+    intra_job jobs[256];
+    for (int t = 0; t < T; t++) {
+        jobs[t].s = s;
+        jobs[t].v0 = (uint32_t)((uint64_t)s->n * t / T);
+        jobs[t].v1 = (uint32_t)((uint64_t)s->n * (t + 1) / T);
+        if (pthread_create(&th[t], NULL, intra_worker, &jobs[t]) != 0) {
+            jobs[t].out = intra_range(s, jobs[t].v0, jobs[t].v1);
+            th[t] = 0;
+        }
+    }
+    double intra = 0.0;
+    for (int t = 0; t < T; t++) {
+        if (th[t]) pthread_join(th[t], NULL);
+        intra += jobs[t].out;
+    }
+    return intra;
+}
+
+static double state_modularity(const mstate *s) {
+    /* louvian.py:101-113 (FP64 mode): sum of squares with builtin sum()
+     * over communities in ascending order, intra weight in plain order. */
+    double intra = intra_weight(s);
     double asq;
     if (s->prec == ORC_PREC_FP64) {
         neu_sum ns = {0.0, 0.0};
@@ -351,18 +400,18 @@ static inline int is_lower_idx(const mstate *s, uint32_t cv, uint32_t ce) {
     return 1;
 }
 
-static void decide(mstate *s, uint32_t v, int rule) {
+static void decide(mstate *s, uint32_t v, int rule, double *acc_s, uint32_t *touched) {
     const uint64_t b = s->off[v], e_end = s->off[v + 1];
     const uint32_t cv = s->comm[v];
     uint32_t nt = 0;
     /* neighbour-community sums (louvian.py:122-124) */
     for (uint64_t j = b; j < e_end; j++) {
         uint32_t c = s->comm[s->col[j]];
-        if (s->acc[c] == 0.0 && nt < (uint32_t)(e_end - b)) {
+        if (acc_s[c] == 0.0 && nt < (uint32_t)(e_end - b)) {
             /* track every community once; zero weights re-track harmlessly */
-            s->touched[nt++] = c;
+            touched[nt++] = c;
         }
-        s->acc[c] += s->w[j];
+        acc_s[c] += s->w[j];
     }
     uint32_t target = cv;
     if (s->prec == ORC_PREC_FP64) {
@@ -375,7 +424,7 @@ static void decide(mstate *s, uint32_t v, int rule) {
             uint32_t ce = s->comm[e];
             if (ce == cv && e != v) e_own += s->w[j];
             if (!is_lower_idx(s, cv, ce)) continue;
-            double gain = (s->acc[ce] / m) +
+            double gain = (acc_s[ce] / m) +
                           (kv * ((s->a[cv] - kv) - s->a[ce]) / (2 * (m * m)));
             if (gain > max_gain || (gain == max_gain && ce < max_comm)) {
                 max_gain = gain;
@@ -397,7 +446,7 @@ static void decide(mstate *s, uint32_t v, int rule) {
             uint32_t ce = s->comm[e];
             if (ce == cv && e != v) e_own64 += s->w[j];
             if (!is_lower_idx(s, cv, ce)) continue;
-            float ec = (float)s->acc[ce];
+            float ec = (float)acc_s[ce];
             float ac = (float)s->a[ce];
             volatile float t1 = ec / m;
             volatile float t2 = (aown - kv) - ac;
@@ -418,10 +467,53 @@ static void decide(mstate *s, uint32_t v, int rule) {
         }
         if (move) target = max_comm;
     }
-    for (uint32_t i = 0; i < nt; i++) s->acc[s->touched[i]] = 0.0;
+    for (uint32_t i = 0; i < nt; i++) acc_s[touched[i]] = 0.0;
     /* acc entries that summed to exactly zero without being tracked twice
      * are already zero, so the scratch is clean again. */
     s->new_comm[v] = target;
+}
+
+typedef struct {
+    mstate *s;
+    const uint32_t *vset;
+    uint32_t i0, i1;
+    int rule;
+    double *acc;
+    uint32_t *touched;
+} decide_job;
+
+static void *decide_worker(void *arg) {
+    decide_job *j = (decide_job *)arg;
+    for (uint32_t i = j->i0; i < j->i1; i++) decide(j->s, j->vset[i], j->rule, j->acc, j->touched);
+    return NULL;
+}
+
+/* Every vertex of a bucket decides against the same state (one Jacobi
+ * step, modularity.cu:466-499), so the decisions split over threads; each
+ * thread has its own scratch and every decision is the sequential one. */
+static void decide_bucket(mstate *s, const uint32_t *vset, uint32_t cnt, int rule,
+                          double **acc_t, uint32_t **touched_t, int T) {
+    if (T <= 1 || cnt < 4096) {
+        for (uint32_t i = 0; i < cnt; i++) decide(s, vset[i], rule, acc_t[0], touched_t[0]);
+        return;
+    }
+    pthread_t th[256];
+    decide_job jobs[256];
+    for (int t = 0; t < T; t++) {
+        jobs[t].s = s;
+        jobs[t].vset = vset;
+        jobs[t].i0 = (uint32_t)((uint64_t)cnt * t / T);
+        jobs[t].i1 = (uint32_t)((uint64_t)cnt * (t + 1) / T);
+        jobs[t].rule = rule;
+        jobs[t].acc = acc_t[t];
+        jobs[t].touched = touched_t[t];
+        if (pthread_create(&th[t], NULL, decide_worker, &jobs[t]) != 0) {
+            decide_worker(&jobs[t]);
+            th[t] = 0;
+        }
+    }
+    for (int t = 0; t < T; t++)
+        if (th[t]) pthread_join(th[t], NULL);
 }
 
 static void recompute_totals(mstate *s) {
@@ -457,6 +549,22 @@ int orc_move_phase(uint32_t n, const uint64_t *off, const uint32_t *col,
         free(s.acc); free(s.touched); free(vset); free(bk);
         return -ORC_ERR_NOMEM;
     }
+    /* decision scratch per thread (thread 0 uses the state's own) */
+    int T = g_threads;
+    double *acc_t[256];
+    uint32_t *touched_t[256];
+    acc_t[0] = s.acc;
+    touched_t[0] = s.touched;
+    for (int t = 1; t < T; t++) {
+        acc_t[t] = (double *)calloc(nn, sizeof(double));
+        touched_t[t] = (uint32_t *)malloc(sizeof(uint32_t) * (maxdeg ? maxdeg : 1));
+        if (!acc_t[t] || !touched_t[t]) { /* fall back to fewer threads */
+            free(acc_t[t]);
+            free(touched_t[t]);
+            T = t;
+            break;
+        }
+    }
     /* weighted degree and m (louvian.py:49-56, modularity.cu:27-49,457) */
     double all_w = 0.0;
     for (uint32_t v = 0; v < n; v++) {
@@ -491,6 +599,7 @@ int orc_move_phase(uint32_t n, const uint64_t *off, const uint32_t *col,
         if (q_end) *q_end = 0.0;
         free(s.k); free(s.comm); free(s.comm_sz); free(s.a); free(s.new_comm);
         free(s.acc); free(s.touched); free(vset); free(bk);
+        for (int t = 1; t < T; t++) { free(acc_t[t]); free(touched_t[t]); }
         return 0;
     }
     act = state_modularity(&s);
@@ -502,7 +611,7 @@ int orc_move_phase(uint32_t n, const uint64_t *off, const uint32_t *col,
             for (uint32_t v = 0; v < n; v++)
                 if (bk[v] == b) vset[cnt++] = v;
             if (!cnt) continue;
-            for (uint32_t i = 0; i < cnt; i++) decide(&s, vset[i], rule);
+            decide_bucket(&s, vset, cnt, rule, acc_t, touched_t, T);
             for (uint32_t i = 0; i < cnt; i++) { /* louvian.py:64-68 */
                 uint32_t v = vset[i];
                 s.comm_sz[s.new_comm[v]]++;
@@ -524,6 +633,7 @@ int orc_move_phase(uint32_t n, const uint64_t *off, const uint32_t *col,
     if (q_end) *q_end = act;
     free(s.k); free(s.comm); free(s.comm_sz); free(s.a); free(s.new_comm);
     free(s.acc); free(s.touched); free(vset); free(bk);
+    for (int t = 1; t < T; t++) { free(acc_t[t]); free(touched_t[t]); }
     return ret;
 }
 

@@ -105,6 +105,15 @@ int orc_louvain(uint32_t n, const uint64_t *off, const uint32_t *col,
                 uint32_t *assignment, double *q_final, orc_level_stat *stats,
                 uint32_t max_stats, uint32_t *n_levels);
 
+/* Host threads of the move decisions and the intra-weight sum (default 1:
+ * the sequential restatement, every sum in louvian.py's order).  Each
+ * bucket is one Jacobi step, so the decisions do not depend on the thread
+ * count; with several threads the intra weight is summed per vertex range
+ * and the ranges added in order (equal to the sequential sum whenever the
+ * sums are exact, as with integer weights).                               */
+void orc_set_threads(int t);
+int orc_get_threads(void);
+
 /* FP64 modularity of an arbitrary partition (part[v] < n):
  * Q = sum_v sum_{u in N(v), part(u)=part(v)} w / 2m - sum_c a_c^2 / 4m^2.  */
 double orc_modularity(uint32_t n, const uint64_t *off, const uint32_t *col,

@@ -84,8 +84,20 @@ def lib():
             ctypes.c_void_p,
         ]
         L.orc_modularity.restype = ctypes.c_double
+        L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_get_threads.restype = ctypes.c_int
         _lib = L
     return _lib
+
+
+def set_threads(t: int):
+    """Host threads of the oracle's move decisions and intra-weight sum
+    (1: the sequential restatement in louvian.py's summation order)."""
+    lib().orc_set_threads(int(t))
+
+
+def get_threads() -> int:
+    return int(lib().orc_get_threads())
 
 
 def _p(a: np.ndarray):
