@@ -26,8 +26,9 @@ does not shard); value = edges of all ranks / max-over-ranks time.
              engine looped over the same graphs: graphs/s of each, and whether
              every partition is identical
   served     (N=1) the served form (continuous batching, 120 GB budget) on
-             Poisson arrivals of R-MAT / LFR-style requests: graphs/s and
-             p50/p99 latency against the plain engine run per request
+             2,000 R-MAT / LFR-style requests: saturated capacity (all queued
+             at t=0) in graphs/s, and p50/p99 latency under Poisson arrivals
+             at 200/s, both against the plain engine run per request
   hbm_scale  (N=1) the plain engine on R-MAT scale 24 (16.8 M vertices,
              521 M entries): ms per run, edges/s per pass and the dominant
              move group's roofline; then, untimed, one run with FP64 gains
@@ -402,83 +403,88 @@ def served_requests(count: int, seed: int):
     return out
 
 
-def served_measure(count: int, rate: float, budget: int, seed: int = 0):
-    """Served form under Poisson arrivals (rate per second): every request
-    is submitted to lv_serve at its arrival time (host clock), the loop
-    steps the server and polls results; latency = result time - arrival.
-    Against it, the plain engine runs the same requests one by one through
-    lv_run (host graphs, as the server's are): graphs/s from the summed
-    run times, and the latencies a first-come-first-served single engine
-    would give for the same arrivals."""
-    reqs = served_requests(count, seed)
+def served_measure(count: int, rate: float, budget: int, distinct: int, seed: int = 0):
+    """Served form on `count` requests whose graphs are drawn (seeded, with
+    repetition) from `distinct` generated request graphs.  Two runs of the
+    server: every request queued at t=0 (saturated capacity: graphs/s over
+    the makespan), and Poisson arrivals at `rate` per second (latency =
+    result time - arrival, p50/p99).  Against them the plain engine run per
+    request through lv_run (host graphs, as the server's): its graphs/s from
+    the summed run times, and the latencies a first-come-first-served single
+    engine gives for the same arrivals.  Every served partition is compared
+    with its graph's plain run."""
+    pool = served_requests(distinct, seed)
+    rng = np.random.default_rng(seed + 2)
+    pick = rng.integers(0, len(pool), size=count)
+    reqs = [pool[i] for i in pick]
     arrivals = np.cumsum(np.random.default_rng(seed + 1).exponential(1.0 / rate, size=count))
-    return served_report(reqs, arrivals, rate, budget)
+    return served_report(pool, pick, reqs, arrivals, rate, budget)
 
 
 def serve_run(reqs, arrivals, budget, lanes=4):
-    """Replays the arrivals against a server (lanes > 1: the default size
-    lanes stepped by worker threads; 1: one union stepped by this loop);
-    returns (results by request, completion times, steps, most graphs
+    """Replays the arrivals against a server with its default lanes (two
+    union lanes for smaller graphs, two solo lanes for larger ones, each
+    stepped by a worker thread); arrivals None queues every request at
+    t=0.  Returns (results by request, completion times, steps, most graphs
     resident at once)."""
     import lvb200
 
     count = len(reqs)
-    background = lanes > 1
-    with lvb200.Server(MIN_GAIN, budget, lanes=lanes, background=background) as server:
+    with lvb200.Server(MIN_GAIN, budget, lanes=lanes, background=True) as server:
         # warm-up request (kernel set-up, first graph instantiations)
         server.submit(reqs[0][0], n_vertices=reqs[0][1])
         server.drain()
         ticket_of, done, done_t = {}, {}, np.zeros(count)
         max_res, i = 0, 0
         t0 = time.perf_counter()
+        if arrivals is None:
+            arrivals = np.zeros(count)
         while len(done) < count:
             now = time.perf_counter() - t0
             while i < count and arrivals[i] <= now:
                 ticket_of[server.submit(reqs[i][0], n_vertices=reqs[i][1])] = i
                 i += 1
-            if background:
-                wait_s = (arrivals[i] - now) if i < count else 0.05
-                server.wait(max(1, int(wait_s * 1000)))
-                r = server.stats()["resident"]
-                q = 0
-            else:
-                r, q = server.step()
-            max_res = max(max_res, r)
+            wait_s = (arrivals[i] - now) if i < count else 0.05
+            server.wait(max(1, int(wait_s * 1000)))
+            max_res = max(max_res, server.stats()["resident"])
             t = time.perf_counter() - t0
             while (x := server.poll()) is not None:
                 j = ticket_of[x.ticket]
                 done[j] = x
                 done_t[j] = t
-            if not background and r == 0 and q == 0 and i < count:
-                time.sleep(max(0.0, arrivals[i] - (time.perf_counter() - t0)))
         stats = server.stats()
     return done, done_t, int(stats["steps"]), max_res
 
 
-def served_report(reqs, arrivals, rate, budget):
+def served_report(pool, pick, reqs, arrivals, rate, budget):
     import lvb200
 
     count = len(reqs)
-    done1, done_t1, _, _ = serve_run(reqs, arrivals, budget, lanes=1)
-    lat1 = (done_t1 - arrivals) * 1000.0
-    makespan1 = float(done_t1.max() - arrivals[0])
-    done, done_t, steps, max_res = serve_run(reqs, arrivals, budget, lanes=4)
+    # saturated: everything queued at t=0
+    done_s, done_ts, _, max_res_s = serve_run(reqs, None, budget)
+    makespan_s = float(done_ts.max())
+    # Poisson arrivals
+    done, done_t, steps, max_res = serve_run(reqs, arrivals, budget)
     lat = (done_t - arrivals) * 1000.0
     makespan = float(done_t.max() - arrivals[0])
-    # plain engine, one request at a time
+    # plain engine, one run per distinct graph (its service time and result)
     eng = lvb200.Engine()
-    eng.run(reqs[0][0], MIN_GAIN)
-    svc = np.zeros(count)
-    same, dq = 0, 0.0
-    for j, (g, n, e, kind) in enumerate(reqs):
+    eng.run(pool[0][0], MIN_GAIN)
+    svc_pool, res_pool = np.zeros(len(pool)), []
+    for k, (g, n, e, kind) in enumerate(pool):
         t = time.perf_counter()
         res = eng.run(g, MIN_GAIN)
-        svc[j] = time.perf_counter() - t
-        same += int(np.array_equal(res.assignment, done[j].assignment) and
-                    np.array_equal(res.assignment, done1[j].assignment))
-        dq = max(dq, abs(res.modularity - done[j].modularity),
-                 abs(res.modularity - done1[j].modularity))
+        svc_pool[k] = time.perf_counter() - t
+        res_pool.append(res)
     eng.close()
+    svc = svc_pool[pick]
+    same, dq = 0, 0.0
+    for j in range(count):
+        res = res_pool[pick[j]]
+        same += int(np.array_equal(res.assignment, done[j].assignment) and
+                    np.array_equal(res.assignment, done_s[j].assignment))
+        dq = max(dq, abs(res.modularity - done[j].modularity),
+                 abs(res.modularity - done_s[j].modularity))
     end, plain_lat = 0.0, np.zeros(count)
     for j in range(count):  # first come first served on one engine
         end = max(end, arrivals[j]) + svc[j]
@@ -492,26 +498,29 @@ def served_report(reqs, arrivals, rate, budget):
     kinds = {}
     for _, _, _, k in reqs:
         kinds[k] = kinds.get(k, 0) + 1
+    plain_gps = count / float(svc.sum())
     return {
-        "workload": "served requests", "requests": count, "arrivals": f"Poisson {rate}/s",
+        "workload": "served requests", "requests": count,
+        "distinct_graphs": len(pool),
+        "requests_note": "graphs drawn with repetition from the distinct seeded request "
+                         "graphs; every request runs in full",
+        "arrivals": f"Poisson {rate}/s",
         "mix": "50% R-MAT scale U{10..21}, 50% LFR-style n log-U[1k,2M] mu U(0.1,0.5)",
         "kinds": kinds, "total_entries": int(sum(r[2] for r in reqs)),
         "total_vertices": int(sum(r[1] for r in reqs)), "budget_gb": budget / 1e9,
-        "served": {"lanes": "4 (<= 2^18, <= 2^23 entries, two for larger ones; "
-                            "10/30/30/30% of the budget), worker threads",
-                   "graphs_per_s": count / makespan, "makespan_s": makespan,
-                   "p50_ms": float(np.percentile(lat, 50)),
-                   "p99_ms": float(np.percentile(lat, 99)),
-                   "max_resident": int(max_res), "steps": steps,
-                   "by_lane": by_lane},
-        "served_one_lane": {"graphs_per_s": count / makespan1, "makespan_s": makespan1,
-                            "p50_ms": float(np.percentile(lat1, 50)),
-                            "p99_ms": float(np.percentile(lat1, 99))},
-        "plain_looped": {"graphs_per_s": count / float(svc.sum()),
-                         "total_s": float(svc.sum()),
-                         "p50_ms": float(np.percentile(plain_lat, 50)),
-                         "p99_ms": float(np.percentile(plain_lat, 99))},
-        "speedup_graphs_per_s": float(svc.sum()) / makespan,
+        "lanes": "2 union lanes (<= 2^18, <= 2^22 entries; 10/30% of the budget), "
+                 "2 solo lanes for larger graphs (30% each), worker threads",
+        "saturated": {"graphs_per_s": count / makespan_s, "makespan_s": makespan_s,
+                      "plain_graphs_per_s": plain_gps,
+                      "speedup_graphs_per_s": (count / makespan_s) / plain_gps,
+                      "max_resident": int(max_res_s)},
+        "poisson": {"graphs_per_s": count / makespan, "makespan_s": makespan,
+                    "p50_ms": float(np.percentile(lat, 50)),
+                    "p99_ms": float(np.percentile(lat, 99)),
+                    "plain_p50_ms": float(np.percentile(plain_lat, 50)),
+                    "plain_p99_ms": float(np.percentile(plain_lat, 99)),
+                    "max_resident": int(max_res), "steps": steps, "by_lane": by_lane},
+        "plain_looped": {"graphs_per_s": plain_gps, "total_s": float(svc.sum())},
         "partitions_identical": f"{same}/{count}", "max_abs_dq": dq,
     }
 
@@ -668,7 +677,8 @@ def run_engine(args, rank, world):
         batched = batched_measure(stream, args.batch_graphs)
     if world == 1 and args.serve_requests > 0:
         served = served_measure(args.serve_requests, args.serve_rate,
-                                int(args.serve_budget_gb * 1e9))
+                                int(args.serve_budget_gb * 1e9),
+                                min(args.serve_distinct, args.serve_requests))
     if world == 1 and args.hbm_scale > 0:
         hbm = hbm_scale_measure(stream, args.hbm_scale, oracle_check=not args.no_oracle_check)
     if rank != 0:
@@ -742,8 +752,10 @@ def main():
                     help="skip the untimed FP64-gain run and host oracle on the HBM-scale graph")
     ap.add_argument("--batch-graphs", type=int, default=4096,
                     help="graphs of the batched-form measurement (0: skip)")
-    ap.add_argument("--serve-requests", type=int, default=200,
+    ap.add_argument("--serve-requests", type=int, default=2000,
                     help="requests of the served-form measurement (0: skip)")
+    ap.add_argument("--serve-distinct", type=int, default=400,
+                    help="distinct request graphs the served requests are drawn from")
     ap.add_argument("--serve-rate", type=float, default=200.0,
                     help="Poisson arrival rate of the served requests, per second")
     ap.add_argument("--serve-budget-gb", type=float, default=120.0,

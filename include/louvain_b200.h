@@ -287,14 +287,22 @@ typedef struct {
                                     takes the rest) */
   float lane_share[4];           /* share of the budget per lane */
   int background;                /* step the lanes on worker threads */
+  uint32_t lane_solo;            /* bit i set: lane i runs its requests one
+                                    at a time through the single-graph path
+                                    (lv_run on the lane's engine and stream)
+                                    instead of a union, so a large graph is
+                                    never paced by others' levels, and solo
+                                    lanes overlap on the device            */
 } lv_serve_config;
 
-/* 4 background lanes: <= 2^18 entries (10% of the budget), <= 2^23 (30%),
- * and two for larger graphs (30% each); budget 8 GiB; min_gain 1e-6.
- * Lanes with the same bound form a group: a request goes to the group's
- * lane with the fewest entries resident or queued.  Each lane holds a
- * fifth of its budget for per-vertex state at 192 B a vertex and the rest
- * for adjacency at 40 B an entry.                                          */
+/* 4 background lanes: unions of graphs with <= 2^18 entries (10% of the
+ * budget) and <= 2^22 (30%), and two solo lanes for larger graphs (30%
+ * each); budget 8 GiB; min_gain 1e-6.  Lanes with the same bound form a
+ * group: a request goes to the group's lane with the fewest entries
+ * resident or queued.  A union lane holds a fifth of its budget for
+ * per-vertex state at 192 B a vertex and the rest for adjacency at 40 B an
+ * entry; a solo lane admits a graph whose sizes fit those capacities and
+ * allocates for it when it runs.                                           */
 void lv_serve_config_default(lv_serve_config *c);
 
 typedef struct {

@@ -1394,6 +1394,7 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 // One union of resident graphs on its own engine (and stream).
 struct ServeLane {
   lv_engine* E = nullptr;
+  bool solo = false;         // one request at a time, single-graph path
   uint64_t max_entries = 0;  // routing: requests with at most this many entries
   uint32_t cap_n = 0, slot_cap = 0;
   uint64_t cap_e = 0;
@@ -1495,8 +1496,47 @@ lv_status serve_append(ServeLane* L, ServeRequest* r) {
   return LV_OK;
 }
 
+// A solo lane's step: its oldest queued request, run alone through the
+// single-graph path (lv_run: upload, every level, assignment).
+lv_status solo_step(lv_server* S, ServeLane* L) {
+  lv_engine* E = L->E;
+  ServeRequest* r = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(S->mu);
+    if (L->queue.empty()) return LV_OK;
+    r = L->queue.front();
+    L->queue.pop_front();
+    L->res_n += r->n;
+    L->res_e += r->nnz;
+    L->n_res++;
+  }
+  r->t_admit = ms_since(S->t0);
+  L->admitted++;
+  lv_result res{};
+  LVTRY(lv_run(E, r->g, S->cfg.min_gain, &res));
+  r->assignment.resize(r->n);
+  LVTRY(lv_get_assignment(E, r->assignment.data(), r->n));
+  r->q = res.modularity;
+  r->levels = res.n_levels;
+  r->n_comm = res.n_communities;
+  E->levels.clear();
+  L->steps++;
+  {
+    std::lock_guard<std::mutex> lock(S->mu);
+    r->t_done = ms_since(S->t0);
+    L->res_n -= r->n;
+    L->res_e -= r->nnz;
+    L->n_res--;
+    L->completed++;
+    S->finished.push_back(r);
+  }
+  S->cv_done.notify_all();
+  return LV_OK;
+}
+
 // One step of a lane: admissions, then one level of its union.
 lv_status lane_step(lv_server* S, ServeLane* L) {
+  if (L->solo) return solo_step(S, L);
   lv_engine* E = L->E;
   cudaSetDevice(E->device);
   AllocScope alloc_scope(E);
@@ -2194,7 +2234,7 @@ void lv_serve_config_default(lv_serve_config* c) {
   c->max_graphs = 0;
   c->n_lanes = 4;
   c->lane_max_entries[0] = 1ull << 18;
-  c->lane_max_entries[1] = 1ull << 23;
+  c->lane_max_entries[1] = 1ull << 22;
   c->lane_max_entries[2] = ~0ull;
   c->lane_max_entries[3] = ~0ull;
   c->lane_share[0] = 0.10f;
@@ -2202,6 +2242,7 @@ void lv_serve_config_default(lv_serve_config* c) {
   c->lane_share[2] = 0.30f;
   c->lane_share[3] = 0.30f;
   c->background = 1;
+  c->lane_solo = 0xCu;  // lanes 2 and 3
 }
 
 lv_status lv_serve_create(const lv_config* cfg, const lv_serve_config* scfg, lv_server** out) {
@@ -2266,6 +2307,12 @@ lv_status lv_serve_create(const lv_config* cfg, const lv_serve_config* scfg, lv_
     L->cap_n = (uint32_t)cap_n;
     L->cap_e = (budget - cap_n * per_v) / per_e;
     L->slot_cap = scfg->max_graphs ? scfg->max_graphs : 4096;
+    L->solo = (scfg->lane_solo >> i) & 1u;
+    if (L->solo) {  // no union: the engine allocates per request
+      L->slot_cap = 1;
+      L->by_slot.assign(1, nullptr);
+      continue;
+    }
     auto setup = [&]() -> lv_status {
       AllocScope alloc_scope(E);
       LVTRY(ensure_capacity(E, L->cap_n, L->cap_e, false));

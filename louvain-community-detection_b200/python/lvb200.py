@@ -95,7 +95,7 @@ class ServeConfig(ctypes.Structure):
     _fields_ = [("min_gain", ctypes.c_float), ("budget_bytes", ctypes.c_uint64),
                 ("max_graphs", ctypes.c_uint32), ("n_lanes", ctypes.c_uint32),
                 ("lane_max_entries", ctypes.c_uint64 * 4), ("lane_share", ctypes.c_float * 4),
-                ("background", ctypes.c_int)]
+                ("background", ctypes.c_int), ("lane_solo", ctypes.c_uint32)]
 
 
 class ServeResult(ctypes.Structure):
@@ -580,7 +580,8 @@ class Server:
     def __init__(self, min_gain: float, budget_bytes: int, max_graphs: int = 0,
                  lanes: int = 1, background: bool = False, lane_max_entries=None,
                  lane_share=None, device: int = 0, rule: str = "py", max_passes: int = 0,
-                 max_levels: int = 0, use_graphs: bool = True, gain: str = "fp32"):
+                 max_levels: int = 0, use_graphs: bool = True, gain: str = "fp32",
+                 lane_solo: int | None = None):
         cfg = Config()
         lib().lv_config_default(ctypes.byref(cfg))
         cfg.device = device
@@ -604,6 +605,10 @@ class Server:
         if lane_share is not None:
             for i, x in enumerate(lane_share):
                 sc.lane_share[i] = x
+        if lane_solo is not None:
+            sc.lane_solo = lane_solo
+        elif lanes == 1:
+            sc.lane_solo = 0
         h = ctypes.c_void_p()
         _check(lib().lv_serve_create(ctypes.byref(cfg), ctypes.byref(sc), ctypes.byref(h)))
         self._h = h

@@ -174,3 +174,35 @@ def test_serve_lane_group():
     big = [served[t].lane for t, e in zip(tickets, entries) if e > 2_000]
     assert all(served[t].lane == 0 for t, e in zip(tickets, entries) if e <= 2_000)
     assert set(big) == {1, 2}
+
+
+@pytest.mark.parametrize("background", [False, True])
+def test_serve_solo_lanes(background):
+    """Solo lanes run one request at a time through the single-graph path
+    beside a union lane; routing by size still holds and every result
+    equals the lone run, whether the lanes are stepped by the caller or by
+    worker threads."""
+    graphs = _mix()
+    alone = _alone(graphs, 1e-6)
+    entries = [g.csr()[2].size for g in graphs]
+    unbounded = 2**64 - 1
+    with lvb200.Server(1e-6, 512 << 20, lanes=3, background=background,
+                       lane_max_entries=[2_000, unbounded, unbounded],
+                       lane_share=[0.2, 0.4, 0.4], lane_solo=0b110) as s:
+        tickets, served = _staggered(s, graphs)
+        st = s.stats()
+    assert st["completed"] == len(graphs)
+    _check(alone, served, tickets)
+    for t, e in zip(tickets, entries):
+        assert (served[t].lane == 0) == (e <= 2_000)
+
+
+def test_serve_all_solo():
+    graphs = _mix()
+    alone = _alone(graphs, 1e-6)
+    with lvb200.Server(1e-6, 512 << 20, lanes=2, background=True,
+                       lane_max_entries=[2**64 - 1, 2**64 - 1], lane_share=[0.5, 0.5],
+                       lane_solo=0b11) as s:
+        tickets = [s.submit(g) for g in graphs]
+        served = s.drain()
+    _check(alone, served, tickets)
