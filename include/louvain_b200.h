@@ -165,6 +165,29 @@ lv_status lv_engine_load_device(lv_engine *e, uint32_t n_vertices,
                                 uint64_t n_entries, const uint64_t *d_offsets,
                                 const uint32_t *d_cols, const float *d_weights);
 
+/* The reference's CSR construction (parseGraph, utils.cu:168-229) built on
+ * the device from edge lines: every row keeps file order, an off-diagonal
+ * line (i, j, w) is stored in rows i and j, i == j once, weights |w| (1
+ * without a weight array).  The rows come from a stable device sort of the
+ * directed entries by row.  Indices 0-based, < n_vertices (else
+ * LV_ERR_PARSE); at most 2^31 - 1 lines.
+ * lv_engine_load_edges: host edge lines -> device -> CSR -> engine (as
+ * lv_engine_load).  lv_engine_load_mtx: the Matrix Market reader of
+ * lv_graph_load_mtx (parallel host parse), then the device build.
+ * lv_csr_from_edges_device: device in, device out on `stream`; d_cols and
+ * d_weights_out need room for 2 * n_edges entries, d_offsets for
+ * n_vertices + 1; *n_entries receives the entry count; scratch is
+ * allocated and freed on the stream.                                      */
+lv_status lv_engine_load_edges(lv_engine *e, uint32_t n_vertices, uint64_t n_edges,
+                               const uint32_t *src, const uint32_t *dst,
+                               const float *weights);
+lv_status lv_engine_load_mtx(lv_engine *e, const char *path);
+lv_status lv_csr_from_edges_device(uint32_t n_vertices, uint64_t n_edges,
+                                   const uint32_t *d_src, const uint32_t *d_dst,
+                                   const float *d_weights, uint64_t *d_offsets,
+                                   uint32_t *d_cols, float *d_weights_out,
+                                   uint64_t *n_entries, void *stream);
+
 /* One phase of local moving on the current level (modularityOptimization,
  * modularity.cu:438-520).  *more = 1 when the first pass gained at least
  * min_gain (the caller should aggregate and call again), 0 when the run
@@ -193,6 +216,15 @@ lv_status lv_run_device(lv_engine *e, uint32_t n_vertices, uint64_t n_entries,
 
 /* Final (or current) community of every input vertex -> host buffer.  */
 lv_status lv_get_assignment(lv_engine *e, uint32_t *out, size_t n);
+
+/* The community listing of printCommunities (utils.cu:270-293) grouped on
+ * the device and copied to the host once: out[0..C] the offsets of every
+ * community's members, out[C+1 .. C+1+n) the input vertices community by
+ * community, ascending within each (a stable device sort by community).
+ * *n_communities receives C; with out NULL only C is returned (the buffer
+ * needs C + 1 + n entries).                                                */
+lv_status lv_get_communities(lv_engine *e, uint32_t *out, size_t cap,
+                             uint32_t *n_communities);
 
 /* Per-level records of the last run; *count receives how many exist.    */
 lv_status lv_get_levels(lv_engine *e, lv_level_info *out, uint32_t cap,

@@ -164,6 +164,9 @@ struct PendingTiming {
 }  // namespace
 
 void lvb_set_error(const std::string& msg) { g_last_error = msg; }
+// graph_io.cpp: a Matrix Market file's edge lines (0-based, validated).
+lv_status lvb_parse_mtx(const char* path, uint32_t* n_out, std::vector<uint32_t>& src,
+                        std::vector<uint32_t>& dst, std::vector<float>& ws);
 
 // Opt-in host-side trace (LVB200_TRACE=1): wall-clock time of each step of
 // the level loop on stderr.
@@ -1793,6 +1796,79 @@ lv_status lv_engine_load(lv_engine* E, const lv_graph* g) {
   return load_common(E, g->n, g->nnz);
 }
 
+// Host edge lines -> device -> the reference reader's CSR built on the
+// device (sort by row) in the engine's input buffers.
+static lv_status load_edges_common(lv_engine* E, uint32_t n, uint64_t m, const uint32_t* src,
+                                   const uint32_t* dst, const float* w) {
+  if (n >= 0xFFFFFFFFu) return fail(LV_ERR_LIMIT, "vertex count must be < 2^32-1");
+  if (m >= (1ull << 31)) return fail(LV_ERR_LIMIT, "at most 2^31 - 1 edge lines");
+  cudaSetDevice(E->device);
+  LVTRY(ensure_capacity(E, n, 2 * m, true));
+  uint32_t *d_src = nullptr, *d_dst = nullptr;
+  float* d_w = nullptr;
+  struct Tmp {
+    uint32_t*& a;
+    uint32_t*& b;
+    float*& c;
+    ~Tmp() {
+      dfree(a);
+      dfree(b);
+      dfree(c);
+    }
+  } tmp{d_src, d_dst, d_w};
+  CU(dalloc(&d_src, m));
+  CU(dalloc(&d_dst, m));
+  if (w) CU(dalloc(&d_w, m));
+  if (m) {
+    CU(cudaMemcpyAsync(d_src, src, m * sizeof(uint32_t), cudaMemcpyHostToDevice, E->st));
+    CU(cudaMemcpyAsync(d_dst, dst, m * sizeof(uint32_t), cudaMemcpyHostToDevice, E->st));
+    if (w) CU(cudaMemcpyAsync(d_w, w, m * sizeof(float), cudaMemcpyHostToDevice, E->st));
+  }
+  uint64_t nnz = 0;
+  uint32_t bad = 0;
+  CU(csr_from_edges_device(n, m, d_src, d_dst, d_w, E->own_off, E->own_col, E->own_w, &nnz, &bad,
+                           E->st));
+  if (bad) return fail(LV_ERR_PARSE, "vertex index exceeds the vertex count");
+  E->in_off = E->own_off;
+  E->in_col = E->own_col;
+  E->in_w = E->own_w;
+  return load_common(E, n, nnz);
+}
+
+lv_status lv_engine_load_edges(lv_engine* E, uint32_t n, uint64_t m, const uint32_t* src,
+                               const uint32_t* dst, const float* w) {
+  AllocScope alloc_scope(E);
+  if (!E || (m && (!src || !dst))) return fail(LV_ERR_ARG, "NULL argument");
+  return load_edges_common(E, n, m, src, dst, w);
+}
+
+lv_status lv_engine_load_mtx(lv_engine* E, const char* path) {
+  AllocScope alloc_scope(E);
+  if (!E || !path) return fail(LV_ERR_ARG, "NULL argument");
+  uint32_t n = 0;
+  std::vector<uint32_t> src, dst;
+  std::vector<float> ws;
+  LVTRY(lvb_parse_mtx(path, &n, src, dst, ws));
+  return load_edges_common(E, n, src.size(), src.data(), dst.data(), ws.data());
+}
+
+lv_status lv_csr_from_edges_device(uint32_t n, uint64_t m, const uint32_t* d_src,
+                                   const uint32_t* d_dst, const float* d_w, uint64_t* d_off,
+                                   uint32_t* d_col, float* d_w_out, uint64_t* nnz,
+                                   void* stream) {
+  if (!d_off || !nnz || (m && (!d_src || !d_dst || !d_col || !d_w_out)))
+    return fail(LV_ERR_ARG, "NULL argument");
+  if (n >= 0xFFFFFFFFu) return fail(LV_ERR_LIMIT, "vertex count must be < 2^32-1");
+  if (m >= (1ull << 31)) return fail(LV_ERR_LIMIT, "at most 2^31 - 1 edge lines");
+  uint32_t bad = 0;
+  uint64_t h_nnz = 0;
+  CU(csr_from_edges_device(n, m, d_src, d_dst, d_w, d_off, d_col, d_w_out, &h_nnz, &bad,
+                           static_cast<cudaStream_t>(stream)));
+  if (bad) return fail(LV_ERR_PARSE, "vertex index exceeds the vertex count");
+  *nnz = h_nnz;
+  return LV_OK;
+}
+
 lv_status lv_engine_load_device(lv_engine* E, uint32_t n, uint64_t nnz,
                                 const uint64_t* d_off, const uint32_t* d_col,
                                 const float* d_w) {
@@ -2035,6 +2111,34 @@ lv_status lv_get_assignment(lv_engine* E, uint32_t* out, size_t n) {
     CU(cudaMemcpyAsync(out, src, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, E->st));
     CU(cudaStreamSynchronize(E->st));
   }
+  return LV_OK;
+}
+
+lv_status lv_get_communities(lv_engine* E, uint32_t* out, size_t cap, uint32_t* n_comm) {
+  AllocScope alloc_scope(E);
+  if (!E || !n_comm) return fail(LV_ERR_ARG, "NULL argument");
+  if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
+  cudaSetDevice(E->device);
+  const uint32_t n = E->n0;
+  // the final communities are dense ids < the level's vertex count
+  const uint32_t c = n ? E->n : 0u;
+  *n_comm = c;
+  const size_t need = (size_t)c + 1 + n;
+  if (!out) return LV_OK;  // size query
+  if (cap < need) return fail(LV_ERR_ARG, "buffer shorter than n_communities + 1 + n");
+  uint32_t* part = E->assignment;
+  if (E->accepted && n) {  // the level's moves count: comm[assignment]
+    CU(launch_gather(E->cb.members, E->assignment, n, E->comm, E->st));
+    part = E->cb.members;
+  }
+  uint32_t* d_out = nullptr;
+  CU(dalloc(&d_out, need));
+  cudaError_t ce = group_by_community(part, n, c, d_out, E->st);
+  if (ce == cudaSuccess)
+    ce = cudaMemcpyAsync(out, d_out, need * sizeof(uint32_t), cudaMemcpyDeviceToHost, E->st);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(E->st);
+  dfree(d_out);
+  CU(ce);
   return LV_OK;
 }
 

@@ -121,11 +121,11 @@ lv_status lvb_graph_build(uint32_t n, uint64_t m, const uint32_t* src,
   return LV_OK;
 }
 
-extern "C" {
-
-lv_status lv_graph_load_mtx(const char* path, lv_graph** out) {
-  if (!path || !out) return io_fail(LV_ERR_ARG, "NULL argument");
-  *out = nullptr;
+// Parses a Matrix Market file into its edge lines (0-based indices, |w|,
+// a weightless line repeating the previous weight), validated against the
+// size line's vertex count.
+lv_status lvb_parse_mtx(const char* path, uint32_t* n_out, std::vector<uint32_t>& src,
+                        std::vector<uint32_t>& dst, std::vector<float>& ws) {
   FILE* f = fopen(path, "rb");
   if (!f) return io_fail(LV_ERR_IO, "Error opening file");
   std::string data;
@@ -172,8 +172,6 @@ lv_status lv_graph_load_mtx(const char* path, lv_graph** out) {
   }
   (void)rows;
   if (cols >= 0xFFFFFFFFull) return io_fail(LV_ERR_LIMIT, "vertex count must be < 2^32-1");
-  std::vector<uint32_t> src, dst;
-  std::vector<float> ws;
   try {
     src.resize(nnz);
     dst.resize(nnz);
@@ -303,8 +301,22 @@ lv_status lv_graph_load_mtx(const char* path, lv_graph** out) {
     if (src[i] >= n || dst[i] >= n)
       return io_fail(LV_ERR_PARSE, "vertex index exceeds the size line's count");
   }
+  *n_out = n;
+  return LV_OK;
+}
+
+extern "C" {
+
+lv_status lv_graph_load_mtx(const char* path, lv_graph** out) {
+  if (!path || !out) return io_fail(LV_ERR_ARG, "NULL argument");
+  *out = nullptr;
+  uint32_t n = 0;
+  std::vector<uint32_t> src, dst;
+  std::vector<float> ws;
+  lv_status s = lvb_parse_mtx(path, &n, src, dst, ws);
+  if (s != LV_OK) return s;
   std::string err;
-  lv_status s = lvb_graph_build(n, nnz, src.data(), dst.data(), ws.data(), out, &err);
+  s = lvb_graph_build(n, src.size(), src.data(), dst.data(), ws.data(), out, &err);
   if (s != LV_OK) return io_fail(s, err.empty() ? "graph construction failed" : err);
   return LV_OK;
 }

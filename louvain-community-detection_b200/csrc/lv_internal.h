@@ -410,6 +410,32 @@ cudaError_t configure_kernels();
 cudaError_t configure_contract_kernels();
 
 // ---------------------------------------------------------------------------
+// sort.cu
+// ---------------------------------------------------------------------------
+// Stable LSD radix sort of (key, u32 value) pairs on the low key_bits bits;
+// the result is in keys/vals, or in keys_alt/vals_alt when *result_in_alt.
+// counts needs radix_sort_scratch_words(n) words, S a scan of that size.
+size_t radix_sort_scratch_words(uint64_t n);
+template <typename K>
+cudaError_t radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
+                             uint64_t n, int key_bits, uint32_t* counts, ScanScratch& S,
+                             cudaStream_t st, bool* result_in_alt);
+// CSR of an edge list with the reference reader's layout (utils.cu:168-229):
+// every row in file order, an off-diagonal edge stored in both rows, a
+// self-loop once, |w| (1 without weights).  col/wout need room for 2m
+// entries; *nnz_host receives the entry count, *bad_host 1 when an index
+// is >= n.  Synchronises the stream; scratch is stream-ordered.
+cudaError_t csr_from_edges_device(uint32_t n, uint64_t m, const uint32_t* src,
+                                  const uint32_t* dst, const float* w, uint64_t* off,
+                                  uint32_t* col, float* wout, uint64_t* nnz_host,
+                                  uint32_t* bad_host, cudaStream_t st);
+// Community listing on the device: out[0..n_comm] the offsets of every
+// community's members, out[n_comm + 1 ..] the members (ascending within a
+// community).  part[v] < n_comm.
+cudaError_t group_by_community(const uint32_t* part, uint32_t n, uint32_t n_comm,
+                               uint32_t* out, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
 // contract.cu
 // ---------------------------------------------------------------------------
 struct ContractBuffers {

@@ -4,6 +4,7 @@
 #include <getopt.h>
 #include <sys/stat.h>
 
+#include <cstdio>
 #include <cstdlib>
 #include <iostream>
 #include <iterator>
@@ -17,10 +18,19 @@ static void check(lv_status s) {
 
 static bool g_use_cache = false;
 void setCsrCache(bool on) { g_use_cache = on; }
+static bool g_device_csr = false;
+void setDeviceCsr(bool on) { g_device_csr = on; }
 
 // With the cache on, `<file>.lvbcsr` (a binary CSR newer than the file)
 // replaces the text parse, and is written after a parse.
 void parseGraph(Graph& graph, const char* filename) {
+  if (g_device_csr) {  // the engine parses and builds the CSR on the device
+    FILE* f = fopen(filename, "rb");
+    if (!f) throw Error(LV_ERR_IO, "Error opening file");
+    fclose(f);
+    graph.path = filename;
+    return;
+  }
   lv_graph* g = nullptr;
   const std::string cache = std::string(filename) + ".lvbcsr";
   struct stat sm {}, sc {};
@@ -46,16 +56,25 @@ void initDevGraph(Graph& dev_graph, const Graph& host_graph, const lv_config* cf
   check(lv_engine_create(cfg, &e));
   dev_graph.dev = e;
   dev_graph.rule = cfg ? cfg->rule : LV_RULE_PY;
-  lv_status s = lv_engine_load(e, host_graph.host);
+  lv_status s = host_graph.host ? lv_engine_load(e, host_graph.host)
+                                : lv_engine_load_mtx(e, host_graph.path.c_str());
   if (s != LV_OK) {
     lv_engine_destroy(e);
     dev_graph.dev = nullptr;
     check(s);
   }
-  dev_graph.vert_sz = host_graph.vert_sz;
-  dev_graph.init_sz = host_graph.init_sz;
-  dev_graph.edges_sz = host_graph.edges_sz;
-  dev_graph.max_deg = host_graph.max_deg;
+  if (host_graph.host) {
+    dev_graph.vert_sz = host_graph.vert_sz;
+    dev_graph.init_sz = host_graph.init_sz;
+    dev_graph.edges_sz = host_graph.edges_sz;
+    dev_graph.max_deg = host_graph.max_deg;
+  } else {
+    uint32_t n = 0;
+    uint64_t ne = 0;
+    check(lv_get_level_size(e, &n, &ne));
+    dev_graph.vert_sz = dev_graph.init_sz = n;
+    dev_graph.edges_sz = ne;
+  }
 }
 
 bool modularityOptimization(Graph& dev_graph, float threshold) {
@@ -78,24 +97,19 @@ void aggregation(Graph& dev_graph) {
   dev_graph.edges_sz = e;
 }
 
-// Groups the vertices by community with one counting sort (vertex ids stay
-// ascending inside a community, as the reference's push_back order leaves
-// them) and writes the listing through one buffer.
+// The vertices grouped by community on the device (lv_get_communities:
+// a stable sort by community, so vertex ids stay ascending inside a
+// community, as the reference's push_back order leaves them; one copy to
+// the host), written through one buffer.
 void printCommunities(Graph& dev_graph) {
   const size_t n0 = dev_graph.init_sz;
-  const size_t nc = dev_graph.vert_sz;
-  std::vector<uint32_t> comm(n0);
-  check(lv_get_assignment(dev_graph.dev, comm.data(), comm.size()));
-  std::vector<uint64_t> start(nc + 1, 0);
-  for (size_t i = 0; i < n0; i++)
-    if (comm[i] < nc) start[(size_t)comm[i] + 1]++;
-  for (size_t c = 0; c < nc; c++) start[c + 1] += start[c];
-  std::vector<uint32_t> members(start[nc]);
-  {
-    std::vector<uint64_t> cur(start.begin(), start.end() - 1);
-    for (size_t i = 0; i < n0; i++)
-      if (comm[i] < nc) members[cur[comm[i]]++] = (uint32_t)i + 1;
-  }
+  uint32_t c = 0;
+  check(lv_get_communities(dev_graph.dev, nullptr, 0, &c));
+  std::vector<uint32_t> grouped((size_t)c + 1 + n0);
+  check(lv_get_communities(dev_graph.dev, grouped.data(), grouped.size(), &c));
+  const size_t nc = c;
+  const uint32_t* start = grouped.data();
+  const uint32_t* members = grouped.data() + nc + 1;
   std::string out;
   out.reserve(16 * (n0 + nc) + 32);
   char num[24];
@@ -115,7 +129,7 @@ void printCommunities(Graph& dev_graph) {
     put(comm_n++);
     out.push_back(' ');
     for (uint64_t k = start[c]; k < start[c + 1]; k++) {
-      put(members[k]);
+      put((uint64_t)members[k] + 1);  // 1-based, utils.cu:287
       out.push_back(' ');
     }
     out.push_back('\n');
@@ -131,6 +145,7 @@ void parseArgs(int argc, char** argv, float& threshold, bool& verbose,
       {"gain", required_argument, nullptr, 'p'},
       {"timing", no_argument, nullptr, 't'},
       {"cache", no_argument, nullptr, 'c'},
+      {"gpu-csr", no_argument, nullptr, 'd'},
       {nullptr, 0, nullptr, 0}};
   const char* usage = "Usage: ./gpulouvain -f mtx-matrix-file -g min-gain [-v]";
   bool fopt = false, gopt = false;
@@ -181,6 +196,9 @@ void parseArgs(int argc, char** argv, float& threshold, bool& verbose,
         break;
       case 'c':
         setCsrCache(true);
+        break;
+      case 'd':
+        setDeviceCsr(true);
         break;
       case '?':
         std::cout << usage << std::endl;

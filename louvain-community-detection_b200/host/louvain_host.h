@@ -31,12 +31,17 @@ struct Graph {
   size_t init_sz = 0;   // input vertex count
   unsigned int max_deg = 0;
   lv_rule rule = LV_RULE_PY;
+  std::string path;  // --gpu-csr: the file the engine parses itself
 };
 
 // parseGraph (utils.cu:168-229): Matrix Market file -> host CSR.
 void parseGraph(Graph& graph, const char* filename);
 // This build's --cache: parseGraph keeps a binary CSR beside the file.
 void setCsrCache(bool on);
+// This build's --gpu-csr: parseGraph only checks the file; initDevGraph
+// parses it on the host and builds the CSR on the device
+// (lv_engine_load_mtx).
+void setDeviceCsr(bool on);
 
 // initDevGraph + copyToDevice + initCommAggr + setInitComm
 // (utils.cu:66-108): create the engine and upload the graph.
@@ -55,8 +60,8 @@ void aggregation(Graph& dev_graph);
 void printCommunities(Graph& dev_graph);
 
 // parseArgs (utils.cu:231-267): -f file -g min_gain [-v]; this build adds
-// --rule py|cuda, --gain fp32|fp64, --timing (per-level times on stderr)
-// and --cache.
+// --rule py|cuda, --gain fp32|fp64, --timing (per-level times on stderr),
+// --cache and --gpu-csr.
 void parseArgs(int argc, char** argv, float& threshold, bool& verbose,
                char*& filename, lv_rule& rule, bool& timing, lv_gain& gain);
 

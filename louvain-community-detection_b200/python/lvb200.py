@@ -159,6 +159,12 @@ _SIGS = {
     "lv_reset_kernel_stats": (ctypes.c_int, [_VP]),
     "lv_get_launch_count": (ctypes.c_int, [ctypes.POINTER(_U64)]),
     "lv_debug_fail_device_alloc": (ctypes.c_int, [_U64]),
+    "lv_engine_load_edges": (ctypes.c_int, [_VP, _U32, _U64, _VP, _VP, _VP]),
+    "lv_engine_load_mtx": (ctypes.c_int, [_VP, ctypes.c_char_p]),
+    "lv_csr_from_edges_device": (ctypes.c_int, [_U32, _U64, _VP, _VP, _VP, _VP, _VP, _VP,
+                                                ctypes.POINTER(_U64), _VP]),
+    "lv_get_communities": (ctypes.c_int, [_VP, _VP, ctypes.c_size_t,
+                                          ctypes.POINTER(_U32)]),
     "lv_modularity_noalloc": (ctypes.c_int, [_U32, _VP, _VP, _VP, _VP, _VP,
                                              ctypes.POINTER(ctypes.c_double), _VP]),
     "lv_batch_run_device": (ctypes.c_int, [_VP, _U32, _VP, _U32, _U64, _VP, _VP, _VP,
@@ -391,6 +397,31 @@ class Engine:
     def load(self, g: Graph):
         _check(lib().lv_engine_load(self._h, g._h))
         self.n0 = self._level_size()[0]
+
+    def load_edges(self, n: int, src, dst, w=None):
+        """Edge lines (host) -> the reference reader's CSR built on the device."""
+        src = np.ascontiguousarray(src, dtype=np.uint32)
+        dst = np.ascontiguousarray(dst, dtype=np.uint32)
+        wp = None
+        if w is not None:
+            w = np.ascontiguousarray(w, dtype=np.float32)
+            wp = _p(w)
+        _check(lib().lv_engine_load_edges(self._h, n, len(src), _p(src), _p(dst), wp))
+        self.n0 = n
+
+    def load_mtx(self, path: str):
+        """Matrix Market file -> host parse -> CSR built on the device."""
+        _check(lib().lv_engine_load_mtx(self._h, path.encode()))
+        self.n0 = self._level_size()[0]  # level 0 = the input graph
+
+    def communities(self):
+        """(offsets, members) of the final partition, grouped on the device."""
+        c = _U32()
+        _check(lib().lv_get_communities(self._h, None, 0, ctypes.byref(c)))
+        out = np.zeros(int(c.value) + 1 + self.n0, dtype=np.uint32)
+        _check(lib().lv_get_communities(self._h, _p(out), out.size, ctypes.byref(c)))
+        k = int(c.value)
+        return out[:k + 1].copy(), out[k + 1:].copy()
 
     def load_device(self, n: int, nnz: int, d_off: int, d_col: int, d_w: int):
         _check(lib().lv_engine_load_device(self._h, n, nnz, d_off, d_col, d_w))
