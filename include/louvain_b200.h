@@ -79,6 +79,10 @@ typedef struct lv_config {
                                persistent cooperative kernel per level; 0
                                (default): per-kernel launches, in a level
                                graph or from the host as use_graphs says    */
+    int contract_sort;      /* 1: contract a single graph by sorting the
+                               entries by (new row, new column) and summing
+                               runs (rows then ordered by column); 0
+                               (default): hash merge per community        */
 } lv_config;
 
 /* Per-level record (the reference prints none of this; -v here adds it). */

@@ -531,6 +531,110 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Contraction by sorting: every entry (u, v) gets the key
+// (new id of comm(u), new id of comm(v)); a stable radix sort brings equal
+// keys together, a segmented reduction sums their weights (FP64, rounded
+// once) and the sorted row ids give the new offsets.  Rows come out sorted
+// by column.
+// ---------------------------------------------------------------------------
+__global__ void cnew_kernel(const uint32_t* __restrict__ comm, const uint32_t* __restrict__ new_id,
+                            uint32_t n, uint32_t* __restrict__ cnew) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    cnew[v] = new_id[comm[v]];
+}
+
+__global__ void sort_keys_kernel(const uint32_t* __restrict__ rowid,
+                                 const uint32_t* __restrict__ col,
+                                 const uint32_t* __restrict__ cnew, uint64_t nnz, int bits,
+                                 uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < nnz;
+       j += (uint64_t)gridDim.x * blockDim.x) {
+    keys[j] = ((uint64_t)cnew[rowid[j]] << bits) | cnew[col[j]];
+    vals[j] = (uint32_t)j;
+  }
+}
+
+__global__ void heads_kernel(const uint64_t* __restrict__ keys, uint64_t nnz,
+                             uint32_t* __restrict__ heads) {
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < nnz;
+       j += (uint64_t)gridDim.x * blockDim.x)
+    heads[j] = (j == 0 || keys[j] != keys[j - 1]) ? 1u : 0u;
+}
+
+__global__ void zero_f64_kernel(double* a, const uint32_t* d_count, uint64_t cap) {
+  const uint64_t n = min((uint64_t)*d_count, cap);
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    a[i] = 0.0;
+}
+
+// Run r(j) = heads up to j - 1.  Weights of a run are summed in the warp
+// (runs are contiguous) and once per warp segment into acc[r]; FP64 sums of
+// FP32 weights are exact whatever the order.  Heads write the new entry's
+// column and row.
+__global__ void __launch_bounds__(256)
+    run_reduce_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                      const uint32_t* __restrict__ heads, const uint32_t* __restrict__ pos,
+                      uint64_t nnz, const float* __restrict__ w, int bits,
+                      double* __restrict__ acc, uint32_t* __restrict__ out_col,
+                      uint32_t* __restrict__ row_of) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t mask = (1ull << bits) - 1ull;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t j0 = blockIdx.x * (uint64_t)blockDim.x; j0 < nnz; j0 += stride) {
+    const uint64_t j = j0 + threadIdx.x;  // whole warps iterate together
+    const bool valid = j < nnz;
+    uint32_t r = 0xFFFFFFFFu;
+    double x = 0.0;
+    if (valid) {
+      const uint32_t h = heads[j];
+      r = pos[j] + h - 1u;
+      x = (double)w[vals[j]];
+      if (h) {
+        const uint64_t k = keys[j];
+        out_col[r] = (uint32_t)(k & mask);
+        row_of[r] = (uint32_t)(k >> bits);
+      }
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const double y = __shfl_down_sync(kFull, x, o);
+      const uint32_t ry = __shfl_down_sync(kFull, r, o);
+      if (lane + o < 32 && ry == r) x += y;
+    }
+    const uint32_t rp = __shfl_up_sync(kFull, r, 1);
+    if (valid && (lane == 0 || rp != r)) atomicAdd(&acc[r], x);
+  }
+}
+
+// off[v] = first new entry of row >= v for v in [0, n_rows]; the entry count
+// is read on the device.
+__global__ void bounds_dev_kernel(const uint32_t* __restrict__ row_of, const uint32_t* d_total,
+                                  uint64_t cap, uint32_t n_rows, uint64_t* __restrict__ off) {
+  const uint64_t total = min((uint64_t)*d_total, cap);
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j <= total;
+       j += (uint64_t)gridDim.x * blockDim.x) {
+    const int64_t prev = j ? (int64_t)row_of[j - 1] : -1;
+    const uint32_t cur = j < total ? row_of[j] : n_rows;
+    for (int64_t v = prev + 1; v <= (int64_t)cur && v <= (int64_t)n_rows; v++) off[v] = j;
+  }
+}
+
+__global__ void round_f64_kernel(const double* __restrict__ acc, const uint32_t* d_count,
+                                 uint64_t cap, float* __restrict__ out) {
+  const uint64_t n = min((uint64_t)*d_count, cap);
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = (float)acc[i];
+}
+
+int bits_of(uint64_t max_value) {
+  int b = 0;
+  while (b < 64 && (max_value >> b)) b++;
+  return b;
+}
+
 unsigned gridcap(uint64_t work, unsigned per_sm) {
   const uint64_t cap = (uint64_t)sm_count_cached() * per_sm;
   if (work == 0) return 1;
@@ -703,6 +807,65 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
   LV_TRY(cudaStreamSynchronize(st));
   res->new_n = new_n;
   res->new_nnz = h_total;
+  return cudaSuccess;
+}
+
+cudaError_t contract_level_sort(const LevelView& L, uint64_t nnz, ContractBuffers& B,
+                                SortBuffers& SB, ScanScratch& S, uint64_t* out_off,
+                                uint32_t* out_col, float* out_w, ContractResult* res,
+                                cudaStream_t st) {
+  const uint32_t n = L.n;
+  uint32_t* h_counts = B.host_counts;
+  const unsigned gv = gridcap((n + 255) / 256, 8);
+  const unsigned ge = gridcap((nnz + 255) / 256, 8);
+  // renumbering as the hash path (aggregation.cu:389-393)
+  (count_launches(1), flags_kernel<<<gv, 256, 0, st>>>(L.comm_sz, n, B.flag_id, B.mem_off, B.cursor));
+  LV_TRY(cudaGetLastError());
+  LV_TRY(exclusive_scan_u32(B.flag_id, B.flag_id, n, B.counts + 0, S, st));
+  (count_launches(1), cnew_kernel<<<gv, 256, 0, st>>>(L.comm, B.flag_id, n, B.cnew));
+  LV_TRY(cudaGetLastError());
+  // keys of every entry; the level's row ids first (the contraction's
+  // column scratch holds no other data at this point)
+  uint32_t* rowid = B.tcol;
+  LV_TRY(launch_row_ids(L.off, n, nnz, rowid, st));
+  const int bits = std::max(1, bits_of(n ? n - 1 : 0));
+  if (nnz) {
+    (count_launches(1), sort_keys_kernel<<<ge, 256, 0, st>>>(rowid, L.col, B.cnew, nnz, bits,
+                                                             SB.keys[0], SB.vals[0]));
+    LV_TRY(cudaGetLastError());
+  }
+  bool alt = false;
+  LV_TRY(radix_sort_pairs<uint64_t>(SB.keys[0], SB.vals[0], SB.keys[1], SB.vals[1], nnz, 2 * bits,
+                                    SB.counts, SB.scan, st, &alt));
+  const uint64_t* keys = SB.keys[alt ? 1 : 0];
+  const uint32_t* vals = SB.vals[alt ? 1 : 0];
+  double* acc = reinterpret_cast<double*>(SB.keys[alt ? 0 : 1]);  // the idle key buffer
+  uint32_t* heads = SB.vals[alt ? 0 : 1];                         // the idle value buffer
+  uint32_t* row_of = reinterpret_cast<uint32_t*>(B.tw);
+  uint32_t* d_new_nnz = B.counts + 2;
+  if (nnz) {
+    (count_launches(1), heads_kernel<<<ge, 256, 0, st>>>(keys, nnz, heads));
+    LV_TRY(cudaGetLastError());
+    LV_TRY(exclusive_scan_u32(heads, SB.pos, nnz, d_new_nnz, SB.scan, st));
+    (count_launches(1), zero_f64_kernel<<<ge, 256, 0, st>>>(acc, d_new_nnz, nnz));
+    LV_TRY(cudaGetLastError());
+    (count_launches(1), run_reduce_kernel<<<ge, 256, 0, st>>>(keys, vals, heads, SB.pos, nnz, L.w,
+                                                              bits, acc, out_col, row_of));
+    LV_TRY(cudaGetLastError());
+  } else {
+    LV_TRY(cudaMemsetAsync(d_new_nnz, 0, sizeof(uint32_t), st));
+  }
+  // new offsets over the old vertex count: rows past the new count are
+  // empty and sit beyond the new CSR's n'+1 offsets
+  (count_launches(1), bounds_dev_kernel<<<gridcap((nnz + 256) / 256, 8), 256, 0, st>>>(
+                          row_of, d_new_nnz, nnz, n, out_off));
+  LV_TRY(cudaGetLastError());
+  (count_launches(1), round_f64_kernel<<<ge, 256, 0, st>>>(acc, d_new_nnz, nnz, out_w));
+  LV_TRY(cudaGetLastError());
+  LV_TRY(cudaMemcpyAsync(h_counts, B.counts, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  LV_TRY(cudaStreamSynchronize(st));
+  res->new_n = h_counts[0];
+  res->new_nnz = h_counts[2];
   return cudaSuccess;
 }
 

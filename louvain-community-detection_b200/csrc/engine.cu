@@ -256,6 +256,8 @@ struct lv_engine {
 
   ContractBuffers cb{};
   ScanScratch scan;
+  SortBuffers sb{};             // contraction by sorting (on demand)
+  unsigned char* sb_scan = nullptr;
 
   // current level
   uint32_t n0 = 0;
@@ -501,6 +503,16 @@ void free_state(lv_engine* E) {
   if (E->scan.buf) cudaFree(E->scan.buf);
   E->scan.buf = nullptr;
   E->scan.bytes = 0;
+  E->sb.cap = 0;
+  dfree(E->sb.keys[0]);
+  dfree(E->sb.keys[1]);
+  dfree(E->sb.vals[0]);
+  dfree(E->sb.vals[1]);
+  dfree(E->sb.pos);
+  dfree(E->sb.counts);
+  dfree(E->sb_scan);
+  E->sb.scan.buf = nullptr;
+  E->sb.scan.bytes = 0;
   E->partials_cap = E->hub_map_cap = 0;
   E->hub_count_cap = E->hub_blocks_cap = E->hub_units_cap = 0;
   E->hub_stage_cap = E->hub_ct_cap = 0;
@@ -1667,6 +1679,7 @@ void lv_config_default(lv_config* cfg) {
   cfg->stream = nullptr;
   cfg->gain = LV_GAIN_FP32;
   cfg->level_kernel = 0;
+  cfg->contract_sort = 0;
 }
 
 lv_status lv_engine_create(const lv_config* cfg, lv_engine** out) {
@@ -1962,6 +1975,33 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
   return LV_OK;
 }
 
+// Entry-sized buffers of the contraction by sorting, grown on demand.
+lv_status ensure_sort_buffers(lv_engine* E, uint64_t nnz) {
+  SortBuffers& S = E->sb;
+  if (nnz <= S.cap && S.keys[0]) return LV_OK;
+  S.cap = 0;  // zeroed before the frees (see grow_tables)
+  dfree(S.keys[0]);
+  dfree(S.keys[1]);
+  dfree(S.vals[0]);
+  dfree(S.vals[1]);
+  dfree(S.pos);
+  dfree(S.counts);
+  dfree(E->sb_scan);
+  S.scan.buf = nullptr;
+  const size_t cap = std::max<uint64_t>(nnz, 1024);
+  CU(dalloc(&S.keys[0], cap));
+  CU(dalloc(&S.keys[1], cap));
+  CU(dalloc(&S.vals[0], cap));
+  CU(dalloc(&S.vals[1], cap));
+  CU(dalloc(&S.pos, cap));
+  CU(dalloc(&S.counts, radix_sort_scratch_words(cap)));
+  S.scan.bytes = scan_scratch_bytes(cap + 1024);
+  CU(dalloc(&E->sb_scan, S.scan.bytes));
+  S.scan.buf = E->sb_scan;
+  S.cap = cap;
+  return LV_OK;
+}
+
 lv_status lv_phase_aggregate(lv_engine* E) {
   AllocScope alloc_scope(E);
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
@@ -1972,8 +2012,14 @@ lv_status lv_phase_aggregate(lv_engine* E) {
   ContractResult r{};
   cudaEvent_t t0 = prof_begin(E);
   g_trace.reset();
-  CU(contract_level(E->view(), E->e, E->cb, E->scan, E->c_off[next], E->c_col[next],
-                    E->c_w[next], &r, E->st, grow_tables, E));
+  if (!E->batch && E->cfg.contract_sort) {
+    LVTRY(ensure_sort_buffers(E, E->e));
+    CU(contract_level_sort(E->view(), E->e, E->cb, E->sb, E->scan, E->c_off[next],
+                           E->c_col[next], E->c_w[next], &r, E->st));
+  } else {
+    CU(contract_level(E->view(), E->e, E->cb, E->scan, E->c_off[next], E->c_col[next],
+                      E->c_w[next], &r, E->st, grow_tables, E));
+  }
   g_trace.mark("contract", (uint32_t)E->levels.size(), E->n);
   // B_agg = E*12 + V*(off + comm + new id + member) + E'*8 + (V'+1)*off
   prof_end(E, t0, K_CONTRACT,

@@ -473,6 +473,22 @@ struct ContractResult {
   uint32_t new_n;
   uint64_t new_nnz;
 };
+// Buffers of the contraction by sorting (entry-sized, engine-owned).
+struct SortBuffers {
+  uint64_t* keys[2] = {nullptr, nullptr};  // (new row << bits) | new column
+  uint32_t* vals[2] = {nullptr, nullptr};  // entry index
+  uint32_t* pos = nullptr;                 // scanned run heads
+  uint32_t* counts = nullptr;              // radix digit counts
+  ScanScratch scan;                        // scans of entry-sized arrays
+  uint64_t cap = 0;                        // entries the buffers hold
+};
+// Contraction by sorting (single graph): the same new ids, offsets and row
+// sets as contract_level, rows sorted by column.  Synchronises the stream
+// once at the end.
+cudaError_t contract_level_sort(const LevelView& L, uint64_t nnz, ContractBuffers& B,
+                                SortBuffers& SB, ScanScratch& S, uint64_t* out_off,
+                                uint32_t* out_col, float* out_w, ContractResult* res,
+                                cudaStream_t st);
 // Contracts level (L, comm) into (out_off, out_col, out_w); writes cnew
 // (vertex -> new id) for composing the assignment.  Synchronises the
 // stream internally (sizes are needed on the host).
