@@ -690,7 +690,7 @@ def run_engine(args, rank, world):
     launches_k = max(st["launches"], 1)
     achieved = (st["bytes"] / launches_k) / (st["total_ms"] / launches_k / 1000.0) / 1e9
     traffic = ncu_traffic(name)
-    cpu = cpu_baseline(n, off, col, ww) if world == 1 else None
+    cpu = cpu_baseline(n, off, col, ww) if world == 1 and not args.no_cpu_baseline else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
@@ -748,6 +748,8 @@ def main():
                          "graphs with conditional nodes)")
     ap.add_argument("--hbm-scale", type=int, default=24,
                     help="R-MAT scale of the HBM-scale plain-engine measurement (0: skip)")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the CPU baseline leg (profiling runs)")
     ap.add_argument("--no-oracle-check", action="store_true",
                     help="skip the untimed FP64-gain run and host oracle on the HBM-scale graph")
     ap.add_argument("--batch-graphs", type=int, default=4096,
