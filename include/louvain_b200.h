@@ -432,6 +432,12 @@ lv_status lv_reset_kernel_stats(lv_engine *e);
 /* Kernels this library has launched in the process so far (all engines). */
 lv_status lv_get_launch_count(uint64_t *count);
 
+/* Times the library has made the host wait for a stream (all engines): a
+ * single graph's level costs the class counts of its set-up, the level
+ * graph's result and the contraction's class sizes (plus one for hubs and
+ * one for the largest communities' tables when a level has them).        */
+lv_status lv_get_sync_count(uint64_t *count);
+
 /* ---- fault injection, for tests (no counterpart in the reference, which
  * exits on any CUDA error, utils.cuh:95-100) -------------------------------
  * From this call on, the nth device allocation the library makes (n >= 1)

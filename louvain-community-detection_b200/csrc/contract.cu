@@ -669,7 +669,7 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
                            uint64_t* out_off, uint32_t* out_col, float* out_w,
                            ContractResult* res, cudaStream_t st,
                            cudaError_t (*grow)(void*, size_t, size_t),
-                           void* grow_ctx) {
+                           void* grow_ctx, bool defer_total) {
   const uint32_t n = L.n;
   (void)nnz;
   uint32_t* h_counts = B.host_counts;
@@ -696,7 +696,7 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
                             kMergeBlockMax, B.comm_cls, B.counts + 4, B.tmp, S, st));
   LV_TRY(cudaMemcpyAsync(h_counts, B.counts, 8 * sizeof(uint32_t),
                          cudaMemcpyDeviceToHost, st));
-  LV_TRY(cudaStreamSynchronize(st));
+  LV_TRY(counted_sync(st));
   const uint32_t new_n = h_counts[0];
   const uint32_t cntW = h_counts[4], cntM = h_counts[5], cntB2 = h_counts[6];
   const uint32_t cntB = cntM + cntB2;  // both block classes
@@ -741,7 +741,7 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
     std::vector<uint64_t> gdeg(cntG);
     LV_TRY(cudaMemcpyAsync(gdeg.data(), B.g_tab_off, cntG * sizeof(uint64_t),
                            cudaMemcpyDeviceToHost, st));
-    LV_TRY(cudaStreamSynchronize(st));
+    LV_TRY(counted_sync(st));
     std::vector<uint64_t> tab_off(cntG);
     std::vector<uint32_t> tab_size(cntG);
     std::vector<uint32_t> blk_comm, blk_chunk, blk_nch;
@@ -793,7 +793,7 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
     (count_launches(1), merge_global_emit_kernel<<<gridcap(nblk, 8), kThreads, 0, st>>>(C, G));
     LV_TRY(cudaGetLastError());
     // host vectors must outlive the async copies
-    LV_TRY(cudaStreamSynchronize(st));
+    LV_TRY(counted_sync(st));
   }
   // new offsets: exclusive scan of the n'+1 counts (last one is 0)
   uint64_t* d_total = reinterpret_cast<uint64_t*>(B.counts + 8);
@@ -801,12 +801,15 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
   (count_launches(1), compress_kernel<<<gridcap((new_n + kWarps - 1) / kWarps, 8), kThreads, 0, st>>>(
       B.seg, out_off, new_n, B.tcol, B.tw, out_col, out_w));
   LV_TRY(cudaGetLastError());
-  uint64_t h_total = 0;
-  LV_TRY(cudaMemcpyAsync(&h_total, d_total, sizeof(uint64_t),
-                         cudaMemcpyDeviceToHost, st));
-  LV_TRY(cudaStreamSynchronize(st));
   res->new_n = new_n;
-  res->new_nnz = h_total;
+  if (defer_total) {  // the caller reads B.counts + 8 at its next sync
+    res->new_nnz = ~0ull;
+    return cudaSuccess;
+  }
+  uint64_t* h_total = reinterpret_cast<uint64_t*>(h_counts + 8);  // pinned
+  LV_TRY(cudaMemcpyAsync(h_total, d_total, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  LV_TRY(counted_sync(st));
+  res->new_nnz = *h_total;
   return cudaSuccess;
 }
 
@@ -863,7 +866,7 @@ cudaError_t contract_level_sort(const LevelView& L, uint64_t nnz, ContractBuffer
   (count_launches(1), round_f64_kernel<<<ge, 256, 0, st>>>(acc, d_new_nnz, nnz, out_w));
   LV_TRY(cudaGetLastError());
   LV_TRY(cudaMemcpyAsync(h_counts, B.counts, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-  LV_TRY(cudaStreamSynchronize(st));
+  LV_TRY(counted_sync(st));
   res->new_n = h_counts[0];
   res->new_nnz = h_counts[2];
   return cudaSuccess;

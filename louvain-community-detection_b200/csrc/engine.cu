@@ -203,6 +203,12 @@ void count_launches(unsigned k) {
   g_launches.fetch_add(k, std::memory_order_relaxed);
 }
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+static std::atomic<unsigned long long> g_syncs{0};
+cudaError_t counted_sync(cudaStream_t st) {
+  g_syncs.fetch_add(1, std::memory_order_relaxed);
+  return cudaStreamSynchronize(st);
+}
+unsigned long long sync_count() { return g_syncs.load(std::memory_order_relaxed); }
 }  // namespace lvb
 
 struct lv_engine {
@@ -276,6 +282,12 @@ struct lv_engine {
   std::vector<lv_level_info> levels;
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // A single graph's contraction leaves its entry count, error flag and
+  // time to be read at the next synchronisation (the next level's class
+  // counts), so a level boundary costs no extra host round trip.
+  bool agg_pending = false;
+  cudaEvent_t agg_ev0 = nullptr, agg_ev1 = nullptr;
+  uint64_t* h_pending = nullptr;  // pinned: the deferred entry count
 
   // kernel timing
   bool profiling = false;
@@ -326,6 +338,8 @@ struct lv_engine {
   // persistent level kernel: barrier / timer state (device) and its pinned
   // host mirror
   LevelLoopState* loop_state = nullptr;
+  PassDesc* desc_host = nullptr;   // pinned staging of the descriptor
+  cudaEvent_t desc_ev = nullptr;   // its last copy
   LevelLoopState* loop_host = nullptr;
   uint8_t tune[8] = {kDefaultVariant[0], kDefaultVariant[1], kDefaultVariant[2],
                      kDefaultVariant[3], kDefaultVariant[4], kDefaultVariant[5],
@@ -612,8 +626,35 @@ lv_status ensure_capacity(lv_engine* E, uint32_t n, uint64_t e, bool need_input)
   return LV_OK;
 }
 
+lv_status check_device_error(lv_engine* E);
+
+// The reads a deferred contraction left (after a synchronisation that
+// covered h_pending and sc_host): the entry count, the contraction's time,
+// the device error flag.
+lv_status finish_pending(lv_engine* E) {
+  if (!E->agg_pending) return LV_OK;
+  E->agg_pending = false;
+  E->e = E->h_pending[0];
+  float ms = 0.0f;
+  if (cudaEventElapsedTime(&ms, E->agg_ev0, E->agg_ev1) == cudaSuccess && !E->levels.empty())
+    E->levels.back().aggregate_ms = ms;
+  cudaGetLastError();
+  return check_device_error(E);
+}
+
+// Completes a deferred contraction's reads now (entry points that look at
+// the level outside the level loop).
+lv_status resolve_pending(lv_engine* E) {
+  if (!E || !E->agg_pending) return LV_OK;
+  CU(cudaMemcpyAsync(E->h_pending, E->cb.counts + 8, sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                     E->st));
+  CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost, E->st));
+  CU(counted_sync(E->st));
+  return finish_pending(E);
+}
+
 // Degree classes, work plan, hub tables for the current level.
-lv_status prepare_level(lv_engine* E) {
+lv_status prepare_level(lv_engine* E, bool sync_scalars = true) {
   const uint32_t n = E->n;
   cudaStream_t st = E->st;
   drop_pass_graph(E);
@@ -621,7 +662,13 @@ lv_status prepare_level(lv_engine* E) {
                          E->scan, st));
   CU(cudaMemcpyAsync(E->h_counts, E->cls_count, kClasses * sizeof(uint32_t),
                      cudaMemcpyDeviceToHost, st));
-  CU(cudaStreamSynchronize(st));
+  if (E->agg_pending) {  // the previous contraction's reads ride on this sync
+    CU(cudaMemcpyAsync(E->h_pending, E->cb.counts + 8, sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                       st));
+    CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost, st));
+  }
+  CU(counted_sync(st));
+  LVTRY(finish_pending(E));
   g_trace.mark("  degree classes", (uint32_t)E->levels.size(), n);
   DispatchPlan& P = E->plan;
   memset(&P, 0, sizeof(P));
@@ -667,7 +714,7 @@ lv_status prepare_level(lv_engine* E) {
     std::vector<uint64_t> deg(hc);
     CU(cudaMemcpyAsync(deg.data(), E->hub_deg, hc * sizeof(uint64_t),
                        cudaMemcpyDeviceToHost, st));
-    CU(cudaStreamSynchronize(st));
+    CU(counted_sync(st));
     for (uint32_t i = 0; i < hc; i++) {
       const uint32_t nch = (uint32_t)((deg[i] + kHubChunk - 1) / kHubChunk);
       for (uint32_t ch = 0; ch < nch; ch++) {
@@ -787,16 +834,19 @@ lv_status prepare_level(lv_engine* E) {
                          cudaMemcpyDeviceToDevice, st));
   }
   g_trace.mark("  hub plan", (uint32_t)E->levels.size(), n);
-  // entries per move class (byte counts of the kernel timings)
-  if (!E->d_class_deg) CU(dalloc(&E->d_class_deg, kClasses));
-  CU(cudaMemsetAsync(E->d_class_deg, 0, kClasses * sizeof(unsigned long long), st));
-  if (n) {
-    (count_launches(1), class_degree_kernel<<<std::min<uint32_t>((n + 255) / 256, 1184), 256, 0, st>>>(
-        E->off(), n, E->d_class_deg));
-    CU(cudaGetLastError());
+  // entries per move class (byte counts of the kernel timings; profiling
+  // only: the copy into the engine's pageable array blocks the host)
+  if (E->profiling) {
+    if (!E->d_class_deg) CU(dalloc(&E->d_class_deg, kClasses));
+    CU(cudaMemsetAsync(E->d_class_deg, 0, kClasses * sizeof(unsigned long long), st));
+    if (n) {
+      (count_launches(1), class_degree_kernel<<<std::min<uint32_t>((n + 255) / 256, 1184), 256, 0, st>>>(
+          E->off(), n, E->d_class_deg));
+      CU(cudaGetLastError());
+    }
+    CU(cudaMemcpyAsync(E->class_deg, E->d_class_deg, kClasses * sizeof(uint64_t),
+                       cudaMemcpyDeviceToHost, st));
   }
-  CU(cudaMemcpyAsync(E->class_deg, E->d_class_deg, kClasses * sizeof(uint64_t),
-                     cudaMemcpyDeviceToHost, st));
   // single graph: the row of every entry, for the pass loop's modularity
   // sweep (kept in the contraction's column scratch until the level ends)
   if (!E->batch) CU(launch_row_ids(E->off(), n, E->e, E->cb.tcol, st));
@@ -809,10 +859,12 @@ lv_status prepare_level(lv_engine* E) {
   t0 = prof_begin(E);
   CU(launch_modularity(L, E->order, P, hc ? E->hub_map : nullptr, E->partials, st));
   prof_end(E, t0, K_MODULARITY, Ed * 12.0 + Vd * 24.0);
-  CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars),
-                     cudaMemcpyDeviceToHost, st));
-  CU(cudaStreamSynchronize(st));
-  prof_collect(E);
+  if (sync_scalars) {  // else the level graph's own synchronisation reads them
+    CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars),
+                       cudaMemcpyDeviceToHost, st));
+    CU(counted_sync(st));
+    prof_collect(E);
+  }
   g_trace.mark("  level init + Q0", (uint32_t)E->levels.size(), n);
   // tables of E->n vertices (blocking host copies above must be done
   // before the vectors go out of scope: synchronised)
@@ -846,7 +898,12 @@ lv_status upload_desc(lv_engine* E, float min_gain) {
   d.max_passes = E->cfg.max_passes;
   for (int b = 0; b < 8; b++) d.tune[b] = E->tune[b];
   d.loop = E->loop_state;
-  CU(cudaMemcpyAsync(E->d_desc, &d, sizeof(d), cudaMemcpyHostToDevice, E->st));
+  // through pinned memory: a copy from pageable memory would wait for the
+  // stream first; the previous copy must have left the buffer
+  CU(cudaEventSynchronize(E->desc_ev));
+  *E->desc_host = d;
+  CU(cudaMemcpyAsync(E->d_desc, E->desc_host, sizeof(d), cudaMemcpyHostToDevice, E->st));
+  CU(cudaEventRecord(E->desc_ev, E->st));
   return LV_OK;
 }
 
@@ -908,9 +965,15 @@ lv_status run_level_graph(lv_engine* E, float min_gain) {
     } guard{g};
     t_capturing = true;
     t_tally = 0;
+    // the loop's handle first: the init kernel sets its first condition
+    cudaGraphConditionalHandle h;
+    CU(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    PassControl ictl{};
+    ictl.use_handle = E->batch ? 0 : 1;
+    ictl.handle = (unsigned long long)h;
     CU(cudaStreamBeginCaptureToGraph(E->st, g, nullptr, nullptr, 0,
                                      cudaStreamCaptureModeThreadLocal));
-    cudaError_t ce = launch_pass_control_init(E->d_desc, E->st);
+    cudaError_t ce = launch_pass_control_init(E->d_desc, &ictl, E->st);
     cudaGraph_t cap = nullptr;
     cudaError_t ce2 = cudaStreamEndCapture(E->st, &cap);
     t_capturing = false;
@@ -919,8 +982,6 @@ lv_status run_level_graph(lv_engine* E, float min_gain) {
     cudaGraphNode_t init_node = nullptr;
     size_t nn = 1;
     CU(cudaGraphGetNodes(g, &init_node, &nn));
-    cudaGraphConditionalHandle h;
-    CU(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
     cudaGraphNodeParams np{};
     np.type = cudaGraphNodeTypeConditional;
     np.conditional.handle = h;
@@ -958,7 +1019,7 @@ lv_status run_level_graph(lv_engine* E, float min_gain) {
   CU(cudaGraphLaunch(exec, E->st));
   CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost,
                      E->st));
-  CU(cudaStreamSynchronize(E->st));
+  CU(counted_sync(E->st));
   g_trace.mark("graph run (all passes)", (uint32_t)E->levels.size(), E->n);
   return LV_OK;
 }
@@ -1081,7 +1142,7 @@ lv_status run_level_loop(lv_engine* E, float min_gain) {
   if (E->profiling)
     CU(cudaMemcpyAsync(E->loop_host, E->loop_state, sizeof(LevelLoopState),
                        cudaMemcpyDeviceToHost, E->st));
-  CU(cudaStreamSynchronize(E->st));
+  CU(counted_sync(E->st));
   if (E->profiling) {  // per-phase device time, as block 0 saw the barriers
     double bytes[K_COUNT];
     pass_group_bytes(E, bytes);
@@ -1099,6 +1160,7 @@ lv_status run_level_loop(lv_engine* E, float min_gain) {
 
 lv_status load_common(lv_engine* E, uint32_t n, uint64_t e) {
   drop_pass_graph(E);
+  E->agg_pending = false;  // a new graph: nothing deferred is still wanted
   E->n0 = n;
   E->n = n;
   E->e = e;
@@ -1161,7 +1223,7 @@ lv_status batch_passes(lv_engine* E, float min_gain) {
     LVTRY(run_level_graph(E, min_gain));
   } else {
     LVTRY(upload_desc(E, min_gain));
-    CU(launch_pass_control_init(E->d_desc, E->st));
+    CU(launch_pass_control_init(E->d_desc, nullptr, E->st));
     PassControl ctl{};
     ctl.enabled = 1;
     ctl.use_handle = 0;
@@ -1169,7 +1231,7 @@ lv_status batch_passes(lv_engine* E, float min_gain) {
       LVTRY(run_pass(E, &ctl));
       CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost,
                          E->st));
-      CU(cudaStreamSynchronize(E->st));
+      CU(counted_sync(E->st));
       if (E->pass_exec) prof_collect_graph(E);
       prof_collect(E);
       if (!E->sc_host->any_active) break;
@@ -1177,7 +1239,7 @@ lv_status batch_passes(lv_engine* E, float min_gain) {
   }
   CU(cudaMemcpyAsync(E->gs_host, E->gs, sizeof(GraphState) * E->n_graphs,
                      cudaMemcpyDeviceToHost, E->st));
-  CU(cudaStreamSynchronize(E->st));
+  CU(counted_sync(E->st));
   if (E->cfg.use_graphs && !E->profiling) {  // replays of the WHILE body
     uint32_t maxp = 0;
     for (uint32_t g = 0; g < E->n_graphs; g++) maxp = std::max(maxp, E->gs_host[g].passes);
@@ -1270,7 +1332,7 @@ lv_status union_level(lv_engine* E, std::vector<UnionGraph>& graphs, float min_g
   std::vector<UnionGraph> kept;
   for (uint32_t g = 0; g < Gl; g++) (drop[g] ? done : kept).push_back(graphs[g]);
   if (!any_continue) {
-    CU(cudaStreamSynchronize(st));
+    CU(counted_sync(st));
     graphs.clear();
     E->n = 0;
     E->e = 0;
@@ -1294,7 +1356,7 @@ lv_status union_level(lv_engine* E, std::vector<UnionGraph>& graphs, float min_g
   CU(launch_gather_u32(E->cb.flag_id, E->gbase, Gn, E->goff_dev, st));
   std::vector<uint32_t> ng(Gn + 1);
   CU(cudaMemcpyAsync(ng.data(), E->goff_dev, Gn * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-  CU(cudaStreamSynchronize(st));
+  CU(counted_sync(st));
   ng[Gn] = E->n;
   for (uint32_t g = 0, i = 0; g < Gl; g++) {
     if (drop[g]) continue;
@@ -1594,7 +1656,7 @@ lv_status lane_step(lv_server* S, ServeLane* L) {
     r->levels = u.levels;
     r->n_comm = u.nv;
   }
-  CU(cudaStreamSynchronize(E->st));
+  CU(counted_sync(E->st));
   const double now = ms_since(S->t0);
   {
     std::lock_guard<std::mutex> lock(S->mu);
@@ -1744,7 +1806,12 @@ lv_status lv_engine_create(const lv_config* cfg, lv_engine** out) {
       (ce = cudaMallocHost(&E->sc_host, sizeof(LevelScalars))) != cudaSuccess ||
       (ce = cudaMallocHost(&E->h_counts, 32 * sizeof(uint32_t))) != cudaSuccess ||
       (ce = cudaEventCreate(&E->ev0)) != cudaSuccess ||
-      (ce = cudaEventCreate(&E->ev1)) != cudaSuccess) {
+      (ce = cudaEventCreate(&E->ev1)) != cudaSuccess ||
+      (ce = cudaEventCreate(&E->agg_ev0)) != cudaSuccess ||
+      (ce = cudaEventCreateWithFlags(&E->desc_ev, cudaEventDisableTiming)) != cudaSuccess ||
+      (ce = cudaMallocHost(&E->desc_host, sizeof(PassDesc))) != cudaSuccess ||
+      (ce = cudaEventCreate(&E->agg_ev1)) != cudaSuccess ||
+      (ce = cudaMallocHost(&E->h_pending, 2 * sizeof(uint64_t))) != cudaSuccess) {
     lv_engine_destroy(E);
     return cuda_fail(ce, "engine set-up");
   }
@@ -1757,7 +1824,7 @@ void lv_engine_destroy(lv_engine* E) {
   if (!E) return;
   AllocScope alloc_scope(E);
   cudaSetDevice(E->device);
-  if (E->st) cudaStreamSynchronize(E->st);
+  if (E->st) counted_sync(E->st);
   drop_pass_graph(E);
   drop_level_exec(E);
   free_state(E);
@@ -1778,12 +1845,17 @@ void lv_engine_destroy(lv_engine* E) {
   if (E->sc) cudaFree(E->sc);
   if (E->d_desc) cudaFree(E->d_desc);
   if (E->loop_state) cudaFree(E->loop_state);
+  if (E->agg_ev0) cudaEventDestroy(E->agg_ev0);
+  if (E->desc_ev) cudaEventDestroy(E->desc_ev);
+  if (E->desc_host) cudaFreeHost(E->desc_host);
+  if (E->agg_ev1) cudaEventDestroy(E->agg_ev1);
+  if (E->h_pending) cudaFreeHost(E->h_pending);
   if (E->loop_host) cudaFreeHost(E->loop_host);
   if (E->sc_host) cudaFreeHost(E->sc_host);
   if (E->h_counts) cudaFreeHost(E->h_counts);
   if (E->ev0) cudaEventDestroy(E->ev0);
   if (E->ev1) cudaEventDestroy(E->ev1);
-  if (E->st) cudaStreamSynchronize(E->st);  // the frees above are stream-ordered
+  if (E->st) counted_sync(E->st);  // the frees above are stream-ordered
   if (E->pool) cudaMemPoolDestroy(E->pool);
   if (E->own_stream && E->st) cudaStreamDestroy(E->st);
   delete E;
@@ -1905,15 +1977,19 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
   cudaSetDevice(E->device);
   CU(cudaEventRecord(E->ev0, E->st));
   g_trace.reset();
-  if (!E->level_ready) LVTRY(prepare_level(E));
+  // the level graph reads the level's m and initial Q on the device and the
+  // host after the whole level: no synchronisation between set-up and loop
+  const bool graph_path = E->cfg.use_graphs && !E->profiling && !use_level_kernel(E);
+  if (!E->level_ready) LVTRY(prepare_level(E, !graph_path));
   g_trace.mark("prepare", (uint32_t)E->levels.size(), E->n);
   cudaEvent_t ev_prep = take_event(E);
   CU(cudaEventRecord(ev_prep, E->st));
   lv_level_info info{};
   info.n_vertices = E->n;
   info.n_entries = E->e;
+  if (graph_path) LVTRY(run_level_graph(E, min_gain));  // reads sc_host
   const double m64 = E->sc_host->m64;
-  double act = E->sc_host->q, old = act;
+  double act = graph_path ? E->sc_host->q_start : E->sc_host->q, old = act;
   info.q_start = act;
   int ret = 1;
   uint32_t passes = 0;
@@ -1929,8 +2005,7 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
     ret = E->sc_host->first_fail ? 0 : 1;
     act = E->sc_host->q;
     old = E->sc_host->q_before;
-  } else if (E->cfg.use_graphs && !E->profiling) {
-    LVTRY(run_level_graph(E, min_gain));
+  } else if (graph_path) {
     LVTRY(check_device_error(E));
     passes = E->sc_host->passes;
     ret = E->sc_host->first_fail ? 0 : 1;
@@ -1944,7 +2019,7 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
       LVTRY(run_pass(E));
       CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars),
                          cudaMemcpyDeviceToHost, E->st));
-      CU(cudaStreamSynchronize(E->st));
+      CU(counted_sync(E->st));
       if (E->pass_exec) prof_collect_graph(E);
       prof_collect(E);
       LVTRY(check_device_error(E));
@@ -2007,7 +2082,10 @@ lv_status lv_phase_aggregate(lv_engine* E) {
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   if (!E->loaded || !E->level_ready) return fail(LV_ERR_STATE, "no move phase to aggregate");
   cudaSetDevice(E->device);
-  CU(cudaEventRecord(E->ev0, E->st));
+  // a single graph outside profiling defers the reads that follow the
+  // contraction to the next level's first synchronisation
+  const bool defer = !E->batch && !E->profiling && !E->cfg.contract_sort;
+  CU(cudaEventRecord(defer ? E->agg_ev0 : E->ev0, E->st));
   const int next = (E->cur == 0) ? 1 : 0;
   ContractResult r{};
   cudaEvent_t t0 = prof_begin(E);
@@ -2018,7 +2096,7 @@ lv_status lv_phase_aggregate(lv_engine* E) {
                            E->c_col[next], E->c_w[next], &r, E->st));
   } else {
     CU(contract_level(E->view(), E->e, E->cb, E->scan, E->c_off[next], E->c_col[next],
-                      E->c_w[next], &r, E->st, grow_tables, E));
+                      E->c_w[next], &r, E->st, grow_tables, E, defer));
   }
   g_trace.mark("contract", (uint32_t)E->levels.size(), E->n);
   // B_agg = E*12 + V*(off + comm + new id + member) + E'*8 + (V'+1)*off
@@ -2029,10 +2107,19 @@ lv_status lv_phase_aggregate(lv_engine* E) {
   // aggregation.cu:380-385) in one gather: cnew[v] = new_id[comm[v]]
   CU(launch_compose(E->assignment, E->n0, E->cb.cnew, E->st));
   E->accepted = false;
+  if (defer) {
+    CU(cudaEventRecord(E->agg_ev1, E->st));
+    drop_pass_graph(E);
+    E->cur = next;
+    E->n = r.new_n;
+    E->agg_pending = true;  // E->e, the error flag and the time come at the next sync
+    E->level_ready = false;
+    return LV_OK;
+  }
   CU(cudaEventRecord(E->ev1, E->st));
   CU(cudaEventSynchronize(E->ev1));
   CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost, E->st));
-  CU(cudaStreamSynchronize(E->st));
+  CU(counted_sync(E->st));
   LVTRY(check_device_error(E));
   prof_collect(E);
   float ms = 0.0f;
@@ -2078,6 +2165,14 @@ static lv_status run_loaded(lv_engine* E, float min_gain, lv_result* res) {
     if (E->cfg.max_levels && E->levels.size() >= E->cfg.max_levels) {
       E->finished = true;
       break;
+    }
+  }
+  {
+    const lv_status ps = resolve_pending(E);  // a last contraction's reads
+    if (ps != LV_OK) {
+      cudaEventDestroy(a0);
+      cudaEventDestroy(a1);
+      return ps;
     }
   }
   CU(cudaEventRecord(a1, E->st));
@@ -2137,12 +2232,13 @@ lv_status lv_run_device(lv_engine* E, uint32_t n, uint64_t nnz, const uint64_t* 
       CU(cudaMemcpyAsync(d_assignment, E->assignment, (size_t)n * sizeof(uint32_t),
                          cudaMemcpyDeviceToDevice, E->st));
     }
-    CU(cudaStreamSynchronize(E->st));
+    CU(counted_sync(E->st));
   }
   return LV_OK;
 }
 
 lv_status lv_get_assignment(lv_engine* E, uint32_t* out, size_t n) {
+  if (E) LVTRY(resolve_pending(E));
   AllocScope alloc_scope(E);
   if (!E || (!out && n)) return fail(LV_ERR_ARG, "NULL argument");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
@@ -2155,12 +2251,13 @@ lv_status lv_get_assignment(lv_engine* E, uint32_t* out, size_t n) {
       src = E->cb.members;
     }
     CU(cudaMemcpyAsync(out, src, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, E->st));
-    CU(cudaStreamSynchronize(E->st));
+    CU(counted_sync(E->st));
   }
   return LV_OK;
 }
 
 lv_status lv_get_communities(lv_engine* E, uint32_t* out, size_t cap, uint32_t* n_comm) {
+  if (E) LVTRY(resolve_pending(E));
   AllocScope alloc_scope(E);
   if (!E || !n_comm) return fail(LV_ERR_ARG, "NULL argument");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
@@ -2182,13 +2279,14 @@ lv_status lv_get_communities(lv_engine* E, uint32_t* out, size_t cap, uint32_t* 
   cudaError_t ce = group_by_community(part, n, c, d_out, E->st);
   if (ce == cudaSuccess)
     ce = cudaMemcpyAsync(out, d_out, need * sizeof(uint32_t), cudaMemcpyDeviceToHost, E->st);
-  if (ce == cudaSuccess) ce = cudaStreamSynchronize(E->st);
+  if (ce == cudaSuccess) ce = counted_sync(E->st);
   dfree(d_out);
   CU(ce);
   return LV_OK;
 }
 
 lv_status lv_get_levels(lv_engine* E, lv_level_info* out, uint32_t cap, uint32_t* count) {
+  if (E) LVTRY(resolve_pending(E));
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   const uint32_t nl = (uint32_t)E->levels.size();
   if (count) *count = nl;
@@ -2198,6 +2296,7 @@ lv_status lv_get_levels(lv_engine* E, lv_level_info* out, uint32_t cap, uint32_t
 }
 
 lv_status lv_get_level_size(lv_engine* E, uint32_t* n, uint64_t* e) {
+  if (E) LVTRY(resolve_pending(E));
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   if (n) *n = E->n;
   if (e) *e = E->e;
@@ -2206,6 +2305,7 @@ lv_status lv_get_level_size(lv_engine* E, uint32_t* n, uint64_t* e) {
 
 lv_status lv_get_level_state(lv_engine* E, uint32_t* comm, uint32_t* comm_size,
                              float* weighted_degree) {
+  if (E) LVTRY(resolve_pending(E));
   AllocScope alloc_scope(E);
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
@@ -2219,12 +2319,13 @@ lv_status lv_get_level_state(lv_engine* E, uint32_t* comm, uint32_t* comm_size,
     if (weighted_degree)
       CU(cudaMemcpyAsync(weighted_degree, E->k, n * 4, cudaMemcpyDeviceToHost, E->st));
   }
-  CU(cudaStreamSynchronize(E->st));
+  CU(counted_sync(E->st));
   return LV_OK;
 }
 
 lv_status lv_get_level_csr(lv_engine* E, uint64_t* offsets, uint32_t* cols,
                            float* weights) {
+  if (E) LVTRY(resolve_pending(E));
   AllocScope alloc_scope(E);
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
@@ -2237,11 +2338,12 @@ lv_status lv_get_level_csr(lv_engine* E, uint64_t* offsets, uint32_t* cols,
     if (weights)
       CU(cudaMemcpyAsync(weights, E->wts(), E->e * 4, cudaMemcpyDeviceToHost, E->st));
   }
-  CU(cudaStreamSynchronize(E->st));
+  CU(counted_sync(E->st));
   return LV_OK;
 }
 
 lv_status lv_set_level_comm(lv_engine* E, const uint32_t* comm) {
+  if (E) LVTRY(resolve_pending(E));
   AllocScope alloc_scope(E);
   if (!E || !comm) return fail(LV_ERR_ARG, "NULL argument");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
@@ -2255,12 +2357,13 @@ lv_status lv_set_level_comm(lv_engine* E, const uint32_t* comm) {
                        E->plan.hub_count ? E->hub_map : nullptr, E->partials, E->st));
   CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost,
                      E->st));
-  CU(cudaStreamSynchronize(E->st));
+  CU(counted_sync(E->st));
   E->accepted = true;
   return LV_OK;
 }
 
 lv_status lv_modularity_fp64(lv_engine* E, const uint32_t* partition, double* q) {
+  if (E) LVTRY(resolve_pending(E));
   AllocScope alloc_scope(E);
   if (!E || !partition || !q) return fail(LV_ERR_ARG, "NULL argument");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
@@ -2274,13 +2377,14 @@ lv_status lv_modularity_fp64(lv_engine* E, const uint32_t* partition, double* q)
   CU(launch_modularity_of(E->view(), d_part, d_tot, d_out, E->st));
   double h[3] = {0, 0, 0};
   CU(cudaMemcpyAsync(h, d_out, sizeof(h), cudaMemcpyDeviceToHost, E->st));
-  CU(cudaStreamSynchronize(E->st));
+  CU(counted_sync(E->st));
   const double m = h[2] / 2.0;
   *q = (m > 0.0) ? h[0] / (2.0 * m) - h[1] / (4.0 * m * m) : 0.0;
   return LV_OK;
 }
 
 lv_status lv_set_profiling(lv_engine* E, int on) {
+  if (E) LVTRY(resolve_pending(E));
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   E->profiling = on != 0;
   return LV_OK;
@@ -2371,7 +2475,7 @@ lv_status lv_batch_run(lv_engine* E, uint32_t n_graphs, const lv_graph* const* g
   LVTRY(batch_run(E, n_graphs, goff.data(), min_gain, d_out, modularity, levels, res));
   CU(cudaMemcpyAsync(assignment, d_out, (size_t)N * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                      E->st));
-  CU(cudaStreamSynchronize(E->st));
+  CU(counted_sync(E->st));
   return LV_OK;
 }
 
@@ -2474,7 +2578,7 @@ lv_status lv_serve_create(const lv_config* cfg, const lv_serve_config* scfg, lv_
       // (cnew[assignment]) runs over the whole arena, holes included
       CU(cudaMemsetAsync(E->cb.cnew, 0, (size_t)L->cap_n * sizeof(uint32_t), E->st));
       CU(cudaMemsetAsync(E->sc, 0, sizeof(LevelScalars), E->st));
-      CU(cudaStreamSynchronize(E->st));
+      CU(counted_sync(E->st));
       return LV_OK;
     };
     st = setup();
@@ -2678,6 +2782,7 @@ void lv_serve_destroy(lv_server* S) {
 
 // ---- autotuning ------------------------------------------------------------
 lv_status lv_autotune(lv_engine* E, uint32_t reps, lv_tuning* out) {
+  if (E) LVTRY(resolve_pending(E));
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   if (E->batch) return fail(LV_ERR_STATE, "a batched run is in progress");
@@ -2746,6 +2851,12 @@ lv_status lv_debug_fail_device_alloc(uint64_t n) {
   return LV_OK;
 }
 
+lv_status lv_get_sync_count(uint64_t* count) {
+  if (!count) return fail(LV_ERR_ARG, "NULL argument");
+  *count = sync_count();
+  return LV_OK;
+}
+
 lv_status lv_get_launch_count(uint64_t* count) {
   if (!count) return fail(LV_ERR_ARG, "NULL argument");
   *count = launch_count();
@@ -2759,6 +2870,7 @@ lv_status lv_reset_kernel_stats(lv_engine* E) {
 }
 
 lv_status lv_get_buckets(lv_engine* E, uint8_t* bucket_of, size_t n) {
+  if (E) LVTRY(resolve_pending(E));
   AllocScope alloc_scope(E);
   if (!E || (!bucket_of && n)) return fail(LV_ERR_ARG, "NULL argument");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
@@ -2767,7 +2879,7 @@ lv_status lv_get_buckets(lv_engine* E, uint8_t* bucket_of, size_t n) {
   uint8_t* d = reinterpret_cast<uint8_t*>(E->cb.cursor);
   CU(launch_bucket_ids(E->off(), E->n, d, E->st));
   if (n) CU(cudaMemcpyAsync(bucket_of, d, n, cudaMemcpyDeviceToHost, E->st));
-  CU(cudaStreamSynchronize(E->st));
+  CU(counted_sync(E->st));
   return LV_OK;
 }
 

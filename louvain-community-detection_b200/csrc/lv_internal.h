@@ -11,6 +11,10 @@ namespace lvb {
 // Process-wide count of kernels this library has launched.
 void count_launches(unsigned k);
 unsigned long long launch_count();
+// cudaStreamSynchronize, counted: the host waits for the device this many
+// times (process-wide).
+cudaError_t counted_sync(cudaStream_t st);
+unsigned long long sync_count();
 
 // Move-phase degree buckets (modularity.cu:439): bucket b in 1..7 holds the
 // vertices with hi[b-1] < deg <= hi[b]; degree 0 is in no bucket and never
@@ -69,6 +73,7 @@ struct LevelScalars {
   uint32_t any_active;   // some graph's pass loop goes on
   uint32_t act_changed;  // batched form: a graph stopped moving in the last
                          // pass, so the active lists must be compacted again
+  double q_start;        // Q when the level's pass loop began
 };
 
 // Stop rule evaluated by the modularity sweep's last block when the pass
@@ -314,7 +319,9 @@ cudaError_t launch_row_ids(const uint64_t* off, uint32_t n, uint64_t nnz, uint32
 // uses a fixed grid, so a pass captured once replays on every level.
 // passes = 0, first_fail = 0, q_prev = q (start of a level's pass loop),
 // for the single graph and for every graph of a batch.
-cudaError_t launch_pass_control_init(const PassDesc* D, cudaStream_t st);
+// With ctl->use_handle (single graph) the kernel also sets the WHILE
+// node's condition: no pass runs on a level without edge weight.
+cudaError_t launch_pass_control_init(const PassDesc* D, const PassControl* ctl, cudaStream_t st);
 // Proposals of bucket 1..7 (variant[b]: the kernel, null = defaults), or of
 // the hubs (bucket 8); mode = move_mode(rule, fp64 gains).
 cudaError_t launch_move_bucket(const PassDesc* D, int bucket, int mode, const uint8_t* variant,
@@ -491,7 +498,10 @@ cudaError_t contract_level_sort(const LevelView& L, uint64_t nnz, ContractBuffer
                                 cudaStream_t st);
 // Contracts level (L, comm) into (out_off, out_col, out_w); writes cnew
 // (vertex -> new id) for composing the assignment.  Synchronises the
-// stream internally (sizes are needed on the host).
+// stream once for the class sizes (the new vertex count comes with them);
+// with defer_total the new entry count is left at B.counts + 8 (u64) for
+// the caller's next synchronisation (res->new_nnz = ~0), else it is read
+// with a second one.
 cudaError_t contract_level(const LevelView& L, uint64_t nnz,
                            ContractBuffers& B, ScanScratch& S,
                            uint64_t* out_off, uint32_t* out_col, float* out_w,
@@ -499,6 +509,6 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
                            // host-side growable arena callback
                            cudaError_t (*grow)(void* ctx, size_t slots,
                                                size_t entries),
-                           void* grow_ctx);
+                           void* grow_ctx, bool defer_total);
 
 }  // namespace lvb

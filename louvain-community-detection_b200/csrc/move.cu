@@ -1413,7 +1413,7 @@ __global__ void __launch_bounds__(kThreads, kModPerSM)
   modularity_body(L, D->A, ctl, D->rowid, D->nnz);
 }
 
-__global__ void pass_control_init_kernel(const PassDesc* __restrict__ D) {
+__global__ void pass_control_init_kernel(const PassDesc* __restrict__ D, PassControl ctl) {
   LevelScalars* sc = D->L.sc;
   GraphState* gs = D->L.gid ? D->L.gs : nullptr;
   const uint32_t n_graphs = D->L.gid ? D->n_graphs : 0u;
@@ -1423,8 +1423,13 @@ __global__ void pass_control_init_kernel(const PassDesc* __restrict__ D) {
     sc->first_fail = 0u;
     sc->q_prev = sc->q;
     sc->q_before = sc->q;
+    sc->q_start = sc->q;
     sc->any_active = 1u;
     sc->act_changed = 1u;  // the first pass builds the active lists
+    // single graph: a level without edge weight runs no pass (its gains
+    // would divide by m = 0); the host reads m after the level
+    if (ctl.use_handle && !D->L.gid)
+      cudaGraphSetConditional((cudaGraphConditionalHandle)ctl.handle, sc->m64 > 0.0 ? 1u : 0u);
   }
   for (uint32_t g = t; g < n_graphs; g += gridDim.x * blockDim.x) {
     GraphState& s = gs[g];
@@ -1933,8 +1938,10 @@ cudaError_t launch_row_ids(const uint64_t* off, uint32_t n, uint64_t nnz, uint32
   return cudaGetLastError();
 }
 
-cudaError_t launch_pass_control_init(const PassDesc* D, cudaStream_t st) {
-  (count_launches(1), pass_control_init_kernel<<<sm_count(), 256, 0, st>>>(D));
+cudaError_t launch_pass_control_init(const PassDesc* D, const PassControl* ctl, cudaStream_t st) {
+  PassControl c{};
+  if (ctl) c = *ctl;
+  (count_launches(1), pass_control_init_kernel<<<sm_count(), 256, 0, st>>>(D, c));
   return cudaGetLastError();
 }
 

@@ -284,7 +284,7 @@ cudaError_t csr_from_edges_device(uint32_t n, uint64_t m, const uint32_t* src,
     if ((e = cudaMemcpyAsync(bad_host, bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, st)) !=
         cudaSuccess)
       goto done;
-    e = cudaStreamSynchronize(st);
+    e = counted_sync(st);
   }
 done:
   if (keys) cudaFreeAsync(keys, st);

@@ -160,6 +160,7 @@ _SIGS = {
     "lv_reset_kernel_stats": (ctypes.c_int, [_VP]),
     "lv_get_launch_count": (ctypes.c_int, [ctypes.POINTER(_U64)]),
     "lv_debug_fail_device_alloc": (ctypes.c_int, [_U64]),
+    "lv_get_sync_count": (ctypes.c_int, [ctypes.POINTER(_U64)]),
     "lv_engine_load_edges": (ctypes.c_int, [_VP, _U32, _U64, _VP, _VP, _VP]),
     "lv_engine_load_mtx": (ctypes.c_int, [_VP, ctypes.c_char_p]),
     "lv_csr_from_edges_device": (ctypes.c_int, [_U32, _U64, _VP, _VP, _VP, _VP, _VP, _VP,
@@ -252,6 +253,13 @@ def lib() -> ctypes.CDLL:
             f.argtypes = args
         _lib = L
     return _lib
+
+
+def sync_count() -> int:
+    """Host waits on a stream the library has made so far (process-wide)."""
+    c = _U64()
+    _check(lib().lv_get_sync_count(ctypes.byref(c)))
+    return int(c.value)
 
 
 def fail_device_alloc(n: int):

@@ -337,3 +337,35 @@ def test_cli_cache_gives_the_same_output(tmp_path):
         outs.append([lines[0]] + lines[2:])  # line 2 holds times
         assert os.path.exists(mtx + ".lvbcsr")
     assert outs[0] == outs[1]
+
+
+@pytest.mark.parametrize("name", ["planted_small", "ring_of_cliques", "hub3000"])
+def test_host_waits_per_level(name):
+    """A single graph on device inputs makes the host wait about three
+    times a level: the level's class counts (with the previous
+    contraction's entry count and error flag riding along), the level
+    graph's result, and the contraction's class sizes -- plus one for a
+    level with hubs and one for the contraction's largest communities.
+    The results stay those of the oracle."""
+    import torch
+
+    g = lvb200.Graph.load_mtx(golden_mtx(name))
+    n, off, col, w, _ = g.csr()
+    d_off = torch.from_numpy(off.view(np.int64)).cuda()
+    d_col = torch.from_numpy(col.view(np.int32)).cuda()
+    d_w = torch.from_numpy(w).cuda()
+    d_asg = torch.empty(n, dtype=torch.int32, device="cuda")
+    with lvb200.Engine(rule="py") as e:
+        e.run_device(n, len(col), d_off.data_ptr(), d_col.data_ptr(), d_w.data_ptr(), 1e-6,
+                     d_asg.data_ptr())  # warm-up: buffers, level graphs
+        s0 = lvb200.sync_count()
+        r = e.run_device(n, len(col), d_off.data_ptr(), d_col.data_ptr(), d_w.data_ptr(), 1e-6,
+                         d_asg.data_ptr())
+        syncs = lvb200.sync_count() - s0
+    levels = len(r.levels)
+    extra = 2 * levels if name == "hub3000" else 0
+    assert syncs <= 3 * levels + 2 + extra, (syncs, levels)
+    orc = pyoracle.louvain(_oracle_graph(golden_mtx(name)), 1e-6, rule="py", prec="fp32",
+                           rows="sorted")
+    assert np.array_equal(d_asg.cpu().numpy().view(np.uint32), orc.assignment)
+    assert abs(r.modularity - orc.q) < 1e-9
