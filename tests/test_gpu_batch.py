@@ -147,7 +147,8 @@ def test_batch_device_equals_host():
     out = d_out.cpu().numpy().view(np.uint32)
     for g in range(len(edge_lists)):
         assert np.array_equal(out[goff[g]:goff[g + 1]], parts[g])
-        assert q[g] == qh[g] and lv[g] == lh[g]
+        # per-graph Q of a union is summed with FP64 atomics: last bits only
+        assert abs(q[g] - qh[g]) <= 1e-12 * max(1.0, abs(qh[g])) and lv[g] == lh[g]
 
 
 def test_batch_bad_offsets():
