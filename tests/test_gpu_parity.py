@@ -362,7 +362,7 @@ def test_host_waits_per_level(name):
         r = e.run_device(n, len(col), d_off.data_ptr(), d_col.data_ptr(), d_w.data_ptr(), 1e-6,
                          d_asg.data_ptr())
         syncs = lvb200.sync_count() - s0
-    levels = len(r.levels)
+    levels = r.n_levels
     extra = 2 * levels if name == "hub3000" else 0
     assert syncs <= 3 * levels + 2 + extra, (syncs, levels)
     orc = pyoracle.louvain(_oracle_graph(golden_mtx(name)), 1e-6, rule="py", prec="fp32",
