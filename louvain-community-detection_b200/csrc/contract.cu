@@ -86,19 +86,6 @@ __device__ __forceinline__ double warp_sum(double x) {
   return x;
 }
 
-// Sum over the block, returned to every thread (red: kWarps doubles).
-__device__ __forceinline__ double block_sum_d(double x, double* red) {
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  x = warp_sum(x);
-  __syncthreads();
-  if (lane == 0) red[wib] = x;
-  __syncthreads();
-  double t = 0.0;
-#pragma unroll
-  for (int i = 0; i < kWarps; i++) t += red[i];
-  return t;
-}
-
 struct Ctx {
   const uint64_t* off;
   const uint32_t* col;
@@ -391,7 +378,6 @@ __global__ void __launch_bounds__(kThreads)
   uint64_t* s_off = s_start + kThreads;
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + SLOTS * 8 + kThreads * 16);
   __shared__ uint32_t scan_sm[kWarps + 1];
-  __shared__ double red[kWarps];
   for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
     const uint32_t cn = list[idx];
     const uint32_t c = C.comm_list[cn];
@@ -409,11 +395,11 @@ __global__ void __launch_bounds__(kThreads)
     bool hot_seen = false;
     insert_range(C, m0, msz, seg, total, 0, total, keys, vals, tv - 1, s_start, s_off, cn,
                  hot_acc, hot_seen);
-    const double hs = block_sum_d(hot_acc, red);
-    if (__syncthreads_or(hot_seen) && threadIdx.x == 0) {
-      const uint32_t slot = table_insert(keys, tv - 1, cn, C.err);
-      vals[slot] += hs;
-    }
+    // every warp adds its share of the new self-loop (FP64 sums of FP32
+    // weights are exact in any order): no block-wide sum first
+    hot_acc = warp_sum(hot_acc);
+    if (__any_sync(kFull, hot_seen) && (threadIdx.x & 31) == 0)
+      atomicAdd(&vals[table_insert(keys, tv - 1, cn, C.err)], hot_acc);
     __syncthreads();
     // emit: thread t owns slots [t*per, t*per + per)
     const uint32_t per = tv / kThreads;
@@ -453,7 +439,6 @@ __global__ void __launch_bounds__(kThreads)
     merge_global_insert_kernel(Ctx C, GArgs G) {
   __shared__ uint64_t s_start[kThreads];
   __shared__ uint64_t s_off[kThreads];
-  __shared__ double red[kWarps];
   for (uint32_t b = blockIdx.x; b < G.nblocks; b += gridDim.x) {
     const uint32_t gi = G.blk_comm[b], ch = G.blk_chunk[b];
     const uint32_t cn = G.list[gi];
@@ -470,11 +455,9 @@ __global__ void __launch_bounds__(kThreads)
     bool hot_seen = false;
     insert_range(C, m0, msz, seg, total, lo, hi, keys, vals, mask, s_start, s_off, cn,
                  hot_acc, hot_seen);
-    const double hs = block_sum_d(hot_acc, red);
-    if (__syncthreads_or(hot_seen) && threadIdx.x == 0) {
-      const uint32_t slot = table_insert(keys, mask, cn, C.err);
-      atomicAdd(&vals[slot], hs);
-    }
+    hot_acc = warp_sum(hot_acc);  // per warp, as in merge_block_kernel
+    if (__any_sync(kFull, hot_seen) && (threadIdx.x & 31) == 0)
+      atomicAdd(&vals[table_insert(keys, mask, cn, C.err)], hot_acc);
     __syncthreads();
   }
 }
@@ -513,20 +496,32 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// Final CSR: row cn copied from its staging range to new offsets.
+// Final CSR: row cn copied from its staging range to new offsets.  A warp
+// takes 32 consecutive rows: every lane loads one row's bounds (one load
+// round for all 32), then the warp copies the rows one after another, 32
+// entries per store -- rows are short at most levels, so a row per warp
+// would leave most lanes idle and chain three loads per row.
 __global__ void __launch_bounds__(kThreads)
     compress_kernel(const uint64_t* seg, const uint64_t* new_off, uint32_t new_n,
                     const uint32_t* tcol, const float* tw, uint32_t* out_col,
                     float* out_w) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  for (uint32_t cn = blockIdx.x * kWarps + wib; cn < new_n;
-       cn += gridDim.x * kWarps) {
-    const uint64_t dst = new_off[cn];
-    const uint64_t cnt = new_off[cn + 1] - dst;
-    const uint64_t src = seg[cn];
-    for (uint64_t j = lane; j < cnt; j += 32) {
-      out_col[dst + j] = tcol[src + j];
-      out_w[dst + j] = tw[src + j];
+  const uint64_t step = (uint64_t)gridDim.x * kWarps * 32;
+  for (uint64_t c0 = ((uint64_t)blockIdx.x * kWarps + wib) * 32; c0 < new_n; c0 += step) {
+    const uint64_t cn = c0 + lane;
+    uint64_t dst = 0, cnt = 0, src = 0;
+    if (cn < new_n) {
+      dst = new_off[cn];
+      cnt = new_off[cn + 1] - dst;
+      src = seg[cn];
+    }
+    for (int i = 0; i < 32; i++) {
+      const uint64_t di = __shfl_sync(kFull, dst, i), ci = __shfl_sync(kFull, cnt, i);
+      const uint64_t si = __shfl_sync(kFull, src, i);
+      for (uint64_t j = lane; j < ci; j += 32) {
+        out_col[di + j] = tcol[si + j];
+        out_w[di + j] = tw[si + j];
+      }
     }
   }
 }
@@ -798,7 +793,7 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
   // new offsets: exclusive scan of the n'+1 counts (last one is 0)
   uint64_t* d_total = reinterpret_cast<uint64_t*>(B.counts + 8);
   LV_TRY(exclusive_scan_u64(B.new_deg, out_off, (size_t)new_n + 1, d_total, S, st));
-  (count_launches(1), compress_kernel<<<gridcap((new_n + kWarps - 1) / kWarps, 8), kThreads, 0, st>>>(
+  (count_launches(1), compress_kernel<<<gridcap(((uint64_t)new_n + 32 * kWarps - 1) / (32 * kWarps), 8), kThreads, 0, st>>>(
       B.seg, out_off, new_n, B.tcol, B.tw, out_col, out_w));
   LV_TRY(cudaGetLastError());
   res->new_n = new_n;

@@ -660,18 +660,35 @@ __device__ __forceinline__ void block_body(const PassDesc* __restrict__ D, int c
     bool hot_seen = false;
     insert_block_range<MAXW, RULE>(L, s, 0, d, v, cv, keys, vals, tv - 1, own, hot,
                                    hot_seen);
-    const int any_hot = __syncthreads_or(hot_seen);
-    hot = block_sum(hot, red_own);  // thread 0
-    if (threadIdx.x == 0 && any_hot) {
-      const uint32_t slot = table_insert(keys, tv - 1, cv, L.sc);
-      vals[slot] += hot;
-    }
-    __syncthreads();
+    // every warp adds its share of the own community's weight to that
+    // community's slot (FP64 sums of FP32 weights are exact in any order),
+    // so no block-wide sum is needed before the table is complete
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    hot = group_sum<32>(hot);
+    if (__any_sync(kFull, hot_seen) && lane == 0)
+      atomicAdd(&vals[table_insert(keys, tv - 1, cv, L.sc)], hot);
+    if (RULE == LV_RULE_CUDA_I) own = group_sum<32>(own);
+    __syncthreads();  // (A) the table is complete
     K best = scan_table_and_clear<PREC>(L, g, keys, vals, tv, threadIdx.x, kThreads);
-    best = block_max(best, red_best);
-    if (RULE == LV_RULE_CUDA_I) own = block_sum(own, red_own);
-    if (threadIdx.x == 0) prop[vidx] = decide<RULE>(best, own, g);
-    __syncthreads();
+    best = group_max<32>(best);
+    if (lane == 0) {  // written after (A): thread 0 read the last ones before it
+      red_best[wib] = best;
+      if (RULE == LV_RULE_CUDA_I) red_own[wib] = own;
+    }
+    __syncthreads();  // (B) the table is empty again, the partials are in
+    if (threadIdx.x == 0) {
+      K b = red_best[0];
+      double o = red_own[0];
+      for (int i = 1; i < kWarps; i++) {
+        b = best_max(b, red_best[i]);
+        if (RULE == LV_RULE_CUDA_I) o += red_own[i];
+      }
+      prop[vidx] = decide<RULE>(b, RULE == LV_RULE_CUDA_I ? o : 0.0, g);
+    }
+    // no barrier here: the next vertex's first shared writes (the table's
+    // inserts) touch no reduction slot, and the reduction slots are
+    // rewritten only after the next (A), which thread 0 reaches after it
+    // has read them
   }
 }
 
