@@ -496,24 +496,29 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// Final CSR: row cn copied from its staging range to new offsets.  A warp
-// takes 32 consecutive rows: every lane loads one row's bounds (one load
-// round for all 32), then the warp copies the rows one after another, 32
-// entries per store -- rows are short at most levels, so a row per warp
-// would leave most lanes idle and chain three loads per row.
+// Final CSR: row cn copied from its staging range to new offsets.  Rows are
+// dealt round robin to the warps (consecutive new ids -- often the large
+// communities formed around hubs -- land on different warps); a warp takes
+// 32 of its rows at a time, every lane loading one row's bounds, then
+// copies them one after another, 32 entries per store.  Rows longer than
+// kLongRow entries (only communities of the largest class have them) are
+// left to compress_long_kernel, where the whole grid copies each.
+constexpr uint64_t kLongRow = kMergeBlockMax;
 __global__ void __launch_bounds__(kThreads)
     compress_kernel(const uint64_t* seg, const uint64_t* new_off, uint32_t new_n,
                     const uint32_t* tcol, const float* tw, uint32_t* out_col,
                     float* out_w) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const uint64_t step = (uint64_t)gridDim.x * kWarps * 32;
-  for (uint64_t c0 = ((uint64_t)blockIdx.x * kWarps + wib) * 32; c0 < new_n; c0 += step) {
-    const uint64_t cn = c0 + lane;
+  const uint64_t nwarps = (uint64_t)gridDim.x * kWarps;
+  const uint64_t w = (uint64_t)blockIdx.x * kWarps + wib;
+  for (uint64_t k0 = 0; w + k0 * nwarps < new_n; k0 += 32) {
+    const uint64_t cn = w + (k0 + lane) * nwarps;
     uint64_t dst = 0, cnt = 0, src = 0;
     if (cn < new_n) {
       dst = new_off[cn];
       cnt = new_off[cn + 1] - dst;
       src = seg[cn];
+      if (cnt > kLongRow) cnt = 0;
     }
     for (int i = 0; i < 32; i++) {
       const uint64_t di = __shfl_sync(kFull, dst, i), ci = __shfl_sync(kFull, cnt, i);
@@ -522,6 +527,27 @@ __global__ void __launch_bounds__(kThreads)
         out_col[di + j] = tcol[si + j];
         out_w[di + j] = tw[si + j];
       }
+    }
+  }
+}
+
+// The long rows: every class-G community's row of more than kLongRow
+// entries, copied by all threads of the grid, one row after another.
+__global__ void __launch_bounds__(kThreads)
+    compress_long_kernel(const uint32_t* glist, uint32_t count, const uint64_t* seg,
+                         const uint64_t* new_off, const uint32_t* tcol, const float* tw,
+                         uint32_t* out_col, float* out_w) {
+  const uint64_t t0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t nt = (uint64_t)gridDim.x * blockDim.x;
+  for (uint32_t i = 0; i < count; i++) {
+    const uint32_t cn = glist[i];
+    const uint64_t dst = new_off[cn];
+    const uint64_t cnt = new_off[cn + 1] - dst;
+    if (cnt <= kLongRow) continue;
+    const uint64_t src = seg[cn];
+    for (uint64_t j = t0; j < cnt; j += nt) {
+      out_col[dst + j] = tcol[src + j];
+      out_w[dst + j] = tw[src + j];
     }
   }
 }
@@ -793,9 +819,14 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
   // new offsets: exclusive scan of the n'+1 counts (last one is 0)
   uint64_t* d_total = reinterpret_cast<uint64_t*>(B.counts + 8);
   LV_TRY(exclusive_scan_u64(B.new_deg, out_off, (size_t)new_n + 1, d_total, S, st));
-  (count_launches(1), compress_kernel<<<gridcap(((uint64_t)new_n + 32 * kWarps - 1) / (32 * kWarps), 8), kThreads, 0, st>>>(
+  (count_launches(1), compress_kernel<<<gridcap(((uint64_t)new_n + kWarps - 1) / kWarps, 8), kThreads, 0, st>>>(
       B.seg, out_off, new_n, B.tcol, B.tw, out_col, out_w));
   LV_TRY(cudaGetLastError());
+  if (cntG) {
+    (count_launches(1), compress_long_kernel<<<gridcap(1u << 20, 8), kThreads, 0, st>>>(
+        B.comm_cls + cntW + cntB, cntG, B.seg, out_off, B.tcol, B.tw, out_col, out_w));
+    LV_TRY(cudaGetLastError());
+  }
   res->new_n = new_n;
   if (defer_total) {  // the caller reads B.counts + 8 at its next sync
     res->new_nnz = ~0ull;
