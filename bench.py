@@ -271,7 +271,8 @@ def batched_measure(stream, count: int, steps: int = 2):
     return res
 
 
-def hbm_scale_measure(stream, scale: int, steps: int = 2, oracle_check: bool = True):
+def hbm_scale_measure(stream, scale: int, steps: int = 2, oracle_check: bool = True,
+                      apply_launch: bool = False):
     """The plain engine at HBM scale: R-MAT (a, b, c, d = 0.57, 0.19, 0.19,
     0.05, edge factor 16, duplicates merged, unit weights) generated on the
     device; edges/s per pass over `steps` device-timed runs after one
@@ -289,7 +290,7 @@ def hbm_scale_measure(stream, scale: int, steps: int = 2, oracle_check: bool = T
            "n_entries": nnz, "abcd": [0.57, 0.19, 0.19, 0.05], "weights": "unit FP32",
            "seed": 0}
     with torch.cuda.stream(stream):
-        eng = lvb200.Engine(stream=stream.cuda_stream)
+        eng = lvb200.Engine(stream=stream.cuda_stream, apply_launch=apply_launch)
         eng.load_device(n, nnz, off.data_ptr(), col.data_ptr(), w.data_ptr())
         res["tuning"] = {str(b): k for b, (k, _) in eng.autotune().items()}
 
@@ -599,7 +600,7 @@ def run_engine(args, rank, world):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB
     torch.cuda.synchronize()
     eng = lvb200.Engine(device=dev, rule="py", stream=stream.cuda_stream,
-                        use_graphs=not args.no_graphs)
+                        use_graphs=not args.no_graphs, apply_launch=args.apply_launch)
     tuning = None
     if not args.no_tune:  # kernel variant per bucket, timed on level 0 (untimed)
         with torch.cuda.stream(stream):
@@ -680,7 +681,8 @@ def run_engine(args, rank, world):
                                 int(args.serve_budget_gb * 1e9),
                                 min(args.serve_distinct, args.serve_requests))
     if world == 1 and args.hbm_scale > 0:
-        hbm = hbm_scale_measure(stream, args.hbm_scale, oracle_check=not args.no_oracle_check)
+        hbm = hbm_scale_measure(stream, args.hbm_scale, oracle_check=not args.no_oracle_check,
+                                apply_launch=args.apply_launch)
     if rank != 0:
         return
     # roofline of the dominant kernel group
@@ -699,6 +701,8 @@ def run_engine(args, rank, world):
         "config": dict(desc, parallelism="replicas only" if world > 1 else "single GPU",
                        l2="flushed (256 MB write) between timed steps",
                        pass_loop="host loop" if args.no_graphs else "CUDA graph WHILE node",
+                       apply=("a launch per bucket" if args.apply_launch
+                              else "in the bucket steps (second state copy)"),
                        tuning=tuning or "defaults"),
         "final_q": q,
         "levels": [{"V": l["n_vertices"], "E": l["n_entries"], "passes": l["passes"],
@@ -748,6 +752,9 @@ def main():
                          "graphs with conditional nodes)")
     ap.add_argument("--hbm-scale", type=int, default=24,
                     help="R-MAT scale of the HBM-scale plain-engine measurement (0: skip)")
+    ap.add_argument("--apply-launch", action="store_true",
+                    help="apply each bucket's moves in a launch of its own (lv_config.apply_launch) "
+                         "instead of inside the bucket steps")
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the CPU baseline leg (profiling runs)")
     ap.add_argument("--no-oracle-check", action="store_true",

@@ -83,6 +83,12 @@ typedef struct lv_config {
                                entries by (new row, new column) and summing
                                runs (rows then ordered by column); 0
                                (default): hash merge per community        */
+    int apply_launch;       /* 1: apply each bucket's moves in a launch of
+                               its own after the bucket's proposals; 0
+                               (default): every bucket step applies its own
+                               moves into a second copy of the community
+                               state (same results, one launch less per
+                               bucket)                                      */
 } lv_config;
 
 /* Per-level record (the reference prints none of this; -v here adds it). */

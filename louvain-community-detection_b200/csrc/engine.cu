@@ -242,6 +242,10 @@ struct lv_engine {
   uint32_t* comm = nullptr;
   uint32_t* comm_sz = nullptr;
   double* tot = nullptr;
+  // second copy of the community state (fused bucket steps, StepIO)
+  uint32_t* comm_alt = nullptr;
+  uint32_t* sz_alt = nullptr;
+  double* tot_alt = nullptr;
   uint32_t* order = nullptr;
   uint32_t* prop = nullptr;
   uint32_t* cls_count = nullptr;
@@ -359,6 +363,9 @@ struct lv_engine {
     L.comm = comm;
     L.comm_sz = comm_sz;
     L.tot = tot;
+    L.comm_alt = comm_alt;
+    L.sz_alt = sz_alt;
+    L.tot_alt = tot_alt;
     L.sc = sc;
     L.gid = batch ? gid : nullptr;
     L.gs = batch ? gs : nullptr;
@@ -464,6 +471,9 @@ void free_state(lv_engine* E) {
   dfree(E->comm);
   dfree(E->comm_sz);
   dfree(E->tot);
+  dfree(E->comm_alt);
+  dfree(E->sz_alt);
+  dfree(E->tot_alt);
   dfree(E->order);
   dfree(E->prop);
   dfree(E->cls_count);
@@ -581,6 +591,9 @@ lv_status ensure_capacity(lv_engine* E, uint32_t n, uint64_t e, bool need_input)
   CU(dalloc(&E->comm, N));
   CU(dalloc(&E->comm_sz, N));
   CU(dalloc(&E->tot, N));
+  CU(dalloc(&E->comm_alt, N));
+  CU(dalloc(&E->sz_alt, N));
+  CU(dalloc(&E->tot_alt, N));
   CU(dalloc(&E->order, N));
   CU(dalloc(&E->prop, N));
   CU(dalloc(&E->cls_count, 16));
@@ -924,7 +937,8 @@ bool class_nonempty(const lv_engine* E, int c) {
 // classes are non-empty.
 uint64_t level_key(const lv_engine* E) {
   uint64_t k = (E->batch ? 1u : 0u) | ((uint64_t)(E->cfg.rule == LV_RULE_CUDA) << 1) |
-               ((uint64_t)(E->cfg.gain == LV_GAIN_FP64) << 2);
+               ((uint64_t)(E->cfg.gain == LV_GAIN_FP64) << 2) |
+               ((uint64_t)(E->cfg.apply_launch != 0) << 3);
   for (int b = 1; b <= kBuckets; b++) k |= (uint64_t)E->tune[b] << (4 * b);
   for (int c = 1; c <= 8; c++) k |= (uint64_t)class_nonempty(E, c) << (39 + c);
   return k;
@@ -1067,6 +1081,12 @@ lv_status issue_pass(lv_engine* E, const PassControl* ctl) {
   cudaStream_t st = E->st;
   // batched form: this pass visits only the graphs still moving
   if (E->batch) CU(launch_compact_active(D, st));
+  // fused steps: step s reads copy s % 2 of the community state and leaves
+  // every move up to its own in the other (StepIO); the first kernel of a
+  // step re-applies the previous step's moves there
+  const bool fused = !E->cfg.apply_launch;
+  StepIO io{fused ? 1 : 0, 0, 0, 0};
+  int step = 0;
   // the kernels of classes empty on this level are left out (the level
   // graph is keyed by which classes are non-empty)
   for (int b = 1; b <= kBuckets; b++) {
@@ -1079,23 +1099,32 @@ lv_status issue_pass(lv_engine* E, const PassControl* ctl) {
     const double vb = (double)(e - s);
     const double v7 = (double)(E->plan.cls_start[b + 1] - s);
     cudaEvent_t t0;
+    io.parity = fused ? (step & 1) : 0;
     if (class_nonempty(E, b)) {
       t0 = prof_begin(E);
-      CU(launch_move_bucket(D, b, rule, E->tune, st));
+      CU(launch_move_bucket(D, b, rule, E->tune, st, io));
       prof_end(E, t0, K_MOVE1 + b - 1, (double)E->class_deg[b] * 12.0 + v7 * 32.0);
+      io.prev_lo = io.prev_hi = 0;  // re-applied by this launch
     }
     if (hubs) {
       t0 = prof_begin(E);
-      CU(launch_move_bucket(D, 8, rule, nullptr, st));
+      CU(launch_move_bucket(D, 8, rule, nullptr, st, io));
       prof_end(E, t0, K_HUB,
                (double)E->class_deg[8] * 12.0 + (double)E->plan.hub_count * 32.0);
     }
-    t0 = prof_begin(E);
-    CU(launch_apply_bucket(D, b, E->batch, st));
-    prof_end(E, t0, K_APPLY, vb * 12.0);
+    if (fused) {
+      io.prev_lo = b;
+      io.prev_hi = b == 7 ? 8 : b;
+      step++;
+    } else {
+      t0 = prof_begin(E);
+      CU(launch_apply_bucket(D, b, E->batch, st));
+      prof_end(E, t0, K_APPLY, vb * 12.0);
+    }
   }
+  io.parity = fused ? (step & 1) : 0;
   cudaEvent_t t0 = prof_begin(E);
-  CU(launch_modularity_pass(D, ctl, st));
+  CU(launch_modularity_pass(D, ctl, st, io));
   prof_end(E, t0, K_MODULARITY, (double)E->e * 12.0 + (double)E->n * 24.0);
   return LV_OK;
 }
@@ -1742,6 +1771,7 @@ void lv_config_default(lv_config* cfg) {
   cfg->gain = LV_GAIN_FP32;
   cfg->level_kernel = 0;
   cfg->contract_sort = 0;
+  cfg->apply_launch = 0;
 }
 
 lv_status lv_engine_create(const lv_config* cfg, lv_engine** out) {
@@ -2353,6 +2383,12 @@ lv_status lv_set_level_comm(lv_engine* E, const uint32_t* comm) {
   if (!E->level_ready) LVTRY(prepare_level(E));
   if (E->n) CU(cudaMemcpyAsync(E->comm, comm, (size_t)E->n * 4, cudaMemcpyHostToDevice, E->st));
   CU(launch_recount(E->view(), E->st));
+  if (E->n) {  // the second copy of the state starts equal to the first
+    const size_t n = E->n;
+    CU(cudaMemcpyAsync(E->comm_alt, E->comm, n * 4, cudaMemcpyDeviceToDevice, E->st));
+    CU(cudaMemcpyAsync(E->sz_alt, E->comm_sz, n * 4, cudaMemcpyDeviceToDevice, E->st));
+    CU(cudaMemcpyAsync(E->tot_alt, E->tot, n * 8, cudaMemcpyDeviceToDevice, E->st));
+  }
   CU(launch_modularity(E->view(), E->order, E->plan,
                        E->plan.hub_count ? E->hub_map : nullptr, E->partials, E->st));
   CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost,

@@ -132,6 +132,12 @@ struct LevelView {
   uint32_t* comm;      // community of every vertex
   uint32_t* comm_sz;   // vertices per community
   double* tot;         // community totals a_c (FP64, exact for FP32 inputs)
+  // second copy of (comm, comm_sz, tot) for passes whose bucket steps apply
+  // their own moves (StepIO); equal to the first copy between passes.
+  // nullptr where a kernel never needs it.
+  uint32_t* comm_alt = nullptr;
+  uint32_t* sz_alt = nullptr;
+  double* tot_alt = nullptr;
   LevelScalars* sc;
   // batched form only (nullptr for a single graph): graph of every vertex
   // of the level, and the graphs' state
@@ -311,6 +317,24 @@ struct PassDesc {
   LevelLoopState* loop;
 };
 
+// How one bucket step of a pass treats the community state.  fused = 0:
+// the step only proposes (prop[]), a separate apply launch moves the
+// vertices.  fused = 1: the two copies of the state alternate -- the step
+// reads copy `parity` (every decision of the bucket against the same
+// state: one Jacobi step) and writes its own moves into the other copy,
+// which also still lacks the previous step's moves: the step re-applies
+// those from prop[] (classes prev_lo..prev_hi; prev_lo = 0: none), so the
+// copy it leaves holds every move up to its own.  The pass's modularity
+// sweep re-applies the last step's moves, after which both copies are
+// equal again.  No apply launch and no grid-wide wait between a bucket's
+// decisions and its moves.
+struct StepIO {
+  int fused;
+  int parity;
+  int prev_lo;
+  int prev_hi;
+};
+
 // rowid[j] = the row holding entry j of a CSR of n rows and nnz entries.
 cudaError_t launch_row_ids(const uint64_t* off, uint32_t n, uint64_t nnz, uint32_t* rowid,
                            cudaStream_t st);
@@ -325,13 +349,14 @@ cudaError_t launch_pass_control_init(const PassDesc* D, const PassControl* ctl, 
 // Proposals of bucket 1..7 (variant[b]: the kernel, null = defaults), or of
 // the hubs (bucket 8); mode = move_mode(rule, fp64 gains).
 cudaError_t launch_move_bucket(const PassDesc* D, int bucket, int mode, const uint8_t* variant,
-                               cudaStream_t st);
+                               cudaStream_t st, StepIO io = StepIO{});
 // Applies bucket b's proposals (bucket 7: classes 7 and 8; `compacted`:
 // the batched form's active lists, where they are not adjacent).
 cudaError_t launch_apply_bucket(const PassDesc* D, int bucket, bool compacted, cudaStream_t st);
 // Modularity sweep of the pass; with ctl->enabled also the stop rule
 // (limits from D), with ctl->use_handle the WHILE node's condition.
-cudaError_t launch_modularity_pass(const PassDesc* D, const PassControl* ctl, cudaStream_t st);
+cudaError_t launch_modularity_pass(const PassDesc* D, const PassControl* ctl, cudaStream_t st,
+                                   StepIO io = StepIO{});
 // The whole pass loop of a single graph's level (modularity.cu:466-508) in
 // one cooperative launch of a persistent kernel: every bucket step, apply
 // and modularity sweep separated by grid-wide barriers (waits bounded in

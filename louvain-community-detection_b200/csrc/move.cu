@@ -321,6 +321,79 @@ __device__ __forceinline__ uint32_t table_insert(uint32_t* keys, uint32_t mask,
 }
 
 // ---------------------------------------------------------------------------
+// Community state of a bucket step (StepIO).  step_view's comm / comm_sz /
+// tot are the copy the step reads; a fused step writes its moves into the
+// other copy (write_copy), fetched from the descriptor where a move is
+// recorded rather than kept in registers through the step.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ LevelView step_view(const PassDesc* __restrict__ D, const StepIO& io) {
+  LevelView L = D->L;
+  if (io.parity) {
+    L.comm = D->L.comm_alt;
+    L.comm_sz = D->L.sz_alt;
+    L.tot = D->L.tot_alt;
+  }
+  return L;
+}
+
+struct StateCopy {
+  uint32_t* comm;
+  uint32_t* sz;
+  double* tot;
+};
+__device__ __forceinline__ StateCopy write_copy(const PassDesc* __restrict__ D,
+                                                const StepIO& io) {
+  return io.parity ? StateCopy{D->L.comm, D->L.comm_sz, D->L.tot}
+                   : StateCopy{D->L.comm_alt, D->L.sz_alt, D->L.tot_alt};
+}
+
+// assignCommunity + incremental totals (modularity.cu:382-398) of one
+// vertex of weighted degree kv moving from oc to nc, into copy W.  FP64
+// sums of FP32 degrees are exact, so the order of the atomics does not
+// matter.
+__device__ __forceinline__ void move_into(const StateCopy& W, uint32_t v, float kv, uint32_t oc,
+                                          uint32_t nc) {
+  atomicSub(&W.sz[oc], 1u);
+  atomicAdd(&W.sz[nc], 1u);
+  atomicAdd(&W.tot[oc], -(double)kv);
+  atomicAdd(&W.tot[nc], (double)kv);
+  W.comm[v] = nc;
+}
+
+// The previous step's moves into the written copy: a vertex of classes
+// prev_lo..prev_hi still has its old community there (it moves in no
+// other step of the pass), its proposal is in prop[].
+__device__ __forceinline__ void reapply_prev_step(const PassDesc* __restrict__ D,
+                                                  const StepIO& io, uint32_t bid,
+                                                  uint32_t nblk) {
+  if (!io.fused || io.prev_lo == 0) return;
+  const StateCopy W = write_copy(D, io);
+  const float* __restrict__ k = D->L.k;
+  for (int c = io.prev_lo; c <= io.prev_hi; c++) {
+    const uint32_t s0 = D->A.P.cls_start[c];
+    const uint32_t count = (D->act_cnt && c <= kMoveClasses) ? D->act_cnt[c]
+                                                             : D->A.P.cls_start[c + 1] - s0;
+    const uint32_t* __restrict__ verts = D->A.order + s0;
+    const uint32_t* prop = D->prop + s0;
+    for (uint32_t i = bid * blockDim.x + threadIdx.x; i < count; i += nblk * blockDim.x) {
+      const uint32_t v = verts[i];
+      const uint32_t nc = prop[i];
+      const uint32_t oc = W.comm[v];
+      if (nc != oc) move_into(W, v, k[v], oc, nc);
+    }
+  }
+}
+
+// Records a decision: the proposal (read by the next step's re-apply and
+// by the separate apply launch) and, in a fused step, the move itself.
+__device__ __forceinline__ void record_decision(const PassDesc* __restrict__ D,
+                                                const StepIO& io, uint32_t* prop_slot,
+                                                uint32_t v, const GainCtx& g, uint32_t nc) {
+  *prop_slot = nc;
+  if (io.fused && nc != g.cv) move_into(write_copy(D, io), v, g.kv, g.cv, nc);
+}
+
+// ---------------------------------------------------------------------------
 // Move kernels
 // ---------------------------------------------------------------------------
 
@@ -331,10 +404,12 @@ __device__ __forceinline__ uint32_t table_insert(uint32_t* keys, uint32_t mask,
 // its one shared-memory arena.
 template <int G, int MODE>
 __device__ __forceinline__ void small_body(const PassDesc* __restrict__ D, int cls,
-                                           uint32_t bid, uint32_t nblk, double (*sums)[32]) {
+                                           uint32_t bid, uint32_t nblk, double (*sums)[32],
+                                           const StepIO io = StepIO{}) {
   constexpr int RULE = ModeOf<MODE>::kRule, PREC = ModeOf<MODE>::kPrec;
   using K = typename BestOf<PREC>::T;
-  const LevelView L = D->L;
+  const LevelView L = step_view(D, io);
+  reapply_prev_step(D, io, bid, nblk);
   const uint32_t s0 = D->A.P.cls_start[cls];
   const uint32_t* __restrict__ verts = D->A.order + s0;
   uint32_t* __restrict__ prop = D->prop + s0;
@@ -401,7 +476,7 @@ __device__ __forceinline__ void small_body(const PassDesc* __restrict__ D, int c
       best = candidate_loaded<PREC>(g, cu, sums[wib][lane], szc, ac);
     best = group_max<G>(best);
     if (RULE == LV_RULE_CUDA_I) own = group_sum<G>(own);
-    if (vvalid && gl == 0) prop[vidx] = decide<RULE>(best, own, g);
+    if (vvalid && gl == 0) record_decision(D, io, &prop[vidx], v, g, decide<RULE>(best, own, g));
     __syncwarp();
   }
 }
@@ -409,9 +484,9 @@ __device__ __forceinline__ void small_body(const PassDesc* __restrict__ D, int c
 // deg <= G: G lanes per vertex, one edge per lane.
 template <int G, int MODE>
 __global__ void __launch_bounds__(kThreads, kSmallPerSM)
-    move_small_kernel(const PassDesc* __restrict__ D, int cls) {
+    move_small_kernel(const PassDesc* __restrict__ D, int cls, StepIO io) {
   __shared__ double sums[kWarps][32];
-  small_body<G, MODE>(D, cls, blockIdx.x, gridDim.x, sums);
+  small_body<G, MODE>(D, cls, blockIdx.x, gridDim.x, sums, io);
 }
 
 // Best candidate among the taken slots of the first tv slots (nthr
@@ -458,9 +533,11 @@ __device__ __forceinline__ typename BestOf<PREC>::T scan_table_and_clear(
 // so a vertex costs one memory latency chain instead of one per wave.
 template <int T, int MAXW, int MODE>
 __device__ __forceinline__ void warp_body(const PassDesc* __restrict__ D, int cls, uint32_t bid,
-                                          uint32_t nblk, unsigned char* smem_raw) {
+                                          uint32_t nblk, unsigned char* smem_raw,
+                                          const StepIO io = StepIO{}) {
   constexpr int RULE = ModeOf<MODE>::kRule, PREC = ModeOf<MODE>::kPrec;
-  const LevelView L = D->L;
+  const LevelView L = step_view(D, io);
+  reapply_prev_step(D, io, bid, nblk);
   const uint32_t s0 = D->A.P.cls_start[cls];
   const uint32_t* __restrict__ verts = D->A.order + s0;
   uint32_t* __restrict__ prop = D->prop + s0;
@@ -535,16 +612,16 @@ __device__ __forceinline__ void warp_body(const PassDesc* __restrict__ D, int cl
     auto best = scan_table_and_clear<PREC>(L, g, keys, vals, tv, lane, 32);
     best = group_max<32>(best);
     if (RULE == LV_RULE_CUDA_I) own = group_sum<32>(own);
-    if (lane == 0) prop[vidx] = decide<RULE>(best, own, g);
+    if (lane == 0) record_decision(D, io, &prop[vidx], v, g, decide<RULE>(best, own, g));
     __syncwarp();
   }
 }
 
 template <int T, int MAXW, int MODE>
 __global__ void __launch_bounds__(kThreads, T == 128 ? kWarp128PerSM : kWarp512PerSM)
-    move_warp_kernel(const PassDesc* __restrict__ D, int cls) {
+    move_warp_kernel(const PassDesc* __restrict__ D, int cls, StepIO io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  warp_body<T, MAXW, MODE>(D, cls, blockIdx.x, gridDim.x, smem_raw);
+  warp_body<T, MAXW, MODE>(D, cls, blockIdx.x, gridDim.x, smem_raw, io);
 }
 
 template <class K>
@@ -623,10 +700,11 @@ template <int MODE>
 __device__ __forceinline__ void block_body(const PassDesc* __restrict__ D, int cls, uint32_t bid,
                                            uint32_t nblk, unsigned char* smem_raw,
                                            typename BestOf<ModeOf<MODE>::kPrec>::T* red_best,
-                                           double* red_own) {
+                                           double* red_own, const StepIO io = StepIO{}) {
   constexpr int RULE = ModeOf<MODE>::kRule, PREC = ModeOf<MODE>::kPrec;
   using K = typename BestOf<PREC>::T;
-  const LevelView L = D->L;
+  const LevelView L = step_view(D, io);
+  reapply_prev_step(D, io, bid, nblk);
   const uint32_t s0 = D->A.P.cls_start[cls];
   const uint32_t* __restrict__ verts = D->A.order + s0;
   uint32_t* __restrict__ prop = D->prop + s0;
@@ -683,7 +761,8 @@ __device__ __forceinline__ void block_body(const PassDesc* __restrict__ D, int c
         b = best_max(b, red_best[i]);
         if (RULE == LV_RULE_CUDA_I) o += red_own[i];
       }
-      prop[vidx] = decide<RULE>(b, RULE == LV_RULE_CUDA_I ? o : 0.0, g);
+      record_decision(D, io, &prop[vidx], v, g,
+                      decide<RULE>(b, RULE == LV_RULE_CUDA_I ? o : 0.0, g));
     }
     // no barrier here: the next vertex's first shared writes (the table's
     // inserts) touch no reduction slot, and the reduction slots are
@@ -695,11 +774,11 @@ __device__ __forceinline__ void block_body(const PassDesc* __restrict__ D, int c
 // 319 < deg <= 2048: one block per vertex, shared 4096-slot table.
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, kBlockPerSM)
-    move_block_kernel(const PassDesc* __restrict__ D, int cls) {
+    move_block_kernel(const PassDesc* __restrict__ D, int cls, StepIO io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ typename BestOf<ModeOf<MODE>::kPrec>::T red_best[kWarps];
   __shared__ double red_own[kWarps];
-  block_body<MODE>(D, cls, blockIdx.x, gridDim.x, smem_raw, red_best, red_own);
+  block_body<MODE>(D, cls, blockIdx.x, gridDim.x, smem_raw, red_best, red_own, io);
 }
 
 // deg > 2048 (hubs).  The neighbour communities of a hub are split into P
@@ -755,9 +834,10 @@ __device__ __forceinline__ uint32_t block_scan_inplace(uint32_t* a, uint32_t n,
 template <int MODE>
 __device__ __forceinline__ void split_body(const PassDesc* __restrict__ D, uint32_t bid,
                                            uint32_t nblk, uint32_t* cnt, uint32_t* wsum,
-                                           double* red) {
+                                           double* red, const StepIO io = StepIO{}) {
   constexpr int RULE = ModeOf<MODE>::kRule;
-  const LevelView L = D->L;
+  const LevelView L = step_view(D, io);
+  reapply_prev_step(D, io, bid, nblk);
   const uint32_t* __restrict__ hubs = D->A.order + D->A.P.cls_start[8];
   const HubArena H = D->H;
   const uint32_t nblocks = D->A.P.hub_blocks;
@@ -842,21 +922,22 @@ __device__ __forceinline__ void split_body(const PassDesc* __restrict__ D, uint3
 
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, kSplitPerSM)
-    hub_split_kernel(const PassDesc* __restrict__ D) {
+    hub_split_kernel(const PassDesc* __restrict__ D, StepIO io) {
   __shared__ uint32_t cnt[kHubMaxParts];
   __shared__ uint32_t wsum[kWarps];
   __shared__ double red[kWarps];
-  split_body<MODE>(D, blockIdx.x, gridDim.x, cnt, wsum, red);
+  split_body<MODE>(D, blockIdx.x, gridDim.x, cnt, wsum, red, io);
 }
 
 template <int MODE>
 __device__ __forceinline__ void merge_body(const PassDesc* __restrict__ D, uint32_t bid,
                                            uint32_t nblk, unsigned char* smem_raw,
                                            typename BestOf<ModeOf<MODE>::kPrec>::T* red_best,
-                                           uint32_t* seg_a, uint32_t* seg_pre, uint32_t* wsum) {
+                                           uint32_t* seg_a, uint32_t* seg_pre, uint32_t* wsum,
+                                           const StepIO io = StepIO{}) {
   constexpr int PREC = ModeOf<MODE>::kPrec;
   using K = typename BestOf<PREC>::T;
-  const LevelView L = D->L;
+  const LevelView L = step_view(D, io);
   const uint32_t* __restrict__ hubs = D->A.order + D->A.P.cls_start[8];
   const HubArena H = D->H;
   const uint32_t units = H.units;
@@ -926,19 +1007,19 @@ __device__ __forceinline__ void merge_body(const PassDesc* __restrict__ D, uint3
 
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, kMergePerSM)
-    hub_merge_kernel(const PassDesc* __restrict__ D) {
+    hub_merge_kernel(const PassDesc* __restrict__ D, StepIO io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ typename BestOf<ModeOf<MODE>::kPrec>::T red_best[kWarps];
   __shared__ uint32_t seg_a[kThreads], seg_pre[kThreads], wsum[kWarps];
-  merge_body<MODE>(D, blockIdx.x, gridDim.x, smem_raw, red_best, seg_a, seg_pre, wsum);
+  merge_body<MODE>(D, blockIdx.x, gridDim.x, smem_raw, red_best, seg_a, seg_pre, wsum, io);
 }
 
 template <int MODE>
 __device__ __forceinline__ void decide_body(const PassDesc* __restrict__ D, uint32_t bid,
-                                            uint32_t nblk) {
+                                            uint32_t nblk, const StepIO io = StepIO{}) {
   constexpr int RULE = ModeOf<MODE>::kRule, PREC = ModeOf<MODE>::kPrec;
   using K = typename BestOf<PREC>::T;
-  const LevelView L = D->L;
+  const LevelView L = step_view(D, io);
   const uint32_t* __restrict__ hubs = D->A.order + D->A.P.cls_start[8];
   const HubArena H = D->H;
   const uint32_t hub_count = D->A.P.hub_count;
@@ -955,7 +1036,7 @@ __device__ __forceinline__ void decide_body(const PassDesc* __restrict__ D, uint
     }
     // the own community's candidate from the split pass's sums
     if (H.hot_any[i]) best = best_max(best, candidate<PREC>(L, g, g.cv, H.hot[i]));
-    prop[i] = decide<RULE>(best, H.own[i], g);
+    record_decision(D, io, &prop[i], v, g, decide<RULE>(best, H.own[i], g));
     H.best[i] = 0ull;
     H.own[i] = 0.0;
     H.hot[i] = 0.0;
@@ -964,8 +1045,8 @@ __device__ __forceinline__ void decide_body(const PassDesc* __restrict__ D, uint
 }
 
 template <int MODE>
-__global__ void hub_decide_kernel(const PassDesc* __restrict__ D) {
-  decide_body<MODE>(D, blockIdx.x, gridDim.x);
+__global__ void hub_decide_kernel(const PassDesc* __restrict__ D, StepIO io) {
+  decide_body<MODE>(D, blockIdx.x, gridDim.x, io);
 }
 
 // Applies a bucket's proposals (assignCommunity + incremental totals).
@@ -1019,6 +1100,7 @@ struct RowSumOp {
     const float kf = (float)sum;
     L.k[v] = kf;
     L.tot[v] = (double)kf;
+    if (L.tot_alt) L.tot_alt[v] = (double)kf;
     part += (double)kf;
     return (double)kf;
   }
@@ -1257,9 +1339,14 @@ __global__ void __launch_bounds__(kThreads)
   for (uint32_t c = c0 + threadIdx.x; c < c1; c += kThreads) {
     L.comm[c] = c;
     L.comm_sz[c] = 1u;
+    if (L.comm_alt) {  // both copies of the state start equal
+      L.comm_alt[c] = c;
+      L.sz_alt[c] = 1u;
+    }
     if (L.off[c + 1] == L.off[c]) {
       L.k[c] = 0.0f;
       L.tot[c] = 0.0;
+      if (L.tot_alt) L.tot_alt[c] = 0.0;
     }
   }
   if (!publish_and_check_last(part, 0.0, A, L.sc, red)) return;
@@ -1272,6 +1359,7 @@ __global__ void __launch_bounds__(kThreads)
     const float kf = (float)__ldcg(&A.hub_acc[i]);
     L.k[v] = kf;
     L.tot[v] = (double)kf;
+    if (L.tot_alt) L.tot_alt[v] = (double)kf;
     A.hub_acc[i] = 0.0;
     hs += (double)kf;
     if (L.gid && kf != 0.0f) atomicAdd(&L.gs[L.gid[v]].m_acc, (double)kf);
@@ -1305,8 +1393,35 @@ __global__ void __launch_bounds__(kThreads)
 __device__ __forceinline__ double intra_sweep(const LevelView& L, const uint32_t* rowid,
                                              uint64_t nnz, uint32_t bid, uint32_t nblk) {
   double part = 0.0;
+  // 128-bit loads: a 4-entry vector of row ids, columns and weights per
+  // thread and iteration (every array 16-byte aligned: the engine's own
+  // buffers always are; a caller's may not be, and then the 32-bit loop
+  // below takes every entry)
+  uint64_t vec_end = 0;
+  if ((((uintptr_t)rowid | (uintptr_t)L.col | (uintptr_t)L.w) & 15u) == 0) {
+    const uint64_t nvec = nnz / 4;
+    const uint4* __restrict__ r4 = reinterpret_cast<const uint4*>(rowid);
+    const uint4* __restrict__ c4 = reinterpret_cast<const uint4*>(L.col);
+    const float4* __restrict__ w4 = reinterpret_cast<const float4*>(L.w);
+    const uint64_t vstride = (uint64_t)nblk * kThreads;
+    for (uint64_t q = (uint64_t)bid * kThreads + threadIdx.x; q < nvec; q += vstride) {
+      const uint4 r = __ldg(r4 + q);
+      const uint4 c = __ldg(c4 + q);
+      const float4 w = __ldg(w4 + q);
+      const uint32_t a0 = L.comm[r.x], b0 = L.comm[c.x];
+      const uint32_t a1 = L.comm[r.y], b1 = L.comm[c.y];
+      const uint32_t a2 = L.comm[r.z], b2 = L.comm[c.z];
+      const uint32_t a3 = L.comm[r.w], b3 = L.comm[c.w];
+      if (a0 == b0) part += (double)w.x;
+      if (a1 == b1) part += (double)w.y;
+      if (a2 == b2) part += (double)w.z;
+      if (a3 == b3) part += (double)w.w;
+    }
+    vec_end = nvec * 4;
+  }
+  // the entries after the last whole vector (or every entry, unaligned)
   const uint64_t stride = (uint64_t)nblk * kThreads * 4;
-  for (uint64_t b = (uint64_t)bid * kThreads * 4 + threadIdx.x; b < nnz; b += stride) {
+  for (uint64_t b = vec_end + (uint64_t)bid * kThreads * 4 + threadIdx.x; b < nnz; b += stride) {
     uint32_t r[4], c[4];
     float w[4];
 #pragma unroll
@@ -1423,10 +1538,13 @@ __global__ void __launch_bounds__(kThreads)
 // The modularity sweep of a pass (level and stop-rule limits from the
 // descriptor).
 __global__ void __launch_bounds__(kThreads, kModPerSM)
-    modularity_pass_kernel(const PassDesc* __restrict__ D, PassControl ctl) {
+    modularity_pass_kernel(const PassDesc* __restrict__ D, PassControl ctl, StepIO io) {
   ctl.min_gain = D->min_gain;
   ctl.max_passes = D->max_passes;
-  const LevelView L = D->L;
+  // reads the copy holding every move of the pass; the last step's moves
+  // go into the other copy, which leaves both equal for the next pass
+  const LevelView L = step_view(D, io);
+  reapply_prev_step(D, io, blockIdx.x, gridDim.x);
   modularity_body(L, D->A, ctl, D->rowid, D->nnz);
 }
 
@@ -1962,10 +2080,11 @@ cudaError_t launch_pass_control_init(const PassDesc* D, const PassControl* ctl, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_modularity_pass(const PassDesc* D, const PassControl* ctl, cudaStream_t st) {
+cudaError_t launch_modularity_pass(const PassDesc* D, const PassControl* ctl, cudaStream_t st,
+                                   StepIO io) {
   PassControl c{};
   if (ctl) c = *ctl;
-  (count_launches(1), modularity_pass_kernel<<<sm_count() * kModPerSM, kThreads, 0, st>>>(D, c));
+  (count_launches(1), modularity_pass_kernel<<<sm_count() * kModPerSM, kThreads, 0, st>>>(D, c, io));
   return cudaGetLastError();
 }
 
@@ -1973,65 +2092,69 @@ unsigned pass_dispatch_grid() { return sm_count() * kModPerSM; }
 
 // One launch of a move kernel variant over class `cls`.
 template <int MODE>
-static void launch_variant(int kv, const PassDesc* D, int cls, cudaStream_t st) {
+static void launch_variant(int kv, const PassDesc* D, int cls, cudaStream_t st, StepIO io) {
   const unsigned cap = sm_count() * kSmallPerSM;
   switch (kv) {
     case KV_SMALL4:
-      (count_launches(1), move_small_kernel<4, MODE><<<cap, kThreads, 0, st>>>(D, cls));
+      (count_launches(1), move_small_kernel<4, MODE><<<cap, kThreads, 0, st>>>(D, cls, io));
       break;
     case KV_SMALL8:
-      (count_launches(1), move_small_kernel<8, MODE><<<cap, kThreads, 0, st>>>(D, cls));
+      (count_launches(1), move_small_kernel<8, MODE><<<cap, kThreads, 0, st>>>(D, cls, io));
       break;
     case KV_SMALL16:
-      (count_launches(1), move_small_kernel<16, MODE><<<cap, kThreads, 0, st>>>(D, cls));
+      (count_launches(1), move_small_kernel<16, MODE><<<cap, kThreads, 0, st>>>(D, cls, io));
       break;
     case KV_SMALL32:
-      (count_launches(1), move_small_kernel<32, MODE><<<cap, kThreads, 0, st>>>(D, cls));
+      (count_launches(1), move_small_kernel<32, MODE><<<cap, kThreads, 0, st>>>(D, cls, io));
       break;
     case KV_WARP128: {
       constexpr int T = 128;
       (count_launches(1), move_warp_kernel<T, 3, MODE><<<sm_count() * kWarp128PerSM, kThreads,
-                                                       kWarps * T * kSlotBytes, st>>>(D, cls));
+                                                       kWarps * T * kSlotBytes, st>>>(D, cls, io));
       break;
     }
     case KV_WARP512: {
       constexpr int T = 512;
       (count_launches(1), move_warp_kernel<T, 10, MODE><<<sm_count() * kWarp512PerSM, kThreads,
-                                                        kWarps * T * kSlotBytes, st>>>(D, cls));
+                                                        kWarps * T * kSlotBytes, st>>>(D, cls, io));
       break;
     }
     default:  // KV_BLOCK: shared table, one block per vertex
       (count_launches(1), move_block_kernel<MODE><<<sm_count() * kBlockPerSM, kThreads,
-                                                   kBlockTabSmem, st>>>(D, cls));
+                                                   kBlockTabSmem, st>>>(D, cls, io));
       break;
   }
 }
 
 template <int MODE>
 static cudaError_t move_bucket_impl(const PassDesc* D, int bucket, const uint8_t* kv,
-                                    cudaStream_t st) {
+                                    cudaStream_t st, StepIO io) {
   if (bucket >= 1 && bucket <= 7) {
     const int v = kv ? kv[bucket] : kDefaultVariant[bucket];
     if (!variant_fits(v, bucket)) return cudaErrorInvalidValue;
-    launch_variant<MODE>(v, D, bucket, st);
+    launch_variant<MODE>(v, D, bucket, st, io);
     return cudaGetLastError();
   }
   if (bucket != 8) return cudaErrorInvalidValue;
-  // class 8 of bucket 7: split chunks, merge (hub, partition), decide
-  (count_launches(1), hub_split_kernel<MODE><<<sm_count() * kSplitPerSM, kThreads, 0, st>>>(D));
+  // class 8 of bucket 7: split chunks, merge (hub, partition), decide; the
+  // split re-applies the previous step's moves, the decide kernel applies
+  // the hubs' own
+  StepIO later = io;
+  later.prev_lo = later.prev_hi = 0;
+  (count_launches(1), hub_split_kernel<MODE><<<sm_count() * kSplitPerSM, kThreads, 0, st>>>(D, io));
   (count_launches(1), hub_merge_kernel<MODE><<<sm_count() * kMergePerSM, kThreads, kHubPartSmem,
-                                               st>>>(D));
-  (count_launches(1), hub_decide_kernel<MODE><<<sm_count() * 2, 128, 0, st>>>(D));
+                                               st>>>(D, later));
+  (count_launches(1), hub_decide_kernel<MODE><<<sm_count() * 2, 128, 0, st>>>(D, later));
   return cudaGetLastError();
 }
 
 cudaError_t launch_move_bucket(const PassDesc* D, int bucket, int mode, const uint8_t* variant,
-                               cudaStream_t st) {
+                               cudaStream_t st, StepIO io) {
   switch (mode) {
-    case 0: return move_bucket_impl<0>(D, bucket, variant, st);
-    case 1: return move_bucket_impl<1>(D, bucket, variant, st);
-    case 2: return move_bucket_impl<2>(D, bucket, variant, st);
-    case 3: return move_bucket_impl<3>(D, bucket, variant, st);
+    case 0: return move_bucket_impl<0>(D, bucket, variant, st, io);
+    case 1: return move_bucket_impl<1>(D, bucket, variant, st, io);
+    case 2: return move_bucket_impl<2>(D, bucket, variant, st, io);
+    case 3: return move_bucket_impl<3>(D, bucket, variant, st, io);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -251,6 +251,50 @@ def test_pass_loop_forms_agree(name):
 
 @pytest.mark.parametrize("rule", ["py", "cuda"])
 @pytest.mark.parametrize("gain", ["fp32", "fp64"])
+def test_fused_steps_equal_apply_launches(rule, gain):
+    """Bucket steps that apply their own moves into the second copy of the
+    community state (the default) run exactly as steps followed by a
+    separate apply launch: same partition, passes and Q, with the level
+    graph and with the host loop, on a graph with every degree class and on
+    one with hubs (whose decide kernel applies their moves)."""
+    for kind in ("planted", "rmat"):
+        if kind == "planted":
+            n, s, d, w = lvgen.planted_powerlaw(n=60000, target_edges=200000, seed=5,
+                                                unit=False)
+        else:
+            n, s, d, w = lvgen.rmat(15, edge_factor=16, seed=2)
+        off, col, ww = lvgen.csr_from_edges(n, s, d, w)
+        g = lvb200.Graph.from_csr(n, off, col, ww)
+        res = []
+        for al, ug in ((True, True), (False, True), (False, False)):
+            with lvb200.Engine(rule=rule, gain=gain, apply_launch=al, use_graphs=ug) as e:
+                res.append(e.run(g, 1e-6))
+        for r in res[1:]:
+            assert r.modularity == res[0].modularity
+            assert np.array_equal(r.assignment, res[0].assignment)
+            assert [l["passes"] for l in r.levels] == [l["passes"] for l in res[0].levels]
+            assert [l["q_end"] for l in r.levels] == [l["q_end"] for l in res[0].levels]
+
+
+def test_fused_steps_level_state():
+    """After a fused pass loop the level's state (the first copy, which the
+    contraction and the level-state reads use) equals the one the separate
+    apply launches leave, sizes and totals included."""
+    n, s, d, w = lvgen.rmat(13, edge_factor=16, seed=4)
+    off, col, ww = lvgen.csr_from_edges(n, s, d, w)
+    g = lvb200.Graph.from_csr(n, off, col, ww)
+    states = []
+    for al in (True, False):
+        with lvb200.Engine(rule="py", apply_launch=al) as e:
+            e.load(g)
+            e.phase_move(1e-6)
+            states.append(e.level_state())
+    for a, b in zip(states[0], states[1]):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("rule", ["py", "cuda"])
+@pytest.mark.parametrize("gain", ["fp32", "fp64"])
 def test_level_kernel_equals_level_graph_at_scale(rule, gain):
     """The power-law workload (every degree class) and an R-MAT graph with
     hubs, under both rules and both gain arithmetics."""
