@@ -490,8 +490,7 @@ void free_state(lv_engine* E) {
   dfree(E->hub.nparts);
   dfree(E->hub.stage_off);
   dfree(E->hub.ct_off);
-  dfree(E->hub.stage_c);
-  dfree(E->hub.stage_w);
+  dfree(E->hub.stage);
   dfree(E->hub.ct);
   dfree(E->hub.blk_vertex);
   dfree(E->hub.blk_chunk);
@@ -811,10 +810,8 @@ lv_status prepare_level(lv_engine* E, bool sync_scalars = true) {
     HubArena& H = E->hub;
     if (stage_total > E->hub_stage_cap) {
       E->hub_stage_cap = 0;
-      dfree(H.stage_c);
-      dfree(H.stage_w);
-      CU(dalloc(&H.stage_c, stage_total));
-      CU(dalloc(&H.stage_w, stage_total));
+      dfree(H.stage);
+      CU(dalloc(&H.stage, stage_total));
       E->hub_stage_cap = stage_total;
     }
     if (ct_total > E->hub_ct_cap) {

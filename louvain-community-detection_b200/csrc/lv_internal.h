@@ -238,8 +238,8 @@ struct HubArena {
   uint32_t* nparts = nullptr;      // [hub_count] partitions of the hub
   uint64_t* stage_off = nullptr;   // [hub_count] first staging entry of the hub
   uint64_t* ct_off = nullptr;      // [hub_count] first chunk-table entry of the hub
-  uint32_t* stage_c = nullptr;     // [hub entries] staged communities
-  float* stage_w = nullptr;        // [hub entries] staged weights
+  uint2* stage = nullptr;          // [hub entries] staged (community, weight bits):
+                                   // one 8-byte store and load per entry
   uint32_t* ct = nullptr;          // per hub: chunks x (nparts + 1) segment starts
   uint32_t* blk_vertex = nullptr;  // [units] hub index of each merge unit
   uint32_t* blk_chunk = nullptr;   // [units] partition of the unit

@@ -59,7 +59,7 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kSmallPerSM = 8;     // 32 registers
 constexpr int kWarp128PerSM = 5;   // 48 registers, 12 KB tables
 constexpr int kWarp512PerSM = 4;   // 64 registers, 48 KB tables
-constexpr int kBlockPerSM = 4;     // 64 registers, 48 KB table
+constexpr int kBlockPerSM = 3;     // 80 registers, 48 KB table
 constexpr int kSplitPerSM = 4;
 constexpr int kMergePerSM = 3;
 constexpr int kSweepPerSM = 8;     // apply
@@ -211,11 +211,22 @@ __device__ __forceinline__ typename BestOf<PREC>::T candidate_loaded(const GainC
   }
 }
 
+// Size of candidate community c as candidate_loaded needs it: only a
+// singleton vertex tests the candidate's size, and only for c > cv
+// (isLowerIdx), so every other candidate skips the gather -- these
+// per-lane random loads are what the move kernels' L1 pipe spends its
+// cycles on.
+__device__ __forceinline__ uint32_t candidate_size(const LevelView& L, const GainCtx& g,
+                                                   uint32_t c) {
+  if (c == g.cv) return g.szv;
+  return (g.szv == 1u && c > g.cv) ? L.comm_sz[c] : 0u;
+}
+
 template <int PREC>
 __device__ __forceinline__ typename BestOf<PREC>::T candidate(const LevelView& L,
                                                               const GainCtx& g, uint32_t c,
                                                               double ec) {
-  return candidate_loaded<PREC>(g, c, ec, L.comm_sz[c], L.tot[c]);
+  return candidate_loaded<PREC>(g, c, ec, candidate_size(L, g, c), L.tot[c]);
 }
 
 template <int RULE>
@@ -320,6 +331,30 @@ __device__ __forceinline__ uint32_t table_insert(uint32_t* keys, uint32_t mask,
   return 0;
 }
 
+// table_insert that also reports whether this call put the key into the
+// table: that thread owns the key's candidate (exactly one per distinct
+// key), evaluates it once the table is complete and empties its slot.
+__device__ __forceinline__ uint32_t table_claim(uint32_t* keys, uint32_t mask, uint32_t key,
+                                                LevelScalars* sc, bool& claimed) {
+  uint32_t h = hash_slot(key, mask);
+  claimed = false;
+  for (uint32_t it = 0; it <= mask; it++) {
+    uint32_t cur = keys[h];
+    if (cur == key) return h;
+    if (cur == kEmptyKey) {
+      const uint32_t prev = atomicCAS(&keys[h], kEmptyKey, key);
+      if (prev == kEmptyKey) {
+        claimed = true;
+        return h;
+      }
+      if (prev == key) return h;
+    }
+    h = (h + 1) & mask;
+  }
+  atomicExch(&sc->error, 1u);
+  return 0;
+}
+
 // ---------------------------------------------------------------------------
 // Community state of a bucket step (StepIO).  step_view's comm / comm_sz /
 // tot are the copy the step reads; a fused step writes its moves into the
@@ -384,6 +419,27 @@ __device__ __forceinline__ void reapply_prev_step(const PassDesc* __restrict__ D
   }
 }
 
+// A vertex of a class list with its row bounds and community: the block-
+// per-vertex kernel loads the next vertex's while it works on the current
+// one, so its id -> offsets -> community chain is off the critical path.
+struct VertexRow {
+  uint32_t v;
+  uint64_t s, e;
+  uint32_t cv;
+};
+__device__ __forceinline__ VertexRow fetch_vertex(const LevelView& L,
+                                                  const uint32_t* __restrict__ verts,
+                                                  uint32_t vidx, uint32_t count) {
+  VertexRow r{0u, 0ull, 0ull, 0u};
+  if (vidx < count) {
+    r.v = verts[vidx];
+    r.s = L.off[r.v];
+    r.e = L.off[r.v + 1];
+    r.cv = L.comm[r.v];
+  }
+  return r;
+}
+
 // Records a decision: the proposal (read by the next step's re-apply and
 // by the separate apply launch) and, in a fused step, the move itself.
 __device__ __forceinline__ void record_decision(const PassDesc* __restrict__ D,
@@ -442,7 +498,7 @@ __device__ __forceinline__ void small_body(const PassDesc* __restrict__ D, int c
       u = L.col[s + gl];
       wt = L.w[s + gl];
       cu = L.comm[u];
-      szc = L.comm_sz[cu];  // the candidate's data, read before the grouping
+      szc = candidate_size(L, g, cu);  // the candidate's data, read before the grouping
       ac = L.tot[cu];
     }
     // the own community's entries are summed with shuffles (its lowest
@@ -493,7 +549,7 @@ __global__ void __launch_bounds__(kThreads, kSmallPerSM)
 // threads from tid, four slots per thread at a time so the gathers
 // overlap); each thread empties the taken slots it read, leaving the table
 // clean.
-template <int PREC>
+template <int PREC, bool kAllSizes = false>
 __device__ __forceinline__ typename BestOf<PREC>::T scan_table_and_clear(
     const LevelView& L, const GainCtx& g, uint32_t* keys, double* vals,
     uint32_t tv, uint32_t tid, uint32_t nthr) {
@@ -511,7 +567,10 @@ __device__ __forceinline__ typename BestOf<PREC>::T scan_table_and_clear(
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       if (c[q] != kEmptyKey) {
-        szc[q] = L.comm_sz[c[q]];
+        // kAllSizes: every candidate's size, loaded with its total (the hub
+        // merge, 7% faster on R-MAT 24 than gathering only the sizes the
+        // isLowerIdx test reads, which it does after its segment walk)
+        szc[q] = kAllSizes ? L.comm_sz[c[q]] : candidate_size(L, g, c[q]);
         ac[q] = L.tot[c[q]];
       }
     }
@@ -525,6 +584,106 @@ __device__ __forceinline__ typename BestOf<PREC>::T scan_table_and_clear(
       }
     }
   }
+  return best;
+}
+
+// Row entries [s, e_end) spread over NT threads as 4-entry vectors: thread
+// t holds slot i = 4 k + j, the entry at 4 (s / 4 + k NT + t) + j (k < NV),
+// when it falls in the row.  A vector entirely inside the row is one
+// 128-bit load of columns and one of weights (vec_ok: both arrays 16-byte
+// aligned, as every buffer the engine allocates); the vectors at the row's
+// ends are loaded entry by entry, so nothing outside the row is read.
+// Slots outside the row get column `fill` and weight 0.
+template <int NV, int NT>
+__device__ __forceinline__ uint64_t vec_entry(uint64_t s, uint32_t t, int i) {
+  return ((s >> 2) + (uint64_t)(i >> 2) * NT + t) * 4 + (uint64_t)(i & 3);
+}
+template <int NV, int NT>
+__device__ __forceinline__ void load_row_vec(const LevelView& L, uint64_t s, uint64_t e_end,
+                                             uint32_t t, uint32_t fill, bool vec_ok,
+                                             uint32_t (&cu)[4 * NV], float (&wt)[4 * NV]) {
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    const uint64_t base = vec_entry<NV, NT>(s, t, 4 * k);
+    if (vec_ok && base >= s && base + 4 <= e_end) {
+      const uint4 c = __ldg(reinterpret_cast<const uint4*>(L.col) + (base >> 2));
+      const float4 w = __ldg(reinterpret_cast<const float4*>(L.w) + (base >> 2));
+      cu[4 * k] = c.x;
+      cu[4 * k + 1] = c.y;
+      cu[4 * k + 2] = c.z;
+      cu[4 * k + 3] = c.w;
+      wt[4 * k] = w.x;
+      wt[4 * k + 1] = w.y;
+      wt[4 * k + 2] = w.z;
+      wt[4 * k + 3] = w.w;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const uint64_t idx = base + (uint64_t)j;
+        const bool in = idx >= s && idx < e_end;
+        cu[4 * k + j] = in ? L.col[idx] : fill;
+        wt[4 * k + j] = in ? L.w[idx] : 0.0f;
+      }
+    }
+  }
+}
+
+// The candidates of the keys a thread claimed while its entries went into
+// a complete table: entry slot i's table slot is the i-th 16-bit field of
+// `slots` (bit i of `owned` set); the key is read back from the table, so
+// the entries' registers are free once they are inserted.  Four at a time,
+// so their gathers overlap; each slot is emptied after it is read, which
+// leaves the table clean without a scan of its empty slots.
+template <int NE>
+__device__ __forceinline__ void claim_slot(uint32_t (&slots)[(NE + 1) / 2], uint32_t& owned,
+                                           int i, uint32_t slot) {
+  owned |= 1u << i;
+#pragma unroll
+  for (int j = 0; j < (NE + 1) / 2; j++)  // i is a constant of the unrolled caller
+    if (j == (i >> 1)) slots[j] |= slot << (16 * (i & 1));
+}
+template <int PREC, int NE>
+__device__ __forceinline__ typename BestOf<PREC>::T eval_owned(
+    const LevelView& L, const GainCtx& g, uint32_t* keys, double* vals,
+    const uint32_t (&slots)[(NE + 1) / 2], uint32_t owned, typename BestOf<PREC>::T best) {
+#pragma unroll
+  for (int i0 = 0; i0 < NE; i0 += 4) {
+    if (((owned >> i0) & 0xFu) == 0u) continue;
+    uint32_t szc[4], slot[4], c[4];
+    double ec[4], ac[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int i = i0 + q;
+      if (i < NE && (owned >> i & 1u)) {
+        slot[q] = (slots[i >> 1] >> (16 * (i & 1))) & 0xFFFFu;
+        c[q] = keys[slot[q]];
+        ec[q] = vals[slot[q]];
+        szc[q] = candidate_size(L, g, c[q]);
+        ac[q] = L.tot[c[q]];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int i = i0 + q;
+      if (i < NE && (owned >> i & 1u)) {
+        best = best_max(best, candidate_loaded<PREC>(g, c[q], ec[q], szc[q], ac[q]));
+        keys[slot[q]] = kEmptyKey;
+        vals[slot[q]] = 0.0;
+      }
+    }
+  }
+  return best;
+}
+
+// The own community's candidate, for the thread that claimed its slot.
+template <int PREC>
+__device__ __forceinline__ typename BestOf<PREC>::T eval_own_slot(
+    const LevelView& L, const GainCtx& g, uint32_t* keys, double* vals, uint32_t slot,
+    typename BestOf<PREC>::T best) {
+  const double ec = vals[slot];
+  best = best_max(best, candidate_loaded<PREC>(g, g.cv, ec, g.szv, L.tot[g.cv]));
+  keys[slot] = kEmptyKey;
+  vals[slot] = 0.0;
   return best;
 }
 
@@ -547,6 +706,7 @@ __device__ __forceinline__ void warp_body(const PassDesc* __restrict__ D, int cl
   uint32_t* keys =
       reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T * kWarps) + wib * T;
   uint32_t clean = 0;  // leading table slots known to be empty
+  const bool vec_ok = (((uintptr_t)L.col | (uintptr_t)L.w) & 15u) == 0;
   for (uint32_t vidx = bid * kWarps + wib; vidx < count; vidx += nblk * kWarps) {
     const uint32_t v = verts[vidx];
     const uint64_t s = L.off[v];
@@ -566,42 +726,57 @@ __device__ __forceinline__ void warp_body(const PassDesc* __restrict__ D, int cl
       __syncwarp();
     }
     const GainCtx g = make_ctx<PREC>(L, v, cv);
-    uint32_t cu[MAXW];
-    float wt[MAXW];
-    unsigned self_mask = 0u;  // waves whose entry is the self-loop
+    // every load of the row issued before any is used.  Rows of up to 319
+    // entries come in 4-entry vectors (a vector crossing the row's start or
+    // end takes one extra slot): 5% faster on R-MAT 24's bucket 6; the
+    // shorter rows of the 128-slot variant keep one entry per lane per wave
+    // (vectors made it spill and run 17% slower there)
+    constexpr bool kVec = MAXW >= 8;
+    constexpr int NV = kVec ? (8 * MAXW + 1 + 31) / 32 : 0;
+    constexpr int NE = kVec ? 4 * NV : MAXW;
+    static_assert(NE <= 32, "one self-loop bit per slot");
+    uint32_t cu[NE];
+    float wt[NE];
+    const uint64_t e_end = s + d;
+    // absolute entry index of slot i of this lane
+    auto entry_of = [&](int i, uint32_t ln) -> uint64_t {
+      return kVec ? vec_entry<NV, 32>(s, ln, i) : s + (uint64_t)i * 32 + ln;
+    };
+    if constexpr (kVec) {
+      load_row_vec<NV, 32>(L, s, e_end, lane, v, vec_ok, cu, wt);
+    } else {
 #pragma unroll
-    for (int k = 0; k < MAXW; k++) {
-      const uint32_t j = k * 32 + lane;
-      cu[k] = v;
-      wt[k] = 0.0f;
-      if (j < d) {
-        cu[k] = L.col[s + j];
-        wt[k] = L.w[s + j];
+      for (int i = 0; i < NE; i++) {
+        const uint64_t idx = entry_of(i, lane);
+        cu[i] = idx < e_end ? L.col[idx] : v;
+        wt[i] = idx < e_end ? L.w[idx] : 0.0f;
       }
     }
+    unsigned self_mask = 0u;  // slots whose entry is the self-loop
 #pragma unroll
-    for (int k = 0; k < MAXW; k++) {
-      const uint32_t j = k * 32 + lane;
-      if (cu[k] == v) self_mask |= 1u << k;
-      cu[k] = (j < d) ? L.comm[cu[k]] : kEmptyKey;
+    for (int i = 0; i < NE; i++) {
+      const uint64_t idx = entry_of(i, lane);
+      const bool has = idx >= s && idx < e_end;
+      if (has && cu[i] == v) self_mask |= 1u << i;
+      cu[i] = has ? L.comm[cu[i]] : kEmptyKey;  // kEmptyKey: no entry
     }
     double own = 0.0, hot = 0.0;
     bool hot_seen = false;
 #pragma unroll
-    for (int k = 0; k < MAXW; k++) {
-      if ((uint32_t)k * 32 >= d) break;  // warp-uniform
-      const bool has = (uint32_t)k * 32 + lane < d;
+    for (int i = 0; i < NE; i++) {
+      if ((!kVec || (i & 3) == 0) && entry_of(i, 0) >= e_end) break;  // warp-uniform
+      const bool has = cu[i] != kEmptyKey;
       // entries into the vertex's own community (most of them once moves
       // converge) are summed in registers, not in one contended slot
-      const bool is_hot = has && cu[k] == cv;
+      const bool is_hot = has && cu[i] == cv;
       const bool ins = has && !is_hot;
       if (is_hot) {
-        hot += (double)wt[k];
+        hot += (double)wt[i];
         hot_seen = true;
-        if (RULE == LV_RULE_CUDA_I && !(self_mask >> k & 1u)) own += (double)wt[k];
+        if (RULE == LV_RULE_CUDA_I && !(self_mask >> i & 1u)) own += (double)wt[i];
       }
       // every lane inserts its own entry: equal keys meet in the CAS
-      if (ins) atomicAdd(&vals[table_insert(keys, tv - 1, cu[k], L.sc)], (double)wt[k]);
+      if (ins) atomicAdd(&vals[table_insert(keys, tv - 1, cu[i], L.sc)], (double)wt[i]);
     }
     hot = group_sum<32>(hot);
     if (__any_sync(kFull, hot_seen) && lane == 0) {
@@ -609,6 +784,8 @@ __device__ __forceinline__ void warp_body(const PassDesc* __restrict__ D, int cl
       vals[slot] += hot;
     }
     __syncwarp();
+    // (a scan of the row's table range: owner evaluation as in the block
+    // kernel made this kernel spill and run 37% slower at R-MAT 24)
     auto best = scan_table_and_clear<PREC>(L, g, keys, vals, tv, lane, 32);
     best = group_max<32>(best);
     if (RULE == LV_RULE_CUDA_I) own = group_sum<32>(own);
@@ -653,17 +830,21 @@ __device__ __forceinline__ double block_sum(double x, double* red) {
 
 // Loads entries [lo, end) of row s (at most MAXW waves of the block) into
 // registers -- every load issued before any is used -- then inserts them
-// into a table (clear it before, synchronise after).
+// into a table (clear it before, synchronise after).  cu / wt / owned come
+// back as eval_owned reads them.
 template <int MAXW, int RULE>
 __device__ __forceinline__ void insert_block_range(const LevelView& L, uint64_t s,
                                                    uint64_t lo, uint64_t end,
                                                    uint32_t v, uint32_t cv,
                                                    uint32_t* keys, double* vals,
                                                    uint32_t mask, double& own,
-                                                   double& hot, bool& hot_seen) {
+                                                   double& hot, bool& hot_seen,
+                                                   uint32_t (&slots)[(MAXW + 1) / 2],
+                                                   uint32_t& owned) {
   uint32_t cu[MAXW];
   float wt[MAXW];
   unsigned self_mask = 0u;
+  owned = 0u;
 #pragma unroll
   for (int k = 0; k < MAXW; k++) {
     const uint64_t j = lo + (uint64_t)k * kThreads + threadIdx.x;
@@ -692,7 +873,12 @@ __device__ __forceinline__ void insert_block_range(const LevelView& L, uint64_t 
       hot_seen = true;
       if (RULE == LV_RULE_CUDA_I && !(self_mask >> k & 1u)) own += (double)wt[k];
     }
-    if (ins) atomicAdd(&vals[table_insert(keys, mask, cu[k], L.sc)], (double)wt[k]);
+    if (ins) {
+      bool claimed;
+      const uint32_t slot = table_claim(keys, mask, cu[k], L.sc, claimed);
+      atomicAdd(&vals[slot], (double)wt[k]);
+      if (claimed) claim_slot<MAXW>(slots, owned, k, slot);
+    }
   }
 }
 
@@ -714,11 +900,13 @@ __device__ __forceinline__ void block_body(const PassDesc* __restrict__ D, int c
   double* vals = reinterpret_cast<double*>(smem_raw);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + sizeof(double) * T);
   uint32_t clean = 0;  // leading table slots known to be empty
+  VertexRow nxt = fetch_vertex(L, verts, bid, count);
   for (uint32_t vidx = bid; vidx < count; vidx += nblk) {
-    const uint32_t v = verts[vidx];
-    const uint64_t s = L.off[v];
-    const uint32_t d = (uint32_t)(L.off[v + 1] - s);
-    const uint32_t cv = L.comm[v];
+    const uint32_t v = nxt.v;
+    const uint64_t s = nxt.s;
+    const uint32_t d = (uint32_t)(nxt.e - nxt.s);
+    const uint32_t cv = nxt.cv;
+    nxt = fetch_vertex(L, verts, vidx + nblk, count);
     if (!vertex_active(L, v)) {  // block-uniform: one vertex per block
       if (threadIdx.x == 0) prop[vidx] = cv;
       continue;
@@ -736,18 +924,27 @@ __device__ __forceinline__ void block_body(const PassDesc* __restrict__ D, int c
     double own = 0.0;
     double hot = 0.0;
     bool hot_seen = false;
+    uint32_t slots[(MAXW + 1) / 2] = {};
+    uint32_t owned;
     insert_block_range<MAXW, RULE>(L, s, 0, d, v, cv, keys, vals, tv - 1, own, hot,
-                                   hot_seen);
+                                   hot_seen, slots, owned);
     // every warp adds its share of the own community's weight to that
     // community's slot (FP64 sums of FP32 weights are exact in any order),
-    // so no block-wide sum is needed before the table is complete
+    // so no block-wide sum is needed before the table is complete; the
+    // warp whose add put the key in owns the candidate
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     hot = group_sum<32>(hot);
-    if (__any_sync(kFull, hot_seen) && lane == 0)
-      atomicAdd(&vals[table_insert(keys, tv - 1, cv, L.sc)], hot);
+    uint32_t hot_slot = kEmptyKey;
+    if (__any_sync(kFull, hot_seen) && lane == 0) {
+      bool claimed;
+      const uint32_t slot = table_claim(keys, tv - 1, cv, L.sc, claimed);
+      atomicAdd(&vals[slot], hot);
+      if (claimed) hot_slot = slot;
+    }
     if (RULE == LV_RULE_CUDA_I) own = group_sum<32>(own);
     __syncthreads();  // (A) the table is complete
-    K best = scan_table_and_clear<PREC>(L, g, keys, vals, tv, threadIdx.x, kThreads);
+    K best = eval_owned<PREC, MAXW>(L, g, keys, vals, slots, owned, K{});
+    if (hot_slot != kEmptyKey) best = eval_own_slot<PREC>(L, g, keys, vals, hot_slot, best);
     best = group_max<32>(best);
     if (lane == 0) {  // written after (A): thread 0 read the last ones before it
       red_best[wib] = best;
@@ -901,8 +1098,7 @@ __device__ __forceinline__ void split_body(const PassDesc* __restrict__ D, uint3
     for (int k = 0; k < EPT; k++) {
       if (part[k] == kEmptyKey) continue;
       const uint64_t pos = base + cnt[part[k]] + rank[k];
-      H.stage_c[pos] = c[k];
-      H.stage_w[pos] = w[k];
+      H.stage[pos] = make_uint2(c[k], __float_as_uint(w[k]));
     }
     const int any_hot = __syncthreads_or(hot_seen);
     if (any_hot) {
@@ -983,15 +1179,16 @@ __device__ __forceinline__ void merge_body(const PassDesc* __restrict__ D, uint3
             if (seg_pre[mid] <= f) lo = mid; else hi2 = mid - 1;
           }
           const uint64_t pos = sb + (uint64_t)(cb + lo) * kHubChunk + seg_a[lo] + (f - seg_pre[lo]);
-          c = H.stage_c[pos];
-          w = H.stage_w[pos];
+          const uint2 cw = H.stage[pos];
+          c = cw.x;
+          w = __uint_as_float(cw.y);
         }
         if (has) atomicAdd(&vals[table_insert(keys, T - 1, c, L.sc)], (double)w);
       }
       __syncthreads();  // seg_a / seg_pre are refilled
     }
     const GainCtx g = make_ctx<PREC>(L, v, L.comm[v]);
-    K best = scan_table_and_clear<PREC>(L, g, keys, vals, T, threadIdx.x, kThreads);
+    K best = scan_table_and_clear<PREC, true>(L, g, keys, vals, T, threadIdx.x, kThreads);
     best = block_max(best, red_best);
     if (threadIdx.x == 0) {
       if constexpr (PREC) {  // no 96-bit atomic: the decide kernel reduces the units
