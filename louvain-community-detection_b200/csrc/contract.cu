@@ -216,10 +216,19 @@ __global__ void __launch_bounds__(kThreads)
       if (mv) my_off = C.off[C.members[m0 + mi]];
       const uint64_t lo = __shfl_sync(kFull, my_start, 0);
       const uint64_t hi = (mb + 32 < msz) ? C.mstart[m0 + mb + 32] - seg : total;
-      for (uint64_t p0 = lo; p0 < hi; p0 += 32) {
-        const uint64_t p = p0 + lane;
-        const bool has = p < hi;
-        // largest member k with start_k <= p
+      // the batch's entries (at most kMergeWarpMax: a community of this
+      // class has no more) in kWaves waves whose loads are all issued
+      // before the first insert
+      constexpr int kWaves = (int)(kMergeWarpMax / 32);
+      uint32_t key[kWaves];
+      float wt[kWaves];
+#pragma unroll
+      for (int k = 0; k < kWaves; k++) {
+        key[k] = kEmptyKey;
+        wt[k] = 0.0f;
+        if (lo + (uint64_t)k * 32 >= hi) continue;  // warp-uniform: most rows are short
+        const uint64_t p = lo + (uint64_t)k * 32 + lane;
+        // largest member q with start_q <= p
         int klo = 0, khi = (int)nvalid - 1;
 #pragma unroll
         for (int it = 0; it < 5; it++) {
@@ -230,22 +239,24 @@ __global__ void __launch_bounds__(kThreads)
         }
         const uint64_t vo = __shfl_sync(kFull, my_off, klo);
         const uint64_t vs = __shfl_sync(kFull, my_start, klo);
-        uint32_t key = kEmptyKey;
-        float wt = 0.0f;
-        bool ins = false;
-        if (has) {
+        if (p < hi) {
           const uint64_t j = vo + (p - vs);
-          key = C.cnew[C.col[j]];
-          wt = C.w[j];
-          if (key == cn) {  // intra-community edge: the new self-loop
-            hot_acc += (double)wt;
-            hot_seen = true;
-          } else {
-            ins = true;
-          }
+          key[k] = C.col[j];
+          wt[k] = C.w[j];
         }
-        // every lane inserts its own entry: equal keys meet in the CAS
-        if (ins) atomicAdd(&vals[table_insert(keys, mask, key, C.err)], (double)wt);
+      }
+#pragma unroll
+      for (int k = 0; k < kWaves; k++)
+        if (key[k] != kEmptyKey) key[k] = C.cnew[key[k]];
+#pragma unroll
+      for (int k = 0; k < kWaves; k++) {
+        if (key[k] == kEmptyKey) continue;
+        if (key[k] == cn) {  // intra-community edge: the new self-loop
+          hot_acc += (double)wt[k];
+          hot_seen = true;
+        } else {  // every lane inserts its own entry: equal keys meet in the CAS
+          atomicAdd(&vals[table_insert(keys, mask, key[k], C.err)], (double)wt[k]);
+        }
       }
     }
     hot_acc = warp_sum(hot_acc);
@@ -336,29 +347,42 @@ __device__ __forceinline__ void insert_range(const Ctx& C, uint32_t m0,
     const uint32_t nvalid = min((uint32_t)kThreads, msz - k0);
     const uint64_t chunk_end =
         (k0 + kThreads < msz) ? min(hi, C.mstart[m0 + k0 + kThreads] - seg) : hi;
-    for (uint64_t p0 = pos; p0 < chunk_end; p0 += kThreads) {
-      const uint64_t p = p0 + threadIdx.x;
-      const bool has = p < chunk_end;
-      uint32_t key = kEmptyKey;
-      float wt = 0.0f;
-      bool ins = false;
-      if (has) {
-        int a = 0, b = (int)nvalid - 1;
-        while (a < b) {
-          const int mid = (a + b + 1) >> 1;
-          if (s_start[mid] <= p) a = mid; else b = mid - 1;
-        }
-        const uint64_t j = s_off[a] + (p - s_start[a]);
-        key = C.cnew[C.col[j]];
-        wt = C.w[j];
-        if (key == hot) {
-          hot_acc += (double)wt;
-          hot_seen = true;
-        } else {
-          ins = true;
+    // kWaves waves of the block at a time, every load of a batch issued
+    // before its first insert
+    constexpr int kWaves = 4;
+    for (uint64_t p0 = pos; p0 < chunk_end; p0 += (uint64_t)kWaves * kThreads) {
+      uint32_t key[kWaves];
+      float wt[kWaves];
+#pragma unroll
+      for (int k = 0; k < kWaves; k++) {
+        const uint64_t p = p0 + (uint64_t)k * kThreads + threadIdx.x;
+        key[k] = kEmptyKey;
+        wt[k] = 0.0f;
+        if (p0 + (uint64_t)k * kThreads >= chunk_end) continue;  // block-uniform
+        if (p < chunk_end) {
+          int a = 0, b = (int)nvalid - 1;
+          while (a < b) {
+            const int mid = (a + b + 1) >> 1;
+            if (s_start[mid] <= p) a = mid; else b = mid - 1;
+          }
+          const uint64_t j = s_off[a] + (p - s_start[a]);
+          key[k] = C.col[j];
+          wt[k] = C.w[j];
         }
       }
-      if (ins) atomicAdd(&vals[table_insert(keys, mask, key, C.err)], (double)wt);
+#pragma unroll
+      for (int k = 0; k < kWaves; k++)
+        if (key[k] != kEmptyKey) key[k] = C.cnew[key[k]];
+#pragma unroll
+      for (int k = 0; k < kWaves; k++) {
+        if (key[k] == kEmptyKey) continue;
+        if (key[k] == hot) {
+          hot_acc += (double)wt[k];
+          hot_seen = true;
+        } else {
+          atomicAdd(&vals[table_insert(keys, mask, key[k], C.err)], (double)wt[k]);
+        }
+      }
     }
     pos = chunk_end;
     k0 += kThreads;
@@ -505,9 +529,10 @@ __global__ void __launch_bounds__(kThreads)
 // left to compress_long_kernel, where the whole grid copies each.
 constexpr uint64_t kLongRow = kMergeBlockMax;
 __global__ void __launch_bounds__(kThreads)
-    compress_kernel(const uint64_t* seg, const uint64_t* new_off, uint32_t new_n,
-                    const uint32_t* tcol, const float* tw, uint32_t* out_col,
-                    float* out_w) {
+    compress_kernel(const uint64_t* __restrict__ seg, const uint64_t* __restrict__ new_off,
+                    uint32_t new_n, const uint32_t* __restrict__ tcol,
+                    const float* __restrict__ tw, uint32_t* __restrict__ out_col,
+                    float* __restrict__ out_w) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint64_t nwarps = (uint64_t)gridDim.x * kWarps;
   const uint64_t w = (uint64_t)blockIdx.x * kWarps + wib;
@@ -523,9 +548,27 @@ __global__ void __launch_bounds__(kThreads)
     for (int i = 0; i < 32; i++) {
       const uint64_t di = __shfl_sync(kFull, dst, i), ci = __shfl_sync(kFull, cnt, i);
       const uint64_t si = __shfl_sync(kFull, src, i);
-      for (uint64_t j = lane; j < ci; j += 32) {
-        out_col[di + j] = tcol[si + j];
-        out_w[di + j] = tw[si + j];
+      // four loads in flight per lane (the staging and the output do not
+      // overlap), so a long row is not one round trip per 32 entries
+      for (uint64_t j0 = 0; j0 < ci; j0 += 128) {
+        uint32_t c[4];
+        float w[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const uint64_t j = j0 + (uint64_t)k * 32 + lane;
+          if (j < ci) {
+            c[k] = tcol[si + j];
+            w[k] = tw[si + j];
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const uint64_t j = j0 + (uint64_t)k * 32 + lane;
+          if (j < ci) {
+            out_col[di + j] = c[k];
+            out_w[di + j] = w[k];
+          }
+        }
       }
     }
   }

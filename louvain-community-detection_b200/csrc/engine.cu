@@ -908,6 +908,7 @@ lv_status upload_desc(lv_engine* E, float min_gain) {
   d.max_passes = E->cfg.max_passes;
   for (int b = 0; b < 8; b++) d.tune[b] = E->tune[b];
   d.loop = E->loop_state;
+  d.fused = E->cfg.apply_launch ? 0u : 1u;
   // through pinned memory: a copy from pageable memory would wait for the
   // stream first; the previous copy must have left the buffer
   CU(cudaEventSynchronize(E->desc_ev));

@@ -315,6 +315,9 @@ struct PassDesc {
   // barrier / timer state
   uint8_t tune[8];
   LevelLoopState* loop;
+  // persistent level kernel: bucket steps apply their own moves (StepIO)
+  // instead of separate apply phases
+  uint32_t fused;
 };
 
 // How one bucket step of a pass treats the community state.  fused = 0:

@@ -1845,38 +1845,39 @@ __device__ __forceinline__ bool grid_barrier(LevelLoopState* S, uint32_t nblk,
 // to itself instead of sharing one allocation across the whole loop.
 template <int G, int MODE>
 __device__ __noinline__ void small_phase(const PassDesc* __restrict__ D, int cls, uint32_t bid,
-                                         uint32_t nblk, unsigned char* smem) {
-  small_body<G, MODE>(D, cls, bid, nblk, reinterpret_cast<double(*)[32]>(smem));
+                                         uint32_t nblk, unsigned char* smem, StepIO io) {
+  small_body<G, MODE>(D, cls, bid, nblk, reinterpret_cast<double(*)[32]>(smem), io);
 }
 template <int T, int MAXW, int MODE>
 __device__ __noinline__ void warp_phase(const PassDesc* __restrict__ D, int cls, uint32_t bid,
-                                        uint32_t nblk, unsigned char* smem) {
-  warp_body<T, MAXW, MODE>(D, cls, bid, nblk, smem);
+                                        uint32_t nblk, unsigned char* smem, StepIO io) {
+  warp_body<T, MAXW, MODE>(D, cls, bid, nblk, smem, io);
 }
 template <int MODE>
 __device__ __noinline__ void block_phase(const PassDesc* __restrict__ D, int cls, uint32_t bid,
                                          uint32_t nblk, unsigned char* smem,
                                          typename BestOf<ModeOf<MODE>::kPrec>::T* red_best,
-                                         double* red_d) {
-  block_body<MODE>(D, cls, bid, nblk, smem, red_best, red_d);
+                                         double* red_d, StepIO io) {
+  block_body<MODE>(D, cls, bid, nblk, smem, red_best, red_d, io);
 }
 template <int MODE>
 __device__ __noinline__ void split_phase(const PassDesc* __restrict__ D, uint32_t bid,
                                          uint32_t nblk, unsigned char* smem, uint32_t* wsum,
-                                         double* red_d) {
-  split_body<MODE>(D, bid, nblk, reinterpret_cast<uint32_t*>(smem), wsum, red_d);
+                                         double* red_d, StepIO io) {
+  split_body<MODE>(D, bid, nblk, reinterpret_cast<uint32_t*>(smem), wsum, red_d, io);
 }
 template <int MODE>
 __device__ __noinline__ void merge_phase(const PassDesc* __restrict__ D, uint32_t bid,
                                          uint32_t nblk, unsigned char* smem,
                                          typename BestOf<ModeOf<MODE>::kPrec>::T* red_best,
-                                         uint32_t* seg_a, uint32_t* seg_pre, uint32_t* wsum) {
-  merge_body<MODE>(D, bid, nblk, smem, red_best, seg_a, seg_pre, wsum);
+                                         uint32_t* seg_a, uint32_t* seg_pre, uint32_t* wsum,
+                                         StepIO io) {
+  merge_body<MODE>(D, bid, nblk, smem, red_best, seg_a, seg_pre, wsum, io);
 }
 template <int MODE>
 __device__ __noinline__ void decide_phase(const PassDesc* __restrict__ D, uint32_t bid,
-                                          uint32_t nblk) {
-  decide_body<MODE>(D, bid, nblk);
+                                          uint32_t nblk, StepIO io) {
+  decide_body<MODE>(D, bid, nblk, io);
 }
 __device__ __noinline__ void apply_phase(const PassDesc* __restrict__ D, int lo, int hi,
                                          uint32_t bid, uint32_t nblk) {
@@ -1886,8 +1887,11 @@ __device__ __noinline__ void apply_phase(const PassDesc* __restrict__ D, int lo,
 // community totals (modularity.cu:400-436), in partials[bid] and
 // partials[nblk + bid].
 __device__ __noinline__ void modularity_share_phase(const PassDesc* __restrict__ D, uint32_t bid,
-                                                    uint32_t nblk, double* red_d) {
-  const LevelView L = D->L;
+                                                    uint32_t nblk, double* red_d, StepIO io) {
+  // fused steps: the copy holding every move of the pass; the last step's
+  // moves go into the other copy
+  const LevelView L = step_view(D, io);
+  reapply_prev_step(D, io, bid, nblk);
   double part = intra_sweep(L, D->rowid, D->nnz, bid, nblk);
   const uint32_t chunk = (L.n + nblk - 1) / nblk;
   const uint32_t c0 = bid * chunk, c1 = min(L.n, c0 + chunk);
@@ -1908,15 +1912,15 @@ template <int MODE>
 __device__ __forceinline__ void run_variant(int kv, const PassDesc* __restrict__ D, int cls,
                                             uint32_t bid, uint32_t nblk, unsigned char* smem,
                                             typename BestOf<ModeOf<MODE>::kPrec>::T* red_best,
-                                            double* red_d) {
+                                            double* red_d, StepIO io) {
   switch (kv) {
-    case KV_SMALL4: small_phase<4, MODE>(D, cls, bid, nblk, smem); break;
-    case KV_SMALL8: small_phase<8, MODE>(D, cls, bid, nblk, smem); break;
-    case KV_SMALL16: small_phase<16, MODE>(D, cls, bid, nblk, smem); break;
-    case KV_SMALL32: small_phase<32, MODE>(D, cls, bid, nblk, smem); break;
-    case KV_WARP128: warp_phase<128, 3, MODE>(D, cls, bid, nblk, smem); break;
-    case KV_WARP512: warp_phase<512, 10, MODE>(D, cls, bid, nblk, smem); break;
-    default: block_phase<MODE>(D, cls, bid, nblk, smem, red_best, red_d); break;
+    case KV_SMALL4: small_phase<4, MODE>(D, cls, bid, nblk, smem, io); break;
+    case KV_SMALL8: small_phase<8, MODE>(D, cls, bid, nblk, smem, io); break;
+    case KV_SMALL16: small_phase<16, MODE>(D, cls, bid, nblk, smem, io); break;
+    case KV_SMALL32: small_phase<32, MODE>(D, cls, bid, nblk, smem, io); break;
+    case KV_WARP128: warp_phase<128, 3, MODE>(D, cls, bid, nblk, smem, io); break;
+    case KV_WARP512: warp_phase<512, 10, MODE>(D, cls, bid, nblk, smem, io); break;
+    default: block_phase<MODE>(D, cls, bid, nblk, smem, red_best, red_d, io); break;
   }
 }
 
@@ -1955,27 +1959,45 @@ __global__ void __launch_bounds__(kThreads, kLoopPerSM)
   const double min_gain = D->min_gain;
   const uint32_t max_passes = D->max_passes;
   const bool hubs = A.P.hub_count > 0;
+  // fused steps (StepIO): no apply phase and no barrier after it; step s
+  // reads copy s % 2 of the community state, the sweep re-applies the last
+  // step's moves
+  const int fused = D->fused ? 1 : 0;
   for (;;) {
+    StepIO io{fused, 0, 0, 0};
+    int step = 0;
     for (int b = 1; b <= kBuckets; b++) {
       const bool has = A.P.cls_start[b + 1] > A.P.cls_start[b];
       const bool hb = b == kBuckets && hubs;
       if (!has && !hb) continue;  // uniform: the plan is the level's
-      if (has) run_variant<MODE>(D->tune[b], D, b, bid, nblk, smem_raw, red_best, red_d);
+      io.parity = fused ? (step & 1) : 0;
+      if (has) {
+        run_variant<MODE>(D->tune[b], D, b, bid, nblk, smem_raw, red_best, red_d, io);
+        io.prev_lo = io.prev_hi = 0;  // re-applied by this phase
+      }
       if (hb) {
-        split_phase<MODE>(D, bid, nblk, smem_raw, wsum, red_d);
+        split_phase<MODE>(D, bid, nblk, smem_raw, wsum, red_d, io);
+        io.prev_lo = io.prev_hi = 0;
         if (!phase_end(b - 1)) return;
-        merge_phase<MODE>(D, bid, nblk, smem_raw, red_best, seg_a, seg_pre, wsum);
+        merge_phase<MODE>(D, bid, nblk, smem_raw, red_best, seg_a, seg_pre, wsum, io);
         if (!phase_end(7)) return;
-        decide_phase<MODE>(D, bid, nblk);
+        decide_phase<MODE>(D, bid, nblk, io);
         if (!phase_end(7)) return;
       } else if (!phase_end(b - 1)) {
         return;
       }
-      apply_phase(D, b, hb ? 8 : b, bid, nblk);
-      if (!phase_end(8)) return;
+      if (fused) {
+        io.prev_lo = b;
+        io.prev_hi = hb ? 8 : b;
+        step++;
+      } else {
+        apply_phase(D, b, hb ? 8 : b, bid, nblk);
+        if (!phase_end(8)) return;
+      }
     }
+    io.parity = fused ? (step & 1) : 0;
     // modularity of the pass: this block's shares ...
-    modularity_share_phase(D, bid, nblk, red_d);
+    modularity_share_phase(D, bid, nblk, red_d, io);
     if (!phase_end(9)) return;
     // ... then every block sums all shares in the same fixed order, so all
     // blocks hold the same Q and take the same stop decision

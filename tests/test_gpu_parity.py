@@ -306,18 +306,21 @@ def test_level_kernel_equals_level_graph_at_scale(rule, gain):
         off, col, ww = lvgen.csr_from_edges(n, s, d, w)
         g = lvb200.Graph.from_csr(n, off, col, ww)
         res = []
-        for lk in (True, False):
-            with lvb200.Engine(rule=rule, gain=gain, level_kernel=lk) as e:
+        for lk, al in ((True, False), (False, False), (True, True)):
+            with lvb200.Engine(rule=rule, gain=gain, level_kernel=lk, apply_launch=al) as e:
                 res.append(e.run(g, 1e-6))
-        assert abs(res[0].modularity - res[1].modularity) < 1e-12
-        assert np.array_equal(res[0].assignment, res[1].assignment)
-        assert [l["passes"] for l in res[0].levels] == [l["passes"] for l in res[1].levels]
+        for r in res[1:]:
+            assert abs(res[0].modularity - r.modularity) < 1e-12
+            assert np.array_equal(res[0].assignment, r.assignment)
+            assert [l["passes"] for l in res[0].levels] == [l["passes"] for l in r.levels]
 
 
-def test_level_kernel_phase_timers():
+@pytest.mark.parametrize("apply_launch", [False, True])
+def test_level_kernel_phase_timers(apply_launch):
     """With profiling on, the level kernel's barrier timestamps give every
-    phase kind a device time and a count."""
-    with lvb200.Engine(rule="py", level_kernel=True) as eng:
+    phase kind a device time and a count; its bucket phases apply their own
+    moves unless lv_config.apply_launch asks for separate apply phases."""
+    with lvb200.Engine(rule="py", level_kernel=True, apply_launch=apply_launch) as eng:
         eng.set_profiling(True)
         eng.reset_kernel_stats()
         res = eng.run(lvb200.Graph.load_mtx(golden_mtx("hub3000")), 1e-6)
@@ -325,7 +328,10 @@ def test_level_kernel_phase_timers():
     passes = sum(l["passes"] for l in res.levels)
     # one sweep per pass, plus each level's initial one
     assert st["modularity"]["launches"] == passes + len(res.levels)
-    assert st["apply"]["launches"] >= passes
+    if apply_launch:
+        assert st["apply"]["launches"] >= passes
+    else:
+        assert st["apply"]["launches"] == 0
     assert st["move_hub"]["launches"] >= 2
     assert all(v["total_ms"] >= 0.0 for v in st.values())
     assert st["modularity"]["total_ms"] > 0.0
