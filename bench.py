@@ -194,7 +194,7 @@ def cpu_baseline(n, off, col, ww, budget_s=12.0):
             "final_q": q}
 
 
-def batched_measure(stream, count: int, steps: int = 2):
+def batched_measure(stream, count: int, steps: int = 2, apply_launch: bool = False):
     """Batched form on the SBM batch workload (count graphs, sizes
     log-uniform 64..65,536, 4-32 equal blocks, mean degree 16,
     p_in/p_out = 20, weights U(0.5, 1.5), generated on the device):
@@ -215,7 +215,7 @@ def batched_measure(stream, count: int, steps: int = 2):
            "blocks": "4..32", "mean_degree": 16, "p_in/p_out": 20,
            "weights": "U(0.5,1.5) FP32", "seed": 0}
     with torch.cuda.stream(stream):
-        eng = lvb200.Engine(stream=stream.cuda_stream)
+        eng = lvb200.Engine(stream=stream.cuda_stream, apply_launch=apply_launch)
         # kernel variants tuned on the union's level 0 (untimed)
         eng.load_device(N, E, off.data_ptr(), col.data_ptr(), w.data_ptr())
         res["tuning"] = {str(b): k for b, (k, _) in eng.autotune().items()}
@@ -238,7 +238,7 @@ def batched_measure(stream, count: int, steps: int = 2):
         # plain engine looped over the same graphs (local CSR views)
         loff, lcol = lvgen.localize_batch(goff, off, col)
         eoff = off[torch.from_numpy(goff.astype(np.int64)).cuda()].cpu().numpy()
-        plain = lvb200.Engine(stream=stream.cuda_stream)
+        plain = lvb200.Engine(stream=stream.cuda_stream, apply_launch=apply_launch)
         q_p = np.zeros(count)
 
         def one(g):
@@ -675,7 +675,7 @@ def run_engine(args, rank, world):
     eng.close()
     batched = served = hbm = None
     if world == 1 and args.batch_graphs > 0:
-        batched = batched_measure(stream, args.batch_graphs)
+        batched = batched_measure(stream, args.batch_graphs, apply_launch=args.apply_launch)
     if world == 1 and args.serve_requests > 0:
         served = served_measure(args.serve_requests, args.serve_rate,
                                 int(args.serve_budget_gb * 1e9),

@@ -89,6 +89,16 @@ typedef struct lv_config {
                                moves into a second copy of the community
                                state (same results, one launch less per
                                bucket)                                      */
+    int modularity_full;    /* 1: every pass's modularity from a sweep over
+                               all entries; 0 (default): on levels of at
+                               least 2^23 entries, after a pass that moved
+                               under a quarter of the entries, the next
+                               pass's sweep visits only the rows of the
+                               vertices it moved.  That update assumes every
+                               edge is stored in both of its rows with the
+                               same weight, as the reference's reader and
+                               every graph built here store it; set 1 for a
+                               caller's CSR that is not symmetric          */
 } lv_config;
 
 /* Per-level record (the reference prints none of this; -v here adds it). */

@@ -74,6 +74,11 @@ struct LevelScalars {
   uint32_t act_changed;  // batched form: a graph stopped moving in the last
                          // pass, so the active lists must be compacted again
   double q_start;        // Q when the level's pass loop began
+  // single graph: entries of the vertices that moved in the last pass
+  // (accumulated by the sweep), and whether the next sweep updates the
+  // intra-community weight from those rows only
+  unsigned long long moved_acc;
+  uint32_t inc_next;
 };
 
 // Stop rule evaluated by the modularity sweep's last block when the pass
@@ -318,6 +323,9 @@ struct PassDesc {
   // persistent level kernel: bucket steps apply their own moves (StepIO)
   // instead of separate apply phases
   uint32_t fused;
+  // single graph: every vertex's community when the pass began; nullptr
+  // (batched form, lv_config.modularity_full): every sweep is a full one
+  uint32_t* comm_start;
 };
 
 // How one bucket step of a pass treats the community state.  fused = 0:
@@ -336,6 +344,9 @@ struct StepIO {
   int parity;
   int prev_lo;
   int prev_hi;
+  // the pass's first step: records every vertex's community in
+  // PassDesc::comm_start (the incremental modularity sweep reads it)
+  int pass_start;
 };
 
 // rowid[j] = the row holding entry j of a CSR of n rows and nnz entries.

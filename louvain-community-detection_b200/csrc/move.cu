@@ -440,6 +440,19 @@ __device__ __forceinline__ VertexRow fetch_vertex(const LevelView& L,
   return r;
 }
 
+// The pass's first step records every vertex's community (both copies of
+// the state are equal then) for the incremental modularity sweep.
+__device__ __forceinline__ void record_pass_start(const PassDesc* __restrict__ D,
+                                                  const LevelView& L, const StepIO& io,
+                                                  uint32_t bid, uint32_t nblk) {
+  uint32_t* cs = D->comm_start;
+  if (!io.pass_start || !cs) return;
+  for (uint32_t v = bid * blockDim.x + threadIdx.x; v < L.n; v += nblk * blockDim.x) {
+    const uint32_t c = L.comm[v];
+    if (cs[v] != c) cs[v] = c;
+  }
+}
+
 // Records a decision: the proposal (read by the next step's re-apply and
 // by the separate apply launch) and, in a fused step, the move itself.
 __device__ __forceinline__ void record_decision(const PassDesc* __restrict__ D,
@@ -466,6 +479,7 @@ __device__ __forceinline__ void small_body(const PassDesc* __restrict__ D, int c
   using K = typename BestOf<PREC>::T;
   const LevelView L = step_view(D, io);
   reapply_prev_step(D, io, bid, nblk);
+  record_pass_start(D, L, io, bid, nblk);
   const uint32_t s0 = D->A.P.cls_start[cls];
   const uint32_t* __restrict__ verts = D->A.order + s0;
   uint32_t* __restrict__ prop = D->prop + s0;
@@ -697,6 +711,7 @@ __device__ __forceinline__ void warp_body(const PassDesc* __restrict__ D, int cl
   constexpr int RULE = ModeOf<MODE>::kRule, PREC = ModeOf<MODE>::kPrec;
   const LevelView L = step_view(D, io);
   reapply_prev_step(D, io, bid, nblk);
+  record_pass_start(D, L, io, bid, nblk);
   const uint32_t s0 = D->A.P.cls_start[cls];
   const uint32_t* __restrict__ verts = D->A.order + s0;
   uint32_t* __restrict__ prop = D->prop + s0;
@@ -784,8 +799,9 @@ __device__ __forceinline__ void warp_body(const PassDesc* __restrict__ D, int cl
       vals[slot] += hot;
     }
     __syncwarp();
-    // (a scan of the row's table range: owner evaluation as in the block
-    // kernel made this kernel spill and run 37% slower at R-MAT 24)
+    // a scan of the row's table range: owner evaluation as in the block
+    // kernel made this kernel spill and run 37% slower at R-MAT 24, and a
+    // list of the claimed slots (a ballot per wave) 38% slower
     auto best = scan_table_and_clear<PREC>(L, g, keys, vals, tv, lane, 32);
     best = group_max<32>(best);
     if (RULE == LV_RULE_CUDA_I) own = group_sum<32>(own);
@@ -891,6 +907,7 @@ __device__ __forceinline__ void block_body(const PassDesc* __restrict__ D, int c
   using K = typename BestOf<PREC>::T;
   const LevelView L = step_view(D, io);
   reapply_prev_step(D, io, bid, nblk);
+  record_pass_start(D, L, io, bid, nblk);
   const uint32_t s0 = D->A.P.cls_start[cls];
   const uint32_t* __restrict__ verts = D->A.order + s0;
   uint32_t* __restrict__ prop = D->prop + s0;
@@ -1035,6 +1052,7 @@ __device__ __forceinline__ void split_body(const PassDesc* __restrict__ D, uint3
   constexpr int RULE = ModeOf<MODE>::kRule;
   const LevelView L = step_view(D, io);
   reapply_prev_step(D, io, bid, nblk);
+  record_pass_start(D, L, io, bid, nblk);
   const uint32_t* __restrict__ hubs = D->A.order + D->A.P.cls_start[8];
   const HubArena H = D->H;
   const uint32_t nblocks = D->A.P.hub_blocks;
@@ -1288,6 +1306,7 @@ __global__ void __launch_bounds__(kThreads, kSweepPerSM)
 struct RowSumOp {
   static constexpr GraphField kField = &GraphState::m_acc;
   static constexpr bool kAsq = false;
+  __device__ bool row(const LevelView&, uint32_t) const { return true; }
   __device__ uint32_t ctx(const LevelView&, uint32_t) const { return 0; }
   __device__ double edge(const LevelView&, uint32_t, uint32_t, float w) const {
     return (double)w;
@@ -1313,6 +1332,7 @@ struct IntraOp {
   // batched form: the vertex's community total squared (community ids are
   // vertex ids), so an active graph's sum of a_c^2 comes with its rows
   static constexpr bool kAsq = true;
+  __device__ bool row(const LevelView&, uint32_t) const { return true; }
   __device__ uint32_t ctx(const LevelView& L, uint32_t v) const {
     return L.comm[v];
   }
@@ -1328,6 +1348,38 @@ struct IntraOp {
                       double sum, double& part) const {
     part += sum;
     if (L.gid && sum != 0.0) atomicAdd(&L.gs[L.gid[v]].intra_acc, sum);
+  }
+};
+
+// Change of the intra-community weight over a pass (single graph): only the
+// rows of vertices whose community at the pass's start (cs) differs from
+// the current one are swept.  Entry (v, u) changes the sum by
+// w ([c(u) == c(v)] - [cs(u) == cs(v)]); every edge is stored in both of
+// its rows with the same weight, so an entry whose other end did not move
+// (its row is not swept) counts for both copies.  FP64 sums of FP32
+// weights are exact, so the updated sum equals a full sweep's.
+struct DeltaIntraOp {
+  const uint32_t* cs;
+  static constexpr GraphField kField = &GraphState::intra_acc;
+  static constexpr bool kAsq = false;
+  __device__ bool row(const LevelView& L, uint32_t v) const { return cs[v] != L.comm[v]; }
+  __device__ uint2 ctx(const LevelView& L, uint32_t v) const {
+    return make_uint2(cs[v], L.comm[v]);
+  }
+  __device__ double edge(const LevelView& L, uint2 c, uint32_t u, float w) const {
+    const uint32_t csu = cs[u], cu = L.comm[u];
+    const bool was = csu == c.x, now = cu == c.y;
+    if (was == now) return 0.0;
+    const double x = (csu != cu) ? (double)w : 2.0 * (double)w;
+    return now ? x : -x;
+  }
+  __device__ double vertex(const LevelView&, uint32_t, double sum, double& part) const {
+    part += sum;
+    return sum;
+  }
+  __device__ void hub(const LevelView&, const DispatchArgs&, uint32_t, uint32_t, double sum,
+                      double& part) const {
+    part += sum;
   }
 };
 
@@ -1365,8 +1417,8 @@ __device__ __forceinline__ void unit_small(const LevelView& L,
     v = A.order[A.P.cls_start[cls] + idx];
     const uint64_t s = L.off[v];
     const uint32_t d = (uint32_t)(L.off[v + 1] - s);
-    if (gl < (int)d) {
-      const uint32_t c = op.ctx(L, v);
+    if (gl < (int)d && op.row(L, v)) {
+      const auto c = op.ctx(L, v);
       x = op.edge(L, c, L.col[s + gl], L.w[s + gl]);
     }
   }
@@ -1393,9 +1445,10 @@ __device__ __forceinline__ void unit_warp(const LevelView& L,
   const uint32_t idx = unit * kWarps + wib;
   if (idx >= cnt) return;  // warp-uniform
   const uint32_t v = A.order[A.P.cls_start[cls] + idx];
+  if (!op.row(L, v)) return;  // warp-uniform
   const uint64_t s = L.off[v];
   const uint32_t d = (uint32_t)(L.off[v + 1] - s);
-  const uint32_t c = op.ctx(L, v);
+  const auto c = op.ctx(L, v);
   double x = 0.0;
   for (uint32_t j = lane; j < d; j += 32) x += op.edge(L, c, L.col[s + j], L.w[s + j]);
   x = group_sum<32>(x);
@@ -1413,9 +1466,10 @@ __device__ __forceinline__ void unit_block(const LevelView& L,
   const uint32_t idx = unit;
   if (idx >= class_count(A, 7)) return;  // block-uniform
   const uint32_t v = A.order[A.P.cls_start[7] + idx];
+  if (!op.row(L, v)) return;  // block-uniform
   const uint64_t s = L.off[v];
   const uint32_t d = (uint32_t)(L.off[v + 1] - s);
-  const uint32_t c = op.ctx(L, v);
+  const auto c = op.ctx(L, v);
   double x = 0.0;
   for (uint32_t j = threadIdx.x; j < d; j += kThreads)
     x += op.edge(L, c, L.col[s + j], L.w[s + j]);
@@ -1436,10 +1490,11 @@ __device__ __forceinline__ void unit_hub(const LevelView& L,
   const uint32_t v = A.order[A.P.cls_start[8] + hi];
   // batched pass loop: a finished graph's hubs need no sweep (block-uniform)
   if (A.act_cnt && !L.gs[L.gid[v]].active) return;
+  if (!op.row(L, v)) return;  // block-uniform
   const uint64_t s = L.off[v];
   const uint64_t d = L.off[v + 1] - s;
   const uint64_t lo = (uint64_t)ch * kHubChunk, end = min(d, lo + kHubChunk);
-  const uint32_t c = op.ctx(L, v);
+  const auto c = op.ctx(L, v);
   double x = 0.0;
   for (uint64_t j = lo + threadIdx.x; j < end; j += kThreads)
     x += op.edge(L, c, L.col[s + j], L.w[s + j]);
@@ -1642,12 +1697,22 @@ __device__ __forceinline__ double intra_sweep(const LevelView& L, const uint32_t
 // Modularity of the current partition (modularity.cu:400-436): the
 // intra-community weight (over the entries with row ids, else over the
 // class lists) and the sum of squared community totals.
+// cs (single graph, pass sweeps): every vertex's community when the pass
+// began.  With it the sweep also counts the entries of the vertices that
+// moved, and when the previous pass moved fewer than a quarter of the
+// entries it updates the previous intra-community weight from the moved
+// rows only (DeltaIntraOp) instead of sweeping every entry.
 __device__ __forceinline__ void modularity_body(const LevelView& L, const DispatchArgs& A,
                                                 const PassControl& ctl,
-                                                const uint32_t* rowid, uint64_t nnz) {
+                                                const uint32_t* rowid, uint64_t nnz,
+                                                const uint32_t* cs = nullptr) {
   __shared__ double red[kWarps];
   double part = 0.0;
-  if (rowid && !L.gid) {
+  // read before this block publishes: the last block rewrites it
+  const bool inc = cs && !L.gid && *(volatile uint32_t*)&L.sc->inc_next != 0u;
+  if (inc) {
+    dispatch_units(L, A, DeltaIntraOp{cs}, part, red);
+  } else if (rowid && !L.gid) {
     part = intra_sweep(L, rowid, nnz, blockIdx.x, gridDim.x);
   } else {
     dispatch_units(L, A, IntraOp{}, part, red);
@@ -1656,17 +1721,27 @@ __device__ __forceinline__ void modularity_body(const LevelView& L, const Dispat
   const uint32_t c0 = blockIdx.x * chunk;
   const uint32_t c1 = min(L.n, c0 + chunk);
   double asq = 0.0;
+  unsigned long long moved = 0ull;
   if (!L.gid) {  // the batched form summed a_c^2 with the rows above
     for (uint32_t c = c0 + threadIdx.x; c < c1; c += kThreads) {
       const double a = L.tot[c];
       asq += a * a;
+      if (cs && cs[c] != L.comm[c]) moved += L.off[c + 1] - L.off[c];
     }
+  }
+  if (cs) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) moved += __shfl_xor_sync(kFull, moved, o);
+    if ((threadIdx.x & 31) == 0 && moved) atomicAdd(&L.sc->moved_acc, moved);
   }
   if (!publish_and_check_last(part, asq, A, L.sc, red)) return;
   double intra, sq;
   sum_partials(A, red, intra, sq);
   if (!L.gid) {
     if (threadIdx.x == 0) {
+      if (inc) intra += L.sc->intra;  // the pass's change added to the last sweep's sum
+      const unsigned long long mv = cs ? atomicExch(&L.sc->moved_acc, 0ull) : 0ull;
+      L.sc->inc_next = (cs && mv * 4ull < nnz) ? 1u : 0u;
       const double m = L.sc->m64;
       const double q = (m > 0.0) ? (intra / (2.0 * m)) - (sq / (4.0 * m * m)) : 0.0;
       L.sc->intra = intra;
@@ -1742,7 +1817,7 @@ __global__ void __launch_bounds__(kThreads, kModPerSM)
   // go into the other copy, which leaves both equal for the next pass
   const LevelView L = step_view(D, io);
   reapply_prev_step(D, io, blockIdx.x, gridDim.x);
-  modularity_body(L, D->A, ctl, D->rowid, D->nnz);
+  modularity_body(L, D->A, ctl, D->rowid, D->nnz, D->comm_start);
 }
 
 __global__ void pass_control_init_kernel(const PassDesc* __restrict__ D, PassControl ctl) {
@@ -1757,6 +1832,8 @@ __global__ void pass_control_init_kernel(const PassDesc* __restrict__ D, PassCon
     sc->q_before = sc->q;
     sc->q_start = sc->q;
     sc->any_active = 1u;
+    sc->moved_acc = 0ull;
+    sc->inc_next = 0u;  // the first pass of a level sweeps every entry
     sc->act_changed = 1u;  // the first pass builds the active lists
     // single graph: a level without edge weight runs no pass (its gains
     // would divide by m = 0); the host reads m after the level
@@ -2360,6 +2437,7 @@ static cudaError_t move_bucket_impl(const PassDesc* D, int bucket, const uint8_t
   // the hubs' own
   StepIO later = io;
   later.prev_lo = later.prev_hi = 0;
+  later.pass_start = 0;
   (count_launches(1), hub_split_kernel<MODE><<<sm_count() * kSplitPerSM, kThreads, 0, st>>>(D, io));
   (count_launches(1), hub_merge_kernel<MODE><<<sm_count() * kMergePerSM, kThreads, kHubPartSmem,
                                                st>>>(D, later));

@@ -46,6 +46,7 @@ class Config(ctypes.Structure):
         ("level_kernel", ctypes.c_int),
         ("contract_sort", ctypes.c_int),
         ("apply_launch", ctypes.c_int),
+        ("modularity_full", ctypes.c_int),
     ]
 
 
@@ -371,7 +372,8 @@ class Engine:
     def __init__(self, device: int = 0, rule: str = "py", max_passes: int = 0,
                  max_levels: int = 0, use_graphs: bool = True, stream: int = 0,
                  gain: str = "fp32", level_kernel: bool = False,
-                 contract_sort: bool = False, apply_launch: bool = False):
+                 contract_sort: bool = False, apply_launch: bool = False,
+                 modularity_full: bool = False):
         cfg = Config()
         lib().lv_config_default(ctypes.byref(cfg))
         cfg.device = device
@@ -380,6 +382,7 @@ class Engine:
         cfg.level_kernel = int(level_kernel)
         cfg.contract_sort = int(contract_sort)
         cfg.apply_launch = int(apply_launch)
+        cfg.modularity_full = int(modularity_full)
         cfg.max_passes = max_passes
         cfg.max_levels = max_levels
         cfg.use_graphs = int(use_graphs)

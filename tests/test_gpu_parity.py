@@ -276,6 +276,36 @@ def test_fused_steps_equal_apply_launches(rule, gain):
             assert [l["q_end"] for l in r.levels] == [l["q_end"] for l in res[0].levels]
 
 
+@pytest.mark.parametrize("rule", ["py", "cuda"])
+@pytest.mark.parametrize("gain", ["fp32", "fp64"])
+def test_incremental_modularity_equals_full_sweeps(rule, gain):
+    """Pass sweeps that update the intra-community weight from the moved
+    vertices' rows (the default, after passes that moved under a quarter of
+    the entries) give the same runs as a full sweep every pass: partition,
+    passes and every level's Q, with the level graph and the host loop, on
+    unit weights, U(0.1, 1) weights and R-MAT graphs with hubs.  The
+    update runs on levels of at least 2^23 entries (R-MAT 19: 15.7 M at
+    level 0); the small graphs check that the other levels keep full sweeps."""
+    cases = [lvgen.rmat(19, seed=3),
+             lvgen.planted_powerlaw(n=60000, target_edges=200000, seed=5),
+             lvgen.planted_powerlaw(n=40000, target_edges=150000, seed=9, unit=False),
+             lvgen.rmat(15, edge_factor=16, seed=2)]
+    for n, s, d, w in cases:
+        off, col, ww = lvgen.csr_from_edges(n, s, d, w)
+        g = lvb200.Graph.from_csr(n, off, col, ww)
+        res = []
+        for full, ug in ((True, True), (False, True), (False, False)):
+            with lvb200.Engine(rule=rule, gain=gain, modularity_full=full, use_graphs=ug) as e:
+                res.append(e.run(g, 1e-6))
+        assert sum(l["passes"] for l in res[0].levels) > 2 * len(res[0].levels)
+        for r in res[1:]:
+            assert np.array_equal(r.assignment, res[0].assignment)
+            assert [l["passes"] for l in r.levels] == [l["passes"] for l in res[0].levels]
+            assert abs(r.modularity - res[0].modularity) < 1e-12
+            for a, b in zip(r.levels, res[0].levels):
+                assert abs(a["q_end"] - b["q_end"]) < 1e-12
+
+
 def test_fused_steps_level_state():
     """After a fused pass loop the level's state (the first copy, which the
     contraction and the level-state reads use) equals the one the separate
