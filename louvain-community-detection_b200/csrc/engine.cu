@@ -891,6 +891,19 @@ lv_status issue_pass(lv_engine* E, const PassControl* ctl);
 
 constexpr uint64_t kIncrementalMinEntries = 1ull << 23;
 
+// The kernel of bucket b on this level: the tuned (or default) variant,
+// except that a warp-per-vertex bucket with no more vertices than the block
+// kernel has resident blocks gives each vertex a whole block -- there the
+// launch lasts as long as one vertex's chain, which a block shortens
+// (single graph; a union keeps its tuning).
+uint8_t effective_variant(const lv_engine* E, int b) {
+  const uint8_t v = E->tune[b];
+  if (E->batch || b < 1 || b > 6) return v;
+  if (v != KV_WARP128 && v != KV_WARP512) return v;
+  const uint32_t cnt = E->plan.cls_start[b + 1] - E->plan.cls_start[b];
+  return (cnt > 0 && cnt <= move_block_resident()) ? (uint8_t)KV_BLOCK : v;
+}
+
 // Writes the current level into the device pass descriptor (every pass
 // kernel reads it at launch).
 lv_status upload_desc(lv_engine* E, float min_gain) {
@@ -913,7 +926,7 @@ lv_status upload_desc(lv_engine* E, float min_gain) {
   d.nnz = E->e;
   d.min_gain = (double)min_gain;
   d.max_passes = E->cfg.max_passes;
-  for (int b = 0; b < 8; b++) d.tune[b] = E->tune[b];
+  for (int b = 0; b < 8; b++) d.tune[b] = effective_variant(E, b);
   d.loop = E->loop_state;
   d.fused = E->cfg.apply_launch ? 0u : 1u;
   // incremental sweeps only where a sweep is bound by DRAM: below 2^23
@@ -951,7 +964,7 @@ uint64_t level_key(const lv_engine* E) {
   uint64_t k = (E->batch ? 1u : 0u) | ((uint64_t)(E->cfg.rule == LV_RULE_CUDA) << 1) |
                ((uint64_t)(E->cfg.gain == LV_GAIN_FP64) << 2) |
                ((uint64_t)(E->cfg.apply_launch != 0) << 3);
-  for (int b = 1; b <= kBuckets; b++) k |= (uint64_t)E->tune[b] << (4 * b);
+  for (int b = 1; b <= kBuckets; b++) k |= (uint64_t)effective_variant(E, b) << (4 * b);
   for (int c = 1; c <= 8; c++) k |= (uint64_t)class_nonempty(E, c) << (39 + c);
   return k;
 }
@@ -1114,7 +1127,9 @@ lv_status issue_pass(lv_engine* E, const PassControl* ctl) {
     io.parity = fused ? (step & 1) : 0;
     if (class_nonempty(E, b)) {
       t0 = prof_begin(E);
-      CU(launch_move_bucket(D, b, rule, E->tune, st, io));
+      uint8_t kv[8];
+      for (int i = 0; i < 8; i++) kv[i] = effective_variant(E, i);
+      CU(launch_move_bucket(D, b, rule, kv, st, io));
       prof_end(E, t0, K_MOVE1 + b - 1, (double)E->class_deg[b] * 12.0 + v7 * 32.0);
       io.prev_lo = io.prev_hi = 0;  // re-applied by this launch
       io.pass_start = 0;

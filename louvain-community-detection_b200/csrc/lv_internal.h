@@ -450,6 +450,8 @@ cudaError_t launch_modularity_of(const LevelView& L, const uint32_t* part,
 cudaError_t launch_bucket_ids(const uint64_t* off, uint32_t n, uint8_t* out,
                               cudaStream_t st);
 unsigned dispatch_grid(const DispatchPlan& P);
+// Blocks of the block-per-vertex move kernel resident on the device at once.
+unsigned move_block_resident();
 unsigned sm_count_cached();
 // Opts kernels with more than 48 KB of shared memory in (once per device).
 cudaError_t configure_kernels();

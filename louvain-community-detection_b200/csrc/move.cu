@@ -61,7 +61,7 @@ constexpr int kWarp128PerSM = 5;   // 48 registers, 12 KB tables
 constexpr int kWarp512PerSM = 4;   // 64 registers, 48 KB tables
 constexpr int kBlockPerSM = 3;     // 80 registers, 48 KB table
 constexpr int kSplitPerSM = 4;
-constexpr int kMergePerSM = 3;
+constexpr int kMergePerSM = 3;     // 80 registers (4 per SM at 64: 9% slower on R-MAT 24)
 constexpr int kSweepPerSM = 8;     // apply
 constexpr int kModPerSM = 6;       // modularity sweep, 40 registers
 static_assert(class_per_unit(1) * 4 == kThreads && class_per_unit(5) == kWarps,
@@ -2385,6 +2385,7 @@ cudaError_t launch_modularity_pass(const PassDesc* D, const PassControl* ctl, cu
 }
 
 unsigned pass_dispatch_grid() { return sm_count() * kModPerSM; }
+unsigned move_block_resident() { return sm_count() * kBlockPerSM; }
 
 // One launch of a move kernel variant over class `cls`.
 template <int MODE>
