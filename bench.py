@@ -272,7 +272,7 @@ def batched_measure(stream, count: int, steps: int = 2, apply_launch: bool = Fal
 
 
 def hbm_scale_measure(stream, scale: int, steps: int = 2, oracle_check: bool = True,
-                      apply_launch: bool = False):
+                      apply_launch: bool = False, use_graphs: bool = True):
     """The plain engine at HBM scale: R-MAT (a, b, c, d = 0.57, 0.19, 0.19,
     0.05, edge factor 16, duplicates merged, unit weights) generated on the
     device; edges/s per pass over `steps` device-timed runs after one
@@ -290,7 +290,8 @@ def hbm_scale_measure(stream, scale: int, steps: int = 2, oracle_check: bool = T
            "n_entries": nnz, "abcd": [0.57, 0.19, 0.19, 0.05], "weights": "unit FP32",
            "seed": 0}
     with torch.cuda.stream(stream):
-        eng = lvb200.Engine(stream=stream.cuda_stream, apply_launch=apply_launch)
+        eng = lvb200.Engine(stream=stream.cuda_stream, apply_launch=apply_launch,
+                            use_graphs=use_graphs)
         eng.load_device(n, nnz, off.data_ptr(), col.data_ptr(), w.data_ptr())
         res["tuning"] = {str(b): k for b, (k, _) in eng.autotune().items()}
 
@@ -682,7 +683,7 @@ def run_engine(args, rank, world):
                                 min(args.serve_distinct, args.serve_requests))
     if world == 1 and args.hbm_scale > 0:
         hbm = hbm_scale_measure(stream, args.hbm_scale, oracle_check=not args.no_oracle_check,
-                                apply_launch=args.apply_launch)
+                                apply_launch=args.apply_launch, use_graphs=not args.no_graphs)
     if rank != 0:
         return
     # roofline of the dominant kernel group
@@ -748,8 +749,8 @@ def main():
                     help="keep the default move kernel of every bucket (no lv_autotune)")
     ap.add_argument("--no-graphs", action="store_true",
                     help="run each level's pass loop from the host instead of a CUDA graph "
-                         "WHILE node (same kernels; ncu cannot profile kernels inside "
-                         "graphs with conditional nodes)")
+                         "WHILE node, in the headline and HBM-scale legs (same kernels; ncu "
+                         "cannot profile kernels inside graphs with conditional nodes)")
     ap.add_argument("--hbm-scale", type=int, default=24,
                     help="R-MAT scale of the HBM-scale plain-engine measurement (0: skip)")
     ap.add_argument("--apply-launch", action="store_true",
