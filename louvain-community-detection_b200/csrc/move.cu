@@ -355,6 +355,30 @@ __device__ __forceinline__ uint32_t table_claim(uint32_t* keys, uint32_t mask, u
   return 0;
 }
 
+// Adds each lane's (key, w) to a shared table, the lanes holding the same
+// key as the wave's first entry summed with shuffles into one atomic: in
+// late passes a hub's neighbours crowd into a few communities, and
+// hundreds of threads looping on one slot's FP64 compare-and-swap made the
+// merge slower pass after pass.  A wave of distinct keys pays two ballots.
+__device__ __forceinline__ void table_add_wave(uint32_t* keys, double* vals, uint32_t mask,
+                                               bool has, uint32_t key, double w,
+                                               LevelScalars* sc) {
+  const int lane = threadIdx.x & 31;
+  const unsigned hm = __ballot_sync(0xffffffffu, has);
+  if (!hm) return;  // warp-uniform
+  const int lead = __ffs(hm) - 1;
+  const uint32_t kl = __shfl_sync(0xffffffffu, key, lead);
+  const unsigned m = __ballot_sync(0xffffffffu, has && key == kl);
+  if (__popc(m) > 1) {  // warp-uniform
+    double x = (m >> lane & 1u) ? w : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == lead) atomicAdd(&vals[table_insert(keys, mask, kl, sc)], x);
+    if (m >> lane & 1u) return;
+  }
+  if (has) atomicAdd(&vals[table_insert(keys, mask, key, sc)], w);
+}
+
 // ---------------------------------------------------------------------------
 // Community state of a bucket step (StepIO).  step_view's comm / comm_sz /
 // tot are the copy the step reads; a fused step writes its moves into the
@@ -1201,7 +1225,7 @@ __device__ __forceinline__ void merge_body(const PassDesc* __restrict__ D, uint3
           c = cw.x;
           w = __uint_as_float(cw.y);
         }
-        if (has) atomicAdd(&vals[table_insert(keys, T - 1, c, L.sc)], (double)w);
+        table_add_wave(keys, vals, T - 1, has, c, (double)w, L.sc);
       }
       __syncthreads();  // seg_a / seg_pre are refilled
     }
