@@ -29,7 +29,7 @@
 //     atomicCAS winners) only the set of (neighbour, weight) pairs of a row
 //     is defined.
 #include <algorithm>
-#include <vector>
+#include <cstring>
 
 #include "lv_internal.h"
 
@@ -174,11 +174,82 @@ __global__ void comm_deg_kernel(const uint32_t* comm_list, uint32_t n_upper,
   }
 }
 
-__global__ void gather_u64_kernel(const uint64_t* src, const uint32_t* idx, uint32_t n,
-                                  uint64_t* out) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += gridDim.x * blockDim.x)
-    out[i] = src[idx[i]];
+// Class-G plan totals, after the class sizes in counts[0..7] so one copy
+// brings both to the host: [10] blocks (kMergeChunk entries each), [12..13]
+// table slots (u64).  counts[8..9] hold the new entry count later.
+constexpr int kGTotals = 10;
+
+// The class-G plan on the device (one block): every multi-block community
+// (counts[7] of them, listed after the warp and block classes in comm_cls)
+// gets a global table of a power of two >= 2 min(entries, new n) + 1 slots
+// and ceil(entries / kMergeChunk) blocks; table offsets and first blocks
+// are exclusive scans.  `cap` is the capacity of the per-community and
+// per-block arrays; a level past it writes no plan and leaves the totals
+// at ~0 (the host reports it).
+__global__ void __launch_bounds__(1024)
+    g_plan_kernel(const uint64_t* __restrict__ comm_deg, const uint32_t* __restrict__ comm_cls,
+                  uint32_t* counts, uint64_t cap, uint64_t* tab_off, uint32_t* tab_size,
+                  uint32_t* blk_first) {
+  __shared__ unsigned long long sh[33];
+  const uint32_t new_n = counts[0];
+  const uint32_t* list = comm_cls + counts[4] + counts[5] + counts[6];
+  const uint32_t cnt = counts[7];
+  uint64_t* tot64 = reinterpret_cast<uint64_t*>(counts + 12);
+  unsigned long long c_slots = 0, c_blk = 0, t;
+  bool over = cnt > cap;
+  for (uint32_t base = 0; !over && base < cnt; base += blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    unsigned long long T = 0, nch = 0;
+    if (i < cnt) {
+      const unsigned long long d = comm_deg[list[i]];
+      const unsigned long long distinct = d < new_n ? d : new_n;
+      T = 1;
+      while (T < 2 * distinct + 1) T <<= 1;
+      nch = (d + kMergeChunk - 1) / kMergeChunk;
+    }
+    const unsigned long long x_s = block_exclusive_scan(T, sh, &t);
+    const unsigned long long s_s = c_slots;
+    c_slots += t;
+    const unsigned long long x_b = block_exclusive_scan(nch, sh, &t);
+    const unsigned long long s_b = c_blk;
+    c_blk += t;
+    if (i < cnt) {
+      tab_off[i] = s_s + x_s;
+      tab_size[i] = (uint32_t)T;
+      blk_first[i] = (uint32_t)(s_b + x_b);
+    }
+    over = c_blk > cap;  // uniform across the block
+  }
+  if (threadIdx.x == 0) {
+    if (over) {
+      counts[kGTotals] = ~0u;
+      tot64[0] = ~0ull;
+    } else {
+      blk_first[cnt] = (uint32_t)c_blk;
+      counts[kGTotals] = (uint32_t)c_blk;
+      tot64[0] = c_slots;
+    }
+  }
+}
+
+// The class-G block map (a warp per community): block -> community index,
+// chunk, chunks of the community, packed as blk_comm[b], blk_chunk[b] and
+// blk_chunk[nblk + b].
+__global__ void g_fill_kernel(const uint32_t* __restrict__ counts,
+                              const uint32_t* __restrict__ blk_first, uint32_t* blk_comm,
+                              uint32_t* blk_chunk) {
+  const uint32_t cnt = counts[7], nblk = counts[kGTotals];
+  if (nblk == ~0u) return;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < cnt; i += warps) {
+    const uint32_t b0 = blk_first[i], nch = blk_first[i + 1] - b0;
+    for (uint32_t ch = lane; ch < nch; ch += 32) {
+      blk_comm[b0 + ch] = i;
+      blk_chunk[b0 + ch] = ch;
+      blk_chunk[nblk + b0 + ch] = nch;
+    }
+  }
 }
 
 // Class W: one warp per community, flattened member edges, 256-slot table.
@@ -723,12 +794,6 @@ unsigned gridcap(uint64_t work, unsigned per_sm) {
   return (unsigned)(work < cap ? work : cap);
 }
 
-uint64_t next_pow2(uint64_t x) {
-  uint64_t p = 1;
-  while (p < x) p <<= 1;
-  return p;
-}
-
 }  // namespace
 
 cudaError_t configure_contract_kernels() {
@@ -753,7 +818,6 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
                            cudaError_t (*grow)(void*, size_t, size_t),
                            void* grow_ctx, bool defer_total) {
   const uint32_t n = L.n;
-  (void)nnz;
   uint32_t* h_counts = B.host_counts;
 
   const unsigned g1 = gridcap((n + 255) / 256, 8);
@@ -776,13 +840,41 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
   LV_TRY(cudaGetLastError());
   LV_TRY(partition_by_size4(B.comm_deg, n, B.counts + 0, kMergeWarpMax, kMergeMidMax,
                             kMergeBlockMax, B.comm_cls, B.counts + 4, B.tmp, S, st));
-  LV_TRY(cudaMemcpyAsync(h_counts, B.counts, 8 * sizeof(uint32_t),
+  // class-G plan on the device, its totals copied with the class sizes.
+  // Its arrays are sized for the most the level can need: a class-G
+  // community has more than kMergeBlockMax entries and its blocks cover
+  // its entries in kMergeChunk pieces, of the level's nnz in all.
+  auto plan_g = [&](uint64_t cap) -> cudaError_t {
+    if (cap > B.g_cap) LV_TRY(grow(grow_ctx, 0, cap));
+    (count_launches(1), g_plan_kernel<<<1, 1024, 0, st>>>(B.comm_deg, B.comm_cls, B.counts,
+                                                          B.g_cap, B.g_tab_off, B.g_tab_size,
+                                                          B.g_blk_first));
+    LV_TRY(cudaGetLastError());
+    (count_launches(1), g_fill_kernel<<<gridcap(((uint64_t)nnz / (kMergeBlockMax + 1) + 8) / 8, 8),
+                                        kThreads, 0, st>>>(B.counts, B.g_blk_first, B.g_blk_comm,
+                                                           B.g_blk_chunk));
+    return cudaGetLastError();
+  };
+  const uint64_t g_bound = nnz / (kMergeBlockMax + 1) + nnz / kMergeChunk + 1;
+  const bool g_planned = nnz > kMergeBlockMax;
+  if (g_planned) LV_TRY(plan_g(g_bound));
+  LV_TRY(cudaMemcpyAsync(h_counts, B.counts, 16 * sizeof(uint32_t),
                          cudaMemcpyDeviceToHost, st));
   LV_TRY(counted_sync(st));
   const uint32_t new_n = h_counts[0];
   const uint32_t cntW = h_counts[4], cntM = h_counts[5], cntB2 = h_counts[6];
   const uint32_t cntB = cntM + cntB2;  // both block classes
   const uint32_t cntG = h_counts[7];
+  // the bound holds when nnz is the level's entry count; otherwise plan
+  // again with twice the room until the plan fits
+  for (int tries = 0; cntG && (!g_planned || h_counts[kGTotals] == ~0u); tries++) {
+    if (tries == 40) return cudaErrorInvalidValue;
+    LV_TRY(plan_g(std::max<uint64_t>(2 * (uint64_t)B.g_cap, (uint64_t)cntG + 1)));
+    LV_TRY(cudaMemcpyAsync(h_counts, B.counts, 16 * sizeof(uint32_t),
+                           cudaMemcpyDeviceToHost, st));
+    LV_TRY(counted_sync(st));
+    if (h_counts[kGTotals] != ~0u) break;
+  }
 
   Ctx C;
   C.off = L.off;
@@ -815,51 +907,14 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
     LV_TRY(cudaGetLastError());
   }
   if (cntG) {
-    // plan class-G tables and blocks on the host (few, very large rows)
-    if (cntG > B.g_cap) LV_TRY(grow(grow_ctx, 0, cntG));
-    (count_launches(1), gather_u64_kernel<<<gridcap((cntG + 255) / 256, 8), 256, 0, st>>>(
-        B.comm_deg, B.comm_cls + cntW + cntB, cntG, B.g_tab_off));
-    LV_TRY(cudaGetLastError());
-    std::vector<uint64_t> gdeg(cntG);
-    LV_TRY(cudaMemcpyAsync(gdeg.data(), B.g_tab_off, cntG * sizeof(uint64_t),
-                           cudaMemcpyDeviceToHost, st));
-    LV_TRY(counted_sync(st));
-    std::vector<uint64_t> tab_off(cntG);
-    std::vector<uint32_t> tab_size(cntG);
-    std::vector<uint32_t> blk_comm, blk_chunk, blk_nch;
+    // class-G tables and blocks as planned on the device (few, very large
+    // rows); only the table's size is needed here
+    const size_t nblk = h_counts[kGTotals];
     uint64_t slots = 0;
-    for (uint32_t i = 0; i < cntG; i++) {
-      const uint64_t d = gdeg[i];
-      const uint64_t distinct = std::min<uint64_t>(d, new_n);
-      const uint64_t T = next_pow2(2 * distinct + 1);
-      tab_off[i] = slots;
-      tab_size[i] = (uint32_t)T;
-      slots += T;
-      const uint32_t nch = (uint32_t)((d + kMergeChunk - 1) / kMergeChunk);
-      for (uint32_t ch = 0; ch < nch; ch++) {
-        blk_comm.push_back(i);
-        blk_chunk.push_back(ch);
-        blk_nch.push_back(nch);
-      }
-    }
-    const size_t nblk = blk_comm.size();
-    if (slots > B.table_cap || std::max<size_t>(nblk, cntG) > B.g_cap) {
-      LV_TRY(grow(grow_ctx, slots, std::max<size_t>(nblk, cntG)));
-    }
+    memcpy(&slots, h_counts + kGTotals + 2, sizeof(uint64_t));
+    if (slots > B.table_cap) LV_TRY(grow(grow_ctx, slots, 0));
     LV_TRY(cudaMemsetAsync(B.keys, 0xFF, slots * sizeof(uint32_t), st));
     LV_TRY(cudaMemsetAsync(B.vals, 0, slots * sizeof(double), st));
-    // block map packed as [comm | chunk | nchunks] in g_blk_comm/g_blk_chunk
-    LV_TRY(cudaMemcpyAsync(B.g_tab_off, tab_off.data(), cntG * sizeof(uint64_t),
-                           cudaMemcpyHostToDevice, st));
-    LV_TRY(cudaMemcpyAsync(B.g_tab_size, tab_size.data(), cntG * sizeof(uint32_t),
-                           cudaMemcpyHostToDevice, st));
-    std::vector<uint32_t> packed(2 * nblk);
-    std::copy(blk_chunk.begin(), blk_chunk.end(), packed.begin());
-    std::copy(blk_nch.begin(), blk_nch.end(), packed.begin() + nblk);
-    LV_TRY(cudaMemcpyAsync(B.g_blk_comm, blk_comm.data(), nblk * sizeof(uint32_t),
-                           cudaMemcpyHostToDevice, st));
-    LV_TRY(cudaMemcpyAsync(B.g_blk_chunk, packed.data(), 2 * nblk * sizeof(uint32_t),
-                           cudaMemcpyHostToDevice, st));
     GArgs G;
     G.list = B.comm_cls + cntW + cntB;
     G.tab_off = B.g_tab_off;
@@ -874,8 +929,6 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
     LV_TRY(cudaGetLastError());
     (count_launches(1), merge_global_emit_kernel<<<gridcap(nblk, 8), kThreads, 0, st>>>(C, G));
     LV_TRY(cudaGetLastError());
-    // host vectors must outlive the async copies
-    LV_TRY(counted_sync(st));
   }
   // new offsets: exclusive scan of the n'+1 counts (last one is 0)
   uint64_t* d_total = reinterpret_cast<uint64_t*>(B.counts + 8);

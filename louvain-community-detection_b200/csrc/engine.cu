@@ -102,12 +102,100 @@ void dfree(T*& p) {
   p = nullptr;
 }
 
-__global__ void gather_degrees_kernel(const uint64_t* off, const uint32_t* ids,
-                                      uint32_t n, uint64_t* out) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += gridDim.x * blockDim.x) {
-    const uint32_t v = ids[i];
-    out[i] = off[v + 1] - off[v];
+// Hub plan totals, written after the class counts (cls_count[0..8]) so one
+// copy brings both to the host: [10] dispatch chunks, [11] move units,
+// [12..13] staged entries (u64), [14..15] chunk-table words (u64).
+constexpr int kHubTotals = 10;
+
+// The hub plan of a level on the device (one block).  For every hub
+// (class 8 of the degree partition, order[hs .. hs + hc)): its dispatch
+// chunks of kHubChunk entries, its hash partitions (move units: about
+// kHubPartKeys distinct communities each, at most kHubMaxParts), and its
+// offsets in the staging copy and the chunk table, all as exclusive scans
+// over the hubs.  `cap` is the capacity of the per-hub arrays; a level
+// with more hubs writes no plan and leaves the totals at ~0 (the host
+// reports it).
+__global__ void __launch_bounds__(1024)
+    hub_plan_kernel(const uint64_t* __restrict__ off, const uint32_t* __restrict__ order,
+                    uint32_t* cls_count, uint32_t n, uint32_t cap, uint32_t* chunk_start,
+                    uint32_t* unit_start, uint32_t* nparts, uint64_t* stage_off,
+                    uint64_t* ct_off) {
+  __shared__ unsigned long long sh[33];
+  uint32_t hs = 0;
+  for (int c = 0; c < 8; c++) hs += cls_count[c];
+  const uint32_t hc = cls_count[8];
+  uint64_t* tot64 = reinterpret_cast<uint64_t*>(cls_count + 12);
+  if (hc > cap) {
+    if (threadIdx.x == 0) {
+      cls_count[kHubTotals] = cls_count[kHubTotals + 1] = ~0u;
+      tot64[0] = tot64[1] = ~0ull;
+    }
+    return;
+  }
+  unsigned long long c_chunks = 0, c_units = 0, c_stage = 0, c_ct = 0, t;
+  for (uint32_t base = 0; base < hc; base += blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    unsigned long long d = 0, nch = 0, np = 0;
+    if (i < hc) {
+      const uint32_t v = order[hs + i];
+      d = off[v + 1] - off[v];
+      nch = (d + kHubChunk - 1) / kHubChunk;
+      const unsigned long long distinct = d < n ? d : n;
+      np = (distinct + kHubPartKeys - 1) / kHubPartKeys;
+      np = np < 1 ? 1 : (np > kHubMaxParts ? kHubMaxParts : np);
+    }
+    const unsigned long long ct = nch * (np + 1);
+    const unsigned long long x_ch = block_exclusive_scan(nch, sh, &t);
+    const unsigned long long s_ch = c_chunks;
+    c_chunks += t;
+    const unsigned long long x_u = block_exclusive_scan(np, sh, &t);
+    const unsigned long long s_u = c_units;
+    c_units += t;
+    const unsigned long long x_st = block_exclusive_scan(d, sh, &t);
+    const unsigned long long s_st = c_stage;
+    c_stage += t;
+    const unsigned long long x_ct = block_exclusive_scan(ct, sh, &t);
+    const unsigned long long s_ct = c_ct;
+    c_ct += t;
+    if (i < hc) {
+      chunk_start[i] = (uint32_t)(s_ch + x_ch);
+      unit_start[i] = (uint32_t)(s_u + x_u);
+      nparts[i] = (uint32_t)np;
+      stage_off[i] = s_st + x_st;
+      ct_off[i] = s_ct + x_ct;
+    }
+  }
+  if (threadIdx.x == 0) {
+    chunk_start[hc] = (uint32_t)c_chunks;
+    unit_start[hc] = (uint32_t)c_units;
+    cls_count[kHubTotals] = (uint32_t)c_chunks;
+    cls_count[kHubTotals + 1] = (uint32_t)c_units;
+    tot64[0] = c_stage;
+    tot64[1] = c_ct;
+  }
+}
+
+// The hub plan's maps (a warp per hub): dispatch chunk -> (hub, chunk) in
+// hub_map[0 .. hb) and hub_map[hb .. 2 hb); move unit -> (hub, partition,
+// partitions of the hub).
+__global__ void hub_fill_kernel(uint32_t hc, uint32_t hb, const uint32_t* __restrict__ chunk_start,
+                                const uint32_t* __restrict__ unit_start,
+                                const uint32_t* __restrict__ nparts, uint32_t* hub_map,
+                                uint32_t* unit_hub, uint32_t* unit_part, uint32_t* unit_np) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < hc; i += warps) {
+    const uint32_t c0 = chunk_start[i], c1 = chunk_start[i + 1];
+    for (uint32_t j = c0 + lane; j < c1; j += 32) {
+      hub_map[j] = i;
+      hub_map[hb + j] = j - c0;
+    }
+    const uint32_t u0 = unit_start[i], np = nparts[i];
+    for (uint32_t p = lane; p < np; p += 32) {
+      unit_hub[u0 + p] = i;
+      unit_part[u0 + p] = p;
+      unit_np[u0 + p] = np;
+    }
   }
 }
 
@@ -263,7 +351,7 @@ struct lv_engine {
   HubArena hub;
   size_t hub_count_cap = 0, hub_blocks_cap = 0, hub_units_cap = 0;
   size_t hub_stage_cap = 0, hub_ct_cap = 0;
-  uint64_t* hub_deg = nullptr;
+  uint32_t* hub_chunk_start = nullptr;  // [hub cap + 1] first dispatch chunk per hub
 
   ContractBuffers cb{};
   ScanScratch scan;
@@ -500,7 +588,7 @@ void free_state(lv_engine* E) {
   dfree(E->hub.unit_g);
   dfree(E->hub.unit_c);
   dfree(E->hub.unit_start);
-  dfree(E->hub_deg);
+  dfree(E->hub_chunk_start);
   ContractBuffers& B = E->cb;
   dfree(B.flag_id);
   dfree(B.mem_off);
@@ -523,6 +611,7 @@ void free_state(lv_engine* E) {
   dfree(B.g_tab_size);
   dfree(B.g_blk_comm);
   dfree(B.g_blk_chunk);
+  dfree(B.g_blk_first);
   B.table_cap = 0;
   B.g_cap = 0;
   if (E->scan.buf) cudaFree(E->scan.buf);
@@ -570,6 +659,7 @@ cudaError_t grow_tables(void* ctx, size_t slots, size_t entries) {
     dfree(B.g_tab_size);
     dfree(B.g_blk_comm);
     dfree(B.g_blk_chunk);
+    dfree(B.g_blk_first);
     size_t cap = std::max<size_t>(entries, 1024);
     cudaError_t e = dalloc(&B.g_tab_off, cap);
     if (e != cudaSuccess) return e;
@@ -578,6 +668,8 @@ cudaError_t grow_tables(void* ctx, size_t slots, size_t entries) {
     e = dalloc(&B.g_blk_comm, cap);
     if (e != cudaSuccess) return e;
     e = dalloc(&B.g_blk_chunk, 2 * cap);
+    if (e != cudaSuccess) return e;
+    e = dalloc(&B.g_blk_first, cap + 1);
     if (e != cudaSuccess) return e;
     B.g_cap = cap;
   }
@@ -675,35 +767,17 @@ lv_status prepare_level(lv_engine* E, bool sync_scalars = true) {
   drop_pass_graph(E);
   CU(partition_by_degree(E->off(), n, E->order, E->cls_count, E->part_tmp,
                          E->scan, st));
-  CU(cudaMemcpyAsync(E->h_counts, E->cls_count, kClasses * sizeof(uint32_t),
-                     cudaMemcpyDeviceToHost, st));
-  if (E->agg_pending) {  // the previous contraction's reads ride on this sync
-    CU(cudaMemcpyAsync(E->h_pending, E->cb.counts + 8, sizeof(uint64_t), cudaMemcpyDeviceToHost,
-                       st));
-    CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost, st));
-  }
-  CU(counted_sync(st));
-  LVTRY(finish_pending(E));
-  g_trace.mark("  degree classes", (uint32_t)E->levels.size(), n);
-  DispatchPlan& P = E->plan;
-  memset(&P, 0, sizeof(P));
-  P.cls_start[0] = 0;
-  for (int c = 0; c < kClasses; c++) P.cls_start[c + 1] = P.cls_start[c] + E->h_counts[c];
-  const uint32_t hs = P.cls_start[8];
-  const uint32_t hc = P.cls_start[9] - hs;
-  // hub plan: dispatch chunks (row sums, modularity) of kHubChunk entries,
-  // and move units (hub, hash partition of about kHubPartKeys communities)
-  std::vector<uint32_t> blk_vertex, blk_chunk;            // dispatch chunks
-  std::vector<uint32_t> unit_vertex, unit_part, unit_np;  // move units
-  std::vector<uint32_t> hub_np;                           // partitions per hub
-  std::vector<uint32_t> hub_u0;                           // first move unit per hub
-  std::vector<uint64_t> hub_stage, hub_ct;                // staging / chunk-table offsets
-  uint64_t stage_total = 0, ct_total = 0;
-  if (hc) {
-    if (hc > E->hub_count_cap) {
+  // The hub plan is built on the device and its totals ride on the class
+  // counts' copy.  Its per-hub arrays are sized for the most hubs the level
+  // can hold: a hub has more than kHubSmemMaxDeg entries, and E->e (the
+  // previous level's entry count while a contraction's reads are pending)
+  // bounds the level's entries.  A level with more hubs than that (a union
+  // that gained graphs) plans again after the copy.
+  HubArena& H = E->hub;
+  auto plan_hubs = [&](uint64_t cap) -> lv_status {
+    if (cap > E->hub_count_cap) {
       E->hub_count_cap = 0;  // zeroed before the frees (see grow_tables)
-      HubArena& H = E->hub;
-      dfree(E->hub_deg);
+      dfree(E->hub_chunk_start);
       dfree(H.best);
       dfree(H.own);
       dfree(H.hot);
@@ -712,49 +786,59 @@ lv_status prepare_level(lv_engine* E, bool sync_scalars = true) {
       dfree(H.stage_off);
       dfree(H.ct_off);
       dfree(H.unit_start);
-      CU(dalloc(&E->hub_deg, hc));
-      CU(dalloc(&H.unit_start, (size_t)hc + 1));
-      CU(dalloc(&H.best, hc));
-      CU(dalloc(&H.own, hc));
-      CU(dalloc(&H.hot, hc));
-      CU(dalloc(&H.hot_any, hc));
-      CU(dalloc(&H.nparts, hc));
-      CU(dalloc(&H.stage_off, hc));
-      CU(dalloc(&H.ct_off, hc));
-      E->hub_count_cap = hc;
+      CU(dalloc(&E->hub_chunk_start, (size_t)cap + 1));
+      CU(dalloc(&H.unit_start, (size_t)cap + 1));
+      CU(dalloc(&H.best, cap));
+      CU(dalloc(&H.own, cap));
+      CU(dalloc(&H.hot, cap));
+      CU(dalloc(&H.hot_any, cap));
+      CU(dalloc(&H.nparts, cap));
+      CU(dalloc(&H.stage_off, cap));
+      CU(dalloc(&H.ct_off, cap));
+      E->hub_count_cap = cap;
     }
-    (count_launches(1), gather_degrees_kernel<<<(hc + 255) / 256, 256, 0, st>>>(
-        E->off(), E->order + hs, hc, E->hub_deg));
+    (count_launches(1), hub_plan_kernel<<<1, 1024, 0, st>>>(
+        E->off(), E->order, E->cls_count, n, (uint32_t)E->hub_count_cap, E->hub_chunk_start,
+        H.unit_start, H.nparts, H.stage_off, H.ct_off));
     CU(cudaGetLastError());
-    std::vector<uint64_t> deg(hc);
-    CU(cudaMemcpyAsync(deg.data(), E->hub_deg, hc * sizeof(uint64_t),
+    return LV_OK;
+  };
+  const uint64_t hub_bound = std::min<uint64_t>(n, E->e / (kHubSmemMaxDeg + 1));
+  if (hub_bound) LVTRY(plan_hubs(hub_bound));
+  CU(cudaMemcpyAsync(E->h_counts, E->cls_count, 16 * sizeof(uint32_t),
+                     cudaMemcpyDeviceToHost, st));
+  if (E->agg_pending) {  // the previous contraction's reads ride on this sync
+    CU(cudaMemcpyAsync(E->h_pending, E->cb.counts + 8, sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                       st));
+    CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost, st));
+  }
+  CU(counted_sync(st));
+  LVTRY(finish_pending(E));
+  const uint32_t hc = E->h_counts[8];
+  if (hc && (!hub_bound || hc > E->hub_count_cap)) {
+    LVTRY(plan_hubs(hc));
+    CU(cudaMemcpyAsync(E->h_counts, E->cls_count, 16 * sizeof(uint32_t),
                        cudaMemcpyDeviceToHost, st));
     CU(counted_sync(st));
-    for (uint32_t i = 0; i < hc; i++) {
-      const uint32_t nch = (uint32_t)((deg[i] + kHubChunk - 1) / kHubChunk);
-      for (uint32_t ch = 0; ch < nch; ch++) {
-        blk_vertex.push_back(i);
-        blk_chunk.push_back(ch);
-      }
-      const uint64_t distinct = std::min<uint64_t>(deg[i], n);
-      const uint32_t np = (uint32_t)std::min<uint64_t>(
-          kHubMaxParts, std::max<uint64_t>(1, (distinct + kHubPartKeys - 1) / kHubPartKeys));
-      for (uint32_t p = 0; p < np; p++) {  // a hub's partitions are adjacent
-        unit_vertex.push_back(i);
-        unit_part.push_back(p);
-        unit_np.push_back(np);
-      }
-      hub_np.push_back(np);
-      hub_u0.push_back((uint32_t)(unit_vertex.size() - np));
-      hub_stage.push_back(stage_total);
-      hub_ct.push_back(ct_total);
-      stage_total += deg[i];
-      ct_total += (uint64_t)nch * (np + 1);
-    }
+  }
+  g_trace.mark("  degree classes", (uint32_t)E->levels.size(), n);
+  DispatchPlan& P = E->plan;
+  memset(&P, 0, sizeof(P));
+  P.cls_start[0] = 0;
+  for (int c = 0; c < kClasses; c++) P.cls_start[c + 1] = P.cls_start[c] + E->h_counts[c];
+  const uint32_t hs = P.cls_start[8];
+  uint32_t hb = 0, hu = 0;
+  uint64_t stage_total = 0, ct_total = 0;
+  if (hc) {
+    hb = E->h_counts[kHubTotals];
+    hu = E->h_counts[kHubTotals + 1];
+    memcpy(&stage_total, E->h_counts + kHubTotals + 2, sizeof(uint64_t));
+    memcpy(&ct_total, E->h_counts + kHubTotals + 4, sizeof(uint64_t));
+    if (hb == ~0u || hu == ~0u) return fail(LV_ERR_LIMIT, "hub plan: capacity exceeded");
   }
   P.hub_count = hc;
-  P.hub_blocks = (uint32_t)blk_vertex.size();
-  E->hub.units = (uint32_t)unit_vertex.size();
+  P.hub_blocks = hb;
+  H.units = hu;
   // dispatch units per class
   uint32_t u = 0;
   for (int c = 1; c <= 7; c++) {
@@ -776,41 +860,27 @@ lv_status prepare_level(lv_engine* E, bool sync_scalars = true) {
     E->partials_cap = need_partials;
   }
   if (hc) {
-    const size_t hb = P.hub_blocks;
-    const size_t hu = E->hub.units;
     if (hb > E->hub_blocks_cap) {
       E->hub_blocks_cap = 0;
       dfree(E->hub_map);
-      CU(dalloc(&E->hub_map, 2 * hb));
+      CU(dalloc(&E->hub_map, 2 * (size_t)hb));
       E->hub_blocks_cap = hb;
     }
     if (hu > E->hub_units_cap) {
       E->hub_units_cap = 0;
-      dfree(E->hub.blk_vertex);
-      dfree(E->hub.blk_chunk);
-      dfree(E->hub.blk_nchunks);
-      dfree(E->hub.unit_g);
-      dfree(E->hub.unit_c);
-      CU(dalloc(&E->hub.blk_vertex, hu));
-      CU(dalloc(&E->hub.blk_chunk, hu));
-      CU(dalloc(&E->hub.blk_nchunks, hu));
-      CU(dalloc(&E->hub.unit_g, hu));
-      CU(dalloc(&E->hub.unit_c, hu));
+      dfree(H.blk_vertex);
+      dfree(H.blk_chunk);
+      dfree(H.blk_nchunks);
+      dfree(H.unit_g);
+      dfree(H.unit_c);
+      CU(dalloc(&H.blk_vertex, hu));
+      CU(dalloc(&H.blk_chunk, hu));
+      CU(dalloc(&H.blk_nchunks, hu));
+      CU(dalloc(&H.unit_g, hu));
+      CU(dalloc(&H.unit_c, hu));
       E->hub_units_cap = hu;
     }
-    std::vector<uint32_t> map(2 * hb);
-    std::copy(blk_vertex.begin(), blk_vertex.end(), map.begin());
-    std::copy(blk_chunk.begin(), blk_chunk.end(), map.begin() + hb);
-    CU(cudaMemcpyAsync(E->hub_map, map.data(), 2 * hb * sizeof(uint32_t),
-                       cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(E->hub.blk_vertex, unit_vertex.data(), hu * sizeof(uint32_t),
-                       cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(E->hub.blk_chunk, unit_part.data(), hu * sizeof(uint32_t),
-                       cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(E->hub.blk_nchunks, unit_np.data(), hu * sizeof(uint32_t),
-                       cudaMemcpyHostToDevice, st));
-    // split/merge plan: partitions, staging copy of the hub rows, chunk table
-    HubArena& H = E->hub;
+    // split/merge plan: staging copy of the hub rows, chunk table
     if (stage_total > E->hub_stage_cap) {
       E->hub_stage_cap = 0;
       dfree(H.stage);
@@ -823,15 +893,10 @@ lv_status prepare_level(lv_engine* E, bool sync_scalars = true) {
       CU(dalloc(&H.ct, ct_total));
       E->hub_ct_cap = ct_total;
     }
-    CU(cudaMemcpyAsync(H.nparts, hub_np.data(), hc * sizeof(uint32_t), cudaMemcpyHostToDevice,
-                       st));
-    hub_u0.push_back((uint32_t)hu);
-    CU(cudaMemcpyAsync(H.unit_start, hub_u0.data(), ((size_t)hc + 1) * sizeof(uint32_t),
-                       cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(H.stage_off, hub_stage.data(), hc * sizeof(uint64_t),
-                       cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(H.ct_off, hub_ct.data(), hc * sizeof(uint64_t), cudaMemcpyHostToDevice,
-                       st));
+    (count_launches(1), hub_fill_kernel<<<std::min<uint32_t>((hc + 7) / 8, 1184), 256, 0, st>>>(
+        hc, hb, E->hub_chunk_start, H.unit_start, H.nparts, E->hub_map, H.blk_vertex,
+        H.blk_chunk, H.blk_nchunks));
+    CU(cudaGetLastError());
     CU(cudaMemsetAsync(H.best, 0, hc * sizeof(unsigned long long), st));
     CU(cudaMemsetAsync(H.own, 0, hc * sizeof(double), st));
     CU(cudaMemsetAsync(H.hot, 0, hc * sizeof(double), st));

@@ -45,6 +45,39 @@ __host__ __device__ inline int move_class_of_degree(uint64_t d) {
                      : 8;
 }
 
+// Exclusive scan of one value per thread over a block of whole warps (at
+// most 1024 threads); *total receives the block's sum.  `sh` is shared
+// scratch of 33 elements.  Every thread of the block must call it.
+template <typename T>
+__device__ __forceinline__ T block_exclusive_scan(T x, T* sh, T* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nw = (int)(blockDim.x >> 5);
+  T inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const T y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) sh[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    const T s = lane < nw ? sh[lane] : T(0);
+    T si = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const T y = __shfl_up_sync(0xffffffffu, si, o);
+      if (lane >= o) si += y;
+    }
+    sh[lane] = si - s;
+    if (lane == 31) sh[32] = si;
+  }
+  __syncthreads();
+  const T r = sh[wid] + inc - x;
+  *total = sh[32];
+  __syncthreads();  // sh may be reused by the next call
+  return r;
+}
+
 constexpr uint32_t kEmptyKey = 0xFFFFFFFFu;
 
 // Decision rules, numbered as lv_rule in the C ABI.
@@ -509,7 +542,8 @@ struct ContractBuffers {
   uint64_t* g_tab_off;   // [cap] per class-G community table offset
   uint32_t* g_tab_size;  // [cap]
   uint32_t* g_blk_comm;  // [cap] per block: index in class-G list
-  uint32_t* g_blk_chunk; // [cap]
+  uint32_t* g_blk_chunk; // [2 cap] per block: chunk, then chunks of its community
+  uint32_t* g_blk_first; // [cap + 1] per class-G community: first block
   size_t g_cap;          // entries available in the g_* arrays
 };
 constexpr uint64_t kMergeWarpMax = 128;    // entries: warp per community
@@ -539,10 +573,11 @@ cudaError_t contract_level_sort(const LevelView& L, uint64_t nnz, ContractBuffer
                                 cudaStream_t st);
 // Contracts level (L, comm) into (out_off, out_col, out_w); writes cnew
 // (vertex -> new id) for composing the assignment.  Synchronises the
-// stream once for the class sizes (the new vertex count comes with them);
-// with defer_total the new entry count is left at B.counts + 8 (u64) for
-// the caller's next synchronisation (res->new_nnz = ~0), else it is read
-// with a second one.
+// stream once for the class sizes (the new vertex count and the plan of the
+// multi-block class, built on the device, come with them); with
+// defer_total the new entry count is left at B.counts + 8 (u64) for the
+// caller's next synchronisation (res->new_nnz = ~0), else it is read with a
+// second one.
 cudaError_t contract_level(const LevelView& L, uint64_t nnz,
                            ContractBuffers& B, ScanScratch& S,
                            uint64_t* out_off, uint32_t* out_col, float* out_w,
