@@ -811,15 +811,35 @@ cudaError_t configure_contract_kernels() {
     if (e_ != cudaSuccess) return e_;          \
   } while (0)
 
-cudaError_t contract_level(const LevelView& L, uint64_t nnz,
-                           ContractBuffers& B, ScanScratch& S,
-                           uint64_t* out_off, uint32_t* out_col, float* out_w,
-                           ContractResult* res, cudaStream_t st,
-                           cudaError_t (*grow)(void*, size_t, size_t),
-                           void* grow_ctx, bool defer_total) {
-  const uint32_t n = L.n;
-  uint32_t* h_counts = B.host_counts;
+namespace {
 
+// The class-G plan on the device with arrays of capacity >= cap: table
+// offsets and sizes, first block of every community, the block map.
+cudaError_t plan_g(ContractBuffers& B, uint64_t nnz, uint64_t cap, cudaStream_t st,
+                   cudaError_t (*grow)(void*, size_t, size_t), void* grow_ctx) {
+  if (cap > B.g_cap) LV_TRY(grow(grow_ctx, 0, cap));
+  (count_launches(1), g_plan_kernel<<<1, 1024, 0, st>>>(B.comm_deg, B.comm_cls, B.counts,
+                                                        B.g_cap, B.g_tab_off, B.g_tab_size,
+                                                        B.g_blk_first));
+  LV_TRY(cudaGetLastError());
+  (count_launches(1), g_fill_kernel<<<gridcap((nnz / (kMergeBlockMax + 1) + 8) / 8, 8),
+                                      kThreads, 0, st>>>(B.counts, B.g_blk_first, B.g_blk_comm,
+                                                         B.g_blk_chunk));
+  return cudaGetLastError();
+}
+
+// The class-G arrays hold the plan when they have room for the most a
+// level of nnz entries can need: a class-G community has more than
+// kMergeBlockMax entries and its blocks cover its entries in kMergeChunk
+// pieces, of the level's nnz in all.
+uint64_t g_bound_of(uint64_t nnz) { return nnz / (kMergeBlockMax + 1) + nnz / kMergeChunk + 1; }
+
+}  // namespace
+
+cudaError_t contract_front(const LevelView& L, uint64_t nnz, ContractBuffers& B,
+                           ScanScratch& S, cudaStream_t st,
+                           cudaError_t (*grow)(void*, size_t, size_t), void* grow_ctx) {
+  const uint32_t n = L.n;
   const unsigned g1 = gridcap((n + 255) / 256, 8);
   (count_launches(1), flags_kernel<<<g1, 256, 0, st>>>(L.comm_sz, n, B.flag_id, B.mem_off, B.cursor));
   LV_TRY(cudaGetLastError());
@@ -840,27 +860,19 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
   LV_TRY(cudaGetLastError());
   LV_TRY(partition_by_size4(B.comm_deg, n, B.counts + 0, kMergeWarpMax, kMergeMidMax,
                             kMergeBlockMax, B.comm_cls, B.counts + 4, B.tmp, S, st));
-  // class-G plan on the device, its totals copied with the class sizes.
-  // Its arrays are sized for the most the level can need: a class-G
-  // community has more than kMergeBlockMax entries and its blocks cover
-  // its entries in kMergeChunk pieces, of the level's nnz in all.
-  auto plan_g = [&](uint64_t cap) -> cudaError_t {
-    if (cap > B.g_cap) LV_TRY(grow(grow_ctx, 0, cap));
-    (count_launches(1), g_plan_kernel<<<1, 1024, 0, st>>>(B.comm_deg, B.comm_cls, B.counts,
-                                                          B.g_cap, B.g_tab_off, B.g_tab_size,
-                                                          B.g_blk_first));
-    LV_TRY(cudaGetLastError());
-    (count_launches(1), g_fill_kernel<<<gridcap(((uint64_t)nnz / (kMergeBlockMax + 1) + 8) / 8, 8),
-                                        kThreads, 0, st>>>(B.counts, B.g_blk_first, B.g_blk_comm,
-                                                           B.g_blk_chunk));
-    return cudaGetLastError();
-  };
-  const uint64_t g_bound = nnz / (kMergeBlockMax + 1) + nnz / kMergeChunk + 1;
+  // class-G plan on the device, its totals copied with the class sizes
+  if (nnz > kMergeBlockMax) LV_TRY(plan_g(B, nnz, g_bound_of(nnz), st, grow, grow_ctx));
+  return cudaMemcpyAsync(B.host_counts, B.counts, 16 * sizeof(uint32_t),
+                         cudaMemcpyDeviceToHost, st);
+}
+
+cudaError_t contract_back(const LevelView& L, uint64_t nnz, ContractBuffers& B,
+                          ScanScratch& S, uint64_t* out_off, uint32_t* out_col,
+                          float* out_w, ContractResult* res, cudaStream_t st,
+                          cudaError_t (*grow)(void*, size_t, size_t), void* grow_ctx,
+                          bool defer_total) {
+  uint32_t* h_counts = B.host_counts;
   const bool g_planned = nnz > kMergeBlockMax;
-  if (g_planned) LV_TRY(plan_g(g_bound));
-  LV_TRY(cudaMemcpyAsync(h_counts, B.counts, 16 * sizeof(uint32_t),
-                         cudaMemcpyDeviceToHost, st));
-  LV_TRY(counted_sync(st));
   const uint32_t new_n = h_counts[0];
   const uint32_t cntW = h_counts[4], cntM = h_counts[5], cntB2 = h_counts[6];
   const uint32_t cntB = cntM + cntB2;  // both block classes
@@ -869,7 +881,8 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
   // again with twice the room until the plan fits
   for (int tries = 0; cntG && (!g_planned || h_counts[kGTotals] == ~0u); tries++) {
     if (tries == 40) return cudaErrorInvalidValue;
-    LV_TRY(plan_g(std::max<uint64_t>(2 * (uint64_t)B.g_cap, (uint64_t)cntG + 1)));
+    LV_TRY(plan_g(B, nnz, std::max<uint64_t>(2 * (uint64_t)B.g_cap, (uint64_t)cntG + 1), st,
+                  grow, grow_ctx));
     LV_TRY(cudaMemcpyAsync(h_counts, B.counts, 16 * sizeof(uint32_t),
                            cudaMemcpyDeviceToHost, st));
     LV_TRY(counted_sync(st));
@@ -951,6 +964,18 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
   LV_TRY(counted_sync(st));
   res->new_nnz = *h_total;
   return cudaSuccess;
+}
+
+cudaError_t contract_level(const LevelView& L, uint64_t nnz,
+                           ContractBuffers& B, ScanScratch& S,
+                           uint64_t* out_off, uint32_t* out_col, float* out_w,
+                           ContractResult* res, cudaStream_t st,
+                           cudaError_t (*grow)(void*, size_t, size_t),
+                           void* grow_ctx, bool defer_total) {
+  LV_TRY(contract_front(L, nnz, B, S, st, grow, grow_ctx));
+  LV_TRY(counted_sync(st));
+  return contract_back(L, nnz, B, S, out_off, out_col, out_w, res, st, grow, grow_ctx,
+                       defer_total);
 }
 
 cudaError_t contract_level_sort(const LevelView& L, uint64_t nnz, ContractBuffers& B,

@@ -381,6 +381,9 @@ struct lv_engine {
   bool agg_pending = false;
   cudaEvent_t agg_ev0 = nullptr, agg_ev1 = nullptr;
   uint64_t* h_pending = nullptr;  // pinned: the deferred entry count
+  // the contraction's front was launched behind the level graph and its
+  // class sizes read with the level's result (whole-run loop only)
+  bool front_ready = false;
 
   // kernel timing
   bool profiling = false;
@@ -1047,7 +1050,7 @@ void drop_level_exec(lv_engine* E) {
 // sets the loop condition, so the host waits once per level instead of
 // once per pass.  The kernels read the level from the descriptor, so the
 // graph is captured once and replayed on every later level and run.
-lv_status run_level_graph(lv_engine* E, float min_gain) {
+lv_status run_level_graph(lv_engine* E, float min_gain, bool wait = true) {
   LVTRY(upload_desc(E, min_gain));
   const uint64_t key = level_key(E);
   cudaGraphExec_t exec = nullptr;
@@ -1123,6 +1126,7 @@ lv_status run_level_graph(lv_engine* E, float min_gain) {
   CU(cudaGraphLaunch(exec, E->st));
   CU(cudaMemcpyAsync(E->sc_host, E->sc, sizeof(LevelScalars), cudaMemcpyDeviceToHost,
                      E->st));
+  if (!wait) return LV_OK;  // the caller's next synchronisation reads sc_host
   CU(counted_sync(E->st));
   g_trace.mark("graph run (all passes)", (uint32_t)E->levels.size(), E->n);
   return LV_OK;
@@ -2094,12 +2098,19 @@ lv_status lv_engine_load_device(lv_engine* E, uint32_t n, uint64_t nnz,
   return load_common(E, n, nnz);
 }
 
-lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
+// A level's move phase.  With `speculate` (the whole-run loop of a single
+// graph), the contraction's front is launched behind the level graph
+// before its result is known, and one synchronisation reads both: the
+// level's scalars and the contraction's class sizes.  A level that moved
+// nothing drops the front (it wrote only contraction scratch).
+static lv_status phase_move(lv_engine* E, float min_gain, int* more, double* q,
+                            bool speculate) {
   AllocScope alloc_scope(E);
   if (!E) return fail(LV_ERR_ARG, "NULL engine");
   if (!E->loaded) return fail(LV_ERR_STATE, "no graph loaded");
   if (E->finished) return fail(LV_ERR_STATE, "the run has ended; load a graph again");
   cudaSetDevice(E->device);
+  E->front_ready = false;
   CU(cudaEventRecord(E->ev0, E->st));
   g_trace.reset();
   // the level graph reads the level's m and initial Q on the device and the
@@ -2112,7 +2123,15 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
   lv_level_info info{};
   info.n_vertices = E->n;
   info.n_entries = E->e;
-  if (graph_path) LVTRY(run_level_graph(E, min_gain));  // reads sc_host
+  const bool spec = speculate && graph_path && !E->batch && !E->cfg.contract_sort;
+  if (graph_path) LVTRY(run_level_graph(E, min_gain, !spec));  // reads sc_host
+  if (spec) {
+    CU(cudaEventRecord(E->ev1, E->st));  // the level's end
+    CU(cudaEventRecord(E->agg_ev0, E->st));
+    CU(contract_front(E->view(), E->e, E->cb, E->scan, E->st, grow_tables, E));
+    CU(counted_sync(E->st));
+    E->front_ready = true;
+  }
   const double m64 = E->sc_host->m64;
   double act = graph_path ? E->sc_host->q_start : E->sc_host->q, old = act;
   info.q_start = act;
@@ -2156,7 +2175,8 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
     } while (act - old >= (double)min_gain && passes < E->cfg.max_passes);
   }
   E->accepted = ret != 0;  // modularity.cu:515-517 (applied at aggregation)
-  CU(cudaEventRecord(E->ev1, E->st));
+  if (!ret) E->front_ready = false;
+  if (!spec) CU(cudaEventRecord(E->ev1, E->st));
   CU(cudaEventSynchronize(E->ev1));
   float ms = 0.0f, prep_ms = 0.0f;
   cudaEventElapsedTime(&ms, E->ev0, E->ev1);
@@ -2173,6 +2193,10 @@ lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
   if (more) *more = ret;
   if (q) *q = E->q_last;
   return LV_OK;
+}
+
+lv_status lv_phase_move(lv_engine* E, float min_gain, int* more, double* q) {
+  return phase_move(E, min_gain, more, q, false);
 }
 
 // Entry-sized buffers of the contraction by sorting, grown on demand.
@@ -2210,7 +2234,9 @@ lv_status lv_phase_aggregate(lv_engine* E) {
   // a single graph outside profiling defers the reads that follow the
   // contraction to the next level's first synchronisation
   const bool defer = !E->batch && !E->profiling && !E->cfg.contract_sort;
-  CU(cudaEventRecord(defer ? E->agg_ev0 : E->ev0, E->st));
+  const bool front = E->front_ready;  // launched and read with the level's result
+  E->front_ready = false;
+  if (!front) CU(cudaEventRecord(defer ? E->agg_ev0 : E->ev0, E->st));
   const int next = (E->cur == 0) ? 1 : 0;
   ContractResult r{};
   cudaEvent_t t0 = prof_begin(E);
@@ -2219,6 +2245,9 @@ lv_status lv_phase_aggregate(lv_engine* E) {
     LVTRY(ensure_sort_buffers(E, E->e));
     CU(contract_level_sort(E->view(), E->e, E->cb, E->sb, E->scan, E->c_off[next],
                            E->c_col[next], E->c_w[next], &r, E->st));
+  } else if (front) {
+    CU(contract_back(E->view(), E->e, E->cb, E->scan, E->c_off[next], E->c_col[next],
+                     E->c_w[next], &r, E->st, grow_tables, E, defer));
   } else {
     CU(contract_level(E->view(), E->e, E->cb, E->scan, E->c_off[next], E->c_col[next],
                       E->c_w[next], &r, E->st, grow_tables, E, defer));
@@ -2268,7 +2297,7 @@ static lv_status run_loaded(lv_engine* E, float min_gain, lv_result* res) {
   uint64_t processed = 0;
   for (;;) {
     int more = 0;
-    lv_status s = lv_phase_move(E, min_gain, &more, &q);
+    lv_status s = phase_move(E, min_gain, &more, &q, true);
     if (s != LV_OK) {
       cudaEventDestroy(a0);
       cudaEventDestroy(a1);

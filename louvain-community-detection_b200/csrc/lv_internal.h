@@ -586,5 +586,20 @@ cudaError_t contract_level(const LevelView& L, uint64_t nnz,
                            cudaError_t (*grow)(void* ctx, size_t slots,
                                                size_t entries),
                            void* grow_ctx, bool defer_total);
+// contract_level in two halves around its one synchronisation: the front
+// launches everything up to the class sizes and the multi-block plan and
+// queues their copy into B.host_counts; the back, called once the stream
+// has been synchronised after the front, launches the merges and the new
+// CSR.  A caller may put other work and copies between the two and share
+// the synchronisation.
+cudaError_t contract_front(const LevelView& L, uint64_t nnz, ContractBuffers& B,
+                           ScanScratch& S, cudaStream_t st,
+                           cudaError_t (*grow)(void* ctx, size_t slots, size_t entries),
+                           void* grow_ctx);
+cudaError_t contract_back(const LevelView& L, uint64_t nnz, ContractBuffers& B,
+                          ScanScratch& S, uint64_t* out_off, uint32_t* out_col,
+                          float* out_w, ContractResult* res, cudaStream_t st,
+                          cudaError_t (*grow)(void* ctx, size_t slots, size_t entries),
+                          void* grow_ctx, bool defer_total);
 
 }  // namespace lvb

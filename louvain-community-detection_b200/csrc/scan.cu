@@ -56,7 +56,7 @@ __device__ __forceinline__ T block_exclusive(T (&v)[ITEMS], T* warp_sums) {
 
 template <typename T>
 __global__ void __launch_bounds__(kScanThreads)
-    scan_tiles_kernel(const T* in, T* out, size_t n, T* tile_sums) {
+    scan_tiles_kernel(const T* in, T* out, size_t n, T* tile_sums, T* single_total) {
   __shared__ T warp_sums[kScanThreads / 32];
   const size_t base = (size_t)blockIdx.x * kTile + (size_t)threadIdx.x * kScanItems;
   T v[kScanItems];
@@ -66,7 +66,10 @@ __global__ void __launch_bounds__(kScanThreads)
 #pragma unroll
   for (int i = 0; i < kScanItems; i++)
     if (base + i < n) out[base + i] = v[i];
-  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+  if (threadIdx.x == 0) {
+    tile_sums[blockIdx.x] = total;
+    if (single_total) *single_total = total;  // a one-tile scan's total
+  }
 }
 
 template <typename T>
@@ -77,11 +80,6 @@ __global__ void __launch_bounds__(kScanThreads)
 #pragma unroll
   for (int i = 0; i < kScanItems; i++)
     if (base + i < n) out[base + i] += add;
-}
-
-template <typename T>
-__global__ void copy_scalar_kernel(const T* src, T* dst) {
-  *dst = *src;
 }
 
 template <typename T>
@@ -101,13 +99,11 @@ cudaError_t scan_rec(const T* in, T* out, size_t n, T* total, T* scratch,
   const size_t nt = tiles_of(n);
   if (nt > scratch_elems) return cudaErrorInvalidValue;
   T* sums = scratch;
-  (count_launches(1), scan_tiles_kernel<T><<<(unsigned)nt, kScanThreads, 0, st>>>(in, out, n, sums));
+  (count_launches(1), scan_tiles_kernel<T><<<(unsigned)nt, kScanThreads, 0, st>>>(
+                          in, out, n, sums, nt == 1 ? total : nullptr));
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  if (nt == 1) {
-    if (total) (count_launches(1), copy_scalar_kernel<T><<<1, 1, 0, st>>>(sums, total));
-    return cudaGetLastError();
-  }
+  if (nt == 1) return cudaSuccess;
   e = scan_rec<T>(sums, sums, nt, total, scratch + nt, scratch_elems - nt, st);
   if (e != cudaSuccess) return e;
   (count_launches(1), scan_add_kernel<T><<<(unsigned)nt, kScanThreads, 0, st>>>(out, n, sums));
@@ -144,9 +140,16 @@ template <int NC, class ClassFn, class ValueFn>
 __global__ void __launch_bounds__(kPartThreads)
     part_scatter_kernel(uint32_t n, ClassFn fn, ValueFn val,
                         const uint32_t* offsets, uint32_t nblocks,
-                        uint32_t* out) {
+                        uint32_t* out, const uint32_t* grand_total,
+                        uint32_t* cls_count) {
   constexpr int W = kPartThreads / 32;
   __shared__ uint32_t wc[NC][W];
+  if (blockIdx.x == 0 && threadIdx.x < NC) {  // the class sizes
+    const int c = threadIdx.x;
+    const uint32_t start = offsets[c * nblocks];
+    const uint32_t end = (c + 1 < NC) ? offsets[(c + 1) * nblocks] : *grand_total;
+    cls_count[c] = end - start;
+  }
   const uint32_t i = blockIdx.x * kPartThreads + threadIdx.x;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   int c = (i < n) ? fn(i) : -1;
@@ -172,18 +175,6 @@ __global__ void __launch_bounds__(kPartThreads)
   }
 }
 
-template <int NC>
-__global__ void part_totals_kernel(const uint32_t* offsets, uint32_t nblocks,
-                                   const uint32_t* grand_total,
-                                   uint32_t* cls_count) {
-  const int c = threadIdx.x;
-  if (c < NC) {
-    uint32_t start = offsets[c * nblocks];
-    uint32_t end = (c + 1 < NC) ? offsets[(c + 1) * nblocks] : *grand_total;
-    cls_count[c] = end - start;
-  }
-}
-
 template <int NC, class ClassFn, class ValueFn>
 cudaError_t partition_impl(uint32_t n, ClassFn fn, ValueFn val, uint32_t* out,
                            uint32_t* cls_count, uint32_t* tmp, ScanScratch& s,
@@ -201,10 +192,8 @@ cudaError_t partition_impl(uint32_t n, ClassFn fn, ValueFn val, uint32_t* out,
   e = exclusive_scan_u32(counts, counts, (size_t)NC * nb, grand, s, st);
   if (e != cudaSuccess) return e;
   (count_launches(1), part_scatter_kernel<NC, ClassFn, ValueFn>
-                         <<<nb, kPartThreads, 0, st>>>(n, fn, val, counts, nb, out));
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  (count_launches(1), part_totals_kernel<NC><<<1, 32, 0, st>>>(counts, nb, grand, cls_count));
+                         <<<nb, kPartThreads, 0, st>>>(n, fn, val, counts, nb, out, grand,
+                                                       cls_count));
   return cudaGetLastError();
 }
 
