@@ -2360,13 +2360,13 @@ lv_status lv_run(lv_engine* E, const lv_graph* g, float min_gain, lv_result* res
     cudaEventDestroy(c1);
     return s;
   }
-  CU(cudaEventRecord(c1, E->st));
-  CU(cudaEventSynchronize(c1));
+  CU(cudaEventRecord(c1, E->st));  // the run starts behind the copies, no host wait
+  s = run_loaded(E, min_gain, res);  // returns after the stream has finished
   float copy = 0.0f;
-  cudaEventElapsedTime(&copy, c0, c1);
+  if (s == LV_OK && cudaEventSynchronize(c1) == cudaSuccess)
+    cudaEventElapsedTime(&copy, c0, c1);
   cudaEventDestroy(c0);
   cudaEventDestroy(c1);
-  s = run_loaded(E, min_gain, res);
   if (s == LV_OK && res) res->copy_ms = copy;
   return s;
 }

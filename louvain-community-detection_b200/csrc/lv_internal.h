@@ -549,7 +549,7 @@ struct ContractBuffers {
 constexpr uint64_t kMergeWarpMax = 128;    // entries: warp per community
 constexpr uint64_t kMergeMidMax = 1024;    // entries: block, 2048-slot table
 constexpr uint64_t kMergeBlockMax = 4096;  // entries: block, 8192-slot table
-constexpr uint32_t kMergeChunk = 8192;     // entries per block, class G
+constexpr uint32_t kMergeChunk = 2048;     // entries per block, class G
 
 struct ContractResult {
   uint32_t new_n;
