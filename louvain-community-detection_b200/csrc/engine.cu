@@ -928,16 +928,17 @@ lv_status prepare_level(lv_engine* E, bool sync_scalars = true) {
     CU(cudaMemcpyAsync(E->class_deg, E->d_class_deg, kClasses * sizeof(uint64_t),
                        cudaMemcpyDeviceToHost, st));
   }
-  // single graph: the row of every entry, for the pass loop's modularity
-  // sweep (kept in the contraction's column scratch until the level ends)
-  if (!E->batch) CU(launch_row_ids(E->off(), n, E->e, E->cb.tcol, st));
-  // row sums, singleton state, m; then Q of the singleton partition
+  // row sums, singleton state, m; then Q of the singleton partition.  A
+  // single graph's level init also writes the row of every entry, for the
+  // pass loop's modularity sweep (kept in the contraction's column scratch
+  // until the level ends), and the incremental sweep's pass-start
+  // communities (singletons)
   const LevelView L = E->view();
   const double Vd = (double)n, Ed = (double)E->e;
   cudaEvent_t t0 = prof_begin(E);
-  CU(launch_level_init(L, E->order, P, hc ? E->hub_map : nullptr, E->partials, st));
-  // the incremental modularity sweep's pass-start communities: singletons
-  if (!E->batch) CU(launch_fill_iota(E->comm_start, n, st));
+  CU(launch_level_init(L, E->order, P, hc ? E->hub_map : nullptr, E->partials,
+                       E->batch ? nullptr : E->cb.tcol, E->batch ? nullptr : E->comm_start,
+                       st));
   prof_end(E, t0, K_LEVEL_INIT, Ed * 4.0 + Vd * 32.0);
   t0 = prof_begin(E);
   CU(launch_modularity(L, E->order, P, hc ? E->hub_map : nullptr, E->partials, st));

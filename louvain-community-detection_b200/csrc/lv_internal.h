@@ -246,10 +246,12 @@ cudaError_t partition_by_size4(const uint64_t* sizes, uint32_t n_upper,
 // ---------------------------------------------------------------------------
 // move.cu
 // ---------------------------------------------------------------------------
-// Row sums k_v, singleton state (comm=id, sizes 1, totals k) and m.
+// Row sums k_v, singleton state (comm=id, sizes 1, totals k) and m; with
+// rowid the row of every entry, with comm_start comm_start[v] = v.
 cudaError_t launch_level_init(const LevelView& L, const uint32_t* order,
                               const DispatchPlan& P, const uint32_t* hub_map,
-                              double* partials, cudaStream_t st);
+                              double* partials, uint32_t* rowid, uint32_t* comm_start,
+                              cudaStream_t st);
 // Modularity of the current state into sc->q (FP64, deterministic).  With
 // ctl->enabled the last block also applies the pass stop rule and sets the
 // graph condition.

@@ -1604,25 +1604,43 @@ __device__ __forceinline__ void dispatch_units(const LevelView& L,
 }
 
 __global__ void __launch_bounds__(kThreads)
-    level_init_kernel(LevelView L, DispatchArgs A) {
+    level_init_kernel(LevelView L, DispatchArgs A, uint32_t* __restrict__ rowid,
+                      uint32_t* __restrict__ comm_start) {
   __shared__ double red[kWarps];
   double part = 0.0;
   dispatch_units(L, A, RowSumOp{}, part, red);
-  // singleton state for a slice of ids (modularity.cu:459-462)
-  const uint32_t chunk = (L.n + gridDim.x - 1) / gridDim.x;
-  const uint32_t c0 = blockIdx.x * chunk;
-  const uint32_t c1 = min(L.n, c0 + chunk);
-  for (uint32_t c = c0 + threadIdx.x; c < c1; c += kThreads) {
-    L.comm[c] = c;
-    L.comm_sz[c] = 1u;
-    if (L.comm_alt) {  // both copies of the state start equal
-      L.comm_alt[c] = c;
-      L.sz_alt[c] = 1u;
+  // singleton state (modularity.cu:459-462), and for a single graph the
+  // pass-start communities of the incremental sweep and the row of every
+  // entry (the pass loop's flat modularity sweep).  A warp takes 32
+  // consecutive ids, a lane each id's state and bounds, then writes the 32
+  // rows' entry rows one row after another, 32 entries per store.
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t step = (uint64_t)gridDim.x * kWarps * 32;
+  for (uint64_t v0 = ((uint64_t)blockIdx.x * kWarps + (threadIdx.x >> 5)) * 32; v0 < L.n;
+       v0 += step) {  // warp-uniform
+    const uint64_t c = v0 + lane;
+    uint64_t s = 0, e = 0;
+    if (c < L.n) {
+      s = L.off[c];
+      e = L.off[c + 1];
+      L.comm[c] = (uint32_t)c;
+      L.comm_sz[c] = 1u;
+      if (L.comm_alt) {  // both copies of the state start equal
+        L.comm_alt[c] = (uint32_t)c;
+        L.sz_alt[c] = 1u;
+      }
+      if (comm_start) comm_start[c] = (uint32_t)c;
+      if (e == s) {
+        L.k[c] = 0.0f;
+        L.tot[c] = 0.0;
+        if (L.tot_alt) L.tot_alt[c] = 0.0;
+      }
     }
-    if (L.off[c + 1] == L.off[c]) {
-      L.k[c] = 0.0f;
-      L.tot[c] = 0.0;
-      if (L.tot_alt) L.tot_alt[c] = 0.0;
+    if (rowid) {
+      for (int i = 0; i < 32; i++) {
+        const uint64_t si = __shfl_sync(kFull, s, i), ei = __shfl_sync(kFull, e, i);
+        for (uint64_t j = si + lane; j < ei; j += 32) rowid[j] = (uint32_t)(v0 + i);
+      }
     }
   }
   if (!publish_and_check_last(part, 0.0, A, L.sc, red)) return;
@@ -2341,9 +2359,11 @@ unsigned dispatch_grid(const DispatchPlan& P) {
 
 cudaError_t launch_level_init(const LevelView& L, const uint32_t* order,
                               const DispatchPlan& P, const uint32_t* hub_map,
-                              double* partials, cudaStream_t st) {
+                              double* partials, uint32_t* rowid, uint32_t* comm_start,
+                              cudaStream_t st) {
   DispatchArgs A = make_args(order, P, hub_map, partials);
-  (count_launches(1), level_init_kernel<<<dispatch_grid(P), kThreads, 0, st>>>(L, A));
+  (count_launches(1), level_init_kernel<<<dispatch_grid(P), kThreads, 0, st>>>(L, A, rowid,
+                                                                             comm_start));
   return cudaGetLastError();
 }
 
