@@ -2289,6 +2289,12 @@ lv_status lv_phase_aggregate(lv_engine* E) {
 }
 
 static lv_status run_loaded(lv_engine* E, float min_gain, lv_result* res) {
+  // a contraction front launched by this loop is consumed by it: never
+  // left for a later entry point, whatever path the loop leaves by
+  struct FrontGuard {
+    lv_engine* E;
+    ~FrontGuard() { E->front_ready = false; }
+  } front_guard{E};
   CU(cudaEventRecord(E->ev0, E->st));
   cudaEvent_t a0, a1;
   CU(cudaEventCreate(&a0));
